@@ -1,0 +1,209 @@
+/*
+ * nicr.h — C-ABI of the B200 Ni–Cr oxidation phase-field solver.
+ *
+ * One opaque handle owns one simulation domain resident in GPU memory (all
+ * fields, trial buffers, budgets). Host buffers passed in or out are owned by
+ * the caller and copied. Every entry point returns an int status (NICR_OK or a
+ * negative/positive code below); no C++ exception crosses this boundary. A
+ * handle is bound to one CUDA device and one stream and is not thread-safe.
+ *
+ * The reference has no FFI: its in-process surface is the C++ class `Model`
+ * that its test drivers reach with `#define main ...; #include` (reference
+ * mpi3d-slab/tests/regression_driver.cpp:1-8). Each entry point below names the
+ * Model member it replaces (2D = mpi2d/NiCr2D_grains.cpp,
+ * 3S = mpi3d-slab/NiCr3D_grains.cpp). Field data are exchanged in the
+ * reference's interior order: X slowest, Z fastest in 3D (3S:165-167); X
+ * slowest, Y fastest in 2D (2D:149); ghost layers are never exchanged.
+ */
+#ifndef NICR_H
+#define NICR_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (replacing std::runtime_error, 3S:117-127) ---------------- */
+enum {
+    NICR_OK = 0,
+    NICR_ERR_INVALID_ARG = 1,       /* bad parameter / bounds (parse 3S:1055-1081) */
+    NICR_ERR_TRIAL_NONFINITE = 2,   /* "Nonfinite trial field" (3S:790)            */
+    NICR_ERR_TRIAL_BOUNDS = 3,      /* "Out-of-bounds trial at" (3S:799-804)       */
+    NICR_ERR_ETA_RANGE = 4,         /* "Eta trial outside [0,1]" (3S:518-523)      */
+    NICR_ERR_CUDA = 5,              /* CUDA runtime failure                         */
+    NICR_ERR_NO_DEVICE = 6,         /* no usable CUDA device / extension missing    */
+    NICR_ERR_STATE = 7,             /* call not valid in the handle's state         */
+    NICR_ERR_IO = 8                 /* output file could not be written             */
+};
+
+/* ---- enumerations of the reference's string options (3S:56-58) ------------- */
+enum { NICR_BC_CONCENTRATION = 0, NICR_BC_MU = 1, NICR_BC_CLOSED = 2 };
+enum { NICR_CK_LEGACY = 0, NICR_CK_OFF = 1 };
+enum { NICR_BOUNDS_STOP = 0, NICR_BOUNDS_LEGACY = 1 };
+enum { NICR_NUC_KSP = 0, NICR_NUC_CENTER = 1, NICR_NUC_OFF = 2 };
+/* Arithmetic form. FP64 is the drop-in: the same IEEE operations in the same
+ * order as the reference, so single-process results are bit-identical.       */
+enum { NICR_FP64 = 0 };
+
+/* ---- configuration: struct Config + struct Physics (3S:43-79, 2D:39-71) ---- */
+typedef struct nicr_config {
+    int dim;                      /* 2 (mpi2d) or 3 (mpi3d-slab)                */
+    int nx, ny, nz;               /* cells; nz ignored when dim == 2            */
+    int steps, output_every;      /* run-loop controls (CLI level)              */
+    int left_edge_sites;          /* --left-edge-sites / --left-face-sites      */
+    int max_eta_fields;           /* --max-eta-fields                           */
+    unsigned long long random_seed;
+    double dx, dy, dz, dt;
+    double grain_diameter_grid, gb_fwhm_grid;
+    double gb_factor_o, gb_factor_cr;
+    double radius_grid, exclusion_gap_grid, nucleation_period;
+    double mu_res, surface_c_ref;
+    int bc, ck, bounds, nucleation;   /* NICR_BC_*, NICR_CK_*, NICR_BOUNDS_*, NICR_NUC_* */
+    int grains, oxygen_diffusion, grain_evolution, frozen_eta_cache;
+    double eta_W, eta_kappa, eta_L, eta_oxide_penalty;
+    int eta_output_all;           /* --eta-output all (1) | summary (0)         */
+    int output_vti;               /* 3D --output-format vti (1) | vtk (0)       */
+    int output_float64;           /* 3D --output-precision float64 (1) | float32 */
+    int compression_level;        /* 3D --compression-level 0..9                */
+    /* Physics constants that the reference fixes as constexpr (3S:73-79). The
+     * defaults reproduce it; a parameter sweep may change them per run.       */
+    double ksp;                   /* Physics::ksp    = 1.28e-7                  */
+    double bulk_cr;               /* Physics::bulkCr = 0.1986                   */
+    double layer_o;               /* Physics::layerO = 0.0023                   */
+    int precision;                /* NICR_FP64                                  */
+    int device;                   /* CUDA device ordinal                        */
+    int reserved[6];
+} nicr_config;
+
+/* Fills the reference defaults for dim 2 or 3 (Config{} at 2D:39 / 3S:43). */
+void nicr_config_default(nicr_config* cfg, int dim);
+
+/* Parses the reference's command-line flags into cfg (parse, 2D:718-790 /
+ * 3S:986-1082), with the same validation and messages. Returns NICR_OK,
+ * NICR_ERR_INVALID_ARG (message in err), or 100 for --help/--version (text in
+ * err). out_dir receives --out; self_test receives --self-test.               */
+int nicr_config_parse(nicr_config* cfg, int dim, int argc, const char* const* argv,
+                      char* out_dir, size_t out_dir_len, int* self_test,
+                      char* err, size_t err_len);
+
+/* ---- fields --------------------------------------------------------------- */
+enum {
+    NICR_FIELD_O = 0,        /* Model::o              */
+    NICR_FIELD_CR = 1,       /* Model::cr             */
+    NICR_FIELD_PHI = 2,      /* Model::p              */
+    NICR_FIELD_ETA = 3,      /* Model::eta[index]     */
+    NICR_FIELD_MU_O = 4,     /* Model::muO  (after nicr_refresh)            */
+    NICR_FIELD_MU_CR = 5,    /* Model::muCr (after nicr_refresh)            */
+    NICR_FIELD_M_O = 6,      /* Model::mo   (after nicr_refresh)            */
+    NICR_FIELD_M_CR = 7,     /* Model::mc   (after nicr_refresh)            */
+    NICR_FIELD_GB = 8,       /* Model::gb  (Voronoi mask or eta-derived)    */
+    NICR_FIELD_GRAIN = 9,    /* Model::grain (initial Voronoi id, 1-based)  */
+    NICR_FIELD_ETA_S2 = 10,  /* Model::eta_s2                               */
+    NICR_FIELD_ETA_PAIRS = 11, /* 2D Model::eta_pairs                       */
+    NICR_FIELD_GB_INITIAL = 12 /* 2D Model::gb_initial                      */
+};
+
+typedef struct nicr_handle nicr_handle;
+
+/* Model::Model(Config, MPI_COMM_SELF) (2D:208-228, 3S:356-384): allocates the
+ * domain on the GPU, builds the Voronoi grains, initial fields, centre seed and
+ * eta fields, and refreshes. */
+int nicr_create(const nicr_config* cfg, nicr_handle** out);
+void nicr_destroy(nicr_handle* h);
+/* Message of the last failure on this handle, in the reference's wording. */
+const char* nicr_last_error(const nicr_handle* h);
+
+typedef struct nicr_info {
+    int dim, nx, ny, nz;
+    int n_seeds;              /* seeds.size()                                 */
+    int n_eta;                /* eta.size()                                   */
+    int center_seed_cells;    /* Model::center_seed_cells                     */
+    int grain_map_retained;   /* 3D frees the initial id map when eta is active */
+    long long n_cells;
+    long long steps_done;     /* accepted steps since creation                */
+    size_t device_bytes;      /* device memory held by the handle             */
+} nicr_info;
+int nicr_get_info(const nicr_handle* h, nicr_info* info);
+
+/* Seeds (x,y[,z] per seed, grid units) and per-grain cell counts (3S:395-467). */
+int nicr_get_seeds(const nicr_handle* h, double* xyz, long long* volumes);
+
+/* Copies one field between host memory and the device (interior cells only,
+ * reference order). Setting O/CR/PHI/ETA also invalidates the frozen-eta cache
+ * and refreshes, as the reference drivers do after editing fields
+ * (3S:1092-1101 fill_smooth; 3S:347-349 invalidate_eta_cache). */
+int nicr_set_field(nicr_handle* h, int field, int index, const double* host);
+int nicr_get_field(nicr_handle* h, int field, int index, double* host);
+
+/* Model::refresh (3S:597-620): materialises mu_O, mu_Cr, M_O, M_Cr (and the
+ * eta mask) for output. Steps do not need it; they fuse it on chip. */
+int nicr_refresh(nicr_handle* h);
+/* Model::invalidate_eta_cache (3S:349). */
+int nicr_invalidate_eta_cache(nicr_handle* h);
+/* initialO = sum(o), initialCr = sum(cr) (3S:370): used by drivers that inject
+ * fields after construction. */
+int nicr_reset_inventory(nicr_handle* h);
+
+/* Model::step x nsteps (3S:761-826, 2D:551-597). Stops at the first rejected
+ * trial: *completed = accepted steps; the state is the last accepted one, the
+ * budget is restored (3S:812-820) and the status names the failure. */
+int nicr_step(nicr_handle* h, int nsteps, int* completed);
+/* nsteps of run()'s loop (3S:1368-1385, 2D:1219-1236): before each step, Ksp
+ * nucleation when its physical time is due, then Model::step. The schedule
+ * continues across calls. */
+int nicr_run(nicr_handle* h, int nsteps, int* completed);
+/* Model::nucleate (3S:752-759): ordered Ksp scan and hard-seed insertion.   */
+int nicr_nucleate(nicr_handle* h, int* stamped_nuclei);
+/* Model::stamp (3S:704-724); z ignored in 2D. *cells = voxels changed.       */
+int nicr_stamp(nicr_handle* h, int x, int y, int z, int* cells);
+
+/* struct Budget (3S:217). The reference accumulates in long double; each sum
+ * is returned as an unevaluated pair hi+lo of doubles (hi = rounded value).  */
+typedef struct nicr_budget {
+    double nucO[2], nucCr[2], ckO[2], ckCr[2], clipO[2], clipCr[2], bcO[2], bcCr[2];
+    long long nuclei, clipped;
+    double initialO[2], initialCr[2];
+} nicr_budget;
+int nicr_get_budget(const nicr_handle* h, nicr_budget* b);
+
+/* Values of one diagnostics.csv row (Model::log, 3S:963-977 / 2D:697-710). */
+typedef struct nicr_diagnostics {
+    double sum_O[2], sum_Cr[2], sum_phi[2], sum_h[2];
+    double min_O, max_O, min_Cr, max_Cr, min_Ni, min_phi, max_phi;
+} nicr_diagnostics;
+int nicr_get_diagnostics(nicr_handle* h, nicr_diagnostics* d);
+
+/* Values of one grain_diagnostics.csv row and the per-grain history
+ * (Model::grain_log, 3S:566-590 / 2D:382-406). Arrays hold n_eta entries.   */
+typedef struct nicr_grain_stats {
+    double min_eta, max_eta, min_s2, max_s2;
+    double sum_s2[2], mask[2], energy[2];
+    double gb_max;
+    long long alive, unassigned;
+} nicr_grain_stats;
+int nicr_get_grain_stats(nicr_handle* h, nicr_grain_stats* s, long long* cells, double* amount_hi_lo);
+
+/* Output writers (host C++ over device data): the reference's files, byte for
+ * byte where the values are bit-identical. */
+int nicr_write_vtk(nicr_handle* h, const char* path);          /* 2D:598-632, 3S:828-856 */
+int nicr_write_vti(nicr_handle* h, const char* path);          /* 3S:857-869, 238-334    */
+int nicr_write_metadata(nicr_handle* h, const char* out_dir);  /* 2D:633-696, 3S:874-962 */
+/* Formats one diagnostics.csv row / grain rows for step n into buf.          */
+int nicr_format_log_row(nicr_handle* h, int n, char* buf, size_t len);
+int nicr_format_grain_rows(nicr_handle* h, int n, char* diag, size_t diag_len,
+                           char* history, size_t history_len);
+
+/* The solver program: the reference's run()/main() for dim 2 or 3
+ * (2D:1161-1246, 3S:1309-1395), argv as the reference's executable takes it.
+ * Returns the process exit code. */
+int nicr_main(int dim, int argc, const char* const* argv);
+
+/* Stream the handle enqueues on (a cudaStream_t), for callers that overlap. */
+void* nicr_stream(nicr_handle* h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NICR_H */
