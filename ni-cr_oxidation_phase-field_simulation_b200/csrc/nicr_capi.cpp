@@ -1,0 +1,160 @@
+// extern "C" entry points of include/nicr.h. Exceptions never cross this
+// boundary: every call maps failures to a status code and keeps the message
+// for nicr_last_error.
+#include <cstring>
+#include <new>
+#include <string>
+
+#include "../../include/nicr.h"
+#include "nicr_model.h"
+
+struct nicr_handle {
+    nicr::Model* m = nullptr;
+    std::string err;
+};
+
+namespace {
+thread_local std::string g_create_error;
+
+template <class Fn>
+int guarded(nicr_handle* h, Fn fn) {
+    if (!h || !h->m) return NICR_ERR_INVALID_ARG;
+    try {
+        const int rc = fn(*h->m);
+        if (rc != NICR_OK) h->err = h->m->last_error;
+        return rc;
+    } catch (const nicr::Error& e) {
+        h->err = e.what();
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        h->err = "host allocation failed";
+        return NICR_ERR_STATE;
+    } catch (const std::exception& e) {
+        h->err = e.what();
+        return NICR_ERR_STATE;
+    }
+}
+}  // namespace
+
+extern "C" {
+
+int nicr_create(const nicr_config* cfg, nicr_handle** out) {
+    if (!cfg || !out) return NICR_ERR_INVALID_ARG;
+    *out = nullptr;
+    try {
+        auto* h = new nicr_handle;
+        try {
+            h->m = new nicr::Model(*cfg);
+        } catch (...) {
+            delete h;
+            throw;
+        }
+        *out = h;
+        return NICR_OK;
+    } catch (const nicr::Error& e) {
+        g_create_error = e.what();
+        return e.code;
+    } catch (const std::exception& e) {
+        g_create_error = e.what();
+        return NICR_ERR_STATE;
+    }
+}
+
+void nicr_destroy(nicr_handle* h) {
+    if (!h) return;
+    delete h->m;
+    delete h;
+}
+
+const char* nicr_last_error(const nicr_handle* h) { return h ? h->err.c_str() : g_create_error.c_str(); }
+
+int nicr_get_info(const nicr_handle* hc, nicr_info* info) {
+    auto* h = const_cast<nicr_handle*>(hc);
+    return guarded(h, [&](nicr::Model& m) {
+        if (!info) return (int)NICR_ERR_INVALID_ARG;
+        info->dim = m.dim;
+        info->nx = m.c.nx; info->ny = m.c.ny; info->nz = m.dim == 3 ? m.c.nz : 1;
+        info->n_seeds = (int)(m.seeds.size() / m.dim);
+        info->n_eta = m.neta;
+        info->center_seed_cells = m.center_seed_cells;
+        info->grain_map_retained = m.grain_retained ? 1 : 0;
+        info->n_cells = m.g.ncells;
+        info->steps_done = m.steps_done;
+        info->device_bytes = m.device_bytes();
+        return (int)NICR_OK;
+    });
+}
+
+int nicr_get_seeds(const nicr_handle* hc, double* xyz, long long* volumes) {
+    auto* h = const_cast<nicr_handle*>(hc);
+    return guarded(h, [&](nicr::Model& m) {
+        if (xyz) std::memcpy(xyz, m.seeds.data(), m.seeds.size() * sizeof(double));
+        if (volumes) std::memcpy(volumes, m.volumes.data(), m.volumes.size() * sizeof(long long));
+        return (int)NICR_OK;
+    });
+}
+
+int nicr_set_field(nicr_handle* h, int field, int index, const double* host) {
+    return guarded(h, [&](nicr::Model& m) {
+        if (!host) return (int)NICR_ERR_INVALID_ARG;
+        m.set_field(field, index, host);
+        m.refresh();
+        return (int)NICR_OK;
+    });
+}
+
+int nicr_get_field(nicr_handle* h, int field, int index, double* host) {
+    return guarded(h, [&](nicr::Model& m) {
+        if (!host) return (int)NICR_ERR_INVALID_ARG;
+        m.get_field(field, index, host);
+        return (int)NICR_OK;
+    });
+}
+
+int nicr_refresh(nicr_handle* h) {
+    return guarded(h, [&](nicr::Model& m) { m.refresh(); m.sync(); return (int)NICR_OK; });
+}
+int nicr_invalidate_eta_cache(nicr_handle* h) {
+    return guarded(h, [&](nicr::Model& m) { m.invalidate_eta_cache(); return (int)NICR_OK; });
+}
+int nicr_reset_inventory(nicr_handle* h) {
+    return guarded(h, [&](nicr::Model& m) { m.reset_inventory(); return (int)NICR_OK; });
+}
+int nicr_step(nicr_handle* h, int nsteps, int* completed) {
+    return guarded(h, [&](nicr::Model& m) { return m.step(nsteps, completed); });
+}
+int nicr_run(nicr_handle* h, int nsteps, int* completed) {
+    return guarded(h, [&](nicr::Model& m) { return m.run(nsteps, completed); });
+}
+int nicr_nucleate(nicr_handle* h, int* nuclei) {
+    return guarded(h, [&](nicr::Model& m) { return m.nucleate(nuclei); });
+}
+int nicr_stamp(nicr_handle* h, int x, int y, int z, int* cells) {
+    return guarded(h, [&](nicr::Model& m) { return m.stamp(x, y, z, cells); });
+}
+int nicr_get_budget(const nicr_handle* hc, nicr_budget* b) {
+    auto* h = const_cast<nicr_handle*>(hc);
+    return guarded(h, [&](nicr::Model& m) {
+        if (!b) return (int)NICR_ERR_INVALID_ARG;
+        m.budget(b);
+        return (int)NICR_OK;
+    });
+}
+int nicr_get_diagnostics(nicr_handle* h, nicr_diagnostics* d) {
+    return guarded(h, [&](nicr::Model& m) {
+        if (!d) return (int)NICR_ERR_INVALID_ARG;
+        m.diagnostics(d);
+        return (int)NICR_OK;
+    });
+}
+int nicr_get_grain_stats(nicr_handle* h, nicr_grain_stats* s, long long* cells, double* amount) {
+    return guarded(h, [&](nicr::Model& m) {
+        if (!s) return (int)NICR_ERR_INVALID_ARG;
+        m.grain_stats(s, cells, amount);
+        return (int)NICR_OK;
+    });
+}
+
+void* nicr_stream(nicr_handle* h) { return (h && h->m) ? (void*)h->m->stream : nullptr; }
+
+}  // extern "C"

@@ -1,0 +1,125 @@
+// Launch interface between the host model (g++) and the CUDA kernels (nvcc).
+// Plain C++: parameter blocks passed by value to the kernels, and launchers.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace nicr {
+
+// Device layout of one field. X (planes) is slowest like the reference
+// (3S:165-167); inside a plane, rows (3D: Y) then columns (3D: Z, 2D: Y), the
+// column pitch padded to a multiple of 8 doubles so that every row starts on a
+// 64-byte boundary. No ghost cells are stored: the kernels apply Neumann X and
+// periodic row/column boundaries while staging tiles.
+struct Grid {
+    int dim;          // 2 or 3
+    int nx;           // planes (reference X)
+    int na;           // rows: 3D ny, 2D 1
+    int nb;           // columns: 3D nz, 2D ny
+    int pb;           // padded column pitch (elements)
+    long long plane;  // na * pb
+    long long ncells; // nx * na * nb
+    long long nstore; // nx * plane
+};
+
+// Device status word of one domain: sticky failure flag, first failing trial
+// (minimum key in reference loop order), step counters.
+struct Status {
+    unsigned long long err_key;   // ERR_NONE when no trial failed this step
+    int failed;                   // a step of this batch was rejected
+    int pad;
+    long long failed_step;        // index (steps_done) of the rejected step
+    long long steps_done;         // accepted steps since creation
+};
+constexpr unsigned long long ERR_NONE = ~0ull;
+constexpr unsigned long long ERR_ETA_BASE = 1ull << 62;
+
+// Budget in double-double (Budget, 3S:217); order nucO nucCr ckO ckCr clipO clipCr bcO bcCr
+struct DevBudget {
+    double v[8][2];
+    long long nuclei, clipped;
+    double initialO[2], initialCr[2];
+};
+
+// Per-CTA partial sums of one step (ckO ckCr clipO clipCr bcO as hi/lo) + clipped count
+struct StepPartial {
+    double s[5][2];
+    long long clipped;
+    long long pad;
+};
+
+struct StepParams {
+    Grid g;
+    double dx, da, db, dt;       // spacing along X, rows, columns
+    double dxdx, dada, dbdb;     // c.dx*c.dx etc. (lap denominators, 3S:193-195)
+    double dtL;                  // dt * Physics::L
+    double layer_o;
+    double gbm1_o, gbm1_cr;      // gb_factor_o - 1, gb_factor_cr - 1
+    double mu_res, surface_c_ref;
+    double eta_W, eta_A, eta_K, dt_etaL, eta_scale;
+    int bc, ck, bounds;
+    int o_on;                    // oxygen_diffusion
+    int grains;                  // GB mask active in mobility
+    int phi_eta;                 // eta coupling in the phi force (has_eta)
+    int inlet;                   // bc == concentration && oxygen_diffusion
+    int xchunk;                  // planes per CTA along X
+};
+
+// ---- step --------------------------------------------------------------------
+// Main fused step: mu, M, six-face fluxes, phi, Ck, bounds -> trial buffers.
+void launch_step_main(const StepParams& P, const double* o, const double* cr, const double* p,
+                      const double* gb, const double* s2, double* on, double* crn, double* pn,
+                      StepPartial* partials, Status* st, cudaStream_t stream, int* nblocks_out);
+int step_main_blocks(const StepParams& P);
+// Eta mask: S = sum eta^2, pairs, gb = scale*min(1,16*pairs) (3S:495-507)
+void launch_eta_mask(const StepParams& P, int neta, const double* eta, double* gb, double* s2,
+                     double* pairs, Status* st, cudaStream_t stream);
+// Eta trial update (3S:514-526) + next-step mask from the trial values
+void launch_eta_update(const StepParams& P, int neta, const double* eta, const double* s2,
+                       const double* p, double* eta_next, double* gb_next, double* s2_next,
+                       Status* st, cudaStream_t stream);
+// Commit of one step: reduce partials, commit budget unless a trial failed
+void launch_step_finalize(const StepPartial* partials, int nblocks, DevBudget* budget, Status* st,
+                          int accept_mode, cudaStream_t stream);
+// Refresh for output: mu_O, mu_Cr, M_O, M_Cr at every cell (3S:597-620)
+void launch_refresh(const StepParams& P, const double* o, const double* cr, const double* p,
+                    const double* gb, double* muO, double* muCr, double* mo, double* mc,
+                    cudaStream_t stream);
+
+// ---- init --------------------------------------------------------------------
+struct InitParams {
+    Grid g;
+    int ng;
+    double nxd, nyd, nzd;        // grid extents as doubles (periods)
+    double bulk_cr, layer_o;
+    int inlet_layer;             // bc == concentration
+};
+void launch_init_fields(const InitParams& I, double* o, double* cr, double* p, cudaStream_t stream);
+// 3D Voronoi labels (first nearest seed under minimum image) and the distance
+// to the nearest bisector (3S:450-466). seeds: x,y,z per seed.
+void launch_voronoi3(const InitParams& I, const double* seeds, double* grain, double* db,
+                     int* volumes, cudaStream_t stream);
+// 3D eta initial weights: per competitor g, the bisector distance (3S:469-494);
+// the owner's slot receives -1. Output layout eta[g*nstore + idx].
+void launch_eta_dist3(const InitParams& I, const double* seeds, const double* grain, double* eta,
+                      cudaStream_t stream);
+// Centre seed (3S:725-751): stamps the ball and accumulates nucO, nucCr, cells
+void launch_center_seed(const InitParams& I, double cx, double cy, double cz, double r, int neta,
+                        double* o, double* cr, double* p, double* eta, StepPartial* partials,
+                        cudaStream_t stream, int* nblocks_out);
+// Generic dd sum over the partial array (first nsum slots + count) into out
+void launch_reduce_partials(const StepPartial* partials, int nblocks, StepPartial* out,
+                            cudaStream_t stream);
+
+// ---- diagnostics ---------------------------------------------------------------
+// sums o, cr, p, h(p) (dd) and min/max of O, Cr, Ni, phi (3S:963-977)
+struct DiagOut {
+    double sum[4][2];
+    double mn[4], mx[4];   // O, Cr, Ni(=1-o-cr, min only), phi
+    long long mni[4], mxi[4];  // first cell (reference order) attaining each extremum
+};
+void launch_diagnostics(const Grid& g, const double* o, const double* cr, const double* p,
+                        DiagOut* partials, int* nblocks, DiagOut* out, cudaStream_t stream);
+
+}  // namespace nicr

@@ -1,0 +1,373 @@
+// Ordered Ksp nucleation (Model::nucleate / valid_nucleus / stamp,
+// 3S:687-724, 3S:752-759; 2D:493-516, 2D:543-550) on the GPU.
+//
+// The reference scans cells in (i,j,k) order and stamps a hard oxide ball at
+// every cell that (on the state as modified by the earlier stamps of the same
+// scan) has phi <= .01, o*cr > Ksp and no cell with phi > .01 closer than
+// r + gap. Stamps only raise phi (to 1, in cells that had phi < .01), so:
+//   * a cell that fails the test on the pre-scan state fails it later too;
+//   * a pre-scan candidate c is stamped iff it was not itself stamped earlier
+//     in the scan and no cell stamped earlier lies within r + gap of it.
+// Pass 1 (parallel) evaluates the pre-scan test for every cell; pass 2 compacts
+// the candidates in reference order; pass 3 (one CTA) walks them in order,
+// stamps accepted balls, and marks every cell within r + gap of a stamped cell
+// in a "blocked" map (exact: the marked set is the Minkowski sum of the
+// stamped cells and the exclusion ball, precomputed as integer offsets).
+// Distances are integer-valued: 3D compares sqrt(D) < r + gap with IEEE sqrt
+// like the reference; 2D uses the reference's C-library hypot, tabulated on
+// the host for the integer offsets that occur.
+#include <cuda_runtime.h>
+#include "nicr_kernels.h"
+#include "nicr_ksp.h"
+#include "nicr_physics.h"
+
+namespace nicr {
+
+namespace {
+
+struct AxisNb {
+    int count, lo0, hi0, lo1, hi1;
+};
+// periodic_neighborhood (3S:220-231)
+__device__ __forceinline__ int bounded_reach(double radius, int n) { return radius >= n ? n : (int)ceil(radius); }
+__device__ AxisNb periodic_nb(int center, double radius, int n) {
+    const int r = bounded_reach(radius, n);
+    AxisNb a{0, 0, 0, 0, 0};
+    if (2LL * r + 1 >= n) { a.count = 1; a.lo0 = 1; a.hi0 = n; return a; }
+    const long long lo = (long long)center - r, hi = (long long)center + r;
+    if (lo < 1) { a.count = 2; a.lo0 = 1; a.hi0 = (int)hi; a.lo1 = (int)(lo + n); a.hi1 = n; }
+    else if (hi > n) { a.count = 2; a.lo0 = 1; a.hi0 = (int)(hi - n); a.lo1 = (int)lo; a.hi1 = n; }
+    else { a.count = 1; a.lo0 = (int)lo; a.hi0 = (int)hi; }
+    return a;
+}
+
+__device__ __forceinline__ long long gidx(const Grid& g, int i1, int j1, int k1) {
+    // 1-based reference indices -> device index. 3D: (i,j,k); 2D: (i,j) with j the column.
+    if (g.dim == 3) return (long long)(i1 - 1) * g.plane + (long long)(j1 - 1) * g.pb + (k1 - 1);
+    return (long long)(i1 - 1) * g.plane + (j1 - 1);
+}
+
+// valid_nucleus on the pre-scan state (3S:687-703, 2D:493-502)
+__device__ bool valid_prescan(const KspDev& K, const double* __restrict__ p, int x, int y, int z) {
+    const Grid& g = K.g;
+    const double r = K.radius;
+    if (x - r < 5. || x + r > (double)(K.nx - 3)) return false;
+    const double limit = r + K.gap;
+    if (g.dim == 2) {
+        const int sr = (int)ceil(r + K.gap);
+        const int i0 = max(1, x - sr), i1 = min(K.nx, x + sr);
+        for (int i = i0; i <= i1; ++i)
+            for (int j = 1; j <= K.ny; ++j) {
+                if (__ldg(p + gidx(g, i, j, 0)) > .01) {
+                    const int dj = (int)min_image((double)(j - y), (double)K.ny);
+                    if (K.hyp2d[abs(i - x) * K.hyp_stride + abs(dj)]) return false;
+                }
+            }
+        return true;
+    }
+    const AxisNb ys = periodic_nb(y, limit, K.ny), zs = periodic_nb(z, limit, K.nz);
+    const int sr = bounded_reach(limit, K.nx);
+    const long long a0 = (long long)x - sr, a1 = (long long)x + sr;
+    for (int i = (int)(a0 > 1 ? a0 : 1); i <= (int)(a1 < K.nx ? a1 : K.nx); ++i)
+        for (int jy = 0; jy < ys.count; ++jy) {
+            const int jlo = jy ? ys.lo1 : ys.lo0, jhi = jy ? ys.hi1 : ys.hi0;
+            for (int j = jlo; j <= jhi; ++j)
+                for (int kz = 0; kz < zs.count; ++kz) {
+                    const int klo = kz ? zs.lo1 : zs.lo0, khi = kz ? zs.hi1 : zs.hi0;
+                    for (int k = klo; k <= khi; ++k) {
+                        if (__ldg(p + gidx(g, i, j, k)) > .01) {
+                            const double di = (double)(i - x), dj = min_image((double)(j - y), (double)K.ny),
+                                         dk = min_image((double)(k - z), (double)K.nz);
+                            if (sqrt(di * di + dj * dj + dk * dk) < limit) return false;
+                        }
+                    }
+                }
+        }
+    return true;
+}
+
+__global__ void k_ksp_candidates(const KspDev K, const double* __restrict__ o, const double* __restrict__ cr,
+                                 const double* __restrict__ p, unsigned char* __restrict__ flag, Status* st) {
+    if (st->failed) return;
+    const Grid& g = K.g;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < g.ncells; c += (long long)gridDim.x * blockDim.x) {
+        const int col = (int)(c % g.nb);
+        const long long r = c / g.nb;
+        const int row = (int)(r % g.na);
+        const int xi = (int)(r / g.na);
+        const long long idx = (long long)xi * g.plane + (long long)row * g.pb + col;
+        unsigned char f = 0;
+        const double pv = __ldg(p + idx);
+        if (pv <= .01 && __ldg(o + idx) * __ldg(cr + idx) > K.ksp) {
+            const int x = xi + 1;
+            if (g.dim == 3) f = valid_prescan(K, p, x, row + 1, col + 1) ? 1 : 0;
+            else f = valid_prescan(K, p, x, col + 1, 0) ? 1 : 0;
+        }
+        flag[c] = f;
+    }
+}
+
+// Ordered compaction of flagged cells: per-block counts, then ordered writes.
+constexpr int CBLK = 256, CITEMS = 16;  // each block covers CBLK*CITEMS cells
+__global__ void k_ksp_count(const unsigned char* __restrict__ flag, long long n, int* counts) {
+    const long long base = (long long)blockIdx.x * CBLK * CITEMS;
+    int cnt = 0;
+    for (int q = 0; q < CITEMS; ++q) {
+        const long long c = base + (long long)q * CBLK + threadIdx.x;
+        if (c < n && flag[c]) ++cnt;
+    }
+    for (int off = 16; off > 0; off >>= 1) cnt += __shfl_down_sync(0xffffffffu, cnt, off);
+    __shared__ int s[CBLK / 32];
+    if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = cnt;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int t = 0;
+        for (int w = 0; w < CBLK / 32; ++w) t += s[w];
+        counts[blockIdx.x] = t;
+    }
+}
+__global__ void k_ksp_write(const unsigned char* __restrict__ flag, long long n, const int* __restrict__ counts,
+                            long long* __restrict__ list, int* total, int nblocks) {
+    __shared__ long long base_s;
+    __shared__ int wsum[CBLK / 32];
+    if (threadIdx.x == 0) {
+        long long b = 0;
+        for (int q = 0; q < (int)blockIdx.x; ++q) b += counts[q];
+        base_s = b;
+        if (blockIdx.x == nblocks - 1) *total = (int)(b + counts[blockIdx.x]);
+    }
+    __syncthreads();
+    long long running = base_s;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const long long base = (long long)blockIdx.x * CBLK * CITEMS;
+    for (int q = 0; q < CITEMS; ++q) {
+        const long long c = base + (long long)q * CBLK + threadIdx.x;
+        const bool f = c < n && flag[c];
+        const unsigned ball = __ballot_sync(0xffffffffu, f);
+        if (lane == 0) wsum[w] = __popc(ball);
+        __syncthreads();
+        int before = 0, tot = 0;
+        for (int ww = 0; ww < CBLK / 32; ++ww) { if (ww < w) before += wsum[ww]; tot += wsum[ww]; }
+        if (f) list[running + before + __popc(ball & ((1u << lane) - 1u))] = c;
+        running += tot;
+        __syncthreads();
+    }
+}
+
+// One CTA: ordered greedy resolve + stamps + exclusion marks.
+__global__ void __launch_bounds__(1024) k_ksp_resolve(const KspDev K, const long long* __restrict__ list,
+                                                      const int* __restrict__ total, int forced, int fx, int fy,
+                                                      int fz, double* o, double* cr, double* p, double* eta,
+                                                      unsigned char* blocked, DevBudget* budget, KspResult* res,
+                                                      Status* st) {
+    if (st->failed) return;
+    __shared__ long long s_cand;
+    __shared__ int s_next;
+    __shared__ DD s_dd[32][2];
+    __shared__ int s_cnt[32];
+    const Grid& g = K.g;
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const int n = forced ? 1 : *total;
+    int pos = 0, accepted = 0, last_cells = 0;
+    DD nucO{0., 0.}, nucCr{0., 0.};
+    while (true) {
+        // warp 0 finds the next accepted candidate from pos (32 at a time)
+        if (w == 0) {
+            int found = -1;
+            while (pos < n && found < 0) {
+                const int q = pos + lane;
+                bool ok = false;
+                long long cq = 0;
+                if (q < n) {
+                    if (forced) ok = true;
+                    else {
+                        cq = list[q];
+                        const int col = (int)(cq % g.nb);
+                        const long long rr = cq / g.nb;
+                        const int row = (int)(rr % g.na);
+                        const int xi = (int)(rr / g.na);
+                        const long long idx = (long long)xi * g.plane + (long long)row * g.pb + col;
+                        ok = !blocked[cq] && p[idx] <= .01;
+                    }
+                }
+                const unsigned b = __ballot_sync(0xffffffffu, ok);
+                if (b) found = pos + __ffs(b) - 1;
+                else pos += 32;
+            }
+            if (lane == 0) {
+                s_next = found;
+                s_cand = found >= 0 ? (forced ? -1 : list[found]) : -1;
+            }
+        }
+        __syncthreads();
+        const int found = s_next;
+        if (found < 0) break;
+        pos = found + 1;
+        int x, y, z = 0;
+        if (forced) { x = fx; y = fy; z = fz; }
+        else {
+            const long long cq = s_cand;
+            const int col = (int)(cq % g.nb);
+            const long long rr = cq / g.nb;
+            const int row = (int)(rr % g.na);
+            x = (int)(rr / g.na) + 1;
+            if (g.dim == 3) { y = row + 1; z = col + 1; } else { y = col + 1; }
+        }
+        // stamp(x,y,z): ball cells with phi < .01 (3S:704-724 / 2D:503-516)
+        int cells = 0;
+        const double r2 = K.radius * K.radius;
+        if (g.dim == 3) {
+            const int rr = bounded_reach(K.radius, K.nx);
+            const AxisNb ys = periodic_nb(y, K.radius, K.ny), zs = periodic_nb(z, K.radius, K.nz);
+            const int i0 = (int)max(1LL, (long long)x - rr), i1 = (int)min((long long)K.nx, (long long)x + rr);
+            const int ny_n = (ys.hi0 - ys.lo0 + 1) + (ys.count > 1 ? ys.hi1 - ys.lo1 + 1 : 0);
+            const int nz_n = (zs.hi0 - zs.lo0 + 1) + (zs.count > 1 ? zs.hi1 - zs.lo1 + 1 : 0);
+            const long long tot = (long long)(i1 - i0 + 1) * ny_n * nz_n;
+            for (long long q = tid; q < tot; q += blockDim.x) {
+                const int kq = (int)(q % nz_n);
+                const long long t = q / nz_n;
+                const int jq = (int)(t % ny_n);
+                const int i = i0 + (int)(t / ny_n);
+                const int n0y = ys.hi0 - ys.lo0 + 1, n0z = zs.hi0 - zs.lo0 + 1;
+                const int j = jq < n0y ? ys.lo0 + jq : ys.lo1 + (jq - n0y);
+                const int k = kq < n0z ? zs.lo0 + kq : zs.lo1 + (kq - n0z);
+                const double dy = min_image((double)(j - y), (double)K.ny), dz = min_image((double)(k - z), (double)K.nz);
+                const long long idx = gidx(g, i, j, k);
+                if ((double)((i - x) * (i - x)) + dy * dy + dz * dz <= r2 && p[idx] < .01) {
+                    nucO = dd_add(nucO, Phys::oxideO - o[idx]);
+                    nucCr = dd_add(nucCr, Phys::oxideCr - cr[idx]);
+                    o[idx] = Phys::oxideO; cr[idx] = Phys::oxideCr; p[idx] = 1.;
+                    for (int e = 0; e < K.neta; ++e) eta[(long long)e * g.nstore + idx] = 0.;
+                    ++cells;
+                }
+            }
+        } else {
+            const int rr = (int)ceil(K.radius);
+            const int i0 = max(1, x - rr), i1 = min(K.nx, x + rr);
+            const long long tot = (long long)(i1 - i0 + 1) * K.ny;
+            for (long long q = tid; q < tot; q += blockDim.x) {
+                const int j = (int)(q % K.ny) + 1;
+                const int i = i0 + (int)(q / K.ny);
+                const double dy = min_image((double)(j - y), (double)K.ny);
+                const long long idx = gidx(g, i, j, 0);
+                if ((double)((i - x) * (i - x)) + dy * dy <= r2 && p[idx] < .01) {
+                    nucO = dd_add(nucO, Phys::oxideO - o[idx]);
+                    nucCr = dd_add(nucCr, Phys::oxideCr - cr[idx]);
+                    o[idx] = Phys::oxideO; cr[idx] = Phys::oxideCr; p[idx] = 1.;
+                    for (int e = 0; e < K.neta; ++e) eta[(long long)e * g.nstore + idx] = 0.;
+                    ++cells;
+                }
+            }
+        }
+        for (int off = 16; off > 0; off >>= 1) cells += __shfl_down_sync(0xffffffffu, cells, off);
+        if (lane == 0) s_cnt[w] = cells;
+        __syncthreads();
+        int changed = 0;
+        for (int ww = 0; ww < (int)(blockDim.x >> 5); ++ww) changed += s_cnt[ww];
+        if (changed) ++accepted;
+        last_cells = changed;
+        // exclusion marks for the later candidates of this scan
+        if (changed && !forced) {
+            if (changed == K.full_ball) {
+                for (int q = tid; q < K.n_shadow; q += blockDim.x) {
+                    const int di = K.shadow[3 * q], dj = K.shadow[3 * q + 1], dk = K.shadow[3 * q + 2];
+                    const int i = x + di;
+                    if (i < 1 || i > K.nx) continue;
+                    int j, k;
+                    if (g.dim == 3) {
+                        j = ((y - 1 + dj) % K.ny + K.ny) % K.ny;
+                        k = ((z - 1 + dk) % K.nz + K.nz) % K.nz;
+                        blocked[((long long)(i - 1) * K.ny + j) * K.nz + k] = 1;
+                    } else {
+                        j = ((y - 1 + dj) % K.ny + K.ny) % K.ny;
+                        blocked[(long long)(i - 1) * K.ny + j] = 1;
+                    }
+                }
+            } else {
+                // partial stamp (some ball cell had phi == .01 exactly): mark every cell of
+                // the exclusion box whose distance to a stamped cell passes the test
+                if (tid == 0) res->partial_stamps += 1;
+                const int R = K.box_half;
+                const long long side = 2LL * R + 1;
+                const long long tot = g.dim == 3 ? side * side * side : side * side;
+                for (long long q = tid; q < tot; q += blockDim.x) {
+                    int di, dj, dk = 0;
+                    if (g.dim == 3) { dk = (int)(q % side) - R; dj = (int)((q / side) % side) - R; di = (int)(q / (side * side)) - R; }
+                    else { dj = (int)(q % side) - R; di = (int)(q / side) - R; }
+                    const int i = x + di;
+                    if (i < 1 || i > K.nx) continue;
+                    const int jw = ((y - 1 + dj) % K.ny + K.ny) % K.ny + 1;
+                    const int kw = g.dim == 3 ? ((z - 1 + dk) % K.nz + K.nz) % K.nz + 1 : 0;
+                    bool hit = false;
+                    for (int b = 0; b < K.n_ball && !hit; ++b) {
+                        const int si = x + K.ball[3 * b];
+                        if (si < 1 || si > K.nx) continue;
+                        const int sj = ((y - 1 + K.ball[3 * b + 1]) % K.ny + K.ny) % K.ny + 1;
+                        const int sk = g.dim == 3 ? ((z - 1 + K.ball[3 * b + 2]) % K.nz + K.nz) % K.nz + 1 : 0;
+                        if (p[gidx(g, si, sj, sk)] != 1.) continue;   // not (newly) oxide
+                        const int ddi = si - i;
+                        const int ddj = (int)min_image((double)(sj - jw), (double)K.ny);
+                        if (g.dim == 3) {
+                            const int ddk = (int)min_image((double)(sk - kw), (double)K.nz);
+                            hit = sqrt((double)ddi * ddi + (double)ddj * ddj + (double)ddk * ddk) < K.radius + K.gap;
+                        } else {
+                            hit = K.hyp2d[abs(ddi) * K.hyp_stride + abs(ddj)] != 0;
+                        }
+                    }
+                    if (hit) {
+                        if (g.dim == 3) blocked[((long long)(i - 1) * K.ny + (jw - 1)) * K.nz + (kw - 1)] = 1;
+                        else blocked[(long long)(i - 1) * K.ny + (jw - 1)] = 1;
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        if (forced) break;
+    }
+    // budget: nucO, nucCr, nuclei
+    for (int off = 16; off > 0; off >>= 1) {
+        nucO = dd_add(nucO, DD{__shfl_down_sync(0xffffffffu, nucO.hi, off), __shfl_down_sync(0xffffffffu, nucO.lo, off)});
+        nucCr = dd_add(nucCr, DD{__shfl_down_sync(0xffffffffu, nucCr.hi, off), __shfl_down_sync(0xffffffffu, nucCr.lo, off)});
+    }
+    if (lane == 0) { s_dd[w][0] = nucO; s_dd[w][1] = nucCr; }
+    __syncthreads();
+    if (tid == 0) {
+        DD a = s_dd[0][0], b = s_dd[0][1];
+        for (int ww = 1; ww < (int)(blockDim.x >> 5); ++ww) { a = dd_add(a, s_dd[ww][0]); b = dd_add(b, s_dd[ww][1]); }
+        DD bo{budget->v[0][0], budget->v[0][1]}, bc{budget->v[1][0], budget->v[1][1]};
+        bo = dd_add(bo, a); bc = dd_add(bc, b);
+        budget->v[0][0] = bo.hi; budget->v[0][1] = bo.lo;
+        budget->v[1][0] = bc.hi; budget->v[1][1] = bc.lo;
+        budget->nuclei += accepted;
+        res->nuclei = accepted;
+        res->last_cells = last_cells;
+        res->candidates = n;
+    }
+}
+
+int cgrid(long long n, int threads, int cap) {
+    const long long want = (n + threads - 1) / threads;
+    return (int)(want < cap ? (want > 0 ? want : 1) : cap);
+}
+
+}  // namespace
+
+int ksp_compact_blocks(long long ncells) { return (int)((ncells + CBLK * CITEMS - 1) / (CBLK * CITEMS)); }
+
+void launch_ksp_scan(const KspDev& K, double* o, double* cr, double* p, double* eta, KspWork& W, DevBudget* budget,
+                     KspResult* res, Status* st, cudaStream_t stream) {
+    const long long n = K.g.ncells;
+    cudaMemsetAsync(W.blocked, 0, (size_t)n, stream);
+    k_ksp_candidates<<<cgrid(n, 128, 148 * 64), 128, 0, stream>>>(K, o, cr, p, W.flag, st);
+    const int nb = ksp_compact_blocks(n);
+    k_ksp_count<<<nb, CBLK, 0, stream>>>(W.flag, n, W.counts);
+    k_ksp_write<<<nb, CBLK, 0, stream>>>(W.flag, n, W.counts, W.list, W.total, nb);
+    k_ksp_resolve<<<1, 1024, 0, stream>>>(K, W.list, W.total, 0, 0, 0, 0, o, cr, p, eta, W.blocked, budget, res, st);
+}
+
+void launch_ksp_stamp(const KspDev& K, int x, int y, int z, double* o, double* cr, double* p, double* eta,
+                      KspWork& W, DevBudget* budget, KspResult* res, Status* st, cudaStream_t stream) {
+    k_ksp_resolve<<<1, 1024, 0, stream>>>(K, W.list, W.total, 1, x, y, z, o, cr, p, eta, W.blocked, budget, res, st);
+}
+
+}  // namespace nicr

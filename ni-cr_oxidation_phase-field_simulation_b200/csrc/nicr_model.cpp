@@ -1,0 +1,783 @@
+// Host orchestration of one GPU-resident domain (see nicr_model.h).
+#include "nicr_model.h"
+
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <random>
+#include <sstream>
+#include <iomanip>
+#include <thread>
+
+namespace nicr {
+
+void check_cuda(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) throw Error(NICR_ERR_CUDA, std::string("CUDA error in ") + what + ": " + cudaGetErrorString(e));
+}
+
+namespace {
+
+// Runs fn(begin, end) over [0, n) on the host cores.
+template <class Fn>
+void parallel_for(long long n, Fn fn) {
+    unsigned nt = std::max(1u, std::min(64u, std::thread::hardware_concurrency()));
+    if (n < 1 << 16) nt = 1;
+    std::vector<std::thread> th;
+    const long long chunk = (n + nt - 1) / nt;
+    for (unsigned t = 0; t < nt; ++t) {
+        const long long b = t * chunk, e = std::min(n, b + chunk);
+        if (b >= e) break;
+        th.emplace_back([=] { fn(b, e); });
+    }
+    for (auto& t : th) t.join();
+}
+
+int bounded_reach_h(double radius, int n) { return radius >= n ? n : int(std::ceil(radius)); }
+
+}  // namespace
+
+double* Model::dalloc(size_t n) { return dalloc_t<double>(n); }
+template <class T>
+T* Model::dalloc_t(size_t n) {
+    T* p = nullptr;
+    check_cuda(cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T)), "cudaMalloc");
+    dev_bytes += std::max<size_t>(n, 1) * sizeof(T);
+    return p;
+}
+
+Model::Model(const nicr_config& cfg) : c(cfg), dim(cfg.dim) {
+    if (dim != 2 && dim != 3) throw Error(NICR_ERR_INVALID_ARG, "dim must be 2 or 3");
+    if (dim == 3 && (c.nx < 3 || c.ny < 3 || c.nz < 3 || c.nx > INT_MAX - 2 || c.ny > INT_MAX - 2 || c.nz > INT_MAX - 2))
+        throw Error(NICR_ERR_INVALID_ARG, "3D grid dimensions must lie in [3, INT_MAX-2].");
+    if (dim == 2 && (c.nx < 3 || c.ny < 3))
+        throw Error(NICR_ERR_INVALID_ARG, "Invalid parameter bounds (Ksp nucleation period must be >= dt).");
+    if (dim == 2) c.nz = 1;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        throw Error(NICR_ERR_NO_DEVICE, "no CUDA device is available");
+    check_cuda(cudaSetDevice(c.device), "cudaSetDevice");
+    check_cuda(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate");
+
+    g.dim = dim;
+    g.nx = c.nx;
+    g.na = dim == 3 ? c.ny : 1;
+    g.nb = dim == 3 ? c.nz : c.ny;
+    g.pb = (g.nb + 7) / 8 * 8;
+    g.plane = (long long)g.na * g.pb;
+    g.ncells = (long long)g.nx * g.na * g.nb;
+    g.nstore = (long long)g.nx * g.plane;
+
+    has_eta = c.grain_evolution && c.grains;
+    advance_eta = has_eta && (dim == 2 || c.eta_L > 0.);
+    ec = eta_coef(c.gb_fwhm_grid, c.dx, c.eta_W, c.eta_kappa, c.eta_oxide_penalty);
+    next_nucleation = c.nucleation_period;
+
+    sp.g = g;
+    sp.dx = c.dx;
+    sp.da = c.dy;
+    sp.db = dim == 3 ? c.dz : c.dy;
+    sp.dt = c.dt;
+    sp.dxdx = c.dx * c.dx;
+    sp.dada = c.dy * c.dy;
+    sp.dbdb = dim == 3 ? c.dz * c.dz : c.dy * c.dy;
+    sp.dtL = c.dt * Phys::L;
+    sp.layer_o = c.layer_o;
+    sp.gbm1_o = c.gb_factor_o - 1.;
+    sp.gbm1_cr = c.gb_factor_cr - 1.;
+    sp.mu_res = c.mu_res;
+    sp.surface_c_ref = c.surface_c_ref;
+    sp.eta_W = c.eta_W;
+    sp.eta_A = ec.A;
+    sp.eta_K = ec.K;
+    sp.dt_etaL = c.dt * c.eta_L;
+    sp.eta_scale = ec.scale;
+    sp.bc = c.bc;
+    sp.ck = c.ck;
+    sp.bounds = c.bounds;
+    sp.o_on = c.oxygen_diffusion ? 1 : 0;
+    sp.grains = c.grains ? 1 : 0;
+    sp.phi_eta = has_eta ? 1 : 0;
+    sp.inlet = (c.bc == NICR_BC_CONCENTRATION && c.oxygen_diffusion) ? 1 : 0;
+    // X chunking: enough CTAs for a few waves on 148 SMs
+    {
+        const long long tiles = dim == 3 ? (long long)((g.nb + 31) / 32) * ((g.na + 7) / 8) : (g.nb + 127) / 128;
+        int chunk = g.nx;
+        const long long target = 148LL * 2 * 4;
+        while (chunk > 16 && tiles * ((g.nx + chunk - 1) / chunk) < target) chunk = (chunk + 1) / 2;
+        sp.xchunk = std::max(1, chunk);
+    }
+
+    try {
+        const size_t ns = (size_t)g.nstore;
+        for (int q = 0; q < 2; ++q) { o_[q] = dalloc(ns); cr_[q] = dalloc(ns); p_[q] = dalloc(ns); }
+        gb_[0] = dalloc(ns);
+        check_cuda(cudaMemsetAsync(gb_[0], 0, ns * 8, stream), "memset");
+        if (advance_eta) gb_[1] = dalloc(ns);
+        if (has_eta) { s2_[0] = dalloc(ns); if (advance_eta) s2_[1] = dalloc(ns); }
+        grain = dalloc(ns);
+        if (dim == 2) { gb_initial = dalloc(ns); if (has_eta) { pairs = dalloc(ns); check_cuda(cudaMemsetAsync(pairs, 0, ns * 8, stream), "memset"); } }
+        partial_cap = std::max(step_main_blocks(sp), 148 * 4) + 8;
+        partials = dalloc_t<StepPartial>(partial_cap);
+        st = dalloc_t<Status>(1);
+        bud = dalloc_t<DevBudget>(1);
+        diag_part = dalloc_t<DiagOut>(148 * 4 + 8);
+        diag_out = dalloc_t<DiagOut>(1);
+        red_out = dalloc_t<StepPartial>(1);
+        check_cuda(cudaMallocHost(&h_st, sizeof(Status)), "cudaMallocHost");
+        check_cuda(cudaMemsetAsync(bud, 0, sizeof(DevBudget), stream), "memset");
+        Status s0{ERR_NONE, 0, 0, -1, 0};
+        *h_st = s0;
+        check_cuda(cudaMemcpyAsync(st, h_st, sizeof(Status), cudaMemcpyHostToDevice, stream), "memcpy");
+
+        voronoi();
+        InitParams I{};
+        I.g = g; I.bulk_cr = c.bulk_cr; I.layer_o = c.layer_o; I.inlet_layer = c.bc == NICR_BC_CONCENTRATION;
+        launch_init_fields(I, o_[0], cr_[0], p_[0], stream);
+        if (dim == 2) check_cuda(cudaMemcpyAsync(gb_initial, gb_[0], ns * 8, cudaMemcpyDeviceToDevice, stream), "memcpy");
+        reset_inventory();
+        if (c.nucleation == NICR_NUC_CENTER) init_center_seed();
+        if (has_eta) {
+            if ((int)(seeds.size() / dim) > c.max_eta_fields)
+                throw Error(NICR_ERR_INVALID_ARG, dim == 3 ? "Too many eta fields; check --max-eta-fields and memory."
+                                                           : "Too many eta fields. Increase --max-eta-fields only after checking memory, or use --grain-evolution off.");
+            init_eta();
+            if (dim == 3) grain_retained = false;
+        }
+        if (c.nucleation == NICR_NUC_KSP) setup_ksp();
+        if (has_eta) eta_mask_now();
+        check_cuda(cudaStreamSynchronize(stream), "init");
+        check_cuda(cudaGetLastError(), "init kernels");
+    } catch (...) {
+        release();
+        throw;
+    }
+}
+
+Model::~Model() { release(); }
+
+void Model::release() {
+    if (stream) cudaStreamSynchronize(stream);
+    double* bufs[] = {o_[0], o_[1], cr_[0], cr_[1], p_[0], p_[1], gb_[0], gb_[1], s2_[0], s2_[1], eta_[0], eta_[1],
+                      grain, pairs, gb_initial, muO, muCr, mo, mc};
+    for (double* b : bufs) if (b) cudaFree(b);
+    void* others[] = {partials, st, bud, diag_part, diag_out, red_out, kres, d_shadow, d_ball, d_hyp,
+                      kw.flag, kw.blocked, kw.counts, kw.list, kw.total};
+    for (void* b : others) if (b) cudaFree(b);
+    if (h_st) cudaFreeHost(h_st);
+    if (stream) cudaStreamDestroy(stream);
+    std::memset(o_, 0, sizeof o_); std::memset(cr_, 0, sizeof cr_); std::memset(p_, 0, sizeof p_);
+    std::memset(gb_, 0, sizeof gb_); std::memset(s2_, 0, sizeof s2_); std::memset(eta_, 0, sizeof eta_);
+    grain = pairs = gb_initial = muO = muCr = mo = mc = nullptr;
+    partials = nullptr; st = nullptr; bud = nullptr; diag_part = diag_out = nullptr; red_out = nullptr; kres = nullptr;
+    d_shadow = d_ball = nullptr; d_hyp = nullptr; kw = KspWork{}; h_st = nullptr; stream = nullptr;
+}
+
+void Model::sync() { check_cuda(cudaStreamSynchronize(stream), "stream"); }
+
+void Model::copy_out(const double* d, double* host) {
+    check_cuda(cudaMemcpy2DAsync(host, (size_t)g.nb * 8, d, (size_t)g.pb * 8, (size_t)g.nb * 8, (size_t)g.nx * g.na,
+                                 cudaMemcpyDeviceToHost, stream), "D2H");
+    sync();
+}
+void Model::copy_in(double* d, const double* host) {
+    check_cuda(cudaMemcpy2DAsync(d, (size_t)g.pb * 8, host, (size_t)g.nb * 8, (size_t)g.nb * 8, (size_t)g.nx * g.na,
+                                 cudaMemcpyHostToDevice, stream), "H2D");
+    sync();
+}
+
+// ------------------------------------------------------------------ init
+// Voronoi grains (3S:407-467, 2D:233-291). Seeds come from libstdc++'s
+// mt19937_64 + uniform_real_distribution exactly as in the reference.
+void Model::voronoi() {
+    seeds.clear();
+    volumes.clear();
+    const size_t ns = (size_t)g.nstore;
+    if (!c.grains) {
+        seeds.push_back(0.5 * c.nx);
+        seeds.push_back(0.5 * c.ny);
+        if (dim == 3) seeds.push_back(0.5 * c.nz);
+        volumes.push_back(dim == 3 ? (long long)(c.nx * c.ny * c.nz) : (long long)(c.nx * c.ny));
+        std::vector<double> ones((size_t)g.ncells, 1.);
+        copy_in(grain, ones.data());
+        check_cuda(cudaMemsetAsync(gb_[0], 0, ns * 8, stream), "memset");
+        return;
+    }
+    int ng;
+    if (dim == 3) {
+        const double volume = double(c.nx) * c.ny * c.nz;
+        const double ng_real = 6. * volume / (PI * std::pow(c.grain_diameter_grid, 3));
+        if (!std::isfinite(ng_real) || ng_real > volume + .5) throw Error(NICR_ERR_INVALID_ARG, "Too many Voronoi sites for this grid.");
+        ng = std::max(1, int(std::llround(ng_real)));
+        if (ng > volume) throw Error(NICR_ERR_INVALID_ARG, "Too many Voronoi sites for this grid.");
+        if (has_eta && ng > c.max_eta_fields)
+            throw Error(NICR_ERR_INVALID_ARG, "3D grain count exceeds --max-eta-fields; increase grain diameter or check memory before increasing the limit.");
+    } else {
+        const double domain_area = double(c.nx) * c.ny;
+        ng = std::max(1, int(std::llround(4. * domain_area / (PI * c.grain_diameter_grid * c.grain_diameter_grid))));
+        if (ng > c.nx * c.ny) throw Error(NICR_ERR_INVALID_ARG, "Too many Voronoi sites for this grid.");
+    }
+    std::mt19937_64 rng(c.random_seed);
+    std::uniform_real_distribution<double> ux(0., double(c.nx)), uy(0., double(c.ny)), uz(0., double(c.nz));
+    for (int q = 0; q < ng; ++q) {
+        const double x = ux(rng), y = uy(rng);
+        seeds.push_back(x);
+        seeds.push_back(y);
+        if (dim == 3) seeds.push_back(uz(rng));
+    }
+    const int D = dim;
+    if (D == 3) {
+        if (c.left_edge_sites < 0 || c.left_edge_sites > std::min(ng, c.ny * c.nz))
+            throw Error(NICR_ERR_INVALID_ARG, "--left-face-sites must be between 0 and min(volume-based site count, ny*nz).");
+        if (c.left_edge_sites > 0) {  // 3S:430-449
+            const int n = c.left_edge_sites;
+            int rows = std::clamp(int(std::llround(std::sqrt(double(n) * c.ny / c.nz))), 1, std::min(n, c.ny));
+            rows = std::max(rows, (n + c.nz - 1) / c.nz);
+            std::uniform_real_distribution<double> unit(0., 1.);
+            const int phaseY = std::min(c.ny - 1, int(unit(rng) * c.ny));
+            const int phaseZ = std::min(c.nz - 1, int(unit(rng) * c.nz));
+            int q = 0;
+            for (int r = 0; r < rows; ++r) {
+                const int cols = n / rows + (r < n % rows ? 1 : 0);
+                const int yy = (phaseY + int(static_cast<long long>(r) * c.ny / rows)) % c.ny;
+                for (int k = 0; k < cols; ++k) {
+                    const int zz = (phaseZ + int(static_cast<long long>(k) * c.nz / cols)) % c.nz;
+                    seeds[3 * q] = 0.05 + 0.4 * unit(rng);
+                    seeds[3 * q + 1] = yy + 0.5;
+                    seeds[3 * q + 2] = zz + 0.5;
+                    ++q;
+                }
+            }
+            for (int s = n; s < ng; ++s) seeds[3 * s] = 1.5 + (c.nx - 1.5) * (seeds[3 * s] / c.nx);
+        }
+    } else {
+        if (c.left_edge_sites < 0 || c.left_edge_sites > std::min(ng, c.ny))
+            throw Error(NICR_ERR_INVALID_ARG, "--left-edge-sites must be between 0 and min(area-based site count, ny).");
+        if (c.left_edge_sites > 0) {  // 2D:251-265
+            std::uniform_real_distribution<double> unit(0., 1.);
+            const int phase = std::min(c.ny - 1, int(unit(rng) * c.ny));
+            for (int k = 0; k < c.left_edge_sites; ++k) {
+                const int row = (phase + int((static_cast<long long>(k) * c.ny) / c.left_edge_sites)) % c.ny;
+                seeds[2 * k] = 0.05 + 0.4 * unit(rng);
+                seeds[2 * k + 1] = row + 0.5;
+            }
+            for (int k = c.left_edge_sites; k < ng; ++k) seeds[2 * k] = 1.5 + (c.nx - 1.5) * (seeds[2 * k] / c.nx);
+        }
+    }
+    volumes.assign(ng, 0);
+    const double f2 = c.gb_fwhm_grid * c.gb_fwhm_grid;
+    std::vector<double> gb_h((size_t)g.ncells);
+    if (D == 3) {
+        // labels and bisector distances on the GPU; the Gaussian on the host C library
+        double* d_seeds = dalloc(seeds.size());
+        int* d_vol = dalloc_t<int>(ng);
+        double* d_db = gb_[0];
+        check_cuda(cudaMemcpyAsync(d_seeds, seeds.data(), seeds.size() * 8, cudaMemcpyHostToDevice, stream), "H2D");
+        check_cuda(cudaMemsetAsync(d_vol, 0, ng * sizeof(int), stream), "memset");
+        InitParams I{};
+        I.g = g; I.ng = ng; I.nxd = c.nx; I.nyd = c.ny; I.nzd = c.nz;
+        launch_voronoi3(I, d_seeds, grain, d_db, d_vol, stream);
+        std::vector<int> vol(ng);
+        check_cuda(cudaMemcpyAsync(vol.data(), d_vol, ng * sizeof(int), cudaMemcpyDeviceToHost, stream), "D2H");
+        copy_out(d_db, gb_h.data());
+        for (int q = 0; q < ng; ++q) volumes[q] = vol[q];
+        cudaFree(d_seeds);
+        cudaFree(d_vol);
+        dev_bytes -= seeds.size() * 8 + ng * sizeof(int);
+        parallel_for(g.ncells, [&](long long b, long long e) {
+            for (long long q = b; q < e; ++q) {
+                const double db = gb_h[q];
+                gb_h[q] = ng == 1 ? 0. : std::exp(-4. * std::log(2.) * db * db / f2);
+            }
+        });
+        copy_in(gb_[0], gb_h.data());
+    } else {
+        std::vector<double> grain_h((size_t)g.ncells);
+        voronoi2d_host(grain_h, gb_h);
+        copy_in(grain, grain_h.data());
+        copy_in(gb_[0], gb_h.data());
+    }
+}
+
+void Model::voronoi2d_host(std::vector<double>& grain_h, std::vector<double>& gb_h) {
+    const int ng = (int)(seeds.size() / 2);
+    const double f2 = c.gb_fwhm_grid * c.gb_fwhm_grid;
+    std::vector<long long> vol(ng, 0);
+    // labels first (cheap, serial for the area counts), then the mask in parallel
+    std::vector<double> oy((size_t)g.ncells), rb((size_t)g.ncells);
+    for (int i = 1; i <= c.nx; ++i)
+        for (int j = 1; j <= c.ny; ++j) {
+            const double x = i - .5, y = j - .5;
+            int owner = 0;
+            double rbest = std::numeric_limits<double>::infinity(), ownerY = 0.;
+            for (int k = 0; k < ng; ++k) {
+                const double dy = min_image(seeds[2 * k + 1] - y, c.ny);
+                const double r = (seeds[2 * k] - x) * (seeds[2 * k] - x) + dy * dy;
+                if (r < rbest) { rbest = r; owner = k; ownerY = y + dy; }
+            }
+            const size_t q = (size_t)(i - 1) * c.ny + (j - 1);
+            grain_h[q] = owner + 1;
+            oy[q] = ownerY;
+            rb[q] = rbest;
+            ++vol[owner];
+        }
+    parallel_for(g.ncells, [&](long long b, long long e) {
+        for (long long q = b; q < e; ++q) {
+            const int i = (int)(q / c.ny) + 1, j = (int)(q % c.ny) + 1;
+            const double x = i - .5, y = j - .5;
+            const int owner = (int)grain_h[q] - 1;
+            double db = std::numeric_limits<double>::infinity();
+            for (int k = 0; k < ng; ++k) {
+                if (k == owner) continue;
+                for (int im = -1; im <= 1; ++im) {
+                    const double ym = seeds[2 * k + 1] + im * c.ny;
+                    const double rs = (seeds[2 * k] - x) * (seeds[2 * k] - x) + (ym - y) * (ym - y);
+                    const double sep = std::hypot(seeds[2 * k] - seeds[2 * owner], ym - oy[q]);
+                    if (sep > 1.e-14) db = std::min(db, std::max(0., (rs - rb[q]) / (2. * sep)));
+                }
+            }
+            gb_h[q] = ng == 1 ? 0. : std::exp(-4. * std::log(2.) * db * db / f2);
+        }
+    });
+    for (int k = 0; k < ng; ++k) volumes[k] = vol[k];
+}
+
+void Model::reset_inventory() {
+    launch_diagnostics(g, o_[cur], cr_[cur], p_[cur], diag_part, nullptr, diag_out, stream);
+    DiagOut d;
+    check_cuda(cudaMemcpyAsync(&d, diag_out, sizeof d, cudaMemcpyDeviceToHost, stream), "D2H");
+    sync();
+    DevBudget b;
+    check_cuda(cudaMemcpyAsync(&b, bud, sizeof b, cudaMemcpyDeviceToHost, stream), "D2H");
+    sync();
+    b.initialO[0] = d.sum[0][0]; b.initialO[1] = d.sum[0][1];
+    b.initialCr[0] = d.sum[1][0]; b.initialCr[1] = d.sum[1][1];
+    check_cuda(cudaMemcpyAsync(bud, &b, sizeof b, cudaMemcpyHostToDevice, stream), "H2D");
+    sync();
+}
+
+// initialize_center_oxide (3S:725-751, 2D:517-542)
+void Model::init_center_seed() {
+    const double x = 0.5 * (double(c.nx) + 1.), y = 0.5 * (double(c.ny) + 1.), z = 0.5 * (double(c.nz) + 1.);
+    const double r = c.radius_grid;
+    const int mn = dim == 3 ? std::min({c.nx, c.ny, c.nz}) : std::min(c.nx, c.ny);
+    if (r >= 0.5 * (double(mn) - 1.))
+        throw Error(NICR_ERR_INVALID_ARG, dim == 3 ? "Center seed is too large: --radius-grid must be less than (min(nx,ny,nz)-1)/2."
+                                                   : "Center seed is too large: --radius-grid must be less than (min(nx,ny)-1)/2.");
+    InitParams I{};
+    I.g = g;
+    int nb = 0;
+    launch_center_seed(I, x, y, z, r, 0, o_[cur], cr_[cur], p_[cur], nullptr, partials, stream, &nb);
+    launch_reduce_partials(partials, nb, red_out, stream);
+    StepPartial s;
+    check_cuda(cudaMemcpyAsync(&s, red_out, sizeof s, cudaMemcpyDeviceToHost, stream), "D2H");
+    DevBudget b;
+    check_cuda(cudaMemcpyAsync(&b, bud, sizeof b, cudaMemcpyDeviceToHost, stream), "D2H");
+    sync();
+    center_seed_cells = (int)s.clipped;
+    if (center_seed_cells == 0) throw Error(NICR_ERR_INVALID_ARG, "Center seed covers no cell centres: increase --radius-grid.");
+    b.v[0][0] = s.s[0][0]; b.v[0][1] = s.s[0][1];
+    b.v[1][0] = s.s[1][0]; b.v[1][1] = s.s[1][1];
+    b.nuclei += 1;
+    check_cuda(cudaMemcpyAsync(bud, &b, sizeof b, cudaMemcpyHostToDevice, stream), "H2D");
+    sync();
+}
+
+// initialize_eta (3S:469-494, 2D:293-327): weights exp(-d/ell) normalised,
+// times 1-h(phi). Competitor distances on the GPU (3D), exp on the host.
+void Model::init_eta() {
+    const int ng = (int)(seeds.size() / dim);
+    neta = ng;
+    const size_t ns = (size_t)g.nstore;
+    eta_[0] = dalloc(ns * ng);
+    check_cuda(cudaMemsetAsync(eta_[0], 0, ns * ng * 8, stream), "memset");
+    if (advance_eta) eta_[1] = dalloc(ns * ng);
+    const long long n = g.ncells;
+    const double ell_grid = ec.ell / c.dx;
+    std::vector<double> ph((size_t)n), grain_h((size_t)n);
+    copy_out(p_[cur], ph.data());
+    copy_out(grain, grain_h.data());
+    std::vector<double> d((size_t)n * ng);
+    if (dim == 3) {
+        double* d_seeds = dalloc(seeds.size());
+        check_cuda(cudaMemcpyAsync(d_seeds, seeds.data(), seeds.size() * 8, cudaMemcpyHostToDevice, stream), "H2D");
+        InitParams I{};
+        I.g = g; I.ng = ng; I.nxd = c.nx; I.nyd = c.ny; I.nzd = c.nz;
+        launch_eta_dist3(I, d_seeds, grain, eta_[0], stream);
+        for (int q = 0; q < ng; ++q) copy_out(eta_[0] + (size_t)q * ns, d.data() + (size_t)q * n);
+        cudaFree(d_seeds);
+        dev_bytes -= seeds.size() * 8;
+    }
+    std::vector<double> eta_h((size_t)n * ng);
+    parallel_for(n, [&](long long b, long long e) {
+        std::vector<double> w(ng);
+        for (long long q = b; q < e; ++q) {
+            const int owner = int(grain_h[q]) - 1;
+            double norm = 0.;
+            if (dim == 3) {
+                for (int s = 0; s < ng; ++s) {
+                    w[s] = s == owner ? 1. : std::exp(-d[(size_t)s * n + q] / ell_grid);
+                    norm += w[s];
+                }
+            } else {
+                const int i = (int)(q / c.ny) + 1, j = (int)(q % c.ny) + 1;
+                const double x = i - .5, y = j - .5;
+                const double oy = y + min_image(seeds[2 * owner + 1] - y, c.ny);
+                const double rbest = std::pow(seeds[2 * owner] - x, 2) + std::pow(oy - y, 2);
+                for (int s = 0; s < ng; ++s) {
+                    if (s == owner) { w[s] = 1.; norm += 1.; continue; }
+                    double distance = std::numeric_limits<double>::infinity();
+                    for (int im = -1; im <= 1; ++im) {
+                        const double gy = seeds[2 * s + 1] + im * c.ny;
+                        const double sep = std::hypot(seeds[2 * s] - seeds[2 * owner], gy - oy);
+                        const double rr = std::pow(seeds[2 * s] - x, 2) + std::pow(gy - y, 2);
+                        if (sep > 1.e-14) distance = std::min(distance, std::max(0., (rr - rbest) / (2. * sep)));
+                    }
+                    w[s] = std::exp(-distance / ell_grid);
+                    norm += w[s];
+                }
+            }
+            const double metal = 1. - h(ph[q]);
+            for (int s = 0; s < ng; ++s) eta_h[(size_t)s * n + q] = metal * w[s] / norm;
+        }
+    });
+    for (int q = 0; q < ng; ++q) copy_in(eta_[0] + (size_t)q * ns, eta_h.data() + (size_t)q * n);
+    eta_dirty = true;
+}
+
+void Model::eta_mask_now() {
+    if (!has_eta) return;
+    launch_eta_mask(sp, neta, eta_[ecur], gb_[gcur], s2_[gcur], dim == 2 ? pairs : nullptr, st, stream);
+    eta_dirty = false;
+}
+
+// Ksp tables: ball and exclusion offsets, 2D hypot table (C library hypot).
+void Model::setup_ksp() {
+    const double r = c.radius_grid, limit = r + c.exclusion_gap_grid;
+    const int rr = dim == 3 ? bounded_reach_h(r, c.nx) : int(std::ceil(r));
+    const int sr = dim == 3 ? bounded_reach_h(limit, c.nx) : int(std::ceil(limit));
+    const int B = rr + sr;
+    std::vector<int> ball, shadow;
+    if (dim == 3) {
+        for (int di = -rr; di <= rr; ++di)
+            for (int dj = -rr; dj <= rr; ++dj)
+                for (int dk = -rr; dk <= rr; ++dk)
+                    if (double(di * di) + double(dj) * dj + double(dk) * dk <= r * r) { ball.push_back(di); ball.push_back(dj); ball.push_back(dk); }
+    } else {
+        for (int di = -rr; di <= rr; ++di)
+            for (int dj = -rr; dj <= rr; ++dj)
+                if (double(di * di) + double(dj) * dj <= r * r) { ball.push_back(di); ball.push_back(dj); ball.push_back(0); }
+    }
+    const int nball = (int)ball.size() / 3;
+    // 2D predicate table over |di| <= 2B, |dj| <= max(ny/2, 2B)
+    const int hrows = 2 * B + 1, hcols = std::max(c.ny / 2 + 1, 2 * B + 1);
+    std::vector<unsigned char> hyp;
+    if (dim == 2) {
+        hyp.resize((size_t)hrows * hcols);
+        for (int a = 0; a < hrows; ++a)
+            for (int b = 0; b < hcols; ++b) hyp[(size_t)a * hcols + b] = std::hypot(double(a), double(b)) < limit ? 1 : 0;
+    }
+    auto near = [&](int di, int dj, int dk) {
+        if (dim == 3) return std::sqrt(std::pow(double(di), 2) + std::pow(double(dj), 2) + std::pow(double(dk), 2)) < limit;
+        return hyp[(size_t)std::abs(di) * hcols + std::abs(dj)] != 0;
+    };
+    const int kz = dim == 3 ? B : 0;
+    for (int di = -B; di <= B; ++di)
+        for (int dj = -B; dj <= B; ++dj)
+            for (int dk = -kz; dk <= kz; ++dk) {
+                bool hit = false;
+                for (int b = 0; b < nball && !hit; ++b)
+                    hit = near(di - ball[3 * b], dj - ball[3 * b + 1], dk - ball[3 * b + 2]);
+                if (hit) { shadow.push_back(di); shadow.push_back(dj); shadow.push_back(dk); }
+            }
+    d_ball = dalloc_t<int>(ball.size());
+    d_shadow = dalloc_t<int>(shadow.size());
+    check_cuda(cudaMemcpyAsync(d_ball, ball.data(), ball.size() * 4, cudaMemcpyHostToDevice, stream), "H2D");
+    check_cuda(cudaMemcpyAsync(d_shadow, shadow.data(), shadow.size() * 4, cudaMemcpyHostToDevice, stream), "H2D");
+    if (dim == 2) {
+        d_hyp = dalloc_t<unsigned char>(hyp.size());
+        check_cuda(cudaMemcpyAsync(d_hyp, hyp.data(), hyp.size(), cudaMemcpyHostToDevice, stream), "H2D");
+    }
+    kd.g = g;
+    kd.nx = c.nx; kd.ny = c.ny; kd.nz = dim == 3 ? c.nz : 1;
+    kd.radius = r; kd.gap = c.exclusion_gap_grid; kd.ksp = c.ksp;
+    kd.neta = 0;  // set at scan time
+    kd.hyp2d = d_hyp; kd.hyp_stride = hcols;
+    kd.shadow = d_shadow; kd.n_shadow = (int)shadow.size() / 3;
+    kd.ball = d_ball; kd.n_ball = nball;
+    kd.full_ball = nball;
+    kd.box_half = B;
+    kw.flag = dalloc_t<unsigned char>((size_t)g.ncells);
+    kw.blocked = dalloc_t<unsigned char>((size_t)g.ncells);
+    kw.counts = dalloc_t<int>(ksp_compact_blocks(g.ncells) + 1);
+    kw.list = dalloc_t<long long>((size_t)g.ncells);
+    kw.total = dalloc_t<int>(1);
+    kres = dalloc_t<KspResult>(1);
+    check_cuda(cudaMemsetAsync(kres, 0, sizeof(KspResult), stream), "memset");
+    sync();
+}
+
+// ------------------------------------------------------------------ fields
+static bool is_state_field(int f) { return f == NICR_FIELD_O || f == NICR_FIELD_CR || f == NICR_FIELD_PHI || f == NICR_FIELD_ETA; }
+
+void Model::set_field(int field, int index, const double* host) {
+    if (!is_state_field(field)) throw Error(NICR_ERR_INVALID_ARG, "only O, CR, PHI and ETA can be set");
+    double* d = nullptr;
+    if (field == NICR_FIELD_O) d = o_[cur];
+    else if (field == NICR_FIELD_CR) d = cr_[cur];
+    else if (field == NICR_FIELD_PHI) d = p_[cur];
+    else {
+        if (index < 0 || index >= neta) throw Error(NICR_ERR_INVALID_ARG, "eta index out of range");
+        d = eta_[ecur] + (size_t)index * g.nstore;
+    }
+    copy_in(d, host);
+    eta_dirty = true;  // any edit invalidates the frozen-eta cache (3S:347-349)
+}
+
+void Model::refresh() {
+    if (has_eta && (eta_dirty || dim == 2)) eta_mask_now();
+    if (!muO) {
+        const size_t ns = (size_t)g.nstore;
+        muO = dalloc(ns); muCr = dalloc(ns); mo = dalloc(ns); mc = dalloc(ns);
+    }
+    launch_refresh(sp, o_[cur], cr_[cur], p_[cur], gb_[gcur], muO, muCr, mo, mc, stream);
+    check_cuda(cudaGetLastError(), "refresh");
+}
+
+void Model::get_field(int field, int index, double* host) {
+    const double* d = nullptr;
+    switch (field) {
+        case NICR_FIELD_O: d = o_[cur]; break;
+        case NICR_FIELD_CR: d = cr_[cur]; break;
+        case NICR_FIELD_PHI: d = p_[cur]; break;
+        case NICR_FIELD_ETA:
+            if (index < 0 || index >= neta) throw Error(NICR_ERR_INVALID_ARG, "eta index out of range");
+            d = eta_[ecur] + (size_t)index * g.nstore;
+            break;
+        case NICR_FIELD_MU_O: refresh(); d = muO; break;
+        case NICR_FIELD_MU_CR: refresh(); d = muCr; break;
+        case NICR_FIELD_M_O: refresh(); d = mo; break;
+        case NICR_FIELD_M_CR: refresh(); d = mc; break;
+        case NICR_FIELD_GB:
+            if (has_eta && eta_dirty) eta_mask_now();
+            d = gb_[gcur];
+            break;
+        case NICR_FIELD_GRAIN:
+            if (!grain_retained) throw Error(NICR_ERR_STATE, "the initial grain map is not retained when eta evolves (3D)");
+            d = grain;
+            break;
+        case NICR_FIELD_ETA_S2:
+            if (!has_eta) throw Error(NICR_ERR_STATE, "eta_s2 exists only with evolving grains");
+            if (eta_dirty) eta_mask_now();
+            d = s2_[gcur];
+            break;
+        case NICR_FIELD_ETA_PAIRS:
+            if (!has_eta || dim != 2) throw Error(NICR_ERR_STATE, "eta_pairs exists only in 2D with evolving grains");
+            eta_mask_now();
+            d = pairs;
+            break;
+        case NICR_FIELD_GB_INITIAL:
+            if (dim != 2) throw Error(NICR_ERR_STATE, "gb_initial exists only in 2D");
+            d = gb_initial;
+            break;
+        default: throw Error(NICR_ERR_INVALID_ARG, "unknown field");
+    }
+    copy_out(d, host);
+}
+
+// ------------------------------------------------------------------ stepping
+void Model::reset_status() {
+    // keep steps_done; clear the failure state for a new batch
+    h_st->err_key = ERR_NONE;
+    h_st->failed = 0;
+    h_st->failed_step = -1;
+    h_st->steps_done = steps_done;
+    check_cuda(cudaMemcpyAsync(st, h_st, sizeof(Status), cudaMemcpyHostToDevice, stream), "H2D");
+}
+
+void Model::enqueue_step() {
+    const int nxt = cur ^ 1;
+    if (has_eta && eta_dirty) eta_mask_now();
+    int nb = 0;
+    launch_step_main(sp, o_[cur], cr_[cur], p_[cur], gb_[gcur], has_eta ? s2_[gcur] : nullptr, o_[nxt], cr_[nxt],
+                     p_[nxt], partials, st, stream, &nb);
+    if (advance_eta)
+        launch_eta_update(sp, neta, eta_[ecur], s2_[gcur], p_[cur], eta_[ecur ^ 1], gb_[gcur ^ 1], s2_[gcur ^ 1], st, stream);
+    launch_step_finalize(partials, nb, bud, st, 0, stream);
+    cur = nxt;
+    if (advance_eta) { ecur ^= 1; gcur ^= 1; }
+}
+
+std::string Model::describe_failure(unsigned long long key, int nxt) {
+    std::ostringstream msg;
+    auto coords = [&](long long cell, int& i, int& j, int& k) {
+        const int col = (int)(cell % g.nb);
+        const long long r = cell / g.nb;
+        const int row = (int)(r % g.na);
+        i = (int)(r / g.na) + 1;
+        if (dim == 3) { j = row + 1; k = col + 1; } else { j = col + 1; k = 0; }
+        return (long long)(i - 1) * g.plane + (long long)row * g.pb + col;
+    };
+    int i, j, k;
+    if (key < ERR_ETA_BASE) {
+        const long long cell = (long long)(key / 4);
+        if (key % 4 == 0) return "Nonfinite trial field: reduce dt / inspect the model; no update accepted.";
+        const long long idx = coords(cell, i, j, k);
+        double v[3];
+        check_cuda(cudaMemcpyAsync(&v[0], o_[nxt] + idx, 8, cudaMemcpyDeviceToHost, stream), "D2H");
+        check_cuda(cudaMemcpyAsync(&v[1], cr_[nxt] + idx, 8, cudaMemcpyDeviceToHost, stream), "D2H");
+        check_cuda(cudaMemcpyAsync(&v[2], p_[nxt] + idx, 8, cudaMemcpyDeviceToHost, stream), "D2H");
+        sync();
+        msg << std::scientific << std::setprecision(16) << "Out-of-bounds trial at (" << i << "," << j;
+        if (dim == 3) msg << "," << k;
+        msg << "): O=" << v[0] << ", Cr=" << v[1] << ", phi=" << v[2]
+            << ". No clipping/update accepted. Reduce dt; if failure persists, investigate model.";
+        return msg.str();
+    }
+    const unsigned long long q = key - ERR_ETA_BASE;
+    const int gi = (int)(q / (unsigned long long)g.ncells);
+    const long long idx = coords((long long)(q % (unsigned long long)g.ncells), i, j, k);
+    double v;
+    check_cuda(cudaMemcpyAsync(&v, eta_[ecur ^ 1] + (size_t)gi * g.nstore + idx, 8, cudaMemcpyDeviceToHost, stream), "D2H");
+    sync();
+    msg << std::setprecision(17) << "Eta trial outside [0,1]: grain=" << gi + 1 << " cell=(" << i << "," << j;
+    if (dim == 3) msg << "," << k;
+    msg << ") value=" << v << ". All PDE fields rejected together; eta is never clipped. Check eta coefficients/dt.";
+    return msg.str();
+}
+
+int Model::finish_batch(long long before, int enqueued, const std::vector<double>* nuc_sched, int* completed) {
+    check_cuda(cudaMemcpyAsync(h_st, st, sizeof(Status), cudaMemcpyDeviceToHost, stream), "D2H");
+    sync();
+    check_cuda(cudaGetLastError(), "step kernels");
+    if (!h_st->failed) {
+        steps_done = before + enqueued;
+        if (completed) *completed = enqueued;
+        return NICR_OK;
+    }
+    const int accepted = (int)(h_st->failed_step - before);
+    // every step toggled the buffer parity; the valid state is the input of the failed step
+    const int undo = (enqueued - accepted) & 1;
+    cur ^= undo;
+    if (advance_eta) { ecur ^= undo; gcur ^= undo; }
+    steps_done = before + accepted;
+    if (completed) *completed = accepted;
+    if (nuc_sched) next_nucleation = (*nuc_sched)[accepted];
+    const unsigned long long key = h_st->err_key;
+    last_error = describe_failure(key, cur ^ 1);
+    if (dim == 2 && sp.inlet) {
+        // 2D leaves the enforced inlet layer in place after a rejection (2D:553, 2D:1224)
+        std::vector<double> plane((size_t)g.nb, c.layer_o);
+        check_cuda(cudaMemcpyAsync(o_[cur], plane.data(), plane.size() * 8, cudaMemcpyHostToDevice, stream), "H2D");
+        sync();
+        // the enforce_legacy_layer increment is part of the rolled-back budget
+    }
+    if (has_eta) eta_dirty = true;
+    if (key < ERR_ETA_BASE) return key % 4 == 0 ? NICR_ERR_TRIAL_NONFINITE : NICR_ERR_TRIAL_BOUNDS;
+    return NICR_ERR_ETA_RANGE;
+}
+
+int Model::step(int nsteps, int* completed) {
+    if (completed) *completed = 0;
+    if (nsteps <= 0) return NICR_OK;
+    reset_status();
+    const long long before = steps_done;
+    for (int s = 0; s < nsteps; ++s) enqueue_step();
+    return finish_batch(before, nsteps, nullptr, completed);
+}
+
+int Model::run(int nsteps, int* completed) {
+    if (completed) *completed = 0;
+    if (nsteps <= 0) return NICR_OK;
+    reset_status();
+    const long long before = steps_done;
+    std::vector<double> sched((size_t)nsteps + 1);
+    double next = next_nucleation;
+    for (int s = 0; s < nsteps; ++s) {
+        const long long n = before + s + 1;
+        const double time = double(n) * c.dt;
+        if (c.nucleation == NICR_NUC_KSP && time + 1.e-12 * c.nucleation_period >= next) {
+            kd.neta = neta;
+            launch_ksp_scan(kd, o_[cur], cr_[cur], p_[cur], eta_[ecur], kw, bud, kres, st, stream);
+            if (has_eta) eta_dirty = true;
+            next += c.nucleation_period;
+        }
+        sched[s] = next;
+        enqueue_step();
+    }
+    sched[nsteps] = next;
+    const int rc = finish_batch(before, nsteps, &sched, completed);
+    if (rc == NICR_OK) next_nucleation = next;
+    return rc;
+}
+
+int Model::nucleate(int* nuclei) {
+    if (nuclei) *nuclei = 0;
+    if (c.nucleation != NICR_NUC_KSP) return NICR_OK;
+    reset_status();
+    kd.neta = neta;
+    launch_ksp_scan(kd, o_[cur], cr_[cur], p_[cur], eta_[ecur], kw, bud, kres, st, stream);
+    KspResult r;
+    check_cuda(cudaMemcpyAsync(&r, kres, sizeof r, cudaMemcpyDeviceToHost, stream), "D2H");
+    sync();
+    check_cuda(cudaGetLastError(), "ksp");
+    if (has_eta && r.nuclei) eta_dirty = true;
+    if (nuclei) *nuclei = r.nuclei;
+    return NICR_OK;
+}
+
+int Model::stamp(int x, int y, int z, int* cells) {
+    if (cells) *cells = 0;
+    if (x < 1 || x > c.nx || y < 1 || y > c.ny || (dim == 3 && (z < 1 || z > c.nz)))
+        throw Error(NICR_ERR_INVALID_ARG, "stamp centre outside the grid");
+    if (!kres) {
+        // stamps outside Ksp mode need the ball tables too
+        setup_ksp();
+    }
+    reset_status();
+    kd.neta = neta;
+    launch_ksp_stamp(kd, x, y, dim == 3 ? z : 0, o_[cur], cr_[cur], p_[cur], eta_[ecur], kw, bud, kres, st, stream);
+    KspResult r;
+    check_cuda(cudaMemcpyAsync(&r, kres, sizeof r, cudaMemcpyDeviceToHost, stream), "D2H");
+    sync();
+    check_cuda(cudaGetLastError(), "stamp");
+    if (has_eta && r.last_cells) eta_dirty = true;
+    if (cells) *cells = r.last_cells;
+    return NICR_OK;
+}
+
+void Model::budget(nicr_budget* out) {
+    DevBudget b;
+    check_cuda(cudaMemcpyAsync(&b, bud, sizeof b, cudaMemcpyDeviceToHost, stream), "D2H");
+    sync();
+    double* dst[8] = {out->nucO, out->nucCr, out->ckO, out->ckCr, out->clipO, out->clipCr, out->bcO, out->bcCr};
+    for (int q = 0; q < 8; ++q) { dst[q][0] = b.v[q][0]; dst[q][1] = b.v[q][1]; }
+    out->nuclei = b.nuclei;
+    out->clipped = b.clipped;
+    out->initialO[0] = b.initialO[0]; out->initialO[1] = b.initialO[1];
+    out->initialCr[0] = b.initialCr[0]; out->initialCr[1] = b.initialCr[1];
+}
+
+void Model::diagnostics(nicr_diagnostics* d) {
+    launch_diagnostics(g, o_[cur], cr_[cur], p_[cur], diag_part, nullptr, diag_out, stream);
+    DiagOut r;
+    check_cuda(cudaMemcpyAsync(&r, diag_out, sizeof r, cudaMemcpyDeviceToHost, stream), "D2H");
+    sync();
+    check_cuda(cudaGetLastError(), "diagnostics");
+    d->sum_O[0] = r.sum[0][0]; d->sum_O[1] = r.sum[0][1];
+    d->sum_Cr[0] = r.sum[1][0]; d->sum_Cr[1] = r.sum[1][1];
+    d->sum_phi[0] = r.sum[2][0]; d->sum_phi[1] = r.sum[2][1];
+    d->sum_h[0] = r.sum[3][0]; d->sum_h[1] = r.sum[3][1];
+    d->min_O = r.mn[0]; d->max_O = r.mx[0];
+    d->min_Cr = r.mn[1]; d->max_Cr = r.mx[1];
+    d->min_Ni = r.mn[2];
+    d->min_phi = r.mn[3]; d->max_phi = r.mx[3];
+}
+
+void Model::grain_stats(nicr_grain_stats*, long long*, double*) {
+    throw Error(NICR_ERR_STATE, "grain statistics are not available yet");
+}
+
+}  // namespace nicr

@@ -1,0 +1,128 @@
+// Host-side model: the B200 counterpart of the reference's class Model
+// (3S:336-978, 2D:194-711). It owns one domain resident in device memory and
+// orchestrates the kernels; host code does only what must match the C library
+// bit for bit at initialisation (random seeds via libstdc++, exp/hypot of the
+// Voronoi mask and eta weights) and the formatting of output files.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/nicr.h"
+#include "nicr_kernels.h"
+#include "nicr_ksp.h"
+#include "nicr_physics.h"
+
+namespace nicr {
+
+// Error carrying a nicr status code; the message is the reference's text.
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+void check_cuda(cudaError_t e, const char* what);
+
+class Model {
+public:
+    explicit Model(const nicr_config& cfg);
+    ~Model();
+    Model(const Model&) = delete;
+    Model& operator=(const Model&) = delete;
+
+    nicr_config c;
+    Grid g{};
+    int dim;
+    bool has_eta = false;      // grain_evolution && grains (3S:343)
+    bool advance_eta = false;  // eta trial/swap each step (3S:810, 2D:591)
+    int neta = 0;
+    EtaCoef ec{};
+    std::vector<double> seeds;         // dim doubles per seed
+    std::vector<long long> volumes;
+    int center_seed_cells = 0;
+    bool grain_retained = true;        // 3D frees the id map when eta is active (3S:377-380)
+    double next_nucleation;
+    long long steps_done = 0;          // accepted steps (host view)
+    std::string last_error;
+
+    cudaStream_t stream = nullptr;
+
+    // ---- API used by the C-ABI
+    void set_field(int field, int index, const double* host);
+    void get_field(int field, int index, double* host);
+    void refresh();                    // materialise mu/M (and eta mask) for output
+    void invalidate_eta_cache() { eta_dirty = true; }
+    void reset_inventory();
+    int step(int nsteps, int* completed);            // Model::step x n
+    int run(int nsteps, int* completed);             // run() schedule
+    int nucleate(int* nuclei);
+    int stamp(int x, int y, int z, int* cells);
+    void budget(nicr_budget* b);
+    void diagnostics(nicr_diagnostics* d);
+    void grain_stats(nicr_grain_stats* s, long long* cells, double* amount);
+    size_t device_bytes() const { return dev_bytes; }
+    void sync();
+
+    // raw device pointers of the current state (for tests, bench, writers)
+    double* d_o() const { return o_[cur]; }
+    double* d_cr() const { return cr_[cur]; }
+    double* d_p() const { return p_[cur]; }
+    double* d_gb() const { return gb_[gcur]; }
+    double* d_eta(int gi) const { return eta_[ecur] + (size_t)gi * g.nstore; }
+    StepParams params() const { return sp; }
+
+private:
+    StepParams sp{};
+    size_t dev_bytes = 0;
+    // state (ping-pong)
+    double* o_[2] = {nullptr, nullptr};
+    double* cr_[2] = {nullptr, nullptr};
+    double* p_[2] = {nullptr, nullptr};
+    int cur = 0;
+    double* gb_[2] = {nullptr, nullptr};   // mask; [1] used only when eta advances
+    double* s2_[2] = {nullptr, nullptr};
+    int gcur = 0;
+    double* eta_[2] = {nullptr, nullptr};  // neta fields each
+    int ecur = 0;
+    double* grain = nullptr;
+    double* pairs = nullptr;               // 2D eta_pairs (output only)
+    double* gb_initial = nullptr;          // 2D gb_initial (output only)
+    double *muO = nullptr, *muCr = nullptr, *mo = nullptr, *mc = nullptr;
+    bool eta_dirty = true;
+    // reductions / status
+    StepPartial* partials = nullptr;
+    int partial_cap = 0;
+    Status* st = nullptr;
+    DevBudget* bud = nullptr;
+    DiagOut* diag_part = nullptr;
+    DiagOut* diag_out = nullptr;
+    StepPartial* red_out = nullptr;
+    // Ksp
+    KspDev kd{};
+    KspWork kw{};
+    KspResult* kres = nullptr;
+    int* d_shadow = nullptr;
+    int* d_ball = nullptr;
+    unsigned char* d_hyp = nullptr;
+    // pinned host staging for small results
+    Status* h_st = nullptr;
+
+    void release();
+    double* dalloc(size_t n);
+    template <class T> T* dalloc_t(size_t n);
+    void voronoi();
+    void voronoi2d_host(std::vector<double>& grain_h, std::vector<double>& gb_h);
+    void init_center_seed();
+    void init_eta();
+    void setup_ksp();
+    void enqueue_step();
+    void reset_status();
+    int finish_batch(long long steps_before, int enqueued, const std::vector<double>* nuc_sched, int* completed);
+    std::string describe_failure(unsigned long long key, int parity_next);
+    void copy_out(const double* d, double* host);
+    void copy_in(double* d, const double* host);
+    void eta_mask_now();
+};
+
+}  // namespace nicr

@@ -1,0 +1,617 @@
+// Explicit time step of the Ni-Cr phase-field model on sm_100a.
+//
+// One fused pass per step replaces the reference's refresh() + update loop
+// (3S:597-620, 3S:761-826; 2D:412-434, 2D:551-597):
+//   ghosts -> mu_O, mu_Cr (7/5-point Laplacians) -> mobilities -> six-face
+//   conservative fluxes -> c_O, c_Cr, phi trial values -> legacy Ck -> bounds
+// Each CTA owns a rows x columns tile and streams along X (2.5D blocking):
+// o and cr are staged in shared memory with a radius-2 halo (mu at a
+// neighbour needs its Laplacian), phi and the computed mu/M planes with a
+// radius-1 halo. Nothing but the trial fields and per-CTA budget partials is
+// written to HBM: mu and M never leave the chip.
+//
+// The arithmetic is the reference's, operation for operation (nvcc -fmad=false,
+// IEEE division), so the FP64 results are bit-identical. Ghost semantics:
+// Neumann copies in X for o, cr, phi, gb and for the computed mu and M
+// (refresh copies mu(1) into the ghost, 3S:613-615), periodic rows/columns.
+#include <cuda_runtime.h>
+#include "nicr_kernels.h"
+#include "nicr_physics.h"
+
+namespace nicr {
+
+namespace {
+
+__device__ __forceinline__ int wrapi(int v, int n) {
+    v %= n;
+    return v < 0 ? v + n : v;
+}
+
+// Warp + block reduction of double-double values (fixed order => deterministic).
+__device__ __forceinline__ DD shfl_dd(DD v, int off) {
+    DD r;
+    r.hi = __shfl_down_sync(0xffffffffu, v.hi, off);
+    r.lo = __shfl_down_sync(0xffffffffu, v.lo, off);
+    return r;
+}
+template <int N>
+__device__ void block_reduce_dd(DD (&v)[N], long long& cnt, DD* sdd, long long* scnt) {
+    const int lane = threadIdx.x & 31;
+    const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+    const int nthreads = blockDim.x * blockDim.y * blockDim.z;
+    const int w = tid >> 5, nw = (nthreads + 31) >> 5;
+    // lanes of a warp are consecutive linear thread ids because blockDim.x is a multiple of 32
+    for (int off = 16; off > 0; off >>= 1) {
+        for (int q = 0; q < N; ++q) v[q] = dd_add(v[q], shfl_dd(v[q], off));
+        cnt += __shfl_down_sync(0xffffffffu, cnt, off);
+    }
+    if (lane == 0) {
+        for (int q = 0; q < N; ++q) sdd[w * N + q] = v[q];
+        scnt[w] = cnt;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        for (int q = 0; q < N; ++q) v[q] = sdd[q];
+        cnt = scnt[0];
+        for (int ww = 1; ww < nw; ++ww) {
+            for (int q = 0; q < N; ++q) v[q] = dd_add(v[q], sdd[ww * N + q]);
+            cnt += scnt[ww];
+        }
+    }
+}
+
+// Tile geometry of the fused step kernel.
+template <int DIM, int TA, int TB>
+struct Tile {
+    static constexpr int HA2 = DIM == 3 ? 2 : 0;   // row halo of the o/cr tiles
+    static constexpr int HA1 = DIM == 3 ? 1 : 0;   // row halo of the phi/mu/M tiles
+    static constexpr int RA2 = TA + 2 * HA2, RB2 = TB + 4;
+    static constexpr int RA1 = TA + 2 * HA1, RB1 = TB + 2;
+    static constexpr int S2 = RA2 * RB2, S1 = RA1 * RB1;
+    // shared memory: o[3], cr[3] (halo 2); p[3] (halo 1); muO, muCr, mo, mc [2] (halo 1)
+    static constexpr int SMEM_DOUBLES = 6 * S2 + 3 * S1 + 8 * S1;
+    static constexpr size_t SMEM_BYTES = SMEM_DOUBLES * sizeof(double) + 64 * (5 * 16 + 8);
+    static constexpr int NT = TA * TB;
+    __device__ static int i2(int a, int b) { return (a + HA2) * RB2 + (b + 2); }
+    __device__ static int i1(int a, int b) { return (a + HA1) * RB1 + (b + 1); }
+};
+
+struct CenterVals {
+    double o, cr, p, muO, muCr, mo, mc;
+};
+
+template <int DIM, int TA, int TB>
+struct StepKernel {
+    using T = Tile<DIM, TA, TB>;
+
+    // Loads plane xg (clamped to [0,nx-1]) of o and cr with a radius-2 halo
+    // into ring slot `slot`. The concentration inlet replaces o in plane 0 by
+    // layerO before the step (enforce_legacy_layer, 3S:593-596).
+    __device__ static void load_oc(const StepParams& P, const double* __restrict__ o,
+                                   const double* __restrict__ cr, int xg, double* so, double* scr,
+                                   int a0, int b0) {
+        const Grid& g = P.g;
+        xg = xg < 0 ? 0 : (xg > g.nx - 1 ? g.nx - 1 : xg);
+        const bool inlet = P.inlet && xg == 0;
+        const long long base = (long long)xg * g.plane;
+        const int tid = threadIdx.x + TB * threadIdx.y;
+        for (int q = tid; q < T::S2; q += T::NT) {
+            const int a = q / T::RB2 - T::HA2, b = q % T::RB2 - 2;
+            const int row = DIM == 3 ? wrapi(a0 + a, g.na) : 0;
+            const int col = wrapi(b0 + b, g.nb);
+            const long long idx = base + (long long)row * g.pb + col;
+            so[q] = inlet ? P.layer_o : __ldg(o + idx);
+            scr[q] = __ldg(cr + idx);
+        }
+    }
+    __device__ static void load_p(const StepParams& P, const double* __restrict__ p, int xg, double* sp,
+                                  int a0, int b0) {
+        const Grid& g = P.g;
+        xg = xg < 0 ? 0 : (xg > g.nx - 1 ? g.nx - 1 : xg);
+        const long long base = (long long)xg * g.plane;
+        const int tid = threadIdx.x + TB * threadIdx.y;
+        for (int q = tid; q < T::S1; q += T::NT) {
+            const int a = q / T::RB1 - T::HA1, b = q % T::RB1 - 1;
+            const int row = DIM == 3 ? wrapi(a0 + a, g.na) : 0;
+            const int col = wrapi(b0 + b, g.nb);
+            sp[q] = __ldg(p + base + (long long)row * g.pb + col);
+        }
+    }
+
+    // mu and M at tile point (a,b) of real plane x; writes the mu/M slot.
+    __device__ static CenterVals lead_point(const StepParams& P, const double* __restrict__ gb,
+                                            const double* som, const double* so0, const double* sop,
+                                            const double* scm, const double* sc0, const double* scp,
+                                            const double* sp, double* smuO, double* smuCr, double* smo,
+                                            double* smc, int x, int a, int b, int a0, int b0) {
+        const int c2 = T::i2(a, b);
+        const double oc = so0[c2], cc = sc0[c2];
+        double lapO, lapC;
+        if (DIM == 3) {
+            lapO = (sop[c2] - 2. * oc + som[c2]) / P.dxdx
+                 + (so0[T::i2(a + 1, b)] - 2. * oc + so0[T::i2(a - 1, b)]) / P.dada
+                 + (so0[T::i2(a, b + 1)] - 2. * oc + so0[T::i2(a, b - 1)]) / P.dbdb;
+            lapC = (scp[c2] - 2. * cc + scm[c2]) / P.dxdx
+                 + (sc0[T::i2(a + 1, b)] - 2. * cc + sc0[T::i2(a - 1, b)]) / P.dada
+                 + (sc0[T::i2(a, b + 1)] - 2. * cc + sc0[T::i2(a, b - 1)]) / P.dbdb;
+        } else {
+            lapO = (sop[c2] - 2. * oc + som[c2]) / P.dxdx
+                 + (so0[T::i2(a, b + 1)] - 2. * oc + so0[T::i2(a, b - 1)]) / P.dbdb;
+            lapC = (scp[c2] - 2. * cc + scm[c2]) / P.dxdx
+                 + (sc0[T::i2(a, b + 1)] - 2. * cc + sc0[T::i2(a, b - 1)]) / P.dbdb;
+        }
+        const int c1 = T::i1(a, b);
+        const double pc = sp[c1];
+        const double hh = h(pc);
+        CenterVals v;
+        v.o = oc; v.cr = cc; v.p = pc;
+        v.muO = mu_o_local(oc, cc, hh) - 2. * Phys::ko * lapO;
+        v.muCr = mu_cr_local(oc, cc, hh) - 2. * Phys::kc * lapC;
+        double gbv = 0.;
+        if (P.grains) {
+            const Grid& g = P.g;
+            const int row = DIM == 3 ? wrapi(a0 + a, g.na) : 0;
+            const int col = wrapi(b0 + b, g.nb);
+            gbv = __ldg(gb + (long long)x * g.plane + (long long)row * g.pb + col);
+        }
+        v.mo = P.o_on ? mobility(oc, hh, gbv, Phys::bmo, Phys::boo, P.gbm1_o) : 0.;
+        v.mc = mobility(cc, hh, gbv, Phys::bmc, Phys::boc, P.gbm1_cr);
+        smuO[c1] = v.muO; smuCr[c1] = v.muCr; smo[c1] = v.mo; smc[c1] = v.mc;
+        return v;
+    }
+
+    __device__ static void run(const StepParams P, const double* __restrict__ o, const double* __restrict__ cr,
+                               const double* __restrict__ p, const double* __restrict__ gb,
+                               const double* __restrict__ s2, double* __restrict__ on,
+                               double* __restrict__ crn, double* __restrict__ pn,
+                               StepPartial* __restrict__ partials, Status* st) {
+        extern __shared__ __align__(16) double smem[];
+        double* so = smem;                 // 3 slots x S2
+        double* scr = so + 3 * T::S2;      // 3 slots x S2
+        double* sp = scr + 3 * T::S2;      // 3 slots x S1
+        double* smuO = sp + 3 * T::S1;     // 2 slots x S1
+        double* smuCr = smuO + 2 * T::S1;
+        double* smo = smuCr + 2 * T::S1;
+        double* smc = smo + 2 * T::S1;
+        DD* sdd = reinterpret_cast<DD*>(smc + 2 * T::S1);
+        long long* scnt = reinterpret_cast<long long*>(sdd + 32 * 5);
+
+        const Grid& g = P.g;
+        const int ta = DIM == 3 ? threadIdx.y : 0, tb = threadIdx.x;
+        const int a0 = DIM == 3 ? blockIdx.y * TA : 0, b0 = blockIdx.x * TB;
+        const int i0 = blockIdx.z * P.xchunk;
+        const int i1 = min(g.nx, i0 + P.xchunk);
+        const int row = a0 + ta, col = b0 + tb;
+        const bool active = (DIM == 3 ? row < g.na : true) && col < g.nb;
+        const int blin = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+
+        DD acc[5] = {{0., 0.}, {0., 0.}, {0., 0.}, {0., 0.}, {0., 0.}};  // ckO ckCr clipO clipCr bcO
+        long long clipped = 0;
+        unsigned long long errkey = ERR_NONE;
+
+        if (st->failed) return;  // a previous step of this batch was rejected
+
+        auto slot3 = [](int w) { return ((w % 3) + 3) % 3; };
+        auto oslot = [&](int w) { return so + slot3(w) * T::S2; };
+        auto cslot = [&](int w) { return scr + slot3(w) * T::S2; };
+        auto pslot = [&](int x) { return sp + slot3(x) * T::S1; };
+
+        // Computes the lead plane x (real plane) over the tile + radius-1 halo.
+        auto lead = [&](int x) -> CenterVals {
+            const double *som = oslot(x - 1), *so0 = oslot(x), *sop = oslot(x + 1);
+            const double *scm = cslot(x - 1), *sc0 = cslot(x), *scp = cslot(x + 1);
+            const double* spx = pslot(x);
+            double* mO = smuO + (x & 1) * T::S1;
+            double* mC = smuCr + (x & 1) * T::S1;
+            double* mo_ = smo + (x & 1) * T::S1;
+            double* mc_ = smc + (x & 1) * T::S1;
+            CenterVals own = lead_point(P, gb, som, so0, sop, scm, sc0, scp, spx, mO, mC, mo_, mc_, x, ta, tb, a0, b0);
+            // halo ring points, distributed over the first threads
+            constexpr int NH = T::S1 - T::NT;
+            const int tid = threadIdx.x + TB * threadIdx.y;
+            for (int hq = tid; hq < NH; hq += T::NT) {
+                int a, b;
+                // ring enumeration: columns -1 and TB over all halo rows, then rows -1 and TA
+                if (hq < 2 * T::RA1) {
+                    a = hq / 2 - T::HA1;
+                    b = (hq & 1) ? TB : -1;
+                } else {
+                    const int r = hq - 2 * T::RA1;
+                    a = (r / TB) ? TA : -1;
+                    b = r % TB;
+                }
+                lead_point(P, gb, som, so0, sop, scm, sc0, scp, spx, mO, mC, mo_, mc_, x, a, b, a0, b0);
+            }
+            return own;
+        };
+
+        CenterVals C, L;
+        double pP, FxO, FxCr;
+        // ---- prologue: centre values of the first update plane and its left x-face flux
+        if (i0 == 0) {
+            load_oc(P, o, cr, -1, oslot(-1), cslot(-1), a0, b0);
+            load_oc(P, o, cr, 0, oslot(0), cslot(0), a0, b0);
+            load_oc(P, o, cr, 1, oslot(1), cslot(1), a0, b0);
+            load_p(P, p, 0, pslot(0), a0, b0);
+            __syncthreads();
+            C = lead(0);
+            __syncthreads();
+            // ghost plane -1: copies of plane 0 (3S:187, 3S:613-615, 3S:616-619)
+            const double muOg = (P.bc == 1 && P.o_on) ? 2. * P.mu_res - C.muO : C.muO;
+            FxO = -.5 * (C.mo + C.mo) * (C.muO - muOg) / P.dx;
+            FxCr = -.5 * (C.mc + C.mc) * (C.muCr - C.muCr) / P.dx;
+            pP = C.p;
+        } else {
+            load_oc(P, o, cr, i0 - 2, oslot(i0 - 2), cslot(i0 - 2), a0, b0);
+            load_oc(P, o, cr, i0 - 1, oslot(i0 - 1), cslot(i0 - 1), a0, b0);
+            load_oc(P, o, cr, i0, oslot(i0), cslot(i0), a0, b0);
+            load_p(P, p, i0 - 1, pslot(i0 - 1), a0, b0);
+            __syncthreads();
+            const CenterVals Pv = lead(i0 - 1);
+            __syncthreads();  // window i0-2 (read by lead(i0-1)) shares a ring slot with i0+1
+            load_oc(P, o, cr, i0 + 1, oslot(i0 + 1), cslot(i0 + 1), a0, b0);
+            load_p(P, p, i0, pslot(i0), a0, b0);
+            __syncthreads();
+            C = lead(i0);
+            __syncthreads();
+            FxO = -.5 * (Pv.mo + C.mo) * (C.muO - Pv.muO) / P.dx;
+            FxCr = -.5 * (Pv.mc + C.mc) * (C.muCr - Pv.muCr) / P.dx;
+            pP = Pv.p;
+        }
+
+        for (int u = i0; u < i1; ++u) {
+            const int x = u + 1;
+            if (x <= g.nx - 1) {
+                load_oc(P, o, cr, x + 1, oslot(x + 1), cslot(x + 1), a0, b0);
+                load_p(P, p, x, pslot(x), a0, b0);
+                __syncthreads();
+                L = lead(x);
+                __syncthreads();
+            } else {
+                L = C;  // ghost plane nx: Neumann copy of plane nx-1 (mu and M copied too)
+            }
+            if (active) {
+                const double* mO = smuO + (u & 1) * T::S1;
+                const double* mC = smuCr + (u & 1) * T::S1;
+                const double* mo_ = smo + (u & 1) * T::S1;
+                const double* mc_ = smc + (u & 1) * T::S1;
+                const double* spu = pslot(u);
+                const int c1 = T::i1(ta, tb);
+                const int bp = T::i1(ta, tb + 1), bm = T::i1(ta, tb - 1);
+                const int ap = T::i1(ta + 1, tb), am = T::i1(ta - 1, tb);
+                const long long gidx = (long long)u * g.plane + (long long)row * g.pb + col;
+                const long long cell = ((long long)u * g.na + row) * g.nb + col;  // reference loop order
+
+                // x faces: the right face of u is the left face of u+1 (same expression)
+                const double rightO = -.5 * (C.mo + L.mo) * (L.muO - C.muO) / P.dx;
+                const double rightCr = -.5 * (C.mc + L.mc) * (L.muCr - C.muCr) / P.dx;
+                double leftO = FxO;
+                if (u == 0 && P.bc == 1) {
+                    // left_flux (3S:621-628): surface-mobility face closure for bc=mu
+                    double lf = 0.;
+                    if (P.o_on) {
+                        const double gb0 = P.grains ? __ldg(gb + gidx) : 0.;
+                        const double mf = mobility(P.surface_c_ref, h(C.p), gb0, Phys::bmo, Phys::boo, P.gbm1_o);
+                        lf = 2. * mf * (P.mu_res - C.muO) / P.dx;
+                    }
+                    leftO = lf;
+                    acc[4] = dd_add(acc[4], P.dt * lf / P.dx);
+                }
+                if (u == 0 && P.inlet) acc[4] = dd_add(acc[4], P.layer_o - __ldg(o + gidx));
+
+                double divO = 0., divCr;
+                {
+                    const double mc0 = mc_[c1], mu0 = mC[c1];
+                    const double front = -.5 * (mc0 + mc_[bp]) * (mC[bp] - mu0) / P.db;
+                    const double back = -.5 * (mc_[bm] + mc0) * (mu0 - mC[bm]) / P.db;
+                    if (DIM == 3) {
+                        const double top = -.5 * (mc0 + mc_[ap]) * (mC[ap] - mu0) / P.da;
+                        const double bottom = -.5 * (mc_[am] + mc0) * (mu0 - mC[am]) / P.da;
+                        divCr = (FxCr - rightCr) / P.dx + (bottom - top) / P.da + (back - front) / P.db;
+                    } else {
+                        divCr = (FxCr - rightCr) / P.dx + (back - front) / P.db;
+                    }
+                }
+                if (P.o_on) {
+                    const double m0 = mo_[c1], mu0 = mO[c1];
+                    const double front = -.5 * (m0 + mo_[bp]) * (mO[bp] - mu0) / P.db;
+                    const double back = -.5 * (mo_[bm] + m0) * (mu0 - mO[bm]) / P.db;
+                    if (DIM == 3) {
+                        const double top = -.5 * (m0 + mo_[ap]) * (mO[ap] - mu0) / P.da;
+                        const double bottom = -.5 * (mo_[am] + m0) * (mu0 - mO[am]) / P.da;
+                        divO = (leftO - rightO) / P.dx + (bottom - top) / P.da + (back - front) / P.db;
+                    } else {
+                        divO = (leftO - rightO) / P.dx + (back - front) / P.db;
+                    }
+                }
+                const double oo = C.o, cc = C.cr, pp = C.p;
+                double onv = P.o_on ? oo + P.dt * divO : oo;
+                double crv = cc + P.dt * divCr;
+                double lapP;
+                if (DIM == 3)
+                    lapP = (L.p - 2. * pp + pP) / P.dxdx + (spu[ap] - 2. * pp + spu[am]) / P.dada
+                         + (spu[bp] - 2. * pp + spu[bm]) / P.dbdb;
+                else
+                    lapP = (L.p - 2. * pp + pP) / P.dxdx + (spu[bp] - 2. * pp + spu[bm]) / P.dbdb;
+                const double hpv = 30. * pp * pp * (pp - 1.) * (pp - 1.);
+                double fp = Phys::W * (4. * pp * pp * pp - 6. * pp * pp + 2. * pp)
+                          + hpv * (foxide(oo, cc) - fmetal(oo, cc)) - 2. * Phys::kp * lapP;
+                if (P.phi_eta) fp += grain_dphi(__ldg(s2 + gidx), pp, P.eta_W, P.eta_A);
+                double pnv = pp - P.dtL * fp;
+                if (P.ck == 0) {
+                    const double dO = -Phys::ckO * ((Phys::oxideO - onv) * h(pnv) - (Phys::oxideO - oo) * h(pp)) / P.dt;
+                    const double dCr = -Phys::ckCr * ((Phys::oxideCr - crv) * h(pnv) - (Phys::oxideCr - cc) * h(pp)) / P.dt;
+                    onv += dO; crv += dCr;
+                    acc[0] = dd_add(acc[0], dO);
+                    acc[1] = dd_add(acc[1], dCr);
+                }
+                if (!isfinite(onv) || !isfinite(crv) || !isfinite(pnv)) {
+                    errkey = min(errkey, (unsigned long long)cell * 4ull);
+                } else if (P.bounds == 1) {
+                    const double oc = sclamp(onv, 0., 1.), ccr = sclamp(crv, 0., 1.);
+                    acc[2] = dd_add(acc[2], oc - onv);
+                    acc[3] = dd_add(acc[3], ccr - crv);
+                    if (oc != onv || ccr != crv) ++clipped;
+                    onv = oc; crv = ccr;
+                    if (pnv > .99999) pnv = 1.;
+                    if (pnv < 1.e-5) pnv = 0.;
+                } else if (onv < -1.e-12 || crv < -1.e-12 || onv + crv > 1. + 1.e-12 || pnv < -1.e-12 ||
+                           pnv > 1. + 1.e-12) {
+                    errkey = min(errkey, (unsigned long long)cell * 4ull + 1ull);
+                }
+                on[gidx] = onv; crn[gidx] = crv; pn[gidx] = pnv;
+                FxO = rightO; FxCr = rightCr;
+            }
+            pP = C.p;
+            C = L;
+        }
+        if (errkey != ERR_NONE) atomicMin(&st->err_key, errkey);
+        block_reduce_dd<5>(acc, clipped, sdd, scnt);
+        if (threadIdx.x == 0 && threadIdx.y == 0) {
+            StepPartial& out = partials[blin];
+            for (int q = 0; q < 5; ++q) { out.s[q][0] = acc[q].hi; out.s[q][1] = acc[q].lo; }
+            out.clipped = clipped;
+        }
+    }
+};
+
+template <int DIM, int TA, int TB>
+__global__ void __launch_bounds__(TA * TB)
+k_step_main(const StepParams P, const double* __restrict__ o, const double* __restrict__ cr,
+            const double* __restrict__ p, const double* __restrict__ gb, const double* __restrict__ s2,
+            double* __restrict__ on, double* __restrict__ crn, double* __restrict__ pn,
+            StepPartial* __restrict__ partials, Status* st) {
+    StepKernel<DIM, TA, TB>::run(P, o, cr, p, gb, s2, on, crn, pn, partials, st);
+}
+
+constexpr int TA3 = 8, TB3 = 32;    // 3D tile: 8 rows x 32 columns, 256 threads
+constexpr int TA2 = 1, TB2 = 128;   // 2D tile: 128 columns
+
+template <int DIM, int TA, int TB>
+dim3 step_grid(const StepParams& P) {
+    const Grid& g = P.g;
+    return dim3((g.nb + TB - 1) / TB, DIM == 3 ? (g.na + TA - 1) / TA : 1, (g.nx + P.xchunk - 1) / P.xchunk);
+}
+
+// ----------------------------------------------------------------- eta kernels
+// S = sum eta_g^2, pairs = sum_{a<b} eta_a^2 eta_b^2 accumulated as in
+// rebuild_eta_mask (3S:497-505), gb = scale * min(1, 16 pairs).
+__global__ void k_eta_mask(const StepParams P, int neta, const double* __restrict__ eta,
+                           double* __restrict__ gb, double* __restrict__ s2, double* __restrict__ pairs_out,
+                           Status* st) {
+    const Grid& g = P.g;
+    const long long n = (long long)g.nx * g.na * g.nb;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+        const int col = (int)(c % g.nb);
+        const long long r = c / g.nb;
+        const int row = (int)(r % g.na);
+        const int x = (int)(r / g.na);
+        const long long idx = (long long)x * g.plane + (long long)row * g.pb + col;
+        double S = 0., pairs = 0.;
+        for (int q = 0; q < neta; ++q) {
+            const double e = __ldg(eta + (long long)q * g.nstore + idx);
+            const double sq = e * e;
+            pairs += S * sq;
+            S += sq;
+        }
+        s2[idx] = S;
+        if (pairs_out) pairs_out[idx] = pairs;
+        gb[idx] = P.eta_scale * smin(1., 16. * pairs);
+    }
+}
+
+// eta_trial (3S:514-526): v = eta - (dt*L_eta)*(deta - K*lap(eta)); must lie in
+// [-1e-12, 1+1e-12]. Writes the trial and the mask of the trial values (the
+// next step's gb and eta_s2, identical to rebuild_eta_mask on them).
+template <int DIM>
+__global__ void k_eta_update(const StepParams P, int neta, const double* __restrict__ eta,
+                             const double* __restrict__ s2, const double* __restrict__ p,
+                             double* __restrict__ eta_next, double* __restrict__ gb_next,
+                             double* __restrict__ s2_next, Status* st) {
+    if (st->failed) return;
+    const Grid& g = P.g;
+    const int col = blockIdx.x * blockDim.x + threadIdx.x;
+    const int row = DIM == 3 ? blockIdx.y * blockDim.y + threadIdx.y : 0;
+    const int x = blockIdx.z;
+    if (col >= g.nb || row >= g.na) return;
+    const long long idx = (long long)x * g.plane + (long long)row * g.pb + col;
+    const long long cell = ((long long)x * g.na + row) * g.nb + col;
+    const long long ixm = x > 0 ? idx - g.plane : idx, ixp = x < g.nx - 1 ? idx + g.plane : idx;
+    const long long rbase = (long long)x * g.plane;
+    const long long ibm = rbase + (long long)row * g.pb + (col == 0 ? g.nb - 1 : col - 1);
+    const long long ibp = rbase + (long long)row * g.pb + (col == g.nb - 1 ? 0 : col + 1);
+    long long iam = idx, iap = idx;
+    if (DIM == 3) {
+        iam = rbase + (long long)(row == 0 ? g.na - 1 : row - 1) * g.pb + col;
+        iap = rbase + (long long)(row == g.na - 1 ? 0 : row + 1) * g.pb + col;
+    }
+    const double S = __ldg(s2 + idx), phi = __ldg(p + idx);
+    unsigned long long errkey = ERR_NONE;
+    double Sn = 0., pairs = 0.;
+    for (int q = 0; q < neta; ++q) {
+        const double* e = eta + (long long)q * g.nstore;
+        const double ec = __ldg(e + idx);
+        double lap;
+        if (DIM == 3)
+            lap = (__ldg(e + ixp) - 2. * ec + __ldg(e + ixm)) / P.dxdx
+                + (__ldg(e + iap) - 2. * ec + __ldg(e + iam)) / P.dada
+                + (__ldg(e + ibp) - 2. * ec + __ldg(e + ibm)) / P.dbdb;
+        else
+            lap = (__ldg(e + ixp) - 2. * ec + __ldg(e + ixm)) / P.dxdx
+                + (__ldg(e + ibp) - 2. * ec + __ldg(e + ibm)) / P.dbdb;
+        const double force = grain_deta(ec, S, phi, P.eta_W, P.eta_A) - P.eta_K * lap;
+        const double v = ec - P.dt_etaL * force;
+        if (!isfinite(v) || v < -1.e-12 || v > 1. + 1.e-12)
+            errkey = min(errkey, ERR_ETA_BASE + (unsigned long long)q * (unsigned long long)g.ncells + (unsigned long long)cell);
+        eta_next[(long long)q * g.nstore + idx] = v;
+        const double sq = v * v;
+        pairs += Sn * sq;
+        Sn += sq;
+    }
+    s2_next[idx] = Sn;
+    gb_next[idx] = P.eta_scale * smin(1., 16. * pairs);
+    if (errkey != ERR_NONE) atomicMin(&st->err_key, errkey);
+}
+
+// Step commit: partial sums in block order (deterministic), then the budget is
+// advanced only when no trial failed (fields swap only on acceptance, 3S:821).
+__global__ void k_step_finalize(const StepPartial* __restrict__ partials, int nblocks, DevBudget* budget,
+                                Status* st, int accept_mode) {
+    __shared__ DD sdd[32 * 5];
+    __shared__ long long scnt[32];
+    if (st->failed) return;
+    DD acc[5] = {{0., 0.}, {0., 0.}, {0., 0.}, {0., 0.}, {0., 0.}};
+    long long clipped = 0;
+    for (int b = threadIdx.x; b < nblocks; b += blockDim.x) {
+        for (int q = 0; q < 5; ++q) acc[q] = dd_add(acc[q], DD{partials[b].s[q][0], partials[b].s[q][1]});
+        clipped += partials[b].clipped;
+    }
+    block_reduce_dd<5>(acc, clipped, sdd, scnt);
+    if (threadIdx.x == 0) {
+        if (st->err_key != ERR_NONE) {
+            st->failed = 1;
+            st->failed_step = st->steps_done;
+            return;
+        }
+        if (accept_mode == 0) {
+            // slots: ckO ckCr clipO clipCr bcO -> budget indices 2 3 4 5 6
+            for (int q = 0; q < 5; ++q) {
+                DD b{budget->v[2 + q][0], budget->v[2 + q][1]};
+                b = dd_add(b, acc[q]);
+                budget->v[2 + q][0] = b.hi;
+                budget->v[2 + q][1] = b.lo;
+            }
+            budget->clipped += clipped;
+            st->steps_done += 1;
+        }
+    }
+}
+
+// refresh() for output: mu at interior cells, M at interior cells.
+template <int DIM>
+__global__ void k_refresh(const StepParams P, const double* __restrict__ o, const double* __restrict__ cr,
+                          const double* __restrict__ p, const double* __restrict__ gb, double* __restrict__ muO,
+                          double* __restrict__ muCr, double* __restrict__ mo, double* __restrict__ mc) {
+    const Grid& g = P.g;
+    const int col = blockIdx.x * blockDim.x + threadIdx.x;
+    const int row = DIM == 3 ? blockIdx.y * blockDim.y + threadIdx.y : 0;
+    const int x = blockIdx.z;
+    if (col >= g.nb || row >= g.na) return;
+    const long long idx = (long long)x * g.plane + (long long)row * g.pb + col;
+    const long long ixm = x > 0 ? idx - g.plane : idx, ixp = x < g.nx - 1 ? idx + g.plane : idx;
+    const long long rbase = (long long)x * g.plane;
+    const long long ibm = rbase + (long long)row * g.pb + (col == 0 ? g.nb - 1 : col - 1);
+    const long long ibp = rbase + (long long)row * g.pb + (col == g.nb - 1 ? 0 : col + 1);
+    long long iam = idx, iap = idx;
+    if (DIM == 3) {
+        iam = rbase + (long long)(row == 0 ? g.na - 1 : row - 1) * g.pb + col;
+        iap = rbase + (long long)(row == g.na - 1 ? 0 : row + 1) * g.pb + col;
+    }
+    auto lapf = [&](const double* a) {
+        const double c = a[idx];
+        if (DIM == 3)
+            return (a[ixp] - 2. * c + a[ixm]) / P.dxdx + (a[iap] - 2. * c + a[iam]) / P.dada
+                 + (a[ibp] - 2. * c + a[ibm]) / P.dbdb;
+        return (a[ixp] - 2. * c + a[ixm]) / P.dxdx + (a[ibp] - 2. * c + a[ibm]) / P.dbdb;
+    };
+    const double oc = o[idx], cc = cr[idx];
+    const double hh = h(p[idx]);
+    muO[idx] = mu_o_local(oc, cc, hh) - 2. * Phys::ko * lapf(o);
+    muCr[idx] = mu_cr_local(oc, cc, hh) - 2. * Phys::kc * lapf(cr);
+    const double gbv = P.grains ? gb[idx] : 0.;
+    mo[idx] = P.o_on ? mobility(oc, hh, gbv, Phys::bmo, Phys::boo, P.gbm1_o) : 0.;
+    mc[idx] = mobility(cc, hh, gbv, Phys::bmc, Phys::boc, P.gbm1_cr);
+}
+
+}  // namespace
+
+// ----------------------------------------------------------------- launchers
+int step_main_blocks(const StepParams& P) {
+    const dim3 grid = P.g.dim == 3 ? step_grid<3, TA3, TB3>(P) : step_grid<2, TA2, TB2>(P);
+    return (int)(grid.x * grid.y * grid.z);
+}
+
+void launch_step_main(const StepParams& P, const double* o, const double* cr, const double* p, const double* gb,
+                      const double* s2, double* on, double* crn, double* pn, StepPartial* partials, Status* st,
+                      cudaStream_t stream, int* nblocks_out) {
+    if (P.g.dim == 3) {
+        using T = Tile<3, TA3, TB3>;
+        static bool attr = false;
+        if (!attr) {
+            cudaFuncSetAttribute(k_step_main<3, TA3, TB3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM_BYTES);
+            attr = true;
+        }
+        const dim3 grid = step_grid<3, TA3, TB3>(P);
+        k_step_main<3, TA3, TB3><<<grid, dim3(TB3, TA3), T::SMEM_BYTES, stream>>>(P, o, cr, p, gb, s2, on, crn, pn, partials, st);
+        if (nblocks_out) *nblocks_out = (int)(grid.x * grid.y * grid.z);
+    } else {
+        using T = Tile<2, TA2, TB2>;
+        const dim3 grid = step_grid<2, TA2, TB2>(P);
+        k_step_main<2, TA2, TB2><<<grid, dim3(TB2, TA2), T::SMEM_BYTES, stream>>>(P, o, cr, p, gb, s2, on, crn, pn, partials, st);
+        if (nblocks_out) *nblocks_out = (int)(grid.x * grid.y * grid.z);
+    }
+}
+
+void launch_eta_mask(const StepParams& P, int neta, const double* eta, double* gb, double* s2, double* pairs,
+                     Status* st, cudaStream_t stream) {
+    const long long n = P.g.ncells;
+    const int threads = 256;
+    const long long want = (n + threads - 1) / threads;
+    const int blocks = (int)(want < 148 * 32 ? want : 148 * 32);
+    k_eta_mask<<<blocks, threads, 0, stream>>>(P, neta, eta, gb, s2, pairs, st);
+}
+
+void launch_eta_update(const StepParams& P, int neta, const double* eta, const double* s2, const double* p,
+                       double* eta_next, double* gb_next, double* s2_next, Status* st, cudaStream_t stream) {
+    const Grid& g = P.g;
+    if (g.dim == 3) {
+        const dim3 block(32, 8);
+        const dim3 grid((g.nb + 31) / 32, (g.na + 7) / 8, g.nx);
+        k_eta_update<3><<<grid, block, 0, stream>>>(P, neta, eta, s2, p, eta_next, gb_next, s2_next, st);
+    } else {
+        const dim3 block(128, 1);
+        const dim3 grid((g.nb + 127) / 128, 1, g.nx);
+        k_eta_update<2><<<grid, block, 0, stream>>>(P, neta, eta, s2, p, eta_next, gb_next, s2_next, st);
+    }
+}
+
+void launch_step_finalize(const StepPartial* partials, int nblocks, DevBudget* budget, Status* st, int accept_mode,
+                          cudaStream_t stream) {
+    k_step_finalize<<<1, 256, 0, stream>>>(partials, nblocks, budget, st, accept_mode);
+}
+
+void launch_refresh(const StepParams& P, const double* o, const double* cr, const double* p, const double* gb,
+                    double* muO, double* muCr, double* mo, double* mc, cudaStream_t stream) {
+    const Grid& g = P.g;
+    if (g.dim == 3) {
+        const dim3 block(32, 8);
+        const dim3 grid((g.nb + 31) / 32, (g.na + 7) / 8, g.nx);
+        k_refresh<3><<<grid, block, 0, stream>>>(P, o, cr, p, gb, muO, muCr, mo, mc);
+    } else {
+        const dim3 block(128, 1);
+        const dim3 grid((g.nb + 127) / 128, 1, g.nx);
+        k_refresh<2><<<grid, block, 0, stream>>>(P, o, cr, p, gb, muO, muCr, mo, mc);
+    }
+}
+
+}  // namespace nicr

@@ -1,0 +1,307 @@
+"""Python access to the B200 Ni-Cr oxidation solver through its C-ABI.
+
+``Solver`` wraps one ``nicr_handle`` (include/nicr.h): a domain resident on the
+GPU. The methods mirror the reference's ``Model`` members (step, refresh,
+nucleate, stamp, log/grain_log values) and exchange fields as numpy arrays in
+the reference's interior order (X slowest). The compute runs only in the CUDA
+library ``lib/libnicr.so``; importing this module raises if it is missing.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+import numpy as np
+
+from ._abi import (BC, BOUNDS, CK, FIELD, NUCLEATION, NicrConfig, config_to_flags, default_config,
+                   make_config)
+
+PKG = Path(__file__).resolve().parent.parent
+LIB_PATH = PKG / "lib" / "libnicr.so"
+
+_lib = None
+
+
+class NicrError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"[{code}] {message}")
+        self.code = code
+        self.message = message
+
+
+class NicrInfo(ctypes.Structure):
+    _fields_ = [("dim", ctypes.c_int), ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+                ("n_seeds", ctypes.c_int), ("n_eta", ctypes.c_int), ("center_seed_cells", ctypes.c_int),
+                ("grain_map_retained", ctypes.c_int), ("n_cells", ctypes.c_longlong),
+                ("steps_done", ctypes.c_longlong), ("device_bytes", ctypes.c_size_t)]
+
+
+class NicrBudget(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_double * 2) for n in ("nucO", "nucCr", "ckO", "ckCr", "clipO", "clipCr", "bcO", "bcCr")] + \
+               [("nuclei", ctypes.c_longlong), ("clipped", ctypes.c_longlong),
+                ("initialO", ctypes.c_double * 2), ("initialCr", ctypes.c_double * 2)]
+
+
+class NicrDiagnostics(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_double * 2) for n in ("sum_O", "sum_Cr", "sum_phi", "sum_h")] + \
+               [(n, ctypes.c_double) for n in ("min_O", "max_O", "min_Cr", "max_Cr", "min_Ni", "min_phi", "max_phi")]
+
+
+class NicrGrainStats(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_double) for n in ("min_eta", "max_eta", "min_s2", "max_s2")] + \
+               [(n, ctypes.c_double * 2) for n in ("sum_s2", "mask", "energy")] + \
+               [("gb_max", ctypes.c_double), ("alive", ctypes.c_longlong), ("unassigned", ctypes.c_longlong)]
+
+
+def library_path() -> Path:
+    return LIB_PATH
+
+
+def lib():
+    """Loads lib/libnicr.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise ImportError(f"CUDA library {LIB_PATH} is missing: run `make -C {PKG}` (or __graft_entry__.build())")
+    L = ctypes.CDLL(str(LIB_PATH))
+    H = ctypes.c_void_p
+    ip = ctypes.POINTER(ctypes.c_int)
+    dp = ctypes.POINTER(ctypes.c_double)
+    L.nicr_config_default.argtypes = [ctypes.POINTER(NicrConfig), ctypes.c_int]
+    L.nicr_config_default.restype = None
+    L.nicr_config_parse.argtypes = [ctypes.POINTER(NicrConfig), ctypes.c_int, ctypes.c_int,
+                                    ctypes.POINTER(ctypes.c_char_p), ctypes.c_char_p, ctypes.c_size_t, ip,
+                                    ctypes.c_char_p, ctypes.c_size_t]
+    L.nicr_create.argtypes = [ctypes.POINTER(NicrConfig), ctypes.POINTER(H)]
+    L.nicr_destroy.argtypes = [H]
+    L.nicr_destroy.restype = None
+    L.nicr_last_error.argtypes = [H]
+    L.nicr_last_error.restype = ctypes.c_char_p
+    L.nicr_get_info.argtypes = [H, ctypes.POINTER(NicrInfo)]
+    L.nicr_get_seeds.argtypes = [H, dp, ctypes.POINTER(ctypes.c_longlong)]
+    L.nicr_set_field.argtypes = [H, ctypes.c_int, ctypes.c_int, dp]
+    L.nicr_get_field.argtypes = [H, ctypes.c_int, ctypes.c_int, dp]
+    for f in ("nicr_refresh", "nicr_invalidate_eta_cache", "nicr_reset_inventory"):
+        getattr(L, f).argtypes = [H]
+    L.nicr_step.argtypes = [H, ctypes.c_int, ip]
+    L.nicr_run.argtypes = [H, ctypes.c_int, ip]
+    L.nicr_nucleate.argtypes = [H, ip]
+    L.nicr_stamp.argtypes = [H, ctypes.c_int, ctypes.c_int, ctypes.c_int, ip]
+    L.nicr_get_budget.argtypes = [H, ctypes.POINTER(NicrBudget)]
+    L.nicr_get_diagnostics.argtypes = [H, ctypes.POINTER(NicrDiagnostics)]
+    L.nicr_get_grain_stats.argtypes = [H, ctypes.POINTER(NicrGrainStats), ctypes.POINTER(ctypes.c_longlong), dp]
+    L.nicr_write_vtk.argtypes = [H, ctypes.c_char_p]
+    L.nicr_write_vti.argtypes = [H, ctypes.c_char_p]
+    L.nicr_write_metadata.argtypes = [H, ctypes.c_char_p]
+    L.nicr_format_log_row.argtypes = [H, ctypes.c_int, ctypes.c_char_p, ctypes.c_size_t]
+    L.nicr_format_grain_rows.argtypes = [H, ctypes.c_int, ctypes.c_char_p, ctypes.c_size_t, ctypes.c_char_p,
+                                         ctypes.c_size_t]
+    L.nicr_main.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_char_p)]
+    L.nicr_stream.argtypes = [H]
+    L.nicr_stream.restype = ctypes.c_void_p
+    _lib = L
+    return L
+
+
+def c_default_config(dim: int) -> NicrConfig:
+    c = NicrConfig()
+    lib().nicr_config_default(ctypes.byref(c), dim)
+    return c
+
+
+def parse_args(dim: int, argv: list[str]):
+    """nicr_config_parse: returns (config, out_dir, self_test) or raises NicrError."""
+    c = NicrConfig()
+    arr = (ctypes.c_char_p * max(1, len(argv)))(*[a.encode() for a in argv])
+    out = ctypes.create_string_buffer(4096)
+    err = ctypes.create_string_buffer(8192)
+    st = ctypes.c_int(0)
+    rc = lib().nicr_config_parse(ctypes.byref(c), dim, len(argv), arr, out, 4096, ctypes.byref(st), err, 8192)
+    if rc != 0:
+        raise NicrError(rc, err.value.decode())
+    return c, out.value.decode(), bool(st.value)
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+class Solver:
+    """One simulation domain on the GPU (the reference's Model)."""
+
+    def __init__(self, cfg: NicrConfig | None = None, dim: int = 3, **kw):
+        if cfg is None:
+            cfg = make_config(dim, **kw)
+        self.cfg = cfg
+        self.h = ctypes.c_void_p()
+        rc = lib().nicr_create(ctypes.byref(cfg), ctypes.byref(self.h))
+        if rc != 0:
+            raise NicrError(rc, lib().nicr_last_error(None).decode())
+        self.info_ = self.info()
+        self.shape = (cfg.nx, cfg.ny, cfg.nz) if cfg.dim == 3 else (cfg.nx, cfg.ny)
+        self.n = int(np.prod(self.shape))
+
+    def close(self):
+        if getattr(self, "h", None) and self.h.value:
+            lib().nicr_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # -------------------------------------------------------------- helpers
+    def _check(self, rc: int):
+        if rc != 0:
+            raise NicrError(rc, self.last_error)
+        return rc
+
+    @property
+    def last_error(self) -> str:
+        return lib().nicr_last_error(self.h).decode()
+
+    def info(self) -> NicrInfo:
+        i = NicrInfo()
+        self._check(lib().nicr_get_info(self.h, ctypes.byref(i)))
+        return i
+
+    @property
+    def n_eta(self) -> int:
+        return self.info().n_eta
+
+    def seeds(self):
+        i = self.info()
+        xyz = np.zeros(i.n_seeds * self.cfg.dim)
+        vol = np.zeros(i.n_seeds, dtype=np.int64)
+        self._check(lib().nicr_get_seeds(self.h, _dp(xyz), vol.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong))))
+        return xyz.reshape(i.n_seeds, self.cfg.dim), vol
+
+    def get(self, name: str, index: int = 0) -> np.ndarray:
+        if name.startswith("eta") and name[3:].isdigit():
+            index, name = int(name[3:]) - 1, "eta"
+        out = np.empty(self.n)
+        self._check(lib().nicr_get_field(self.h, FIELD[name], index, _dp(out)))
+        return out.reshape(self.shape)
+
+    def set(self, name: str, arr, index: int = 0):
+        if name.startswith("eta") and name[3:].isdigit():
+            index, name = int(name[3:]) - 1, "eta"
+        a = np.ascontiguousarray(arr, dtype=np.float64).ravel()
+        if a.size != self.n:
+            raise ValueError(f"field has {a.size} values, grid has {self.n}")
+        self._check(lib().nicr_set_field(self.h, FIELD[name], index, _dp(a)))
+
+    def set_fields(self, o, cr, p, eta=None):
+        self.set("o", o)
+        self.set("cr", cr)
+        self.set("p", p)
+        if eta is not None:
+            for g, e in enumerate(eta):
+                self.set("eta", e, g)
+
+    def refresh(self):
+        self._check(lib().nicr_refresh(self.h))
+
+    def invalidate_eta_cache(self):
+        self._check(lib().nicr_invalidate_eta_cache(self.h))
+
+    def reset_inventory(self):
+        self._check(lib().nicr_reset_inventory(self.h))
+
+    def step(self, n: int = 1, check: bool = True):
+        done = ctypes.c_int(0)
+        rc = lib().nicr_step(self.h, n, ctypes.byref(done))
+        if check:
+            self._check(rc)
+        return rc, done.value
+
+    def run(self, n: int, check: bool = True):
+        done = ctypes.c_int(0)
+        rc = lib().nicr_run(self.h, n, ctypes.byref(done))
+        if check:
+            self._check(rc)
+        return rc, done.value
+
+    def nucleate(self) -> int:
+        k = ctypes.c_int(0)
+        self._check(lib().nicr_nucleate(self.h, ctypes.byref(k)))
+        return k.value
+
+    def stamp(self, x: int, y: int, z: int = 0) -> int:
+        k = ctypes.c_int(0)
+        self._check(lib().nicr_stamp(self.h, x, y, z, ctypes.byref(k)))
+        return k.value
+
+    def budget(self) -> dict:
+        b = NicrBudget()
+        self._check(lib().nicr_get_budget(self.h, ctypes.byref(b)))
+        d = {n: (getattr(b, n)[0], getattr(b, n)[1]) for n in
+             ("nucO", "nucCr", "ckO", "ckCr", "clipO", "clipCr", "bcO", "bcCr", "initialO", "initialCr")}
+        d["nuclei"], d["clipped"] = int(b.nuclei), int(b.clipped)
+        return d
+
+    def diagnostics(self) -> dict:
+        d = NicrDiagnostics()
+        self._check(lib().nicr_get_diagnostics(self.h, ctypes.byref(d)))
+        out = {n: (getattr(d, n)[0], getattr(d, n)[1]) for n in ("sum_O", "sum_Cr", "sum_phi", "sum_h")}
+        for n in ("min_O", "max_O", "min_Cr", "max_Cr", "min_Ni", "min_phi", "max_phi"):
+            out[n] = getattr(d, n)
+        return out
+
+    def grain_stats(self):
+        ne = max(1, self.n_eta)
+        s = NicrGrainStats()
+        cells = np.zeros(ne, dtype=np.int64)
+        amount = np.zeros(2 * ne)
+        self._check(lib().nicr_get_grain_stats(self.h, ctypes.byref(s), cells.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong)), _dp(amount)))
+        out = {n: getattr(s, n) for n in ("min_eta", "max_eta", "min_s2", "max_s2", "gb_max")}
+        for n in ("sum_s2", "mask", "energy"):
+            out[n] = (getattr(s, n)[0], getattr(s, n)[1])
+        out["alive"], out["unassigned"] = int(s.alive), int(s.unassigned)
+        out["cells"] = cells[: self.n_eta]
+        out["amount"] = amount[: 2 * self.n_eta].reshape(-1, 2)
+        return out
+
+    def write_vtk(self, path):
+        self._check(lib().nicr_write_vtk(self.h, str(path).encode()))
+
+    def write_vti(self, path):
+        self._check(lib().nicr_write_vti(self.h, str(path).encode()))
+
+    def write_metadata(self, out_dir):
+        self._check(lib().nicr_write_metadata(self.h, str(out_dir).encode()))
+
+    def log_row(self, n: int) -> str:
+        buf = ctypes.create_string_buffer(8192)
+        self._check(lib().nicr_format_log_row(self.h, n, buf, 8192))
+        return buf.value.decode()
+
+    def grain_rows(self, n: int):
+        sz = 4096 + 256 * max(1, self.n_eta)
+        a, b = ctypes.create_string_buffer(sz), ctypes.create_string_buffer(sz)
+        self._check(lib().nicr_format_grain_rows(self.h, n, a, sz, b, sz))
+        return a.value.decode(), b.value.decode()
+
+    def stream(self) -> int:
+        return lib().nicr_stream(self.h) or 0
+
+
+def main(dim: int, argv: list[str]) -> int:
+    """Runs the solver program (the reference's run()) with argv."""
+    args = ["nicr%dd" % dim] + list(argv)
+    arr = (ctypes.c_char_p * len(args))(*[a.encode() for a in args])
+    return lib().nicr_main(dim, len(args), arr)
+
+
+__all__ = ["Solver", "NicrError", "NicrConfig", "make_config", "default_config", "c_default_config", "parse_args",
+           "config_to_flags", "main", "lib", "library_path", "BC", "CK", "BOUNDS", "NUCLEATION", "FIELD"]
