@@ -1,0 +1,358 @@
+#!/usr/bin/env python3
+"""Benchmark of the explicit Ni-Cr phase-field step on B200.
+
+Workload (one "step" = one explicit time step of every field of one domain):
+3D 256^3, evolving grains with 8 eta order parameters (Voronoi of 8 seeds from
+seed 2), Cr = 0.25 +- 0.01 uniform noise, O supplied at the x=0 face
+(bc=concentration), Ksp insertion on, legacy Ck, bounds=legacy, FP64 (the
+drop-in arithmetic, bit-identical to the reference). Inputs (~3 GB of fields)
+are far larger than L2, so no flush is needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl nicr|reference]
+
+One JSON line on stdout (rank 0). Under torchrun every rank advances its own
+independent domain (a parameter sweep shards by domain: weak scaling); times
+are the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+PKG = ROOT / "ni-cr_oxidation_phase-field_simulation_b200"
+sys.path.insert(0, str(PKG))
+
+METRIC = "Mcell-updates/s at 256^3 vs plain FP64 GPU path at ≤1e-4 L∞ err; % HBM peak"
+UNIT = "Mcell-updates/s"
+KERNELS = ["step_main", "eta_update", "step_finalize", "eta_mask", "ksp_scan", "refresh", "diagnostics"]
+
+
+def grain_diameter_for(n_grains: int, shape) -> float:
+    """Volume-equivalent diameter giving round(6V/(pi d^3)) = n_grains (3S:416-418)."""
+    v = float(np.prod(shape))
+    return (6.0 * v / (math.pi * n_grains)) ** (1.0 / 3.0)
+
+
+def workload_config(size: int, neta: int, device: int = 0, seed: int = 2):
+    from nicr import make_config
+    shape = (size, size, size)
+    return make_config(3, nx=size, ny=size, nz=size, grains=1, grain_evolution=1, random_seed=seed,
+                       grain_diameter_grid=grain_diameter_for(neta, shape), bc="concentration", ck="legacy",
+                       bounds="legacy", nucleation="ksp", device=device)
+
+
+def algorithmic_bytes(kernel: str, neta: int) -> int:
+    """Compulsory HBM bytes per cell of one launch (each field read/written once)."""
+    if kernel == "step_main":      # r: o cr p gb eta_s2   w: o cr p
+        return 8 * 8
+    if kernel == "eta_update":     # r: eta_1..N eta_s2 p  w: eta_1..N gb eta_s2
+        return (2 * neta + 4) * 8
+    if kernel == "eta_mask":       # r: eta_1..N  w: gb eta_s2
+        return (neta + 2) * 8
+    return 0
+
+
+def measured_peak_hbm():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic(kernel: str, size: int):
+    """DRAM bytes per launch from the committed ncu summary (scaled per cell)."""
+    p = ROOT / "profiles" / "traffic.json"
+    if not p.exists():
+        return None
+    d = json.loads(p.read_text())
+    e = d.get(kernel)
+    if not e:
+        return None
+    return float(e["dram_bytes_per_cell"]) * size ** 3
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.gpu), "-lms", "50"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ reference (CPU) timing
+def reference_exe(threads: bool):
+    exe = ROOT / "oracle" / "_ref" / ("ref3d_threads" if threads else "ref3d")
+    return exe if exe.exists() else None
+
+
+def time_reference(size: int, neta: int, steps: int, ranks: int, budget_s: float = 60.0, timeout: float = 900):
+    """Times the unmodified reference (built from its sources into oracle/_ref)
+    on the same workload: one warm-up step, then up to `steps` steps bounded by
+    budget_s seconds. Returns (Mcell-updates/s, steps timed, seconds)."""
+    from nicr import config_to_flags
+    exe = reference_exe(threads=ranks > 1)
+    if exe is None:
+        return None
+    cfg = workload_config(size, neta)
+    flags = config_to_flags(cfg)
+    base = [str(exe)] + ([str(ranks)] if ranks > 1 else []) + flags + ["--"]
+    with tempfile.TemporaryDirectory() as td:
+        t = subprocess.run(base + ["time_run", "1"], capture_output=True, text=True, timeout=timeout, cwd=td)
+        if t.returncode != 0:
+            raise RuntimeError(t.stderr)
+        one = float([ln for ln in t.stdout.splitlines() if ln.startswith("TIME_RUN")][-1].split()[2])
+        n = int(max(1, min(steps, budget_s / max(one, 1e-6))))
+        t = subprocess.run(base + ["time_run", "1", "time_run", str(n)], capture_output=True, text=True,
+                           timeout=timeout, cwd=td)
+        if t.returncode != 0:
+            raise RuntimeError(t.stderr)
+        sec = float([ln for ln in t.stdout.splitlines() if ln.startswith("TIME_RUN")][-1].split()[2])
+    return size ** 3 * n / sec / 1e6, n, sec
+
+
+def reference_arm(args, rank: int, world: int):
+    if rank != 0:
+        return 0
+    ranks = os.cpu_count() or 1
+    exe = reference_exe(threads=ranks > 1)
+    if exe is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref was not built (reference sources absent)"}))
+        return 0
+    val, n, sec = time_reference(args.size, args.neta, max(1, args.steps), ranks, budget_s=args.ref_budget)
+    line = {"metric": METRIC, "value": val, "unit": UNIT, "n_gpus": world, "steps": n, "warmup": 1,
+            "ms_per_step": 1e3 * sec / n, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic (reference initial state of the same workload)",
+            "impl": "reference",
+            "config": {"workload": f"3D {args.size}^3, {args.neta} evolving eta, bc=concentration, Ksp on, "
+                                   f"legacy Ck, bounds=legacy", "cells": args.size ** 3},
+            "cpu_baseline": {"value": val, "unit": UNIT, "cores": ranks, "kind": "reference",
+                             "sample": f"{n} timed steps of the full {args.size}^3 domain after 1 warm-up step, "
+                                       f"{ranks} thread-emulated MPI ranks (reference tests/mpi_threads.h)"},
+            "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+# ------------------------------------------------------------------ GPU arm
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=400)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["nicr", "reference"], default="nicr")
+    ap.add_argument("--size", type=int, default=256)
+    ap.add_argument("--neta", type=int, default=8)
+    ap.add_argument("--e2e-steps", type=int, default=50)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-budget", type=float, default=60.0, help="seconds of CPU stepping for the reference")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        return reference_arm(args, rank, world)
+
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+
+    import nicr
+    cfg = workload_config(args.size, args.neta, device=local, seed=2)
+    sol = nicr.Solver(cfg)
+    assert sol.n_eta == args.neta, (sol.n_eta, args.neta)
+    n = sol.n
+    rng = np.random.default_rng(2 + rank)
+    cr = 0.25 + rng.uniform(-0.01, 0.01, size=sol.shape)
+    cr[0] = sol.get("cr")[0]          # the inlet layer keeps its Cr
+    sol.set("cr", cr)
+    sol.reset_inventory()
+    stream = torch.cuda.ExternalStream(sol.stream(), device=local)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    # ---- warm-up
+    sol.run(args.warmup)
+    torch.cuda.synchronize()
+
+    # ---- device-timed region: K steps resident in HBM
+    L = nicr.lib()
+    L.nicr_profile.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    L.nicr_profile_read.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+                                    ctypes.POINTER(ctypes.c_longlong)]
+    L.nicr_kernel_launches.argtypes = [ctypes.c_void_p]
+    L.nicr_kernel_launches.restype = ctypes.c_longlong
+    L.nicr_profile(sol.h, 1)
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches0 = L.nicr_kernel_launches(sol.h)
+    e0.record(stream)
+    rc, done = sol.run(args.steps, check=False)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clocks = sampler.stop()
+    launches = L.nicr_kernel_launches(sol.h) - launches0
+    if rc != 0 or done != args.steps:
+        raise SystemExit(f"step rejected: {sol.last_error}")
+    ms = e0.elapsed_time(e1)
+    prof = {}
+    for k, name in enumerate(KERNELS):
+        tot, cnt = ctypes.c_double(0), ctypes.c_longlong(0)
+        L.nicr_profile_read(sol.h, k, ctypes.byref(tot), ctypes.byref(cnt))
+        if cnt.value:
+            prof[name] = (tot.value, cnt.value)
+    L.nicr_profile(sol.h, 0)
+
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = world * n * args.steps / (ms_max * 1e-3) / 1e6
+
+    # ---- end to end through the C-ABI with host buffers: upload the state from
+    # pinned memory, one nicr_run(1) call per step (each returns the accept status
+    # to the host), download the final state
+    fields = ["o", "cr", "p"] + [f"eta{g + 1}" for g in range(args.neta)]
+    host = {f: torch.empty(n, dtype=torch.float64).pin_memory().numpy() for f in fields}
+    for f in fields:
+        host[f][:] = sol.get(f).ravel()
+    torch.cuda.synchronize()
+    barrier()
+    t0 = time.perf_counter()
+    for f in fields:
+        sol.set(f, host[f])
+    for _ in range(args.e2e_steps):
+        sol.run(1)
+    for f in fields:
+        host[f][:] = sol.get(f).ravel()
+    e2e_s = time.perf_counter() - t0
+    te = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_val = world * n * args.e2e_steps / float(te.item()) / 1e6
+    state_bytes = len(fields) * n * 8
+    status_bytes = 40  # device status word read back by every nicr_run call
+
+    # ---- roofline of the dominant kernel
+    peak, peak_kind = measured_peak_hbm()
+    dom = max(prof, key=lambda k: prof[k][0]) if prof else "step_main"
+    dom_ms = prof[dom][0] / prof[dom][1] if prof else ms_max / args.steps
+    algo = algorithmic_bytes(dom, args.neta) * n
+    achieved = algo / (dom_ms * 1e-3) / 1e9
+    step_bytes = (6 + 2 * args.neta) * 8          # fused-minimum bytes of one whole step per cell
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded Cr noise, Voronoi seed 2); inputs ~3 GB > L2, no flush needed",
+        "config": {"workload": f"3D {args.size}^3, {args.neta} evolving eta (Voronoi seed 2), Cr 0.25+-0.01, "
+                               f"bc=concentration, Ksp on, legacy Ck, bounds=legacy, FP64 drop-in",
+                   "cells": n, "parallelism": f"independent domains x{world}", "l2": "inputs larger than L2"},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": peak_kind,
+                     "algorithmic_bytes_per_launch": algo, "avg_launch_ms": dom_ms,
+                     "traffic": ncu_traffic(dom, args.size)},
+        "step_hbm": {"bytes_per_cell": step_bytes, "achieved": step_bytes * value * 1e6 / world / 1e9,
+                     "frac": step_bytes * value * 1e6 / world / 1e9 / peak, "unit": "GB/s"},
+        "kernels": {k: {"ms_per_launch": v[0] / v[1], "launches": v[1], "share": v[0] / sum(x[0] for x in prof.values())}
+                    for k, v in prof.items()},
+        "e2e": {"value": e2e_val, "unit": UNIT, "steps": args.e2e_steps,
+                "h2d_bytes_per_step": state_bytes / args.e2e_steps,
+                "d2h_bytes_per_step": (state_bytes + status_bytes * args.e2e_steps) / args.e2e_steps},
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        ranks = os.cpu_count() or 1
+        try:
+            r = time_reference(args.size, args.neta, 10, ranks, budget_s=20.0)
+        except Exception as e:  # the baseline is reported, not required
+            r = None
+            line["cpu_baseline"] = {"value": None, "error": str(e)[:200]}
+        if r:
+            val, ns, sec = r
+            line["cpu_baseline"] = {"value": val, "unit": UNIT, "cores": ranks, "kind": "reference",
+                                    "sample": f"{ns} timed steps of the full {args.size}^3 domain after 1 warm-up "
+                                              f"step, {ranks} thread-emulated MPI ranks"}
+        elif "cpu_baseline" not in line:
+            line["cpu_baseline"] = {"value": None, "error": "oracle/_ref not built"}
+    if rank == 0:
+        print(json.dumps(line))
+    sol.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -203,6 +203,17 @@ int nicr_main(int dim, int argc, const char* const* argv);
 /* Stream the handle enqueues on (a cudaStream_t), for callers that overlap. */
 void* nicr_stream(nicr_handle* h);
 
+/* Measurement hooks (no counterpart in the reference, which has no GPU). When
+ * enabled, CUDA events bracket every kernel launch on the handle's stream;
+ * nicr_profile_read returns the accumulated device time and launch count of
+ * one kernel (0 step_main, 1 eta_update, 2 step_finalize, 3 eta_mask,
+ * 4 ksp_scan, 5 refresh, 6 diagnostics). nicr_kernel_launches counts every
+ * kernel the handle has launched since creation. */
+int nicr_profile(nicr_handle* h, int enable);
+int nicr_profile_read(nicr_handle* h, int kernel, double* total_ms, long long* launches);
+const char* nicr_profile_kernel_name(int kernel);
+long long nicr_kernel_launches(const nicr_handle* h);
+
 #ifdef __cplusplus
 }
 #endif

@@ -155,6 +155,24 @@ int nicr_get_grain_stats(nicr_handle* h, nicr_grain_stats* s, long long* cells, 
     });
 }
 
+int nicr_profile(nicr_handle* h, int enable) {
+    return guarded(h, [&](nicr::Model& m) { m.profile_enable(enable != 0); return (int)NICR_OK; });
+}
+
+int nicr_profile_read(nicr_handle* h, int kernel, double* total_ms, long long* launches) {
+    return guarded(h, [&](nicr::Model& m) {
+        if (kernel < 0 || kernel >= nicr::Model::K_COUNT) return (int)NICR_ERR_INVALID_ARG;
+        m.profile_collect();
+        if (total_ms) *total_ms = m.prof_ms[kernel];
+        if (launches) *launches = m.prof_n[kernel];
+        return (int)NICR_OK;
+    });
+}
+
+const char* nicr_profile_kernel_name(int kernel) { return nicr::Model::kernel_name(kernel); }
+
+long long nicr_kernel_launches(const nicr_handle* h) { return (h && h->m) ? h->m->launches : -1; }
+
 void* nicr_stream(nicr_handle* h) { return (h && h->m) ? (void*)h->m->stream : nullptr; }
 
 }  // extern "C"

@@ -167,6 +167,8 @@ void Model::release() {
                       kw.flag, kw.blocked, kw.counts, kw.list, kw.total};
     for (void* b : others) if (b) cudaFree(b);
     if (h_st) cudaFreeHost(h_st);
+    for (cudaEvent_t e : prof_pool) cudaEventDestroy(e);
+    prof_pool.clear();
     if (stream) cudaStreamDestroy(stream);
     std::memset(o_, 0, sizeof o_); std::memset(cr_, 0, sizeof cr_); std::memset(p_, 0, sizeof p_);
     std::memset(gb_, 0, sizeof gb_); std::memset(s2_, 0, sizeof s2_); std::memset(eta_, 0, sizeof eta_);
@@ -449,7 +451,9 @@ void Model::init_eta() {
 
 void Model::eta_mask_now() {
     if (!has_eta) return;
+    const size_t e = prof_begin();
     launch_eta_mask(sp, neta, eta_[ecur], gb_[gcur], s2_[gcur], dim == 2 ? pairs : nullptr, st, stream);
+    prof_end(K_ETA_MASK, e, 1);
     eta_dirty = false;
 }
 
@@ -542,7 +546,9 @@ void Model::refresh() {
         const size_t ns = (size_t)g.nstore;
         muO = dalloc(ns); muCr = dalloc(ns); mo = dalloc(ns); mc = dalloc(ns);
     }
+    const size_t e = prof_begin();
     launch_refresh(sp, o_[cur], cr_[cur], p_[cur], gb_[gcur], muO, muCr, mo, mc, stream);
+    prof_end(K_REFRESH, e, 1);
     check_cuda(cudaGetLastError(), "refresh");
 }
 
@@ -601,11 +607,18 @@ void Model::enqueue_step() {
     const int nxt = cur ^ 1;
     if (has_eta && eta_dirty) eta_mask_now();
     int nb = 0;
+    size_t e = prof_begin();
     launch_step_main(sp, o_[cur], cr_[cur], p_[cur], gb_[gcur], has_eta ? s2_[gcur] : nullptr, o_[nxt], cr_[nxt],
                      p_[nxt], partials, st, stream, &nb);
-    if (advance_eta)
+    prof_end(K_STEP_MAIN, e, 1);
+    if (advance_eta) {
+        e = prof_begin();
         launch_eta_update(sp, neta, eta_[ecur], s2_[gcur], p_[cur], eta_[ecur ^ 1], gb_[gcur ^ 1], s2_[gcur ^ 1], st, stream);
+        prof_end(K_ETA_UPDATE, e, 1);
+    }
+    e = prof_begin();
     launch_step_finalize(partials, nb, bud, st, 0, stream);
+    prof_end(K_FINALIZE, e, 1);
     cur = nxt;
     if (advance_eta) { ecur ^= 1; gcur ^= 1; }
 }
@@ -652,6 +665,7 @@ int Model::finish_batch(long long before, int enqueued, const std::vector<double
     check_cuda(cudaMemcpyAsync(h_st, st, sizeof(Status), cudaMemcpyDeviceToHost, stream), "D2H");
     sync();
     check_cuda(cudaGetLastError(), "step kernels");
+    profile_collect();
     if (!h_st->failed) {
         steps_done = before + enqueued;
         if (completed) *completed = enqueued;
@@ -700,7 +714,9 @@ int Model::run(int nsteps, int* completed) {
         const double time = double(n) * c.dt;
         if (c.nucleation == NICR_NUC_KSP && time + 1.e-12 * c.nucleation_period >= next) {
             kd.neta = neta;
+            const size_t e = prof_begin();
             launch_ksp_scan(kd, o_[cur], cr_[cur], p_[cur], eta_[ecur], kw, bud, kres, st, stream);
+            prof_end(K_KSP, e, 4);
             if (has_eta) eta_dirty = true;
             next += c.nucleation_period;
         }
@@ -778,6 +794,56 @@ void Model::diagnostics(nicr_diagnostics* d) {
 
 void Model::grain_stats(nicr_grain_stats*, long long*, double*) {
     throw Error(NICR_ERR_STATE, "grain statistics are not available yet");
+}
+
+// ------------------------------------------------------------------ measurement hooks
+const char* Model::kernel_name(int k) {
+    static const char* names[K_COUNT] = {"step_main", "eta_update", "step_finalize", "eta_mask", "ksp_scan",
+                                         "refresh", "diagnostics"};
+    return (k >= 0 && k < K_COUNT) ? names[k] : "?";
+}
+
+void Model::profile_enable(bool on) {
+    sync();
+    prof_on = on;
+    prof_used = 0;
+    prof_marks.clear();
+    for (int k = 0; k < K_COUNT; ++k) { prof_ms[k] = 0.; prof_n[k] = 0; }
+}
+
+size_t Model::prof_begin() {
+    if (!prof_on) return 0;
+    if (prof_used + 2 > prof_pool.size()) {
+        for (int q = 0; q < 64; ++q) {
+            cudaEvent_t e;
+            check_cuda(cudaEventCreate(&e), "cudaEventCreate");
+            prof_pool.push_back(e);
+        }
+    }
+    const size_t e0 = prof_used;
+    prof_used += 2;
+    check_cuda(cudaEventRecord(prof_pool[e0], stream), "cudaEventRecord");
+    return e0;
+}
+
+void Model::prof_end(int k, size_t e0, int kernels) {
+    launches += kernels;
+    if (!prof_on) return;
+    check_cuda(cudaEventRecord(prof_pool[e0 + 1], stream), "cudaEventRecord");
+    prof_marks.push_back(Mark{k, e0});
+}
+
+void Model::profile_collect() {
+    if (!prof_on) return;
+    sync();
+    for (const Mark& m : prof_marks) {
+        float ms = 0.f;
+        check_cuda(cudaEventElapsedTime(&ms, prof_pool[m.e0], prof_pool[m.e0 + 1]), "cudaEventElapsedTime");
+        prof_ms[m.k] += ms;
+        prof_n[m.k] += 1;
+    }
+    prof_marks.clear();
+    prof_used = 0;
 }
 
 }  // namespace nicr

@@ -64,6 +64,16 @@ public:
     size_t device_bytes() const { return dev_bytes; }
     void sync();
 
+    // measurement hooks: CUDA events around every kernel launch (when enabled)
+    // and a count of the kernels this model launched
+    enum Kern { K_STEP_MAIN, K_ETA_UPDATE, K_FINALIZE, K_ETA_MASK, K_KSP, K_REFRESH, K_DIAG, K_COUNT };
+    static const char* kernel_name(int k);
+    void profile_enable(bool on);
+    void profile_collect();
+    double prof_ms[K_COUNT] = {};
+    long long prof_n[K_COUNT] = {};
+    long long launches = 0;
+
     // raw device pointers of the current state (for tests, bench, writers)
     double* d_o() const { return o_[cur]; }
     double* d_cr() const { return cr_[cur]; }
@@ -107,6 +117,14 @@ private:
     unsigned char* d_hyp = nullptr;
     // pinned host staging for small results
     Status* h_st = nullptr;
+    // profiling
+    bool prof_on = false;
+    std::vector<cudaEvent_t> prof_pool;
+    size_t prof_used = 0;
+    struct Mark { int k; size_t e0; };
+    std::vector<Mark> prof_marks;
+    size_t prof_begin();
+    void prof_end(int k, size_t e0, int kernels);
 
     void release();
     double* dalloc(size_t n);
