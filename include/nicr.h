@@ -214,6 +214,13 @@ int nicr_profile_read(nicr_handle* h, int kernel, double* total_ms, long long* l
 const char* nicr_profile_kernel_name(int kernel);
 long long nicr_kernel_launches(const nicr_handle* h);
 
+/* Device self-check of the correctly rounded division by a run constant that
+ * the FP64 kernels use in place of IEEE a/b: n pseudo-random numerators
+ * (seeded) divided by b both ways on the current device. Returns the number
+ * of results that differ (0 expected) or -1 on a CUDA error; *tested receives
+ * the number of finite numerators checked. No counterpart in the reference. */
+long long nicr_check_division(double b, long long n, unsigned long long seed, long long* tested);
+
 #ifdef __cplusplus
 }
 #endif

@@ -173,6 +173,10 @@ const char* nicr_profile_kernel_name(int kernel) { return nicr::Model::kernel_na
 
 long long nicr_kernel_launches(const nicr_handle* h) { return (h && h->m) ? h->m->launches : -1; }
 
+long long nicr_check_division(double b, long long n, unsigned long long seed, long long* tested) {
+    return nicr::check_division(b, n, seed, tested);
+}
+
 void* nicr_stream(nicr_handle* h) { return (h && h->m) ? (void*)h->m->stream : nullptr; }
 
 }  // extern "C"

@@ -83,6 +83,13 @@ Model::Model(const nicr_config& cfg) : c(cfg), dim(cfg.dim) {
     sp.dxdx = c.dx * c.dx;
     sp.dada = c.dy * c.dy;
     sp.dbdb = dim == 3 ? c.dz * c.dz : c.dy * c.dy;
+    sp.v_dxdx = make_divc(sp.dxdx);
+    sp.v_dada = make_divc(sp.dada);
+    sp.v_dbdb = make_divc(sp.dbdb);
+    sp.v_dx = make_divc(sp.dx);
+    sp.v_da = make_divc(sp.da);
+    sp.v_db = make_divc(sp.db);
+    sp.v_dt = make_divc(sp.dt);
     sp.dtL = c.dt * Phys::L;
     sp.layer_o = c.layer_o;
     sp.gbm1_o = c.gb_factor_o - 1.;

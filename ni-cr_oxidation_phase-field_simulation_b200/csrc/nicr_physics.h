@@ -91,6 +91,58 @@ inline EtaCoef eta_coef(double fwhm, double dx, double W, double kappa, double p
     return e;
 }
 
+// Division by a run constant b, correctly rounded (bit-identical to a / b).
+// q1 = a*RN(1/b) refined by one FMA residual step is accepted only when an
+// exact FMA residual proves it is the nearest double: |a - q1*b| < |b|*ulp(q1)/2
+// (strict, so ties are excluded; q1 a power of two is excluded because its
+// lower neighbour is closer). The residual is exact whenever q1 is within an
+// ulp of a/b, and when it is not, its rounded value cannot pass the test, so
+// an accepted q1 is always RN(a/b). Outside the guarded exponent range (and
+// for zeros, infinities, NaNs) the IEEE division is used. The scale factor
+// 2^(53-E) (E = exponent of q1) keeps the comparison free of underflow.
+struct DivC {
+    double b, rb;   // divisor and RN(1/b)
+    int fast;       // b normal with 2^-60 <= |b| <= 2^60
+    int pad;
+};
+inline DivC make_divc(double b) {
+    DivC d;
+    d.b = b;
+    d.rb = 1.0 / b;
+    const double ab = std::fabs(b);
+    d.fast = (std::isnormal(b) && ab >= std::ldexp(1.0, -60) && ab <= std::ldexp(1.0, 60)) ? 1 : 0;
+    d.pad = 0;
+    return d;
+}
+#ifdef __CUDACC__
+// IEEE division kept out of line: it is only the rare fallback, and inlining
+// it at every call site would multiply the kernels' instruction footprint.
+__device__ __noinline__ double ieee_div(double a, double b);
+__device__ __forceinline__ double xdiv(double a, const DivC& d) {
+#if defined(NICR_DIV_IEEE)
+    return __ddiv_rn(a, d.b);
+#else
+    const long long ab = __double_as_longlong(a);
+    const int ea = (int)((ab >> 52) & 0x7FF);
+    if (d.fast && ea >= 123 && ea <= 1923) {
+        const double q0 = __dmul_rn(a, d.rb);
+        const double r0 = __fma_rn(-q0, d.b, a);
+        const double q1 = __fma_rn(r0, d.rb, q0);
+        const double r1 = __fma_rn(-q1, d.b, a);
+        const long long qb = __double_as_longlong(q1);
+        const int eq = (int)((qb >> 52) & 0x7FF);
+        const double scale = __longlong_as_double((long long)(2099 - eq) << 52);
+        if ((qb & 0x000FFFFFFFFFFFFFLL) != 0 && __dmul_rn(fabs(r1), scale) < fabs(d.b)) return q1;
+    }
+#if defined(NICR_DIV_INLINE_FALLBACK)
+    return __ddiv_rn(a, d.b);
+#else
+    return ieee_div(a, d.b);
+#endif
+#endif
+}
+#endif
+
 // Double-double accumulation (Knuth two-sum). Budget sums that the reference
 // keeps in 80-bit long double are kept as hi+lo pairs with ~106-bit precision.
 struct DD {

@@ -10,15 +10,19 @@
 // radius-1 halo. Nothing but the trial fields and per-CTA budget partials is
 // written to HBM: mu and M never leave the chip.
 //
-// The arithmetic is the reference's, operation for operation (nvcc -fmad=false,
-// IEEE division), so the FP64 results are bit-identical. Ghost semantics:
+// The arithmetic is the reference's, operation for operation (nvcc -fmad=false;
+// divisions by the run constants dx^2, dx, dt use xdiv, which returns the
+// correctly rounded quotient), so the FP64 results are bit-identical. Ghost semantics:
 // Neumann copies in X for o, cr, phi, gb and for the computed mu and M
 // (refresh copies mu(1) into the ghost, 3S:613-615), periodic rows/columns.
+#include <cstdlib>
 #include <cuda_runtime.h>
 #include "nicr_kernels.h"
 #include "nicr_physics.h"
 
 namespace nicr {
+
+__device__ __noinline__ double ieee_div(double a, double b) { return __ddiv_rn(a, b); }
 
 namespace {
 
@@ -76,45 +80,92 @@ struct Tile {
     __device__ static int i1(int a, int b) { return (a + HA1) * RB1 + (b + 1); }
 };
 
+// Divisions of the fused step: IEEE a / b (measured faster than xdiv here,
+// where registers are capped for occupancy).
+__device__ __forceinline__ double sdiv(double a, const DivC& d) { return __ddiv_rn(a, d.b); }
+
 struct CenterVals {
-    double o, cr, p, muO, muCr, mo, mc;
+    double o, cr, p, hh, muO, muCr, mo, mc;   // hh = h(p), reused by Ck
 };
 
 template <int DIM, int TA, int TB>
 struct StepKernel {
     using T = Tile<DIM, TA, TB>;
 
+    // Per-thread in-plane offsets (row*pitch + col, periodic wrap applied once
+    // per CTA) of the staging slots this thread fills: slot q = tid + k*NT.
+    struct Offs {
+        int o2[2];   // radius-2 tile points (o, cr)
+        int o1[2];   // radius-1 tile points (phi)
+        int gl[2];   // lead points: own cell, then the halo ring point tid (gb)
+    };
+    __device__ static Offs make_offs(const Grid& g, int a0, int b0) {
+        Offs f;
+        const int tid = threadIdx.x + TB * threadIdx.y;
+        for (int k = 0; k < 2; ++k) {
+            int q = tid + k * T::NT;
+            f.o2[k] = -1;
+            if (q < T::S2) {
+                const int a = q / T::RB2 - T::HA2, b = q % T::RB2 - 2;
+                f.o2[k] = (DIM == 3 ? wrapi(a0 + a, g.na) : 0) * g.pb + wrapi(b0 + b, g.nb);
+            }
+            f.o1[k] = -1;
+            if (q < T::S1) {
+                const int a = q / T::RB1 - T::HA1, b = q % T::RB1 - 1;
+                f.o1[k] = (DIM == 3 ? wrapi(a0 + a, g.na) : 0) * g.pb + wrapi(b0 + b, g.nb);
+            }
+        }
+        const int ta = DIM == 3 ? threadIdx.y : 0, tb = threadIdx.x;
+        f.gl[0] = (DIM == 3 ? wrapi(a0 + ta, g.na) : 0) * g.pb + wrapi(b0 + tb, g.nb);
+        f.gl[1] = -1;
+        if (tid < T::S1 - T::NT) {
+            int a, b;
+            ring_point(tid, a, b);
+            f.gl[1] = (DIM == 3 ? wrapi(a0 + a, g.na) : 0) * g.pb + wrapi(b0 + b, g.nb);
+        }
+        return f;
+    }
+    // halo ring enumeration: columns -1 and TB over all halo rows, then rows -1 and TA
+    __device__ static void ring_point(int hq, int& a, int& b) {
+        if (hq < 2 * T::RA1) {
+            a = hq / 2 - T::HA1;
+            b = (hq & 1) ? TB : -1;
+        } else {
+            const int r = hq - 2 * T::RA1;
+            a = (r / TB) ? TA : -1;
+            b = r % TB;
+        }
+    }
+
     // Loads plane xg (clamped to [0,nx-1]) of o and cr with a radius-2 halo
-    // into ring slot `slot`. The concentration inlet replaces o in plane 0 by
+    // into a ring slot. The concentration inlet replaces o in plane 0 by
     // layerO before the step (enforce_legacy_layer, 3S:593-596).
     __device__ static void load_oc(const StepParams& P, const double* __restrict__ o,
-                                   const double* __restrict__ cr, int xg, double* so, double* scr,
-                                   int a0, int b0) {
+                                   const double* __restrict__ cr, int xg, double* so, double* scr, const Offs& f) {
         const Grid& g = P.g;
         xg = xg < 0 ? 0 : (xg > g.nx - 1 ? g.nx - 1 : xg);
         const bool inlet = P.inlet && xg == 0;
         const long long base = (long long)xg * g.plane;
         const int tid = threadIdx.x + TB * threadIdx.y;
-        for (int q = tid; q < T::S2; q += T::NT) {
-            const int a = q / T::RB2 - T::HA2, b = q % T::RB2 - 2;
-            const int row = DIM == 3 ? wrapi(a0 + a, g.na) : 0;
-            const int col = wrapi(b0 + b, g.nb);
-            const long long idx = base + (long long)row * g.pb + col;
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            if (f.o2[k] < 0) continue;
+            const int q = tid + k * T::NT;
+            const long long idx = base + f.o2[k];
             so[q] = inlet ? P.layer_o : __ldg(o + idx);
             scr[q] = __ldg(cr + idx);
         }
     }
     __device__ static void load_p(const StepParams& P, const double* __restrict__ p, int xg, double* sp,
-                                  int a0, int b0) {
+                                  const Offs& f) {
         const Grid& g = P.g;
         xg = xg < 0 ? 0 : (xg > g.nx - 1 ? g.nx - 1 : xg);
         const long long base = (long long)xg * g.plane;
         const int tid = threadIdx.x + TB * threadIdx.y;
-        for (int q = tid; q < T::S1; q += T::NT) {
-            const int a = q / T::RB1 - T::HA1, b = q % T::RB1 - 1;
-            const int row = DIM == 3 ? wrapi(a0 + a, g.na) : 0;
-            const int col = wrapi(b0 + b, g.nb);
-            sp[q] = __ldg(p + base + (long long)row * g.pb + col);
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            if (f.o1[k] < 0) continue;
+            sp[tid + k * T::NT] = __ldg(p + base + f.o1[k]);
         }
     }
 
@@ -123,37 +174,31 @@ struct StepKernel {
                                             const double* som, const double* so0, const double* sop,
                                             const double* scm, const double* sc0, const double* scp,
                                             const double* sp, double* smuO, double* smuCr, double* smo,
-                                            double* smc, int x, int a, int b, int a0, int b0) {
+                                            double* smc, int x, int a, int b, int goff) {
         const int c2 = T::i2(a, b);
         const double oc = so0[c2], cc = sc0[c2];
         double lapO, lapC;
         if (DIM == 3) {
-            lapO = (sop[c2] - 2. * oc + som[c2]) / P.dxdx
-                 + (so0[T::i2(a + 1, b)] - 2. * oc + so0[T::i2(a - 1, b)]) / P.dada
-                 + (so0[T::i2(a, b + 1)] - 2. * oc + so0[T::i2(a, b - 1)]) / P.dbdb;
-            lapC = (scp[c2] - 2. * cc + scm[c2]) / P.dxdx
-                 + (sc0[T::i2(a + 1, b)] - 2. * cc + sc0[T::i2(a - 1, b)]) / P.dada
-                 + (sc0[T::i2(a, b + 1)] - 2. * cc + sc0[T::i2(a, b - 1)]) / P.dbdb;
+            lapO = sdiv((sop[c2] - 2. * oc + som[c2]), P.v_dxdx)
+                 + sdiv((so0[T::i2(a + 1, b)] - 2. * oc + so0[T::i2(a - 1, b)]), P.v_dada)
+                 + sdiv((so0[T::i2(a, b + 1)] - 2. * oc + so0[T::i2(a, b - 1)]), P.v_dbdb);
+            lapC = sdiv((scp[c2] - 2. * cc + scm[c2]), P.v_dxdx)
+                 + sdiv((sc0[T::i2(a + 1, b)] - 2. * cc + sc0[T::i2(a - 1, b)]), P.v_dada)
+                 + sdiv((sc0[T::i2(a, b + 1)] - 2. * cc + sc0[T::i2(a, b - 1)]), P.v_dbdb);
         } else {
-            lapO = (sop[c2] - 2. * oc + som[c2]) / P.dxdx
-                 + (so0[T::i2(a, b + 1)] - 2. * oc + so0[T::i2(a, b - 1)]) / P.dbdb;
-            lapC = (scp[c2] - 2. * cc + scm[c2]) / P.dxdx
-                 + (sc0[T::i2(a, b + 1)] - 2. * cc + sc0[T::i2(a, b - 1)]) / P.dbdb;
+            lapO = sdiv((sop[c2] - 2. * oc + som[c2]), P.v_dxdx)
+                 + sdiv((so0[T::i2(a, b + 1)] - 2. * oc + so0[T::i2(a, b - 1)]), P.v_dbdb);
+            lapC = sdiv((scp[c2] - 2. * cc + scm[c2]), P.v_dxdx)
+                 + sdiv((sc0[T::i2(a, b + 1)] - 2. * cc + sc0[T::i2(a, b - 1)]), P.v_dbdb);
         }
         const int c1 = T::i1(a, b);
         const double pc = sp[c1];
         const double hh = h(pc);
         CenterVals v;
-        v.o = oc; v.cr = cc; v.p = pc;
+        v.o = oc; v.cr = cc; v.p = pc; v.hh = hh;
         v.muO = mu_o_local(oc, cc, hh) - 2. * Phys::ko * lapO;
         v.muCr = mu_cr_local(oc, cc, hh) - 2. * Phys::kc * lapC;
-        double gbv = 0.;
-        if (P.grains) {
-            const Grid& g = P.g;
-            const int row = DIM == 3 ? wrapi(a0 + a, g.na) : 0;
-            const int col = wrapi(b0 + b, g.nb);
-            gbv = __ldg(gb + (long long)x * g.plane + (long long)row * g.pb + col);
-        }
+        const double gbv = P.grains ? __ldg(gb + (long long)x * P.g.plane + goff) : 0.;
         v.mo = P.o_on ? mobility(oc, hh, gbv, Phys::bmo, Phys::boo, P.gbm1_o) : 0.;
         v.mc = mobility(cc, hh, gbv, Phys::bmc, Phys::boc, P.gbm1_cr);
         smuO[c1] = v.muO; smuCr[c1] = v.muCr; smo[c1] = v.mo; smc[c1] = v.mc;
@@ -184,6 +229,7 @@ struct StepKernel {
         const int row = a0 + ta, col = b0 + tb;
         const bool active = (DIM == 3 ? row < g.na : true) && col < g.nb;
         const int blin = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+        const Offs offs = make_offs(g, a0, b0);
 
         DD acc[5] = {{0., 0.}, {0., 0.}, {0., 0.}, {0., 0.}, {0., 0.}};  // ckO ckCr clipO clipCr bcO
         long long clipped = 0;
@@ -205,22 +251,14 @@ struct StepKernel {
             double* mC = smuCr + (x & 1) * T::S1;
             double* mo_ = smo + (x & 1) * T::S1;
             double* mc_ = smc + (x & 1) * T::S1;
-            CenterVals own = lead_point(P, gb, som, so0, sop, scm, sc0, scp, spx, mO, mC, mo_, mc_, x, ta, tb, a0, b0);
-            // halo ring points, distributed over the first threads
-            constexpr int NH = T::S1 - T::NT;
+            CenterVals own = lead_point(P, gb, som, so0, sop, scm, sc0, scp, spx, mO, mC, mo_, mc_, x, ta, tb, offs.gl[0]);
+            // halo ring points: one per thread for the first S1-NT threads
+            static_assert(T::S1 - T::NT <= T::NT, "ring larger than the CTA");
             const int tid = threadIdx.x + TB * threadIdx.y;
-            for (int hq = tid; hq < NH; hq += T::NT) {
+            if (offs.gl[1] >= 0) {
                 int a, b;
-                // ring enumeration: columns -1 and TB over all halo rows, then rows -1 and TA
-                if (hq < 2 * T::RA1) {
-                    a = hq / 2 - T::HA1;
-                    b = (hq & 1) ? TB : -1;
-                } else {
-                    const int r = hq - 2 * T::RA1;
-                    a = (r / TB) ? TA : -1;
-                    b = r % TB;
-                }
-                lead_point(P, gb, som, so0, sop, scm, sc0, scp, spx, mO, mC, mo_, mc_, x, a, b, a0, b0);
+                ring_point(tid, a, b);
+                lead_point(P, gb, som, so0, sop, scm, sc0, scp, spx, mO, mC, mo_, mc_, x, a, b, offs.gl[1]);
             }
             return own;
         };
@@ -229,41 +267,41 @@ struct StepKernel {
         double pP, FxO, FxCr;
         // ---- prologue: centre values of the first update plane and its left x-face flux
         if (i0 == 0) {
-            load_oc(P, o, cr, -1, oslot(-1), cslot(-1), a0, b0);
-            load_oc(P, o, cr, 0, oslot(0), cslot(0), a0, b0);
-            load_oc(P, o, cr, 1, oslot(1), cslot(1), a0, b0);
-            load_p(P, p, 0, pslot(0), a0, b0);
+            load_oc(P, o, cr, -1, oslot(-1), cslot(-1), offs);
+            load_oc(P, o, cr, 0, oslot(0), cslot(0), offs);
+            load_oc(P, o, cr, 1, oslot(1), cslot(1), offs);
+            load_p(P, p, 0, pslot(0), offs);
             __syncthreads();
             C = lead(0);
             __syncthreads();
             // ghost plane -1: copies of plane 0 (3S:187, 3S:613-615, 3S:616-619)
             const double muOg = (P.bc == 1 && P.o_on) ? 2. * P.mu_res - C.muO : C.muO;
-            FxO = -.5 * (C.mo + C.mo) * (C.muO - muOg) / P.dx;
-            FxCr = -.5 * (C.mc + C.mc) * (C.muCr - C.muCr) / P.dx;
+            FxO = sdiv(-.5 * (C.mo + C.mo) * (C.muO - muOg), P.v_dx);
+            FxCr = sdiv(-.5 * (C.mc + C.mc) * (C.muCr - C.muCr), P.v_dx);
             pP = C.p;
         } else {
-            load_oc(P, o, cr, i0 - 2, oslot(i0 - 2), cslot(i0 - 2), a0, b0);
-            load_oc(P, o, cr, i0 - 1, oslot(i0 - 1), cslot(i0 - 1), a0, b0);
-            load_oc(P, o, cr, i0, oslot(i0), cslot(i0), a0, b0);
-            load_p(P, p, i0 - 1, pslot(i0 - 1), a0, b0);
+            load_oc(P, o, cr, i0 - 2, oslot(i0 - 2), cslot(i0 - 2), offs);
+            load_oc(P, o, cr, i0 - 1, oslot(i0 - 1), cslot(i0 - 1), offs);
+            load_oc(P, o, cr, i0, oslot(i0), cslot(i0), offs);
+            load_p(P, p, i0 - 1, pslot(i0 - 1), offs);
             __syncthreads();
             const CenterVals Pv = lead(i0 - 1);
             __syncthreads();  // window i0-2 (read by lead(i0-1)) shares a ring slot with i0+1
-            load_oc(P, o, cr, i0 + 1, oslot(i0 + 1), cslot(i0 + 1), a0, b0);
-            load_p(P, p, i0, pslot(i0), a0, b0);
+            load_oc(P, o, cr, i0 + 1, oslot(i0 + 1), cslot(i0 + 1), offs);
+            load_p(P, p, i0, pslot(i0), offs);
             __syncthreads();
             C = lead(i0);
             __syncthreads();
-            FxO = -.5 * (Pv.mo + C.mo) * (C.muO - Pv.muO) / P.dx;
-            FxCr = -.5 * (Pv.mc + C.mc) * (C.muCr - Pv.muCr) / P.dx;
+            FxO = sdiv(-.5 * (Pv.mo + C.mo) * (C.muO - Pv.muO), P.v_dx);
+            FxCr = sdiv(-.5 * (Pv.mc + C.mc) * (C.muCr - Pv.muCr), P.v_dx);
             pP = Pv.p;
         }
 
         for (int u = i0; u < i1; ++u) {
             const int x = u + 1;
             if (x <= g.nx - 1) {
-                load_oc(P, o, cr, x + 1, oslot(x + 1), cslot(x + 1), a0, b0);
-                load_p(P, p, x, pslot(x), a0, b0);
+                load_oc(P, o, cr, x + 1, oslot(x + 1), cslot(x + 1), offs);
+                load_p(P, p, x, pslot(x), offs);
                 __syncthreads();
                 L = lead(x);
                 __syncthreads();
@@ -283,8 +321,8 @@ struct StepKernel {
                 const long long cell = ((long long)u * g.na + row) * g.nb + col;  // reference loop order
 
                 // x faces: the right face of u is the left face of u+1 (same expression)
-                const double rightO = -.5 * (C.mo + L.mo) * (L.muO - C.muO) / P.dx;
-                const double rightCr = -.5 * (C.mc + L.mc) * (L.muCr - C.muCr) / P.dx;
+                const double rightO = sdiv(-.5 * (C.mo + L.mo) * (L.muO - C.muO), P.v_dx);
+                const double rightCr = sdiv(-.5 * (C.mc + L.mc) * (L.muCr - C.muCr), P.v_dx);
                 double leftO = FxO;
                 if (u == 0 && P.bc == 1) {
                     // left_flux (3S:621-628): surface-mobility face closure for bc=mu
@@ -292,36 +330,36 @@ struct StepKernel {
                     if (P.o_on) {
                         const double gb0 = P.grains ? __ldg(gb + gidx) : 0.;
                         const double mf = mobility(P.surface_c_ref, h(C.p), gb0, Phys::bmo, Phys::boo, P.gbm1_o);
-                        lf = 2. * mf * (P.mu_res - C.muO) / P.dx;
+                        lf = sdiv(2. * mf * (P.mu_res - C.muO), P.v_dx);
                     }
                     leftO = lf;
-                    acc[4] = dd_add(acc[4], P.dt * lf / P.dx);
+                    acc[4] = dd_add(acc[4], sdiv(P.dt * lf, P.v_dx));
                 }
                 if (u == 0 && P.inlet) acc[4] = dd_add(acc[4], P.layer_o - __ldg(o + gidx));
 
                 double divO = 0., divCr;
                 {
                     const double mc0 = mc_[c1], mu0 = mC[c1];
-                    const double front = -.5 * (mc0 + mc_[bp]) * (mC[bp] - mu0) / P.db;
-                    const double back = -.5 * (mc_[bm] + mc0) * (mu0 - mC[bm]) / P.db;
+                    const double front = sdiv(-.5 * (mc0 + mc_[bp]) * (mC[bp] - mu0), P.v_db);
+                    const double back = sdiv(-.5 * (mc_[bm] + mc0) * (mu0 - mC[bm]), P.v_db);
                     if (DIM == 3) {
-                        const double top = -.5 * (mc0 + mc_[ap]) * (mC[ap] - mu0) / P.da;
-                        const double bottom = -.5 * (mc_[am] + mc0) * (mu0 - mC[am]) / P.da;
-                        divCr = (FxCr - rightCr) / P.dx + (bottom - top) / P.da + (back - front) / P.db;
+                        const double top = sdiv(-.5 * (mc0 + mc_[ap]) * (mC[ap] - mu0), P.v_da);
+                        const double bottom = sdiv(-.5 * (mc_[am] + mc0) * (mu0 - mC[am]), P.v_da);
+                        divCr = sdiv(FxCr - rightCr, P.v_dx) + sdiv(bottom - top, P.v_da) + sdiv(back - front, P.v_db);
                     } else {
-                        divCr = (FxCr - rightCr) / P.dx + (back - front) / P.db;
+                        divCr = sdiv(FxCr - rightCr, P.v_dx) + sdiv(back - front, P.v_db);
                     }
                 }
                 if (P.o_on) {
                     const double m0 = mo_[c1], mu0 = mO[c1];
-                    const double front = -.5 * (m0 + mo_[bp]) * (mO[bp] - mu0) / P.db;
-                    const double back = -.5 * (mo_[bm] + m0) * (mu0 - mO[bm]) / P.db;
+                    const double front = sdiv(-.5 * (m0 + mo_[bp]) * (mO[bp] - mu0), P.v_db);
+                    const double back = sdiv(-.5 * (mo_[bm] + m0) * (mu0 - mO[bm]), P.v_db);
                     if (DIM == 3) {
-                        const double top = -.5 * (m0 + mo_[ap]) * (mO[ap] - mu0) / P.da;
-                        const double bottom = -.5 * (mo_[am] + m0) * (mu0 - mO[am]) / P.da;
-                        divO = (leftO - rightO) / P.dx + (bottom - top) / P.da + (back - front) / P.db;
+                        const double top = sdiv(-.5 * (m0 + mo_[ap]) * (mO[ap] - mu0), P.v_da);
+                        const double bottom = sdiv(-.5 * (mo_[am] + m0) * (mu0 - mO[am]), P.v_da);
+                        divO = sdiv(leftO - rightO, P.v_dx) + sdiv(bottom - top, P.v_da) + sdiv(back - front, P.v_db);
                     } else {
-                        divO = (leftO - rightO) / P.dx + (back - front) / P.db;
+                        divO = sdiv(leftO - rightO, P.v_dx) + sdiv(back - front, P.v_db);
                     }
                 }
                 const double oo = C.o, cc = C.cr, pp = C.p;
@@ -329,18 +367,19 @@ struct StepKernel {
                 double crv = cc + P.dt * divCr;
                 double lapP;
                 if (DIM == 3)
-                    lapP = (L.p - 2. * pp + pP) / P.dxdx + (spu[ap] - 2. * pp + spu[am]) / P.dada
-                         + (spu[bp] - 2. * pp + spu[bm]) / P.dbdb;
+                    lapP = sdiv((L.p - 2. * pp + pP), P.v_dxdx) + sdiv((spu[ap] - 2. * pp + spu[am]), P.v_dada)
+                         + sdiv((spu[bp] - 2. * pp + spu[bm]), P.v_dbdb);
                 else
-                    lapP = (L.p - 2. * pp + pP) / P.dxdx + (spu[bp] - 2. * pp + spu[bm]) / P.dbdb;
+                    lapP = sdiv((L.p - 2. * pp + pP), P.v_dxdx) + sdiv((spu[bp] - 2. * pp + spu[bm]), P.v_dbdb);
                 const double hpv = 30. * pp * pp * (pp - 1.) * (pp - 1.);
                 double fp = Phys::W * (4. * pp * pp * pp - 6. * pp * pp + 2. * pp)
                           + hpv * (foxide(oo, cc) - fmetal(oo, cc)) - 2. * Phys::kp * lapP;
                 if (P.phi_eta) fp += grain_dphi(__ldg(s2 + gidx), pp, P.eta_W, P.eta_A);
                 double pnv = pp - P.dtL * fp;
                 if (P.ck == 0) {
-                    const double dO = -Phys::ckO * ((Phys::oxideO - onv) * h(pnv) - (Phys::oxideO - oo) * h(pp)) / P.dt;
-                    const double dCr = -Phys::ckCr * ((Phys::oxideCr - crv) * h(pnv) - (Phys::oxideCr - cc) * h(pp)) / P.dt;
+                    const double hn = h(pnv);
+                    const double dO = sdiv(-Phys::ckO * ((Phys::oxideO - onv) * hn - (Phys::oxideO - oo) * C.hh), P.v_dt);
+                    const double dCr = sdiv(-Phys::ckCr * ((Phys::oxideCr - crv) * hn - (Phys::oxideCr - cc) * C.hh), P.v_dt);
                     onv += dO; crv += dCr;
                     acc[0] = dd_add(acc[0], dO);
                     acc[1] = dd_add(acc[1], dCr);
@@ -375,8 +414,8 @@ struct StepKernel {
     }
 };
 
-template <int DIM, int TA, int TB>
-__global__ void __launch_bounds__(TA * TB)
+template <int DIM, int TA, int TB, int MINB>
+__global__ void __launch_bounds__(TA * TB, MINB)
 k_step_main(const StepParams P, const double* __restrict__ o, const double* __restrict__ cr,
             const double* __restrict__ p, const double* __restrict__ gb, const double* __restrict__ s2,
             double* __restrict__ on, double* __restrict__ crn, double* __restrict__ pn,
@@ -453,12 +492,12 @@ __global__ void k_eta_update(const StepParams P, int neta, const double* __restr
         const double ec = __ldg(e + idx);
         double lap;
         if (DIM == 3)
-            lap = (__ldg(e + ixp) - 2. * ec + __ldg(e + ixm)) / P.dxdx
-                + (__ldg(e + iap) - 2. * ec + __ldg(e + iam)) / P.dada
-                + (__ldg(e + ibp) - 2. * ec + __ldg(e + ibm)) / P.dbdb;
+            lap = xdiv((__ldg(e + ixp) - 2. * ec + __ldg(e + ixm)), P.v_dxdx)
+                + xdiv((__ldg(e + iap) - 2. * ec + __ldg(e + iam)), P.v_dada)
+                + xdiv((__ldg(e + ibp) - 2. * ec + __ldg(e + ibm)), P.v_dbdb);
         else
-            lap = (__ldg(e + ixp) - 2. * ec + __ldg(e + ixm)) / P.dxdx
-                + (__ldg(e + ibp) - 2. * ec + __ldg(e + ibm)) / P.dbdb;
+            lap = xdiv((__ldg(e + ixp) - 2. * ec + __ldg(e + ixm)), P.v_dxdx)
+                + xdiv((__ldg(e + ibp) - 2. * ec + __ldg(e + ibm)), P.v_dbdb);
         const double force = grain_deta(ec, S, phi, P.eta_W, P.eta_A) - P.eta_K * lap;
         const double v = ec - P.dt_etaL * force;
         if (!isfinite(v) || v < -1.e-12 || v > 1. + 1.e-12)
@@ -471,6 +510,117 @@ __global__ void k_eta_update(const StepParams P, int neta, const double* __restr
     s2_next[idx] = Sn;
     gb_next[idx] = P.eta_scale * smin(1., 16. * pairs);
     if (errkey != ERR_NONE) atomicMin(&st->err_key, errkey);
+}
+
+// Streaming form of the eta update: each CTA owns a rows x columns tile,
+// marches along X and stages every eta plane once (radius-1 halo) in a
+// three-plane shared-memory ring, so every field is read from HBM about once.
+// S = sum eta_g^2 is rebuilt from the staged centres in g order, which is the
+// same arithmetic as rebuild_eta_mask and therefore the same value as eta_s2.
+template <int DIM, int TA, int TB>
+__global__ void __launch_bounds__(TA * TB)
+k_eta_stream(const StepParams P, int neta, const double* __restrict__ eta, const double* __restrict__ p,
+             double* __restrict__ eta_next, double* __restrict__ gb_next, double* __restrict__ s2_next,
+             Status* st) {
+    constexpr int HA = DIM == 3 ? 1 : 0;
+    constexpr int RA = TA + 2 * HA, RB = TB + 2, S1 = RA * RB, NT = TA * TB;
+    extern __shared__ __align__(16) double ring[];   // [3][neta][S1], then S1 int offsets
+    if (st->failed) return;
+    const Grid& g = P.g;
+    const int ta = DIM == 3 ? threadIdx.y : 0, tb = threadIdx.x;
+    const int a0 = DIM == 3 ? blockIdx.y * TA : 0, b0 = blockIdx.x * TB;
+    const int i0 = blockIdx.z * P.xchunk, i1 = min(g.nx, i0 + P.xchunk);
+    const int row = a0 + ta, col = b0 + tb;
+    const bool active = (DIM == 3 ? row < g.na : true) && col < g.nb;
+    const int tid = threadIdx.x + TB * threadIdx.y;
+    int* toff = reinterpret_cast<int*>(ring + (size_t)3 * neta * S1);
+    for (int r = tid; r < S1; r += NT) {
+        const int a = r / RB - HA, b = r % RB - 1;
+        toff[r] = (DIM == 3 ? wrapi(a0 + a, g.na) : 0) * g.pb + wrapi(b0 + b, g.nb);
+    }
+    __syncthreads();
+    auto slot = [&](int x) { return ring + (size_t)(((x % 3) + 3) % 3) * neta * S1; };
+    auto load = [&](int x) {
+        const int xg = x < 0 ? 0 : (x > g.nx - 1 ? g.nx - 1 : x);
+        double* dst = slot(x);
+        const double* src = eta + (long long)xg * g.plane;
+        for (int e = 0; e < neta; ++e) {
+            const double* se = src + (long long)e * g.nstore;
+            double* de = dst + e * S1;
+            for (int r = tid; r < S1; r += NT) de[r] = __ldg(se + toff[r]);
+        }
+    };
+    const int c1 = (ta + HA) * RB + (tb + 1);
+    const int bp = c1 + 1, bm = c1 - 1, ap = c1 + RB, am = c1 - RB;
+    unsigned long long errkey = ERR_NONE;
+    load(i0 - 1);
+    load(i0);
+    for (int u = i0; u < i1; ++u) {
+        load(u + 1);
+        __syncthreads();
+        if (active) {
+            const double* sm = slot(u - 1);
+            const double* s0 = slot(u);
+            const double* sp = slot(u + 1);
+            const long long idx = (long long)u * g.plane + (long long)row * g.pb + col;
+            const long long cell = ((long long)u * g.na + row) * g.nb + col;
+            double S = 0.;
+            for (int e = 0; e < neta; ++e) {
+                const double v = s0[e * S1 + c1];
+                S += v * v;
+            }
+            const double phi = __ldg(p + idx);
+            double Sn = 0., pairs = 0.;
+            for (int e = 0; e < neta; ++e) {
+                const int o = e * S1;
+                const double ec = s0[o + c1];
+                double lap;
+                if (DIM == 3)
+                    lap = xdiv((sp[o + c1] - 2. * ec + sm[o + c1]), P.v_dxdx)
+                        + xdiv((s0[o + ap] - 2. * ec + s0[o + am]), P.v_dada)
+                        + xdiv((s0[o + bp] - 2. * ec + s0[o + bm]), P.v_dbdb);
+                else
+                    lap = xdiv((sp[o + c1] - 2. * ec + sm[o + c1]), P.v_dxdx)
+                        + xdiv((s0[o + bp] - 2. * ec + s0[o + bm]), P.v_dbdb);
+                const double force = grain_deta(ec, S, phi, P.eta_W, P.eta_A) - P.eta_K * lap;
+                const double v = ec - P.dt_etaL * force;
+                if (!isfinite(v) || v < -1.e-12 || v > 1. + 1.e-12)
+                    errkey = min(errkey, ERR_ETA_BASE + (unsigned long long)e * (unsigned long long)g.ncells + (unsigned long long)cell);
+                eta_next[(long long)e * g.nstore + idx] = v;
+                const double sq = v * v;
+                pairs += Sn * sq;
+                Sn += sq;
+            }
+            s2_next[idx] = Sn;
+            gb_next[idx] = P.eta_scale * smin(1., 16. * pairs);
+        }
+        __syncthreads();   // slot(u-1) is refilled with plane u+2 next
+    }
+    if (errkey != ERR_NONE) atomicMin(&st->err_key, errkey);
+}
+
+// Self-check of xdiv on the device: random numerators (all finite bit
+// patterns, and values of typical magnitude) against IEEE division.
+__global__ void k_check_division(DivC d, long long n, unsigned long long seed, unsigned long long* counts) {
+    unsigned long long bad = 0, total = 0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        unsigned long long x = seed ^ (0x9E3779B97F4A7C15ull * (unsigned long long)(i + 1));
+        x ^= x >> 33; x *= 0xff51afd7ed558ccdull; x ^= x >> 33; x *= 0xc4ceb9fe1a85ec53ull; x ^= x >> 33;
+        double a;
+        if (i & 3) {
+            const int e = (int)((x >> 56) % 120) - 60;
+            a = ldexp((double)(x >> 11) * (1.0 / 9007199254740992.0) + 0.5, e);
+            if (x & 1) a = -a;
+        } else {
+            a = __longlong_as_double((long long)x);
+            if (!isfinite(a)) continue;
+        }
+        const double q = xdiv(a, d), w = __ddiv_rn(a, d.b);
+        bad += __double_as_longlong(q) != __double_as_longlong(w);
+        ++total;
+    }
+    atomicAdd(counts, bad);
+    atomicAdd(counts + 1, total);
 }
 
 // Step commit: partial sums in block order (deterministic), then the budget is
@@ -530,9 +680,9 @@ __global__ void k_refresh(const StepParams P, const double* __restrict__ o, cons
     auto lapf = [&](const double* a) {
         const double c = a[idx];
         if (DIM == 3)
-            return (a[ixp] - 2. * c + a[ixm]) / P.dxdx + (a[iap] - 2. * c + a[iam]) / P.dada
-                 + (a[ibp] - 2. * c + a[ibm]) / P.dbdb;
-        return (a[ixp] - 2. * c + a[ixm]) / P.dxdx + (a[ibp] - 2. * c + a[ibm]) / P.dbdb;
+            return xdiv((a[ixp] - 2. * c + a[ixm]), P.v_dxdx) + xdiv((a[iap] - 2. * c + a[iam]), P.v_dada)
+                 + xdiv((a[ibp] - 2. * c + a[ibm]), P.v_dbdb);
+        return xdiv((a[ixp] - 2. * c + a[ixm]), P.v_dxdx) + xdiv((a[ibp] - 2. * c + a[ibm]), P.v_dbdb);
     };
     const double oc = o[idx], cc = cr[idx];
     const double hh = h(p[idx]);
@@ -551,23 +701,43 @@ int step_main_blocks(const StepParams& P) {
     return (int)(grid.x * grid.y * grid.z);
 }
 
+// Occupancy variant of the 3D step kernel: 3 CTAs/SM (80 registers, the
+// default, measured faster on B200) or 2 CTAs/SM (no register cap).
+// NICR_STEP_MINB=2|3 selects one for tuning runs.
+static int step_minb() {
+    static int v = 0;
+    if (!v) {
+        const char* e = getenv("NICR_STEP_MINB");
+        v = (e && e[0] == '2') ? 2 : 3;
+    }
+    return v;
+}
+
+template <int MINB>
+static void launch_step3(const StepParams& P, const double* o, const double* cr, const double* p, const double* gb,
+                         const double* s2, double* on, double* crn, double* pn, StepPartial* partials, Status* st,
+                         cudaStream_t stream, int* nblocks_out) {
+    using T = Tile<3, TA3, TB3>;
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_step_main<3, TA3, TB3, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM_BYTES);
+        attr = true;
+    }
+    const dim3 grid = step_grid<3, TA3, TB3>(P);
+    k_step_main<3, TA3, TB3, MINB><<<grid, dim3(TB3, TA3), T::SMEM_BYTES, stream>>>(P, o, cr, p, gb, s2, on, crn, pn, partials, st);
+    if (nblocks_out) *nblocks_out = (int)(grid.x * grid.y * grid.z);
+}
+
 void launch_step_main(const StepParams& P, const double* o, const double* cr, const double* p, const double* gb,
                       const double* s2, double* on, double* crn, double* pn, StepPartial* partials, Status* st,
                       cudaStream_t stream, int* nblocks_out) {
     if (P.g.dim == 3) {
-        using T = Tile<3, TA3, TB3>;
-        static bool attr = false;
-        if (!attr) {
-            cudaFuncSetAttribute(k_step_main<3, TA3, TB3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM_BYTES);
-            attr = true;
-        }
-        const dim3 grid = step_grid<3, TA3, TB3>(P);
-        k_step_main<3, TA3, TB3><<<grid, dim3(TB3, TA3), T::SMEM_BYTES, stream>>>(P, o, cr, p, gb, s2, on, crn, pn, partials, st);
-        if (nblocks_out) *nblocks_out = (int)(grid.x * grid.y * grid.z);
+        if (step_minb() == 3) launch_step3<3>(P, o, cr, p, gb, s2, on, crn, pn, partials, st, stream, nblocks_out);
+        else launch_step3<2>(P, o, cr, p, gb, s2, on, crn, pn, partials, st, stream, nblocks_out);
     } else {
         using T = Tile<2, TA2, TB2>;
         const dim3 grid = step_grid<2, TA2, TB2>(P);
-        k_step_main<2, TA2, TB2><<<grid, dim3(TB2, TA2), T::SMEM_BYTES, stream>>>(P, o, cr, p, gb, s2, on, crn, pn, partials, st);
+        k_step_main<2, TA2, TB2, 4><<<grid, dim3(TB2, TA2), T::SMEM_BYTES, stream>>>(P, o, cr, p, gb, s2, on, crn, pn, partials, st);
         if (nblocks_out) *nblocks_out = (int)(grid.x * grid.y * grid.z);
     }
 }
@@ -584,11 +754,43 @@ void launch_eta_mask(const StepParams& P, int neta, const double* eta, double* g
 void launch_eta_update(const StepParams& P, int neta, const double* eta, const double* s2, const double* p,
                        double* eta_next, double* gb_next, double* s2_next, Status* st, cudaStream_t stream) {
     const Grid& g = P.g;
+    // The per-cell kernel (stencil neighbours through L1/L2) is the default: the
+    // streaming kernel stalls on its per-plane barriers until the next plane
+    // has arrived. NICR_ETA_KERNEL=stream selects it for tuning runs.
+    static int simple = -1;
+    if (simple < 0) {
+        const char* e = getenv("NICR_ETA_KERNEL");
+        simple = (e && e[0] == 's' && e[1] == 't') ? 0 : 1;
+    }
     if (g.dim == 3) {
+        constexpr int TA = 8, TB = 32, S1 = (TA + 2) * (TB + 2);
+        const size_t smem = (size_t)3 * neta * S1 * sizeof(double) + S1 * sizeof(int);
+        if (!simple && smem <= 200 * 1024) {
+            static size_t attr = 0;
+            if (smem > 48 * 1024 && smem > attr) {
+                cudaFuncSetAttribute(k_eta_stream<3, TA, TB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                attr = smem;
+            }
+            const dim3 grid((g.nb + TB - 1) / TB, (g.na + TA - 1) / TA, (g.nx + P.xchunk - 1) / P.xchunk);
+            k_eta_stream<3, TA, TB><<<grid, dim3(TB, TA), smem, stream>>>(P, neta, eta, p, eta_next, gb_next, s2_next, st);
+            return;
+        }
         const dim3 block(32, 8);
         const dim3 grid((g.nb + 31) / 32, (g.na + 7) / 8, g.nx);
         k_eta_update<3><<<grid, block, 0, stream>>>(P, neta, eta, s2, p, eta_next, gb_next, s2_next, st);
     } else {
+        constexpr int TB = 128, S1 = TB + 2;
+        const size_t smem = (size_t)3 * neta * S1 * sizeof(double) + S1 * sizeof(int);
+        if (smem <= 200 * 1024) {
+            static size_t attr = 0;
+            if (smem > 48 * 1024 && smem > attr) {
+                cudaFuncSetAttribute(k_eta_stream<2, 1, TB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                attr = smem;
+            }
+            const dim3 grid((g.nb + TB - 1) / TB, 1, (g.nx + P.xchunk - 1) / P.xchunk);
+            k_eta_stream<2, 1, TB><<<grid, dim3(TB, 1), smem, stream>>>(P, neta, eta, p, eta_next, gb_next, s2_next, st);
+            return;
+        }
         const dim3 block(128, 1);
         const dim3 grid((g.nb + 127) / 128, 1, g.nx);
         k_eta_update<2><<<grid, block, 0, stream>>>(P, neta, eta, s2, p, eta_next, gb_next, s2_next, st);
@@ -612,6 +814,19 @@ void launch_refresh(const StepParams& P, const double* o, const double* cr, cons
         const dim3 grid((g.nb + 127) / 128, 1, g.nx);
         k_refresh<2><<<grid, block, 0, stream>>>(P, o, cr, p, gb, muO, muCr, mo, mc);
     }
+}
+
+long long check_division(double b, long long n, unsigned long long seed, long long* tested) {
+    unsigned long long* d = nullptr;
+    if (cudaMalloc(&d, 2 * sizeof(unsigned long long)) != cudaSuccess) return -1;
+    cudaMemset(d, 0, 2 * sizeof(unsigned long long));
+    k_check_division<<<148 * 8, 256>>>(make_divc(b), n, seed, d);
+    unsigned long long h[2] = {0, 0};
+    const cudaError_t e = cudaMemcpy(h, d, sizeof h, cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) return -1;
+    if (tested) *tested = (long long)h[1];
+    return (long long)h[0];
 }
 
 }  // namespace nicr

@@ -18,7 +18,7 @@ from ._abi import (BC, BOUNDS, CK, FIELD, NUCLEATION, NicrConfig, config_to_flag
                    make_config)
 
 PKG = Path(__file__).resolve().parent.parent
-LIB_PATH = PKG / "lib" / "libnicr.so"
+LIB_PATH = Path(os.environ["NICR_LIBRARY"]) if os.environ.get("NICR_LIBRARY") else PKG / "lib" / "libnicr.so"
 
 _lib = None
 

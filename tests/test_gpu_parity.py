@@ -140,3 +140,17 @@ def test_run_schedule_with_ksp(require_gpu, dim):
     assert done2 == 30
     compare_state(sol, orc)
     assert sol.budget()["nuclei"] > 0
+
+
+@pytest.mark.parametrize("b", [1e-16, 1.0000000000000002e-16, 1e-8, 2e-10, 1e-12, 3.3e-9, 0.7, 3.0])
+def test_verified_division_matches_ieee(require_gpu, b):
+    """xdiv (reciprocal + FMA correction + exact residual proof, IEEE fallback)
+    returns exactly a/b on the device for 2^27 seeded numerators per divisor."""
+    import ctypes
+    L = nicr.lib()
+    L.nicr_check_division.argtypes = [ctypes.c_double, ctypes.c_longlong, ctypes.c_ulonglong,
+                                      ctypes.POINTER(ctypes.c_longlong)]
+    L.nicr_check_division.restype = ctypes.c_longlong
+    tested = ctypes.c_longlong(0)
+    bad = L.nicr_check_division(b, 1 << 27, 12345, ctypes.byref(tested))
+    assert bad == 0 and tested.value > (1 << 26)
