@@ -8,10 +8,6 @@
 #include "../../include/nicr.h"
 #include "nicr_model.h"
 
-struct nicr_handle {
-    nicr::Model* m = nullptr;
-    std::string err;
-};
 
 namespace {
 thread_local std::string g_create_error;

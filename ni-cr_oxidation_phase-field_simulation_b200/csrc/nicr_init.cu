@@ -260,6 +260,144 @@ __global__ void k_diag_finalize(const DiagOut* __restrict__ partials, int nblock
     *out = r;
 }
 
+// ---- grain statistics (Model::grain_log, 3S:566-590; grain_energy 3S:546-565)
+// Scalars per block: lo/hi of eta (first-in-order extrema over (cell, g)),
+// slo/shi of S, sums of S, (1-h)gb and the energy density (dd), max gb,
+// unassigned cells; the dominant-grain cell counts go through integer atomics.
+struct GrainPart {
+    double sum[3][2];        // S, mask, energy
+    Ext lo, hi, slo, shi, gbmax;
+    long long unassigned;
+};
+__global__ void k_grain_scalar(const GrainParams G, const double* __restrict__ eta, const double* __restrict__ s2,
+                               const double* __restrict__ p, const double* __restrict__ gb,
+                               unsigned long long* __restrict__ cells, GrainPart* parts) {
+    const Grid& g = G.g;
+    DD acc[3] = {{0., 0.}, {0., 0.}, {0., 0.}};
+    Ext lo{1., -1}, hi{0., -1}, slo{CUDART_INF, -1}, shi{0., -1}, gbmax{0., -1};
+    long long unassigned = 0;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < g.ncells; c += (long long)gridDim.x * blockDim.x) {
+        int xi, row, col;
+        decode(g, c, xi, row, col);
+        const long long idx = (long long)xi * g.plane + (long long)row * g.pb + col;
+        const double S = s2[idx], pv = p[idx], metal = 1. - h(pv), gbv = gb[idx];
+        slo = ext_min(slo, Ext{S, c});
+        shi = ext_max(shi, Ext{S, c});
+        acc[0] = dd_add(acc[0], S);
+        acc[1] = dd_add(acc[1], metal * gbv);
+        gbmax = ext_max(gbmax, Ext{gbv, c});
+        // current_grain (3S:527-533): eta argmax above 1e-12 in metal (phi < .5)
+        int id = 0;
+        double best = 1.e-12;
+        double pairs = 0., Sr = 0.;
+        for (int q = 0; q < G.neta; ++q) {
+            const double v = eta[(long long)q * g.nstore + idx];
+            lo = ext_min(lo, Ext{v, c * G.neta + q});
+            hi = ext_max(hi, Ext{v, c * G.neta + q});
+            if (v > best) { best = v; id = q + 1; }
+            const double sq = v * v;
+            pairs += Sr * sq;
+            Sr += sq;
+        }
+        if (pv >= .5) id = 0;
+        if (id) atomicAdd(cells + (id - 1), 1ull);
+        else if (pv < .5) ++unassigned;
+        // energy density: local terms + forward-face gradients (Neumann X, periodic rows/cols)
+        double density = grain_energy_density(S, G.dim == 3 ? pairs : G.pairs[idx], pv, G.W, G.A);
+        const long long ixp = idx + g.plane;
+        const long long iap = (long long)xi * g.plane + (long long)(row == g.na - 1 ? 0 : row + 1) * g.pb + col;
+        const long long ibp = (long long)xi * g.plane + (long long)row * g.pb + (col == g.nb - 1 ? 0 : col + 1);
+        for (int q = 0; q < G.neta; ++q) {
+            const double* e = eta + (long long)q * g.nstore;
+            const double ec = e[idx];
+            if (xi < g.nx - 1) { const double t = (e[ixp] - ec) / G.dx; density += .5 * G.K * (t * t); }
+            if (G.dim == 3) {
+                { const double t = (e[iap] - ec) / G.da; density += .5 * G.K * (t * t); }
+                { const double t = (e[ibp] - ec) / G.db; density += .5 * G.K * (t * t); }
+            } else {
+                const double t = (e[ibp] - ec) / G.db;
+                density += .5 * G.K * (t * t);
+            }
+        }
+        acc[2] = dd_add(acc[2], G.dim == 3 ? density * G.dx * G.da * G.db : density * G.dx * G.db);
+    }
+    // block reduction
+    for (int off = 16; off > 0; off >>= 1) {
+        lo = ext_min(lo, shfl_ext(lo, off)); hi = ext_max(hi, shfl_ext(hi, off));
+        slo = ext_min(slo, shfl_ext(slo, off)); shi = ext_max(shi, shfl_ext(shi, off));
+        gbmax = ext_max(gbmax, shfl_ext(gbmax, off));
+    }
+    __shared__ Ext se[32][5];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    if (lane == 0) { se[w][0] = lo; se[w][1] = hi; se[w][2] = slo; se[w][3] = shi; se[w][4] = gbmax; }
+    block_reduce<3>(acc, unassigned);
+    if (threadIdx.x == 0) {
+        for (int ww = 1; ww < nw; ++ww) {
+            lo = ext_min(lo, se[ww][0]); hi = ext_max(hi, se[ww][1]);
+            slo = ext_min(slo, se[ww][2]); shi = ext_max(shi, se[ww][3]); gbmax = ext_max(gbmax, se[ww][4]);
+        }
+        GrainPart& o = parts[blockIdx.x];
+        for (int q = 0; q < 3; ++q) { o.sum[q][0] = acc[q].hi; o.sum[q][1] = acc[q].lo; }
+        o.lo = lo; o.hi = hi; o.slo = slo; o.shi = shi; o.gbmax = gbmax;
+        o.unassigned = unassigned;
+    }
+}
+
+// weighted metal amount of grain q: sum of (1-h) eta_q^2 / S over cells with S > 1e-24
+__global__ void k_grain_amount(const GrainParams G, const double* __restrict__ eta, const double* __restrict__ s2,
+                               const double* __restrict__ p, double* amount_parts /* [gridDim.x][neta][2] */) {
+    const Grid& g = G.g;
+    const int q = blockIdx.y;
+    DD acc[1] = {{0., 0.}};
+    long long dummy = 0;
+    const double* e = eta + (long long)q * g.nstore;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < g.ncells; c += (long long)gridDim.x * blockDim.x) {
+        int xi, row, col;
+        decode(g, c, xi, row, col);
+        const long long idx = (long long)xi * g.plane + (long long)row * g.pb + col;
+        const double S = s2[idx];
+        if (S > 1.e-24) {
+            const double v = e[idx], metal = 1. - h(p[idx]);
+            acc[0] = dd_add(acc[0], metal * v * v / S);
+        }
+    }
+    block_reduce<1>(acc, dummy);
+    if (threadIdx.x == 0) {
+        amount_parts[((long long)blockIdx.x * G.neta + q) * 2] = acc[0].hi;
+        amount_parts[((long long)blockIdx.x * G.neta + q) * 2 + 1] = acc[0].lo;
+    }
+}
+
+__global__ void k_grain_finalize(const GrainParams G, const GrainPart* __restrict__ parts, int nparts,
+                                 const double* __restrict__ amount_parts, const unsigned long long* __restrict__ cells,
+                                 GrainOut* out, double* amount_out, long long* cells_out) {
+    // one thread per grain for the amounts (block order), thread 0 for the scalars
+    for (int q = threadIdx.x; q < G.neta; q += blockDim.x) {
+        DD a{0., 0.};
+        for (int b = 0; b < nparts; ++b)
+            a = dd_add(a, DD{amount_parts[((long long)b * G.neta + q) * 2], amount_parts[((long long)b * G.neta + q) * 2 + 1]});
+        amount_out[2 * q] = a.hi;
+        amount_out[2 * q + 1] = a.lo;
+        cells_out[q] = (long long)cells[q];
+    }
+    if (threadIdx.x == 0) {
+        GrainPart r = parts[0];
+        for (int b = 1; b < nparts; ++b) {
+            for (int q = 0; q < 3; ++q) {
+                DD s = dd_add(DD{r.sum[q][0], r.sum[q][1]}, DD{parts[b].sum[q][0], parts[b].sum[q][1]});
+                r.sum[q][0] = s.hi; r.sum[q][1] = s.lo;
+            }
+            r.lo = ext_min(r.lo, parts[b].lo); r.hi = ext_max(r.hi, parts[b].hi);
+            r.slo = ext_min(r.slo, parts[b].slo); r.shi = ext_max(r.shi, parts[b].shi);
+            r.gbmax = ext_max(r.gbmax, parts[b].gbmax);
+            r.unassigned += parts[b].unassigned;
+        }
+        out->lo = r.lo.v; out->hi = r.hi.v; out->slo = r.slo.v; out->shi = r.shi.v; out->gbmax = r.gbmax.v;
+        for (int q = 0; q < 3; ++q) { out->sum[q][0] = r.sum[q][0]; out->sum[q][1] = r.sum[q][1]; }
+        out->unassigned = r.unassigned;
+    }
+}
+
 int grid_for(long long n, int threads, int cap) {
     const long long want = (n + threads - 1) / threads;
     return (int)(want < cap ? (want > 0 ? want : 1) : cap);
@@ -291,6 +429,18 @@ void launch_center_seed(const InitParams& I, double cx, double cy, double cz, do
 void launch_reduce_partials(const StepPartial* partials, int nblocks, StepPartial* out, cudaStream_t stream) {
     k_reduce_partials<<<1, 256, 0, stream>>>(partials, nblocks, out);
 }
+void launch_grain_stats(const GrainParams& G, const double* eta, const double* s2, const double* p, const double* gb,
+                        GrainWork& W, GrainOut* out, double* amount_out, long long* cells_out, cudaStream_t stream) {
+    const int nb = grid_for(G.g.ncells, 256, 148 * 2);
+    cudaMemsetAsync(W.cells, 0, (size_t)G.neta * sizeof(unsigned long long), stream);
+    k_grain_scalar<<<nb, 256, 0, stream>>>(G, eta, s2, p, gb, W.cells, reinterpret_cast<GrainPart*>(W.parts));
+    k_grain_amount<<<dim3(nb, G.neta), 256, 0, stream>>>(G, eta, s2, p, W.amount_parts);
+    k_grain_finalize<<<1, 256, 0, stream>>>(G, reinterpret_cast<const GrainPart*>(W.parts), nb, W.amount_parts, W.cells,
+                                           out, amount_out, cells_out);
+}
+size_t grain_part_bytes() { return sizeof(GrainPart); }
+int grain_blocks(long long ncells) { return grid_for(ncells, 256, 148 * 2); }
+
 void launch_diagnostics(const Grid& g, const double* o, const double* cr, const double* p, DiagOut* partials,
                         int* nblocks, DiagOut* out, cudaStream_t stream) {
     const int nb = grid_for(g.ncells, 256, 148 * 4);

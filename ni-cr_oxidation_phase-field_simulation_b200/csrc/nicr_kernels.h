@@ -125,6 +125,29 @@ struct DiagOut {
     double mn[4], mx[4];   // O, Cr, Ni(=1-o-cr, min only), phi
     long long mni[4], mxi[4];  // first cell (reference order) attaining each extremum
 };
+// grain_log statistics (3S:566-590): scalars, per-grain dominant cells and
+// weighted amounts, and the discrete grain energy (3S:546-565)
+struct GrainParams {
+    Grid g;
+    int dim, neta;
+    double dx, da, db, K, W, A;
+    const double* pairs;   // 2D: eta_pairs of the last mask (2D:337); unused in 3D
+};
+struct GrainOut {
+    double lo, hi, slo, shi, gbmax;
+    double sum[3][2];      // S, (1-h) gb, energy
+    long long unassigned;
+};
+struct GrainWork {
+    unsigned long long* cells;  // neta
+    void* parts;                // grain_blocks() * grain_part_bytes()
+    double* amount_parts;       // grain_blocks() * neta * 2
+};
+size_t grain_part_bytes();
+int grain_blocks(long long ncells);
+void launch_grain_stats(const GrainParams& G, const double* eta, const double* s2, const double* p, const double* gb,
+                        GrainWork& W, GrainOut* out, double* amount_out, long long* cells_out, cudaStream_t stream);
+
 void launch_diagnostics(const Grid& g, const double* o, const double* cr, const double* p,
                         DiagOut* partials, int* nblocks, DiagOut* out, cudaStream_t stream);
 

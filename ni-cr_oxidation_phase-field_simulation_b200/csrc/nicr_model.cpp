@@ -171,7 +171,8 @@ void Model::release() {
                       grain, pairs, gb_initial, muO, muCr, mo, mc};
     for (double* b : bufs) if (b) cudaFree(b);
     void* others[] = {partials, st, bud, diag_part, diag_out, red_out, kres, d_shadow, d_ball, d_hyp,
-                      kw.flag, kw.blocked, kw.counts, kw.list, kw.total};
+                      kw.flag, kw.blocked, kw.counts, kw.list, kw.total, gw.cells, gw.parts, gw.amount_parts,
+                      g_out, g_amount, g_cells};
     for (void* b : others) if (b) cudaFree(b);
     if (h_st) cudaFreeHost(h_st);
     for (cudaEvent_t e : prof_pool) cudaEventDestroy(e);
@@ -182,6 +183,7 @@ void Model::release() {
     grain = pairs = gb_initial = muO = muCr = mo = mc = nullptr;
     partials = nullptr; st = nullptr; bud = nullptr; diag_part = diag_out = nullptr; red_out = nullptr; kres = nullptr;
     d_shadow = d_ball = nullptr; d_hyp = nullptr; kw = KspWork{}; h_st = nullptr; stream = nullptr;
+    gw = GrainWork{}; g_out = nullptr; g_amount = nullptr; g_cells = nullptr;
 }
 
 void Model::sync() { check_cuda(cudaStreamSynchronize(stream), "stream"); }
@@ -799,8 +801,41 @@ void Model::diagnostics(nicr_diagnostics* d) {
     d->min_phi = r.mn[3]; d->max_phi = r.mx[3];
 }
 
-void Model::grain_stats(nicr_grain_stats*, long long*, double*) {
-    throw Error(NICR_ERR_STATE, "grain statistics are not available yet");
+// grain_log values (3S:566-590, 2D:382-406)
+void Model::grain_stats(nicr_grain_stats* out, long long* cells, double* amount) {
+    if (!has_eta) throw Error(NICR_ERR_STATE, "grain statistics exist only with evolving grains");
+    if (eta_dirty || dim == 2) eta_mask_now();
+    if (!gw.cells) {
+        gw.cells = dalloc_t<unsigned long long>((size_t)neta);
+        gw.parts = dalloc_t<unsigned char>((size_t)grain_blocks(g.ncells) * grain_part_bytes());
+        gw.amount_parts = dalloc((size_t)grain_blocks(g.ncells) * neta * 2);
+        g_out = dalloc_t<GrainOut>(1);
+        g_amount = dalloc((size_t)neta * 2);
+        g_cells = dalloc_t<long long>((size_t)neta);
+    }
+    GrainParams G{};
+    G.g = g; G.dim = dim; G.neta = neta;
+    G.dx = c.dx; G.da = c.dy; G.db = dim == 3 ? c.dz : c.dy;
+    G.K = ec.K; G.W = c.eta_W; G.A = ec.A;
+    G.pairs = pairs;
+    launch_grain_stats(G, eta_[ecur], s2_[gcur], p_[cur], gb_[gcur], gw, g_out, g_amount, g_cells, stream);
+    GrainOut r;
+    check_cuda(cudaMemcpyAsync(&r, g_out, sizeof r, cudaMemcpyDeviceToHost, stream), "D2H");
+    if (cells) check_cuda(cudaMemcpyAsync(cells, g_cells, (size_t)neta * sizeof(long long), cudaMemcpyDeviceToHost, stream), "D2H");
+    if (amount) check_cuda(cudaMemcpyAsync(amount, g_amount, (size_t)neta * 2 * sizeof(double), cudaMemcpyDeviceToHost, stream), "D2H");
+    sync();
+    check_cuda(cudaGetLastError(), "grain statistics");
+    out->min_eta = r.lo; out->max_eta = r.hi; out->min_s2 = r.slo; out->max_s2 = r.shi;
+    out->sum_s2[0] = r.sum[0][0]; out->sum_s2[1] = r.sum[0][1];
+    out->mask[0] = r.sum[1][0]; out->mask[1] = r.sum[1][1];
+    out->energy[0] = r.sum[2][0]; out->energy[1] = r.sum[2][1];
+    out->gb_max = r.gbmax;
+    out->unassigned = r.unassigned;
+    long long alive = 0;
+    std::vector<long long> cc((size_t)neta);
+    check_cuda(cudaMemcpy(cc.data(), g_cells, (size_t)neta * sizeof(long long), cudaMemcpyDeviceToHost), "D2H");
+    for (long long v : cc) alive += v > 0;
+    out->alive = alive;
 }
 
 // ------------------------------------------------------------------ measurement hooks

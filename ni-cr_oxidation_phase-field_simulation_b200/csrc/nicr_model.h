@@ -23,6 +23,7 @@ struct Error : std::runtime_error {
 };
 
 void check_cuda(cudaError_t e, const char* what);
+int run_self_test(int dim);   // --self-test (nicr_selftest.cpp)
 
 class Model {
 public:
@@ -81,6 +82,13 @@ public:
     double* d_gb() const { return gb_[gcur]; }
     double* d_eta(int gi) const { return eta_[ecur] + (size_t)gi * g.nstore; }
     StepParams params() const { return sp; }
+    // device buffers the writers read (after refresh())
+    const double* d_mu_o() const { return muO; }
+    const double* d_mu_cr() const { return muCr; }
+    const double* d_m_o() const { return mo; }
+    const double* d_m_cr() const { return mc; }
+    void fetch(const double* d, double* host) { copy_out(d, host); }
+    void ensure_mask() { if (has_eta && (eta_dirty || dim == 2)) eta_mask_now(); }
 
 private:
     StepParams sp{};
@@ -115,6 +123,11 @@ private:
     int* d_shadow = nullptr;
     int* d_ball = nullptr;
     unsigned char* d_hyp = nullptr;
+    // grain statistics work buffers (allocated on first use)
+    GrainWork gw{};
+    GrainOut* g_out = nullptr;
+    double* g_amount = nullptr;
+    long long* g_cells = nullptr;
     // pinned host staging for small results
     Status* h_st = nullptr;
     // profiling
@@ -144,3 +157,9 @@ private:
 };
 
 }  // namespace nicr
+
+// The opaque handle of include/nicr.h: one model and its last error message.
+struct nicr_handle {
+    nicr::Model* m = nullptr;
+    std::string err;
+};

@@ -1,10 +1,661 @@
-// Output writers (placeholder until the writers land).
+// Output files and the solver program (host C++ over device data).
+//   VTK legacy ASCII (2D:598-632, 3S:828-856), compressed VTI (3S:238-334,
+//   3S:857-869), diagnostics.csv rows (2D:697-710, 3S:963-977), grain CSV rows
+//   (2D:382-406, 3S:566-590), parameters.txt and grains.csv (2D:633-696,
+//   3S:874-962), and run()/main() (2D:1161-1254, 3S:1309-1403).
+// Formats (array names, column order, iostream precision 16/17, X-fastest
+// order, the VTI block layout) follow the reference so that files written
+// from bit-identical fields are byte-identical.
+#include <zlib.h>
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <filesystem>
+#include <fstream>
+#include <functional>
+#include <iomanip>
+#include <iostream>
+#include <limits>
+#include <locale>
+#include <sstream>
+#include <string>
+#include <vector>
+
 #include "../../include/nicr.h"
-extern "C" {
-int nicr_write_vtk(nicr_handle*, const char*) { return NICR_ERR_STATE; }
-int nicr_write_vti(nicr_handle*, const char*) { return NICR_ERR_STATE; }
-int nicr_write_metadata(nicr_handle*, const char*) { return NICR_ERR_STATE; }
-int nicr_format_log_row(nicr_handle*, int, char*, size_t) { return NICR_ERR_STATE; }
-int nicr_format_grain_rows(nicr_handle*, int, char*, size_t, char*, size_t) { return NICR_ERR_STATE; }
-int nicr_main(int, int, const char* const*) { return 1; }
+#include "nicr_model.h"
+
+
+namespace fs = std::filesystem;
+
+namespace {
+
+using nicr::Model;
+
+constexpr const char* VERSION2 = "mpi-eta-v1";
+constexpr const char* VERSION3 = "mpi-eta-3d-xslab-optimized-v1";
+
+long double ld(const double v[2]) { return (long double)v[0] + (long double)v[1]; }
+
+// Host copies of the fields an output needs, in reference interior order.
+struct Snapshot {
+    const Model& m;
+    long long n;
+    std::vector<double> o, cr, p, gb, grain, muO, muCr, mo, mc, s2, pairs, gb_initial;
+    std::vector<std::vector<double>> eta;
+    explicit Snapshot(Model& mm, bool mu_m = true) : m(mm), n(mm.g.ncells) {
+        mm.refresh();
+        mm.ensure_mask();
+        auto get = [&](int f, int idx, std::vector<double>& v) {
+            v.resize((size_t)n);
+            mm.get_field(f, idx, v.data());
+        };
+        get(NICR_FIELD_O, 0, o);
+        get(NICR_FIELD_CR, 0, cr);
+        get(NICR_FIELD_PHI, 0, p);
+        get(NICR_FIELD_GB, 0, gb);
+        if (mm.grain_retained) get(NICR_FIELD_GRAIN, 0, grain);
+        if (mu_m) {
+            muO.resize((size_t)n); muCr.resize((size_t)n); mo.resize((size_t)n); mc.resize((size_t)n);
+            mm.fetch(mm.d_mu_o(), muO.data());
+            mm.fetch(mm.d_mu_cr(), muCr.data());
+            mm.fetch(mm.d_m_o(), mo.data());
+            mm.fetch(mm.d_m_cr(), mc.data());
+        }
+        if (mm.has_eta) {
+            get(NICR_FIELD_ETA_S2, 0, s2);
+            eta.resize((size_t)mm.neta);
+            for (int g = 0; g < mm.neta; ++g) get(NICR_FIELD_ETA, g, eta[(size_t)g]);
+            if (mm.dim == 2) {
+                get(NICR_FIELD_ETA_PAIRS, 0, pairs);
+                get(NICR_FIELD_GB_INITIAL, 0, gb_initial);
+            }
+        } else if (mm.dim == 2) {
+            get(NICR_FIELD_GB_INITIAL, 0, gb_initial);
+        }
+    }
+    // current_grain (3S:527-533, 2D:360-366)
+    int current_grain(long long q) const {
+        if (p[q] >= .5) return 0;
+        if (!m.has_eta) return int(grain[q]);
+        double best = 1.e-12;
+        int id = 0;
+        for (size_t g = 0; g < eta.size(); ++g)
+            if (eta[g][q] > best) { best = eta[g][q]; id = int(g) + 1; }
+        return id;
+    }
+    // grain_sum (3S:534-545)
+    double grain_sum(long long q) const {
+        if (m.has_eta) {
+            double value = 0.;
+            for (size_t g = 0; g < eta.size(); ++g) value += double(g + 1) * eta[g][q];
+            return value;
+        }
+        return grain[q] * (1. - nicr::h(p[q]));
+    }
+};
+
+// ------------------------------------------------------------------ VTK
+void write_vtk2(Model& m, const std::string& path) {
+    Snapshot s(m);
+    const auto& c = m.c;
+    std::ofstream f(path);
+    if (!f) throw nicr::Error(NICR_ERR_IO, "Cannot write " + path);
+    f << std::setprecision(16) << "# vtk DataFile Version 3.0\n"
+      << (m.has_eta ? "NiCr evolving metal grains; coordinates in metres\n" : "NiCr fixed-grain prototype; coordinates in metres\n")
+      << "ASCII\nDATASET STRUCTURED_POINTS\n"
+      << "DIMENSIONS " << c.nx << " " << c.ny << " 1\nORIGIN " << .5 * c.dx << " " << .5 * c.dy << " 0\nSPACING " << c.dx
+      << " " << c.dy << " 1\nPOINT_DATA " << c.nx * c.ny << "\n";
+    auto write = [&](const std::string& name, const std::function<double(long long)>& fn) {
+        f << "SCALARS " << name << " double 1\nLOOKUP_TABLE default\n";
+        for (int j = 1; j <= c.ny; ++j) {
+            for (int i = 1; i <= c.nx; ++i) f << fn((long long)(i - 1) * c.ny + (j - 1)) << " ";
+            f << "\n";
+        }
+    };
+    write("phi", [&](long long q) { return s.p[q]; });
+    write("conc_O", [&](long long q) { return s.o[q]; });
+    write("conc_Cr", [&](long long q) { return s.cr[q]; });
+    write("conc_Ni", [&](long long q) { return 1. - s.o[q] - s.cr[q]; });
+    write("grain_id", [&](long long q) { return m.has_eta ? double(s.current_grain(q)) : s.grain[q]; });
+    write("GB_mask", [&](long long q) { return s.gb[q]; });
+    write("GB_active", [&](long long q) { return (1. - nicr::h(s.p[q])) * s.gb[q]; });
+    write("mu_O", [&](long long q) { return s.muO[q]; });
+    write("mu_Cr", [&](long long q) { return s.muCr[q]; });
+    write("M_O", [&](long long q) { return s.mo[q]; });
+    write("M_Cr", [&](long long q) { return s.mc[q]; });
+    if (m.has_eta) {
+        write("grain_id_initial", [&](long long q) { return s.grain[q]; });
+        write("GB_initial", [&](long long q) { return s.gb_initial[q]; });
+        write("GB_eta_indicator", [&](long long q) { return std::min(1., 16. * s.pairs[q]); });
+        write("metal_fraction", [&](long long q) { return 1. - nicr::h(s.p[q]); });
+        write("eta_sum_sq", [&](long long q) { return s.s2[q]; });
+        write("active_grain_id", [&](long long q) { return double(s.current_grain(q)); });
+        if (c.eta_output_all)
+            for (size_t g = 0; g < s.eta.size(); ++g)
+                write("eta_" + std::to_string(g + 1), [&](long long q) { return s.eta[g][q]; });
+    }
+    if (!f) throw nicr::Error(NICR_ERR_IO, "Output write failed: " + path);
 }
+
+// X-fastest traversal of a 3D domain stored X-slowest
+template <class Fn>
+void for_x_fastest(const nicr_config& c, Fn fn) {
+    for (int k = 1; k <= c.nz; ++k)
+        for (int j = 1; j <= c.ny; ++j)
+            for (int i = 1; i <= c.nx; ++i) fn(((long long)(i - 1) * c.ny + (j - 1)) * c.nz + (k - 1), i == c.nx);
+}
+
+std::array<std::function<double(long long)>, 7> arrays3(const Snapshot& s) {
+    return {[&](long long q) { return s.p[q]; }, [&](long long q) { return s.o[q]; },
+            [&](long long q) { return s.cr[q]; }, [&](long long q) { return s.muO[q]; },
+            [&](long long q) { return s.muCr[q]; }, [&](long long q) { return s.grain_sum(q); },
+            [&](long long q) { return s.gb[q]; }};
+}
+constexpr std::array<const char*, 7> NAMES3 = {"phi", "conc_O", "conc_Cr", "mu_O", "mu_Cr", "grain_sum", "GB_mask"};
+
+void write_vtk3(Model& m, const std::string& path) {
+    Snapshot s(m);
+    const auto& c = m.c;
+    std::ofstream f(path);
+    if (!f) throw nicr::Error(NICR_ERR_IO, "Cannot write " + path);
+    f << std::setprecision(17) << "# vtk DataFile Version 3.0\nNiCr 3D oxidation and metal grains; metres\n"
+      << "ASCII\nDATASET STRUCTURED_POINTS\nDIMENSIONS " << c.nx << " " << c.ny << " " << c.nz << "\nORIGIN "
+      << .5 * c.dx << " " << .5 * c.dy << " " << .5 * c.dz << "\nSPACING " << c.dx << " " << c.dy << " " << c.dz
+      << "\nPOINT_DATA " << c.nx * c.ny * c.nz << "\n";
+    const auto fns = arrays3(s);
+    for (size_t a = 0; a < NAMES3.size(); ++a) {
+        f << "SCALARS " << NAMES3[a] << " double 1\nLOOKUP_TABLE default\n";
+        for_x_fastest(c, [&](long long q, bool last) {
+            f << fns[a](q) << " ";
+            if (last) f << "\n";
+        });
+    }
+    if (!f) throw nicr::Error(NICR_ERR_IO, "Output write failed: " + path);
+}
+
+// ------------------------------------------------------------------ VTI
+// VTK XML ImageData, raw appended data, zlib blocks of 64 KiB with UInt64
+// headers (block count, block size, last block size, compressed sizes),
+// written to path.tmp and renamed on success.
+class VtiFile {
+    static constexpr std::uint64_t kBlock = 65536;
+    const nicr_config& c;
+    std::string final_path, temp_path;
+    std::ofstream f;
+    std::array<std::streampos, 7> offset_pos{};
+    std::streampos data_start;
+    size_t next = 0;
+    bool done = false;
+    void check() {
+        if (!f) throw nicr::Error(NICR_ERR_IO, "VTI write failed (check storage/quota): " + temp_path);
+    }
+    void u64(std::uint64_t v) {
+        unsigned char b[8];
+        for (int q = 0; q < 8; ++q) b[q] = (unsigned char)(v >> (8 * q));
+        f.write(reinterpret_cast<const char*>(b), 8);
+    }
+
+public:
+    VtiFile(const std::string& path, const nicr_config& cfg) : c(cfg), final_path(path), temp_path(path + ".tmp") {
+        f.open(temp_path, std::ios::binary | std::ios::trunc);
+        if (!f) throw nicr::Error(NICR_ERR_IO, "Cannot open " + temp_path);
+        f.imbue(std::locale::classic());
+        f << std::setprecision(17) << "<?xml version=\"1.0\"?>\n"
+          << "<VTKFile type=\"ImageData\" version=\"1.0\" byte_order=\"LittleEndian\" header_type=\"UInt64\" compressor=\"vtkZLibDataCompressor\">\n"
+          << " <ImageData WholeExtent=\"0 " << c.nx - 1 << " 0 " << c.ny - 1 << " 0 " << c.nz - 1 << "\" Origin=\""
+          << .5 * c.dx << " " << .5 * c.dy << " " << .5 * c.dz << "\" Spacing=\"" << c.dx << " " << c.dy << " " << c.dz
+          << "\">\n  <Piece Extent=\"0 " << c.nx - 1 << " 0 " << c.ny - 1 << " 0 " << c.nz - 1 << "\">\n"
+          << "   <PointData Scalars=\"phi\">\n";
+        for (size_t a = 0; a < NAMES3.size(); ++a) {
+            f << "    <DataArray type=\"" << (c.output_float64 ? "Float64" : "Float32") << "\" Name=\"" << NAMES3[a]
+              << "\" NumberOfComponents=\"1\" format=\"appended\" offset=\"";
+            offset_pos[a] = f.tellp();
+            f << "00000000000000000000\"/>\n";
+        }
+        f << "   </PointData>\n   <CellData/>\n  </Piece>\n </ImageData>\n <AppendedData encoding=\"raw\">\n_";
+        data_start = f.tellp();
+        check();
+    }
+    ~VtiFile() {
+        if (!done) {
+            f.close();
+            std::error_code ec;
+            fs::remove(temp_path, ec);
+        }
+    }
+    template <class T>
+    void array(const std::function<double(long long)>& value) {
+        const auto start = f.tellp();
+        const auto offset = static_cast<std::uint64_t>(start - data_start);
+        f.seekp(offset_pos[next]);
+        f << std::setw(20) << std::setfill('0') << offset << std::setfill(' ');
+        f.seekp(start);
+        check();
+        const std::uint64_t n = std::uint64_t(c.nx) * c.ny * c.nz, total = n * sizeof(T);
+        const std::uint64_t nb = (total + kBlock - 1) / kBlock;
+        const auto header = f.tellp();
+        std::vector<std::uint64_t> sizes((size_t)nb, 0);
+        u64(nb); u64(kBlock); u64(total % kBlock);
+        for (std::uint64_t b = 0; b < nb; ++b) u64(0);
+        std::vector<T> buf((size_t)(kBlock / sizeof(T)));
+        std::vector<unsigned char> packed((size_t)compressBound(kBlock));
+        size_t used = 0, block = 0;
+        auto flush = [&] {
+            if (!used) return;
+            uLongf dest = (uLongf)packed.size();
+            const int rc = compress2(packed.data(), &dest, reinterpret_cast<const Bytef*>(buf.data()),
+                                     (uLong)(used * sizeof(T)), c.compression_level);
+            if (rc != Z_OK) throw nicr::Error(NICR_ERR_IO, "zlib compression failed: " + std::to_string(rc));
+            sizes.at(block++) = dest;
+            f.write(reinterpret_cast<const char*>(packed.data()), (std::streamsize)dest);
+            check();
+            used = 0;
+        };
+        for_x_fastest(c, [&](long long q, bool) {
+            const double v = value(q);
+            if (std::isfinite(v) && std::abs(v) > std::numeric_limits<T>::max())
+                throw nicr::Error(NICR_ERR_IO, std::string("VTI ") + NAMES3[next] +
+                                                   " exceeds output type range; use --output-precision float64.");
+            buf[used++] = static_cast<T>(v);
+            if (used == buf.size()) flush();
+        });
+        flush();
+        if (block != sizes.size()) throw nicr::Error(NICR_ERR_IO, "Internal VTI block-count mismatch.");
+        const auto end = f.tellp();
+        f.seekp(header + std::streamoff(24));
+        for (auto v : sizes) u64(v);
+        f.seekp(end);
+        check();
+        ++next;
+    }
+    void finish() {
+        if (next != NAMES3.size()) throw nicr::Error(NICR_ERR_IO, "Missing VTI arrays.");
+        f << "\n </AppendedData>\n</VTKFile>\n";
+        f.flush();
+        check();
+        f.close();
+        check();
+        fs::rename(temp_path, final_path);
+        done = true;
+    }
+};
+
+void write_vti3(Model& m, const std::string& path) {
+    Snapshot s(m);
+    VtiFile w(path, m.c);
+    for (const auto& fn : arrays3(s)) {
+        if (m.c.output_float64) w.array<double>(fn);
+        else w.array<float>(fn);
+    }
+    w.finish();
+}
+
+void write_visualization(Model& m, const std::string& stem) {
+    if (m.dim == 2) write_vtk2(m, stem + ".vtk");
+    else if (m.c.output_vti) write_vti3(m, stem + ".vti");
+    else write_vtk3(m, stem + ".vtk");
+}
+
+// ------------------------------------------------------------------ CSV rows
+std::string log_row(Model& m, int n) {
+    nicr_diagnostics d;
+    m.diagnostics(&d);
+    nicr_budget b;
+    m.budget(&b);
+    const auto& c = m.c;
+    const long double so = ld(d.sum_O), sc = ld(d.sum_Cr), po = ld(d.sum_phi), sumH = ld(d.sum_h);
+    const long double ro = so - ld(b.initialO) - ld(b.bcO) - ld(b.nucO) - ld(b.ckO) - ld(b.clipO);
+    const long double rc = sc - ld(b.initialCr) - ld(b.bcCr) - ld(b.nucCr) - ld(b.ckCr) - ld(b.clipCr);
+    const int cells = m.dim == 3 ? c.nx * c.ny * c.nz : c.nx * c.ny;
+    std::ostringstream f;
+    f << std::setprecision(17) << n << "," << n * c.dt << "," << so << "," << sc << "," << po / cells << ","
+      << ld(b.bcO) << "," << ld(b.nucO) << "," << ld(b.nucCr) << "," << ld(b.ckO) << "," << ld(b.ckCr) << ","
+      << ld(b.clipO) << "," << ld(b.clipCr) << "," << ro << "," << rc << "," << b.nuclei << "," << b.clipped << ","
+      << d.min_O << "," << d.max_O << "," << d.min_Cr << "," << d.max_Cr << "," << d.min_Ni << "," << d.min_phi << ","
+      << d.max_phi;
+    if (m.dim == 3) f << "," << sumH / cells << "," << sumH * c.dx * c.dy * c.dz;
+    f << "\n";
+    return f.str();
+}
+
+void grain_rows(Model& m, int n, std::string& diag, std::string& history) {
+    diag.clear();
+    history.clear();
+    if (!m.has_eta) return;
+    nicr_grain_stats s;
+    std::vector<long long> cells((size_t)m.neta);
+    std::vector<double> amount((size_t)m.neta * 2);
+    m.grain_stats(&s, cells.data(), amount.data());
+    const auto& c = m.c;
+    const int ncell = m.dim == 3 ? c.nx * c.ny * c.nz : c.nx * c.ny;
+    const long double vol = m.dim == 3 ? (long double)1 : 1;
+    (void)vol;
+    std::ostringstream f, h;
+    f << std::setprecision(17) << n << "," << n * c.dt << "," << s.min_eta << "," << s.max_eta << "," << s.min_s2 << ","
+      << s.max_s2 << "," << ld(s.sum_s2) / ncell << "," << s.alive << "," << s.unassigned << ",";
+    if (m.dim == 3) f << ld(s.mask) * c.dx * c.dy * c.dz;
+    else f << ld(s.mask) * c.dx * c.dy;
+    f << "," << s.gb_max << "," << ld(s.energy) << "\n";
+    for (int g = 0; g < m.neta; ++g) {
+        const long double a = (long double)amount[2 * g] + (long double)amount[2 * g + 1];
+        h << std::setprecision(17) << n << "," << n * c.dt << "," << g + 1 << "," << cells[(size_t)g] << "," << a << ",";
+        if (m.dim == 3) h << a * c.dx * c.dy * c.dz;
+        else h << a * c.dx * c.dy;
+        h << "\n";
+    }
+    diag = f.str();
+    history = h.str();
+}
+
+// ------------------------------------------------------------------ metadata
+void metadata(Model& m, const std::string& out) {
+    const auto& c = m.c;
+    const nicr::EtaCoef ec = m.ec;
+    const double pi = nicr::PI;
+    const std::string backend = "execution_backend=cuda_sm100a_single_gpu\n";
+    std::ofstream f(out + "/parameters.txt");
+    auto onoff = [](bool b) { return b ? "on" : "off"; };
+    const char* bc = c.bc == NICR_BC_MU ? "mu" : c.bc == NICR_BC_CLOSED ? "closed" : "concentration";
+    const char* ck = c.ck == NICR_CK_OFF ? "off" : "legacy";
+    const char* bounds = c.bounds == NICR_BOUNDS_LEGACY ? "legacy" : "stop";
+    const char* nuc = c.nucleation == NICR_NUC_CENTER ? "center" : c.nucleation == NICR_NUC_OFF ? "off" : "ksp";
+    const std::string eta_output = c.eta_output_all ? "all" : "summary";
+    if (m.dim == 2) {
+        f << std::setprecision(17)
+          << (m.has_eta ? "STATUS: COUPLED ETA/OXIDATION MODEL; GRAIN PARAMETERS REQUIRE CALIBRATION\n"
+                        : "STATUS: UNCALIBRATED FIXED-GRAIN TRANSPORT PROTOTYPE\n")
+          << "nx=" << c.nx << "\nny=" << c.ny << "\ndx_m=" << c.dx << "\ndy_m=" << c.dy << "\ndt_s=" << c.dt
+          << "\nsteps=" << c.steps << "\noxygen_bc=" << bc << "\nCk=" << ck << "\nbounds=" << bounds
+          << "\nmpi_processes=1\nmpi_decomposition=X slabs"
+          << "\nversion=" << VERSION2 << "\nnucleation_mode=" << nuc
+          << "\ninitial_center_seed_cells=" << m.center_seed_cells << "\ngrain_structure=" << onoff(c.grains)
+          << "\noxygen_diffusion=" << onoff(c.oxygen_diffusion)
+          << "\noxygen_boundary_supply=" << (c.oxygen_diffusion ? bc : "disabled") << "\nW=" << nicr::Phys::W
+          << "\nkappa_phi=" << nicr::Phys::kp << "\nL_phi=" << nicr::Phys::L << "\nmu_res_model_units=" << c.mu_res
+          << "\nsurface_mobility_concentration_reference=" << c.surface_c_ref
+          << "\nleft_edge_sites_requested=" << c.left_edge_sites
+          << "\nleft_edge_sites_active=" << (c.grains ? c.left_edge_sites : 0)
+          << "\ngrain_diameter_target_grid=" << c.grain_diameter_grid
+          << "\ngrain_diameter_target_m=" << c.grain_diameter_grid * c.dx << "\nvoronoi_sites=" << m.seeds.size() / 2
+          << "\ngb_mask_FWHM_grid=" << c.gb_fwhm_grid << "\ngb_mask_FWHM_m=" << c.gb_fwhm_grid * c.dx
+          << "\ngb_mask_integral_effective_width_grid=" << c.gb_fwhm_grid * std::sqrt(pi) / (2. * std::sqrt(std::log(2.)))
+          << "\ngb_mask_integral_effective_width_m=" << c.gb_fwhm_grid * c.dx * std::sqrt(pi) / (2. * std::sqrt(std::log(2.)))
+          << "\ngb_peak_mobility_factor_O=" << c.gb_factor_o << "\ngb_peak_mobility_factor_Cr=" << c.gb_factor_cr
+          << "\nrandom_seed=" << c.random_seed << "\nnucleus_geometric_radius_grid=" << c.radius_grid
+          << "\nnucleus_geometric_radius_m=" << c.radius_grid * c.dx << "\nnucleation_period_s=" << c.nucleation_period
+          << "\nNOTE: Vm=1 is retained, not evidence that energy/mobility units have been physically audited.\n"
+          << "NOTE: no GB migration, GB energy, segregation, oxide GBs, or interphase enhancement.\n"
+          << "NOTE: cell-centred grid; periodic Y; no-flux right; natural concentration/phi derivatives in X.\n";
+        f << backend;
+        f << "grain_evolution_requested=" << onoff(c.grain_evolution) << "\ngrain_evolution_active=" << onoff(m.has_eta) << "\n";
+        if (m.has_eta) {
+            f << "eta_fields=" << m.neta << "\neta_W=" << c.eta_W << "\neta_kappa=" << ec.K << "\neta_L=" << c.eta_L
+              << "\neta_oxide_penalty=" << ec.A << "\neta_width_10_90_grid=" << 2. * std::log(9.) * ec.ell / c.dx
+              << "\neta_mask_integrated_width_m=" << 8. * ec.ell / 3. << "\neta_transport_scale=" << ec.scale
+              << "\neta_planar_GB_energy_model_units=" << std::sqrt(2. * ec.K * c.eta_W) / 3.
+              << "\neta_planar_geometric_mobility_model_units=" << 3. * c.eta_L * ec.ell << "\neta_output=" << eta_output
+              << "\nNOTE: New grain coefficients are provisional, not experimental Ni-Cr calibration.\n"
+              << "NOTE: Dynamic eta modifies the GB pathways AND adds the reciprocal grain-energy force to phi.\n"
+              << "NOTE: GB factors refer to the original integrated-width convention; GB_mask includes eta_transport_scale.\n";
+        } else
+            f << "NOTE: fixed initial grain map and Gaussian GB mask.\n";
+        if (c.nucleation == NICR_NUC_CENTER)
+            f << "initial_oxide_center_x_m=" << 0.5 * c.nx * c.dx << "\ninitial_oxide_center_y_m=" << 0.5 * c.ny * c.dy
+              << "\ninitial_oxide_center_i=" << 0.5 * (double(c.nx) + 1.) << "\ninitial_oxide_center_j="
+              << 0.5 * (double(c.ny) + 1.)
+              << "\nNOTE: one initial hard oxide only; no later Ksp insertion or replacement seed.\n";
+        if (!c.grains) f << "NOTE: single grain; grain_id=1 and GB_mask=0; configured GB factors are inactive.\n";
+        if (!c.oxygen_diffusion)
+            f << "NOTE: O transport and continuing O boundary supply are off; initial inventory, hard seed assignments, optional Ck and bounds treatment remain.\n";
+        std::ofstream g(out + "/grains.csv");
+        g << "grain_id,seed_x_grid,seed_y_grid,area_cells,equivalent_diameter_grid,equivalent_diameter_m\n";
+        long double mean = 0;
+        const size_t ng = m.volumes.size();
+        for (size_t k = 0; k < ng; ++k) {
+            const double d = 2. * std::sqrt(m.volumes[k] / pi);
+            mean += d;
+            g << std::setprecision(17) << k + 1 << "," << m.seeds[2 * k] << "," << m.seeds[2 * k + 1] << ","
+              << m.volumes[k] << "," << d << "," << d * c.dx << "\n";
+        }
+        mean /= ng;
+        f << "measured_arithmetic_mean_equivalent_diameter_grid=" << mean << "\n";
+        if (!f || !g) throw nicr::Error(NICR_ERR_IO, "Metadata write failed.");
+        return;
+    }
+    const std::string fmt = c.output_vti ? "vti" : "vtk";
+    const std::string prec = c.output_float64 ? "float64" : "float32";
+    f << std::setprecision(17) << "model=NiCr_3D_oxidation_metal_grains\nversion=" << VERSION3 << "\nnx=" << c.nx
+      << "\nny=" << c.ny << "\nnz=" << c.nz << "\ndx_m=" << c.dx << "\ndy_m=" << c.dy << "\ndz_m=" << c.dz
+      << "\ndt_s=" << c.dt << "\nsteps=" << c.steps << "\noutput_every=" << c.output_every
+      << "\nvtk_fields=phi,conc_O,conc_Cr,mu_O,mu_Cr,grain_sum,GB_mask"
+      << "\noutput_format=" << fmt
+      << "\noutput_precision=" << (fmt == "vtk" ? std::string("float64_ascii_17digits") : prec)
+      << "\noutput_compression=" << (fmt == "vti" ? "zlib_raw_appended" : "none")
+      << "\ncompression_level=" << c.compression_level << "\nfrozen_eta_cache=" << onoff(c.frozen_eta_cache)
+      << "\nnucleation_search=bounded_periodic_neighborhoods_original_order_and_predicates"
+      << "\nGB_mask_definition="
+      << (!c.grains ? "zero;single_crystal"
+                    : (m.has_eta ? "eta_transport_scale*min(1,16*sum_(a<b) eta_a^2*eta_b^2);no_extra_phi_mask"
+                                 : "exp(-4*ln(2)*distance_to_GB_grid^2/gb_fwhm_grid^2);fixed_Voronoi;zero_when_one_grain;no_extra_phi_mask"))
+      << "\ngrain_sum_definition="
+      << (m.has_eta ? "sum_(g=1..N) g*eta_g;unnormalized;no_extra_phi_mask" : "initial_grain_id*(1-h(phi));fixed_grain_fallback_no_eta_fields")
+      << "\noxygen_bc=" << bc << "\nCk=" << ck << "\nbounds=" << bounds
+      << "\nmpi_processes=1\nmpi_decomposition=X_slabs_YZ_planes"
+      << "\ntransverse_bc=periodic_Y_and_Z\nright_bc=no_flux"
+      << "\nnucleation_mode=" << nuc << "\ninitial_center_seed_cells=" << m.center_seed_cells
+      << "\ngrain_structure=" << onoff(c.grains) << "\ngrain_evolution_requested=" << onoff(c.grain_evolution)
+      << "\ngrain_evolution_active=" << onoff(m.has_eta) << "\noxygen_diffusion=" << onoff(c.oxygen_diffusion)
+      << "\noxygen_boundary_supply=" << (c.oxygen_diffusion ? bc : "disabled")
+      << "\nVm=" << 1. << "\nW=" << nicr::Phys::W << "\nkappa_phi=" << nicr::Phys::kp << "\nL_phi=" << nicr::Phys::L
+      << "\nkappa_O=" << nicr::Phys::ko << "\nkappa_Cr=" << nicr::Phys::kc
+      << "\nmatrix_mobility_prefactor_O=" << nicr::Phys::bmo << "\nmatrix_mobility_prefactor_Cr=" << nicr::Phys::bmc
+      << "\noxide_mobility_prefactor_O=" << nicr::Phys::boo << "\noxide_mobility_prefactor_Cr=" << nicr::Phys::boc
+      << "\nbulk_O=" << nicr::Phys::bulkO << "\nbulk_Cr=" << c.bulk_cr << "\nlayer_O=" << c.layer_o
+      << "\nlayer_Cr=" << nicr::Phys::layerCr << "\noxide_O=" << nicr::Phys::oxideO << "\noxide_Cr=" << nicr::Phys::oxideCr
+      << "\nCk_O=" << nicr::Phys::ckO << "\nCk_Cr=" << nicr::Phys::ckCr << "\nKsp=" << c.ksp
+      << "\nmu_res_model_units=" << c.mu_res << "\nsurface_mobility_concentration_reference=" << c.surface_c_ref
+      << "\nleft_face_sites_requested=" << c.left_edge_sites << "\nleft_face_sites_active=" << (c.grains ? c.left_edge_sites : 0)
+      << "\ngrain_diameter_target_grid=" << c.grain_diameter_grid << "\ngrain_diameter_target_m=" << c.grain_diameter_grid * c.dx
+      << "\ngrain_count_rule=round(6*nx*ny*nz/(pi*d_grid^3)),minimum_1"
+      << "\nvoronoi_sites=" << m.seeds.size() / 3 << "\nrandom_seed=" << c.random_seed
+      << "\ngb_mask_FWHM_grid=" << c.gb_fwhm_grid << "\ngb_mask_FWHM_m=" << c.gb_fwhm_grid * c.dx
+      << "\ngb_mask_integral_effective_width_m=" << nicr::reference_gb_width(c.gb_fwhm_grid, c.dx)
+      << "\ngb_peak_mobility_factor_O=" << c.gb_factor_o << "\ngb_peak_mobility_factor_Cr=" << c.gb_factor_cr
+      << "\nnucleus_shape=sphere\nnucleus_geometric_radius_grid=" << c.radius_grid
+      << "\nnucleus_geometric_radius_m=" << c.radius_grid * c.dx << "\nexclusion_gap_grid=" << c.exclusion_gap_grid
+      << "\nnucleation_period_s=" << c.nucleation_period << "\neta_output=" << eta_output
+      << "\nmax_eta_fields=" << c.max_eta_fields << "\n";
+    f << backend;
+    f << "device_field_storage_MiB=" << m.device_bytes() / (1024. * 1024.)
+      << "\nfield_memory_estimates=device_resident_fields_trial_buffers_and_reduction_scratch\n";
+    if (m.has_eta) {
+        f << "eta_fields=" << m.neta << "\neta_W=" << c.eta_W << "\neta_kappa=" << ec.K << "\neta_L=" << c.eta_L
+          << "\neta_oxide_penalty=" << ec.A << "\neta_width_10_90_grid=" << 2. * std::log(9.) * ec.ell / c.dx
+          << "\neta_mask_integrated_width_m=" << 8. * ec.ell / 3. << "\neta_transport_scale=" << ec.scale
+          << "\neta_planar_GB_energy_model_units=" << std::sqrt(2. * ec.K * c.eta_W) / 3.
+          << "\neta_planar_geometric_mobility_model_units=" << 3. * c.eta_L * ec.ell << "\n";
+    }
+    if (c.nucleation == NICR_NUC_CENTER)
+        f << "initial_oxide_center_x_m=" << 0.5 * c.nx * c.dx << "\ninitial_oxide_center_y_m=" << 0.5 * c.ny * c.dy
+          << "\ninitial_oxide_center_z_m=" << 0.5 * c.nz * c.dz << "\ninitial_oxide_center_i=" << 0.5 * (c.nx + 1.)
+          << "\ninitial_oxide_center_j=" << 0.5 * (c.ny + 1.) << "\ninitial_oxide_center_k=" << 0.5 * (c.nz + 1.) << "\n";
+    f << "mobility_note=prefactors_retained_from_uploaded_18wtpct_setup;local_M_includes_concentration_phase_and_GB_factors\n"
+      << "calibration_note=eta_and_GB_transport_parameters_require_material_calibration\n";
+    std::ofstream g(out + "/grains.csv");
+    g << "grain_id,seed_x_grid,seed_y_grid,seed_z_grid,volume_cells,volume_m3,equivalent_diameter_grid,equivalent_diameter_m\n";
+    long double mean = 0.;
+    for (size_t q = 0; q < m.volumes.size(); ++q) {
+        const double d = std::cbrt(6. * m.volumes[q] / pi);
+        mean += d;
+        g << std::setprecision(17) << q + 1 << "," << m.seeds[3 * q] << "," << m.seeds[3 * q + 1] << "," << m.seeds[3 * q + 2]
+          << "," << m.volumes[q] << "," << m.volumes[q] * c.dx * c.dy * c.dz << "," << d << "," << d * c.dx << "\n";
+    }
+    mean /= m.volumes.size();
+    f << "measured_arithmetic_mean_equivalent_diameter_grid=" << mean << "\n";
+    if (!f || !g) throw nicr::Error(NICR_ERR_IO, "Metadata write failed.");
+}
+
+template <class Fn>
+int guarded(nicr_handle* h, Fn fn) {
+    if (!h || !h->m) return NICR_ERR_INVALID_ARG;
+    try {
+        fn(*h->m);
+        return NICR_OK;
+    } catch (const nicr::Error& e) {
+        h->err = e.what();
+        return e.code;
+    } catch (const std::exception& e) {
+        h->err = e.what();
+        return NICR_ERR_IO;
+    }
+}
+
+void copy_out(char* buf, size_t len, const std::string& s) {
+    if (!buf || !len) return;
+    std::strncpy(buf, s.c_str(), len - 1);
+    buf[len - 1] = 0;
+}
+
+int self_test(int dim) { return nicr::run_self_test(dim); }
+
+// ------------------------------------------------------------------ run()
+int run_program(int dim, int argc, const char* const* argv) {
+    nicr_config c;
+    std::vector<char> out(4096), err(16384);
+    int self = 0;
+    const int rc = nicr_config_parse(&c, dim, argc - 1, argv + 1, out.data(), out.size(), &self, err.data(), err.size());
+    if (rc == 100) {
+        std::cout << err.data();
+        return 0;
+    }
+    if (rc != NICR_OK) {
+        std::cerr << "ERROR: " << err.data() << "\n";
+        return 1;
+    }
+    if (self) return self_test(dim);
+    const std::string dir = out.data();
+    try {
+        if (fs::exists(dir) && !fs::is_empty(dir)) throw std::runtime_error("Output directory is not empty; choose a new --out.");
+        fs::create_directories(dir);
+        Model m(c);
+        metadata(m, dir);
+        std::ofstream log(dir + "/diagnostics.csv"), gd, gh;
+        if (!log) throw std::runtime_error("Cannot open diagnostics.csv");
+        log << "step,time_s,sum_O,sum_Cr,mean_phi,O_boundary,O_seed,Cr_seed,O_Ck,Cr_Ck,O_clipping,Cr_clipping,"
+               "O_budget_residual,Cr_budget_residual,nuclei,clipped_cells,min_O,max_O,min_Cr,max_Cr,min_Ni,min_phi,max_phi"
+            << (dim == 3 ? ",mean_h_phi,oxide_volume_m3" : "") << "\n";
+        if (m.has_eta) {
+            gd.open(dir + "/grain_diagnostics.csv");
+            gh.open(dir + "/grain_history.csv");
+            if (!gd || !gh) throw std::runtime_error("Cannot open grain diagnostics.");
+            gd << "step,time_s,min_eta,max_eta,min_sum_eta2,max_sum_eta2,mean_sum_eta2,grains_with_metal_cells,"
+                  "unassigned_metal_cells,"
+               << (dim == 3 ? "integrated_active_GB_m3,max_GB_mask,grain_energy_model_units\n"
+                            : "integrated_active_GB_m2,max_GB_mask,grain_energy_per_depth\n");
+            gh << "step,time_s,grain_id,dominant_metal_cells,"
+               << (dim == 3 ? "weighted_metal_volume_cells,weighted_metal_volume_m3\n"
+                            : "weighted_metal_area_cells,weighted_metal_area_m2\n");
+        }
+        auto do_log = [&](int n) {
+            log << log_row(m, n);
+            if (m.has_eta) {
+                std::string a, b;
+                grain_rows(m, n, a, b);
+                gd << a;
+                gh << b;
+            }
+        };
+        do_log(0);
+        write_visualization(m, dir + "/fields_0");
+        std::cout << "EXECUTION BACKEND: CUDA sm_100a, one GPU holds the whole domain.\n";
+        std::cout << "MPI processes: 1 (domain resident on one GPU)\n";
+        if (dim == 3)
+            std::cout << "Output: " << (c.output_vti ? "vti" : "vtk") << ", "
+                      << (!c.output_vti ? "ASCII Float64" : (c.output_float64 ? "float64" : "float32"))
+                      << "; zlib level=" << c.compression_level
+                      << "; frozen-eta cache=" << (c.frozen_eta_cache ? "on" : "off") << ".\n";
+        std::cout << "Version " << (dim == 3 ? VERSION3 : VERSION2) << "; grains=" << (c.grains ? "on" : "off")
+                  << "; oxygen_diffusion=" << (c.oxygen_diffusion ? "on" : "off") << "; nucleation="
+                  << (c.nucleation == NICR_NUC_CENTER ? "center" : c.nucleation == NICR_NUC_OFF ? "off" : "ksp") << "; "
+                  << m.seeds.size() / dim << " grain(s).\n";
+        int last = 0, n = 0;
+        try {
+            while (n < c.steps) {
+                // advance to the next progress line or output, in one batch
+                int next = std::min(c.steps, (n / 1000 + 1) * 1000);
+                next = std::min(next, (n / c.output_every + 1) * c.output_every);
+                int done = 0;
+                const int r = m.run(next - n, &done);
+                last = n + done;
+                if (r != NICR_OK) throw nicr::Error(r, m.last_error);
+                n = next;
+                if (n % 1000 == 0 || n == c.steps)
+                    std::cout << "step " << n << "/" << c.steps << " (" << 100.0 * n / c.steps << "%), time=" << n * c.dt
+                              << " s" << std::endl;
+                if (n % c.output_every == 0 || n == c.steps) {
+                    do_log(n);
+                    log.flush();
+                    if (!log) throw std::runtime_error("Diagnostics write failed.");
+                    if (m.has_eta) {
+                        gd.flush();
+                        gh.flush();
+                        if (!gd || !gh) throw std::runtime_error("Grain diagnostics write failed.");
+                    }
+                    write_visualization(m, dir + "/fields_" + std::to_string(n));
+                }
+            }
+        } catch (const std::exception& e) {
+            std::ofstream stop(dir + "/STOPPED.txt");
+            stop << "Last accepted time step: " << last << "\n" << e.what() << "\n";
+            write_visualization(m, dir + "/state_at_failure");
+            throw;
+        }
+        std::cout << "Finished " << last << " steps. Output: " << dir << "\n";
+        return 0;
+    } catch (const std::exception& e) {
+        std::cerr << "ERROR: " << e.what() << "\n";
+        return 1;
+    }
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ C-ABI
+extern "C" {
+
+int nicr_write_vtk(nicr_handle* h, const char* path) {
+    return guarded(h, [&](Model& m) {
+        if (m.dim == 2) write_vtk2(m, path);
+        else write_vtk3(m, path);
+    });
+}
+int nicr_write_vti(nicr_handle* h, const char* path) {
+    return guarded(h, [&](Model& m) {
+        if (m.dim != 3) throw nicr::Error(NICR_ERR_STATE, "VTI output exists only in 3D");
+        write_vti3(m, path);
+    });
+}
+int nicr_write_metadata(nicr_handle* h, const char* out_dir) {
+    return guarded(h, [&](Model& m) { metadata(m, out_dir); });
+}
+int nicr_format_log_row(nicr_handle* h, int n, char* buf, size_t len) {
+    return guarded(h, [&](Model& m) { copy_out(buf, len, log_row(m, n)); });
+}
+int nicr_format_grain_rows(nicr_handle* h, int n, char* diag, size_t diag_len, char* history, size_t history_len) {
+    return guarded(h, [&](Model& m) {
+        std::string a, b;
+        grain_rows(m, n, a, b);
+        copy_out(diag, diag_len, a);
+        copy_out(history, history_len, b);
+    });
+}
+int nicr_main(int dim, int argc, const char* const* argv) {
+    if (dim != 2 && dim != 3) return 1;
+    return run_program(dim, argc, argv);
+}
+
+}  // extern "C"

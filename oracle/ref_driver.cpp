@@ -17,6 +17,7 @@
 //   nucleate | refresh | invalidate
 //   stamp X Y [Z]
 //   scale_eta G I J [K] F  eta_G(I,J,K) *= F and invalidate the eta cache
+//   scale_eta_if ...       the same, skipped when there is no eta_G
 //   dump FILE            refresh + tagged binary dump of fields, budget and scalars
 //   log FILE N           append Model::log and Model::grain_log rows for step N
 //   vtk FILE | vti FILE | metadata
@@ -226,6 +227,19 @@ static int exercise(int argc, char** argv) {
             const int cells = m.stamp(x, y);
 #endif
             if (m.domain.rank == 0) std::printf("STAMP %d\n", cells);
+        } else if (cmd == "scale_eta_if") {
+            // regression_driver.cpp:50-54: edit eta_G only when eta fields exist
+            const int g = std::stoi(arg()), i = std::stoi(arg()), j = std::stoi(arg());
+#if NICR_DIM == 3
+            const int k = std::stoi(arg());
+#endif
+            const double fct = std::stod(arg());
+            if ((size_t)g < m.eta.size()) {
+                if (i >= m.domain.first && i <= m.domain.last) AT(m.eta[(size_t)g], i, j, k) *= fct;
+#if NICR_DIM == 3
+                m.invalidate_eta_cache();
+#endif
+            }
         } else if (cmd == "scale_eta") {
             const int g = std::stoi(arg()), i = std::stoi(arg()), j = std::stoi(arg());
 #if NICR_DIM == 3
