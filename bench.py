@@ -4,9 +4,13 @@
 Workload (one "step" = one explicit time step of every field of one domain):
 3D 256^3, evolving grains with 8 eta order parameters (Voronoi of 8 seeds from
 seed 2), Cr = 0.25 +- 0.01 uniform noise, O supplied at the x=0 face
-(bc=concentration), Ksp insertion on, legacy Ck, bounds=legacy, FP64 (the
-drop-in arithmetic, bit-identical to the reference). Inputs (~3 GB of fields)
-are far larger than L2, so no flush is needed between steps.
+(bc=concentration), Ksp insertion on, legacy Ck, bounds=legacy. Inputs (~3 GB
+of fields) are far larger than L2, so no flush is needed between steps.
+
+The headline value is the fp64-fast form (FP64 state, reciprocal divisions);
+the drop-in fp64 form (bit-identical to the reference) is timed beside it from
+the same initial state, and the L-inf deviation between the two after the
+timed steps is reported against the metric's 1e-4 bound.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl nicr|reference]
 
@@ -220,63 +224,87 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
 
     import nicr
-    cfg = workload_config(args.size, args.neta, device=local, seed=2)
-    sol = nicr.Solver(cfg)
-    assert sol.n_eta == args.neta, (sol.n_eta, args.neta)
-    n = sol.n
-    rng = np.random.default_rng(2 + rank)
-    cr = 0.25 + rng.uniform(-0.01, 0.01, size=sol.shape)
-    cr[0] = sol.get("cr")[0]          # the inlet layer keeps its Cr
-    sol.set("cr", cr)
-    sol.reset_inventory()
-    stream = torch.cuda.ExternalStream(sol.stream(), device=local)
-
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    # ---- warm-up
-    sol.run(args.warmup)
-    torch.cuda.synchronize()
-
-    # ---- device-timed region: K steps resident in HBM
     L = nicr.lib()
     L.nicr_profile.argtypes = [ctypes.c_void_p, ctypes.c_int]
     L.nicr_profile_read.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
                                     ctypes.POINTER(ctypes.c_longlong)]
     L.nicr_kernel_launches.argtypes = [ctypes.c_void_p]
     L.nicr_kernel_launches.restype = ctypes.c_longlong
-    L.nicr_profile(sol.h, 1)
-    sampler = ClockSampler(local)
-    sampler.start()
-    time.sleep(0.3)
-    barrier()
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    launches0 = L.nicr_kernel_launches(sol.h)
-    e0.record(stream)
-    rc, done = sol.run(args.steps, check=False)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    barrier()
-    clocks = sampler.stop()
-    launches = L.nicr_kernel_launches(sol.h) - launches0
-    if rc != 0 or done != args.steps:
-        raise SystemExit(f"step rejected: {sol.last_error}")
-    ms = e0.elapsed_time(e1)
-    prof = {}
-    for k, name in enumerate(KERNELS):
-        tot, cnt = ctypes.c_double(0), ctypes.c_longlong(0)
-        L.nicr_profile_read(sol.h, k, ctypes.byref(tot), ctypes.byref(cnt))
-        if cnt.value:
-            prof[name] = (tot.value, cnt.value)
-    L.nicr_profile(sol.h, 0)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def make_solver(precision):
+        cfg = workload_config(args.size, args.neta, device=local, seed=2)
+        cfg.precision = precision
+        sol = nicr.Solver(cfg)
+        assert sol.n_eta == args.neta, (sol.n_eta, args.neta)
+        rng = np.random.default_rng(2 + rank)
+        cr = 0.25 + rng.uniform(-0.01, 0.01, size=sol.shape)
+        cr[0] = sol.get("cr")[0]          # the inlet layer keeps its Cr
+        sol.set("cr", cr)
+        sol.reset_inventory()
+        return sol
+
+    def timed_run(sol, with_clocks):
+        """W untimed steps, then K steps between CUDA events on the library's stream."""
+        stream = torch.cuda.ExternalStream(sol.stream(), device=local)
+        sol.run(args.warmup)
+        torch.cuda.synchronize()
+        L.nicr_profile(sol.h, 1)
+        sampler = ClockSampler(local) if with_clocks else None
+        if sampler:
+            sampler.start()
+            time.sleep(0.3)
+        barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        launches0 = L.nicr_kernel_launches(sol.h)
+        e0.record(stream)
+        rc, done = sol.run(args.steps, check=False)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        clocks = sampler.stop() if sampler else None
+        launches = L.nicr_kernel_launches(sol.h) - launches0
+        if rc != 0 or done != args.steps:
+            raise SystemExit(f"step rejected: {sol.last_error}")
+        prof = {}
+        for k, name in enumerate(KERNELS):
+            tot, cnt = ctypes.c_double(0), ctypes.c_longlong(0)
+            L.nicr_profile_read(sol.h, k, ctypes.byref(tot), ctypes.byref(cnt))
+            if cnt.value:
+                prof[name] = (tot.value, cnt.value)
+        L.nicr_profile(sol.h, 0)
+        return e0.elapsed_time(e1), prof, clocks, launches
+
+    # the drop-in (bit-identical) form, then the reciprocal-division form from
+    # the same initial state; both advance W + K steps on the same schedule
+    plain = make_solver(0)
+    ms_plain, prof_plain, _, _ = timed_run(plain, False)
+    sol = make_solver(1)
+    ms, prof, clocks, launches = timed_run(sol, True)
+    err = 0.0
+    for f in ["o", "cr", "p"] + [f"eta{g + 1}" for g in range(args.neta)]:
+        a, b = sol.get(f), plain.get(f)
+        err = max(err, float(np.max(np.abs(a - b)) / max(float(np.max(np.abs(b))), 1e-300)))
+    plain.close()
+    tp = torch.tensor([ms_plain], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(tp, op=dist.ReduceOp.MAX)
+    n = sol.n
+    value_plain = world * n * args.steps / (float(tp.item()) * 1e-3) / 1e6
 
     t = torch.tensor([ms], dtype=torch.float64, device="cuda")
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     ms_max = float(t.item())
     value = world * n * args.steps / (ms_max * 1e-3) / 1e6
+    form = "fp64-fast (reciprocal divisions; FP64 state and operation order)"
+    if not err <= 1e-4:
+        # outside the metric's bound: the headline falls back to the drop-in form
+        value, ms_max, prof, form = value_plain, float(tp.item()), prof_plain, "fp64 (drop-in)"
 
     # ---- end to end through the C-ABI with host buffers: upload the state from
     # pinned memory, one nicr_run(1) call per step (each returns the accept status
@@ -313,9 +341,15 @@ def main():
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64",
+        "form": form,
+        "plain_fp64": {"value": value_plain, "unit": UNIT, "ms_per_step": float(tp.item()) / args.steps,
+                       "kernels": {k: {"ms_per_launch": v[0] / v[1]} for k, v in prof_plain.items()},
+                       "note": "bit-identical to the reference"},
+        "error_vs_plain": {"linf_rel_max": err, "fields": "o, cr, phi, eta_1..N",
+                           "steps": args.warmup + args.steps, "bound": 1e-4},
         "data": "synthetic (seeded Cr noise, Voronoi seed 2); inputs ~3 GB > L2, no flush needed",
         "config": {"workload": f"3D {args.size}^3, {args.neta} evolving eta (Voronoi seed 2), Cr 0.25+-0.01, "
-                               f"bc=concentration, Ksp on, legacy Ck, bounds=legacy, FP64 drop-in",
+                               f"bc=concentration, Ksp on, legacy Ck, bounds=legacy",
                    "cells": n, "parallelism": f"independent domains x{world}", "l2": "inputs larger than L2"},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind,

@@ -46,7 +46,8 @@ std::string help_text(int dim) {
          "--nucleation ksp|center|off --radius-grid R --nucleation-period s\n"
          "--bc concentration|mu|closed --mu-res v --surface-c-ref v\n"
          "--ck legacy|off --bounds stop|legacy --out directory --self-test --version\n"
-         "Extensions (defaults reproduce the fixed reference constants): --ksp v --bulk-cr v --layer-o v\n";
+         "Extensions (defaults reproduce the fixed reference constants): --ksp v --bulk-cr v --layer-o v\n"
+         "--precision fp64|fp64-fast (fp64: bit-identical to the reference; fp64-fast: reciprocal divisions)\n";
     return s;
 }
 
@@ -116,6 +117,11 @@ void parse_into(nicr_config& c, int dim, int argc, const char* const* argv, std:
         else if (a == "--ksp") c.ksp = std::stod(v);
         else if (a == "--bulk-cr") c.bulk_cr = std::stod(v);
         else if (a == "--layer-o") c.layer_o = std::stod(v);
+        else if (a == "--precision") {
+            if (v == "fp64") c.precision = NICR_FP64;
+            else if (v == "fp64-fast") c.precision = NICR_FP64_FAST;
+            else throw std::runtime_error("--precision expects fp64 or fp64-fast.");
+        }
         else throw std::runtime_error("Unknown argument: " + a);
     }
     // validation, in the reference's order (3S:1055-1081, 2D:770-789)

@@ -67,6 +67,7 @@ struct StepParams {
     int phi_eta;                 // eta coupling in the phi force (has_eta)
     int inlet;                   // bc == concentration && oxygen_diffusion
     int xchunk;                  // planes per CTA along X
+    int fast;                    // arithmetic form: 0 drop-in (bit-identical), 1 reciprocal divisions
 };
 
 // ---- step --------------------------------------------------------------------

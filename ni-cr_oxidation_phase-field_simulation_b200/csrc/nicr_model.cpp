@@ -108,6 +108,9 @@ Model::Model(const nicr_config& cfg) : c(cfg), dim(cfg.dim) {
     sp.grains = c.grains ? 1 : 0;
     sp.phi_eta = has_eta ? 1 : 0;
     sp.inlet = (c.bc == NICR_BC_CONCENTRATION && c.oxygen_diffusion) ? 1 : 0;
+    if (c.precision != NICR_FP64 && c.precision != NICR_FP64_FAST)
+        throw Error(NICR_ERR_INVALID_ARG, "precision must be NICR_FP64 or NICR_FP64_FAST");
+    sp.fast = c.precision == NICR_FP64_FAST ? 1 : 0;
     // X chunking: enough CTAs for a few waves on 148 SMs
     {
         const long long tiles = dim == 3 ? (long long)((g.nb + 31) / 32) * ((g.na + 7) / 8) : (g.nb + 127) / 128;

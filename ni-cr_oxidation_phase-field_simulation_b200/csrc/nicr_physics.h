@@ -97,8 +97,9 @@ inline EtaCoef eta_coef(double fwhm, double dx, double W, double kappa, double p
 // (strict, so ties are excluded; q1 a power of two is excluded because its
 // lower neighbour is closer). The residual is exact whenever q1 is within an
 // ulp of a/b, and when it is not, its rounded value cannot pass the test, so
-// an accepted q1 is always RN(a/b). Outside the guarded exponent range (and
-// for zeros, infinities, NaNs) the IEEE division is used. The scale factor
+// an accepted q1 is always RN(a/b). Zeros return a * RN(1/b), the exactly
+// signed zero. Outside the guarded exponent range (subnormals, infinities,
+// NaNs) the IEEE division is used. The scale factor
 // 2^(53-E) (E = exponent of q1) keeps the comparison free of underflow.
 struct DivC {
     double b, rb;   // divisor and RN(1/b)
@@ -119,11 +120,15 @@ inline DivC make_divc(double b) {
 // it at every call site would multiply the kernels' instruction footprint.
 __device__ __noinline__ double ieee_div(double a, double b);
 __device__ __forceinline__ double xdiv(double a, const DivC& d) {
-#if defined(NICR_DIV_IEEE)
+#if defined(NICR_DIV_RECIP)
+    return __dmul_rn(a, d.rb);
+#elif defined(NICR_DIV_IEEE)
     return __ddiv_rn(a, d.b);
 #else
     const long long ab = __double_as_longlong(a);
     const int ea = (int)((ab >> 52) & 0x7FF);
+    // +-0 / b is an exactly signed zero, which a * RN(1/b) reproduces
+    if (d.fast && (ab << 1) == 0) return __dmul_rn(a, d.rb);
     if (d.fast && ea >= 123 && ea <= 1923) {
         const double q0 = __dmul_rn(a, d.rb);
         const double r0 = __fma_rn(-q0, d.b, a);

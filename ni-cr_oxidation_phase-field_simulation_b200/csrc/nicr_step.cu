@@ -80,15 +80,20 @@ struct Tile {
     __device__ static int i1(int a, int b) { return (a + HA1) * RB1 + (b + 1); }
 };
 
-// Divisions of the fused step: IEEE a / b (measured faster than xdiv here,
-// where registers are capped for occupancy).
-__device__ __forceinline__ double sdiv(double a, const DivC& d) { return __ddiv_rn(a, d.b); }
+// Division by a run constant in the two arithmetic forms: FAST=false is the
+// drop-in (xdiv: the correctly rounded quotient, bit-identical to a / b);
+// FAST=true multiplies by RN(1/b) (within one ulp of a / b).
+template <bool FAST>
+__device__ __forceinline__ double fdiv(double a, const DivC& d) {
+    if (FAST) return __dmul_rn(a, d.rb);
+    return xdiv(a, d);
+}
 
 struct CenterVals {
     double o, cr, p, hh, muO, muCr, mo, mc;   // hh = h(p), reused by Ck
 };
 
-template <int DIM, int TA, int TB>
+template <int DIM, int TA, int TB, bool FAST>
 struct StepKernel {
     using T = Tile<DIM, TA, TB>;
 
@@ -179,17 +184,17 @@ struct StepKernel {
         const double oc = so0[c2], cc = sc0[c2];
         double lapO, lapC;
         if (DIM == 3) {
-            lapO = sdiv((sop[c2] - 2. * oc + som[c2]), P.v_dxdx)
-                 + sdiv((so0[T::i2(a + 1, b)] - 2. * oc + so0[T::i2(a - 1, b)]), P.v_dada)
-                 + sdiv((so0[T::i2(a, b + 1)] - 2. * oc + so0[T::i2(a, b - 1)]), P.v_dbdb);
-            lapC = sdiv((scp[c2] - 2. * cc + scm[c2]), P.v_dxdx)
-                 + sdiv((sc0[T::i2(a + 1, b)] - 2. * cc + sc0[T::i2(a - 1, b)]), P.v_dada)
-                 + sdiv((sc0[T::i2(a, b + 1)] - 2. * cc + sc0[T::i2(a, b - 1)]), P.v_dbdb);
+            lapO = fdiv<FAST>((sop[c2] - 2. * oc + som[c2]), P.v_dxdx)
+                 + fdiv<FAST>((so0[T::i2(a + 1, b)] - 2. * oc + so0[T::i2(a - 1, b)]), P.v_dada)
+                 + fdiv<FAST>((so0[T::i2(a, b + 1)] - 2. * oc + so0[T::i2(a, b - 1)]), P.v_dbdb);
+            lapC = fdiv<FAST>((scp[c2] - 2. * cc + scm[c2]), P.v_dxdx)
+                 + fdiv<FAST>((sc0[T::i2(a + 1, b)] - 2. * cc + sc0[T::i2(a - 1, b)]), P.v_dada)
+                 + fdiv<FAST>((sc0[T::i2(a, b + 1)] - 2. * cc + sc0[T::i2(a, b - 1)]), P.v_dbdb);
         } else {
-            lapO = sdiv((sop[c2] - 2. * oc + som[c2]), P.v_dxdx)
-                 + sdiv((so0[T::i2(a, b + 1)] - 2. * oc + so0[T::i2(a, b - 1)]), P.v_dbdb);
-            lapC = sdiv((scp[c2] - 2. * cc + scm[c2]), P.v_dxdx)
-                 + sdiv((sc0[T::i2(a, b + 1)] - 2. * cc + sc0[T::i2(a, b - 1)]), P.v_dbdb);
+            lapO = fdiv<FAST>((sop[c2] - 2. * oc + som[c2]), P.v_dxdx)
+                 + fdiv<FAST>((so0[T::i2(a, b + 1)] - 2. * oc + so0[T::i2(a, b - 1)]), P.v_dbdb);
+            lapC = fdiv<FAST>((scp[c2] - 2. * cc + scm[c2]), P.v_dxdx)
+                 + fdiv<FAST>((sc0[T::i2(a, b + 1)] - 2. * cc + sc0[T::i2(a, b - 1)]), P.v_dbdb);
         }
         const int c1 = T::i1(a, b);
         const double pc = sp[c1];
@@ -276,8 +281,8 @@ struct StepKernel {
             __syncthreads();
             // ghost plane -1: copies of plane 0 (3S:187, 3S:613-615, 3S:616-619)
             const double muOg = (P.bc == 1 && P.o_on) ? 2. * P.mu_res - C.muO : C.muO;
-            FxO = sdiv(-.5 * (C.mo + C.mo) * (C.muO - muOg), P.v_dx);
-            FxCr = sdiv(-.5 * (C.mc + C.mc) * (C.muCr - C.muCr), P.v_dx);
+            FxO = fdiv<FAST>(-.5 * (C.mo + C.mo) * (C.muO - muOg), P.v_dx);
+            FxCr = fdiv<FAST>(-.5 * (C.mc + C.mc) * (C.muCr - C.muCr), P.v_dx);
             pP = C.p;
         } else {
             load_oc(P, o, cr, i0 - 2, oslot(i0 - 2), cslot(i0 - 2), offs);
@@ -292,8 +297,8 @@ struct StepKernel {
             __syncthreads();
             C = lead(i0);
             __syncthreads();
-            FxO = sdiv(-.5 * (Pv.mo + C.mo) * (C.muO - Pv.muO), P.v_dx);
-            FxCr = sdiv(-.5 * (Pv.mc + C.mc) * (C.muCr - Pv.muCr), P.v_dx);
+            FxO = fdiv<FAST>(-.5 * (Pv.mo + C.mo) * (C.muO - Pv.muO), P.v_dx);
+            FxCr = fdiv<FAST>(-.5 * (Pv.mc + C.mc) * (C.muCr - Pv.muCr), P.v_dx);
             pP = Pv.p;
         }
 
@@ -321,8 +326,8 @@ struct StepKernel {
                 const long long cell = ((long long)u * g.na + row) * g.nb + col;  // reference loop order
 
                 // x faces: the right face of u is the left face of u+1 (same expression)
-                const double rightO = sdiv(-.5 * (C.mo + L.mo) * (L.muO - C.muO), P.v_dx);
-                const double rightCr = sdiv(-.5 * (C.mc + L.mc) * (L.muCr - C.muCr), P.v_dx);
+                const double rightO = fdiv<FAST>(-.5 * (C.mo + L.mo) * (L.muO - C.muO), P.v_dx);
+                const double rightCr = fdiv<FAST>(-.5 * (C.mc + L.mc) * (L.muCr - C.muCr), P.v_dx);
                 double leftO = FxO;
                 if (u == 0 && P.bc == 1) {
                     // left_flux (3S:621-628): surface-mobility face closure for bc=mu
@@ -330,36 +335,36 @@ struct StepKernel {
                     if (P.o_on) {
                         const double gb0 = P.grains ? __ldg(gb + gidx) : 0.;
                         const double mf = mobility(P.surface_c_ref, h(C.p), gb0, Phys::bmo, Phys::boo, P.gbm1_o);
-                        lf = sdiv(2. * mf * (P.mu_res - C.muO), P.v_dx);
+                        lf = fdiv<FAST>(2. * mf * (P.mu_res - C.muO), P.v_dx);
                     }
                     leftO = lf;
-                    acc[4] = dd_add(acc[4], sdiv(P.dt * lf, P.v_dx));
+                    acc[4] = dd_add(acc[4], fdiv<FAST>(P.dt * lf, P.v_dx));
                 }
                 if (u == 0 && P.inlet) acc[4] = dd_add(acc[4], P.layer_o - __ldg(o + gidx));
 
                 double divO = 0., divCr;
                 {
                     const double mc0 = mc_[c1], mu0 = mC[c1];
-                    const double front = sdiv(-.5 * (mc0 + mc_[bp]) * (mC[bp] - mu0), P.v_db);
-                    const double back = sdiv(-.5 * (mc_[bm] + mc0) * (mu0 - mC[bm]), P.v_db);
+                    const double front = fdiv<FAST>(-.5 * (mc0 + mc_[bp]) * (mC[bp] - mu0), P.v_db);
+                    const double back = fdiv<FAST>(-.5 * (mc_[bm] + mc0) * (mu0 - mC[bm]), P.v_db);
                     if (DIM == 3) {
-                        const double top = sdiv(-.5 * (mc0 + mc_[ap]) * (mC[ap] - mu0), P.v_da);
-                        const double bottom = sdiv(-.5 * (mc_[am] + mc0) * (mu0 - mC[am]), P.v_da);
-                        divCr = sdiv(FxCr - rightCr, P.v_dx) + sdiv(bottom - top, P.v_da) + sdiv(back - front, P.v_db);
+                        const double top = fdiv<FAST>(-.5 * (mc0 + mc_[ap]) * (mC[ap] - mu0), P.v_da);
+                        const double bottom = fdiv<FAST>(-.5 * (mc_[am] + mc0) * (mu0 - mC[am]), P.v_da);
+                        divCr = fdiv<FAST>(FxCr - rightCr, P.v_dx) + fdiv<FAST>(bottom - top, P.v_da) + fdiv<FAST>(back - front, P.v_db);
                     } else {
-                        divCr = sdiv(FxCr - rightCr, P.v_dx) + sdiv(back - front, P.v_db);
+                        divCr = fdiv<FAST>(FxCr - rightCr, P.v_dx) + fdiv<FAST>(back - front, P.v_db);
                     }
                 }
                 if (P.o_on) {
                     const double m0 = mo_[c1], mu0 = mO[c1];
-                    const double front = sdiv(-.5 * (m0 + mo_[bp]) * (mO[bp] - mu0), P.v_db);
-                    const double back = sdiv(-.5 * (mo_[bm] + m0) * (mu0 - mO[bm]), P.v_db);
+                    const double front = fdiv<FAST>(-.5 * (m0 + mo_[bp]) * (mO[bp] - mu0), P.v_db);
+                    const double back = fdiv<FAST>(-.5 * (mo_[bm] + m0) * (mu0 - mO[bm]), P.v_db);
                     if (DIM == 3) {
-                        const double top = sdiv(-.5 * (m0 + mo_[ap]) * (mO[ap] - mu0), P.v_da);
-                        const double bottom = sdiv(-.5 * (mo_[am] + m0) * (mu0 - mO[am]), P.v_da);
-                        divO = sdiv(leftO - rightO, P.v_dx) + sdiv(bottom - top, P.v_da) + sdiv(back - front, P.v_db);
+                        const double top = fdiv<FAST>(-.5 * (m0 + mo_[ap]) * (mO[ap] - mu0), P.v_da);
+                        const double bottom = fdiv<FAST>(-.5 * (mo_[am] + m0) * (mu0 - mO[am]), P.v_da);
+                        divO = fdiv<FAST>(leftO - rightO, P.v_dx) + fdiv<FAST>(bottom - top, P.v_da) + fdiv<FAST>(back - front, P.v_db);
                     } else {
-                        divO = sdiv(leftO - rightO, P.v_dx) + sdiv(back - front, P.v_db);
+                        divO = fdiv<FAST>(leftO - rightO, P.v_dx) + fdiv<FAST>(back - front, P.v_db);
                     }
                 }
                 const double oo = C.o, cc = C.cr, pp = C.p;
@@ -367,10 +372,10 @@ struct StepKernel {
                 double crv = cc + P.dt * divCr;
                 double lapP;
                 if (DIM == 3)
-                    lapP = sdiv((L.p - 2. * pp + pP), P.v_dxdx) + sdiv((spu[ap] - 2. * pp + spu[am]), P.v_dada)
-                         + sdiv((spu[bp] - 2. * pp + spu[bm]), P.v_dbdb);
+                    lapP = fdiv<FAST>((L.p - 2. * pp + pP), P.v_dxdx) + fdiv<FAST>((spu[ap] - 2. * pp + spu[am]), P.v_dada)
+                         + fdiv<FAST>((spu[bp] - 2. * pp + spu[bm]), P.v_dbdb);
                 else
-                    lapP = sdiv((L.p - 2. * pp + pP), P.v_dxdx) + sdiv((spu[bp] - 2. * pp + spu[bm]), P.v_dbdb);
+                    lapP = fdiv<FAST>((L.p - 2. * pp + pP), P.v_dxdx) + fdiv<FAST>((spu[bp] - 2. * pp + spu[bm]), P.v_dbdb);
                 const double hpv = 30. * pp * pp * (pp - 1.) * (pp - 1.);
                 double fp = Phys::W * (4. * pp * pp * pp - 6. * pp * pp + 2. * pp)
                           + hpv * (foxide(oo, cc) - fmetal(oo, cc)) - 2. * Phys::kp * lapP;
@@ -378,8 +383,8 @@ struct StepKernel {
                 double pnv = pp - P.dtL * fp;
                 if (P.ck == 0) {
                     const double hn = h(pnv);
-                    const double dO = sdiv(-Phys::ckO * ((Phys::oxideO - onv) * hn - (Phys::oxideO - oo) * C.hh), P.v_dt);
-                    const double dCr = sdiv(-Phys::ckCr * ((Phys::oxideCr - crv) * hn - (Phys::oxideCr - cc) * C.hh), P.v_dt);
+                    const double dO = fdiv<FAST>(-Phys::ckO * ((Phys::oxideO - onv) * hn - (Phys::oxideO - oo) * C.hh), P.v_dt);
+                    const double dCr = fdiv<FAST>(-Phys::ckCr * ((Phys::oxideCr - crv) * hn - (Phys::oxideCr - cc) * C.hh), P.v_dt);
                     onv += dO; crv += dCr;
                     acc[0] = dd_add(acc[0], dO);
                     acc[1] = dd_add(acc[1], dCr);
@@ -414,13 +419,13 @@ struct StepKernel {
     }
 };
 
-template <int DIM, int TA, int TB, int MINB>
+template <int DIM, int TA, int TB, int MINB, bool FAST>
 __global__ void __launch_bounds__(TA * TB, MINB)
 k_step_main(const StepParams P, const double* __restrict__ o, const double* __restrict__ cr,
             const double* __restrict__ p, const double* __restrict__ gb, const double* __restrict__ s2,
             double* __restrict__ on, double* __restrict__ crn, double* __restrict__ pn,
             StepPartial* __restrict__ partials, Status* st) {
-    StepKernel<DIM, TA, TB>::run(P, o, cr, p, gb, s2, on, crn, pn, partials, st);
+    StepKernel<DIM, TA, TB, FAST>::run(P, o, cr, p, gb, s2, on, crn, pn, partials, st);
 }
 
 constexpr int TA3 = 8, TB3 = 32;    // 3D tile: 8 rows x 32 columns, 256 threads
@@ -462,7 +467,7 @@ __global__ void k_eta_mask(const StepParams P, int neta, const double* __restric
 // eta_trial (3S:514-526): v = eta - (dt*L_eta)*(deta - K*lap(eta)); must lie in
 // [-1e-12, 1+1e-12]. Writes the trial and the mask of the trial values (the
 // next step's gb and eta_s2, identical to rebuild_eta_mask on them).
-template <int DIM>
+template <int DIM, bool FAST>
 __global__ void k_eta_update(const StepParams P, int neta, const double* __restrict__ eta,
                              const double* __restrict__ s2, const double* __restrict__ p,
                              double* __restrict__ eta_next, double* __restrict__ gb_next,
@@ -492,12 +497,12 @@ __global__ void k_eta_update(const StepParams P, int neta, const double* __restr
         const double ec = __ldg(e + idx);
         double lap;
         if (DIM == 3)
-            lap = xdiv((__ldg(e + ixp) - 2. * ec + __ldg(e + ixm)), P.v_dxdx)
-                + xdiv((__ldg(e + iap) - 2. * ec + __ldg(e + iam)), P.v_dada)
-                + xdiv((__ldg(e + ibp) - 2. * ec + __ldg(e + ibm)), P.v_dbdb);
+            lap = fdiv<FAST>((__ldg(e + ixp) - 2. * ec + __ldg(e + ixm)), P.v_dxdx)
+                + fdiv<FAST>((__ldg(e + iap) - 2. * ec + __ldg(e + iam)), P.v_dada)
+                + fdiv<FAST>((__ldg(e + ibp) - 2. * ec + __ldg(e + ibm)), P.v_dbdb);
         else
-            lap = xdiv((__ldg(e + ixp) - 2. * ec + __ldg(e + ixm)), P.v_dxdx)
-                + xdiv((__ldg(e + ibp) - 2. * ec + __ldg(e + ibm)), P.v_dbdb);
+            lap = fdiv<FAST>((__ldg(e + ixp) - 2. * ec + __ldg(e + ixm)), P.v_dxdx)
+                + fdiv<FAST>((__ldg(e + ibp) - 2. * ec + __ldg(e + ibm)), P.v_dbdb);
         const double force = grain_deta(ec, S, phi, P.eta_W, P.eta_A) - P.eta_K * lap;
         const double v = ec - P.dt_etaL * force;
         if (!isfinite(v) || v < -1.e-12 || v > 1. + 1.e-12)
@@ -517,7 +522,7 @@ __global__ void k_eta_update(const StepParams P, int neta, const double* __restr
 // three-plane shared-memory ring, so every field is read from HBM about once.
 // S = sum eta_g^2 is rebuilt from the staged centres in g order, which is the
 // same arithmetic as rebuild_eta_mask and therefore the same value as eta_s2.
-template <int DIM, int TA, int TB>
+template <int DIM, int TA, int TB, bool FAST>
 __global__ void __launch_bounds__(TA * TB)
 k_eta_stream(const StepParams P, int neta, const double* __restrict__ eta, const double* __restrict__ p,
              double* __restrict__ eta_next, double* __restrict__ gb_next, double* __restrict__ s2_next,
@@ -576,12 +581,12 @@ k_eta_stream(const StepParams P, int neta, const double* __restrict__ eta, const
                 const double ec = s0[o + c1];
                 double lap;
                 if (DIM == 3)
-                    lap = xdiv((sp[o + c1] - 2. * ec + sm[o + c1]), P.v_dxdx)
-                        + xdiv((s0[o + ap] - 2. * ec + s0[o + am]), P.v_dada)
-                        + xdiv((s0[o + bp] - 2. * ec + s0[o + bm]), P.v_dbdb);
+                    lap = fdiv<FAST>((sp[o + c1] - 2. * ec + sm[o + c1]), P.v_dxdx)
+                        + fdiv<FAST>((s0[o + ap] - 2. * ec + s0[o + am]), P.v_dada)
+                        + fdiv<FAST>((s0[o + bp] - 2. * ec + s0[o + bm]), P.v_dbdb);
                 else
-                    lap = xdiv((sp[o + c1] - 2. * ec + sm[o + c1]), P.v_dxdx)
-                        + xdiv((s0[o + bp] - 2. * ec + s0[o + bm]), P.v_dbdb);
+                    lap = fdiv<FAST>((sp[o + c1] - 2. * ec + sm[o + c1]), P.v_dxdx)
+                        + fdiv<FAST>((s0[o + bp] - 2. * ec + s0[o + bm]), P.v_dbdb);
                 const double force = grain_deta(ec, S, phi, P.eta_W, P.eta_A) - P.eta_K * lap;
                 const double v = ec - P.dt_etaL * force;
                 if (!isfinite(v) || v < -1.e-12 || v > 1. + 1.e-12)
@@ -607,7 +612,9 @@ __global__ void k_check_division(DivC d, long long n, unsigned long long seed, u
         unsigned long long x = seed ^ (0x9E3779B97F4A7C15ull * (unsigned long long)(i + 1));
         x ^= x >> 33; x *= 0xff51afd7ed558ccdull; x ^= x >> 33; x *= 0xc4ceb9fe1a85ec53ull; x ^= x >> 33;
         double a;
-        if (i & 3) {
+        if (i % 97 == 0) {
+            a = (i & 1) ? -0.0 : 0.0;
+        } else if (i & 3) {
             const int e = (int)((x >> 56) % 120) - 60;
             a = ldexp((double)(x >> 11) * (1.0 / 9007199254740992.0) + 0.5, e);
             if (x & 1) a = -a;
@@ -713,33 +720,44 @@ static int step_minb() {
     return v;
 }
 
-template <int MINB>
+template <int MINB, bool FAST>
 static void launch_step3(const StepParams& P, const double* o, const double* cr, const double* p, const double* gb,
                          const double* s2, double* on, double* crn, double* pn, StepPartial* partials, Status* st,
                          cudaStream_t stream, int* nblocks_out) {
     using T = Tile<3, TA3, TB3>;
     static bool attr = false;
     if (!attr) {
-        cudaFuncSetAttribute(k_step_main<3, TA3, TB3, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM_BYTES);
+        cudaFuncSetAttribute(k_step_main<3, TA3, TB3, MINB, FAST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)T::SMEM_BYTES);
         attr = true;
     }
     const dim3 grid = step_grid<3, TA3, TB3>(P);
-    k_step_main<3, TA3, TB3, MINB><<<grid, dim3(TB3, TA3), T::SMEM_BYTES, stream>>>(P, o, cr, p, gb, s2, on, crn, pn, partials, st);
+    k_step_main<3, TA3, TB3, MINB, FAST><<<grid, dim3(TB3, TA3), T::SMEM_BYTES, stream>>>(P, o, cr, p, gb, s2, on, crn,
+                                                                                         pn, partials, st);
     if (nblocks_out) *nblocks_out = (int)(grid.x * grid.y * grid.z);
+}
+
+template <bool FAST>
+static void launch_step_form(const StepParams& P, const double* o, const double* cr, const double* p,
+                             const double* gb, const double* s2, double* on, double* crn, double* pn,
+                             StepPartial* partials, Status* st, cudaStream_t stream, int* nblocks_out) {
+    if (P.g.dim == 3) {
+        if (step_minb() == 3) launch_step3<3, FAST>(P, o, cr, p, gb, s2, on, crn, pn, partials, st, stream, nblocks_out);
+        else launch_step3<2, FAST>(P, o, cr, p, gb, s2, on, crn, pn, partials, st, stream, nblocks_out);
+    } else {
+        using T = Tile<2, TA2, TB2>;
+        const dim3 grid = step_grid<2, TA2, TB2>(P);
+        k_step_main<2, TA2, TB2, 4, FAST><<<grid, dim3(TB2, TA2), T::SMEM_BYTES, stream>>>(P, o, cr, p, gb, s2, on,
+                                                                                          crn, pn, partials, st);
+        if (nblocks_out) *nblocks_out = (int)(grid.x * grid.y * grid.z);
+    }
 }
 
 void launch_step_main(const StepParams& P, const double* o, const double* cr, const double* p, const double* gb,
                       const double* s2, double* on, double* crn, double* pn, StepPartial* partials, Status* st,
                       cudaStream_t stream, int* nblocks_out) {
-    if (P.g.dim == 3) {
-        if (step_minb() == 3) launch_step3<3>(P, o, cr, p, gb, s2, on, crn, pn, partials, st, stream, nblocks_out);
-        else launch_step3<2>(P, o, cr, p, gb, s2, on, crn, pn, partials, st, stream, nblocks_out);
-    } else {
-        using T = Tile<2, TA2, TB2>;
-        const dim3 grid = step_grid<2, TA2, TB2>(P);
-        k_step_main<2, TA2, TB2, 4><<<grid, dim3(TB2, TA2), T::SMEM_BYTES, stream>>>(P, o, cr, p, gb, s2, on, crn, pn, partials, st);
-        if (nblocks_out) *nblocks_out = (int)(grid.x * grid.y * grid.z);
-    }
+    if (P.fast) launch_step_form<true>(P, o, cr, p, gb, s2, on, crn, pn, partials, st, stream, nblocks_out);
+    else launch_step_form<false>(P, o, cr, p, gb, s2, on, crn, pn, partials, st, stream, nblocks_out);
 }
 
 void launch_eta_mask(const StepParams& P, int neta, const double* eta, double* gb, double* s2, double* pairs,
@@ -751,8 +769,9 @@ void launch_eta_mask(const StepParams& P, int neta, const double* eta, double* g
     k_eta_mask<<<blocks, threads, 0, stream>>>(P, neta, eta, gb, s2, pairs, st);
 }
 
-void launch_eta_update(const StepParams& P, int neta, const double* eta, const double* s2, const double* p,
-                       double* eta_next, double* gb_next, double* s2_next, Status* st, cudaStream_t stream) {
+template <bool FAST>
+static void launch_eta_form(const StepParams& P, int neta, const double* eta, const double* s2, const double* p,
+                            double* eta_next, double* gb_next, double* s2_next, Status* st, cudaStream_t stream) {
     const Grid& g = P.g;
     // The per-cell kernel (stencil neighbours through L1/L2) is the default: the
     // streaming kernel stalls on its per-plane barriers until the next plane
@@ -768,33 +787,39 @@ void launch_eta_update(const StepParams& P, int neta, const double* eta, const d
         if (!simple && smem <= 200 * 1024) {
             static size_t attr = 0;
             if (smem > 48 * 1024 && smem > attr) {
-                cudaFuncSetAttribute(k_eta_stream<3, TA, TB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                cudaFuncSetAttribute(k_eta_stream<3, TA, TB, FAST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
                 attr = smem;
             }
             const dim3 grid((g.nb + TB - 1) / TB, (g.na + TA - 1) / TA, (g.nx + P.xchunk - 1) / P.xchunk);
-            k_eta_stream<3, TA, TB><<<grid, dim3(TB, TA), smem, stream>>>(P, neta, eta, p, eta_next, gb_next, s2_next, st);
+            k_eta_stream<3, TA, TB, FAST><<<grid, dim3(TB, TA), smem, stream>>>(P, neta, eta, p, eta_next, gb_next, s2_next, st);
             return;
         }
         const dim3 block(32, 8);
         const dim3 grid((g.nb + 31) / 32, (g.na + 7) / 8, g.nx);
-        k_eta_update<3><<<grid, block, 0, stream>>>(P, neta, eta, s2, p, eta_next, gb_next, s2_next, st);
+        k_eta_update<3, FAST><<<grid, block, 0, stream>>>(P, neta, eta, s2, p, eta_next, gb_next, s2_next, st);
     } else {
         constexpr int TB = 128, S1 = TB + 2;
         const size_t smem = (size_t)3 * neta * S1 * sizeof(double) + S1 * sizeof(int);
-        if (smem <= 200 * 1024) {
+        if (!simple && smem <= 200 * 1024) {
             static size_t attr = 0;
             if (smem > 48 * 1024 && smem > attr) {
-                cudaFuncSetAttribute(k_eta_stream<2, 1, TB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                cudaFuncSetAttribute(k_eta_stream<2, 1, TB, FAST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
                 attr = smem;
             }
             const dim3 grid((g.nb + TB - 1) / TB, 1, (g.nx + P.xchunk - 1) / P.xchunk);
-            k_eta_stream<2, 1, TB><<<grid, dim3(TB, 1), smem, stream>>>(P, neta, eta, p, eta_next, gb_next, s2_next, st);
+            k_eta_stream<2, 1, TB, FAST><<<grid, dim3(TB, 1), smem, stream>>>(P, neta, eta, p, eta_next, gb_next, s2_next, st);
             return;
         }
         const dim3 block(128, 1);
         const dim3 grid((g.nb + 127) / 128, 1, g.nx);
-        k_eta_update<2><<<grid, block, 0, stream>>>(P, neta, eta, s2, p, eta_next, gb_next, s2_next, st);
+        k_eta_update<2, FAST><<<grid, block, 0, stream>>>(P, neta, eta, s2, p, eta_next, gb_next, s2_next, st);
     }
+}
+
+void launch_eta_update(const StepParams& P, int neta, const double* eta, const double* s2, const double* p,
+                       double* eta_next, double* gb_next, double* s2_next, Status* st, cudaStream_t stream) {
+    if (P.fast) launch_eta_form<true>(P, neta, eta, s2, p, eta_next, gb_next, s2_next, st, stream);
+    else launch_eta_form<false>(P, neta, eta, s2, p, eta_next, gb_next, s2_next, st, stream);
 }
 
 void launch_step_finalize(const StepPartial* partials, int nblocks, DevBudget* budget, Status* st, int accept_mode,

@@ -154,3 +154,22 @@ def test_verified_division_matches_ieee(require_gpu, b):
     tested = ctypes.c_longlong(0)
     bad = L.nicr_check_division(b, 1 << 27, 12345, ctypes.byref(tested))
     assert bad == 0 and tested.value > (1 << 26)
+
+
+@pytest.mark.parametrize("dim,mode", [(3, "evolving"), (3, "static"), (2, "evolving")])
+def test_fast_form_deviation_from_drop_in(require_gpu, dim, mode):
+    """NICR_FP64_FAST (reciprocal divisions) stays within 1e-10 relative L-inf of
+    the bit-identical form after 200 steps of the regression-like case."""
+    shape = SHAPES[dim][1]
+    kw = dict(bc="concentration", ck="legacy", nucleation="off", **MODES[mode])
+    exact = nicr.Solver(cfg_for(dim, shape, **kw))
+    fast = nicr.Solver(cfg_for(dim, shape, precision=1, **kw))
+    o, cr, p, eta = smooth_fields(shape, exact.n_eta, seed=11)
+    for s in (exact, fast):
+        s.set_fields(o, cr, p, eta if eta else None)
+        s.step(200)
+    names = ["o", "cr", "p"] + [f"eta{g + 1}" for g in range(exact.n_eta)]
+    for n in names:
+        a, b = fast.get(n), exact.get(n)
+        err = np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300)
+        assert err <= 1e-10, (n, err)
