@@ -517,6 +517,108 @@ __global__ void k_eta_update(const StepParams P, int neta, const double* __restr
     if (errkey != ERR_NONE) atomicMin(&st->err_key, errkey);
 }
 
+// X-marching form of the eta update for a compile-time number of fields N:
+// each thread owns one (row, col) column of a chunk of planes and keeps
+// eta(x-1), eta(x), eta(x+1) of its column in registers, so each field value
+// is read from HBM once; the four in-plane neighbours come from L1 (they are
+// the neighbouring threads' own loads). All N loads of the next plane are
+// issued before the arithmetic of the current plane.
+template <int DIM, bool FAST, int N>
+__global__ void __launch_bounds__(256)
+k_eta_march(const StepParams P, const double* __restrict__ eta, const double* __restrict__ p,
+            double* __restrict__ eta_next, double* __restrict__ gb_next, double* __restrict__ s2_next, Status* st) {
+    if (st->failed) return;
+    const Grid& g = P.g;
+    const int col = blockIdx.x * blockDim.x + threadIdx.x;
+    const int row = DIM == 3 ? blockIdx.y * blockDim.y + threadIdx.y : 0;
+    if (col >= g.nb || row >= g.na) return;
+    const int i0 = blockIdx.z * P.xchunk, i1 = min(g.nx, i0 + P.xchunk);
+    const long long rc = (long long)row * g.pb + col;
+    const long long cbm = (long long)row * g.pb + (col == 0 ? g.nb - 1 : col - 1);
+    const long long cbp = (long long)row * g.pb + (col == g.nb - 1 ? 0 : col + 1);
+    long long cam = rc, cap = rc;
+    if (DIM == 3) {
+        cam = (long long)(row == 0 ? g.na - 1 : row - 1) * g.pb + col;
+        cap = (long long)(row == g.na - 1 ? 0 : row + 1) * g.pb + col;
+    }
+    double ep[N], ec[N], en[N];
+    {
+        const long long bm = (long long)(i0 > 0 ? i0 - 1 : 0) * g.plane, b0 = (long long)i0 * g.plane;
+#pragma unroll
+        for (int q = 0; q < N; ++q) {
+            ep[q] = __ldg(eta + (long long)q * g.nstore + bm + rc);
+            ec[q] = __ldg(eta + (long long)q * g.nstore + b0 + rc);
+        }
+    }
+    unsigned long long errkey = ERR_NONE;
+    for (int x = i0; x < i1; ++x) {
+        const long long base = (long long)x * g.plane;
+        const long long bnext = (long long)(x < g.nx - 1 ? x + 1 : x) * g.plane;
+#pragma unroll
+        for (int q = 0; q < N; ++q) en[q] = __ldg(eta + (long long)q * g.nstore + bnext + rc);
+        const double phi = __ldg(p + base + rc);
+        double S = 0.;
+#pragma unroll
+        for (int q = 0; q < N; ++q) S += ec[q] * ec[q];
+        const long long cell = ((long long)x * g.na + row) * g.nb + col;
+        double Sn = 0., pairs = 0.;
+#pragma unroll
+        for (int q = 0; q < N; ++q) {
+            const double* e = eta + (long long)q * g.nstore + base;
+            const double c0 = ec[q];
+            double lap;
+            if (DIM == 3)
+                lap = fdiv<FAST>((en[q] - 2. * c0 + ep[q]), P.v_dxdx)
+                    + fdiv<FAST>((__ldg(e + cap) - 2. * c0 + __ldg(e + cam)), P.v_dada)
+                    + fdiv<FAST>((__ldg(e + cbp) - 2. * c0 + __ldg(e + cbm)), P.v_dbdb);
+            else
+                lap = fdiv<FAST>((en[q] - 2. * c0 + ep[q]), P.v_dxdx)
+                    + fdiv<FAST>((__ldg(e + cbp) - 2. * c0 + __ldg(e + cbm)), P.v_dbdb);
+            const double force = grain_deta(c0, S, phi, P.eta_W, P.eta_A) - P.eta_K * lap;
+            const double v = c0 - P.dt_etaL * force;
+            if (!isfinite(v) || v < -1.e-12 || v > 1. + 1.e-12)
+                errkey = min(errkey, ERR_ETA_BASE + (unsigned long long)q * (unsigned long long)g.ncells + (unsigned long long)cell);
+            eta_next[(long long)q * g.nstore + base + rc] = v;
+            const double sq = v * v;
+            pairs += Sn * sq;
+            Sn += sq;
+        }
+        s2_next[base + rc] = Sn;
+        gb_next[base + rc] = P.eta_scale * smin(1., 16. * pairs);
+#pragma unroll
+        for (int q = 0; q < N; ++q) { ep[q] = ec[q]; ec[q] = en[q]; }
+    }
+    if (errkey != ERR_NONE) atomicMin(&st->err_key, errkey);
+}
+
+template <int DIM, bool FAST, int N>
+static void launch_eta_march(const StepParams& P, const double* eta, const double* p, double* eta_next,
+                             double* gb_next, double* s2_next, Status* st, cudaStream_t stream) {
+    const Grid& g = P.g;
+    if (DIM == 3) {
+        const dim3 grid((g.nb + 31) / 32, (g.na + 7) / 8, (g.nx + P.xchunk - 1) / P.xchunk);
+        k_eta_march<3, FAST, N><<<grid, dim3(32, 8), 0, stream>>>(P, eta, p, eta_next, gb_next, s2_next, st);
+    } else {
+        const dim3 grid((g.nb + 127) / 128, 1, (g.nx + P.xchunk - 1) / P.xchunk);
+        k_eta_march<2, FAST, N><<<grid, dim3(128, 1), 0, stream>>>(P, eta, p, eta_next, gb_next, s2_next, st);
+    }
+}
+
+// Dispatch to the compile-time field counts 1..16; false when N is larger.
+template <int DIM, bool FAST>
+static bool eta_march_dispatch(int neta, const StepParams& P, const double* eta, const double* p, double* eta_next,
+                               double* gb_next, double* s2_next, Status* st, cudaStream_t stream) {
+    switch (neta) {
+#define NICR_ETA_CASE(n) \
+    case n: launch_eta_march<DIM, FAST, n>(P, eta, p, eta_next, gb_next, s2_next, st, stream); return true;
+        NICR_ETA_CASE(1) NICR_ETA_CASE(2) NICR_ETA_CASE(3) NICR_ETA_CASE(4) NICR_ETA_CASE(5) NICR_ETA_CASE(6)
+        NICR_ETA_CASE(7) NICR_ETA_CASE(8) NICR_ETA_CASE(9) NICR_ETA_CASE(10) NICR_ETA_CASE(11) NICR_ETA_CASE(12)
+        NICR_ETA_CASE(13) NICR_ETA_CASE(14) NICR_ETA_CASE(15) NICR_ETA_CASE(16)
+#undef NICR_ETA_CASE
+        default: return false;
+    }
+}
+
 // Streaming form of the eta update: each CTA owns a rows x columns tile,
 // marches along X and stages every eta plane once (radius-1 halo) in a
 // three-plane shared-memory ring, so every field is read from HBM about once.
@@ -773,13 +875,23 @@ template <bool FAST>
 static void launch_eta_form(const StepParams& P, int neta, const double* eta, const double* s2, const double* p,
                             double* eta_next, double* gb_next, double* s2_next, Status* st, cudaStream_t stream) {
     const Grid& g = P.g;
-    // The per-cell kernel (stencil neighbours through L1/L2) is the default: the
-    // streaming kernel stalls on its per-plane barriers until the next plane
-    // has arrived. NICR_ETA_KERNEL=stream selects it for tuning runs.
-    static int simple = -1;
+    // The streaming kernel stalls on its per-plane barriers until the next
+    // plane has arrived; it is kept only as a tuning option.
+    // Kernel choice (measured on B200 at 256^3 with 8 fields): the X-marching
+    // kernel for the reciprocal form (0.63 ms vs 0.94 ms per step), the
+    // per-cell kernel for the drop-in form, where the unrolled verified
+    // divisions of the marching kernel cost more than its saved loads (1.84 ms
+    // vs 1.29 ms). NICR_ETA_KERNEL=march|simple|stream overrides for tuning.
+    static int simple = -1, march = -1;
     if (simple < 0) {
         const char* e = getenv("NICR_ETA_KERNEL");
         simple = (e && e[0] == 's' && e[1] == 't') ? 0 : 1;
+        march = e ? (e[0] == 'm' ? 1 : 0) : -2;
+    }
+    if (march == 1 || (march == -2 && FAST)) {
+        const bool done = g.dim == 3 ? eta_march_dispatch<3, FAST>(neta, P, eta, p, eta_next, gb_next, s2_next, st, stream)
+                                     : eta_march_dispatch<2, FAST>(neta, P, eta, p, eta_next, gb_next, s2_next, st, stream);
+        if (done) return;
     }
     if (g.dim == 3) {
         constexpr int TA = 8, TB = 32, S1 = (TA + 2) * (TB + 2);
