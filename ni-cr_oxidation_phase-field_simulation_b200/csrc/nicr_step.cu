@@ -174,6 +174,37 @@ struct StepKernel {
         }
     }
 
+    // Software pipelining of the staging: the loads of a later plane are issued
+    // into registers before the arithmetic of the current plane and stored to
+    // shared memory after it, so their latency overlaps the computation.
+    struct Prefetch {
+        double o[2], cr[2], p[2];
+    };
+    __device__ static void fetch(const StepParams& P, const double* __restrict__ o, const double* __restrict__ cr,
+                                 const double* __restrict__ p, int xoc, int xp, const Offs& f, Prefetch& r) {
+        const Grid& g = P.g;
+        const int xo = xoc < 0 ? 0 : (xoc > g.nx - 1 ? g.nx - 1 : xoc);
+        const int xq = xp < 0 ? 0 : (xp > g.nx - 1 ? g.nx - 1 : xp);
+        const bool inlet = P.inlet && xo == 0;
+        const long long bo = (long long)xo * g.plane, bq = (long long)xq * g.plane;
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            if (f.o2[k] >= 0) {
+                r.o[k] = inlet ? P.layer_o : __ldg(o + bo + f.o2[k]);
+                r.cr[k] = __ldg(cr + bo + f.o2[k]);
+            }
+            if (f.o1[k] >= 0) r.p[k] = __ldg(p + bq + f.o1[k]);
+        }
+    }
+    __device__ static void store(const Prefetch& r, double* so, double* scr, double* sp, const Offs& f) {
+        const int tid = threadIdx.x + TB * threadIdx.y;
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            if (f.o2[k] >= 0) { so[tid + k * T::NT] = r.o[k]; scr[tid + k * T::NT] = r.cr[k]; }
+            if (f.o1[k] >= 0) sp[tid + k * T::NT] = r.p[k];
+        }
+    }
+
     // mu and M at tile point (a,b) of real plane x; writes the mu/M slot.
     __device__ static CenterVals lead_point(const StepParams& P, const double* __restrict__ gb,
                                             const double* som, const double* so0, const double* sop,
@@ -302,12 +333,14 @@ struct StepKernel {
             pP = Pv.p;
         }
 
+        Prefetch pf;
+        if (i0 + 1 <= g.nx - 1) fetch(P, o, cr, p, i0 + 2, i0 + 1, offs, pf);
         for (int u = i0; u < i1; ++u) {
             const int x = u + 1;
             if (x <= g.nx - 1) {
-                load_oc(P, o, cr, x + 1, oslot(x + 1), cslot(x + 1), offs);
-                load_p(P, p, x, pslot(x), offs);
+                store(pf, oslot(x + 1), cslot(x + 1), pslot(x), offs);
                 __syncthreads();
+                if (x + 1 <= g.nx - 1 && u + 1 < i1) fetch(P, o, cr, p, x + 2, x + 1, offs, pf);
                 L = lead(x);
                 __syncthreads();
             } else {
@@ -810,14 +843,15 @@ int step_main_blocks(const StepParams& P) {
     return (int)(grid.x * grid.y * grid.z);
 }
 
-// Occupancy variant of the 3D step kernel: 3 CTAs/SM (80 registers, the
-// default, measured faster on B200) or 2 CTAs/SM (no register cap).
-// NICR_STEP_MINB=2|3 selects one for tuning runs.
+// Occupancy variant of the 3D step kernel: 2 CTAs/SM (no register cap, the
+// default: with the staging loads software-pipelined it is measured faster on
+// B200) or 3 CTAs/SM (80 registers, which spills). NICR_STEP_MINB=2|3 selects
+// one for tuning runs.
 static int step_minb() {
     static int v = 0;
     if (!v) {
         const char* e = getenv("NICR_STEP_MINB");
-        v = (e && e[0] == '2') ? 2 : 3;
+        v = (e && e[0] == '3') ? 3 : 2;
     }
     return v;
 }
