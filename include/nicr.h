@@ -228,6 +228,39 @@ int nicr_step_noalloc(const nicr_config* cfg, const double* o, const double* cr,
                       const double* gb, const double* eta_s2, double* o_next, double* cr_next,
                       double* p_next, nicr_step_result* result, void* stream);
 
+/* Batched multi-domain form: n independent domains on one device (all
+ * cfgs[i].device equal), e.g. a parameter sweep of many small grids. Each
+ * domain is created exactly as nicr_create(&cfgs[i]) would create it and
+ * evolves exactly as its own handle would (same kernels, same reduction
+ * order: fields and budgets are bit-identical to n separate handles); the
+ * batch only changes the launch structure of a step: one step launch per
+ * group of up to 48 consecutive domains of one dimensionality and precision,
+ * one commit launch for all domains, all on the batch's stream. The
+ * reference runs one domain per program (3S:1309-1395); there is no
+ * counterpart of the batch itself.
+ *
+ * nicr_batch_domain returns a borrowed handle of domain i for every per-domain
+ * call of this header (fields, budgets, diagnostics, writers, nucleate,
+ * stamp); nicr_destroy ignores it, nicr_batch_destroy frees it. Running a
+ * borrowed handle on its own (nicr_step/nicr_run) is allowed and uses the
+ * batch's stream. nicr_batch_step advances every domain nsteps steps
+ * (Model::step), nicr_batch_run follows each domain's run() schedule (Ksp
+ * scans); completed[i] (n entries, may be NULL) receives the accepted steps of
+ * domain i. A domain whose trial fails stops at its last accepted state, as
+ * nicr_run leaves a handle, while the others complete; the return value is
+ * the status of the first failing domain (NICR_OK when none failed) and
+ * nicr_batch_last_error names it ("domain i: <message>"). */
+typedef struct nicr_batch nicr_batch;
+int nicr_batch_create(const nicr_config* cfgs, int n, nicr_batch** out);
+void nicr_batch_destroy(nicr_batch* b);
+int nicr_batch_size(const nicr_batch* b);
+nicr_handle* nicr_batch_domain(nicr_batch* b, int i);
+int nicr_batch_step(nicr_batch* b, int nsteps, int* completed);
+int nicr_batch_run(nicr_batch* b, int nsteps, int* completed);
+const char* nicr_batch_last_error(const nicr_batch* b);
+long long nicr_batch_kernel_launches(const nicr_batch* b);
+void* nicr_batch_stream(const nicr_batch* b);
+
 /* The solver program: the reference's run()/main() for dim 2 or 3
  * (2D:1161-1246, 3S:1309-1395), argv as the reference's executable takes it.
  * Returns the process exit code. */

@@ -1,0 +1,177 @@
+// Batched multi-domain form: many independent domains of one device advanced
+// together. Each domain is an ordinary Model (its own buffers, initialisation,
+// Ksp schedule, budgets and failure handling, all identical to a single
+// handle); what the batch changes is the launch structure of a step: one
+// k_step_batch launch per group of up to kBatchMax domains instead of one
+// step launch per domain, and one finalize launch for all domains, all on the
+// batch's stream. Small domains (32^3..96^3) would otherwise leave the GPU
+// launch-bound and mostly idle.
+#include <algorithm>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/nicr.h"
+#include "nicr_model.h"
+
+struct nicr_batch {
+    std::vector<nicr_handle*> doms;
+    cudaStream_t stream = nullptr;
+    int device = 0;
+    std::string err;
+    long long launches = 0;   // batch-level launches (grouped step + finalize)
+
+    ~nicr_batch() {
+        if (stream) cudaStreamSynchronize(stream);
+        for (nicr_handle* h : doms) {
+            delete h->m;
+            delete h;
+        }
+        if (stream) cudaStreamDestroy(stream);
+    }
+
+    // Advances every domain nsteps steps (run() schedule when `schedule`).
+    int advance(int nsteps, int* completed, bool schedule) {
+        const int n = (int)doms.size();
+        if (completed)
+            for (int i = 0; i < n; ++i) completed[i] = 0;
+        if (nsteps <= 0) return NICR_OK;
+        std::vector<nicr::Model::RunPlan> plans((size_t)n);
+        std::vector<nicr::BatchDomain> descs((size_t)n);
+        std::vector<nicr::FinalizeDomain> fins((size_t)n);
+        for (int i = 0; i < n; ++i) doms[i]->m->run_begin(plans[i], nsteps, schedule);
+        for (int s = 0; s < nsteps; ++s) {
+            for (int i = 0; i < n; ++i) {
+                nicr::Model& m = *doms[i]->m;
+                m.run_pre_step(plans[i], s);
+                m.prepare_step();
+                descs[i] = m.step_desc();
+            }
+            launches += nicr::launch_step_batch(descs.data(), n, stream);
+            for (int i = 0; i < n; ++i) {
+                nicr::Model& m = *doms[i]->m;
+                m.complete_step(descs[i].nblocks, false);
+                fins[i] = m.finalize_desc(descs[i].nblocks);
+            }
+            nicr::launch_finalize_batch(fins.data(), n, stream);
+            launches += (n + nicr::kFinalizeMax - 1) / nicr::kFinalizeMax;
+        }
+        int rc = NICR_OK;
+        err.clear();
+        for (int i = 0; i < n; ++i) {
+            nicr::Model& m = *doms[i]->m;
+            const int r = m.run_end(plans[i], completed ? completed + i : nullptr);
+            if (r != NICR_OK) {
+                doms[i]->err = m.last_error;
+                if (rc == NICR_OK) {
+                    rc = r;
+                    err = "domain " + std::to_string(i) + ": " + m.last_error;
+                }
+            }
+        }
+        return rc;
+    }
+};
+
+namespace {
+thread_local std::string g_batch_error;
+
+template <class Fn>
+int batch_guarded(nicr_batch* b, Fn fn) {
+    if (!b) return NICR_ERR_INVALID_ARG;
+    try {
+        return fn(*b);
+    } catch (const nicr::Error& e) {
+        b->err = e.what();
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        b->err = "host allocation failed";
+        return NICR_ERR_STATE;
+    } catch (const std::exception& e) {
+        b->err = e.what();
+        return NICR_ERR_STATE;
+    }
+}
+}  // namespace
+
+extern "C" {
+
+int nicr_batch_create(const nicr_config* cfgs, int n, nicr_batch** out) {
+    if (!out) return NICR_ERR_INVALID_ARG;
+    *out = nullptr;
+    if (!cfgs || n <= 0) {
+        g_batch_error = "a batch needs at least one configuration";
+        return NICR_ERR_INVALID_ARG;
+    }
+    for (int i = 1; i < n; ++i)
+        if (cfgs[i].device != cfgs[0].device) {
+            g_batch_error = "all domains of a batch must use the same device";
+            return NICR_ERR_INVALID_ARG;
+        }
+    nicr_batch* b = nullptr;
+    try {
+        b = new nicr_batch;
+        b->device = cfgs[0].device;
+        int count = 0;
+        if (cudaGetDeviceCount(&count) != cudaSuccess || b->device < 0 || b->device >= count) {
+            delete b;
+            g_batch_error = "no CUDA device " + std::to_string(cfgs[0].device);
+            return NICR_ERR_NO_DEVICE;
+        }
+        nicr::check_cuda(cudaSetDevice(b->device), "cudaSetDevice");
+        nicr::check_cuda(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        b->doms.reserve((size_t)n);
+        for (int i = 0; i < n; ++i) {
+            auto* h = new nicr_handle;
+            h->borrowed = true;
+            try {
+                h->m = new nicr::Model(cfgs[i]);
+            } catch (...) {
+                delete h;
+                throw;
+            }
+            b->doms.push_back(h);
+            h->m->adopt_stream(b->stream);
+        }
+        *out = b;
+        return NICR_OK;
+    } catch (const nicr::Error& e) {
+        g_batch_error = e.what();
+        delete b;
+        return e.code;
+    } catch (const std::exception& e) {
+        g_batch_error = e.what();
+        delete b;
+        return NICR_ERR_STATE;
+    }
+}
+
+void nicr_batch_destroy(nicr_batch* b) { delete b; }
+
+int nicr_batch_size(const nicr_batch* b) { return b ? (int)b->doms.size() : 0; }
+
+nicr_handle* nicr_batch_domain(nicr_batch* b, int i) {
+    if (!b || i < 0 || i >= (int)b->doms.size()) return nullptr;
+    return b->doms[(size_t)i];
+}
+
+int nicr_batch_step(nicr_batch* b, int nsteps, int* completed) {
+    return batch_guarded(b, [&](nicr_batch& bb) { return bb.advance(nsteps, completed, false); });
+}
+
+int nicr_batch_run(nicr_batch* b, int nsteps, int* completed) {
+    return batch_guarded(b, [&](nicr_batch& bb) { return bb.advance(nsteps, completed, true); });
+}
+
+const char* nicr_batch_last_error(const nicr_batch* b) { return b ? b->err.c_str() : g_batch_error.c_str(); }
+
+long long nicr_batch_kernel_launches(const nicr_batch* b) {
+    if (!b) return 0;
+    long long n = b->launches;
+    for (const nicr_handle* h : b->doms) n += h->m->launches;
+    return n;
+}
+
+void* nicr_batch_stream(const nicr_batch* b) { return b ? static_cast<void*>(b->stream) : nullptr; }
+
+}  // extern "C"

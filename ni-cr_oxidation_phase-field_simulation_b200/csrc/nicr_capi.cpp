@@ -57,7 +57,7 @@ int nicr_create(const nicr_config* cfg, nicr_handle** out) {
 }
 
 void nicr_destroy(nicr_handle* h) {
-    if (!h) return;
+    if (!h || h->borrowed) return;
     delete h->m;
     delete h;
 }

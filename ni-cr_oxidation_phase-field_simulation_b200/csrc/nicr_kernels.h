@@ -83,6 +83,39 @@ void launch_eta_mask(const StepParams& P, int neta, const double* eta, double* g
 void launch_eta_update(const StepParams& P, int neta, const double* eta, const double* s2,
                        const double* p, double* eta_next, double* gb_next, double* s2_next,
                        Status* st, cudaStream_t stream);
+// Batched step of many domains in one launch per group of <= kBatchMax domains
+// of one dimensionality and arithmetic form (consecutive entries). Each entry
+// carries the domain's parameters and buffers; gx, gy, block0 are filled by the
+// launcher, nblocks (the domain's partial-sum count) is written back.
+struct BatchDomain {
+    StepParams sp;
+    const double *o, *cr, *p, *gb, *s2;
+    double *on, *crn, *pn;
+    StepPartial* partials;
+    Status* st;
+    int gx, gy, block0, nblocks;
+};
+constexpr int kBatchMax = 48;   // 48 entries: ~24 KB of kernel parameters (limit 32 KB)
+struct StepBatch {
+    int n, pad;
+    BatchDomain d[kBatchMax];
+};
+// returns the number of launches
+int launch_step_batch(BatchDomain* doms, int n, cudaStream_t stream);
+
+struct FinalizeDomain {
+    const StepPartial* partials;
+    int nblocks, pad;
+    DevBudget* budget;
+    Status* st;
+};
+constexpr int kFinalizeMax = 512;
+struct FinalizeBatch {
+    int n, pad;
+    FinalizeDomain d[kFinalizeMax];
+};
+void launch_finalize_batch(const FinalizeDomain* doms, int n, cudaStream_t stream);
+
 // Commit of one step: reduce partials, commit budget unless a trial failed
 void launch_step_finalize(const StepPartial* partials, int nblocks, DevBudget* budget, Status* st,
                           int accept_mode, cudaStream_t stream);

@@ -180,7 +180,7 @@ void Model::release() {
     if (h_st) cudaFreeHost(h_st);
     for (cudaEvent_t e : prof_pool) cudaEventDestroy(e);
     prof_pool.clear();
-    if (stream) cudaStreamDestroy(stream);
+    if (stream && owns_stream) cudaStreamDestroy(stream);
     std::memset(o_, 0, sizeof o_); std::memset(cr_, 0, sizeof cr_); std::memset(p_, 0, sizeof p_);
     std::memset(gb_, 0, sizeof gb_); std::memset(s2_, 0, sizeof s2_); std::memset(eta_, 0, sizeof eta_);
     grain = pairs = gb_initial = muO = muCr = mo = mc = nullptr;
@@ -615,24 +615,55 @@ void Model::reset_status() {
     check_cuda(cudaMemcpyAsync(st, h_st, sizeof(Status), cudaMemcpyHostToDevice, stream), "H2D");
 }
 
-void Model::enqueue_step() {
-    const int nxt = cur ^ 1;
+void Model::prepare_step() {
     if (has_eta && eta_dirty) eta_mask_now();
-    int nb = 0;
-    size_t e = prof_begin();
-    launch_step_main(sp, o_[cur], cr_[cur], p_[cur], gb_[gcur], has_eta ? s2_[gcur] : nullptr, o_[nxt], cr_[nxt],
-                     p_[nxt], partials, st, stream, &nb);
-    prof_end(K_STEP_MAIN, e, 1);
+}
+
+BatchDomain Model::step_desc() const {
+    BatchDomain d{};
+    const int nxt = cur ^ 1;
+    d.sp = sp;
+    d.o = o_[cur]; d.cr = cr_[cur]; d.p = p_[cur];
+    d.gb = gb_[gcur];
+    d.s2 = has_eta ? s2_[gcur] : nullptr;
+    d.on = o_[nxt]; d.crn = cr_[nxt]; d.pn = p_[nxt];
+    d.partials = partials;
+    d.st = st;
+    return d;
+}
+
+FinalizeDomain Model::finalize_desc(int nb) const {
+    FinalizeDomain f{};
+    f.partials = partials;
+    f.nblocks = nb;
+    f.budget = bud;
+    f.st = st;
+    return f;
+}
+
+void Model::complete_step(int nb, bool finalize) {
     if (advance_eta) {
-        e = prof_begin();
+        const size_t e = prof_begin();
         launch_eta_update(sp, neta, eta_[ecur], s2_[gcur], p_[cur], eta_[ecur ^ 1], gb_[gcur ^ 1], s2_[gcur ^ 1], st, stream);
         prof_end(K_ETA_UPDATE, e, 1);
     }
-    e = prof_begin();
-    launch_step_finalize(partials, nb, bud, st, 0, stream);
-    prof_end(K_FINALIZE, e, 1);
-    cur = nxt;
+    if (finalize) {
+        const size_t e = prof_begin();
+        launch_step_finalize(partials, nb, bud, st, 0, stream);
+        prof_end(K_FINALIZE, e, 1);
+    }
+    cur ^= 1;
     if (advance_eta) { ecur ^= 1; gcur ^= 1; }
+}
+
+void Model::enqueue_step() {
+    prepare_step();
+    const BatchDomain d = step_desc();
+    int nb = 0;
+    const size_t e = prof_begin();
+    launch_step_main(sp, d.o, d.cr, d.p, d.gb, d.s2, d.on, d.crn, d.pn, partials, st, stream, &nb);
+    prof_end(K_STEP_MAIN, e, 1);
+    complete_step(nb, true);
 }
 
 std::string Model::describe_failure(unsigned long long key, int nxt) {
@@ -705,40 +736,64 @@ int Model::finish_batch(long long before, int enqueued, const std::vector<double
     return NICR_ERR_ETA_RANGE;
 }
 
+void Model::run_begin(RunPlan& r, int nsteps, bool schedule) {
+    reset_status();
+    r.before = steps_done;
+    r.nsteps = nsteps;
+    r.schedule = schedule;
+    r.next = next_nucleation;
+    r.sched.assign(schedule ? (size_t)nsteps + 1 : 0, 0.);
+}
+
+void Model::run_pre_step(RunPlan& r, int s) {
+    if (!r.schedule) return;
+    const long long n = r.before + s + 1;
+    const double time = double(n) * c.dt;
+    if (c.nucleation == NICR_NUC_KSP && time + 1.e-12 * c.nucleation_period >= r.next) {
+        kd.neta = neta;
+        const size_t e = prof_begin();
+        launch_ksp_scan(kd, o_[cur], cr_[cur], p_[cur], eta_[ecur], kw, bud, kres, st, stream);
+        prof_end(K_KSP, e, 4);
+        if (has_eta) eta_dirty = true;
+        r.next += c.nucleation_period;
+    }
+    r.sched[(size_t)s] = r.next;
+}
+
+int Model::run_end(RunPlan& r, int* completed) {
+    if (!r.schedule) return finish_batch(r.before, r.nsteps, nullptr, completed);
+    r.sched[(size_t)r.nsteps] = r.next;
+    const int rc = finish_batch(r.before, r.nsteps, &r.sched, completed);
+    if (rc == NICR_OK) next_nucleation = r.next;
+    return rc;
+}
+
 int Model::step(int nsteps, int* completed) {
     if (completed) *completed = 0;
     if (nsteps <= 0) return NICR_OK;
-    reset_status();
-    const long long before = steps_done;
+    RunPlan r;
+    run_begin(r, nsteps, false);
     for (int s = 0; s < nsteps; ++s) enqueue_step();
-    return finish_batch(before, nsteps, nullptr, completed);
+    return run_end(r, completed);
 }
 
 int Model::run(int nsteps, int* completed) {
     if (completed) *completed = 0;
     if (nsteps <= 0) return NICR_OK;
-    reset_status();
-    const long long before = steps_done;
-    std::vector<double> sched((size_t)nsteps + 1);
-    double next = next_nucleation;
+    RunPlan r;
+    run_begin(r, nsteps, true);
     for (int s = 0; s < nsteps; ++s) {
-        const long long n = before + s + 1;
-        const double time = double(n) * c.dt;
-        if (c.nucleation == NICR_NUC_KSP && time + 1.e-12 * c.nucleation_period >= next) {
-            kd.neta = neta;
-            const size_t e = prof_begin();
-            launch_ksp_scan(kd, o_[cur], cr_[cur], p_[cur], eta_[ecur], kw, bud, kres, st, stream);
-            prof_end(K_KSP, e, 4);
-            if (has_eta) eta_dirty = true;
-            next += c.nucleation_period;
-        }
-        sched[s] = next;
+        run_pre_step(r, s);
         enqueue_step();
     }
-    sched[nsteps] = next;
-    const int rc = finish_batch(before, nsteps, &sched, completed);
-    if (rc == NICR_OK) next_nucleation = next;
-    return rc;
+    return run_end(r, completed);
+}
+
+void Model::adopt_stream(cudaStream_t s) {
+    sync();
+    if (stream && owns_stream) cudaStreamDestroy(stream);
+    stream = s;
+    owns_stream = false;
 }
 
 int Model::nucleate(int* nuclei) {

@@ -48,6 +48,9 @@ public:
     std::string last_error;
 
     cudaStream_t stream = nullptr;
+    bool owns_stream = true;
+    // Use stream s (owned by the caller, e.g. a batch) for all further work.
+    void adopt_stream(cudaStream_t s);
 
     // ---- API used by the C-ABI
     void set_field(int field, int index, const double* host);
@@ -74,6 +77,26 @@ public:
     double prof_ms[K_COUNT] = {};
     long long prof_n[K_COUNT] = {};
     long long launches = 0;
+
+    // One step split into phases, for batches that launch the step kernel of
+    // many domains at once: prepare_step (eta mask when stale), step_desc (the
+    // step kernel's parameters and buffers), then complete_step (eta update,
+    // optional finalize, buffer parity). run_begin / run_pre_step / run_end are
+    // run()'s schedule (Ksp scans) and commit around those steps.
+    struct RunPlan {
+        long long before = 0;
+        int nsteps = 0;
+        bool schedule = false;
+        double next = 0.;
+        std::vector<double> sched;
+    };
+    void prepare_step();
+    BatchDomain step_desc() const;
+    FinalizeDomain finalize_desc(int nblocks) const;
+    void complete_step(int nblocks, bool finalize);
+    void run_begin(RunPlan& r, int nsteps, bool schedule);
+    void run_pre_step(RunPlan& r, int s);
+    int run_end(RunPlan& r, int* completed);
 
     // raw device pointers of the current state (for tests, bench, writers)
     double* d_o() const { return o_[cur]; }
@@ -162,4 +185,5 @@ private:
 struct nicr_handle {
     nicr::Model* m = nullptr;
     std::string err;
+    bool borrowed = false;   // a domain owned by a nicr_batch: nicr_destroy leaves it alone
 };

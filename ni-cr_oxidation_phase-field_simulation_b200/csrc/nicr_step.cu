@@ -245,7 +245,7 @@ struct StepKernel {
                                const double* __restrict__ p, const double* __restrict__ gb,
                                const double* __restrict__ s2, double* __restrict__ on,
                                double* __restrict__ crn, double* __restrict__ pn,
-                               StepPartial* __restrict__ partials, Status* st) {
+                               StepPartial* __restrict__ partials, Status* st, int bx, int by, int bz, int blin) {
         extern __shared__ __align__(16) double smem[];
         double* so = smem;                 // 3 slots x S2
         double* scr = so + 3 * T::S2;      // 3 slots x S2
@@ -259,12 +259,11 @@ struct StepKernel {
 
         const Grid& g = P.g;
         const int ta = DIM == 3 ? threadIdx.y : 0, tb = threadIdx.x;
-        const int a0 = DIM == 3 ? blockIdx.y * TA : 0, b0 = blockIdx.x * TB;
-        const int i0 = blockIdx.z * P.xchunk;
+        const int a0 = DIM == 3 ? by * TA : 0, b0 = bx * TB;
+        const int i0 = bz * P.xchunk;
         const int i1 = min(g.nx, i0 + P.xchunk);
         const int row = a0 + ta, col = b0 + tb;
         const bool active = (DIM == 3 ? row < g.na : true) && col < g.nb;
-        const int blin = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
         const Offs offs = make_offs(g, a0, b0);
 
         DD acc[5] = {{0., 0.}, {0., 0.}, {0., 0.}, {0., 0.}, {0., 0.}};  // ckO ckCr clipO clipCr bcO
@@ -458,7 +457,8 @@ k_step_main(const StepParams P, const double* __restrict__ o, const double* __re
             const double* __restrict__ p, const double* __restrict__ gb, const double* __restrict__ s2,
             double* __restrict__ on, double* __restrict__ crn, double* __restrict__ pn,
             StepPartial* __restrict__ partials, Status* st) {
-    StepKernel<DIM, TA, TB, FAST>::run(P, o, cr, p, gb, s2, on, crn, pn, partials, st);
+    StepKernel<DIM, TA, TB, FAST>::run(P, o, cr, p, gb, s2, on, crn, pn, partials, st, blockIdx.x, blockIdx.y,
+                                       blockIdx.z, blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z));
 }
 
 constexpr int TA3 = 8, TB3 = 32;    // 3D tile: 8 rows x 32 columns, 256 threads
@@ -501,16 +501,12 @@ __global__ void k_eta_mask(const StepParams P, int neta, const double* __restric
 // [-1e-12, 1+1e-12]. Writes the trial and the mask of the trial values (the
 // next step's gb and eta_s2, identical to rebuild_eta_mask on them).
 template <int DIM, bool FAST>
-__global__ void k_eta_update(const StepParams P, int neta, const double* __restrict__ eta,
-                             const double* __restrict__ s2, const double* __restrict__ p,
-                             double* __restrict__ eta_next, double* __restrict__ gb_next,
-                             double* __restrict__ s2_next, Status* st) {
-    if (st->failed) return;
+__device__ __forceinline__ void eta_cell(const StepParams& P, int neta, const double* __restrict__ eta,
+                                         const double* __restrict__ s2, const double* __restrict__ p,
+                                         double* __restrict__ eta_next, double* __restrict__ gb_next,
+                                         double* __restrict__ s2_next, int x, int row, int col,
+                                         unsigned long long& errkey) {
     const Grid& g = P.g;
-    const int col = blockIdx.x * blockDim.x + threadIdx.x;
-    const int row = DIM == 3 ? blockIdx.y * blockDim.y + threadIdx.y : 0;
-    const int x = blockIdx.z;
-    if (col >= g.nb || row >= g.na) return;
     const long long idx = (long long)x * g.plane + (long long)row * g.pb + col;
     const long long cell = ((long long)x * g.na + row) * g.nb + col;
     const long long ixm = x > 0 ? idx - g.plane : idx, ixp = x < g.nx - 1 ? idx + g.plane : idx;
@@ -523,7 +519,6 @@ __global__ void k_eta_update(const StepParams P, int neta, const double* __restr
         iap = rbase + (long long)(row == g.na - 1 ? 0 : row + 1) * g.pb + col;
     }
     const double S = __ldg(s2 + idx), phi = __ldg(p + idx);
-    unsigned long long errkey = ERR_NONE;
     double Sn = 0., pairs = 0.;
     for (int q = 0; q < neta; ++q) {
         const double* e = eta + (long long)q * g.nstore;
@@ -547,6 +542,20 @@ __global__ void k_eta_update(const StepParams P, int neta, const double* __restr
     }
     s2_next[idx] = Sn;
     gb_next[idx] = P.eta_scale * smin(1., 16. * pairs);
+}
+
+template <int DIM, bool FAST>
+__global__ void k_eta_update(const StepParams P, int neta, const double* __restrict__ eta,
+                             const double* __restrict__ s2, const double* __restrict__ p,
+                             double* __restrict__ eta_next, double* __restrict__ gb_next,
+                             double* __restrict__ s2_next, Status* st) {
+    if (st->failed) return;
+    const Grid& g = P.g;
+    const int col = blockIdx.x * blockDim.x + threadIdx.x;
+    const int row = DIM == 3 ? blockIdx.y * blockDim.y + threadIdx.y : 0;
+    if (col >= g.nb || row >= g.na) return;
+    unsigned long long errkey = ERR_NONE;
+    eta_cell<DIM, FAST>(P, neta, eta, s2, p, eta_next, gb_next, s2_next, blockIdx.z, row, col, errkey);
     if (errkey != ERR_NONE) atomicMin(&st->err_key, errkey);
 }
 
@@ -556,16 +565,19 @@ __global__ void k_eta_update(const StepParams P, int neta, const double* __restr
 // is read from HBM once; the four in-plane neighbours come from L1 (they are
 // the neighbouring threads' own loads). All N loads of the next plane are
 // issued before the arithmetic of the current plane.
-template <int DIM, bool FAST, int N>
-__global__ void __launch_bounds__(256)
-k_eta_march(const StepParams P, const double* __restrict__ eta, const double* __restrict__ p,
-            double* __restrict__ eta_next, double* __restrict__ gb_next, double* __restrict__ s2_next, Status* st) {
+// NCAP is the register capacity; the first n <= NCAP fields are updated (the
+// stand-alone kernel instantiates NCAP = n, so the guards fold away).
+template <int DIM, bool FAST, int NCAP>
+__device__ __forceinline__ void eta_march_body(const StepParams& P, int n, const double* __restrict__ eta,
+                                               const double* __restrict__ p, double* __restrict__ eta_next,
+                                               double* __restrict__ gb_next, double* __restrict__ s2_next,
+                                               Status* st, int bx, int by, int bz) {
     if (st->failed) return;
     const Grid& g = P.g;
-    const int col = blockIdx.x * blockDim.x + threadIdx.x;
-    const int row = DIM == 3 ? blockIdx.y * blockDim.y + threadIdx.y : 0;
+    const int col = bx * blockDim.x + threadIdx.x;
+    const int row = DIM == 3 ? by * blockDim.y + threadIdx.y : 0;
     if (col >= g.nb || row >= g.na) return;
-    const int i0 = blockIdx.z * P.xchunk, i1 = min(g.nx, i0 + P.xchunk);
+    const int i0 = bz * P.xchunk, i1 = min(g.nx, i0 + P.xchunk);
     const long long rc = (long long)row * g.pb + col;
     const long long cbm = (long long)row * g.pb + (col == 0 ? g.nb - 1 : col - 1);
     const long long cbp = (long long)row * g.pb + (col == g.nb - 1 ? 0 : col + 1);
@@ -574,13 +586,15 @@ k_eta_march(const StepParams P, const double* __restrict__ eta, const double* __
         cam = (long long)(row == 0 ? g.na - 1 : row - 1) * g.pb + col;
         cap = (long long)(row == g.na - 1 ? 0 : row + 1) * g.pb + col;
     }
-    double ep[N], ec[N], en[N];
+    double ep[NCAP], ec[NCAP], en[NCAP];
     {
         const long long bm = (long long)(i0 > 0 ? i0 - 1 : 0) * g.plane, b0 = (long long)i0 * g.plane;
 #pragma unroll
-        for (int q = 0; q < N; ++q) {
-            ep[q] = __ldg(eta + (long long)q * g.nstore + bm + rc);
-            ec[q] = __ldg(eta + (long long)q * g.nstore + b0 + rc);
+        for (int q = 0; q < NCAP; ++q) {
+            if (q < n) {
+                ep[q] = __ldg(eta + (long long)q * g.nstore + bm + rc);
+                ec[q] = __ldg(eta + (long long)q * g.nstore + b0 + rc);
+            }
         }
     }
     unsigned long long errkey = ERR_NONE;
@@ -588,15 +602,18 @@ k_eta_march(const StepParams P, const double* __restrict__ eta, const double* __
         const long long base = (long long)x * g.plane;
         const long long bnext = (long long)(x < g.nx - 1 ? x + 1 : x) * g.plane;
 #pragma unroll
-        for (int q = 0; q < N; ++q) en[q] = __ldg(eta + (long long)q * g.nstore + bnext + rc);
+        for (int q = 0; q < NCAP; ++q)
+            if (q < n) en[q] = __ldg(eta + (long long)q * g.nstore + bnext + rc);
         const double phi = __ldg(p + base + rc);
         double S = 0.;
 #pragma unroll
-        for (int q = 0; q < N; ++q) S += ec[q] * ec[q];
+        for (int q = 0; q < NCAP; ++q)
+            if (q < n) S += ec[q] * ec[q];
         const long long cell = ((long long)x * g.na + row) * g.nb + col;
         double Sn = 0., pairs = 0.;
 #pragma unroll
-        for (int q = 0; q < N; ++q) {
+        for (int q = 0; q < NCAP; ++q) {
+            if (q >= n) break;
             const double* e = eta + (long long)q * g.nstore + base;
             const double c0 = ec[q];
             double lap;
@@ -619,9 +636,17 @@ k_eta_march(const StepParams P, const double* __restrict__ eta, const double* __
         s2_next[base + rc] = Sn;
         gb_next[base + rc] = P.eta_scale * smin(1., 16. * pairs);
 #pragma unroll
-        for (int q = 0; q < N; ++q) { ep[q] = ec[q]; ec[q] = en[q]; }
+        for (int q = 0; q < NCAP; ++q)
+            if (q < n) { ep[q] = ec[q]; ec[q] = en[q]; }
     }
     if (errkey != ERR_NONE) atomicMin(&st->err_key, errkey);
+}
+
+template <int DIM, bool FAST, int N>
+__global__ void __launch_bounds__(256)
+k_eta_march(const StepParams P, const double* __restrict__ eta, const double* __restrict__ p,
+            double* __restrict__ eta_next, double* __restrict__ gb_next, double* __restrict__ s2_next, Status* st) {
+    eta_march_body<DIM, FAST, N>(P, N, eta, p, eta_next, gb_next, s2_next, st, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 template <int DIM, bool FAST, int N>
@@ -767,8 +792,8 @@ __global__ void k_check_division(DivC d, long long n, unsigned long long seed, u
 
 // Step commit: partial sums in block order (deterministic), then the budget is
 // advanced only when no trial failed (fields swap only on acceptance, 3S:821).
-__global__ void k_step_finalize(const StepPartial* __restrict__ partials, int nblocks, DevBudget* budget,
-                                Status* st, int accept_mode) {
+__device__ __forceinline__ void finalize_body(const StepPartial* __restrict__ partials, int nblocks,
+                                              DevBudget* budget, Status* st, int accept_mode) {
     __shared__ DD sdd[32 * 5];
     __shared__ long long scnt[32];
     if (st->failed) return;
@@ -797,6 +822,39 @@ __global__ void k_step_finalize(const StepPartial* __restrict__ partials, int nb
             st->steps_done += 1;
         }
     }
+}
+
+__global__ void k_step_finalize(const StepPartial* __restrict__ partials, int nblocks, DevBudget* budget,
+                                Status* st, int accept_mode) {
+    finalize_body(partials, nblocks, budget, st, accept_mode);
+}
+
+// Batched commit: block b commits domain b (same arithmetic as k_step_finalize).
+__global__ void k_finalize_batch(const __grid_constant__ FinalizeBatch B) {
+    const FinalizeDomain& d = B.d[blockIdx.x];
+    finalize_body(d.partials, d.nblocks, d.budget, d.st, 0);
+}
+
+// Batched step: one launch advances up to kBatchMax domains of one
+// dimensionality and arithmetic form. The per-domain parameters and buffers
+// sit in the kernel's parameter space (read through the constant cache with a
+// block-uniform index); block b belongs to the last domain whose first block
+// is <= b and runs exactly the CTA (bx, by, bz) the single-domain launch would
+// run, with the same partial-sum slot, so every domain's result is identical
+// to its own nicr_step.
+template <int DIM, int TA, int TB, int MINB, bool FAST>
+__global__ void __launch_bounds__(TA * TB, MINB) k_step_batch(const __grid_constant__ StepBatch B) {
+    int lo = 0, hi = B.n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (B.d[mid].block0 <= (int)blockIdx.x) lo = mid;
+        else hi = mid - 1;
+    }
+    const BatchDomain& D = B.d[lo];
+    const int t = (int)blockIdx.x - D.block0;
+    const int bx = t % D.gx, r = t / D.gx, by = r % D.gy, bz = r / D.gy;
+    StepKernel<DIM, TA, TB, FAST>::run(D.sp, D.o, D.cr, D.p, D.gb, D.s2, D.on, D.crn, D.pn, D.partials, D.st, bx, by,
+                                       bz, t);
 }
 
 // refresh() for output: mu at interior cells, M at interior cells.
@@ -971,6 +1029,58 @@ void launch_eta_update(const StepParams& P, int neta, const double* eta, const d
 void launch_step_finalize(const StepPartial* partials, int nblocks, DevBudget* budget, Status* st, int accept_mode,
                           cudaStream_t stream) {
     k_step_finalize<<<1, 256, 0, stream>>>(partials, nblocks, budget, st, accept_mode);
+}
+
+void launch_finalize_batch(const FinalizeDomain* doms, int n, cudaStream_t stream) {
+    for (int i0 = 0; i0 < n; i0 += kFinalizeMax) {
+        FinalizeBatch B{};
+        B.n = n - i0 < kFinalizeMax ? n - i0 : kFinalizeMax;
+        for (int i = 0; i < B.n; ++i) B.d[i] = doms[i0 + i];
+        k_finalize_batch<<<B.n, 256, 0, stream>>>(B);
+    }
+}
+
+template <int DIM, int TA, int TB, int MINB, bool FAST>
+static void launch_batch_group(StepBatch& B, int nblocks, cudaStream_t stream) {
+    using T = Tile<DIM, TA, TB>;
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_step_batch<DIM, TA, TB, MINB, FAST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)T::SMEM_BYTES);
+        attr = true;
+    }
+    k_step_batch<DIM, TA, TB, MINB, FAST><<<nblocks, dim3(TB, TA), T::SMEM_BYTES, stream>>>(B);
+}
+
+int launch_step_batch(BatchDomain* doms, int n, cudaStream_t stream) {
+    int launches = 0;
+    int i = 0;
+    while (i < n) {
+        // a group: consecutive domains of one dimensionality and form, at most kBatchMax
+        StepBatch B{};
+        const int dim = doms[i].sp.g.dim, fast = doms[i].sp.fast;
+        int nb = 0;
+        while (i < n && B.n < kBatchMax && doms[i].sp.g.dim == dim && doms[i].sp.fast == fast) {
+            BatchDomain d = doms[i];
+            const dim3 grid = dim == 3 ? step_grid<3, TA3, TB3>(d.sp) : step_grid<2, TA2, TB2>(d.sp);
+            d.gx = (int)grid.x;
+            d.gy = (int)grid.y;
+            d.block0 = nb;
+            nb += (int)(grid.x * grid.y * grid.z);
+            doms[i].nblocks = (int)(grid.x * grid.y * grid.z);
+            B.d[B.n++] = d;
+            ++i;
+        }
+        if (dim == 3) {
+            if (fast) launch_batch_group<3, TA3, TB3, 2, true>(B, nb, stream);
+            else launch_batch_group<3, TA3, TB3, 2, false>(B, nb, stream);
+        } else {
+            if (fast) launch_batch_group<2, TA2, TB2, 4, true>(B, nb, stream);
+            else launch_batch_group<2, TA2, TB2, 4, false>(B, nb, stream);
+        }
+        ++launches;
+    }
+    return launches;
 }
 
 void launch_refresh(const StepParams& P, const double* o, const double* cr, const double* p, const double* gb,

@@ -101,6 +101,22 @@ def lib():
     L.nicr_main.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_char_p)]
     L.nicr_stream.argtypes = [H]
     L.nicr_stream.restype = ctypes.c_void_p
+    L.nicr_batch_create.argtypes = [ctypes.POINTER(NicrConfig), ctypes.c_int, ctypes.POINTER(H)]
+    L.nicr_batch_destroy.argtypes = [H]
+    L.nicr_batch_destroy.restype = None
+    L.nicr_batch_size.argtypes = [H]
+    L.nicr_batch_domain.argtypes = [H, ctypes.c_int]
+    L.nicr_batch_domain.restype = H
+    L.nicr_batch_step.argtypes = [H, ctypes.c_int, ip]
+    L.nicr_batch_run.argtypes = [H, ctypes.c_int, ip]
+    L.nicr_batch_last_error.argtypes = [H]
+    L.nicr_batch_last_error.restype = ctypes.c_char_p
+    L.nicr_batch_kernel_launches.argtypes = [H]
+    L.nicr_batch_kernel_launches.restype = ctypes.c_longlong
+    L.nicr_batch_stream.argtypes = [H]
+    L.nicr_batch_stream.restype = ctypes.c_void_p
+    L.nicr_kernel_launches.argtypes = [H]
+    L.nicr_kernel_launches.restype = ctypes.c_longlong
     _lib = L
     return L
 
@@ -135,17 +151,33 @@ class Solver:
         if cfg is None:
             cfg = make_config(dim, **kw)
         self.cfg = cfg
+        self.owner = None
         self.h = ctypes.c_void_p()
         rc = lib().nicr_create(ctypes.byref(cfg), ctypes.byref(self.h))
         if rc != 0:
             raise NicrError(rc, lib().nicr_last_error(None).decode())
+        self._describe()
+
+    def _describe(self):
+        cfg = self.cfg
         self.info_ = self.info()
         self.shape = (cfg.nx, cfg.ny, cfg.nz) if cfg.dim == 3 else (cfg.nx, cfg.ny)
         self.n = int(np.prod(self.shape))
 
+    @classmethod
+    def _borrowed(cls, handle: int, cfg: NicrConfig, owner):
+        """A domain handle owned by a Batch (freed with the batch)."""
+        s = cls.__new__(cls)
+        s.cfg = cfg
+        s.owner = owner
+        s.h = ctypes.c_void_p(handle)
+        s._describe()
+        return s
+
     def close(self):
         if getattr(self, "h", None) and self.h.value:
-            lib().nicr_destroy(self.h)
+            if getattr(self, "owner", None) is None:
+                lib().nicr_destroy(self.h)
             self.h = ctypes.c_void_p()
 
     def __del__(self):
@@ -294,6 +326,71 @@ class Solver:
 
     def stream(self) -> int:
         return lib().nicr_stream(self.h) or 0
+
+
+class Batch:
+    """Independent domains on one GPU advanced together (nicr_batch_*): one
+    step launch per group of up to 48 domains, one commit launch per step.
+    ``domains[i]`` is a Solver view of domain i (owned by the batch)."""
+
+    def __init__(self, cfgs):
+        cfgs = list(cfgs)
+        arr = (NicrConfig * len(cfgs))(*cfgs)
+        self.b = ctypes.c_void_p()
+        rc = lib().nicr_batch_create(arr, len(cfgs), ctypes.byref(self.b))
+        if rc != 0:
+            raise NicrError(rc, lib().nicr_batch_last_error(None).decode())
+        self.domains = [Solver._borrowed(lib().nicr_batch_domain(self.b, i), cfgs[i], self)
+                        for i in range(len(cfgs))]
+
+    def __len__(self):
+        return len(self.domains)
+
+    def close(self):
+        if getattr(self, "b", None) and self.b.value:
+            for d in self.domains:
+                d.h = ctypes.c_void_p()
+            lib().nicr_batch_destroy(self.b)
+            self.b = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def last_error(self) -> str:
+        return lib().nicr_batch_last_error(self.b).decode()
+
+    def _advance(self, fn, n: int, check: bool):
+        done = (ctypes.c_int * len(self.domains))()
+        rc = fn(self.b, n, done)
+        if check and rc != 0:
+            raise NicrError(rc, self.last_error)
+        return list(done), rc
+
+    def step(self, n: int = 1, check: bool = True):
+        """Model::step x n on every domain; returns (completed per domain, status)."""
+        return self._advance(lib().nicr_batch_step, n, check)
+
+    def run(self, n: int, check: bool = True):
+        """n steps of every domain on its run() schedule (Ksp scans)."""
+        return self._advance(lib().nicr_batch_run, n, check)
+
+    @property
+    def kernel_launches(self) -> int:
+        return int(lib().nicr_batch_kernel_launches(self.b))
+
+    @property
+    def stream(self) -> int:
+        return lib().nicr_batch_stream(self.b) or 0
 
 
 def main(dim: int, argv: list[str]) -> int:
