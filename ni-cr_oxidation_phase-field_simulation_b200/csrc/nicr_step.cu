@@ -72,8 +72,8 @@ struct Tile {
     static constexpr int RA2 = TA + 2 * HA2, RB2 = TB + 4;
     static constexpr int RA1 = TA + 2 * HA1, RB1 = TB + 2;
     static constexpr int S2 = RA2 * RB2, S1 = RA1 * RB1;
-    // shared memory: o[3], cr[3] (halo 2); p[3] (halo 1); muO, muCr, mo, mc [2] (halo 1)
-    static constexpr int SMEM_DOUBLES = 6 * S2 + 3 * S1 + 8 * S1;
+    // shared memory: o[4], cr[4] (halo 2); p[3] (halo 1); muO, muCr, mo, mc [2] (halo 1)
+    static constexpr int SMEM_DOUBLES = 8 * S2 + 3 * S1 + 8 * S1;
     static constexpr size_t SMEM_BYTES = SMEM_DOUBLES * sizeof(double) + 64 * (5 * 16 + 8);
     static constexpr int NT = TA * TB;
     __device__ static int i2(int a, int b) { return (a + HA2) * RB2 + (b + 2); }
@@ -179,9 +179,22 @@ struct StepKernel {
     // shared memory after it, so their latency overlaps the computation.
     struct Prefetch {
         double o[2], cr[2], p[2];
+        double gbl[2];   // gb at the lead points (own cell, ring point) of the next lead plane
+        double s2;       // eta_s2 at the own cell of the next update plane
     };
+    // gb at the lead points of plane x (0 when grains are off)
+    __device__ static void fetch_gb(const StepParams& P, const double* __restrict__ gb, int x, const Offs& f,
+                                    double (&r)[2]) {
+        const long long base = (long long)x * P.g.plane;
+        r[0] = P.grains ? __ldg(gb + base + f.gl[0]) : 0.;
+        r[1] = (P.grains && f.gl[1] >= 0) ? __ldg(gb + base + f.gl[1]) : 0.;
+    }
     __device__ static void fetch(const StepParams& P, const double* __restrict__ o, const double* __restrict__ cr,
-                                 const double* __restrict__ p, int xoc, int xp, const Offs& f, Prefetch& r) {
+                                 const double* __restrict__ p, const double* __restrict__ gb,
+                                 const double* __restrict__ s2, int xoc, int xp, int xs, bool own, const Offs& f,
+                                 Prefetch& r) {
+        fetch_gb(P, gb, xp, f, r.gbl);
+        r.s2 = (P.phi_eta && own) ? __ldg(s2 + (long long)xs * P.g.plane + f.gl[0]) : 0.;
         const Grid& g = P.g;
         const int xo = xoc < 0 ? 0 : (xoc > g.nx - 1 ? g.nx - 1 : xoc);
         const int xq = xp < 0 ? 0 : (xp > g.nx - 1 ? g.nx - 1 : xp);
@@ -210,7 +223,7 @@ struct StepKernel {
                                             const double* som, const double* so0, const double* sop,
                                             const double* scm, const double* sc0, const double* scp,
                                             const double* sp, double* smuO, double* smuCr, double* smo,
-                                            double* smc, int x, int a, int b, int goff) {
+                                            double* smc, int a, int b, double gbv) {
         const int c2 = T::i2(a, b);
         const double oc = so0[c2], cc = sc0[c2];
         double lapO, lapC;
@@ -234,7 +247,6 @@ struct StepKernel {
         v.o = oc; v.cr = cc; v.p = pc; v.hh = hh;
         v.muO = mu_o_local(oc, cc, hh) - 2. * Phys::ko * lapO;
         v.muCr = mu_cr_local(oc, cc, hh) - 2. * Phys::kc * lapC;
-        const double gbv = P.grains ? __ldg(gb + (long long)x * P.g.plane + goff) : 0.;
         v.mo = P.o_on ? mobility(oc, hh, gbv, Phys::bmo, Phys::boo, P.gbm1_o) : 0.;
         v.mc = mobility(cc, hh, gbv, Phys::bmc, Phys::boc, P.gbm1_cr);
         smuO[c1] = v.muO; smuCr[c1] = v.muCr; smo[c1] = v.mo; smc[c1] = v.mc;
@@ -247,9 +259,9 @@ struct StepKernel {
                                double* __restrict__ crn, double* __restrict__ pn,
                                StepPartial* __restrict__ partials, Status* st, int bx, int by, int bz, int blin) {
         extern __shared__ __align__(16) double smem[];
-        double* so = smem;                 // 3 slots x S2
-        double* scr = so + 3 * T::S2;      // 3 slots x S2
-        double* sp = scr + 3 * T::S2;      // 3 slots x S1
+        double* so = smem;                 // 4 slots x S2
+        double* scr = so + 4 * T::S2;      // 4 slots x S2
+        double* sp = scr + 4 * T::S2;      // 3 slots x S1
         double* smuO = sp + 3 * T::S1;     // 2 slots x S1
         double* smuCr = smuO + 2 * T::S1;
         double* smo = smuCr + 2 * T::S1;
@@ -273,12 +285,15 @@ struct StepKernel {
         if (st->failed) return;  // a previous step of this batch was rejected
 
         auto slot3 = [](int w) { return ((w % 3) + 3) % 3; };
-        auto oslot = [&](int w) { return so + slot3(w) * T::S2; };
-        auto cslot = [&](int w) { return scr + slot3(w) * T::S2; };
+        // o/cr ring of 4 planes: the plane staged at the top of an iteration
+        // (x+2) never overlaps the window x-1..x+1 that slower warps may still
+        // be reading in lead(x), so one barrier per plane suffices
+        auto oslot = [&](int w) { return so + (w & 3) * T::S2; };
+        auto cslot = [&](int w) { return scr + (w & 3) * T::S2; };
         auto pslot = [&](int x) { return sp + slot3(x) * T::S1; };
 
         // Computes the lead plane x (real plane) over the tile + radius-1 halo.
-        auto lead = [&](int x) -> CenterVals {
+        auto lead = [&](int x, const double (&gbl)[2]) -> CenterVals {
             const double *som = oslot(x - 1), *so0 = oslot(x), *sop = oslot(x + 1);
             const double *scm = cslot(x - 1), *sc0 = cslot(x), *scp = cslot(x + 1);
             const double* spx = pslot(x);
@@ -286,14 +301,14 @@ struct StepKernel {
             double* mC = smuCr + (x & 1) * T::S1;
             double* mo_ = smo + (x & 1) * T::S1;
             double* mc_ = smc + (x & 1) * T::S1;
-            CenterVals own = lead_point(P, gb, som, so0, sop, scm, sc0, scp, spx, mO, mC, mo_, mc_, x, ta, tb, offs.gl[0]);
+            CenterVals own = lead_point(P, gb, som, so0, sop, scm, sc0, scp, spx, mO, mC, mo_, mc_, ta, tb, gbl[0]);
             // halo ring points: one per thread for the first S1-NT threads
             static_assert(T::S1 - T::NT <= T::NT, "ring larger than the CTA");
             const int tid = threadIdx.x + TB * threadIdx.y;
             if (offs.gl[1] >= 0) {
                 int a, b;
                 ring_point(tid, a, b);
-                lead_point(P, gb, som, so0, sop, scm, sc0, scp, spx, mO, mC, mo_, mc_, x, a, b, offs.gl[1]);
+                lead_point(P, gb, som, so0, sop, scm, sc0, scp, spx, mO, mC, mo_, mc_, a, b, gbl[1]);
             }
             return own;
         };
@@ -306,8 +321,10 @@ struct StepKernel {
             load_oc(P, o, cr, 0, oslot(0), cslot(0), offs);
             load_oc(P, o, cr, 1, oslot(1), cslot(1), offs);
             load_p(P, p, 0, pslot(0), offs);
+            double gb0[2];
+            fetch_gb(P, gb, 0, offs, gb0);
             __syncthreads();
-            C = lead(0);
+            C = lead(0, gb0);
             __syncthreads();
             // ghost plane -1: copies of plane 0 (3S:187, 3S:613-615, 3S:616-619)
             const double muOg = (P.bc == 1 && P.o_on) ? 2. * P.mu_res - C.muO : C.muO;
@@ -319,31 +336,44 @@ struct StepKernel {
             load_oc(P, o, cr, i0 - 1, oslot(i0 - 1), cslot(i0 - 1), offs);
             load_oc(P, o, cr, i0, oslot(i0), cslot(i0), offs);
             load_p(P, p, i0 - 1, pslot(i0 - 1), offs);
+            double gbm[2];
+            fetch_gb(P, gb, i0 - 1, offs, gbm);
             __syncthreads();
-            const CenterVals Pv = lead(i0 - 1);
-            __syncthreads();  // window i0-2 (read by lead(i0-1)) shares a ring slot with i0+1
+            const CenterVals Pv = lead(i0 - 1, gbm);
             load_oc(P, o, cr, i0 + 1, oslot(i0 + 1), cslot(i0 + 1), offs);
             load_p(P, p, i0, pslot(i0), offs);
+            double gb0[2];
+            fetch_gb(P, gb, i0, offs, gb0);
             __syncthreads();
-            C = lead(i0);
+            C = lead(i0, gb0);
             __syncthreads();
             FxO = fdiv<FAST>(-.5 * (Pv.mo + C.mo) * (C.muO - Pv.muO), P.v_dx);
             FxCr = fdiv<FAST>(-.5 * (Pv.mc + C.mc) * (C.muCr - Pv.muCr), P.v_dx);
             pP = Pv.p;
         }
 
+        double s2u = (P.phi_eta && active) ? __ldg(s2 + (long long)i0 * g.plane + offs.gl[0]) : 0.;
         Prefetch pf;
-        if (i0 + 1 <= g.nx - 1) fetch(P, o, cr, p, i0 + 2, i0 + 1, offs, pf);
+        if (i0 + 1 <= g.nx - 1) fetch(P, o, cr, p, gb, s2, i0 + 2, i0 + 1, i0 + 1, active, offs, pf);
         for (int u = i0; u < i1; ++u) {
             const int x = u + 1;
+            double s2n = 0.;
             if (x <= g.nx - 1) {
+                // one barrier per plane: it orders this plane's staging before
+                // lead(x), and the previous update(u-1) (which read the mu/M
+                // slot lead(x) now overwrites) before lead(x)
                 store(pf, oslot(x + 1), cslot(x + 1), pslot(x), offs);
+                const double gbl[2] = {pf.gbl[0], pf.gbl[1]};
+                s2n = pf.s2;
                 __syncthreads();
-                if (x + 1 <= g.nx - 1 && u + 1 < i1) fetch(P, o, cr, p, x + 2, x + 1, offs, pf);
-                L = lead(x);
-                __syncthreads();
+                if (x + 1 <= g.nx - 1 && u + 1 < i1)
+                    fetch(P, o, cr, p, gb, s2, x + 2, x + 1, x + 1, active, offs, pf);
+                L = lead(x, gbl);
             } else {
                 L = C;  // ghost plane nx: Neumann copy of plane nx-1 (mu and M copied too)
+                // no staging in this iteration, but update(nx-1) reads the mu/M
+                // that lead(nx-1) of other warps wrote in the previous one
+                __syncthreads();
             }
             if (active) {
                 const double* mO = smuO + (u & 1) * T::S1;
@@ -411,7 +441,7 @@ struct StepKernel {
                 const double hpv = 30. * pp * pp * (pp - 1.) * (pp - 1.);
                 double fp = Phys::W * (4. * pp * pp * pp - 6. * pp * pp + 2. * pp)
                           + hpv * (foxide(oo, cc) - fmetal(oo, cc)) - 2. * Phys::kp * lapP;
-                if (P.phi_eta) fp += grain_dphi(__ldg(s2 + gidx), pp, P.eta_W, P.eta_A);
+                if (P.phi_eta) fp += grain_dphi(s2u, pp, P.eta_W, P.eta_A);
                 double pnv = pp - P.dtL * fp;
                 if (P.ck == 0) {
                     const double hn = h(pnv);
@@ -440,6 +470,7 @@ struct StepKernel {
             }
             pP = C.p;
             C = L;
+            s2u = s2n;
         }
         if (errkey != ERR_NONE) atomicMin(&st->err_key, errkey);
         block_reduce_dd<5>(acc, clipped, sdd, scnt);

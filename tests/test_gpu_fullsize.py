@@ -1,0 +1,66 @@
+"""Parity at the benchmark's full size: 3D 256^3 with 8 evolving eta (the
+bench.py workload: Voronoi seed 2, Cr 0.25 +- 0.01, O inlet, Ksp, legacy Ck
+and bounds). The tile/X-chunk decomposition, the CTA count and the per-CTA
+budget partials at this size are the ones the benchmark times, so the drop-in
+form is checked bit for bit against the oracle here, and the reciprocal form
+for run-to-run determinism and its deviation from the drop-in form."""
+import numpy as np
+import pytest
+
+import bench
+import nicr
+from oracle import Oracle
+from parity import assert_bitexact, assert_budget
+
+pytestmark = pytest.mark.gpu
+
+SIZE, NETA = 256, 8
+
+
+def bench_inputs(shape, inlet_cr):
+    cr = 0.25 + np.random.default_rng(2).uniform(-0.01, 0.01, size=shape)
+    cr[0] = inlet_cr
+    return cr
+
+
+def make_solver(precision):
+    cfg = bench.workload_config(SIZE, NETA, device=0, seed=2)
+    cfg.precision = precision
+    sol = nicr.Solver(cfg)
+    sol.set("cr", bench_inputs(sol.shape, sol.get("cr")[0]))
+    sol.reset_inventory()
+    return sol
+
+
+def test_full_size_drop_in_matches_oracle(require_gpu):
+    sol = make_solver(0)
+    orc = Oracle(bench.workload_config(SIZE, NETA, device=0, seed=2))
+    assert orc.neta == NETA
+    eta = np.array([orc.get(f"eta{g + 1}") for g in range(NETA)])
+    orc.set_fields(orc.get("o"), bench_inputs(orc.shape, orc.get("cr")[0]), orc.get("p"), eta)
+    orc.reset_inventory()
+    rc, done = orc.run(3)
+    assert rc == 0 and done == 3
+    sol.run(3)
+    orc.refresh()   # eta_s2 of the current eta, as the handle reports it
+    for f in ("o", "cr", "p"):
+        assert_bitexact(f, sol.get(f), orc.get(f))
+    for g in range(NETA):
+        assert_bitexact(f"eta{g + 1}", sol.get("eta", g), orc.get(f"eta{g + 1}"))
+    assert_bitexact("eta_s2", sol.get("eta_s2"), orc.get("eta_s2"))
+    assert_budget(sol.budget(), orc.budget())
+    sol.close()
+
+
+def test_full_size_fast_form_is_deterministic_and_close(require_gpu):
+    a, b, ref = make_solver(1), make_solver(1), make_solver(0)
+    for s in (a, b, ref):
+        s.run(8)
+    for f in ("o", "cr", "p"):
+        assert_bitexact(f"{f} run-to-run", a.get(f), b.get(f))
+        x, y = a.get(f), ref.get(f)
+        assert np.max(np.abs(x - y)) <= 1e-10 * max(np.max(np.abs(y)), 1e-300), f
+    for g in range(NETA):
+        assert_bitexact(f"eta{g + 1} run-to-run", a.get("eta", g), b.get("eta", g))
+    for s in (a, b, ref):
+        s.close()
