@@ -58,12 +58,14 @@ def workload_config(size: int, neta: int, device: int = 0, seed: int = 2):
                        bounds="legacy", nucleation="ksp", device=device)
 
 
-def algorithmic_bytes(kernel: str, neta: int) -> int:
-    """Compulsory HBM bytes per cell of one launch (each field read/written once)."""
+def algorithmic_bytes(kernel: str, neta: int, fast: bool) -> int:
+    """Compulsory HBM bytes per cell of one launch (each field it touches read or
+    written once). The reciprocal form's eta kernel (register marching along X)
+    rebuilds S = sum eta^2 from the eta it reads instead of reading eta_s2."""
     if kernel == "step_main":      # r: o cr p gb eta_s2   w: o cr p
         return 8 * 8
-    if kernel == "eta_update":     # r: eta_1..N eta_s2 p  w: eta_1..N gb eta_s2
-        return (2 * neta + 4) * 8
+    if kernel == "eta_update":     # r: eta_1..N [eta_s2] p  w: eta_1..N gb eta_s2
+        return (2 * neta + (3 if fast else 4)) * 8
     if kernel == "eta_mask":       # r: eta_1..N  w: gb eta_s2
         return (neta + 2) * 8
     return 0
@@ -77,13 +79,13 @@ def measured_peak_hbm():
     return 6650.0, "fallback"
 
 
-def ncu_traffic(kernel: str, size: int):
-    """DRAM bytes per launch from the committed ncu summary (scaled per cell)."""
+def ncu_traffic(kernel: str, size: int, form: str):
+    """DRAM bytes per launch from the committed ncu summary of this arithmetic
+    form ("fp64" or "fp64-fast"), scaled per cell to size^3."""
     p = ROOT / "profiles" / "traffic.json"
     if not p.exists():
         return None
-    d = json.loads(p.read_text())
-    e = d.get(kernel)
+    e = json.loads(p.read_text()).get(form, {}).get(kernel)
     if not e:
         return None
     return float(e["dram_bytes_per_cell"]) * size ** 3
@@ -302,9 +304,11 @@ def main():
     ms_max = float(t.item())
     value = world * n * args.steps / (ms_max * 1e-3) / 1e6
     form = "fp64-fast (reciprocal divisions; FP64 state and operation order)"
+    form_key = "fp64-fast"
     if not err <= 1e-4:
         # outside the metric's bound: the headline falls back to the drop-in form
         value, ms_max, prof, form = value_plain, float(tp.item()), prof_plain, "fp64 (drop-in)"
+        form_key = "fp64"
 
     # ---- end to end through the C-ABI with host buffers: upload the state from
     # pinned memory, one nicr_run(1) call per step (each returns the accept status
@@ -334,7 +338,7 @@ def main():
     peak, peak_kind = measured_peak_hbm()
     dom = max(prof, key=lambda k: prof[k][0]) if prof else "step_main"
     dom_ms = prof[dom][0] / prof[dom][1] if prof else ms_max / args.steps
-    algo = algorithmic_bytes(dom, args.neta) * n
+    algo = algorithmic_bytes(dom, args.neta, form_key == "fp64-fast" and args.neta <= 16) * n
     achieved = algo / (dom_ms * 1e-3) / 1e9
     step_bytes = (6 + 2 * args.neta) * 8          # fused-minimum bytes of one whole step per cell
     line = {
@@ -354,7 +358,7 @@ def main():
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind,
                      "algorithmic_bytes_per_launch": algo, "avg_launch_ms": dom_ms,
-                     "traffic": ncu_traffic(dom, args.size)},
+                     "traffic": ncu_traffic(dom, args.size, form_key)},
         "step_hbm": {"bytes_per_cell": step_bytes, "achieved": step_bytes * value * 1e6 / world / 1e9,
                      "frac": step_bytes * value * 1e6 / world / 1e9 / peak, "unit": "GB/s"},
         "kernels": {k: {"ms_per_launch": v[0] / v[1], "launches": v[1], "share": v[0] / sum(x[0] for x in prof.values())}
