@@ -228,6 +228,22 @@ int nicr_step_noalloc(const nicr_config* cfg, const double* o, const double* cr,
                       const double* gb, const double* eta_s2, double* o_next, double* cr_next,
                       double* p_next, nicr_step_result* result, void* stream);
 
+/* Checkpoint / restart (no counterpart in the reference, which cannot resume
+ * a run). nicr_save_state writes the handle's state to `path`: a header (the
+ * configuration, accepted steps, nucleation clock, budget, Voronoi seeds),
+ * then the refreshed interior fields o, cr, p, muO, muCr, mo, mc, gb,
+ * [eta_s2], eta_1..N in the order and layout of the reference's
+ * snapshot_state dump (mpi3d-slab/tests/regression_driver.cpp:17-32: X
+ * slowest, Z fastest, FP64), then the grain map when kept and the 2D initial
+ * GB mask, and a checksum. nicr_load_state restores such a file into a handle
+ * created from the same configuration (run length, output options, device and
+ * arithmetic form may differ; any other difference is NICR_ERR_INVALID_ARG
+ * naming the field), after which stepping continues bit for bit as the
+ * uninterrupted run would. A truncated or corrupted file is rejected before
+ * the handle is touched. */
+int nicr_save_state(nicr_handle* h, const char* path);
+int nicr_load_state(nicr_handle* h, const char* path);
+
 /* Batched multi-domain form: n independent domains on one device (all
  * cfgs[i].device equal), e.g. a parameter sweep of many small grids. Each
  * domain is created exactly as nicr_create(&cfgs[i]) would create it and

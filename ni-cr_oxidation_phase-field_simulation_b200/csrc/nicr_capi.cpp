@@ -107,6 +107,22 @@ int nicr_get_field(nicr_handle* h, int field, int index, double* host) {
     });
 }
 
+int nicr_save_state(nicr_handle* h, const char* path) {
+    return guarded(h, [&](nicr::Model& m) {
+        if (!path) return (int)NICR_ERR_INVALID_ARG;
+        m.save_state(path);
+        return (int)NICR_OK;
+    });
+}
+
+int nicr_load_state(nicr_handle* h, const char* path) {
+    return guarded(h, [&](nicr::Model& m) {
+        if (!path) return (int)NICR_ERR_INVALID_ARG;
+        m.load_state(path);
+        return (int)NICR_OK;
+    });
+}
+
 int nicr_refresh(nicr_handle* h) {
     return guarded(h, [&](nicr::Model& m) { m.refresh(); m.sync(); return (int)NICR_OK; });
 }

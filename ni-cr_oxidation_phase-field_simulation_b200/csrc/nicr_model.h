@@ -66,6 +66,9 @@ public:
     void diagnostics(nicr_diagnostics* d);
     void grain_stats(nicr_grain_stats* s, long long* cells, double* amount);
     size_t device_bytes() const { return dev_bytes; }
+    // checkpoint / restart (nicr_checkpoint.cpp)
+    void save_state(const std::string& path);
+    void load_state(const std::string& path);
     void sync();
 
     // measurement hooks: CUDA events around every kernel launch (when enabled)

@@ -101,6 +101,8 @@ def lib():
     L.nicr_main.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_char_p)]
     L.nicr_stream.argtypes = [H]
     L.nicr_stream.restype = ctypes.c_void_p
+    L.nicr_save_state.argtypes = [H, ctypes.c_char_p]
+    L.nicr_load_state.argtypes = [H, ctypes.c_char_p]
     L.nicr_batch_create.argtypes = [ctypes.POINTER(NicrConfig), ctypes.c_int, ctypes.POINTER(H)]
     L.nicr_batch_destroy.argtypes = [H]
     L.nicr_batch_destroy.restype = None
@@ -303,6 +305,14 @@ class Solver:
         out["cells"] = cells[: self.n_eta]
         out["amount"] = amount[: 2 * self.n_eta].reshape(-1, 2)
         return out
+
+    def save(self, path):
+        """Checkpoint of the current state (nicr_save_state)."""
+        self._check(lib().nicr_save_state(self.h, str(path).encode()))
+
+    def load(self, path):
+        """Restores a checkpoint written from the same configuration (nicr_load_state)."""
+        self._check(lib().nicr_load_state(self.h, str(path).encode()))
 
     def write_vtk(self, path):
         self._check(lib().nicr_write_vtk(self.h, str(path).encode()))
