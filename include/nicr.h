@@ -193,6 +193,17 @@ int nicr_get_grain_stats(nicr_handle* h, nicr_grain_stats* s, long long* cells, 
  * byte where the values are bit-identical. */
 int nicr_write_vtk(nicr_handle* h, const char* path);          /* 2D:598-632, 3S:828-856 */
 int nicr_write_vti(nicr_handle* h, const char* path);          /* 3S:857-869, 238-334    */
+/* Asynchronous VTI frame (the reference writes synchronously, 3S:238-334).
+ * nicr_write_vti_async enqueues on the handle's stream the frame's arrays,
+ * built on the GPU in file order and type, and their copy to pinned host
+ * memory, then returns; a library thread compresses (64 KiB zlib blocks, in
+ * parallel) and writes the file while the caller keeps stepping. The file is
+ * byte-identical to nicr_write_vti's of the same state. One frame is in
+ * flight per handle: the next nicr_write_vti(_async) or nicr_output_wait
+ * first completes it and returns its error, if any (NICR_ERR_IO with the
+ * reference's message). nicr_destroy completes it too. */
+int nicr_write_vti_async(nicr_handle* h, const char* path);
+int nicr_output_wait(nicr_handle* h);
 int nicr_write_metadata(nicr_handle* h, const char* out_dir);  /* 2D:633-696, 3S:874-962 */
 /* Formats one diagnostics.csv row / grain rows for step n into buf.          */
 int nicr_format_log_row(nicr_handle* h, int n, char* buf, size_t len);

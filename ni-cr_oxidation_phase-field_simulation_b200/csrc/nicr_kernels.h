@@ -116,6 +116,16 @@ struct FinalizeBatch {
 };
 void launch_finalize_batch(const FinalizeDomain* doms, int n, cudaStream_t stream);
 
+// The seven arrays of a 3D VTI frame in file order (X fastest) and type, for
+// the output path (nicr_vti.cu). range gets bit a set when array a holds a
+// finite value outside the Float32 range.
+struct VtiArgs {
+    Grid g;
+    int has_eta, neta;
+    const double *p, *o, *cr, *muO, *muCr, *gb, *grain, *eta;
+};
+void launch_vti_arrays(const VtiArgs& a, void* out, bool f64, unsigned* range, cudaStream_t stream);
+
 // Commit of one step: reduce partials, commit budget unless a trial failed
 void launch_step_finalize(const StepPartial* partials, int nblocks, DevBudget* budget, Status* st,
                           int accept_mode, cudaStream_t stream);

@@ -166,7 +166,10 @@ Model::Model(const nicr_config& cfg) : c(cfg), dim(cfg.dim) {
     }
 }
 
-Model::~Model() { release(); }
+Model::~Model() {
+    output_writer.reset();   // finishes pending output before the buffers go
+    release();
+}
 
 void Model::release() {
     if (stream) cudaStreamSynchronize(stream);

@@ -5,6 +5,7 @@
 // Voronoi mask and eta weights) and the formatting of output files.
 #pragma once
 #include <cuda_runtime.h>
+#include <memory>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -49,6 +50,10 @@ public:
 
     cudaStream_t stream = nullptr;
     bool owns_stream = true;
+    // Output machinery that outlives single calls (the asynchronous VTI
+    // writer of nicr_output.cpp); released, after its pending writes, first
+    // thing in the destructor.
+    std::shared_ptr<void> output_writer;
     // Use stream s (owned by the caller, e.g. a batch) for all further work.
     void adopt_stream(cudaStream_t s);
 
@@ -107,6 +112,7 @@ public:
     double* d_p() const { return p_[cur]; }
     double* d_gb() const { return gb_[gcur]; }
     double* d_eta(int gi) const { return eta_[ecur] + (size_t)gi * g.nstore; }
+    double* d_grain() const { return grain; }
     StepParams params() const { return sp; }
     // device buffers the writers read (after refresh())
     const double* d_mu_o() const { return muO; }

@@ -10,6 +10,7 @@
 
 #include <algorithm>
 #include <array>
+#include <atomic>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -23,6 +24,7 @@
 #include <locale>
 #include <sstream>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/nicr.h"
@@ -180,124 +182,237 @@ void write_vtk3(Model& m, const std::string& path) {
 // ------------------------------------------------------------------ VTI
 // VTK XML ImageData, raw appended data, zlib blocks of 64 KiB with UInt64
 // headers (block count, block size, last block size, compressed sizes),
-// written to path.tmp and renamed on success.
-class VtiFile {
-    static constexpr std::uint64_t kBlock = 65536;
-    const nicr_config& c;
-    std::string final_path, temp_path;
-    std::ofstream f;
-    std::array<std::streampos, 7> offset_pos{};
-    std::streampos data_start;
-    size_t next = 0;
-    bool done = false;
-    void check() {
-        if (!f) throw nicr::Error(NICR_ERR_IO, "VTI write failed (check storage/quota): " + temp_path);
+// written to path.tmp and renamed on success (write_vti, 3S:238-334). The
+// arrays arrive in file order and type from the GPU (launch_vti_arrays); the
+// blocks are independent zlib streams, compressed here by a pool of host
+// threads, so the file is the same byte for byte as a serial writer's.
+constexpr std::uint64_t kVtiBlock = 65536;
+
+void put_u64(std::string& s, std::uint64_t v) {
+    for (int q = 0; q < 8; ++q) s.push_back((char)(unsigned char)(v >> (8 * q)));
+}
+
+void compose_vti(const nicr_config& c, const unsigned char* arrays, bool f64, const std::string& path) {
+    const std::uint64_t esz = f64 ? 8 : 4;
+    const std::uint64_t n = std::uint64_t(c.nx) * c.ny * c.nz, total = n * esz;
+    const std::uint64_t nb = (total + kVtiBlock - 1) / kVtiBlock;
+    const size_t narr = NAMES3.size(), jobs = narr * (size_t)nb;
+    std::vector<std::vector<unsigned char>> blocks(jobs);
+    std::atomic<size_t> next{0};
+    std::atomic<int> zrc{Z_OK};
+    auto work = [&] {
+        for (size_t b; (b = next.fetch_add(1)) < jobs;) {
+            const size_t arr = b / (size_t)nb;
+            const std::uint64_t bi = b % nb, off = bi * kVtiBlock;
+            const std::uint64_t len = std::min<std::uint64_t>(kVtiBlock, total - off);
+            std::vector<unsigned char>& dst = blocks[b];
+            dst.resize((size_t)compressBound((uLong)len));
+            uLongf dlen = (uLongf)dst.size();
+            const int rc = compress2(dst.data(), &dlen, arrays + arr * total + off, (uLong)len, c.compression_level);
+            if (rc != Z_OK) zrc = rc;
+            dst.resize(dlen);
+        }
+    };
+    const unsigned hw = std::thread::hardware_concurrency();
+    const size_t nthreads = std::min<size_t>(jobs, std::max(1u, std::min(hw, 32u)));
+    std::vector<std::thread> pool;
+    for (size_t t = 1; t < nthreads; ++t) pool.emplace_back(work);
+    work();
+    for (auto& t : pool) t.join();
+    if (zrc != Z_OK) throw nicr::Error(NICR_ERR_IO, "zlib compression failed: " + std::to_string(zrc.load()));
+
+    std::vector<std::uint64_t> offset(narr);
+    std::uint64_t run = 0;
+    for (size_t arr = 0; arr < narr; ++arr) {
+        offset[arr] = run;
+        run += 24 + 8 * nb;
+        for (std::uint64_t bi = 0; bi < nb; ++bi) run += blocks[arr * (size_t)nb + (size_t)bi].size();
     }
-    void u64(std::uint64_t v) {
-        unsigned char b[8];
-        for (int q = 0; q < 8; ++q) b[q] = (unsigned char)(v >> (8 * q));
-        f.write(reinterpret_cast<const char*>(b), 8);
+    std::ostringstream h;
+    h.imbue(std::locale::classic());
+    h << std::setprecision(17) << "<?xml version=\"1.0\"?>\n"
+      << "<VTKFile type=\"ImageData\" version=\"1.0\" byte_order=\"LittleEndian\" header_type=\"UInt64\" compressor=\"vtkZLibDataCompressor\">\n"
+      << " <ImageData WholeExtent=\"0 " << c.nx - 1 << " 0 " << c.ny - 1 << " 0 " << c.nz - 1 << "\" Origin=\""
+      << .5 * c.dx << " " << .5 * c.dy << " " << .5 * c.dz << "\" Spacing=\"" << c.dx << " " << c.dy << " " << c.dz
+      << "\">\n  <Piece Extent=\"0 " << c.nx - 1 << " 0 " << c.ny - 1 << " 0 " << c.nz - 1 << "\">\n"
+      << "   <PointData Scalars=\"phi\">\n";
+    for (size_t arr = 0; arr < narr; ++arr)
+        h << "    <DataArray type=\"" << (f64 ? "Float64" : "Float32") << "\" Name=\"" << NAMES3[arr]
+          << "\" NumberOfComponents=\"1\" format=\"appended\" offset=\"" << std::setw(20) << std::setfill('0')
+          << offset[arr] << std::setfill(' ') << "\"/>\n";
+    h << "   </PointData>\n   <CellData/>\n  </Piece>\n </ImageData>\n <AppendedData encoding=\"raw\">\n_";
+
+    const std::string temp = path + ".tmp";
+    std::ofstream f(temp, std::ios::binary | std::ios::trunc);
+    if (!f) throw nicr::Error(NICR_ERR_IO, "Cannot open " + temp);
+    auto fail = [&] {
+        f.close();
+        std::error_code ec;
+        fs::remove(temp, ec);
+        throw nicr::Error(NICR_ERR_IO, "VTI write failed (check storage/quota): " + temp);
+    };
+    const std::string head = h.str();
+    f.write(head.data(), (std::streamsize)head.size());
+    for (size_t arr = 0; arr < narr; ++arr) {
+        std::string bh;
+        put_u64(bh, nb);
+        put_u64(bh, kVtiBlock);
+        put_u64(bh, total % kVtiBlock);
+        for (std::uint64_t bi = 0; bi < nb; ++bi) put_u64(bh, blocks[arr * (size_t)nb + (size_t)bi].size());
+        f.write(bh.data(), (std::streamsize)bh.size());
+        for (std::uint64_t bi = 0; bi < nb; ++bi) {
+            const auto& blk = blocks[arr * (size_t)nb + (size_t)bi];
+            f.write(reinterpret_cast<const char*>(blk.data()), (std::streamsize)blk.size());
+        }
+        if (!f) fail();
+    }
+    f << "\n </AppendedData>\n</VTKFile>\n";
+    f.flush();
+    if (!f) fail();
+    f.close();
+    if (!f) fail();
+    fs::rename(temp, path);
+}
+
+// Asynchronous VTI writer of one model. submit() enqueues, on the model's
+// stream, the refresh of mu/M, the kernel that builds the frame's arrays in a
+// device staging buffer, and (on a copy stream, after an event) their copy to
+// pinned host memory; a host thread then waits for the copy, compresses and
+// writes the file while the model keeps stepping. One frame is in flight at a
+// time: submit() and wait() first finish the previous one and report its
+// error, if any.
+class AsyncVti {
+    int device = 0;
+    cudaStream_t copy = nullptr;
+    cudaEvent_t ready = nullptr, copied = nullptr;
+    void* d_stage = nullptr;
+    unsigned char* h_stage = nullptr;
+    unsigned* d_range = nullptr;
+    unsigned* h_range = nullptr;
+    size_t bytes = 0;
+    std::thread worker;
+    std::string error;
+    int error_code = NICR_OK;
+
+    void release_buffers() {
+        if (d_stage) cudaFree(d_stage);
+        if (h_stage) cudaFreeHost(h_stage);
+        d_stage = nullptr;
+        h_stage = nullptr;
+        bytes = 0;
     }
 
 public:
-    VtiFile(const std::string& path, const nicr_config& cfg) : c(cfg), final_path(path), temp_path(path + ".tmp") {
-        f.open(temp_path, std::ios::binary | std::ios::trunc);
-        if (!f) throw nicr::Error(NICR_ERR_IO, "Cannot open " + temp_path);
-        f.imbue(std::locale::classic());
-        f << std::setprecision(17) << "<?xml version=\"1.0\"?>\n"
-          << "<VTKFile type=\"ImageData\" version=\"1.0\" byte_order=\"LittleEndian\" header_type=\"UInt64\" compressor=\"vtkZLibDataCompressor\">\n"
-          << " <ImageData WholeExtent=\"0 " << c.nx - 1 << " 0 " << c.ny - 1 << " 0 " << c.nz - 1 << "\" Origin=\""
-          << .5 * c.dx << " " << .5 * c.dy << " " << .5 * c.dz << "\" Spacing=\"" << c.dx << " " << c.dy << " " << c.dz
-          << "\">\n  <Piece Extent=\"0 " << c.nx - 1 << " 0 " << c.ny - 1 << " 0 " << c.nz - 1 << "\">\n"
-          << "   <PointData Scalars=\"phi\">\n";
-        for (size_t a = 0; a < NAMES3.size(); ++a) {
-            f << "    <DataArray type=\"" << (c.output_float64 ? "Float64" : "Float32") << "\" Name=\"" << NAMES3[a]
-              << "\" NumberOfComponents=\"1\" format=\"appended\" offset=\"";
-            offset_pos[a] = f.tellp();
-            f << "00000000000000000000\"/>\n";
-        }
-        f << "   </PointData>\n   <CellData/>\n  </Piece>\n </ImageData>\n <AppendedData encoding=\"raw\">\n_";
-        data_start = f.tellp();
-        check();
+    explicit AsyncVti(int dev) : device(dev) {
+        nicr::check_cuda(cudaStreamCreateWithFlags(&copy, cudaStreamNonBlocking), "cudaStreamCreate");
+        nicr::check_cuda(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming), "cudaEventCreate");
+        nicr::check_cuda(cudaEventCreateWithFlags(&copied, cudaEventDisableTiming), "cudaEventCreate");
+        nicr::check_cuda(cudaMalloc(&d_range, sizeof(unsigned)), "cudaMalloc");
+        nicr::check_cuda(cudaMallocHost(&h_range, sizeof(unsigned)), "cudaMallocHost");
     }
-    ~VtiFile() {
-        if (!done) {
-            f.close();
-            std::error_code ec;
-            fs::remove(temp_path, ec);
-        }
+    ~AsyncVti() {
+        finish();
+        cudaSetDevice(device);
+        release_buffers();
+        if (d_range) cudaFree(d_range);
+        if (h_range) cudaFreeHost(h_range);
+        if (ready) cudaEventDestroy(ready);
+        if (copied) cudaEventDestroy(copied);
+        if (copy) cudaStreamDestroy(copy);
     }
-    template <class T>
-    void array(const std::function<double(long long)>& value) {
-        const auto start = f.tellp();
-        const auto offset = static_cast<std::uint64_t>(start - data_start);
-        f.seekp(offset_pos[next]);
-        f << std::setw(20) << std::setfill('0') << offset << std::setfill(' ');
-        f.seekp(start);
-        check();
-        const std::uint64_t n = std::uint64_t(c.nx) * c.ny * c.nz, total = n * sizeof(T);
-        const std::uint64_t nb = (total + kBlock - 1) / kBlock;
-        const auto header = f.tellp();
-        std::vector<std::uint64_t> sizes((size_t)nb, 0);
-        u64(nb); u64(kBlock); u64(total % kBlock);
-        for (std::uint64_t b = 0; b < nb; ++b) u64(0);
-        std::vector<T> buf((size_t)(kBlock / sizeof(T)));
-        std::vector<unsigned char> packed((size_t)compressBound(kBlock));
-        size_t used = 0, block = 0;
-        auto flush = [&] {
-            if (!used) return;
-            uLongf dest = (uLongf)packed.size();
-            const int rc = compress2(packed.data(), &dest, reinterpret_cast<const Bytef*>(buf.data()),
-                                     (uLong)(used * sizeof(T)), c.compression_level);
-            if (rc != Z_OK) throw nicr::Error(NICR_ERR_IO, "zlib compression failed: " + std::to_string(rc));
-            sizes.at(block++) = dest;
-            f.write(reinterpret_cast<const char*>(packed.data()), (std::streamsize)dest);
-            check();
-            used = 0;
-        };
-        for_x_fastest(c, [&](long long q, bool) {
-            const double v = value(q);
-            if (std::isfinite(v) && std::abs(v) > std::numeric_limits<T>::max())
-                throw nicr::Error(NICR_ERR_IO, std::string("VTI ") + NAMES3[next] +
-                                                   " exceeds output type range; use --output-precision float64.");
-            buf[used++] = static_cast<T>(v);
-            if (used == buf.size()) flush();
+    // joins the writer thread; returns (and clears) the error of the last frame
+    int finish(std::string* msg = nullptr) {
+        if (worker.joinable()) worker.join();
+        const int rc = error_code;
+        if (msg) *msg = error;
+        error_code = NICR_OK;
+        error.clear();
+        return rc;
+    }
+    void submit(Model& m, const std::string& path) {
+        std::string msg;
+        const int rc = finish(&msg);
+        if (rc != NICR_OK) throw nicr::Error(rc, msg);
+        const nicr_config c = m.c;
+        const bool f64 = c.output_float64 != 0;
+        const size_t need = NAMES3.size() * (size_t)m.g.ncells * (f64 ? 8 : 4);
+        if (need != bytes) {
+            release_buffers();
+            nicr::check_cuda(cudaMalloc(&d_stage, need), "cudaMalloc (VTI staging)");
+            nicr::check_cuda(cudaMallocHost(&h_stage, need), "cudaMallocHost (VTI staging)");
+            bytes = need;
+        }
+        m.refresh();
+        m.ensure_mask();
+        nicr::VtiArgs a{};
+        a.g = m.g;
+        a.has_eta = m.has_eta ? 1 : 0;
+        a.neta = m.neta;
+        a.p = m.d_p(); a.o = m.d_o(); a.cr = m.d_cr();
+        a.muO = m.d_mu_o(); a.muCr = m.d_mu_cr();
+        a.gb = m.d_gb();
+        a.grain = m.grain_retained ? m.d_grain() : nullptr;
+        a.eta = m.has_eta ? m.d_eta(0) : nullptr;
+        if (!m.has_eta && !a.grain) throw nicr::Error(NICR_ERR_STATE, "grain map missing for grain_sum");
+        nicr::check_cuda(cudaMemsetAsync(d_range, 0, sizeof(unsigned), m.stream), "memset");
+        nicr::launch_vti_arrays(a, d_stage, f64, d_range, m.stream);
+        nicr::check_cuda(cudaGetLastError(), "VTI arrays");
+        nicr::check_cuda(cudaEventRecord(ready, m.stream), "cudaEventRecord");
+        nicr::check_cuda(cudaStreamWaitEvent(copy, ready, 0), "cudaStreamWaitEvent");
+        nicr::check_cuda(cudaMemcpyAsync(h_stage, d_stage, bytes, cudaMemcpyDeviceToHost, copy), "D2H");
+        nicr::check_cuda(cudaMemcpyAsync(h_range, d_range, sizeof(unsigned), cudaMemcpyDeviceToHost, copy), "D2H");
+        nicr::check_cuda(cudaEventRecord(copied, copy), "cudaEventRecord");
+        worker = std::thread([this, c, f64, path] {
+            try {
+                cudaSetDevice(device);
+                nicr::check_cuda(cudaEventSynchronize(copied), "VTI copy");
+                const unsigned r = *h_range;
+                if (r) {
+                    int arr = 0;
+                    while (!(r & (1u << arr))) ++arr;
+                    throw nicr::Error(NICR_ERR_IO, std::string("VTI ") + NAMES3[(size_t)arr] +
+                                                       " exceeds output type range; use --output-precision float64.");
+                }
+                compose_vti(c, h_stage, f64, path);
+            } catch (const nicr::Error& e) {
+                error_code = e.code;
+                error = e.what();
+            } catch (const std::exception& e) {
+                error_code = NICR_ERR_IO;
+                error = e.what();
+            }
         });
-        flush();
-        if (block != sizes.size()) throw nicr::Error(NICR_ERR_IO, "Internal VTI block-count mismatch.");
-        const auto end = f.tellp();
-        f.seekp(header + std::streamoff(24));
-        for (auto v : sizes) u64(v);
-        f.seekp(end);
-        check();
-        ++next;
-    }
-    void finish() {
-        if (next != NAMES3.size()) throw nicr::Error(NICR_ERR_IO, "Missing VTI arrays.");
-        f << "\n </AppendedData>\n</VTKFile>\n";
-        f.flush();
-        check();
-        f.close();
-        check();
-        fs::rename(temp_path, final_path);
-        done = true;
     }
 };
 
-void write_vti3(Model& m, const std::string& path) {
-    Snapshot s(m);
-    VtiFile w(path, m.c);
-    for (const auto& fn : arrays3(s)) {
-        if (m.c.output_float64) w.array<double>(fn);
-        else w.array<float>(fn);
-    }
-    w.finish();
+AsyncVti& vti_writer(Model& m) {
+    if (!m.output_writer) m.output_writer = std::make_shared<AsyncVti>(m.c.device);
+    return *static_cast<AsyncVti*>(m.output_writer.get());
 }
 
-void write_visualization(Model& m, const std::string& stem) {
+void write_vti3_async(Model& m, const std::string& path) { vti_writer(m).submit(m, path); }
+
+void output_wait(Model& m) {
+    if (!m.output_writer) return;
+    std::string msg;
+    const int rc = static_cast<AsyncVti*>(m.output_writer.get())->finish(&msg);
+    if (rc != NICR_OK) throw nicr::Error(rc, msg);
+}
+
+void write_vti3(Model& m, const std::string& path) {
+    write_vti3_async(m, path);
+    output_wait(m);
+}
+
+// One output frame. With `async`, a 3D VTI frame is finished by the model's
+// writer thread while stepping continues (output_wait joins it); the ASCII
+// VTK frames are written at once.
+void write_visualization(Model& m, const std::string& stem, bool async = false) {
     if (m.dim == 2) write_vtk2(m, stem + ".vtk");
-    else if (m.c.output_vti) write_vti3(m, stem + ".vti");
-    else write_vtk3(m, stem + ".vtk");
+    else if (m.c.output_vti) {
+        if (async) write_vti3_async(m, stem + ".vti");
+        else write_vti3(m, stem + ".vti");
+    } else write_vtk3(m, stem + ".vtk");
 }
 
 // ------------------------------------------------------------------ CSV rows
@@ -605,10 +720,15 @@ int run_program(int dim, int argc, const char* const* argv) {
                         gh.flush();
                         if (!gd || !gh) throw std::runtime_error("Grain diagnostics write failed.");
                     }
-                    write_visualization(m, dir + "/fields_" + std::to_string(n));
+                    write_visualization(m, dir + "/fields_" + std::to_string(n), true);
                 }
             }
+            output_wait(m);
         } catch (const std::exception& e) {
+            try {
+                output_wait(m);   // the failure is reported; a pending frame is completed if it can be
+            } catch (const std::exception&) {
+            }
             std::ofstream stop(dir + "/STOPPED.txt");
             stop << "Last accepted time step: " << last << "\n" << e.what() << "\n";
             write_visualization(m, dir + "/state_at_failure");
@@ -638,6 +758,15 @@ int nicr_write_vti(nicr_handle* h, const char* path) {
         if (m.dim != 3) throw nicr::Error(NICR_ERR_STATE, "VTI output exists only in 3D");
         write_vti3(m, path);
     });
+}
+int nicr_write_vti_async(nicr_handle* h, const char* path) {
+    return guarded(h, [&](Model& m) {
+        if (m.dim != 3) throw nicr::Error(NICR_ERR_STATE, "VTI output exists only in 3D");
+        write_vti3_async(m, path);
+    });
+}
+int nicr_output_wait(nicr_handle* h) {
+    return guarded(h, [&](Model& m) { output_wait(m); });
 }
 int nicr_write_metadata(nicr_handle* h, const char* out_dir) {
     return guarded(h, [&](Model& m) { metadata(m, out_dir); });

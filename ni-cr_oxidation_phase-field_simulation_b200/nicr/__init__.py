@@ -94,6 +94,8 @@ def lib():
     L.nicr_get_grain_stats.argtypes = [H, ctypes.POINTER(NicrGrainStats), ctypes.POINTER(ctypes.c_longlong), dp]
     L.nicr_write_vtk.argtypes = [H, ctypes.c_char_p]
     L.nicr_write_vti.argtypes = [H, ctypes.c_char_p]
+    L.nicr_write_vti_async.argtypes = [H, ctypes.c_char_p]
+    L.nicr_output_wait.argtypes = [H]
     L.nicr_write_metadata.argtypes = [H, ctypes.c_char_p]
     L.nicr_format_log_row.argtypes = [H, ctypes.c_int, ctypes.c_char_p, ctypes.c_size_t]
     L.nicr_format_grain_rows.argtypes = [H, ctypes.c_int, ctypes.c_char_p, ctypes.c_size_t, ctypes.c_char_p,
@@ -319,6 +321,14 @@ class Solver:
 
     def write_vti(self, path):
         self._check(lib().nicr_write_vti(self.h, str(path).encode()))
+
+    def write_vti_async(self, path):
+        """Starts a VTI frame of the current state; stepping may continue at once."""
+        self._check(lib().nicr_write_vti_async(self.h, str(path).encode()))
+
+    def output_wait(self):
+        """Completes the pending asynchronous frame (raises its error)."""
+        self._check(lib().nicr_output_wait(self.h))
 
     def write_metadata(self, out_dir):
         self._check(lib().nicr_write_metadata(self.h, str(out_dir).encode()))

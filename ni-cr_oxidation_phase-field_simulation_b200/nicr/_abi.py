@@ -125,5 +125,8 @@ def config_to_flags(c: NicrConfig) -> list[str]:
           "--eta-oxide-penalty", repr(c.eta_oxide_penalty), "--max-eta-fields", str(c.max_eta_fields),
           "--left-edge-sites", str(c.left_edge_sites)]
     if c.dim == 3:
-        f += ["--frozen-eta-cache", onoff(c.frozen_eta_cache)]
+        f += ["--frozen-eta-cache", onoff(c.frozen_eta_cache),
+              "--output-format", "vti" if c.output_vti else "vtk",
+              "--output-precision", "float64" if c.output_float64 else "float32",
+              "--compression-level", str(c.compression_level)]
     return f
