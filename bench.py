@@ -197,6 +197,105 @@ def reference_arm(args, rank: int, world: int):
     return 0
 
 
+# ------------------------------------------------------------------ secondary workloads
+def output_workload(args) -> int:
+    """VTI frame cost: a synchronous frame, and 100 steps alone vs 100 steps with
+    one asynchronous frame in flight, at 151x101x101 (reference defaults) and at
+    the bench workload; the reference's own writer timed beside it (one vti
+    command of oracle/_ref/ref3d, with minus without)."""
+    import torch
+    import nicr
+    out = {"workload": "output", "unit": "s", "host_threads": os.cpu_count()}
+    with tempfile.TemporaryDirectory(prefix="nicr-vti-") as d:
+        for shape in ((151, 101, 101), (args.size,) * 3):
+            if shape[0] == 151:
+                cfg = nicr.make_config(3, nx=151, ny=101, nz=101, bounds="legacy")
+            else:
+                cfg = workload_config(args.size, args.neta)
+            s = nicr.Solver(cfg)
+            s.run(2)
+            s.write_vti(os.path.join(d, "w.vti"))
+            t0 = time.perf_counter()
+            s.write_vti(os.path.join(d, "a.vti"))
+            t1 = time.perf_counter()
+            key = "x".join(str(v) for v in shape)
+            r = {"frame_bytes": os.path.getsize(os.path.join(d, "a.vti")), "sync_frame_s": t1 - t0}
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            s.run(100)
+            t1 = time.perf_counter()
+            s.write_vti_async(os.path.join(d, "b.vti"))
+            t2 = time.perf_counter()
+            s.run(100)
+            t3 = time.perf_counter()
+            s.output_wait()
+            t4 = time.perf_counter()
+            r.update({"steps100_s": t1 - t0, "async_submit_s": t2 - t1, "steps100_with_frame_in_flight_s": t3 - t2,
+                      "wait_after_s": t4 - t3})
+            out[key] = r
+            s.close()
+        sys.path.insert(0, str(ROOT / "oracle"))
+        from oracle import reference_available, run_reference
+        if reference_available():
+            cfg = nicr.make_config(3, nx=151, ny=101, nz=101, bounds="legacy")
+            t0 = time.perf_counter()
+            run_reference(cfg, [])
+            t1 = time.perf_counter()
+            run_reference(cfg, [("vti", os.path.join(d, "r.vti"))])
+            t2 = time.perf_counter()
+            out["cpu_baseline"] = {"kind": "reference", "frame_151x101x101_s": (t2 - t1) - (t1 - t0), "cores": 1}
+    print(json.dumps(out))
+    return 0
+
+
+def sweep_workload(args, rank: int, world: int, local: int) -> int:
+    """The batched form on a seeded sweep of 64 uneven domains (edges from
+    {32,48,64,80,96}, static grains, per-domain Cr, O supply and Ksp): this
+    rank's share (LPT partition by cells) as one batch, W untimed steps, then
+    K steps between CUDA events on the batch's stream; max over ranks."""
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    import nicr
+    from nicr.sweep import cells, partition_domains, sweep_configs
+    cfgs = sweep_configs(64, seed=3, precision=args.precision, device=local)
+    part = partition_domains([cells(c) for c in cfgs], world)[rank]
+    b = nicr.Batch([cfgs[i] for i in part])
+    stream = torch.cuda.ExternalStream(b.stream, device=local)
+    b.run(args.warmup)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    l0 = b.kernel_launches
+    e0.record(stream)
+    done, rc = b.run(args.steps, check=False)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total = sum(cells(c) for c in cfgs)
+    line = {"metric": "Mcell-updates/s, 64-domain sweep (batched form)", "value": total * args.steps / (float(t.item()) * 1e-3) / 1e6,
+            "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": float(t.item()) / args.steps, "higher_is_better": True, "scaling": "strong",
+            "dtype": "f64", "form": "fp64-fast" if args.precision else "fp64 (drop-in)",
+            "config": {"workload": "64 domains, edges in {32,48,64,80,96}, static grains 8-32, Ksp on (seed 3)",
+                       "cells": total, "domains_this_rank": len(part)},
+            "gpu_launches": b.kernel_launches - l0, "status": rc}
+    b.close()
+    if rank == 0:
+        print(json.dumps(line))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
 # ------------------------------------------------------------------ GPU arm
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
@@ -209,6 +308,10 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=50)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-budget", type=float, default=60.0, help="seconds of CPU stepping for the reference")
+    ap.add_argument("--workload", choices=["step", "output", "sweep"], default="step",
+                    help="step: the headline line (default); output: VTI frame cost and overlap with stepping; "
+                         "sweep: 64 uneven domains advanced as one batch")
+    ap.add_argument("--precision", type=int, default=0, help="arithmetic form of --workload sweep (0 drop-in, 1 fast)")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -217,6 +320,10 @@ def main():
 
     if args.impl == "reference":
         return reference_arm(args, rank, world)
+    if args.workload == "output":
+        return output_workload(args)
+    if args.workload == "sweep":
+        return sweep_workload(args, rank, world, local)
 
     import torch
     import torch.distributed as dist
