@@ -296,6 +296,44 @@ def sweep_workload(args, rank: int, world: int, local: int) -> int:
     return 0
 
 
+def small_workload(args) -> int:
+    """Step rate of the small configurations, where launch latency and X
+    serialisation decide: 2D 128^2 single crystal with a centre seed of radius
+    4 (Cr 0.20 +- 0.005 from seed 0 outside the seed), 3D 64^3 static grains,
+    3D 128^3 with 32 static grains from seed 1 and Ksp. nicr_run batches of
+    N steps (step pairs replayed as CUDA graphs), wall clock around the batch
+    after a synchronize on both sides."""
+    import torch
+    import nicr
+    cases = {
+        "2d_128sq_center": (2, dict(nx=128, ny=128, grains=0, nucleation="center", radius_grid=4.0,
+                                    bc="concentration", ck="legacy", bounds="legacy"), 4000),
+        "3d_64cube_static": (3, dict(nx=64, ny=64, nz=64, grains=1, bounds="legacy"), 2000),
+        "3d_128cube_32grains": (3, dict(nx=128, ny=128, nz=128, grains=1, grain_diameter_grid=50., random_seed=1,
+                                        bounds="legacy"), 400),
+    }
+    out = {"workload": "small", "unit": "Mcell-updates/s", "form": "fp64 (drop-in)"}
+    for name, (dim, kw, n) in cases.items():
+        s = nicr.Solver(nicr.make_config(dim, **kw))
+        if dim == 2:
+            cr = s.get("cr")
+            noise = 0.20 + np.random.Generator(np.random.MT19937(0)).uniform(-0.005, 0.005, size=cr.shape)
+            keep = s.get("p") > 0.5
+            cr[1:] = np.where(keep[1:], cr[1:], noise[1:])   # the inlet column and the seed keep their values
+            s.set("cr", cr)
+            s.reset_inventory()
+        s.run(50)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        s.run(n)
+        torch.cuda.synchronize()
+        t = time.perf_counter() - t0
+        out[name] = {"cells": s.n, "steps": n, "steps_per_s": n / t, "value": s.n * n / t / 1e6}
+        s.close()
+    print(json.dumps(out))
+    return 0
+
+
 # ------------------------------------------------------------------ GPU arm
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
@@ -308,9 +346,9 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=50)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-budget", type=float, default=60.0, help="seconds of CPU stepping for the reference")
-    ap.add_argument("--workload", choices=["step", "output", "sweep"], default="step",
+    ap.add_argument("--workload", choices=["step", "output", "sweep", "small"], default="step",
                     help="step: the headline line (default); output: VTI frame cost and overlap with stepping; "
-                         "sweep: 64 uneven domains advanced as one batch")
+                         "sweep: 64 uneven domains advanced as one batch; small: step rate of the small configs")
     ap.add_argument("--precision", type=int, default=0, help="arithmetic form of --workload sweep (0 drop-in, 1 fast)")
     args = ap.parse_args()
 
@@ -324,6 +362,8 @@ def main():
         return output_workload(args)
     if args.workload == "sweep":
         return sweep_workload(args, rank, world, local)
+    if args.workload == "small":
+        return small_workload(args)
 
     import torch
     import torch.distributed as dist

@@ -258,11 +258,13 @@ int nicr_load_state(nicr_handle* h, const char* path);
 /* Batched multi-domain form: n independent domains on one device (all
  * cfgs[i].device equal), e.g. a parameter sweep of many small grids. Each
  * domain is created exactly as nicr_create(&cfgs[i]) would create it and
- * evolves exactly as its own handle would (same kernels, same reduction
- * order: fields and budgets are bit-identical to n separate handles); the
- * batch only changes the launch structure of a step: one step launch per
- * group of up to 48 consecutive domains of one dimensionality and precision,
- * one commit launch for all domains, all on the batch's stream. The
+ * evolves as its own handle would: the same kernels give bit-identical
+ * fields; the batch gives all its domains one X chunk (planes per CTA, chosen
+ * for their total CTA count), so budget sums, reduced per CTA, agree with a
+ * lone handle's to ~1e-16 relative rather than bit for bit. The batch changes
+ * the launch structure of a step: one step launch per group of up to 48
+ * consecutive domains of one dimensionality and precision, one commit launch
+ * for all domains, all on the batch's stream. The
  * reference runs one domain per program (3S:1309-1395); there is no
  * counterpart of the batch itself.
  *

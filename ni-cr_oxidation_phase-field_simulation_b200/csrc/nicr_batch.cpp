@@ -133,6 +133,11 @@ int nicr_batch_create(const nicr_config* cfgs, int n, nicr_batch** out) {
             b->doms.push_back(h);
             h->m->adopt_stream(b->stream);
         }
+        // the domains share the GPU: one X chunk for all, from their total CTAs
+        std::vector<nicr::Grid> grids;
+        for (nicr_handle* h : b->doms) grids.push_back(h->m->g);
+        const int chunk = nicr::choose_xchunk_batch(grids.data(), (int)grids.size());
+        for (nicr_handle* h : b->doms) h->m->set_xchunk(chunk);
         *out = b;
         return NICR_OK;
     } catch (const nicr::Error& e) {

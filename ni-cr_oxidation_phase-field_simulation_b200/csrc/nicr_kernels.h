@@ -76,6 +76,13 @@ void launch_step_main(const StepParams& P, const double* o, const double* cr, co
                       const double* gb, const double* s2, double* on, double* crn, double* pn,
                       StepPartial* partials, Status* st, cudaStream_t stream, int* nblocks_out);
 int step_main_blocks(const StepParams& P);
+// Planes per CTA along X for grid g (step and eta kernels), and one chunk for
+// the n domains of a batch. NICR_XCHUNK forces a chunk for tuning runs.
+int choose_xchunk(const Grid& g);
+int choose_xchunk_batch(const Grid* grids, int n);
+// Per-device kernel attributes of the step kernel P selects, set outside any
+// stream capture (launch_step_main sets them on first use otherwise).
+void step_kernels_prepare(const StepParams& P);
 // Eta mask: S = sum eta^2, pairs, gb = scale*min(1,16*pairs) (3S:495-507)
 void launch_eta_mask(const StepParams& P, int neta, const double* eta, double* gb, double* s2,
                      double* pairs, Status* st, cudaStream_t stream);

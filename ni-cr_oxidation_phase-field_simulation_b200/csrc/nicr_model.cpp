@@ -111,14 +111,7 @@ Model::Model(const nicr_config& cfg) : c(cfg), dim(cfg.dim) {
     if (c.precision != NICR_FP64 && c.precision != NICR_FP64_FAST)
         throw Error(NICR_ERR_INVALID_ARG, "precision must be NICR_FP64 or NICR_FP64_FAST");
     sp.fast = c.precision == NICR_FP64_FAST ? 1 : 0;
-    // X chunking: enough CTAs for a few waves on 148 SMs
-    {
-        const long long tiles = dim == 3 ? (long long)((g.nb + 31) / 32) * ((g.na + 7) / 8) : (g.nb + 127) / 128;
-        int chunk = g.nx;
-        const long long target = 148LL * 2 * 4;
-        while (chunk > 16 && tiles * ((g.nx + chunk - 1) / chunk) < target) chunk = (chunk + 1) / 2;
-        sp.xchunk = std::max(1, chunk);
-    }
+    sp.xchunk = choose_xchunk(g);
 
     try {
         const size_t ns = (size_t)g.nstore;
@@ -183,6 +176,8 @@ void Model::release() {
     if (h_st) cudaFreeHost(h_st);
     for (cudaEvent_t e : prof_pool) cudaEventDestroy(e);
     prof_pool.clear();
+    for (auto& q : pair_graphs)
+        if (q.exec) { cudaGraphExecDestroy(q.exec); q.exec = nullptr; }
     if (stream && owns_stream) cudaStreamDestroy(stream);
     std::memset(o_, 0, sizeof o_); std::memset(cr_, 0, sizeof cr_); std::memset(p_, 0, sizeof p_);
     std::memset(gb_, 0, sizeof gb_); std::memset(s2_, 0, sizeof s2_); std::memset(eta_, 0, sizeof eta_);
@@ -618,6 +613,20 @@ void Model::reset_status() {
     check_cuda(cudaMemcpyAsync(st, h_st, sizeof(Status), cudaMemcpyHostToDevice, stream), "H2D");
 }
 
+void Model::set_xchunk(int c) {
+    sync();
+    sp.xchunk = std::max(1, std::min(c, g.nx));
+    const int need = std::max(step_main_blocks(sp), 148 * 4) + 8;
+    if (need > partial_cap) {
+        cudaFree(partials);
+        partials = nullptr;
+        partial_cap = need;
+        partials = dalloc_t<StepPartial>(partial_cap);
+    }
+    for (auto& q : pair_graphs)   // captured launches carry the old grid
+        if (q.exec) { cudaGraphExecDestroy(q.exec); q.exec = nullptr; }
+}
+
 void Model::prepare_step() {
     if (has_eta && eta_dirty) eta_mask_now();
 }
@@ -771,12 +780,73 @@ int Model::run_end(RunPlan& r, int* completed) {
     return rc;
 }
 
+bool Model::ksp_due(const RunPlan& r, int s) const {
+    if (!r.schedule || c.nucleation != NICR_NUC_KSP) return false;
+    const long long n = r.before + s + 1;
+    return double(n) * c.dt + 1.e-12 * c.nucleation_period >= r.next;
+}
+
+// Step-pair graphs. Replaying a captured pair of steps costs one host launch
+// instead of two or three per step, which decides the step rate of small
+// domains (a 2D 128^2 step is a few microseconds of GPU work). A pair returns
+// the buffer parity to where it started, so one graph per starting parity
+// serves every pair; the kernels read their run constants from their
+// parameters and the batch-stop flag from device memory, both unchanged
+// between replays. Not used while profiling (the per-kernel events) or when
+// NICR_GRAPHS=0.
+bool Model::graphs_enabled() const {
+    static int v = -1;
+    if (v < 0) {
+        const char* e = getenv("NICR_GRAPHS");
+        v = (e && e[0] == '0') ? 0 : 1;
+    }
+    return v == 1 && !prof_on;
+}
+
+void Model::launch_step_pair() {
+    prepare_step();   // a stale eta mask is rebuilt outside the graph
+    const int key = cur | (ecur << 1) | (gcur << 2);
+    PairGraph* pg = nullptr;
+    for (auto& q : pair_graphs)
+        if (q.exec && q.key == key) pg = &q;
+    if (!pg) {
+        for (auto& q : pair_graphs)
+            if (!q.exec) { pg = &q; break; }
+        if (!pg) throw Error(NICR_ERR_STATE, "step graph slots exhausted");
+        step_kernels_prepare(sp);
+        const long long l0 = launches;
+        cudaGraph_t graph = nullptr;
+        check_cuda(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
+        enqueue_step();
+        enqueue_step();
+        check_cuda(cudaStreamEndCapture(stream, &graph), "cudaStreamEndCapture");
+        const cudaError_t e = cudaGraphInstantiate(&pg->exec, graph, 0);
+        cudaGraphDestroy(graph);
+        check_cuda(e, "cudaGraphInstantiate");
+        pg->key = key;
+        pg->kernels = launches - l0;
+        launches = l0;   // nothing ran while capturing; each replay counts them
+        // the two captured enqueue_step calls toggled the parity twice: back at key
+    }
+    check_cuda(cudaGraphLaunch(pg->exec, stream), "cudaGraphLaunch");
+    launches += pg->kernels;
+}
+
 int Model::step(int nsteps, int* completed) {
     if (completed) *completed = 0;
     if (nsteps <= 0) return NICR_OK;
     RunPlan r;
     run_begin(r, nsteps, false);
-    for (int s = 0; s < nsteps; ++s) enqueue_step();
+    const bool graphs = graphs_enabled();
+    for (int s = 0; s < nsteps;) {
+        if (graphs && s + 1 < nsteps) {
+            launch_step_pair();
+            s += 2;
+        } else {
+            enqueue_step();
+            ++s;
+        }
+    }
     return run_end(r, completed);
 }
 
@@ -785,9 +855,17 @@ int Model::run(int nsteps, int* completed) {
     if (nsteps <= 0) return NICR_OK;
     RunPlan r;
     run_begin(r, nsteps, true);
-    for (int s = 0; s < nsteps; ++s) {
+    const bool graphs = graphs_enabled();
+    for (int s = 0; s < nsteps;) {
         run_pre_step(r, s);
-        enqueue_step();
+        if (graphs && s + 1 < nsteps && !ksp_due(r, s + 1)) {
+            launch_step_pair();
+            run_pre_step(r, s + 1);   // no scan is due: records the schedule entry only
+            s += 2;
+        } else {
+            enqueue_step();
+            ++s;
+        }
     }
     return run_end(r, completed);
 }

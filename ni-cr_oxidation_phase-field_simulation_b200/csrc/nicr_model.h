@@ -98,6 +98,9 @@ public:
         double next = 0.;
         std::vector<double> sched;
     };
+    // Planes per CTA of this domain's step and eta kernels (a batch sets one
+    // chunk for all its domains). Grows the partial-sum buffer when needed.
+    void set_xchunk(int c);
     void prepare_step();
     BatchDomain step_desc() const;
     FinalizeDomain finalize_desc(int nblocks) const;
@@ -170,6 +173,17 @@ private:
     std::vector<Mark> prof_marks;
     size_t prof_begin();
     void prof_end(int k, size_t e0, int kernels);
+
+    // captured step pairs, one per starting buffer parity (cur, ecur, gcur)
+    struct PairGraph {
+        cudaGraphExec_t exec = nullptr;
+        int key = 0;
+        long long kernels = 0;
+    };
+    PairGraph pair_graphs[8];
+    bool graphs_enabled() const;
+    bool ksp_due(const RunPlan& r, int s) const;
+    void launch_step_pair();
 
     void release();
     double* dalloc(size_t n);

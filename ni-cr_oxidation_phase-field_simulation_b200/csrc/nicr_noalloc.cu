@@ -137,11 +137,7 @@ nicr::StepParams params_for(const nicr_config& c) {
     sp.phi_eta = has_eta ? 1 : 0;
     sp.inlet = (c.bc == NICR_BC_CONCENTRATION && c.oxygen_diffusion) ? 1 : 0;
     sp.fast = c.precision == NICR_FP64_FAST ? 1 : 0;
-    const long long tiles = dim == 3 ? (long long)((g.nb + 31) / 32) * ((g.na + 7) / 8) : (g.nb + 127) / 128;
-    int chunk = g.nx;
-    const long long target = 148LL * 2 * 4;
-    while (chunk > 16 && tiles * ((g.nx + chunk - 1) / chunk) < target) chunk = (chunk + 1) / 2;
-    sp.xchunk = chunk < 1 ? 1 : chunk;
+    sp.xchunk = choose_xchunk(g);
     return sp;
 }
 

@@ -15,7 +15,12 @@
 // correctly rounded quotient), so the FP64 results are bit-identical. Ghost semantics:
 // Neumann copies in X for o, cr, phi, gb and for the computed mu and M
 // (refresh copies mu(1) into the ghost, 3S:613-615), periodic rows/columns.
+#include <algorithm>
 #include <cstdlib>
+#include <mutex>
+#include <set>
+#include <utility>
+#include <vector>
 #include <cuda_runtime.h>
 #include "nicr_kernels.h"
 #include "nicr_physics.h"
@@ -927,6 +932,70 @@ __global__ void k_refresh(const StepParams P, const double* __restrict__ o, cons
 }  // namespace
 
 // ----------------------------------------------------------------- launchers
+// Dynamic shared memory above 48 KB is opted into per kernel and per device,
+// once (setting it again is harmless, skipping it on a second device is not).
+static void ensure_smem_attr(const void* kernel, int bytes) {
+    static std::mutex mu;
+    static std::set<std::pair<const void*, int>> done;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lock(mu);
+    if (done.insert({kernel, dev}).second)
+        cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+}
+// X chunk of the step and eta kernels. A CTA marching c planes also computes
+// mu and M of the plane before its chunk and stages that plane's halo, about
+// two planes of extra work, and CTAs run in waves of 2 (3D) or 4 (2D) per SM,
+// so the chunk minimising waves x (c + 2) is taken among nx halved repeatedly
+// and the powers of two below nx, the longer chunk on ties. Small domains get short chunks and use the whole GPU
+// (2D 128^2: 1 plane per CTA; 64^3: 4), large ones long chunks (256^3: 32).
+// NICR_XCHUNK forces a chunk for tuning runs.
+static long long step_tiles(const Grid& g) {
+    return g.dim == 3 ? (long long)((g.nb + TB3 - 1) / TB3) * ((g.na + TA3 - 1) / TA3) : (g.nb + TB2 - 1) / TB2;
+}
+static int forced_xchunk() {
+    static int forced = -1;
+    if (forced < 0) {
+        const char* e = getenv("NICR_XCHUNK");
+        forced = e ? std::max(1, atoi(e)) : 0;
+    }
+    return forced;
+}
+
+int choose_xchunk(const Grid& g) {
+    return choose_xchunk_batch(&g, 1);
+}
+
+// One chunk for all domains of a batch: the same cost with the CTAs of every
+// domain sharing the waves (chunks above a domain's nx clamp to it).
+int choose_xchunk_batch(const Grid* grids, int n) {
+    int nxmax = 1;
+    bool any3 = false;
+    for (int d = 0; d < n; ++d) {
+        nxmax = std::max(nxmax, grids[d].nx);
+        any3 = any3 || grids[d].dim == 3;
+    }
+    if (forced_xchunk() > 0) return std::min(forced_xchunk(), nxmax);
+    const long long slots = 148LL * (any3 ? 2 : 4);
+    // candidates: nx halved repeatedly, and the powers of two below it
+    std::vector<int> cand;
+    for (int c = nxmax;; c = (c + 1) / 2) {
+        cand.push_back(c);
+        if (c == 1) break;
+    }
+    for (int c = 1; c < nxmax; c *= 2) cand.push_back(c);
+    std::sort(cand.begin(), cand.end(), [](int a, int b) { return a > b; });
+    int best = nxmax;
+    long long best_cost = -1;
+    for (int c : cand) {
+        long long ctas = 0;
+        for (int d = 0; d < n; ++d) ctas += step_tiles(grids[d]) * ((grids[d].nx + c - 1) / c);
+        const long long cost = ((ctas + slots - 1) / slots) * (c + 2);
+        if (best_cost < 0 || cost < best_cost) { best_cost = cost; best = c; }
+    }
+    return best;
+}
+
 int step_main_blocks(const StepParams& P) {
     const dim3 grid = P.g.dim == 3 ? step_grid<3, TA3, TB3>(P) : step_grid<2, TA2, TB2>(P);
     return (int)(grid.x * grid.y * grid.z);
@@ -950,12 +1019,7 @@ static void launch_step3(const StepParams& P, const double* o, const double* cr,
                          const double* s2, double* on, double* crn, double* pn, StepPartial* partials, Status* st,
                          cudaStream_t stream, int* nblocks_out) {
     using T = Tile<3, TA3, TB3>;
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k_step_main<3, TA3, TB3, MINB, FAST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)T::SMEM_BYTES);
-        attr = true;
-    }
+    ensure_smem_attr((const void*)k_step_main<3, TA3, TB3, MINB, FAST>, (int)T::SMEM_BYTES);
     const dim3 grid = step_grid<3, TA3, TB3>(P);
     k_step_main<3, TA3, TB3, MINB, FAST><<<grid, dim3(TB3, TA3), T::SMEM_BYTES, stream>>>(P, o, cr, p, gb, s2, on, crn,
                                                                                          pn, partials, st);
@@ -976,6 +1040,15 @@ static void launch_step_form(const StepParams& P, const double* o, const double*
                                                                                           crn, pn, partials, st);
         if (nblocks_out) *nblocks_out = (int)(grid.x * grid.y * grid.z);
     }
+}
+
+void step_kernels_prepare(const StepParams& P) {
+    if (P.g.dim != 3) return;   // the 2D tile fits the default 48 KB
+    using T = Tile<3, TA3, TB3>;
+    const bool m3 = step_minb() == 3;
+    const void* k = P.fast ? (m3 ? (const void*)k_step_main<3, TA3, TB3, 3, true> : (const void*)k_step_main<3, TA3, TB3, 2, true>)
+                           : (m3 ? (const void*)k_step_main<3, TA3, TB3, 3, false> : (const void*)k_step_main<3, TA3, TB3, 2, false>);
+    ensure_smem_attr(k, (int)T::SMEM_BYTES);
 }
 
 void launch_step_main(const StepParams& P, const double* o, const double* cr, const double* p, const double* gb,
@@ -1020,11 +1093,7 @@ static void launch_eta_form(const StepParams& P, int neta, const double* eta, co
         constexpr int TA = 8, TB = 32, S1 = (TA + 2) * (TB + 2);
         const size_t smem = (size_t)3 * neta * S1 * sizeof(double) + S1 * sizeof(int);
         if (!simple && smem <= 200 * 1024) {
-            static size_t attr = 0;
-            if (smem > 48 * 1024 && smem > attr) {
-                cudaFuncSetAttribute(k_eta_stream<3, TA, TB, FAST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-                attr = smem;
-            }
+            ensure_smem_attr((const void*)k_eta_stream<3, TA, TB, FAST>, 200 * 1024);
             const dim3 grid((g.nb + TB - 1) / TB, (g.na + TA - 1) / TA, (g.nx + P.xchunk - 1) / P.xchunk);
             k_eta_stream<3, TA, TB, FAST><<<grid, dim3(TB, TA), smem, stream>>>(P, neta, eta, p, eta_next, gb_next, s2_next, st);
             return;
@@ -1036,11 +1105,7 @@ static void launch_eta_form(const StepParams& P, int neta, const double* eta, co
         constexpr int TB = 128, S1 = TB + 2;
         const size_t smem = (size_t)3 * neta * S1 * sizeof(double) + S1 * sizeof(int);
         if (!simple && smem <= 200 * 1024) {
-            static size_t attr = 0;
-            if (smem > 48 * 1024 && smem > attr) {
-                cudaFuncSetAttribute(k_eta_stream<2, 1, TB, FAST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-                attr = smem;
-            }
+            ensure_smem_attr((const void*)k_eta_stream<2, 1, TB, FAST>, 200 * 1024);
             const dim3 grid((g.nb + TB - 1) / TB, 1, (g.nx + P.xchunk - 1) / P.xchunk);
             k_eta_stream<2, 1, TB, FAST><<<grid, dim3(TB, 1), smem, stream>>>(P, neta, eta, p, eta_next, gb_next, s2_next, st);
             return;
@@ -1074,12 +1139,7 @@ void launch_finalize_batch(const FinalizeDomain* doms, int n, cudaStream_t strea
 template <int DIM, int TA, int TB, int MINB, bool FAST>
 static void launch_batch_group(StepBatch& B, int nblocks, cudaStream_t stream) {
     using T = Tile<DIM, TA, TB>;
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k_step_batch<DIM, TA, TB, MINB, FAST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)T::SMEM_BYTES);
-        attr = true;
-    }
+    ensure_smem_attr((const void*)k_step_batch<DIM, TA, TB, MINB, FAST>, (int)T::SMEM_BYTES);
     k_step_batch<DIM, TA, TB, MINB, FAST><<<nblocks, dim3(TB, TA), T::SMEM_BYTES, stream>>>(B);
 }
 

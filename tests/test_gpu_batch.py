@@ -1,15 +1,17 @@
 """Batched multi-domain form (nicr_batch_*). Every domain of a batch must
-evolve exactly as its own handle would: same fields bit for bit, same budget
-words, same accepted-step counts and error messages. Solo handles are pinned
-to the oracle by test_gpu_parity.py; one batch domain is also checked against
-the oracle directly."""
+evolve exactly as its own handle would: same fields bit for bit, same
+accepted-step counts, nuclei, clipped cells and error messages; budget sums
+to 1e-13 relative (the batch gives all its domains one X chunk, so the
+per-CTA partial sums group differently than in a lone handle). Solo handles
+are pinned to the oracle by test_gpu_parity.py; one batch domain is also
+checked against the oracle directly."""
 import numpy as np
 import pytest
 
 import nicr
 from nicr.sweep import sweep_configs
 from oracle import Oracle
-from parity import assert_bitexact, compare_state, smooth_fields
+from parity import assert_bitexact, assert_budget, compare_state, smooth_fields
 
 pytestmark = pytest.mark.gpu
 
@@ -42,7 +44,7 @@ def assert_same_domain(a, b, label):
         assert_bitexact(f"{label} {f}", a.get(f), b.get(f))
     for g in range(a.n_eta):
         assert_bitexact(f"{label} eta{g + 1}", a.get("eta", g), b.get("eta", g))
-    assert a.budget() == b.budget(), label
+    assert_budget(a.budget(), b.budget())
     assert a.info().steps_done == b.info().steps_done, label
 
 
