@@ -78,7 +78,9 @@ typedef struct nicr_config {
     double layer_o;               /* Physics::layerO = 0.0023                   */
     int precision;                /* NICR_FP64 (drop-in) or NICR_FP64_FAST      */
     int device;                   /* CUDA device ordinal                        */
-    int reserved[6];
+    int checkpoint_every;         /* programs: write out/checkpoint.bin every N
+                                     steps (0: never); no reference counterpart */
+    int reserved[5];
 } nicr_config;
 
 /* Fills the reference defaults for dim 2 or 3 (Config{} at 2D:39 / 3S:43). */

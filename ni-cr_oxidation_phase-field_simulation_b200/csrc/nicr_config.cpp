@@ -47,7 +47,8 @@ std::string help_text(int dim) {
          "--bc concentration|mu|closed --mu-res v --surface-c-ref v\n"
          "--ck legacy|off --bounds stop|legacy --out directory --self-test --version\n"
          "Extensions (defaults reproduce the fixed reference constants): --ksp v --bulk-cr v --layer-o v\n"
-         "--precision fp64|fp64-fast (fp64: bit-identical to the reference; fp64-fast: reciprocal divisions)\n";
+         "--precision fp64|fp64-fast (fp64: bit-identical to the reference; fp64-fast: reciprocal divisions)\n"
+         "--checkpoint-every N (write <out>/checkpoint.bin every N steps) --restart FILE (continue from a checkpoint)\n";
     return s;
 }
 
@@ -117,6 +118,13 @@ void parse_into(nicr_config& c, int dim, int argc, const char* const* argv, std:
         else if (a == "--ksp") c.ksp = std::stod(v);
         else if (a == "--bulk-cr") c.bulk_cr = std::stod(v);
         else if (a == "--layer-o") c.layer_o = std::stod(v);
+        else if (a == "--checkpoint-every") {
+            size_t used = 0;
+            const long long n = std::stoll(v, &used);
+            if (used != v.size() || n < 0 || n > INT_MAX)
+                throw std::runtime_error("--checkpoint-every expects a nonnegative integer.");
+            c.checkpoint_every = (int)n;
+        }
         else if (a == "--precision") {
             if (v == "fp64") c.precision = NICR_FP64;
             else if (v == "fp64-fast") c.precision = NICR_FP64_FAST;

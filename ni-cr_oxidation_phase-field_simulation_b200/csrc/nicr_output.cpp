@@ -642,6 +642,23 @@ int run_program(int dim, int argc, const char* const* argv) {
     nicr_config c;
     std::vector<char> out(4096), err(16384);
     int self = 0;
+    // --restart FILE is a program-level flag (the state to continue from); the
+    // rest is the configuration
+    std::string restart;
+    std::vector<const char*> args;
+    for (int q = 0; q < argc; ++q) {
+        if (q > 0 && std::string(argv[q]) == "--restart") {
+            if (q + 1 >= argc) {
+                std::cerr << "ERROR: Missing value for --restart\n";
+                return 1;
+            }
+            restart = argv[++q];
+            continue;
+        }
+        args.push_back(argv[q]);
+    }
+    argc = (int)args.size();
+    argv = args.data();
     const int rc = nicr_config_parse(&c, dim, argc - 1, argv + 1, out.data(), out.size(), &self, err.data(), err.size());
     if (rc == 100) {
         std::cout << err.data();
@@ -657,6 +674,8 @@ int run_program(int dim, int argc, const char* const* argv) {
         if (fs::exists(dir) && !fs::is_empty(dir)) throw std::runtime_error("Output directory is not empty; choose a new --out.");
         fs::create_directories(dir);
         Model m(c);
+        if (!restart.empty()) m.load_state(restart);
+        const int start = (int)m.steps_done;
         metadata(m, dir);
         std::ofstream log(dir + "/diagnostics.csv"), gd, gh;
         if (!log) throw std::runtime_error("Cannot open diagnostics.csv");
@@ -684,8 +703,13 @@ int run_program(int dim, int argc, const char* const* argv) {
                 gh << b;
             }
         };
-        do_log(0);
-        write_visualization(m, dir + "/fields_0");
+        auto checkpoint = [&](int n) {
+            if (c.checkpoint_every <= 0 || n % c.checkpoint_every != 0) return;
+            m.save_state(dir + "/checkpoint.bin.tmp");
+            fs::rename(dir + "/checkpoint.bin.tmp", dir + "/checkpoint.bin");
+        };
+        do_log(start);
+        write_visualization(m, dir + "/fields_" + std::to_string(start));
         std::cout << "EXECUTION BACKEND: CUDA sm_100a, one GPU holds the whole domain.\n";
         std::cout << "MPI processes: 1 (domain resident on one GPU)\n";
         if (dim == 3)
@@ -697,12 +721,13 @@ int run_program(int dim, int argc, const char* const* argv) {
                   << "; oxygen_diffusion=" << (c.oxygen_diffusion ? "on" : "off") << "; nucleation="
                   << (c.nucleation == NICR_NUC_CENTER ? "center" : c.nucleation == NICR_NUC_OFF ? "off" : "ksp") << "; "
                   << m.seeds.size() / dim << " grain(s).\n";
-        int last = 0, n = 0;
+        int last = start, n = start;
         try {
             while (n < c.steps) {
-                // advance to the next progress line or output, in one batch
+                // advance to the next progress line, output or checkpoint, in one batch
                 int next = std::min(c.steps, (n / 1000 + 1) * 1000);
                 next = std::min(next, (n / c.output_every + 1) * c.output_every);
+                if (c.checkpoint_every > 0) next = std::min(next, (n / c.checkpoint_every + 1) * c.checkpoint_every);
                 int done = 0;
                 const int r = m.run(next - n, &done);
                 last = n + done;
@@ -722,6 +747,7 @@ int run_program(int dim, int argc, const char* const* argv) {
                     }
                     write_visualization(m, dir + "/fields_" + std::to_string(n), true);
                 }
+                checkpoint(n);
             }
             output_wait(m);
         } catch (const std::exception& e) {

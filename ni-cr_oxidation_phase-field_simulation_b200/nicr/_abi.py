@@ -54,7 +54,8 @@ class NicrConfig(ctypes.Structure):
         ("ksp", ctypes.c_double), ("bulk_cr", ctypes.c_double), ("layer_o", ctypes.c_double),
         ("precision", ctypes.c_int),
         ("device", ctypes.c_int),
-        ("reserved", ctypes.c_int * 6),
+        ("checkpoint_every", ctypes.c_int),
+        ("reserved", ctypes.c_int * 5),
     ]
 
 

@@ -134,3 +134,23 @@ def test_rejections_leave_the_handle_untouched(require_gpu, tmp_path):
     assert d.info().steps_done == 4
     for s in (a, b, c, d):
         s.close()
+
+
+def test_program_checkpoint_and_restart(require_gpu, tmp_path):
+    """bin/nicr3d --checkpoint-every / --restart: a run stopped at step 20 and
+    restarted from its checkpoint writes the same step-30 frame and
+    diagnostics row as the uninterrupted run."""
+    args = ["--nx", "31", "--ny", "21", "--nz", "19", "--dt", "1e-12", "--nucleation-period", "5e-12",
+            "--radius-grid", "2.5", "--grain-diameter-grid", "12", "--bc", "mu", "--bounds", "legacy",
+            "--output-every", "10"]
+    full, first, second = tmp_path / "full", tmp_path / "first", tmp_path / "second"
+    assert nicr.main(3, args + ["--steps", "30", "--out", str(full)]) == 0
+    assert nicr.main(3, args + ["--steps", "20", "--checkpoint-every", "10", "--out", str(first)]) == 0
+    assert (first / "checkpoint.bin").exists() and not (first / "checkpoint.bin.tmp").exists()
+    assert nicr.main(3, args + ["--steps", "30", "--restart", str(first / "checkpoint.bin"), "--out", str(second)]) == 0
+    assert (second / "fields_30.vti").read_bytes() == (full / "fields_30.vti").read_bytes()
+    assert (second / "fields_20.vti").read_bytes() == (full / "fields_20.vti").read_bytes()
+    last = lambda d: (d / "diagnostics.csv").read_text().strip().splitlines()[-1]
+    assert last(second) == last(full)
+    assert nicr.main(3, args + ["--steps", "30", "--restart", str(tmp_path / "none.bin"),
+                                "--out", str(tmp_path / "x")]) == 1
