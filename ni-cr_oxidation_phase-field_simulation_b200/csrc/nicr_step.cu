@@ -580,8 +580,11 @@ __device__ __forceinline__ void eta_cell(const StepParams& P, int neta, const do
     gb_next[idx] = P.eta_scale * smin(1., 16. * pairs);
 }
 
+// Bounds for 5 CTAs/SM (<= 51 registers, no spills): the load-latency-bound
+// per-cell kernel measured 1.13 ms vs 1.29 ms unbounded (62 registers, 4/SM)
+// at 256^3 with 8 fields; 6/SM spills (1.27 ms).
 template <int DIM, bool FAST>
-__global__ void k_eta_update(const StepParams P, int neta, const double* __restrict__ eta,
+__global__ void __launch_bounds__(256, 5) k_eta_update(const StepParams P, int neta, const double* __restrict__ eta,
                              const double* __restrict__ s2, const double* __restrict__ p,
                              double* __restrict__ eta_next, double* __restrict__ gb_next,
                              double* __restrict__ s2_next, Status* st) {
