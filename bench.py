@@ -472,7 +472,7 @@ def main():
     for _ in range(args.e2e_steps):
         sol.run(1)
     for f in fields:
-        host[f][:] = sol.get(f).ravel()
+        sol.get(f, out=host[f])
     e2e_s = time.perf_counter() - t0
     te = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
     if world > 1:

@@ -93,8 +93,7 @@ int nicr_get_seeds(const nicr_handle* hc, double* xyz, long long* volumes) {
 int nicr_set_field(nicr_handle* h, int field, int index, const double* host) {
     return guarded(h, [&](nicr::Model& m) {
         if (!host) return (int)NICR_ERR_INVALID_ARG;
-        m.set_field(field, index, host);
-        m.refresh();
+        m.set_field(field, index, host);   // mu/M and a stale eta mask are recomputed when next needed
         return (int)NICR_OK;
     });
 }

@@ -222,10 +222,15 @@ class Solver:
         self._check(lib().nicr_get_seeds(self.h, _dp(xyz), vol.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong))))
         return xyz.reshape(i.n_seeds, self.cfg.dim), vol
 
-    def get(self, name: str, index: int = 0) -> np.ndarray:
+    def get(self, name: str, index: int = 0, out: np.ndarray | None = None) -> np.ndarray:
+        """Field values in interior order; `out` (contiguous float64, one value
+        per cell, e.g. pinned host memory) receives them without a copy."""
         if name.startswith("eta") and name[3:].isdigit():
             index, name = int(name[3:]) - 1, "eta"
-        out = np.empty(self.n)
+        if out is None:
+            out = np.empty(self.n)
+        elif out.dtype != np.float64 or out.size != self.n or not out.flags["C_CONTIGUOUS"]:
+            raise ValueError("out must be a contiguous float64 array with one value per cell")
         self._check(lib().nicr_get_field(self.h, FIELD[name], index, _dp(out)))
         return out.reshape(self.shape)
 
