@@ -83,6 +83,14 @@ int choose_xchunk_batch(const Grid* grids, int n);
 // Per-device kernel attributes of the step kernel P selects, set outside any
 // stream capture (launch_step_main sets them on first use otherwise).
 void step_kernels_prepare(const StepParams& P);
+// The reciprocal form's launchers (nicr_step_fast.cu, compiled with FMA
+// contraction); the generic launchers dispatch to them when P.fast is set.
+void launch_step_main_fast(const StepParams& P, const double* o, const double* cr, const double* p, const double* gb,
+                           const double* s2, double* on, double* crn, double* pn, StepPartial* partials, Status* st,
+                           cudaStream_t stream, int* nblocks_out);
+void launch_eta_update_fast(const StepParams& P, int neta, const double* eta, const double* s2, const double* p,
+                            double* eta_next, double* gb_next, double* s2_next, Status* st, cudaStream_t stream);
+void step_kernels_prepare_fast(const StepParams& P);
 // Eta mask: S = sum eta^2, pairs, gb = scale*min(1,16*pairs) (3S:495-507)
 void launch_eta_mask(const StepParams& P, int neta, const double* eta, double* gb, double* s2,
                      double* pairs, Status* st, cudaStream_t stream);
@@ -109,6 +117,7 @@ struct StepBatch {
 };
 // returns the number of launches
 int launch_step_batch(BatchDomain* doms, int n, cudaStream_t stream);
+void launch_batch_group_fast(StepBatch& B, int nblocks, int dim, cudaStream_t stream);
 
 struct FinalizeDomain {
     const StepPartial* partials;

@@ -12,500 +12,18 @@
 //
 // The arithmetic is the reference's, operation for operation (nvcc -fmad=false;
 // divisions by the run constants dx^2, dx, dt use xdiv, which returns the
-// correctly rounded quotient), so the FP64 results are bit-identical. Ghost semantics:
+// correctly rounded quotient), so the FP64 results are bit-identical. The
+// kernels themselves are in nicr_step_impl.cuh; this unit compiles the drop-in
+// form, nicr_step_fast.cu the reciprocal form. Ghost semantics:
 // Neumann copies in X for o, cr, phi, gb and for the computed mu and M
 // (refresh copies mu(1) into the ghost, 3S:613-615), periodic rows/columns.
-#include <algorithm>
-#include <cstdlib>
-#include <mutex>
-#include <set>
-#include <utility>
-#include <vector>
-#include <cuda_runtime.h>
-#include "nicr_kernels.h"
-#include "nicr_physics.h"
+#include "nicr_step_impl.cuh"
 
 namespace nicr {
 
 __device__ __noinline__ double ieee_div(double a, double b) { return __ddiv_rn(a, b); }
 
 namespace {
-
-__device__ __forceinline__ int wrapi(int v, int n) {
-    v %= n;
-    return v < 0 ? v + n : v;
-}
-
-// Warp + block reduction of double-double values (fixed order => deterministic).
-__device__ __forceinline__ DD shfl_dd(DD v, int off) {
-    DD r;
-    r.hi = __shfl_down_sync(0xffffffffu, v.hi, off);
-    r.lo = __shfl_down_sync(0xffffffffu, v.lo, off);
-    return r;
-}
-template <int N>
-__device__ void block_reduce_dd(DD (&v)[N], long long& cnt, DD* sdd, long long* scnt) {
-    const int lane = threadIdx.x & 31;
-    const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
-    const int nthreads = blockDim.x * blockDim.y * blockDim.z;
-    const int w = tid >> 5, nw = (nthreads + 31) >> 5;
-    // lanes of a warp are consecutive linear thread ids because blockDim.x is a multiple of 32
-    for (int off = 16; off > 0; off >>= 1) {
-        for (int q = 0; q < N; ++q) v[q] = dd_add(v[q], shfl_dd(v[q], off));
-        cnt += __shfl_down_sync(0xffffffffu, cnt, off);
-    }
-    if (lane == 0) {
-        for (int q = 0; q < N; ++q) sdd[w * N + q] = v[q];
-        scnt[w] = cnt;
-    }
-    __syncthreads();
-    if (tid == 0) {
-        for (int q = 0; q < N; ++q) v[q] = sdd[q];
-        cnt = scnt[0];
-        for (int ww = 1; ww < nw; ++ww) {
-            for (int q = 0; q < N; ++q) v[q] = dd_add(v[q], sdd[ww * N + q]);
-            cnt += scnt[ww];
-        }
-    }
-}
-
-// Tile geometry of the fused step kernel.
-template <int DIM, int TA, int TB>
-struct Tile {
-    static constexpr int HA2 = DIM == 3 ? 2 : 0;   // row halo of the o/cr tiles
-    static constexpr int HA1 = DIM == 3 ? 1 : 0;   // row halo of the phi/mu/M tiles
-    static constexpr int RA2 = TA + 2 * HA2, RB2 = TB + 4;
-    static constexpr int RA1 = TA + 2 * HA1, RB1 = TB + 2;
-    static constexpr int S2 = RA2 * RB2, S1 = RA1 * RB1;
-    // shared memory: o[4], cr[4] (halo 2); p[3] (halo 1); muO, muCr, mo, mc [2] (halo 1)
-    static constexpr int SMEM_DOUBLES = 8 * S2 + 3 * S1 + 8 * S1;
-    static constexpr size_t SMEM_BYTES = SMEM_DOUBLES * sizeof(double) + 64 * (5 * 16 + 8);
-    static constexpr int NT = TA * TB;
-    __device__ static int i2(int a, int b) { return (a + HA2) * RB2 + (b + 2); }
-    __device__ static int i1(int a, int b) { return (a + HA1) * RB1 + (b + 1); }
-};
-
-// Division by a run constant in the two arithmetic forms: FAST=false is the
-// drop-in (xdiv: the correctly rounded quotient, bit-identical to a / b);
-// FAST=true multiplies by RN(1/b) (within one ulp of a / b).
-template <bool FAST>
-__device__ __forceinline__ double fdiv(double a, const DivC& d) {
-    if (FAST) return __dmul_rn(a, d.rb);
-    return xdiv(a, d);
-}
-
-struct CenterVals {
-    double o, cr, p, hh, muO, muCr, mo, mc;   // hh = h(p), reused by Ck
-};
-
-template <int DIM, int TA, int TB, bool FAST>
-struct StepKernel {
-    using T = Tile<DIM, TA, TB>;
-
-    // Per-thread in-plane offsets (row*pitch + col, periodic wrap applied once
-    // per CTA) of the staging slots this thread fills: slot q = tid + k*NT.
-    struct Offs {
-        int o2[2];   // radius-2 tile points (o, cr)
-        int o1[2];   // radius-1 tile points (phi)
-        int gl[2];   // lead points: own cell, then the halo ring point tid (gb)
-    };
-    __device__ static Offs make_offs(const Grid& g, int a0, int b0) {
-        Offs f;
-        const int tid = threadIdx.x + TB * threadIdx.y;
-        for (int k = 0; k < 2; ++k) {
-            int q = tid + k * T::NT;
-            f.o2[k] = -1;
-            if (q < T::S2) {
-                const int a = q / T::RB2 - T::HA2, b = q % T::RB2 - 2;
-                f.o2[k] = (DIM == 3 ? wrapi(a0 + a, g.na) : 0) * g.pb + wrapi(b0 + b, g.nb);
-            }
-            f.o1[k] = -1;
-            if (q < T::S1) {
-                const int a = q / T::RB1 - T::HA1, b = q % T::RB1 - 1;
-                f.o1[k] = (DIM == 3 ? wrapi(a0 + a, g.na) : 0) * g.pb + wrapi(b0 + b, g.nb);
-            }
-        }
-        const int ta = DIM == 3 ? threadIdx.y : 0, tb = threadIdx.x;
-        f.gl[0] = (DIM == 3 ? wrapi(a0 + ta, g.na) : 0) * g.pb + wrapi(b0 + tb, g.nb);
-        f.gl[1] = -1;
-        if (tid < T::S1 - T::NT) {
-            int a, b;
-            ring_point(tid, a, b);
-            f.gl[1] = (DIM == 3 ? wrapi(a0 + a, g.na) : 0) * g.pb + wrapi(b0 + b, g.nb);
-        }
-        return f;
-    }
-    // halo ring enumeration: columns -1 and TB over all halo rows, then rows -1 and TA
-    __device__ static void ring_point(int hq, int& a, int& b) {
-        if (hq < 2 * T::RA1) {
-            a = hq / 2 - T::HA1;
-            b = (hq & 1) ? TB : -1;
-        } else {
-            const int r = hq - 2 * T::RA1;
-            a = (r / TB) ? TA : -1;
-            b = r % TB;
-        }
-    }
-
-    // Loads plane xg (clamped to [0,nx-1]) of o and cr with a radius-2 halo
-    // into a ring slot. The concentration inlet replaces o in plane 0 by
-    // layerO before the step (enforce_legacy_layer, 3S:593-596).
-    __device__ static void load_oc(const StepParams& P, const double* __restrict__ o,
-                                   const double* __restrict__ cr, int xg, double* so, double* scr, const Offs& f) {
-        const Grid& g = P.g;
-        xg = xg < 0 ? 0 : (xg > g.nx - 1 ? g.nx - 1 : xg);
-        const bool inlet = P.inlet && xg == 0;
-        const long long base = (long long)xg * g.plane;
-        const int tid = threadIdx.x + TB * threadIdx.y;
-#pragma unroll
-        for (int k = 0; k < 2; ++k) {
-            if (f.o2[k] < 0) continue;
-            const int q = tid + k * T::NT;
-            const long long idx = base + f.o2[k];
-            so[q] = inlet ? P.layer_o : __ldg(o + idx);
-            scr[q] = __ldg(cr + idx);
-        }
-    }
-    __device__ static void load_p(const StepParams& P, const double* __restrict__ p, int xg, double* sp,
-                                  const Offs& f) {
-        const Grid& g = P.g;
-        xg = xg < 0 ? 0 : (xg > g.nx - 1 ? g.nx - 1 : xg);
-        const long long base = (long long)xg * g.plane;
-        const int tid = threadIdx.x + TB * threadIdx.y;
-#pragma unroll
-        for (int k = 0; k < 2; ++k) {
-            if (f.o1[k] < 0) continue;
-            sp[tid + k * T::NT] = __ldg(p + base + f.o1[k]);
-        }
-    }
-
-    // Software pipelining of the staging: the loads of a later plane are issued
-    // into registers before the arithmetic of the current plane and stored to
-    // shared memory after it, so their latency overlaps the computation.
-    struct Prefetch {
-        double o[2], cr[2], p[2];
-        double gbl[2];   // gb at the lead points (own cell, ring point) of the next lead plane
-        double s2;       // eta_s2 at the own cell of the next update plane
-    };
-    // gb at the lead points of plane x (0 when grains are off)
-    __device__ static void fetch_gb(const StepParams& P, const double* __restrict__ gb, int x, const Offs& f,
-                                    double (&r)[2]) {
-        const long long base = (long long)x * P.g.plane;
-        r[0] = P.grains ? __ldg(gb + base + f.gl[0]) : 0.;
-        r[1] = (P.grains && f.gl[1] >= 0) ? __ldg(gb + base + f.gl[1]) : 0.;
-    }
-    __device__ static void fetch(const StepParams& P, const double* __restrict__ o, const double* __restrict__ cr,
-                                 const double* __restrict__ p, const double* __restrict__ gb,
-                                 const double* __restrict__ s2, int xoc, int xp, int xs, bool own, const Offs& f,
-                                 Prefetch& r) {
-        fetch_gb(P, gb, xp, f, r.gbl);
-        r.s2 = (P.phi_eta && own) ? __ldg(s2 + (long long)xs * P.g.plane + f.gl[0]) : 0.;
-        const Grid& g = P.g;
-        const int xo = xoc < 0 ? 0 : (xoc > g.nx - 1 ? g.nx - 1 : xoc);
-        const int xq = xp < 0 ? 0 : (xp > g.nx - 1 ? g.nx - 1 : xp);
-        const bool inlet = P.inlet && xo == 0;
-        const long long bo = (long long)xo * g.plane, bq = (long long)xq * g.plane;
-#pragma unroll
-        for (int k = 0; k < 2; ++k) {
-            if (f.o2[k] >= 0) {
-                r.o[k] = inlet ? P.layer_o : __ldg(o + bo + f.o2[k]);
-                r.cr[k] = __ldg(cr + bo + f.o2[k]);
-            }
-            if (f.o1[k] >= 0) r.p[k] = __ldg(p + bq + f.o1[k]);
-        }
-    }
-    __device__ static void store(const Prefetch& r, double* so, double* scr, double* sp, const Offs& f) {
-        const int tid = threadIdx.x + TB * threadIdx.y;
-#pragma unroll
-        for (int k = 0; k < 2; ++k) {
-            if (f.o2[k] >= 0) { so[tid + k * T::NT] = r.o[k]; scr[tid + k * T::NT] = r.cr[k]; }
-            if (f.o1[k] >= 0) sp[tid + k * T::NT] = r.p[k];
-        }
-    }
-
-    // mu and M at tile point (a,b) of real plane x; writes the mu/M slot.
-    __device__ static CenterVals lead_point(const StepParams& P, const double* __restrict__ gb,
-                                            const double* som, const double* so0, const double* sop,
-                                            const double* scm, const double* sc0, const double* scp,
-                                            const double* sp, double* smuO, double* smuCr, double* smo,
-                                            double* smc, int a, int b, double gbv) {
-        const int c2 = T::i2(a, b);
-        const double oc = so0[c2], cc = sc0[c2];
-        double lapO, lapC;
-        if (DIM == 3) {
-            lapO = fdiv<FAST>((sop[c2] - 2. * oc + som[c2]), P.v_dxdx)
-                 + fdiv<FAST>((so0[T::i2(a + 1, b)] - 2. * oc + so0[T::i2(a - 1, b)]), P.v_dada)
-                 + fdiv<FAST>((so0[T::i2(a, b + 1)] - 2. * oc + so0[T::i2(a, b - 1)]), P.v_dbdb);
-            lapC = fdiv<FAST>((scp[c2] - 2. * cc + scm[c2]), P.v_dxdx)
-                 + fdiv<FAST>((sc0[T::i2(a + 1, b)] - 2. * cc + sc0[T::i2(a - 1, b)]), P.v_dada)
-                 + fdiv<FAST>((sc0[T::i2(a, b + 1)] - 2. * cc + sc0[T::i2(a, b - 1)]), P.v_dbdb);
-        } else {
-            lapO = fdiv<FAST>((sop[c2] - 2. * oc + som[c2]), P.v_dxdx)
-                 + fdiv<FAST>((so0[T::i2(a, b + 1)] - 2. * oc + so0[T::i2(a, b - 1)]), P.v_dbdb);
-            lapC = fdiv<FAST>((scp[c2] - 2. * cc + scm[c2]), P.v_dxdx)
-                 + fdiv<FAST>((sc0[T::i2(a, b + 1)] - 2. * cc + sc0[T::i2(a, b - 1)]), P.v_dbdb);
-        }
-        const int c1 = T::i1(a, b);
-        const double pc = sp[c1];
-        const double hh = h(pc);
-        CenterVals v;
-        v.o = oc; v.cr = cc; v.p = pc; v.hh = hh;
-        v.muO = mu_o_local(oc, cc, hh) - 2. * Phys::ko * lapO;
-        v.muCr = mu_cr_local(oc, cc, hh) - 2. * Phys::kc * lapC;
-        v.mo = P.o_on ? mobility(oc, hh, gbv, Phys::bmo, Phys::boo, P.gbm1_o) : 0.;
-        v.mc = mobility(cc, hh, gbv, Phys::bmc, Phys::boc, P.gbm1_cr);
-        smuO[c1] = v.muO; smuCr[c1] = v.muCr; smo[c1] = v.mo; smc[c1] = v.mc;
-        return v;
-    }
-
-    __device__ static void run(const StepParams P, const double* __restrict__ o, const double* __restrict__ cr,
-                               const double* __restrict__ p, const double* __restrict__ gb,
-                               const double* __restrict__ s2, double* __restrict__ on,
-                               double* __restrict__ crn, double* __restrict__ pn,
-                               StepPartial* __restrict__ partials, Status* st, int bx, int by, int bz, int blin) {
-        extern __shared__ __align__(16) double smem[];
-        double* so = smem;                 // 4 slots x S2
-        double* scr = so + 4 * T::S2;      // 4 slots x S2
-        double* sp = scr + 4 * T::S2;      // 3 slots x S1
-        double* smuO = sp + 3 * T::S1;     // 2 slots x S1
-        double* smuCr = smuO + 2 * T::S1;
-        double* smo = smuCr + 2 * T::S1;
-        double* smc = smo + 2 * T::S1;
-        DD* sdd = reinterpret_cast<DD*>(smc + 2 * T::S1);
-        long long* scnt = reinterpret_cast<long long*>(sdd + 32 * 5);
-
-        const Grid& g = P.g;
-        const int ta = DIM == 3 ? threadIdx.y : 0, tb = threadIdx.x;
-        const int a0 = DIM == 3 ? by * TA : 0, b0 = bx * TB;
-        const int i0 = bz * P.xchunk;
-        const int i1 = min(g.nx, i0 + P.xchunk);
-        const int row = a0 + ta, col = b0 + tb;
-        const bool active = (DIM == 3 ? row < g.na : true) && col < g.nb;
-        const Offs offs = make_offs(g, a0, b0);
-
-        DD acc[5] = {{0., 0.}, {0., 0.}, {0., 0.}, {0., 0.}, {0., 0.}};  // ckO ckCr clipO clipCr bcO
-        long long clipped = 0;
-        unsigned long long errkey = ERR_NONE;
-
-        if (st->failed) return;  // a previous step of this batch was rejected
-
-        auto slot3 = [](int w) { return ((w % 3) + 3) % 3; };
-        // o/cr ring of 4 planes: the plane staged at the top of an iteration
-        // (x+2) never overlaps the window x-1..x+1 that slower warps may still
-        // be reading in lead(x), so one barrier per plane suffices
-        auto oslot = [&](int w) { return so + (w & 3) * T::S2; };
-        auto cslot = [&](int w) { return scr + (w & 3) * T::S2; };
-        auto pslot = [&](int x) { return sp + slot3(x) * T::S1; };
-
-        // Computes the lead plane x (real plane) over the tile + radius-1 halo.
-        auto lead = [&](int x, const double (&gbl)[2]) -> CenterVals {
-            const double *som = oslot(x - 1), *so0 = oslot(x), *sop = oslot(x + 1);
-            const double *scm = cslot(x - 1), *sc0 = cslot(x), *scp = cslot(x + 1);
-            const double* spx = pslot(x);
-            double* mO = smuO + (x & 1) * T::S1;
-            double* mC = smuCr + (x & 1) * T::S1;
-            double* mo_ = smo + (x & 1) * T::S1;
-            double* mc_ = smc + (x & 1) * T::S1;
-            CenterVals own = lead_point(P, gb, som, so0, sop, scm, sc0, scp, spx, mO, mC, mo_, mc_, ta, tb, gbl[0]);
-            // halo ring points: one per thread for the first S1-NT threads
-            static_assert(T::S1 - T::NT <= T::NT, "ring larger than the CTA");
-            const int tid = threadIdx.x + TB * threadIdx.y;
-            if (offs.gl[1] >= 0) {
-                int a, b;
-                ring_point(tid, a, b);
-                lead_point(P, gb, som, so0, sop, scm, sc0, scp, spx, mO, mC, mo_, mc_, a, b, gbl[1]);
-            }
-            return own;
-        };
-
-        CenterVals C, L;
-        double pP, FxO, FxCr;
-        // ---- prologue: centre values of the first update plane and its left x-face flux
-        if (i0 == 0) {
-            load_oc(P, o, cr, -1, oslot(-1), cslot(-1), offs);
-            load_oc(P, o, cr, 0, oslot(0), cslot(0), offs);
-            load_oc(P, o, cr, 1, oslot(1), cslot(1), offs);
-            load_p(P, p, 0, pslot(0), offs);
-            double gb0[2];
-            fetch_gb(P, gb, 0, offs, gb0);
-            __syncthreads();
-            C = lead(0, gb0);
-            __syncthreads();
-            // ghost plane -1: copies of plane 0 (3S:187, 3S:613-615, 3S:616-619)
-            const double muOg = (P.bc == 1 && P.o_on) ? 2. * P.mu_res - C.muO : C.muO;
-            FxO = fdiv<FAST>(-.5 * (C.mo + C.mo) * (C.muO - muOg), P.v_dx);
-            FxCr = fdiv<FAST>(-.5 * (C.mc + C.mc) * (C.muCr - C.muCr), P.v_dx);
-            pP = C.p;
-        } else {
-            load_oc(P, o, cr, i0 - 2, oslot(i0 - 2), cslot(i0 - 2), offs);
-            load_oc(P, o, cr, i0 - 1, oslot(i0 - 1), cslot(i0 - 1), offs);
-            load_oc(P, o, cr, i0, oslot(i0), cslot(i0), offs);
-            load_p(P, p, i0 - 1, pslot(i0 - 1), offs);
-            double gbm[2];
-            fetch_gb(P, gb, i0 - 1, offs, gbm);
-            __syncthreads();
-            const CenterVals Pv = lead(i0 - 1, gbm);
-            load_oc(P, o, cr, i0 + 1, oslot(i0 + 1), cslot(i0 + 1), offs);
-            load_p(P, p, i0, pslot(i0), offs);
-            double gb0[2];
-            fetch_gb(P, gb, i0, offs, gb0);
-            __syncthreads();
-            C = lead(i0, gb0);
-            __syncthreads();
-            FxO = fdiv<FAST>(-.5 * (Pv.mo + C.mo) * (C.muO - Pv.muO), P.v_dx);
-            FxCr = fdiv<FAST>(-.5 * (Pv.mc + C.mc) * (C.muCr - Pv.muCr), P.v_dx);
-            pP = Pv.p;
-        }
-
-        double s2u = (P.phi_eta && active) ? __ldg(s2 + (long long)i0 * g.plane + offs.gl[0]) : 0.;
-        Prefetch pf;
-        if (i0 + 1 <= g.nx - 1) fetch(P, o, cr, p, gb, s2, i0 + 2, i0 + 1, i0 + 1, active, offs, pf);
-        for (int u = i0; u < i1; ++u) {
-            const int x = u + 1;
-            double s2n = 0.;
-            if (x <= g.nx - 1) {
-                // one barrier per plane: it orders this plane's staging before
-                // lead(x), and the previous update(u-1) (which read the mu/M
-                // slot lead(x) now overwrites) before lead(x)
-                store(pf, oslot(x + 1), cslot(x + 1), pslot(x), offs);
-                const double gbl[2] = {pf.gbl[0], pf.gbl[1]};
-                s2n = pf.s2;
-                __syncthreads();
-                if (x + 1 <= g.nx - 1 && u + 1 < i1)
-                    fetch(P, o, cr, p, gb, s2, x + 2, x + 1, x + 1, active, offs, pf);
-                L = lead(x, gbl);
-            } else {
-                L = C;  // ghost plane nx: Neumann copy of plane nx-1 (mu and M copied too)
-                // no staging in this iteration, but update(nx-1) reads the mu/M
-                // that lead(nx-1) of other warps wrote in the previous one
-                __syncthreads();
-            }
-            if (active) {
-                const double* mO = smuO + (u & 1) * T::S1;
-                const double* mC = smuCr + (u & 1) * T::S1;
-                const double* mo_ = smo + (u & 1) * T::S1;
-                const double* mc_ = smc + (u & 1) * T::S1;
-                const double* spu = pslot(u);
-                const int c1 = T::i1(ta, tb);
-                const int bp = T::i1(ta, tb + 1), bm = T::i1(ta, tb - 1);
-                const int ap = T::i1(ta + 1, tb), am = T::i1(ta - 1, tb);
-                const long long gidx = (long long)u * g.plane + (long long)row * g.pb + col;
-                const long long cell = ((long long)u * g.na + row) * g.nb + col;  // reference loop order
-
-                // x faces: the right face of u is the left face of u+1 (same expression)
-                const double rightO = fdiv<FAST>(-.5 * (C.mo + L.mo) * (L.muO - C.muO), P.v_dx);
-                const double rightCr = fdiv<FAST>(-.5 * (C.mc + L.mc) * (L.muCr - C.muCr), P.v_dx);
-                double leftO = FxO;
-                if (u == 0 && P.bc == 1) {
-                    // left_flux (3S:621-628): surface-mobility face closure for bc=mu
-                    double lf = 0.;
-                    if (P.o_on) {
-                        const double gb0 = P.grains ? __ldg(gb + gidx) : 0.;
-                        const double mf = mobility(P.surface_c_ref, h(C.p), gb0, Phys::bmo, Phys::boo, P.gbm1_o);
-                        lf = fdiv<FAST>(2. * mf * (P.mu_res - C.muO), P.v_dx);
-                    }
-                    leftO = lf;
-                    acc[4] = dd_add(acc[4], fdiv<FAST>(P.dt * lf, P.v_dx));
-                }
-                if (u == 0 && P.inlet) acc[4] = dd_add(acc[4], P.layer_o - __ldg(o + gidx));
-
-                double divO = 0., divCr;
-                {
-                    const double mc0 = mc_[c1], mu0 = mC[c1];
-                    const double front = fdiv<FAST>(-.5 * (mc0 + mc_[bp]) * (mC[bp] - mu0), P.v_db);
-                    const double back = fdiv<FAST>(-.5 * (mc_[bm] + mc0) * (mu0 - mC[bm]), P.v_db);
-                    if (DIM == 3) {
-                        const double top = fdiv<FAST>(-.5 * (mc0 + mc_[ap]) * (mC[ap] - mu0), P.v_da);
-                        const double bottom = fdiv<FAST>(-.5 * (mc_[am] + mc0) * (mu0 - mC[am]), P.v_da);
-                        divCr = fdiv<FAST>(FxCr - rightCr, P.v_dx) + fdiv<FAST>(bottom - top, P.v_da) + fdiv<FAST>(back - front, P.v_db);
-                    } else {
-                        divCr = fdiv<FAST>(FxCr - rightCr, P.v_dx) + fdiv<FAST>(back - front, P.v_db);
-                    }
-                }
-                if (P.o_on) {
-                    const double m0 = mo_[c1], mu0 = mO[c1];
-                    const double front = fdiv<FAST>(-.5 * (m0 + mo_[bp]) * (mO[bp] - mu0), P.v_db);
-                    const double back = fdiv<FAST>(-.5 * (mo_[bm] + m0) * (mu0 - mO[bm]), P.v_db);
-                    if (DIM == 3) {
-                        const double top = fdiv<FAST>(-.5 * (m0 + mo_[ap]) * (mO[ap] - mu0), P.v_da);
-                        const double bottom = fdiv<FAST>(-.5 * (mo_[am] + m0) * (mu0 - mO[am]), P.v_da);
-                        divO = fdiv<FAST>(leftO - rightO, P.v_dx) + fdiv<FAST>(bottom - top, P.v_da) + fdiv<FAST>(back - front, P.v_db);
-                    } else {
-                        divO = fdiv<FAST>(leftO - rightO, P.v_dx) + fdiv<FAST>(back - front, P.v_db);
-                    }
-                }
-                const double oo = C.o, cc = C.cr, pp = C.p;
-                double onv = P.o_on ? oo + P.dt * divO : oo;
-                double crv = cc + P.dt * divCr;
-                double lapP;
-                if (DIM == 3)
-                    lapP = fdiv<FAST>((L.p - 2. * pp + pP), P.v_dxdx) + fdiv<FAST>((spu[ap] - 2. * pp + spu[am]), P.v_dada)
-                         + fdiv<FAST>((spu[bp] - 2. * pp + spu[bm]), P.v_dbdb);
-                else
-                    lapP = fdiv<FAST>((L.p - 2. * pp + pP), P.v_dxdx) + fdiv<FAST>((spu[bp] - 2. * pp + spu[bm]), P.v_dbdb);
-                const double hpv = 30. * pp * pp * (pp - 1.) * (pp - 1.);
-                double fp = Phys::W * (4. * pp * pp * pp - 6. * pp * pp + 2. * pp)
-                          + hpv * (foxide(oo, cc) - fmetal(oo, cc)) - 2. * Phys::kp * lapP;
-                if (P.phi_eta) fp += grain_dphi(s2u, pp, P.eta_W, P.eta_A);
-                double pnv = pp - P.dtL * fp;
-                if (P.ck == 0) {
-                    const double hn = h(pnv);
-                    const double dO = fdiv<FAST>(-Phys::ckO * ((Phys::oxideO - onv) * hn - (Phys::oxideO - oo) * C.hh), P.v_dt);
-                    const double dCr = fdiv<FAST>(-Phys::ckCr * ((Phys::oxideCr - crv) * hn - (Phys::oxideCr - cc) * C.hh), P.v_dt);
-                    onv += dO; crv += dCr;
-                    acc[0] = dd_add(acc[0], dO);
-                    acc[1] = dd_add(acc[1], dCr);
-                }
-                if (!isfinite(onv) || !isfinite(crv) || !isfinite(pnv)) {
-                    errkey = min(errkey, (unsigned long long)cell * 4ull);
-                } else if (P.bounds == 1) {
-                    const double oc = sclamp(onv, 0., 1.), ccr = sclamp(crv, 0., 1.);
-                    acc[2] = dd_add(acc[2], oc - onv);
-                    acc[3] = dd_add(acc[3], ccr - crv);
-                    if (oc != onv || ccr != crv) ++clipped;
-                    onv = oc; crv = ccr;
-                    if (pnv > .99999) pnv = 1.;
-                    if (pnv < 1.e-5) pnv = 0.;
-                } else if (onv < -1.e-12 || crv < -1.e-12 || onv + crv > 1. + 1.e-12 || pnv < -1.e-12 ||
-                           pnv > 1. + 1.e-12) {
-                    errkey = min(errkey, (unsigned long long)cell * 4ull + 1ull);
-                }
-                on[gidx] = onv; crn[gidx] = crv; pn[gidx] = pnv;
-                FxO = rightO; FxCr = rightCr;
-            }
-            pP = C.p;
-            C = L;
-            s2u = s2n;
-        }
-        if (errkey != ERR_NONE) atomicMin(&st->err_key, errkey);
-        block_reduce_dd<5>(acc, clipped, sdd, scnt);
-        if (threadIdx.x == 0 && threadIdx.y == 0) {
-            StepPartial& out = partials[blin];
-            for (int q = 0; q < 5; ++q) { out.s[q][0] = acc[q].hi; out.s[q][1] = acc[q].lo; }
-            out.clipped = clipped;
-        }
-    }
-};
-
-template <int DIM, int TA, int TB, int MINB, bool FAST>
-__global__ void __launch_bounds__(TA * TB, MINB)
-k_step_main(const StepParams P, const double* __restrict__ o, const double* __restrict__ cr,
-            const double* __restrict__ p, const double* __restrict__ gb, const double* __restrict__ s2,
-            double* __restrict__ on, double* __restrict__ crn, double* __restrict__ pn,
-            StepPartial* __restrict__ partials, Status* st) {
-    StepKernel<DIM, TA, TB, FAST>::run(P, o, cr, p, gb, s2, on, crn, pn, partials, st, blockIdx.x, blockIdx.y,
-                                       blockIdx.z, blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z));
-}
-
-constexpr int TA3 = 8, TB3 = 32;    // 3D tile: 8 rows x 32 columns, 256 threads
-constexpr int TA2 = 1, TB2 = 128;   // 2D tile: 128 columns
-
-template <int DIM, int TA, int TB>
-dim3 step_grid(const StepParams& P) {
-    const Grid& g = P.g;
-    return dim3((g.nb + TB - 1) / TB, DIM == 3 ? (g.na + TA - 1) / TA : 1, (g.nx + P.xchunk - 1) / P.xchunk);
-}
-
 // ----------------------------------------------------------------- eta kernels
 // S = sum eta_g^2, pairs = sum_{a<b} eta_a^2 eta_b^2 accumulated as in
 // rebuild_eta_mask (3S:497-505), gb = scale * min(1, 16 pairs).
@@ -531,279 +49,6 @@ __global__ void k_eta_mask(const StepParams P, int neta, const double* __restric
         if (pairs_out) pairs_out[idx] = pairs;
         gb[idx] = P.eta_scale * smin(1., 16. * pairs);
     }
-}
-
-// eta_trial (3S:514-526): v = eta - (dt*L_eta)*(deta - K*lap(eta)); must lie in
-// [-1e-12, 1+1e-12]. Writes the trial and the mask of the trial values (the
-// next step's gb and eta_s2, identical to rebuild_eta_mask on them).
-template <int DIM, bool FAST>
-__device__ __forceinline__ void eta_cell(const StepParams& P, int neta, const double* __restrict__ eta,
-                                         const double* __restrict__ s2, const double* __restrict__ p,
-                                         double* __restrict__ eta_next, double* __restrict__ gb_next,
-                                         double* __restrict__ s2_next, int x, int row, int col,
-                                         unsigned long long& errkey) {
-    const Grid& g = P.g;
-    const long long idx = (long long)x * g.plane + (long long)row * g.pb + col;
-    const long long cell = ((long long)x * g.na + row) * g.nb + col;
-    const long long ixm = x > 0 ? idx - g.plane : idx, ixp = x < g.nx - 1 ? idx + g.plane : idx;
-    const long long rbase = (long long)x * g.plane;
-    const long long ibm = rbase + (long long)row * g.pb + (col == 0 ? g.nb - 1 : col - 1);
-    const long long ibp = rbase + (long long)row * g.pb + (col == g.nb - 1 ? 0 : col + 1);
-    long long iam = idx, iap = idx;
-    if (DIM == 3) {
-        iam = rbase + (long long)(row == 0 ? g.na - 1 : row - 1) * g.pb + col;
-        iap = rbase + (long long)(row == g.na - 1 ? 0 : row + 1) * g.pb + col;
-    }
-    const double S = __ldg(s2 + idx), phi = __ldg(p + idx);
-    double Sn = 0., pairs = 0.;
-    for (int q = 0; q < neta; ++q) {
-        const double* e = eta + (long long)q * g.nstore;
-        const double ec = __ldg(e + idx);
-        double lap;
-        if (DIM == 3)
-            lap = fdiv<FAST>((__ldg(e + ixp) - 2. * ec + __ldg(e + ixm)), P.v_dxdx)
-                + fdiv<FAST>((__ldg(e + iap) - 2. * ec + __ldg(e + iam)), P.v_dada)
-                + fdiv<FAST>((__ldg(e + ibp) - 2. * ec + __ldg(e + ibm)), P.v_dbdb);
-        else
-            lap = fdiv<FAST>((__ldg(e + ixp) - 2. * ec + __ldg(e + ixm)), P.v_dxdx)
-                + fdiv<FAST>((__ldg(e + ibp) - 2. * ec + __ldg(e + ibm)), P.v_dbdb);
-        const double force = grain_deta(ec, S, phi, P.eta_W, P.eta_A) - P.eta_K * lap;
-        const double v = ec - P.dt_etaL * force;
-        if (!isfinite(v) || v < -1.e-12 || v > 1. + 1.e-12)
-            errkey = min(errkey, ERR_ETA_BASE + (unsigned long long)q * (unsigned long long)g.ncells + (unsigned long long)cell);
-        eta_next[(long long)q * g.nstore + idx] = v;
-        const double sq = v * v;
-        pairs += Sn * sq;
-        Sn += sq;
-    }
-    s2_next[idx] = Sn;
-    gb_next[idx] = P.eta_scale * smin(1., 16. * pairs);
-}
-
-// Bounds for 5 CTAs/SM (<= 51 registers, no spills): the load-latency-bound
-// per-cell kernel measured 1.13 ms vs 1.29 ms unbounded (62 registers, 4/SM)
-// at 256^3 with 8 fields; 6/SM spills (1.27 ms).
-template <int DIM, bool FAST>
-__global__ void __launch_bounds__(256, 5) k_eta_update(const StepParams P, int neta, const double* __restrict__ eta,
-                             const double* __restrict__ s2, const double* __restrict__ p,
-                             double* __restrict__ eta_next, double* __restrict__ gb_next,
-                             double* __restrict__ s2_next, Status* st) {
-    if (st->failed) return;
-    const Grid& g = P.g;
-    const int col = blockIdx.x * blockDim.x + threadIdx.x;
-    const int row = DIM == 3 ? blockIdx.y * blockDim.y + threadIdx.y : 0;
-    if (col >= g.nb || row >= g.na) return;
-    unsigned long long errkey = ERR_NONE;
-    eta_cell<DIM, FAST>(P, neta, eta, s2, p, eta_next, gb_next, s2_next, blockIdx.z, row, col, errkey);
-    if (errkey != ERR_NONE) atomicMin(&st->err_key, errkey);
-}
-
-// X-marching form of the eta update for a compile-time number of fields N:
-// each thread owns one (row, col) column of a chunk of planes and keeps
-// eta(x-1), eta(x), eta(x+1) of its column in registers, so each field value
-// is read from HBM once; the four in-plane neighbours come from L1 (they are
-// the neighbouring threads' own loads). All N loads of the next plane are
-// issued before the arithmetic of the current plane.
-// NCAP is the register capacity; the first n <= NCAP fields are updated (the
-// stand-alone kernel instantiates NCAP = n, so the guards fold away).
-template <int DIM, bool FAST, int NCAP>
-__device__ __forceinline__ void eta_march_body(const StepParams& P, int n, const double* __restrict__ eta,
-                                               const double* __restrict__ p, double* __restrict__ eta_next,
-                                               double* __restrict__ gb_next, double* __restrict__ s2_next,
-                                               Status* st, int bx, int by, int bz) {
-    if (st->failed) return;
-    const Grid& g = P.g;
-    const int col = bx * blockDim.x + threadIdx.x;
-    const int row = DIM == 3 ? by * blockDim.y + threadIdx.y : 0;
-    if (col >= g.nb || row >= g.na) return;
-    const int i0 = bz * P.xchunk, i1 = min(g.nx, i0 + P.xchunk);
-    const long long rc = (long long)row * g.pb + col;
-    const long long cbm = (long long)row * g.pb + (col == 0 ? g.nb - 1 : col - 1);
-    const long long cbp = (long long)row * g.pb + (col == g.nb - 1 ? 0 : col + 1);
-    long long cam = rc, cap = rc;
-    if (DIM == 3) {
-        cam = (long long)(row == 0 ? g.na - 1 : row - 1) * g.pb + col;
-        cap = (long long)(row == g.na - 1 ? 0 : row + 1) * g.pb + col;
-    }
-    double ep[NCAP], ec[NCAP], en[NCAP];
-    {
-        const long long bm = (long long)(i0 > 0 ? i0 - 1 : 0) * g.plane, b0 = (long long)i0 * g.plane;
-#pragma unroll
-        for (int q = 0; q < NCAP; ++q) {
-            if (q < n) {
-                ep[q] = __ldg(eta + (long long)q * g.nstore + bm + rc);
-                ec[q] = __ldg(eta + (long long)q * g.nstore + b0 + rc);
-            }
-        }
-    }
-    unsigned long long errkey = ERR_NONE;
-    for (int x = i0; x < i1; ++x) {
-        const long long base = (long long)x * g.plane;
-        const long long bnext = (long long)(x < g.nx - 1 ? x + 1 : x) * g.plane;
-#pragma unroll
-        for (int q = 0; q < NCAP; ++q)
-            if (q < n) en[q] = __ldg(eta + (long long)q * g.nstore + bnext + rc);
-        const double phi = __ldg(p + base + rc);
-        double S = 0.;
-#pragma unroll
-        for (int q = 0; q < NCAP; ++q)
-            if (q < n) S += ec[q] * ec[q];
-        const long long cell = ((long long)x * g.na + row) * g.nb + col;
-        double Sn = 0., pairs = 0.;
-#pragma unroll
-        for (int q = 0; q < NCAP; ++q) {
-            if (q >= n) break;
-            const double* e = eta + (long long)q * g.nstore + base;
-            const double c0 = ec[q];
-            double lap;
-            if (DIM == 3)
-                lap = fdiv<FAST>((en[q] - 2. * c0 + ep[q]), P.v_dxdx)
-                    + fdiv<FAST>((__ldg(e + cap) - 2. * c0 + __ldg(e + cam)), P.v_dada)
-                    + fdiv<FAST>((__ldg(e + cbp) - 2. * c0 + __ldg(e + cbm)), P.v_dbdb);
-            else
-                lap = fdiv<FAST>((en[q] - 2. * c0 + ep[q]), P.v_dxdx)
-                    + fdiv<FAST>((__ldg(e + cbp) - 2. * c0 + __ldg(e + cbm)), P.v_dbdb);
-            const double force = grain_deta(c0, S, phi, P.eta_W, P.eta_A) - P.eta_K * lap;
-            const double v = c0 - P.dt_etaL * force;
-            if (!isfinite(v) || v < -1.e-12 || v > 1. + 1.e-12)
-                errkey = min(errkey, ERR_ETA_BASE + (unsigned long long)q * (unsigned long long)g.ncells + (unsigned long long)cell);
-            eta_next[(long long)q * g.nstore + base + rc] = v;
-            const double sq = v * v;
-            pairs += Sn * sq;
-            Sn += sq;
-        }
-        s2_next[base + rc] = Sn;
-        gb_next[base + rc] = P.eta_scale * smin(1., 16. * pairs);
-#pragma unroll
-        for (int q = 0; q < NCAP; ++q)
-            if (q < n) { ep[q] = ec[q]; ec[q] = en[q]; }
-    }
-    if (errkey != ERR_NONE) atomicMin(&st->err_key, errkey);
-}
-
-// 2 CTAs/SM stated in the bounds: the register count stays <= 128 either way,
-// but the schedule compiled for it measured 15% faster on B200 (0.58 vs 0.69
-// ms at 256^3 with 8 fields, same box); bounds for 3 CTAs/SM spill and lose.
-template <int DIM, bool FAST, int N>
-__global__ void __launch_bounds__(256, 2)
-k_eta_march(const StepParams P, const double* __restrict__ eta, const double* __restrict__ p,
-            double* __restrict__ eta_next, double* __restrict__ gb_next, double* __restrict__ s2_next, Status* st) {
-    eta_march_body<DIM, FAST, N>(P, N, eta, p, eta_next, gb_next, s2_next, st, blockIdx.x, blockIdx.y, blockIdx.z);
-}
-
-template <int DIM, bool FAST, int N>
-static void launch_eta_march(const StepParams& P, const double* eta, const double* p, double* eta_next,
-                             double* gb_next, double* s2_next, Status* st, cudaStream_t stream) {
-    const Grid& g = P.g;
-    if (DIM == 3) {
-        const dim3 grid((g.nb + 31) / 32, (g.na + 7) / 8, (g.nx + P.xchunk - 1) / P.xchunk);
-        k_eta_march<3, FAST, N><<<grid, dim3(32, 8), 0, stream>>>(P, eta, p, eta_next, gb_next, s2_next, st);
-    } else {
-        const dim3 grid((g.nb + 127) / 128, 1, (g.nx + P.xchunk - 1) / P.xchunk);
-        k_eta_march<2, FAST, N><<<grid, dim3(128, 1), 0, stream>>>(P, eta, p, eta_next, gb_next, s2_next, st);
-    }
-}
-
-// Dispatch to the compile-time field counts 1..16; false when N is larger.
-template <int DIM, bool FAST>
-static bool eta_march_dispatch(int neta, const StepParams& P, const double* eta, const double* p, double* eta_next,
-                               double* gb_next, double* s2_next, Status* st, cudaStream_t stream) {
-    switch (neta) {
-#define NICR_ETA_CASE(n) \
-    case n: launch_eta_march<DIM, FAST, n>(P, eta, p, eta_next, gb_next, s2_next, st, stream); return true;
-        NICR_ETA_CASE(1) NICR_ETA_CASE(2) NICR_ETA_CASE(3) NICR_ETA_CASE(4) NICR_ETA_CASE(5) NICR_ETA_CASE(6)
-        NICR_ETA_CASE(7) NICR_ETA_CASE(8) NICR_ETA_CASE(9) NICR_ETA_CASE(10) NICR_ETA_CASE(11) NICR_ETA_CASE(12)
-        NICR_ETA_CASE(13) NICR_ETA_CASE(14) NICR_ETA_CASE(15) NICR_ETA_CASE(16)
-#undef NICR_ETA_CASE
-        default: return false;
-    }
-}
-
-// Streaming form of the eta update: each CTA owns a rows x columns tile,
-// marches along X and stages every eta plane once (radius-1 halo) in a
-// three-plane shared-memory ring, so every field is read from HBM about once.
-// S = sum eta_g^2 is rebuilt from the staged centres in g order, which is the
-// same arithmetic as rebuild_eta_mask and therefore the same value as eta_s2.
-template <int DIM, int TA, int TB, bool FAST>
-__global__ void __launch_bounds__(TA * TB)
-k_eta_stream(const StepParams P, int neta, const double* __restrict__ eta, const double* __restrict__ p,
-             double* __restrict__ eta_next, double* __restrict__ gb_next, double* __restrict__ s2_next,
-             Status* st) {
-    constexpr int HA = DIM == 3 ? 1 : 0;
-    constexpr int RA = TA + 2 * HA, RB = TB + 2, S1 = RA * RB, NT = TA * TB;
-    extern __shared__ __align__(16) double ring[];   // [3][neta][S1], then S1 int offsets
-    if (st->failed) return;
-    const Grid& g = P.g;
-    const int ta = DIM == 3 ? threadIdx.y : 0, tb = threadIdx.x;
-    const int a0 = DIM == 3 ? blockIdx.y * TA : 0, b0 = blockIdx.x * TB;
-    const int i0 = blockIdx.z * P.xchunk, i1 = min(g.nx, i0 + P.xchunk);
-    const int row = a0 + ta, col = b0 + tb;
-    const bool active = (DIM == 3 ? row < g.na : true) && col < g.nb;
-    const int tid = threadIdx.x + TB * threadIdx.y;
-    int* toff = reinterpret_cast<int*>(ring + (size_t)3 * neta * S1);
-    for (int r = tid; r < S1; r += NT) {
-        const int a = r / RB - HA, b = r % RB - 1;
-        toff[r] = (DIM == 3 ? wrapi(a0 + a, g.na) : 0) * g.pb + wrapi(b0 + b, g.nb);
-    }
-    __syncthreads();
-    auto slot = [&](int x) { return ring + (size_t)(((x % 3) + 3) % 3) * neta * S1; };
-    auto load = [&](int x) {
-        const int xg = x < 0 ? 0 : (x > g.nx - 1 ? g.nx - 1 : x);
-        double* dst = slot(x);
-        const double* src = eta + (long long)xg * g.plane;
-        for (int e = 0; e < neta; ++e) {
-            const double* se = src + (long long)e * g.nstore;
-            double* de = dst + e * S1;
-            for (int r = tid; r < S1; r += NT) de[r] = __ldg(se + toff[r]);
-        }
-    };
-    const int c1 = (ta + HA) * RB + (tb + 1);
-    const int bp = c1 + 1, bm = c1 - 1, ap = c1 + RB, am = c1 - RB;
-    unsigned long long errkey = ERR_NONE;
-    load(i0 - 1);
-    load(i0);
-    for (int u = i0; u < i1; ++u) {
-        load(u + 1);
-        __syncthreads();
-        if (active) {
-            const double* sm = slot(u - 1);
-            const double* s0 = slot(u);
-            const double* sp = slot(u + 1);
-            const long long idx = (long long)u * g.plane + (long long)row * g.pb + col;
-            const long long cell = ((long long)u * g.na + row) * g.nb + col;
-            double S = 0.;
-            for (int e = 0; e < neta; ++e) {
-                const double v = s0[e * S1 + c1];
-                S += v * v;
-            }
-            const double phi = __ldg(p + idx);
-            double Sn = 0., pairs = 0.;
-            for (int e = 0; e < neta; ++e) {
-                const int o = e * S1;
-                const double ec = s0[o + c1];
-                double lap;
-                if (DIM == 3)
-                    lap = fdiv<FAST>((sp[o + c1] - 2. * ec + sm[o + c1]), P.v_dxdx)
-                        + fdiv<FAST>((s0[o + ap] - 2. * ec + s0[o + am]), P.v_dada)
-                        + fdiv<FAST>((s0[o + bp] - 2. * ec + s0[o + bm]), P.v_dbdb);
-                else
-                    lap = fdiv<FAST>((sp[o + c1] - 2. * ec + sm[o + c1]), P.v_dxdx)
-                        + fdiv<FAST>((s0[o + bp] - 2. * ec + s0[o + bm]), P.v_dbdb);
-                const double force = grain_deta(ec, S, phi, P.eta_W, P.eta_A) - P.eta_K * lap;
-                const double v = ec - P.dt_etaL * force;
-                if (!isfinite(v) || v < -1.e-12 || v > 1. + 1.e-12)
-                    errkey = min(errkey, ERR_ETA_BASE + (unsigned long long)e * (unsigned long long)g.ncells + (unsigned long long)cell);
-                eta_next[(long long)e * g.nstore + idx] = v;
-                const double sq = v * v;
-                pairs += Sn * sq;
-                Sn += sq;
-            }
-            s2_next[idx] = Sn;
-            gb_next[idx] = P.eta_scale * smin(1., 16. * pairs);
-        }
-        __syncthreads();   // slot(u-1) is refilled with plane u+2 next
-    }
-    if (errkey != ERR_NONE) atomicMin(&st->err_key, errkey);
 }
 
 // Self-check of xdiv on the device: random numerators (all finite bit
@@ -877,28 +122,6 @@ __global__ void k_finalize_batch(const __grid_constant__ FinalizeBatch B) {
     finalize_body(d.partials, d.nblocks, d.budget, d.st, 0);
 }
 
-// Batched step: one launch advances up to kBatchMax domains of one
-// dimensionality and arithmetic form. The per-domain parameters and buffers
-// sit in the kernel's parameter space (read through the constant cache with a
-// block-uniform index); block b belongs to the last domain whose first block
-// is <= b and runs exactly the CTA (bx, by, bz) the single-domain launch would
-// run, with the same partial-sum slot, so every domain's result is identical
-// to its own nicr_step.
-template <int DIM, int TA, int TB, int MINB, bool FAST>
-__global__ void __launch_bounds__(TA * TB, MINB) k_step_batch(const __grid_constant__ StepBatch B) {
-    int lo = 0, hi = B.n - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (B.d[mid].block0 <= (int)blockIdx.x) lo = mid;
-        else hi = mid - 1;
-    }
-    const BatchDomain& D = B.d[lo];
-    const int t = (int)blockIdx.x - D.block0;
-    const int bx = t % D.gx, r = t / D.gx, by = r % D.gy, bz = r / D.gy;
-    StepKernel<DIM, TA, TB, FAST>::run(D.sp, D.o, D.cr, D.p, D.gb, D.s2, D.on, D.crn, D.pn, D.partials, D.st, bx, by,
-                                       bz, t);
-}
-
 // refresh() for output: mu at interior cells, M at interior cells.
 template <int DIM>
 __global__ void k_refresh(const StepParams P, const double* __restrict__ o, const double* __restrict__ cr,
@@ -938,24 +161,6 @@ __global__ void k_refresh(const StepParams P, const double* __restrict__ o, cons
 }  // namespace
 
 // ----------------------------------------------------------------- launchers
-// Dynamic shared memory above 48 KB is opted into per kernel and per device,
-// once (setting it again is harmless, skipping it on a second device is not).
-static void ensure_smem_attr(const void* kernel, int bytes) {
-    static std::mutex mu;
-    static std::set<std::pair<const void*, int>> done;
-    int dev = 0;
-    cudaGetDevice(&dev);
-    std::lock_guard<std::mutex> lock(mu);
-    if (done.insert({kernel, dev}).second)
-        cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-}
-// X chunk of the step and eta kernels. A CTA marching c planes also computes
-// mu and M of the plane before its chunk and stages that plane's halo, about
-// two planes of extra work, and CTAs run in waves of 2 (3D) or 4 (2D) per SM,
-// so the chunk minimising waves x (c + 2) is taken among nx halved repeatedly
-// and the powers of two below nx, the longer chunk on ties. Small domains get short chunks and use the whole GPU
-// (2D 128^2: 1 plane per CTA; 64^3: 4), large ones long chunks (256^3: 32).
-// NICR_XCHUNK forces a chunk for tuning runs.
 static long long step_tiles(const Grid& g) {
     return g.dim == 3 ? (long long)((g.nb + TB3 - 1) / TB3) * ((g.na + TA3 - 1) / TA3) : (g.nb + TB2 - 1) / TB2;
 }
@@ -1007,60 +212,22 @@ int step_main_blocks(const StepParams& P) {
     return (int)(grid.x * grid.y * grid.z);
 }
 
-// Occupancy variant of the 3D step kernel: 2 CTAs/SM (no register cap, the
-// default: with the staging loads software-pipelined it is measured faster on
-// B200) or 3 CTAs/SM (80 registers, which spills). NICR_STEP_MINB=2|3 selects
-// one for tuning runs.
-static int step_minb() {
-    static int v = 0;
-    if (!v) {
-        const char* e = getenv("NICR_STEP_MINB");
-        v = (e && e[0] == '3') ? 3 : 2;
-    }
-    return v;
-}
-
-template <int MINB, bool FAST>
-static void launch_step3(const StepParams& P, const double* o, const double* cr, const double* p, const double* gb,
-                         const double* s2, double* on, double* crn, double* pn, StepPartial* partials, Status* st,
-                         cudaStream_t stream, int* nblocks_out) {
-    using T = Tile<3, TA3, TB3>;
-    ensure_smem_attr((const void*)k_step_main<3, TA3, TB3, MINB, FAST>, (int)T::SMEM_BYTES);
-    const dim3 grid = step_grid<3, TA3, TB3>(P);
-    k_step_main<3, TA3, TB3, MINB, FAST><<<grid, dim3(TB3, TA3), T::SMEM_BYTES, stream>>>(P, o, cr, p, gb, s2, on, crn,
-                                                                                         pn, partials, st);
-    if (nblocks_out) *nblocks_out = (int)(grid.x * grid.y * grid.z);
-}
-
-template <bool FAST>
-static void launch_step_form(const StepParams& P, const double* o, const double* cr, const double* p,
-                             const double* gb, const double* s2, double* on, double* crn, double* pn,
-                             StepPartial* partials, Status* st, cudaStream_t stream, int* nblocks_out) {
-    if (P.g.dim == 3) {
-        if (step_minb() == 3) launch_step3<3, FAST>(P, o, cr, p, gb, s2, on, crn, pn, partials, st, stream, nblocks_out);
-        else launch_step3<2, FAST>(P, o, cr, p, gb, s2, on, crn, pn, partials, st, stream, nblocks_out);
-    } else {
-        using T = Tile<2, TA2, TB2>;
-        const dim3 grid = step_grid<2, TA2, TB2>(P);
-        k_step_main<2, TA2, TB2, 4, FAST><<<grid, dim3(TB2, TA2), T::SMEM_BYTES, stream>>>(P, o, cr, p, gb, s2, on,
-                                                                                          crn, pn, partials, st);
-        if (nblocks_out) *nblocks_out = (int)(grid.x * grid.y * grid.z);
-    }
-}
-
 void step_kernels_prepare(const StepParams& P) {
+    if (P.fast) {
+        step_kernels_prepare_fast(P);
+        return;
+    }
     if (P.g.dim != 3) return;   // the 2D tile fits the default 48 KB
     using T = Tile<3, TA3, TB3>;
     const bool m3 = step_minb() == 3;
-    const void* k = P.fast ? (m3 ? (const void*)k_step_main<3, TA3, TB3, 3, true> : (const void*)k_step_main<3, TA3, TB3, 2, true>)
-                           : (m3 ? (const void*)k_step_main<3, TA3, TB3, 3, false> : (const void*)k_step_main<3, TA3, TB3, 2, false>);
+    const void* k = m3 ? (const void*)k_step_main<3, TA3, TB3, 3, false> : (const void*)k_step_main<3, TA3, TB3, 2, false>;
     ensure_smem_attr(k, (int)T::SMEM_BYTES);
 }
 
 void launch_step_main(const StepParams& P, const double* o, const double* cr, const double* p, const double* gb,
                       const double* s2, double* on, double* crn, double* pn, StepPartial* partials, Status* st,
                       cudaStream_t stream, int* nblocks_out) {
-    if (P.fast) launch_step_form<true>(P, o, cr, p, gb, s2, on, crn, pn, partials, st, stream, nblocks_out);
+    if (P.fast) launch_step_main_fast(P, o, cr, p, gb, s2, on, crn, pn, partials, st, stream, nblocks_out);
     else launch_step_form<false>(P, o, cr, p, gb, s2, on, crn, pn, partials, st, stream, nblocks_out);
 }
 
@@ -1073,58 +240,9 @@ void launch_eta_mask(const StepParams& P, int neta, const double* eta, double* g
     k_eta_mask<<<blocks, threads, 0, stream>>>(P, neta, eta, gb, s2, pairs, st);
 }
 
-template <bool FAST>
-static void launch_eta_form(const StepParams& P, int neta, const double* eta, const double* s2, const double* p,
-                            double* eta_next, double* gb_next, double* s2_next, Status* st, cudaStream_t stream) {
-    const Grid& g = P.g;
-    // The streaming kernel stalls on its per-plane barriers until the next
-    // plane has arrived; it is kept only as a tuning option.
-    // Kernel choice (measured on B200 at 256^3 with 8 fields): the X-marching
-    // kernel for the reciprocal form (0.63 ms vs 0.94 ms per step), the
-    // per-cell kernel for the drop-in form, where the unrolled verified
-    // divisions of the marching kernel cost more than its saved loads (1.84 ms
-    // vs 1.29 ms). NICR_ETA_KERNEL=march|simple|stream overrides for tuning.
-    static int simple = -1, march = -1;
-    if (simple < 0) {
-        const char* e = getenv("NICR_ETA_KERNEL");
-        simple = (e && e[0] == 's' && e[1] == 't') ? 0 : 1;
-        march = e ? (e[0] == 'm' ? 1 : 0) : -2;
-    }
-    if (march == 1 || (march == -2 && FAST)) {
-        const bool done = g.dim == 3 ? eta_march_dispatch<3, FAST>(neta, P, eta, p, eta_next, gb_next, s2_next, st, stream)
-                                     : eta_march_dispatch<2, FAST>(neta, P, eta, p, eta_next, gb_next, s2_next, st, stream);
-        if (done) return;
-    }
-    if (g.dim == 3) {
-        constexpr int TA = 8, TB = 32, S1 = (TA + 2) * (TB + 2);
-        const size_t smem = (size_t)3 * neta * S1 * sizeof(double) + S1 * sizeof(int);
-        if (!simple && smem <= 200 * 1024) {
-            ensure_smem_attr((const void*)k_eta_stream<3, TA, TB, FAST>, 200 * 1024);
-            const dim3 grid((g.nb + TB - 1) / TB, (g.na + TA - 1) / TA, (g.nx + P.xchunk - 1) / P.xchunk);
-            k_eta_stream<3, TA, TB, FAST><<<grid, dim3(TB, TA), smem, stream>>>(P, neta, eta, p, eta_next, gb_next, s2_next, st);
-            return;
-        }
-        const dim3 block(32, 8);
-        const dim3 grid((g.nb + 31) / 32, (g.na + 7) / 8, g.nx);
-        k_eta_update<3, FAST><<<grid, block, 0, stream>>>(P, neta, eta, s2, p, eta_next, gb_next, s2_next, st);
-    } else {
-        constexpr int TB = 128, S1 = TB + 2;
-        const size_t smem = (size_t)3 * neta * S1 * sizeof(double) + S1 * sizeof(int);
-        if (!simple && smem <= 200 * 1024) {
-            ensure_smem_attr((const void*)k_eta_stream<2, 1, TB, FAST>, 200 * 1024);
-            const dim3 grid((g.nb + TB - 1) / TB, 1, (g.nx + P.xchunk - 1) / P.xchunk);
-            k_eta_stream<2, 1, TB, FAST><<<grid, dim3(TB, 1), smem, stream>>>(P, neta, eta, p, eta_next, gb_next, s2_next, st);
-            return;
-        }
-        const dim3 block(128, 1);
-        const dim3 grid((g.nb + 127) / 128, 1, g.nx);
-        k_eta_update<2, FAST><<<grid, block, 0, stream>>>(P, neta, eta, s2, p, eta_next, gb_next, s2_next, st);
-    }
-}
-
 void launch_eta_update(const StepParams& P, int neta, const double* eta, const double* s2, const double* p,
                        double* eta_next, double* gb_next, double* s2_next, Status* st, cudaStream_t stream) {
-    if (P.fast) launch_eta_form<true>(P, neta, eta, s2, p, eta_next, gb_next, s2_next, st, stream);
+    if (P.fast) launch_eta_update_fast(P, neta, eta, s2, p, eta_next, gb_next, s2_next, st, stream);
     else launch_eta_form<false>(P, neta, eta, s2, p, eta_next, gb_next, s2_next, st, stream);
 }
 
@@ -1140,13 +258,6 @@ void launch_finalize_batch(const FinalizeDomain* doms, int n, cudaStream_t strea
         for (int i = 0; i < B.n; ++i) B.d[i] = doms[i0 + i];
         k_finalize_batch<<<B.n, 256, 0, stream>>>(B);
     }
-}
-
-template <int DIM, int TA, int TB, int MINB, bool FAST>
-static void launch_batch_group(StepBatch& B, int nblocks, cudaStream_t stream) {
-    using T = Tile<DIM, TA, TB>;
-    ensure_smem_attr((const void*)k_step_batch<DIM, TA, TB, MINB, FAST>, (int)T::SMEM_BYTES);
-    k_step_batch<DIM, TA, TB, MINB, FAST><<<nblocks, dim3(TB, TA), T::SMEM_BYTES, stream>>>(B);
 }
 
 int launch_step_batch(BatchDomain* doms, int n, cudaStream_t stream) {
@@ -1168,13 +279,9 @@ int launch_step_batch(BatchDomain* doms, int n, cudaStream_t stream) {
             B.d[B.n++] = d;
             ++i;
         }
-        if (dim == 3) {
-            if (fast) launch_batch_group<3, TA3, TB3, 2, true>(B, nb, stream);
-            else launch_batch_group<3, TA3, TB3, 2, false>(B, nb, stream);
-        } else {
-            if (fast) launch_batch_group<2, TA2, TB2, 4, true>(B, nb, stream);
-            else launch_batch_group<2, TA2, TB2, 4, false>(B, nb, stream);
-        }
+        if (fast) launch_batch_group_fast(B, nb, dim, stream);
+        else if (dim == 3) launch_batch_group<3, TA3, TB3, 2, false>(B, nb, stream);
+        else launch_batch_group<2, TA2, TB2, 4, false>(B, nb, stream);
         ++launches;
     }
     return launches;

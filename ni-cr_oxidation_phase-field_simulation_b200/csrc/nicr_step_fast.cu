@@ -1,0 +1,36 @@
+// The reciprocal-division form (NICR_FP64_FAST) of the step and eta kernels.
+// This unit is compiled with FMA contraction (nvcc -fmad=true): the form
+// already trades bit-identity for speed (division by a run constant becomes a
+// multiplication by its rounded reciprocal), and fused multiply-adds remove a
+// third of its FP64 instructions at an error of the same order (a few ulp per
+// step, far inside the 1e-4 bound against the drop-in form). The kernels are
+// the shared templates of nicr_step_impl.cuh, instantiated with FAST = true.
+#include "nicr_step_impl.cuh"
+
+namespace nicr {
+
+void launch_step_main_fast(const StepParams& P, const double* o, const double* cr, const double* p, const double* gb,
+                           const double* s2, double* on, double* crn, double* pn, StepPartial* partials, Status* st,
+                           cudaStream_t stream, int* nblocks_out) {
+    launch_step_form<true>(P, o, cr, p, gb, s2, on, crn, pn, partials, st, stream, nblocks_out);
+}
+
+void launch_eta_update_fast(const StepParams& P, int neta, const double* eta, const double* s2, const double* p,
+                            double* eta_next, double* gb_next, double* s2_next, Status* st, cudaStream_t stream) {
+    launch_eta_form<true>(P, neta, eta, s2, p, eta_next, gb_next, s2_next, st, stream);
+}
+
+void launch_batch_group_fast(StepBatch& B, int nblocks, int dim, cudaStream_t stream) {
+    if (dim == 3) launch_batch_group<3, TA3, TB3, 2, true>(B, nblocks, stream);
+    else launch_batch_group<2, TA2, TB2, 4, true>(B, nblocks, stream);
+}
+
+void step_kernels_prepare_fast(const StepParams& P) {
+    if (P.g.dim != 3) return;   // the 2D tile fits the default 48 KB
+    using T = Tile<3, TA3, TB3>;
+    const void* k = step_minb() == 3 ? (const void*)k_step_main<3, TA3, TB3, 3, true>
+                                     : (const void*)k_step_main<3, TA3, TB3, 2, true>;
+    ensure_smem_attr(k, (int)T::SMEM_BYTES);
+}
+
+}  // namespace nicr
