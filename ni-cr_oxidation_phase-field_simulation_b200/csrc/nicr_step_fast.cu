@@ -1,10 +1,11 @@
 // The reciprocal-division form (NICR_FP64_FAST) of the step and eta kernels.
 // This unit is compiled with FMA contraction (nvcc -fmad=true): the form
 // already trades bit-identity for speed (division by a run constant becomes a
-// multiplication by its rounded reciprocal), and fused multiply-adds remove a
-// third of its FP64 instructions at an error of the same order (a few ulp per
-// step, far inside the 1e-4 bound against the drop-in form). The kernels are
-// the shared templates of nicr_step_impl.cuh, instantiated with FAST = true.
+// multiplication by its rounded reciprocal), and fused multiply-adds change
+// its results by a few ulp per step, far inside the 1e-4 bound against the
+// drop-in form (measured 4e-16 after 203 steps at 256^3), for 3-4% less time
+// in both kernels on B200. The kernels are the shared templates of
+// nicr_step_impl.cuh, instantiated with FAST = true.
 #include "nicr_step_impl.cuh"
 
 namespace nicr {
