@@ -441,15 +441,18 @@ struct StepKernel {
                     const double dO = fdiv<FAST>(-Phys::ckO * ((Phys::oxideO - onv) * hn - (Phys::oxideO - oo) * C.hh), P.v_dt);
                     const double dCr = fdiv<FAST>(-Phys::ckCr * ((Phys::oxideCr - crv) * hn - (Phys::oxideCr - cc) * C.hh), P.v_dt);
                     onv += dO; crv += dCr;
-                    acc[0] = dd_add(acc[0], dO);
-                    acc[1] = dd_add(acc[1], dCr);
+                    // adding +-0 to a normalised double-double leaves it unchanged,
+                    // so zero increments (metal cells: h(pn) == h(p) == 0) are skipped
+                    if (dO != 0.) acc[0] = dd_add(acc[0], dO);
+                    if (dCr != 0.) acc[1] = dd_add(acc[1], dCr);
                 }
                 if (!isfinite(onv) || !isfinite(crv) || !isfinite(pnv)) {
                     errkey = min(errkey, (unsigned long long)cell * 4ull);
                 } else if (P.bounds == 1) {
                     const double oc = sclamp(onv, 0., 1.), ccr = sclamp(crv, 0., 1.);
-                    acc[2] = dd_add(acc[2], oc - onv);
-                    acc[3] = dd_add(acc[3], ccr - crv);
+                    const double clO = oc - onv, clCr = ccr - crv;
+                    if (clO != 0.) acc[2] = dd_add(acc[2], clO);
+                    if (clCr != 0.) acc[3] = dd_add(acc[3], clCr);
                     if (oc != onv || ccr != crv) ++clipped;
                     onv = oc; crv = ccr;
                     if (pnv > .99999) pnv = 1.;
