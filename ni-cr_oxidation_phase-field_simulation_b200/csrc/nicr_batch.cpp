@@ -23,11 +23,89 @@ struct nicr_batch {
 
     ~nicr_batch() {
         if (stream) cudaStreamSynchronize(stream);
+        for (auto& q : graphs)
+            if (q.exec) cudaGraphExecDestroy(q.exec);
         for (nicr_handle* h : doms) {
             delete h->m;
             delete h;
         }
         if (stream) cudaStreamDestroy(stream);
+    }
+
+    // Advances every domain nsteps steps (run() schedule when `schedule`).
+    // Step pairs of the whole batch captured as CUDA graphs, one per parity
+    // state of all domains (they toggle together; a domain that was rolled
+    // back after a failed trial may differ), replayed when no domain scans
+    // for Ksp in either step. Each graph holds the grouped step launches, the
+    // domains' eta updates and the batched commit of two steps.
+    struct PairGraph {
+        std::vector<int> key;
+        cudaGraphExec_t exec = nullptr;
+        long long batch_kernels = 0;
+        std::vector<long long> domain_kernels;
+    };
+    std::vector<PairGraph> graphs;
+
+    void enqueue_step(std::vector<nicr::BatchDomain>& descs, std::vector<nicr::FinalizeDomain>& fins) {
+        const int n = (int)doms.size();
+        for (int i = 0; i < n; ++i) {
+            nicr::Model& m = *doms[i]->m;
+            m.prepare_step();
+            descs[i] = m.step_desc();
+        }
+        launches += nicr::launch_step_batch(descs.data(), n, stream);
+        for (int i = 0; i < n; ++i) {
+            nicr::Model& m = *doms[i]->m;
+            m.complete_step(descs[i].nblocks, false);
+            fins[i] = m.finalize_desc(descs[i].nblocks);
+        }
+        nicr::launch_finalize_batch(fins.data(), n, stream);
+        launches += (n + nicr::kFinalizeMax - 1) / nicr::kFinalizeMax;
+    }
+
+    void launch_pair(std::vector<nicr::BatchDomain>& descs, std::vector<nicr::FinalizeDomain>& fins) {
+        const int n = (int)doms.size();
+        std::vector<int> key((size_t)n);
+        for (int i = 0; i < n; ++i) {
+            doms[i]->m->prepare_step();   // stale eta masks are rebuilt outside the graph
+            key[i] = doms[i]->m->parity_key();
+        }
+        PairGraph* pg = nullptr;
+        for (auto& q : graphs)
+            if (q.key == key) pg = &q;
+        if (!pg) {
+            if (graphs.size() >= 4) {   // parities this varied: drop the oldest capture
+                cudaGraphExecDestroy(graphs.front().exec);
+                graphs.erase(graphs.begin());
+            }
+            for (auto* h : doms) nicr::step_kernels_prepare(h->m->params());
+            PairGraph q;
+            q.key = key;
+            const long long b0 = launches;
+            std::vector<long long> d0((size_t)n);
+            for (int i = 0; i < n; ++i) d0[i] = doms[i]->m->launches;
+            cudaGraph_t graph = nullptr;
+            nicr::check_cuda(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
+            enqueue_step(descs, fins);
+            enqueue_step(descs, fins);
+            nicr::check_cuda(cudaStreamEndCapture(stream, &graph), "cudaStreamEndCapture");
+            const cudaError_t e = cudaGraphInstantiate(&q.exec, graph, 0);
+            cudaGraphDestroy(graph);
+            nicr::check_cuda(e, "cudaGraphInstantiate");
+            // nothing ran while capturing: each replay counts the kernels
+            q.batch_kernels = launches - b0;
+            launches = b0;
+            q.domain_kernels.resize((size_t)n);
+            for (int i = 0; i < n; ++i) {
+                q.domain_kernels[i] = doms[i]->m->launches - d0[i];
+                doms[i]->m->launches = d0[i];
+            }
+            graphs.push_back(std::move(q));
+            pg = &graphs.back();
+        }
+        nicr::check_cuda(cudaGraphLaunch(pg->exec, stream), "cudaGraphLaunch");
+        launches += pg->batch_kernels;
+        for (int i = 0; i < n; ++i) doms[i]->m->launches += pg->domain_kernels[i];
     }
 
     // Advances every domain nsteps steps (run() schedule when `schedule`).
@@ -40,21 +118,19 @@ struct nicr_batch {
         std::vector<nicr::BatchDomain> descs((size_t)n);
         std::vector<nicr::FinalizeDomain> fins((size_t)n);
         for (int i = 0; i < n; ++i) doms[i]->m->run_begin(plans[i], nsteps, schedule);
-        for (int s = 0; s < nsteps; ++s) {
-            for (int i = 0; i < n; ++i) {
-                nicr::Model& m = *doms[i]->m;
-                m.run_pre_step(plans[i], s);
-                m.prepare_step();
-                descs[i] = m.step_desc();
+        const bool use_graphs = doms[0]->m->graphs_enabled();
+        for (int s = 0; s < nsteps;) {
+            for (int i = 0; i < n; ++i) doms[i]->m->run_pre_step(plans[i], s);
+            bool pair = use_graphs && s + 1 < nsteps;
+            for (int i = 0; pair && i < n; ++i) pair = !doms[i]->m->ksp_due(plans[i], s + 1);
+            if (pair) {
+                launch_pair(descs, fins);
+                for (int i = 0; i < n; ++i) doms[i]->m->run_pre_step(plans[i], s + 1);   // schedule entry only
+                s += 2;
+            } else {
+                enqueue_step(descs, fins);
+                ++s;
             }
-            launches += nicr::launch_step_batch(descs.data(), n, stream);
-            for (int i = 0; i < n; ++i) {
-                nicr::Model& m = *doms[i]->m;
-                m.complete_step(descs[i].nblocks, false);
-                fins[i] = m.finalize_desc(descs[i].nblocks);
-            }
-            nicr::launch_finalize_batch(fins.data(), n, stream);
-            launches += (n + nicr::kFinalizeMax - 1) / nicr::kFinalizeMax;
         }
         int rc = NICR_OK;
         err.clear();

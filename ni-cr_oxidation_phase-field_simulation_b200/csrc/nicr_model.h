@@ -105,6 +105,11 @@ public:
     BatchDomain step_desc() const;
     FinalizeDomain finalize_desc(int nblocks) const;
     void complete_step(int nblocks, bool finalize);
+    // step-pair graphs: whether they are used, whether step s of plan r
+    // starts with a Ksp scan, and the buffer parity a captured pair keys on
+    bool graphs_enabled() const;
+    bool ksp_due(const RunPlan& r, int s) const;
+    int parity_key() const { return cur | (ecur << 1) | (gcur << 2); }
     void run_begin(RunPlan& r, int nsteps, bool schedule);
     void run_pre_step(RunPlan& r, int s);
     int run_end(RunPlan& r, int* completed);
@@ -181,8 +186,6 @@ private:
         long long kernels = 0;
     };
     PairGraph pair_graphs[8];
-    bool graphs_enabled() const;
-    bool ksp_due(const RunPlan& r, int s) const;
     void launch_step_pair();
 
     void release();

@@ -80,3 +80,48 @@ def test_graph_pairs_match_plain_launches(require_gpu, tmp_path, name):
     assert ja["launches"] == jb["launches"]
     if name == "3d-rejection":
         assert ja["rcs"][0][0] != 0
+
+
+BATCH_CHILD = textwrap.dedent("""
+    import sys, json, numpy as np
+    sys.path.insert(0, sys.argv[1] + "/ni-cr_oxidation_phase-field_simulation_b200"); sys.path.insert(0, sys.argv[1] + "/tests")
+    import nicr
+    from nicr.sweep import sweep_configs
+    from parity import smooth_fields
+    out = sys.argv[2]
+    base = dict(bounds="legacy", nucleation="ksp", dt=1e-12, radius_grid=2.5, nucleation_period=5e-12)
+    cfgs = sweep_configs(5, seed=11, edges=(20, 33, 40), **base)
+    cfgs.append(nicr.make_config(3, nx=24, ny=19, nz=35, grains=1, grain_evolution=1, grain_diameter_grid=10., bc="mu", **base))
+    cfgs.append(nicr.make_config(2, nx=61, ny=45, grains=1, grain_diameter_grid=12., **base))
+    with nicr.Batch(cfgs) as b:
+        for i, d in enumerate(b.domains):
+            o, cr, p, eta = smooth_fields(d.shape, d.n_eta, seed=i)
+            d.set_fields(o, cr, p, eta if eta else None)
+            d.reset_inventory()
+        res = []
+        for n in (7, 12, 1, 9):
+            res.append(b.run(n, check=False))
+        arrs = {}
+        for i, d in enumerate(b.domains):
+            for f in ("o", "cr", "p", "gb"):
+                arrs["%d_%s" % (i, f)] = d.get(f)
+        np.savez(out, **arrs)
+        json.dump({"res": res, "budgets": [d.budget() for d in b.domains], "launches": b.kernel_launches,
+                   "nuclei": sum(d.budget()["nuclei"] for d in b.domains)}, open(out + ".json", "w"))
+""")
+
+
+def test_batch_graph_pairs_match_plain_launches(require_gpu, tmp_path):
+    outs = []
+    for graphs in ("1", "0"):
+        out = tmp_path / f"batch{graphs}"
+        env = dict(os.environ, NICR_GRAPHS=graphs)
+        r = subprocess.run([sys.executable, "-c", BATCH_CHILD, str(ROOT), str(out)], env=env, capture_output=True,
+                           text=True, timeout=600)
+        assert r.returncode == 0, r.stderr
+        outs.append((np.load(str(out) + ".npz"), json.load(open(str(out) + ".json"))))
+    (a, ja), (b, jb) = outs
+    for k in b.files:
+        assert np.array_equal(a[k].view(np.int64), b[k].view(np.int64)), k
+    assert ja["res"] == jb["res"] and ja["budgets"] == jb["budgets"] and ja["launches"] == jb["launches"]
+    assert ja["nuclei"] > 0
