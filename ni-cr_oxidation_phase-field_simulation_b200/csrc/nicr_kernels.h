@@ -30,7 +30,7 @@ struct Grid {
 struct Status {
     unsigned long long err_key;   // ERR_NONE when no trial failed this step
     int failed;                   // a step of this batch was rejected
-    int pad;
+    int timeout;                  // a kernel's bounded wait for its own copies ran out
     long long failed_step;        // index (steps_done) of the rejected step
     long long steps_done;         // accepted steps since creation
 };

@@ -608,6 +608,7 @@ void Model::reset_status() {
     // keep steps_done; clear the failure state for a new batch
     h_st->err_key = ERR_NONE;
     h_st->failed = 0;
+    h_st->timeout = 0;
     h_st->failed_step = -1;
     h_st->steps_done = steps_done;
     check_cuda(cudaMemcpyAsync(st, h_st, sizeof(Status), cudaMemcpyHostToDevice, stream), "H2D");
@@ -721,6 +722,8 @@ int Model::finish_batch(long long before, int enqueued, const std::vector<double
     sync();
     check_cuda(cudaGetLastError(), "step kernels");
     profile_collect();
+    if (h_st->timeout)
+        throw Error(NICR_ERR_CUDA, "a step kernel's bounded wait for its own copies ran out; the step results are not valid");
     if (!h_st->failed) {
         steps_done = before + enqueued;
         if (completed) *completed = enqueued;

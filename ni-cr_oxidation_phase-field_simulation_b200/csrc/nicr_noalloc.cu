@@ -46,6 +46,7 @@ std::mutex g_mu;
 __global__ void k_status_clear(nicr::Status* st) {
     st->err_key = nicr::ERR_NONE;
     st->failed = 0;
+    st->timeout = 0;
     st->failed_step = -1;
 }
 

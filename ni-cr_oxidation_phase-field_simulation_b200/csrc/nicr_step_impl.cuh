@@ -10,11 +10,26 @@
 #include <set>
 #include <utility>
 #include <vector>
+#include <cuda.h>
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 #include "nicr_kernels.h"
 #include "nicr_physics.h"
 
 namespace nicr {
+
+// Dynamic shared memory above 48 KB is opted into per kernel and per device,
+// once (setting it again is harmless, skipping it on a second device is not).
+static void ensure_smem_attr(const void* kernel, int bytes) {
+    static std::mutex mu;
+    static std::set<std::pair<const void*, int>> done;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lock(mu);
+    if (done.insert({kernel, dev}).second)
+        cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+}
+
 namespace {
 
 __device__ __forceinline__ int wrapi(int v, int n) {
@@ -683,6 +698,250 @@ static bool eta_march_dispatch(int neta, const StepParams& P, const double* eta,
     }
 }
 
+// TMA-staged form of the eta update (3D, row count a multiple of 8, column
+// count a multiple of 32, N <= 16 fields), selected by NICR_ETA_KERNEL=tma.
+// Measured at 256^3 with 8 fields it is slower than the register march
+// (0.72 vs 0.58 ms reciprocal, 1.31 vs 1.15 ms drop-in): the per-plane
+// barrier and the seven shared-memory reads per field leave 16 warps per SM
+// latency-bound, where the march runs barrier-free from registers and L1. Each CTA owns an 8 x 32 tile and
+// marches along its X chunk; one thread stages every plane of all N fields
+// with five tensor copies (cp.async.bulk.tensor, the fields as the fourth
+// dimension): the tile, the two halo rows (periodic wrap by coordinate) and
+// the two 2-column halo strips, into a four-plane shared-memory ring whose
+// slots complete on mbarriers. The copy of plane x+2 is issued while plane x
+// is updated, and the threads read the stencil from shared memory, so the
+// loads hold no registers and cost one instruction per box. Every x
+// coordinate is b0, b0 +- 2, b0 + 32, nb - 2 or 0: a multiple of 2 doubles
+// (16 bytes) because nb is a multiple of 32. Waits are bounded: a wait that
+// runs out sets st->timeout, and the CTA returns after a bounded wait for its
+// copies in flight. The arithmetic is the other forms' (same operand order).
+__device__ __forceinline__ unsigned smem_u32(const void* ptr) { return (unsigned)__cvta_generic_to_shared(ptr); }
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+    unsigned done;
+    asm volatile(
+        "{\n"
+        " .reg .pred p;\n"
+        " mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n"
+        "}\n"
+        : "=r"(done)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+__device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, int x, int y, int z, int w,
+                                            unsigned long long* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+        "[%6];\n" ::"r"(smem_u32(dst)),
+        "l"(map), "r"(x), "r"(y), "r"(z), "r"(w), "r"(smem_u32(bar))
+        : "memory");
+}
+
+constexpr int kTmaRing = 4;
+constexpr long long kTmaWaitLimit = 1LL << 22;   // try_wait rounds before a wait is declared lost
+
+template <int N>
+struct TmaStage {
+    static constexpr int TA = 8, TB = 32;
+    static constexpr int INT = N * TA * TB, ROW = N * TB, COL = N * TA * 2;
+    static constexpr int DOUBLES = INT + 2 * ROW + 2 * COL;   // 128-byte multiple for every N
+    static constexpr unsigned BYTES = DOUBLES * 8;
+    static constexpr size_t SMEM = (size_t)kTmaRing * BYTES + 128;   // + alignment slack
+};
+
+template <bool FAST, int N>
+__global__ void __launch_bounds__(256, 2)
+k_eta_tma(const StepParams P, const __grid_constant__ CUtensorMap m_int, const __grid_constant__ CUtensorMap m_row,
+          const __grid_constant__ CUtensorMap m_col, const double* __restrict__ p, double* __restrict__ eta_next,
+          double* __restrict__ gb_next, double* __restrict__ s2_next, Status* st) {
+    using S = TmaStage<N>;
+    constexpr int TA = S::TA, TB = S::TB;
+    extern __shared__ unsigned char tma_smem_raw[];
+    __shared__ unsigned long long bars[kTmaRing];
+    if (st->failed) return;
+    const Grid& g = P.g;
+    double* ring = reinterpret_cast<double*>(((unsigned long long)tma_smem_raw + 127ull) & ~127ull);
+    const int ta = threadIdx.y, tb = threadIdx.x, tid = tb + TB * ta;
+    const int a0 = blockIdx.y * TA, b0 = blockIdx.x * TB;
+    const int i0 = blockIdx.z * P.xchunk, i1 = min(g.nx, i0 + P.xchunk);
+    const int row = a0 + ta, col = b0 + tb;
+    const int ytop = a0 == 0 ? g.na - 1 : a0 - 1, ybot = a0 + TA == g.na ? 0 : a0 + TA;
+    const int xl = b0 == 0 ? g.nb - 2 : b0 - 2, xr = b0 + TB == g.nb ? 0 : b0 + TB;
+    // plane q >= i0 - 1 lives in ring slot (q - i0 + 1) % kTmaRing
+    auto slot_of = [&](int q) { return (q - i0 + 1) % kTmaRing; };
+    auto stage_of = [&](int q) { return ring + (size_t)slot_of(q) * S::DOUBLES; };
+    auto issue = [&](int q) {   // thread 0
+        const int xg = q < 0 ? 0 : (q > g.nx - 1 ? g.nx - 1 : q);
+        double* s = stage_of(q);
+        unsigned long long* bar = &bars[slot_of(q)];
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        mbar_expect_tx(bar, S::BYTES);
+        tma_load_4d(s, &m_int, b0, a0, xg, 0, bar);
+        tma_load_4d(s + S::INT, &m_row, b0, ytop, xg, 0, bar);
+        tma_load_4d(s + S::INT + S::ROW, &m_row, b0, ybot, xg, 0, bar);
+        tma_load_4d(s + S::INT + 2 * S::ROW, &m_col, xl, a0, xg, 0, bar);
+        tma_load_4d(s + S::INT + 2 * S::ROW + S::COL, &m_col, xr, a0, xg, 0, bar);
+    };
+    bool ok = true;
+    auto wait = [&](int q) {
+        const int k = q - i0 + 1;
+        const unsigned parity = (unsigned)((k / kTmaRing) & 1);
+        unsigned long long* bar = &bars[k % kTmaRing];
+        for (long long it = 0; ok && !mbar_try_wait(bar, parity); ++it)
+            if (it > kTmaWaitLimit) ok = false;
+    };
+    if (tid == 0) {
+        for (int r = 0; r < kTmaRing; ++r) mbar_init(&bars[r], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    __syncthreads();
+    int issued = i0 - 2;   // last plane whose copy was issued
+    if (tid == 0) {
+        for (int q = i0 - 1; q <= i0 + 1 && q <= i1; ++q) issue(q);
+    }
+    issued = min(i0 + 1, i1);
+    wait(i0 - 1);
+    wait(i0);
+    const long long own = (long long)row * g.pb + col;
+    const int c = ta * TB + tb;   // own point in the tile
+    unsigned long long errkey = ERR_NONE;
+    int x = i0;
+    for (; x < i1; ++x) {
+        // all threads finished plane x-1 (the slot of plane x+2 held plane x-2)
+        if (__syncthreads_or(!ok)) break;
+        if (x + 2 <= i1) {
+            if (tid == 0) issue(x + 2);
+            issued = x + 2;
+        }
+        wait(x + 1);
+        if (!ok) continue;   // reported at the next barrier
+        const double* sm = stage_of(x - 1);
+        const double* s0 = stage_of(x);
+        const double* sp = stage_of(x + 1);
+        const double* top = s0 + S::INT;
+        const double* bot = top + S::ROW;
+        const double* lft = bot + S::ROW;
+        const double* rgt = lft + S::COL;
+        const long long base = (long long)x * g.plane;
+        const double phi = __ldg(p + base + own);
+        double S2 = 0.;
+#pragma unroll
+        for (int q = 0; q < N; ++q) {
+            const double v = s0[q * TA * TB + c];
+            S2 += v * v;
+        }
+        const long long cell = ((long long)x * g.na + row) * g.nb + col;
+        double Sn = 0., pairs = 0.;
+#pragma unroll
+        for (int q = 0; q < N; ++q) {
+            const int o = q * TA * TB;
+            const double c0 = s0[o + c];
+            const double am = ta == 0 ? top[q * TB + tb] : s0[o + c - TB];
+            const double ap = ta == TA - 1 ? bot[q * TB + tb] : s0[o + c + TB];
+            const double bm = tb == 0 ? lft[(q * TA + ta) * 2 + 1] : s0[o + c - 1];
+            const double bp = tb == TB - 1 ? rgt[(q * TA + ta) * 2] : s0[o + c + 1];
+            const double lap = fdiv<FAST>((sp[o + c] - 2. * c0 + sm[o + c]), P.v_dxdx)
+                             + fdiv<FAST>((ap - 2. * c0 + am), P.v_dada)
+                             + fdiv<FAST>((bp - 2. * c0 + bm), P.v_dbdb);
+            const double force = grain_deta(c0, S2, phi, P.eta_W, P.eta_A) - P.eta_K * lap;
+            const double v = c0 - P.dt_etaL * force;
+            if (!isfinite(v) || v < -1.e-12 || v > 1. + 1.e-12)
+                errkey = min(errkey, ERR_ETA_BASE + (unsigned long long)q * (unsigned long long)g.ncells + (unsigned long long)cell);
+            eta_next[(long long)q * g.nstore + base + own] = v;
+            const double sq = v * v;
+            pairs += Sn * sq;
+            Sn += sq;
+        }
+        s2_next[base + own] = Sn;
+        gb_next[base + own] = P.eta_scale * smin(1., 16. * pairs);
+    }
+    if (__syncthreads_or(!ok)) {
+        // a wait ran out: flag it, give the copies in flight a bounded time to land, leave
+        if (tid == 0) {
+            atomicOr(&st->timeout, 1);
+            for (int q = i0 - 1; q <= issued; ++q) {
+                const int k = q - i0 + 1;
+                unsigned long long* bar = &bars[k % kTmaRing];
+                for (long long it = 0; it <= kTmaWaitLimit && !mbar_try_wait(bar, (unsigned)((k / kTmaRing) & 1)); ++it) {
+                }
+            }
+        }
+        __syncthreads();
+        return;
+    }
+    if (errkey != ERR_NONE) atomicMin(&st->err_key, errkey);
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (the
+// library links the CUDA runtime statically and not libcuda).
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+    }
+    return fn;
+}
+
+// The N eta fields of one buffer as a 4D tensor (columns, rows, planes,
+// fields), boxes of bx x by x 1 x N.
+static bool encode_eta_map(CUtensorMap* m, const Grid& g, int n, const double* eta, unsigned bx, unsigned by) {
+    const auto enc = tensor_map_encoder();
+    if (!enc) return false;
+    const cuuint64_t dims[4] = {(cuuint64_t)g.nb, (cuuint64_t)g.na, (cuuint64_t)g.nx, (cuuint64_t)n};
+    const cuuint64_t strides[3] = {(cuuint64_t)g.pb * 8, (cuuint64_t)g.plane * 8, (cuuint64_t)g.nstore * 8};
+    const cuuint32_t box[4] = {bx, by, 1, (cuuint32_t)n};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, const_cast<double*>(eta), dims, strides, box, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// Launches the TMA-staged eta update when the grid allows it; false otherwise.
+template <bool FAST, int N>
+static bool launch_eta_tma_n(const StepParams& P, const double* eta, const double* p, double* eta_next,
+                             double* gb_next, double* s2_next, Status* st, cudaStream_t stream) {
+    const Grid& g = P.g;
+    CUtensorMap mi, mr, mc;
+    if (!encode_eta_map(&mi, g, N, eta, 32, 8) || !encode_eta_map(&mr, g, N, eta, 32, 1) ||
+        !encode_eta_map(&mc, g, N, eta, 2, 8))
+        return false;
+    const size_t smem = TmaStage<N>::SMEM;
+    ensure_smem_attr((const void*)k_eta_tma<FAST, N>, (int)smem);
+    const dim3 grid(g.nb / 32, g.na / 8, (g.nx + P.xchunk - 1) / P.xchunk);
+    k_eta_tma<FAST, N><<<grid, dim3(32, 8), smem, stream>>>(P, mi, mr, mc, p, eta_next, gb_next, s2_next, st);
+    return true;
+}
+
+template <bool FAST>
+static bool launch_eta_tma(int neta, const StepParams& P, const double* eta, const double* p, double* eta_next,
+                           double* gb_next, double* s2_next, Status* st, cudaStream_t stream) {
+    const Grid& g = P.g;
+    if (g.dim != 3 || g.nb % 32 != 0 || g.na % 8 != 0 || g.nb < 32 || neta < 1 || neta > 16) return false;
+    if ((reinterpret_cast<unsigned long long>(eta) & 15ull) != 0) return false;
+    switch (neta) {
+#define NICR_TMA_CASE(n) \
+    case n: return launch_eta_tma_n<FAST, n>(P, eta, p, eta_next, gb_next, s2_next, st, stream);
+        NICR_TMA_CASE(1) NICR_TMA_CASE(2) NICR_TMA_CASE(3) NICR_TMA_CASE(4) NICR_TMA_CASE(5) NICR_TMA_CASE(6)
+        NICR_TMA_CASE(7) NICR_TMA_CASE(8) NICR_TMA_CASE(9) NICR_TMA_CASE(10) NICR_TMA_CASE(11) NICR_TMA_CASE(12)
+        NICR_TMA_CASE(13) NICR_TMA_CASE(14) NICR_TMA_CASE(15) NICR_TMA_CASE(16)
+#undef NICR_TMA_CASE
+        default: return false;
+    }
+}
+
 // Streaming form of the eta update: each CTA owns a rows x columns tile,
 // marches along X and stages every eta plane once (radius-1 halo) in a
 // three-plane shared-memory ring, so every field is read from HBM about once.
@@ -794,17 +1053,6 @@ __global__ void __launch_bounds__(TA * TB, MINB) k_step_batch(const __grid_const
 
 }  // namespace
 
-// Dynamic shared memory above 48 KB is opted into per kernel and per device,
-// once (setting it again is harmless, skipping it on a second device is not).
-static void ensure_smem_attr(const void* kernel, int bytes) {
-    static std::mutex mu;
-    static std::set<std::pair<const void*, int>> done;
-    int dev = 0;
-    cudaGetDevice(&dev);
-    std::lock_guard<std::mutex> lock(mu);
-    if (done.insert({kernel, dev}).second)
-        cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-}
 // X chunk of the step and eta kernels. A CTA marching c planes also computes
 // mu and M of the plane before its chunk and stages that plane's halo, about
 // two planes of extra work, and CTAs run in waves of 2 (3D) or 4 (2D) per SM,
@@ -864,12 +1112,14 @@ static void launch_eta_form(const StepParams& P, int neta, const double* eta, co
     // per-cell kernel for the drop-in form, where the unrolled verified
     // divisions of the marching kernel cost more than its saved loads (1.84 ms
     // vs 1.29 ms). NICR_ETA_KERNEL=march|simple|stream overrides for tuning.
-    static int simple = -1, march = -1;
+    static int simple = -1, march = -1, tma = -1;
     if (simple < 0) {
         const char* e = getenv("NICR_ETA_KERNEL");
         simple = (e && e[0] == 's' && e[1] == 't') ? 0 : 1;
         march = e ? (e[0] == 'm' ? 1 : 0) : -2;
+        tma = (e && e[0] == 't') ? 1 : 0;
     }
+    if (tma && launch_eta_tma<FAST>(neta, P, eta, p, eta_next, gb_next, s2_next, st, stream)) return;
     if (march == 1 || (march == -2 && FAST)) {
         const bool done = g.dim == 3 ? eta_march_dispatch<3, FAST>(neta, P, eta, p, eta_next, gb_next, s2_next, st, stream)
                                      : eta_march_dispatch<2, FAST>(neta, P, eta, p, eta_next, gb_next, s2_next, st, stream);

@@ -125,3 +125,4 @@ def test_batch_graph_pairs_match_plain_launches(require_gpu, tmp_path):
         assert np.array_equal(a[k].view(np.int64), b[k].view(np.int64)), k
     assert ja["res"] == jb["res"] and ja["budgets"] == jb["budgets"] and ja["launches"] == jb["launches"]
     assert ja["nuclei"] > 0
+
