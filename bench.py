@@ -302,7 +302,8 @@ def small_workload(args) -> int:
     4 (Cr 0.20 +- 0.005 from seed 0 outside the seed), 3D 64^3 static grains,
     3D 128^3 with 32 static grains from seed 1 and Ksp. nicr_run batches of
     N steps (step pairs replayed as CUDA graphs), wall clock around the batch
-    after a synchronize on both sides."""
+    after a synchronize on both sides; once with the X chunk of the cost
+    model, once after nicr_tune."""
     import torch
     import nicr
     cases = {
@@ -323,12 +324,18 @@ def small_workload(args) -> int:
             s.set("cr", cr)
             s.reset_inventory()
         s.run(50)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        s.run(n)
-        torch.cuda.synchronize()
-        t = time.perf_counter() - t0
-        out[name] = {"cells": s.n, "steps": n, "steps_per_s": n / t, "value": s.n * n / t / 1e6}
+        r = {"cells": s.n, "steps": n}
+        for label in ("model", "tuned"):
+            if label == "tuned":
+                r["tuned_xchunk"], r["tuned_minb"] = s.tune(3)
+                s.run(10)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            s.run(n)
+            torch.cuda.synchronize()
+            t = time.perf_counter() - t0
+            r[label] = {"steps_per_s": n / t, "value": s.n * n / t / 1e6}
+        out[name] = r
         s.close()
     print(json.dumps(out))
     return 0

@@ -241,6 +241,19 @@ int nicr_step_noalloc(const nicr_config* cfg, const double* o, const double* cr,
                       const double* gb, const double* eta_s2, double* o_next, double* cr_next,
                       double* p_next, nicr_step_result* result, void* stream);
 
+/* Autotuning (no counterpart in the reference). nicr_tune times `reps`
+ * passes of the step kernels (and the eta update) on the handle's current
+ * state for every X chunk the chooser considers (planes per CTA) and, in 3D,
+ * both occupancy variants of the step kernel, writing only trial buffers, and
+ * keeps the fastest; the state, budget and step count are unchanged. Fields
+ * of later steps are the same bit for bit whatever is chosen; budget sums,
+ * reduced per CTA, may differ in the last digits (~1e-16 relative).
+ * nicr_batch_tune chooses the batch's common X chunk the same way. The choice
+ * is returned in *xchunk / *minb when not NULL. */
+typedef struct nicr_batch nicr_batch;
+int nicr_tune(nicr_handle* h, int reps, int* xchunk, int* minb);
+int nicr_batch_tune(nicr_batch* b, int reps, int* xchunk);
+
 /* Checkpoint / restart (no counterpart in the reference, which cannot resume
  * a run). nicr_save_state writes the handle's state to `path`: a header (the
  * configuration, accepted steps, nucleation clock, budget, Voronoi seeds),
@@ -281,7 +294,6 @@ int nicr_load_state(nicr_handle* h, const char* path);
  * nicr_run leaves a handle, while the others complete; the return value is
  * the status of the first failing domain (NICR_OK when none failed) and
  * nicr_batch_last_error names it ("domain i: <message>"). */
-typedef struct nicr_batch nicr_batch;
 int nicr_batch_create(const nicr_config* cfgs, int n, nicr_batch** out);
 void nicr_batch_destroy(nicr_batch* b);
 int nicr_batch_size(const nicr_batch* b);

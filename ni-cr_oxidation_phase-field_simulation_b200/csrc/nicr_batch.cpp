@@ -32,7 +32,6 @@ struct nicr_batch {
         if (stream) cudaStreamDestroy(stream);
     }
 
-    // Advances every domain nsteps steps (run() schedule when `schedule`).
     // Step pairs of the whole batch captured as CUDA graphs, one per parity
     // state of all domains (they toggle together; a domain that was rolled
     // back after a failed trial may differ), replayed when no domain scans
@@ -106,6 +105,51 @@ struct nicr_batch {
         nicr::check_cuda(cudaGraphLaunch(pg->exec, stream), "cudaGraphLaunch");
         launches += pg->batch_kernels;
         for (int i = 0; i < n; ++i) doms[i]->m->launches += pg->domain_kernels[i];
+    }
+
+    // The batch's common X chunk by measurement: `reps` timed passes of the
+    // grouped step launches and the domains' eta updates per candidate, on
+    // the current states, into the trial buffers only.
+    int tune(int reps, int* chunk_out) {
+        const int n = (int)doms.size();
+        reps = std::max(1, reps);
+        int nxmax = 1;
+        for (auto* h : doms) {
+            h->m->prepare_step();
+            nxmax = std::max(nxmax, h->m->g.nx);
+        }
+        std::vector<nicr::BatchDomain> descs((size_t)n);
+        cudaEvent_t e0, e1;
+        nicr::check_cuda(cudaEventCreate(&e0), "cudaEventCreate");
+        nicr::check_cuda(cudaEventCreate(&e1), "cudaEventCreate");
+        auto pass = [&] {
+            for (int i = 0; i < n; ++i) descs[i] = doms[i]->m->step_desc();
+            nicr::launch_step_batch(descs.data(), n, stream);
+            for (auto* h : doms)
+                if (h->m->advance_eta) h->m->launch_trial_eta();   // the step kernel ran batched above
+        };
+        int best = doms[0]->m->params().xchunk;
+        float best_ms = -1.f;
+        for (int c : nicr::xchunk_candidates(nxmax)) {
+            for (auto* h : doms) h->m->set_xchunk(c);
+            pass();
+            nicr::check_cuda(cudaEventRecord(e0, stream), "cudaEventRecord");
+            for (int r = 0; r < reps; ++r) pass();
+            nicr::check_cuda(cudaEventRecord(e1, stream), "cudaEventRecord");
+            nicr::check_cuda(cudaEventSynchronize(e1), "cudaEventSynchronize");
+            float ms = 0.f;
+            nicr::check_cuda(cudaEventElapsedTime(&ms, e0, e1), "cudaEventElapsedTime");
+            if (best_ms < 0.f || ms < best_ms) { best_ms = ms; best = c; }
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        nicr::check_cuda(cudaGetLastError(), "tune");
+        for (auto* h : doms) h->m->set_xchunk(best);
+        for (auto& q : graphs)
+            if (q.exec) cudaGraphExecDestroy(q.exec);
+        graphs.clear();
+        if (chunk_out) *chunk_out = best;
+        return NICR_OK;
     }
 
     // Advances every domain nsteps steps (run() schedule when `schedule`).
@@ -238,6 +282,10 @@ nicr_handle* nicr_batch_domain(nicr_batch* b, int i) {
 
 int nicr_batch_step(nicr_batch* b, int nsteps, int* completed) {
     return batch_guarded(b, [&](nicr_batch& bb) { return bb.advance(nsteps, completed, false); });
+}
+
+int nicr_batch_tune(nicr_batch* b, int reps, int* xchunk) {
+    return batch_guarded(b, [&](nicr_batch& bb) { return bb.tune(reps, xchunk); });
 }
 
 int nicr_batch_run(nicr_batch* b, int nsteps, int* completed) {

@@ -122,6 +122,13 @@ int nicr_load_state(nicr_handle* h, const char* path) {
     });
 }
 
+int nicr_tune(nicr_handle* h, int reps, int* xchunk, int* minb) {
+    return guarded(h, [&](nicr::Model& m) {
+        m.tune(reps, xchunk, minb);
+        return (int)NICR_OK;
+    });
+}
+
 int nicr_refresh(nicr_handle* h) {
     return guarded(h, [&](nicr::Model& m) { m.refresh(); m.sync(); return (int)NICR_OK; });
 }

@@ -5,6 +5,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include <vector>
+
 #include "nicr_physics.h"
 
 namespace nicr {
@@ -68,6 +70,7 @@ struct StepParams {
     int inlet;                   // bc == concentration && oxygen_diffusion
     int xchunk;                  // planes per CTA along X
     int fast;                    // arithmetic form: 0 drop-in (bit-identical), 1 reciprocal divisions
+    int minb;                    // 3D step kernel: CTAs/SM variant 2 or 3 (0: the default)
 };
 
 // ---- step --------------------------------------------------------------------
@@ -80,6 +83,9 @@ int step_main_blocks(const StepParams& P);
 // the n domains of a batch. NICR_XCHUNK forces a chunk for tuning runs.
 int choose_xchunk(const Grid& g);
 int choose_xchunk_batch(const Grid* grids, int n);
+// The chunks the choosers consider for a largest X extent nxmax: nxmax halved
+// repeatedly and the powers of two below it, longest first.
+std::vector<int> xchunk_candidates(int nxmax);
 // Per-device kernel attributes of the step kernel P selects, set outside any
 // stream capture (launch_step_main sets them on first use otherwise).
 void step_kernels_prepare(const StepParams& P);

@@ -628,6 +628,55 @@ void Model::set_xchunk(int c) {
         if (q.exec) { cudaGraphExecDestroy(q.exec); q.exec = nullptr; }
 }
 
+void Model::launch_trial_eta() {
+    if (advance_eta)
+        launch_eta_update(sp, neta, eta_[ecur], s2_[gcur], p_[cur], eta_[ecur ^ 1], gb_[gcur ^ 1], s2_[gcur ^ 1], st,
+                          stream);
+}
+
+void Model::launch_trial_kernels() {
+    const BatchDomain d = step_desc();
+    int nb = 0;
+    launch_step_main(sp, d.o, d.cr, d.p, d.gb, d.s2, d.on, d.crn, d.pn, partials, st, stream, &nb);
+    launch_trial_eta();
+}
+
+void Model::tune(int reps, int* xchunk, int* minb) {
+    reps = std::max(1, reps);
+    prepare_step();
+    reset_status();   // trial kernels of a failing state must not stop the timing runs
+    cudaEvent_t e0, e1;
+    check_cuda(cudaEventCreate(&e0), "cudaEventCreate");
+    check_cuda(cudaEventCreate(&e1), "cudaEventCreate");
+    int best_c = sp.xchunk, best_m = sp.minb;
+    float best_ms = -1.f;
+    const std::vector<int> minbs = dim == 3 ? std::vector<int>{2, 3} : std::vector<int>{0};
+    for (int c : xchunk_candidates(g.nx)) {
+        set_xchunk(c);
+        for (int mb : minbs) {
+            sp.minb = mb;
+            step_kernels_prepare(sp);
+            launch_trial_kernels();   // warm-up
+            check_cuda(cudaEventRecord(e0, stream), "cudaEventRecord");
+            for (int r = 0; r < reps; ++r) launch_trial_kernels();
+            check_cuda(cudaEventRecord(e1, stream), "cudaEventRecord");
+            check_cuda(cudaEventSynchronize(e1), "cudaEventSynchronize");
+            float ms = 0.f;
+            check_cuda(cudaEventElapsedTime(&ms, e0, e1), "cudaEventElapsedTime");
+            if (best_ms < 0.f || ms < best_ms) { best_ms = ms; best_c = c; best_m = mb; }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    check_cuda(cudaGetLastError(), "tune");
+    set_xchunk(best_c);   // also drops captured step graphs
+    sp.minb = best_m;
+    reset_status();
+    sync();
+    if (xchunk) *xchunk = best_c;
+    if (minb) *minb = best_m;
+}
+
 void Model::prepare_step() {
     if (has_eta && eta_dirty) eta_mask_now();
 }

@@ -101,6 +101,14 @@ public:
     // Planes per CTA of this domain's step and eta kernels (a batch sets one
     // chunk for all its domains). Grows the partial-sum buffer when needed.
     void set_xchunk(int c);
+    // Times `reps` launches of this domain's step (and eta update) kernels for
+    // each X chunk candidate and, in 3D, each occupancy variant, on the current
+    // state without committing anything, and keeps the fastest pair.
+    void tune(int reps, int* xchunk, int* minb);
+    // One pass of the step kernels into the trial buffers (no commit), and of
+    // the eta update alone.
+    void launch_trial_kernels();
+    void launch_trial_eta();
     void prepare_step();
     BatchDomain step_desc() const;
     FinalizeDomain finalize_desc(int nblocks) const;

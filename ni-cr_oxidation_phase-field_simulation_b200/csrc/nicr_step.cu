@@ -179,6 +179,18 @@ int choose_xchunk(const Grid& g) {
 
 // One chunk for all domains of a batch: the same cost with the CTAs of every
 // domain sharing the waves (chunks above a domain's nx clamp to it).
+std::vector<int> xchunk_candidates(int nxmax) {
+    std::vector<int> cand;
+    for (int c = nxmax;; c = (c + 1) / 2) {
+        cand.push_back(c);
+        if (c == 1) break;
+    }
+    for (int c = 1; c < nxmax; c *= 2) cand.push_back(c);
+    std::sort(cand.begin(), cand.end(), [](int a, int b) { return a > b; });
+    cand.erase(std::unique(cand.begin(), cand.end()), cand.end());
+    return cand;
+}
+
 int choose_xchunk_batch(const Grid* grids, int n) {
     int nxmax = 1;
     bool any3 = false;
@@ -188,14 +200,7 @@ int choose_xchunk_batch(const Grid* grids, int n) {
     }
     if (forced_xchunk() > 0) return std::min(forced_xchunk(), nxmax);
     const long long slots = 148LL * (any3 ? 2 : 4);
-    // candidates: nx halved repeatedly, and the powers of two below it
-    std::vector<int> cand;
-    for (int c = nxmax;; c = (c + 1) / 2) {
-        cand.push_back(c);
-        if (c == 1) break;
-    }
-    for (int c = 1; c < nxmax; c *= 2) cand.push_back(c);
-    std::sort(cand.begin(), cand.end(), [](int a, int b) { return a > b; });
+    const std::vector<int> cand = xchunk_candidates(nxmax);
     int best = nxmax;
     long long best_cost = -1;
     for (int c : cand) {
@@ -219,7 +224,7 @@ void step_kernels_prepare(const StepParams& P) {
     }
     if (P.g.dim != 3) return;   // the 2D tile fits the default 48 KB
     using T = Tile<3, TA3, TB3>;
-    const bool m3 = step_minb() == 3;
+    const bool m3 = step_minb_for(P) == 3;
     const void* k = m3 ? (const void*)k_step_main<3, TA3, TB3, 3, false> : (const void*)k_step_main<3, TA3, TB3, 2, false>;
     ensure_smem_attr(k, (int)T::SMEM_BYTES);
 }

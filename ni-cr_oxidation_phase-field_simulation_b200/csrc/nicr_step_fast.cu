@@ -29,7 +29,7 @@ void launch_batch_group_fast(StepBatch& B, int nblocks, int dim, cudaStream_t st
 void step_kernels_prepare_fast(const StepParams& P) {
     if (P.g.dim != 3) return;   // the 2D tile fits the default 48 KB
     using T = Tile<3, TA3, TB3>;
-    const void* k = step_minb() == 3 ? (const void*)k_step_main<3, TA3, TB3, 3, true>
+    const void* k = step_minb_for(P) == 3 ? (const void*)k_step_main<3, TA3, TB3, 3, true>
                                      : (const void*)k_step_main<3, TA3, TB3, 2, true>;
     ensure_smem_attr(k, (int)T::SMEM_BYTES);
 }

@@ -1072,6 +1072,7 @@ static int step_minb() {
     }
     return v;
 }
+static int step_minb_for(const StepParams& P) { return P.minb == 2 || P.minb == 3 ? P.minb : step_minb(); }
 
 template <int MINB, bool FAST>
 static void launch_step3(const StepParams& P, const double* o, const double* cr, const double* p, const double* gb,
@@ -1090,7 +1091,7 @@ static void launch_step_form(const StepParams& P, const double* o, const double*
                              const double* gb, const double* s2, double* on, double* crn, double* pn,
                              StepPartial* partials, Status* st, cudaStream_t stream, int* nblocks_out) {
     if (P.g.dim == 3) {
-        if (step_minb() == 3) launch_step3<3, FAST>(P, o, cr, p, gb, s2, on, crn, pn, partials, st, stream, nblocks_out);
+        if (step_minb_for(P) == 3) launch_step3<3, FAST>(P, o, cr, p, gb, s2, on, crn, pn, partials, st, stream, nblocks_out);
         else launch_step3<2, FAST>(P, o, cr, p, gb, s2, on, crn, pn, partials, st, stream, nblocks_out);
     } else {
         using T = Tile<2, TA2, TB2>;

@@ -103,6 +103,8 @@ def lib():
     L.nicr_main.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_char_p)]
     L.nicr_stream.argtypes = [H]
     L.nicr_stream.restype = ctypes.c_void_p
+    L.nicr_tune.argtypes = [H, ctypes.c_int, ip, ip]
+    L.nicr_batch_tune.argtypes = [H, ctypes.c_int, ip]
     L.nicr_save_state.argtypes = [H, ctypes.c_char_p]
     L.nicr_load_state.argtypes = [H, ctypes.c_char_p]
     L.nicr_batch_create.argtypes = [ctypes.POINTER(NicrConfig), ctypes.c_int, ctypes.POINTER(H)]
@@ -313,6 +315,13 @@ class Solver:
         out["amount"] = amount[: 2 * self.n_eta].reshape(-1, 2)
         return out
 
+    def tune(self, reps: int = 3):
+        """Measures and keeps the fastest X chunk / occupancy variant (nicr_tune);
+        returns (xchunk, minb). The state is unchanged."""
+        c, m = ctypes.c_int(0), ctypes.c_int(0)
+        self._check(lib().nicr_tune(self.h, reps, ctypes.byref(c), ctypes.byref(m)))
+        return c.value, m.value
+
     def save(self, path):
         """Checkpoint of the current state (nicr_save_state)."""
         self._check(lib().nicr_save_state(self.h, str(path).encode()))
@@ -408,6 +417,14 @@ class Batch:
     def run(self, n: int, check: bool = True):
         """n steps of every domain on its run() schedule (Ksp scans)."""
         return self._advance(lib().nicr_batch_run, n, check)
+
+    def tune(self, reps: int = 3) -> int:
+        """Measures and keeps the fastest common X chunk (nicr_batch_tune)."""
+        c = ctypes.c_int(0)
+        rc = lib().nicr_batch_tune(self.b, reps, ctypes.byref(c))
+        if rc != 0:
+            raise NicrError(rc, self.last_error)
+        return c.value
 
     @property
     def kernel_launches(self) -> int:
