@@ -100,10 +100,10 @@ enum {
     NICR_FIELD_CR = 1,       /* Model::cr             */
     NICR_FIELD_PHI = 2,      /* Model::p              */
     NICR_FIELD_ETA = 3,      /* Model::eta[index]     */
-    NICR_FIELD_MU_O = 4,     /* Model::muO  (after nicr_refresh)            */
-    NICR_FIELD_MU_CR = 5,    /* Model::muCr (after nicr_refresh)            */
-    NICR_FIELD_M_O = 6,      /* Model::mo   (after nicr_refresh)            */
-    NICR_FIELD_M_CR = 7,     /* Model::mc   (after nicr_refresh)            */
+    NICR_FIELD_MU_O = 4,     /* Model::muO  (refreshed when read)           */
+    NICR_FIELD_MU_CR = 5,    /* Model::muCr (refreshed when read)           */
+    NICR_FIELD_M_O = 6,      /* Model::mo   (refreshed when read)           */
+    NICR_FIELD_M_CR = 7,     /* Model::mc   (refreshed when read)           */
     NICR_FIELD_GB = 8,       /* Model::gb  (Voronoi mask or eta-derived)    */
     NICR_FIELD_GRAIN = 9,    /* Model::grain (initial Voronoi id, 1-based)  */
     NICR_FIELD_ETA_S2 = 10,  /* Model::eta_s2                               */
@@ -137,9 +137,11 @@ int nicr_get_info(const nicr_handle* h, nicr_info* info);
 int nicr_get_seeds(const nicr_handle* h, double* xyz, long long* volumes);
 
 /* Copies one field between host memory and the device (interior cells only,
- * reference order). Setting O/CR/PHI/ETA also invalidates the frozen-eta cache
- * and refreshes, as the reference drivers do after editing fields
- * (3S:1092-1101 fill_smooth; 3S:347-349 invalidate_eta_cache). */
+ * reference order). Setting O/CR/PHI/ETA also invalidates the frozen-eta
+ * cache, as the reference drivers do after editing fields (3S:1092-1101
+ * fill_smooth; 3S:347-349 invalidate_eta_cache); the eta mask and mu/M are
+ * recomputed when next needed (the next step, or reading GB, ETA_S2, MU_*,
+ * M_*). Host buffers in pinned memory transfer at full PCIe speed. */
 int nicr_set_field(nicr_handle* h, int field, int index, const double* host);
 int nicr_get_field(nicr_handle* h, int field, int index, double* host);
 
@@ -154,7 +156,9 @@ int nicr_reset_inventory(nicr_handle* h);
 
 /* Model::step x nsteps (3S:761-826, 2D:551-597). Stops at the first rejected
  * trial: *completed = accepted steps; the state is the last accepted one, the
- * budget is restored (3S:812-820) and the status names the failure. */
+ * budget is restored (3S:812-820) and the status names the failure. Pairs of
+ * steps are replayed as captured CUDA graphs (results identical to launching
+ * each kernel; NICR_GRAPHS=0 in the environment launches them one by one). */
 int nicr_step(nicr_handle* h, int nsteps, int* completed);
 /* nsteps of run()'s loop (3S:1368-1385, 2D:1219-1236): before each step, Ksp
  * nucleation when its physical time is due, then Model::step. The schedule
