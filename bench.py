@@ -350,7 +350,8 @@ def main():
     ap.add_argument("--impl", choices=["nicr", "reference"], default="nicr")
     ap.add_argument("--size", type=int, default=256)
     ap.add_argument("--neta", type=int, default=8)
-    ap.add_argument("--e2e-steps", type=int, default=50)
+    ap.add_argument("--e2e-steps", type=int, default=0,
+                    help="steps of the end-to-end leg (default: --steps, the device-timed workload)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-budget", type=float, default=60.0, help="seconds of CPU stepping for the reference")
     ap.add_argument("--workload", choices=["step", "output", "sweep", "small"], default="step",
@@ -358,6 +359,8 @@ def main():
                          "sweep: 64 uneven domains advanced as one batch; small: step rate of the small configs")
     ap.add_argument("--precision", type=int, default=0, help="arithmetic form of --workload sweep (0 drop-in, 1 fast)")
     args = ap.parse_args()
+    if args.e2e_steps <= 0:
+        args.e2e_steps = args.steps
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
