@@ -341,6 +341,51 @@ def small_workload(args) -> int:
     return 0
 
 
+def accuracy_workload(args) -> int:
+    """The reciprocal form against the drop-in form on the bench workload over a
+    long run (the run() schedule, Ksp scans included): per-field relative L-inf
+    and L2 deviation and the oxide-front position difference every 1000 steps.
+    --steps sets the length (5000 when left at the step workload's default)."""
+    import nicr
+    steps = 5000 if args.steps == 400 else args.steps
+    sols = []
+    for precision in (0, 1):
+        cfg = workload_config(args.size, args.neta, seed=2)
+        cfg.precision = precision
+        s = nicr.Solver(cfg)
+        cr = 0.25 + np.random.default_rng(2).uniform(-0.01, 0.01, size=s.shape)
+        cr[0] = s.get("cr")[0]
+        s.set("cr", cr)
+        s.reset_inventory()
+        sols.append(s)
+
+    def depth(ph):
+        ox = ph >= 0.5
+        return np.where(ox.all(axis=0), ph.shape[0], np.argmin(ox, axis=0))
+
+    rows = []
+    done = 0
+    while done < steps:
+        n = min(1000, steps - done)
+        for s in sols:
+            s.run(n)
+        done += n
+        row = {"step": done}
+        for f in ["o", "cr", "p"] + [f"eta{g + 1}" for g in range(args.neta)]:
+            b, a = sols[0].get(f), sols[1].get(f)
+            row[f] = {"linf_rel": float(np.max(np.abs(a - b)) / max(float(np.max(np.abs(b))), 1e-300)),
+                      "l2_rel": float(np.sqrt(np.mean((a - b) ** 2)) / max(float(np.sqrt(np.mean(b ** 2))), 1e-300))}
+        row["oxide_front_max_cells"] = int(np.max(np.abs(depth(sols[0].get("p")) - depth(sols[1].get("p")))))
+        row["nuclei"] = [s.budget()["nuclei"] for s in sols]
+        rows.append(row)
+    worst = max(max(v["linf_rel"] for k, v in r.items() if isinstance(v, dict)) for r in rows)
+    print(json.dumps({"workload": "accuracy", "config": f"3D {args.size}^3, {args.neta} evolving eta (bench workload)",
+                      "steps": steps, "linf_rel_max": worst, "bound": 1e-4, "checkpoints": rows}))
+    for s in sols:
+        s.close()
+    return 0
+
+
 # ------------------------------------------------------------------ GPU arm
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
@@ -354,9 +399,10 @@ def main():
                     help="steps of the end-to-end leg (default: --steps, the device-timed workload)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-budget", type=float, default=60.0, help="seconds of CPU stepping for the reference")
-    ap.add_argument("--workload", choices=["step", "output", "sweep", "small"], default="step",
+    ap.add_argument("--workload", choices=["step", "output", "sweep", "small", "accuracy"], default="step",
                     help="step: the headline line (default); output: VTI frame cost and overlap with stepping; "
-                         "sweep: 64 uneven domains advanced as one batch; small: step rate of the small configs")
+                         "sweep: 64 uneven domains advanced as one batch; small: step rate of the small configs; "
+                         "accuracy: the fast form against the drop-in form over --steps (5000 by default here)")
     ap.add_argument("--precision", type=int, default=0, help="arithmetic form of --workload sweep (0 drop-in, 1 fast)")
     args = ap.parse_args()
     if args.e2e_steps <= 0:
@@ -374,6 +420,8 @@ def main():
         return sweep_workload(args, rank, world, local)
     if args.workload == "small":
         return small_workload(args)
+    if args.workload == "accuracy":
+        return accuracy_workload(args)
 
     import torch
     import torch.distributed as dist
