@@ -341,6 +341,59 @@ def small_workload(args) -> int:
     return 0
 
 
+def slabs_workload(args) -> int:
+    """The slab form (one domain split along X, nicr_slabs_*) on the bench
+    workload: 256^3, 8 evolving eta, reciprocal form, Ksp on, the same initial
+    state. First one handle, then the domain in 2 and 4 slabs on this GPU
+    (--slab-devices lists one device per slab to spread them over GPUs),
+    each advanced by nicr_run for --steps steps after --warmup, wall clock
+    with a device synchronize on both sides. On one GPU the ratio is the cost
+    of the split (halo copies, the cross-slab commit, one stream per slab);
+    halo_bytes_per_step counts what crosses the seams each step."""
+    import torch
+    import nicr
+    cfg = workload_config(args.size, args.neta, seed=2)
+    cfg.precision = 1
+
+    def prepare(obj):
+        cr = 0.25 + np.random.default_rng(2).uniform(-0.01, 0.01, size=obj.shape)
+        cr[0] = obj.get("cr")[0]
+        obj.set("cr", cr)
+        obj.reset_inventory()
+
+    def timed(obj):
+        obj.run(args.warmup)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        obj.run(args.steps)
+        torch.cuda.synchronize()
+        return time.perf_counter() - t0
+
+    cells = args.size ** 3
+    solo = nicr.Solver(cfg)
+    prepare(solo)
+    t1 = timed(solo)
+    solo.close()
+    out = {"workload": "slabs", "config": f"3D {args.size}^3, {args.neta} evolving eta, fp64-fast, Ksp",
+           "unit": "Mcell-updates/s", "steps": args.steps,
+           "single_handle": {"value": cells * args.steps / t1 / 1e6, "ms_per_step": 1e3 * t1 / args.steps}}
+    devices = [int(d) for d in args.slab_devices.split(",")] if args.slab_devices else None
+    counts = [len(devices)] if devices else [2, 4]
+    plane_bytes = args.size * ((args.size + 7) // 8 * 8) * 8
+    for k in counts:
+        s = nicr.Slabs(cfg, k, devices or [0] * k)
+        prepare(s)
+        tk = timed(s)
+        seams = k - 1
+        out[f"{k}_slabs"] = {"value": cells * args.steps / tk / 1e6, "ms_per_step": 1e3 * tk / args.steps,
+                             "vs_single_handle": t1 / tk, "devices": devices or [0] * k,
+                             "halo": s.slab(0)["halo"],
+                             "halo_bytes_per_step": seams * 2 * (2 + 2 + 1 + 1 + args.neta) * plane_bytes}
+        s.close()
+    print(json.dumps(out))
+    return 0
+
+
 def accuracy_workload(args) -> int:
     """The reciprocal form against the drop-in form on the bench workload over a
     long run (the run() schedule, Ksp scans included): per-field relative L-inf
@@ -399,10 +452,12 @@ def main():
                     help="steps of the end-to-end leg (default: --steps, the device-timed workload)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-budget", type=float, default=60.0, help="seconds of CPU stepping for the reference")
-    ap.add_argument("--workload", choices=["step", "output", "sweep", "small", "accuracy"], default="step",
+    ap.add_argument("--slab-devices", default="", help="--workload slabs: comma-separated device per slab")
+    ap.add_argument("--workload", choices=["step", "output", "sweep", "small", "accuracy", "slabs"], default="step",
                     help="step: the headline line (default); output: VTI frame cost and overlap with stepping; "
                          "sweep: 64 uneven domains advanced as one batch; small: step rate of the small configs; "
-                         "accuracy: the fast form against the drop-in form over --steps (5000 by default here)")
+                         "accuracy: the fast form against the drop-in form over --steps (5000 by default here); "
+                         "slabs: the domain split along X into slabs against one handle")
     ap.add_argument("--precision", type=int, default=0, help="arithmetic form of --workload sweep (0 drop-in, 1 fast)")
     args = ap.parse_args()
     if args.e2e_steps <= 0:
@@ -422,6 +477,8 @@ def main():
         return small_workload(args)
     if args.workload == "accuracy":
         return accuracy_workload(args)
+    if args.workload == "slabs":
+        return slabs_workload(args)
 
     import torch
     import torch.distributed as dist

@@ -308,6 +308,46 @@ const char* nicr_batch_last_error(const nicr_batch* b);
 long long nicr_batch_kernel_launches(const nicr_batch* b);
 void* nicr_batch_stream(const nicr_batch* b);
 
+/* Slab form: one 3D domain split along X into nslabs slabs of near-equal
+ * plane counts, slab i on GPU devices[i] (devices may repeat; NULL puts every
+ * slab on cfg->device). This is mpi3d-slab's own decomposition (each MPI rank
+ * owns a range of X planes and trades ghost planes with its neighbours,
+ * 3S:146-191, MPI_Allreduce of the budget, root-gathered Ksp scan 3S:666-686),
+ * with GPUs in place of ranks: each slab stores its planes plus `halo` planes
+ * of each neighbour (2, or ceil(radius + gap) with Ksp nucleation), refreshed
+ * after every step by a copy kernel that stores into the neighbour's memory
+ * (P2P over NVLink between GPUs); the slabs agree on each step's acceptance
+ * on the device, and Ksp scans resolve slab after slab in X order. Fields
+ * are bit-identical to a single handle's on the same configuration in the
+ * drop-in form (in the reciprocal form, where the slab kernels are compiled
+ * with FMA contraction apart from the whole-domain ones, to rounding: 1e-13
+ * relative); budget sums (per-slab double-double sums added) agree to ~1e-16
+ * relative. Every
+ * slab needs at least `halo` planes; peer access must be possible between all
+ * devices used. nicr_slabs_step / _run follow nicr_step / nicr_run
+ * (failures: all slabs stop at the last accepted state, the message names the
+ * failing cell as nicr_last_error would). Fields are exchanged whole-domain
+ * (X slowest, like nicr_get_field). No 2D form. */
+typedef struct nicr_slabs nicr_slabs;
+int nicr_slabs_create(const nicr_config* cfg, int nslabs, const int* devices, nicr_slabs** out);
+void nicr_slabs_destroy(nicr_slabs* s);
+int nicr_slabs_count(const nicr_slabs* s);
+/* domain planes [*x0, *x1) of slab i, its device and the halo width */
+int nicr_slabs_info(const nicr_slabs* s, int i, int* x0, int* x1, int* device, int* halo);
+int nicr_slabs_step(nicr_slabs* s, int nsteps, int* completed);
+int nicr_slabs_run(nicr_slabs* s, int nsteps, int* completed);
+int nicr_slabs_nucleate(nicr_slabs* s, int* nuclei);
+int nicr_slabs_get_field(nicr_slabs* s, int field, int index, double* host);
+int nicr_slabs_set_field(nicr_slabs* s, int field, int index, const double* host);
+int nicr_slabs_reset_inventory(nicr_slabs* s);
+int nicr_slabs_get_budget(nicr_slabs* s, nicr_budget* b);
+int nicr_slabs_get_diagnostics(nicr_slabs* s, nicr_diagnostics* d);
+long long nicr_slabs_steps_done(const nicr_slabs* s);
+long long nicr_slabs_kernel_launches(const nicr_slabs* s);
+/* stream (a cudaStream_t) slab i enqueues on */
+void* nicr_slabs_stream(const nicr_slabs* s, int i);
+const char* nicr_slabs_last_error(const nicr_slabs* s);
+
 /* The solver program: the reference's run()/main() for dim 2 or 3
  * (2D:1161-1246, 3S:1309-1395), argv as the reference's executable takes it.
  * Returns the process exit code. */

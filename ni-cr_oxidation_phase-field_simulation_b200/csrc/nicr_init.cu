@@ -34,7 +34,7 @@ __global__ void k_init_fields(const InitParams I, double* o, double* cr, double*
         decode(g, c, x, row, col);
         const long long idx = (long long)x * g.plane + (long long)row * g.pb + col;
         double ov = Phys::bulkO, cv = I.bulk_cr;
-        if (I.inlet_layer && x == 0) { ov = I.layer_o; cv = Phys::layerCr; }
+        if (I.inlet_layer && x + I.x_off == 0) { ov = I.layer_o; cv = Phys::layerCr; }
         o[idx] = ov; cr[idx] = cv; p[idx] = 0.;
     }
 }
@@ -66,7 +66,7 @@ __global__ void k_voronoi3(const InitParams I, const double* __restrict__ seeds,
     for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < g.ncells; c += (long long)gridDim.x * blockDim.x) {
         int xi, row, col;
         decode(g, c, xi, row, col);
-        const double x = (xi + 1) - .5, y = (row + 1) - .5, z = (col + 1) - .5;
+        const double x = (xi + I.x_off + 1) - .5, y = (row + 1) - .5, z = (col + 1) - .5;
         int owner = 0;
         double rbest = CUDART_INF, oY = 0., oZ = 0.;
         for (int s = 0; s < I.ng; ++s) {
@@ -81,7 +81,7 @@ __global__ void k_voronoi3(const InitParams I, const double* __restrict__ seeds,
         const long long idx = (long long)xi * g.plane + (long long)row * g.pb + col;
         grain[idx] = owner + 1;
         dbout[idx] = db;
-        atomicAdd(volumes + owner, 1);
+        if (xi >= I.x_lo && xi < I.x_hi) atomicAdd(volumes + owner, 1);
     }
 }
 
@@ -97,7 +97,7 @@ __global__ void k_eta_dist3(const InitParams I, const double* __restrict__ seeds
         decode(g, c, xi, row, col);
         const long long idx = (long long)xi * g.plane + (long long)row * g.pb + col;
         const int owner = (int)grain[idx] - 1;
-        const double x = (xi + 1) - .5, y = (row + 1) - .5, z = (col + 1) - .5;
+        const double x = (xi + I.x_off + 1) - .5, y = (row + 1) - .5, z = (col + 1) - .5;
         const double oy = y + min_image(ss[3 * owner + 1] - y, I.nyd), oz = z + min_image(ss[3 * owner + 2] - z, I.nzd);
         const double ax = ss[3 * owner] - x, ay = oy - y, az = oz - z;
         const double rbest = ax * ax + ay * ay + az * az;
@@ -138,7 +138,7 @@ __global__ void k_center_seed(const InitParams I, double cx, double cy, double c
         int xi, row, col;
         decode(g, c, xi, row, col);
         // reference indices are 1-based: i = xi+1, (3D) j = row+1, k = col+1; (2D) j = col+1
-        const double ddx = (xi + 1) - cx;
+        const double ddx = (xi + I.x_off + 1) - cx;
         double d2;
         if (g.dim == 3) {
             const double ddy = (row + 1) - cy, ddz = (col + 1) - cz;
@@ -149,11 +149,13 @@ __global__ void k_center_seed(const InitParams I, double cx, double cy, double c
         }
         if (d2 <= r * r) {
             const long long idx = (long long)xi * g.plane + (long long)row * g.pb + col;
-            acc[0] = dd_add(acc[0], Phys::oxideO - o[idx]);
-            acc[1] = dd_add(acc[1], Phys::oxideCr - cr[idx]);
+            if (xi >= I.x_lo && xi < I.x_hi) {   // halo planes of a slab are stamped, not counted
+                acc[0] = dd_add(acc[0], Phys::oxideO - o[idx]);
+                acc[1] = dd_add(acc[1], Phys::oxideCr - cr[idx]);
+                ++cnt;
+            }
             o[idx] = Phys::oxideO; cr[idx] = Phys::oxideCr; p[idx] = 1.;
             for (int q = 0; q < neta; ++q) eta[(long long)q * g.nstore + idx] = 0.;
-            ++cnt;
         }
     }
     block_reduce<2>(acc, cnt);

@@ -35,6 +35,10 @@ struct Status {
     int timeout;                  // a kernel's bounded wait for its own copies ran out
     long long failed_step;        // index (steps_done) of the rejected step
     long long steps_done;         // accepted steps since creation
+    // Slab form: first failing trial of the step that reads buffer parity q,
+    // in slot q (the slabs of a domain agree on a step's outcome by reading
+    // every slab's slot of that step; see launch_step_finalize_slab).
+    unsigned long long slot_err[2];
 };
 constexpr unsigned long long ERR_NONE = ~0ull;
 constexpr unsigned long long ERR_ETA_BASE = 1ull << 62;
@@ -71,7 +75,24 @@ struct StepParams {
     int xchunk;                  // planes per CTA along X
     int fast;                    // arithmetic form: 0 drop-in (bit-identical), 1 reciprocal divisions
     int minb;                    // 3D step kernel: CTAs/SM variant 2 or 3 (0: the default)
+    // Planes updated: [x_lo, x_hi) of the g.nx stored planes. A whole domain
+    // updates all of them; an X slab of a larger domain stores halo planes
+    // below and above its own, which the kernels read but do not write.
+    int x_lo, x_hi;
+    // Failing-trial keys in whole-domain reference order: the cell index is
+    // offset by cell_off and eta keys count key_ncells cells per field.
+    long long cell_off, key_ncells;
+    // Error word of this step: -1 st->err_key, 0/1 st->slot_err[err_slot] (slab form)
+    int err_slot, pad_;
 };
+// The whole-domain values of the range fields (every plane, no offset).
+inline void whole_domain_range(StepParams& sp) {
+    sp.x_lo = 0;
+    sp.x_hi = sp.g.nx;
+    sp.cell_off = 0;
+    sp.key_ncells = sp.g.ncells;
+    sp.err_slot = -1;
+}
 
 // ---- step --------------------------------------------------------------------
 // Main fused step: mu, M, six-face fluxes, phi, Ck, bounds -> trial buffers.
@@ -151,6 +172,32 @@ void launch_vti_arrays(const VtiArgs& a, void* out, bool f64, unsigned* range, c
 // Commit of one step: reduce partials, commit budget unless a trial failed
 void launch_step_finalize(const StepPartial* partials, int nblocks, DevBudget* budget, Status* st,
                           int accept_mode, cudaStream_t stream);
+// Slab form of the commit: the step is rejected when any slab's error word
+// of this step (peers[j]->slot_err[slot], read after every slab's step
+// kernels completed) holds a failing trial; the minimum key is recorded in
+// st->err_key. peers may live on other GPUs (peer access enabled).
+constexpr int kMaxSlabs = 16;
+struct SlabPeers {
+    const Status* st[kMaxSlabs];
+    int n, slot;
+};
+void launch_step_finalize_slab(const StepPartial* partials, int nblocks, DevBudget* budget, Status* st,
+                               const SlabPeers& peers, cudaStream_t stream);
+// Copies up to kCopySegs strided runs of doubles (rows x n, 16-byte aligned
+// addresses and counts of whole double pairs) in one launch; destinations may
+// be another GPU's memory (peer access enabled): the halo exchange of the
+// slab form. Skipped when st->failed is set (st may be null).
+constexpr int kCopySegs = 24;
+struct CopySeg {
+    const double* src;
+    double* dst;
+    long long n, rows, src_pitch, dst_pitch;   // doubles
+};
+struct CopyList {
+    CopySeg s[kCopySegs];
+    int count, pad;
+};
+void launch_copy_segments(const CopyList& L, const Status* st, cudaStream_t stream);
 // Refresh for output: mu_O, mu_Cr, M_O, M_Cr at every cell (3S:597-620)
 void launch_refresh(const StepParams& P, const double* o, const double* cr, const double* p,
                     const double* gb, double* muO, double* muCr, double* mo, double* mc,
@@ -166,6 +213,9 @@ struct InitParams {
     double nxd, nyd, nzd;        // grid extents as doubles (periods)
     double bulk_cr, layer_o;
     int inlet_layer;             // bc == concentration
+    // X slab: stored plane 0 is domain plane x_off; sums and counts cover the
+    // own planes [x_lo, x_hi) only. A whole domain: 0, 0, g.nx.
+    int x_off, x_lo, x_hi;
 };
 void launch_init_fields(const InitParams& I, double* o, double* cr, double* p, cudaStream_t stream);
 // 3D Voronoi labels (first nearest seed under minimum image) and the distance

@@ -41,10 +41,17 @@ __device__ AxisNb periodic_nb(int center, double radius, int n) {
     return a;
 }
 
-__device__ __forceinline__ long long gidx(const Grid& g, int i1, int j1, int k1) {
-    // 1-based reference indices -> device index. 3D: (i,j,k); 2D: (i,j) with j the column.
-    if (g.dim == 3) return (long long)(i1 - 1) * g.plane + (long long)(j1 - 1) * g.pb + (k1 - 1);
-    return (long long)(i1 - 1) * g.plane + (j1 - 1);
+__device__ __forceinline__ long long gidx(const KspDev& K, int i1, int j1, int k1) {
+    // 1-based domain indices -> device index of the stored plane i1-1-x_off.
+    // 3D: (i,j,k); 2D: (i,j) with j the column.
+    const Grid& g = K.g;
+    if (g.dim == 3) return (long long)(i1 - 1 - K.x_off) * g.plane + (long long)(j1 - 1) * g.pb + (k1 - 1);
+    return (long long)(i1 - 1 - K.x_off) * g.plane + (j1 - 1);
+}
+// stored plane of domain index i1, or -1 when this domain/slab does not store it
+__device__ __forceinline__ int stored_plane(const KspDev& K, int i1) {
+    const int li = i1 - 1 - K.x_off;
+    return li >= 0 && li < K.g.nx ? li : -1;
 }
 
 // valid_nucleus on the pre-scan state (3S:687-703, 2D:493-502)
@@ -58,7 +65,7 @@ __device__ bool valid_prescan(const KspDev& K, const double* __restrict__ p, int
         const int i0 = max(1, x - sr), i1 = min(K.nx, x + sr);
         for (int i = i0; i <= i1; ++i)
             for (int j = 1; j <= K.ny; ++j) {
-                if (__ldg(p + gidx(g, i, j, 0)) > .01) {
+                if (__ldg(p + gidx(K, i, j, 0)) > .01) {
                     const int dj = (int)min_image((double)(j - y), (double)K.ny);
                     if (K.hyp2d[abs(i - x) * K.hyp_stride + abs(dj)]) return false;
                 }
@@ -75,7 +82,7 @@ __device__ bool valid_prescan(const KspDev& K, const double* __restrict__ p, int
                 for (int kz = 0; kz < zs.count; ++kz) {
                     const int klo = kz ? zs.lo1 : zs.lo0, khi = kz ? zs.hi1 : zs.hi0;
                     for (int k = klo; k <= khi; ++k) {
-                        if (__ldg(p + gidx(g, i, j, k)) > .01) {
+                        if (__ldg(p + gidx(K, i, j, k)) > .01) {
                             const double di = (double)(i - x), dj = min_image((double)(j - y), (double)K.ny),
                                          dk = min_image((double)(k - z), (double)K.nz);
                             if (sqrt(di * di + dj * dj + dk * dk) < limit) return false;
@@ -98,8 +105,8 @@ __global__ void k_ksp_candidates(const KspDev K, const double* __restrict__ o, c
         const long long idx = (long long)xi * g.plane + (long long)row * g.pb + col;
         unsigned char f = 0;
         const double pv = __ldg(p + idx);
-        if (pv <= .01 && __ldg(o + idx) * __ldg(cr + idx) > K.ksp) {
-            const int x = xi + 1;
+        if (xi >= K.x_lo && xi < K.x_hi && pv <= .01 && __ldg(o + idx) * __ldg(cr + idx) > K.ksp) {
+            const int x = xi + K.x_off + 1;
             if (g.dim == 3) f = valid_prescan(K, p, x, row + 1, col + 1) ? 1 : 0;
             else f = valid_prescan(K, p, x, col + 1, 0) ? 1 : 0;
         }
@@ -154,12 +161,139 @@ __global__ void k_ksp_write(const unsigned char* __restrict__ flag, long long n,
     }
 }
 
+// stamp(x,y,z) (3S:704-724 / 2D:503-516) on the stored cells: ball cells with
+// phi < .01 become oxide. nucO/nucCr collect the increments of the own planes
+// (a slab's halo planes are stamped too but counted by their owner). Returns
+// the number of cells this thread set.
+__device__ int stamp_ball(const KspDev& K, int x, int y, int z, double* o, double* cr, double* p, double* eta,
+                          DD& nucO, DD& nucCr) {
+    const Grid& g = K.g;
+    const int tid = threadIdx.x;
+    int cells = 0;
+    const double r2 = K.radius * K.radius;
+    const long long lo = (long long)K.x_off + 1, hi = (long long)K.x_off + g.nx;   // stored domain planes
+    auto set_cell = [&](long long idx, int i) {
+        const int li = i - 1 - K.x_off;
+        if (li >= K.x_lo && li < K.x_hi) {
+            nucO = dd_add(nucO, Phys::oxideO - o[idx]);
+            nucCr = dd_add(nucCr, Phys::oxideCr - cr[idx]);
+        }
+        o[idx] = Phys::oxideO; cr[idx] = Phys::oxideCr; p[idx] = 1.;
+        for (int e = 0; e < K.neta; ++e) eta[(long long)e * g.nstore + idx] = 0.;
+        ++cells;
+    };
+    if (g.dim == 3) {
+        const int rr = bounded_reach(K.radius, K.nx);
+        const AxisNb ys = periodic_nb(y, K.radius, K.ny), zs = periodic_nb(z, K.radius, K.nz);
+        const int i0 = (int)max(lo, max(1LL, (long long)x - rr)), i1 = (int)min(hi, min((long long)K.nx, (long long)x + rr));
+        if (i1 < i0) return 0;
+        const int ny_n = (ys.hi0 - ys.lo0 + 1) + (ys.count > 1 ? ys.hi1 - ys.lo1 + 1 : 0);
+        const int nz_n = (zs.hi0 - zs.lo0 + 1) + (zs.count > 1 ? zs.hi1 - zs.lo1 + 1 : 0);
+        const long long tot = (long long)(i1 - i0 + 1) * ny_n * nz_n;
+        for (long long q = tid; q < tot; q += blockDim.x) {
+            const int kq = (int)(q % nz_n);
+            const long long t = q / nz_n;
+            const int jq = (int)(t % ny_n);
+            const int i = i0 + (int)(t / ny_n);
+            const int n0y = ys.hi0 - ys.lo0 + 1, n0z = zs.hi0 - zs.lo0 + 1;
+            const int j = jq < n0y ? ys.lo0 + jq : ys.lo1 + (jq - n0y);
+            const int k = kq < n0z ? zs.lo0 + kq : zs.lo1 + (kq - n0z);
+            const double dy = min_image((double)(j - y), (double)K.ny), dz = min_image((double)(k - z), (double)K.nz);
+            const long long idx = gidx(K, i, j, k);
+            if ((double)((i - x) * (i - x)) + dy * dy + dz * dz <= r2 && p[idx] < .01) set_cell(idx, i);
+        }
+    } else {
+        const int rr = (int)ceil(K.radius);
+        const int i0 = (int)max(lo, (long long)max(1, x - rr)), i1 = (int)min(hi, (long long)min(K.nx, x + rr));
+        if (i1 < i0) return 0;
+        const long long tot = (long long)(i1 - i0 + 1) * K.ny;
+        for (long long q = tid; q < tot; q += blockDim.x) {
+            const int j = (int)(q % K.ny) + 1;
+            const int i = i0 + (int)(q / K.ny);
+            const double dy = min_image((double)(j - y), (double)K.ny);
+            const long long idx = gidx(K, i, j, 0);
+            if ((double)((i - x) * (i - x)) + dy * dy <= r2 && p[idx] < .01) set_cell(idx, i);
+        }
+    }
+    return cells;
+}
+
+// Exclusion marks of a stamped nucleus for the later candidates of the scan,
+// on the stored cells. full: the stamp set the whole ball, whose marks are the
+// precomputed shadow (Minkowski sum of the ball and the exclusion ball);
+// otherwise (some ball cell had phi == .01 exactly) every cell of the
+// exclusion box is tested against the ball cells that are oxide now.
+__device__ void mark_excluded(const KspDev& K, int x, int y, int z, bool full, const double* p,
+                              unsigned char* blocked, KspResult* res, bool count_partial) {
+    const Grid& g = K.g;
+    const int tid = threadIdx.x;
+    if (full) {
+        for (int q = tid; q < K.n_shadow; q += blockDim.x) {
+            const int di = K.shadow[3 * q], dj = K.shadow[3 * q + 1], dk = K.shadow[3 * q + 2];
+            const int i = x + di;
+            if (i < 1 || i > K.nx) continue;
+            const int li = stored_plane(K, i);
+            if (li < 0) continue;
+            if (g.dim == 3) {
+                const int j = ((y - 1 + dj) % K.ny + K.ny) % K.ny;
+                const int k = ((z - 1 + dk) % K.nz + K.nz) % K.nz;
+                blocked[((long long)li * K.ny + j) * K.nz + k] = 1;
+            } else {
+                const int j = ((y - 1 + dj) % K.ny + K.ny) % K.ny;
+                blocked[(long long)li * K.ny + j] = 1;
+            }
+        }
+        return;
+    }
+    if (count_partial && tid == 0) res->partial_stamps += 1;
+    const int R = K.box_half;
+    const long long side = 2LL * R + 1;
+    const long long tot = g.dim == 3 ? side * side * side : side * side;
+    for (long long q = tid; q < tot; q += blockDim.x) {
+        int di, dj, dk = 0;
+        if (g.dim == 3) { dk = (int)(q % side) - R; dj = (int)((q / side) % side) - R; di = (int)(q / (side * side)) - R; }
+        else { dj = (int)(q % side) - R; di = (int)(q / side) - R; }
+        const int i = x + di;
+        if (i < 1 || i > K.nx) continue;
+        const int li = stored_plane(K, i);
+        if (li < 0) continue;
+        const int jw = ((y - 1 + dj) % K.ny + K.ny) % K.ny + 1;
+        const int kw = g.dim == 3 ? ((z - 1 + dk) % K.nz + K.nz) % K.nz + 1 : 0;
+        bool hit = false;
+        for (int b = 0; b < K.n_ball && !hit; ++b) {
+            const int si = x + K.ball[3 * b];
+            if (si < 1 || si > K.nx || stored_plane(K, si) < 0) continue;
+            const int sj = ((y - 1 + K.ball[3 * b + 1]) % K.ny + K.ny) % K.ny + 1;
+            const int sk = g.dim == 3 ? ((z - 1 + K.ball[3 * b + 2]) % K.nz + K.nz) % K.nz + 1 : 0;
+            if (p[gidx(K, si, sj, sk)] != 1.) continue;   // not (newly) oxide
+            const int ddi = si - i;
+            const int ddj = (int)min_image((double)(sj - jw), (double)K.ny);
+            if (g.dim == 3) {
+                const int ddk = (int)min_image((double)(sk - kw), (double)K.nz);
+                hit = sqrt((double)ddi * ddi + (double)ddj * ddj + (double)ddk * ddk) < K.radius + K.gap;
+            } else {
+                hit = K.hyp2d[abs(ddi) * K.hyp_stride + abs(ddj)] != 0;
+            }
+        }
+        if (hit) {
+            if (g.dim == 3) blocked[((long long)li * K.ny + (jw - 1)) * K.nz + (kw - 1)] = 1;
+            else blocked[(long long)li * K.ny + (jw - 1)] = 1;
+        }
+    }
+}
+
 // One CTA: ordered greedy resolve + stamps + exclusion marks.
+//   mode 0  scan: the nuclei in pre (accepted earlier in the scan by slabs
+//           before this one along X: stamps and marks), then the own
+//           candidates in order; accepted nuclei go to out (when given)
+//   mode 1  one forced stamp at (fx, fy, fz) (Model::stamp)
+//   mode 2  the stamps of the nuclei in pre only (no marks, no candidates)
 __global__ void __launch_bounds__(1024) k_ksp_resolve(const KspDev K, const long long* __restrict__ list,
-                                                      const int* __restrict__ total, int forced, int fx, int fy,
-                                                      int fz, double* o, double* cr, double* p, double* eta,
-                                                      unsigned char* blocked, DevBudget* budget, KspResult* res,
-                                                      Status* st) {
+                                                      const int* __restrict__ total, int mode, int fx, int fy,
+                                                      int fz, const KspNucleus* __restrict__ pre, int npre,
+                                                      KspNucleus* out, int cap, double* o, double* cr, double* p,
+                                                      double* eta, unsigned char* blocked, DevBudget* budget,
+                                                      KspResult* res, Status* st) {
     if (st->failed) return;
     __shared__ long long s_cand;
     __shared__ int s_next;
@@ -167,10 +301,18 @@ __global__ void __launch_bounds__(1024) k_ksp_resolve(const KspDev K, const long
     __shared__ int s_cnt[32];
     const Grid& g = K.g;
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-    const int n = forced ? 1 : *total;
-    int pos = 0, accepted = 0, last_cells = 0;
+    const bool forced = mode == 1;
     DD nucO{0., 0.}, nucCr{0., 0.};
-    while (true) {
+    for (int q = 0; q < npre; ++q) {
+        const KspNucleus nu = pre[q];
+        stamp_ball(K, nu.x, nu.y, nu.z, o, cr, p, eta, nucO, nucCr);
+        __syncthreads();
+        if (mode == 0) mark_excluded(K, nu.x, nu.y, nu.z, nu.full != 0, p, blocked, res, false);
+        __syncthreads();
+    }
+    const int n = mode == 2 ? 0 : (forced ? 1 : *total);
+    int pos = 0, accepted = 0, last_cells = 0, listed = 0;
+    while (mode != 2) {
         // warp 0 finds the next accepted candidate from pos (32 at a time)
         if (w == 0) {
             int found = -1;
@@ -210,117 +352,25 @@ __global__ void __launch_bounds__(1024) k_ksp_resolve(const KspDev K, const long
             const int col = (int)(cq % g.nb);
             const long long rr = cq / g.nb;
             const int row = (int)(rr % g.na);
-            x = (int)(rr / g.na) + 1;
+            x = (int)(rr / g.na) + 1 + K.x_off;
             if (g.dim == 3) { y = row + 1; z = col + 1; } else { y = col + 1; }
         }
-        // stamp(x,y,z): ball cells with phi < .01 (3S:704-724 / 2D:503-516)
-        int cells = 0;
-        const double r2 = K.radius * K.radius;
-        if (g.dim == 3) {
-            const int rr = bounded_reach(K.radius, K.nx);
-            const AxisNb ys = periodic_nb(y, K.radius, K.ny), zs = periodic_nb(z, K.radius, K.nz);
-            const int i0 = (int)max(1LL, (long long)x - rr), i1 = (int)min((long long)K.nx, (long long)x + rr);
-            const int ny_n = (ys.hi0 - ys.lo0 + 1) + (ys.count > 1 ? ys.hi1 - ys.lo1 + 1 : 0);
-            const int nz_n = (zs.hi0 - zs.lo0 + 1) + (zs.count > 1 ? zs.hi1 - zs.lo1 + 1 : 0);
-            const long long tot = (long long)(i1 - i0 + 1) * ny_n * nz_n;
-            for (long long q = tid; q < tot; q += blockDim.x) {
-                const int kq = (int)(q % nz_n);
-                const long long t = q / nz_n;
-                const int jq = (int)(t % ny_n);
-                const int i = i0 + (int)(t / ny_n);
-                const int n0y = ys.hi0 - ys.lo0 + 1, n0z = zs.hi0 - zs.lo0 + 1;
-                const int j = jq < n0y ? ys.lo0 + jq : ys.lo1 + (jq - n0y);
-                const int k = kq < n0z ? zs.lo0 + kq : zs.lo1 + (kq - n0z);
-                const double dy = min_image((double)(j - y), (double)K.ny), dz = min_image((double)(k - z), (double)K.nz);
-                const long long idx = gidx(g, i, j, k);
-                if ((double)((i - x) * (i - x)) + dy * dy + dz * dz <= r2 && p[idx] < .01) {
-                    nucO = dd_add(nucO, Phys::oxideO - o[idx]);
-                    nucCr = dd_add(nucCr, Phys::oxideCr - cr[idx]);
-                    o[idx] = Phys::oxideO; cr[idx] = Phys::oxideCr; p[idx] = 1.;
-                    for (int e = 0; e < K.neta; ++e) eta[(long long)e * g.nstore + idx] = 0.;
-                    ++cells;
-                }
-            }
-        } else {
-            const int rr = (int)ceil(K.radius);
-            const int i0 = max(1, x - rr), i1 = min(K.nx, x + rr);
-            const long long tot = (long long)(i1 - i0 + 1) * K.ny;
-            for (long long q = tid; q < tot; q += blockDim.x) {
-                const int j = (int)(q % K.ny) + 1;
-                const int i = i0 + (int)(q / K.ny);
-                const double dy = min_image((double)(j - y), (double)K.ny);
-                const long long idx = gidx(g, i, j, 0);
-                if ((double)((i - x) * (i - x)) + dy * dy <= r2 && p[idx] < .01) {
-                    nucO = dd_add(nucO, Phys::oxideO - o[idx]);
-                    nucCr = dd_add(nucCr, Phys::oxideCr - cr[idx]);
-                    o[idx] = Phys::oxideO; cr[idx] = Phys::oxideCr; p[idx] = 1.;
-                    for (int e = 0; e < K.neta; ++e) eta[(long long)e * g.nstore + idx] = 0.;
-                    ++cells;
-                }
-            }
-        }
+        int cells = stamp_ball(K, x, y, z, o, cr, p, eta, nucO, nucCr);
         for (int off = 16; off > 0; off >>= 1) cells += __shfl_down_sync(0xffffffffu, cells, off);
         if (lane == 0) s_cnt[w] = cells;
         __syncthreads();
         int changed = 0;
         for (int ww = 0; ww < (int)(blockDim.x >> 5); ++ww) changed += s_cnt[ww];
-        if (changed) ++accepted;
-        last_cells = changed;
-        // exclusion marks for the later candidates of this scan
-        if (changed && !forced) {
-            if (changed == K.full_ball) {
-                for (int q = tid; q < K.n_shadow; q += blockDim.x) {
-                    const int di = K.shadow[3 * q], dj = K.shadow[3 * q + 1], dk = K.shadow[3 * q + 2];
-                    const int i = x + di;
-                    if (i < 1 || i > K.nx) continue;
-                    int j, k;
-                    if (g.dim == 3) {
-                        j = ((y - 1 + dj) % K.ny + K.ny) % K.ny;
-                        k = ((z - 1 + dk) % K.nz + K.nz) % K.nz;
-                        blocked[((long long)(i - 1) * K.ny + j) * K.nz + k] = 1;
-                    } else {
-                        j = ((y - 1 + dj) % K.ny + K.ny) % K.ny;
-                        blocked[(long long)(i - 1) * K.ny + j] = 1;
-                    }
-                }
-            } else {
-                // partial stamp (some ball cell had phi == .01 exactly): mark every cell of
-                // the exclusion box whose distance to a stamped cell passes the test
-                if (tid == 0) res->partial_stamps += 1;
-                const int R = K.box_half;
-                const long long side = 2LL * R + 1;
-                const long long tot = g.dim == 3 ? side * side * side : side * side;
-                for (long long q = tid; q < tot; q += blockDim.x) {
-                    int di, dj, dk = 0;
-                    if (g.dim == 3) { dk = (int)(q % side) - R; dj = (int)((q / side) % side) - R; di = (int)(q / (side * side)) - R; }
-                    else { dj = (int)(q % side) - R; di = (int)(q / side) - R; }
-                    const int i = x + di;
-                    if (i < 1 || i > K.nx) continue;
-                    const int jw = ((y - 1 + dj) % K.ny + K.ny) % K.ny + 1;
-                    const int kw = g.dim == 3 ? ((z - 1 + dk) % K.nz + K.nz) % K.nz + 1 : 0;
-                    bool hit = false;
-                    for (int b = 0; b < K.n_ball && !hit; ++b) {
-                        const int si = x + K.ball[3 * b];
-                        if (si < 1 || si > K.nx) continue;
-                        const int sj = ((y - 1 + K.ball[3 * b + 1]) % K.ny + K.ny) % K.ny + 1;
-                        const int sk = g.dim == 3 ? ((z - 1 + K.ball[3 * b + 2]) % K.nz + K.nz) % K.nz + 1 : 0;
-                        if (p[gidx(g, si, sj, sk)] != 1.) continue;   // not (newly) oxide
-                        const int ddi = si - i;
-                        const int ddj = (int)min_image((double)(sj - jw), (double)K.ny);
-                        if (g.dim == 3) {
-                            const int ddk = (int)min_image((double)(sk - kw), (double)K.nz);
-                            hit = sqrt((double)ddi * ddi + (double)ddj * ddj + (double)ddk * ddk) < K.radius + K.gap;
-                        } else {
-                            hit = K.hyp2d[abs(ddi) * K.hyp_stride + abs(ddj)] != 0;
-                        }
-                    }
-                    if (hit) {
-                        if (g.dim == 3) blocked[((long long)(i - 1) * K.ny + (jw - 1)) * K.nz + (kw - 1)] = 1;
-                        else blocked[(long long)(i - 1) * K.ny + (jw - 1)] = 1;
-                    }
-                }
+        if (changed) {
+            ++accepted;
+            if (!forced) {
+                if (tid == 0 && out && listed < cap) out[listed] = KspNucleus{x, y, z, changed == K.full_ball ? 1 : 0};
+                ++listed;
             }
         }
+        last_cells = changed;
+        // exclusion marks for the later candidates of this scan
+        if (changed && !forced) mark_excluded(K, x, y, z, changed == K.full_ball, p, blocked, res, true);
         __syncthreads();
         if (forced) break;
     }
@@ -339,9 +389,12 @@ __global__ void __launch_bounds__(1024) k_ksp_resolve(const KspDev K, const long
         budget->v[0][0] = bo.hi; budget->v[0][1] = bo.lo;
         budget->v[1][0] = bc.hi; budget->v[1][1] = bc.lo;
         budget->nuclei += accepted;
-        res->nuclei = accepted;
-        res->last_cells = last_cells;
-        res->candidates = n;
+        if (mode != 2) {
+            res->nuclei = accepted;
+            res->last_cells = last_cells;
+            res->candidates = n;
+            res->listed = listed;
+        }
     }
 }
 
@@ -354,20 +407,41 @@ int cgrid(long long n, int threads, int cap) {
 
 int ksp_compact_blocks(long long ncells) { return (int)((ncells + CBLK * CITEMS - 1) / (CBLK * CITEMS)); }
 
-void launch_ksp_scan(const KspDev& K, double* o, double* cr, double* p, double* eta, KspWork& W, DevBudget* budget,
-                     KspResult* res, Status* st, cudaStream_t stream) {
+void launch_ksp_candidates(const KspDev& K, const double* o, const double* cr, const double* p, KspWork& W,
+                           Status* st, cudaStream_t stream) {
     const long long n = K.g.ncells;
     cudaMemsetAsync(W.blocked, 0, (size_t)n, stream);
     k_ksp_candidates<<<cgrid(n, 128, 148 * 64), 128, 0, stream>>>(K, o, cr, p, W.flag, st);
     const int nb = ksp_compact_blocks(n);
     k_ksp_count<<<nb, CBLK, 0, stream>>>(W.flag, n, W.counts);
     k_ksp_write<<<nb, CBLK, 0, stream>>>(W.flag, n, W.counts, W.list, W.total, nb);
-    k_ksp_resolve<<<1, 1024, 0, stream>>>(K, W.list, W.total, 0, 0, 0, 0, o, cr, p, eta, W.blocked, budget, res, st);
+}
+
+void launch_ksp_scan(const KspDev& K, double* o, double* cr, double* p, double* eta, KspWork& W, DevBudget* budget,
+                     KspResult* res, Status* st, cudaStream_t stream) {
+    launch_ksp_candidates(K, o, cr, p, W, st, stream);
+    k_ksp_resolve<<<1, 1024, 0, stream>>>(K, W.list, W.total, 0, 0, 0, 0, nullptr, 0, nullptr, 0, o, cr, p, eta,
+                                          W.blocked, budget, res, st);
 }
 
 void launch_ksp_stamp(const KspDev& K, int x, int y, int z, double* o, double* cr, double* p, double* eta,
                       KspWork& W, DevBudget* budget, KspResult* res, Status* st, cudaStream_t stream) {
-    k_ksp_resolve<<<1, 1024, 0, stream>>>(K, W.list, W.total, 1, x, y, z, o, cr, p, eta, W.blocked, budget, res, st);
+    k_ksp_resolve<<<1, 1024, 0, stream>>>(K, W.list, W.total, 1, x, y, z, nullptr, 0, nullptr, 0, o, cr, p, eta,
+                                          W.blocked, budget, res, st);
+}
+
+void launch_ksp_resolve_slab(const KspDev& K, const KspNucleus* pre, int npre, KspNucleus* out, int cap, double* o,
+                             double* cr, double* p, double* eta, KspWork& W, DevBudget* budget, KspResult* res,
+                             Status* st, cudaStream_t stream) {
+    k_ksp_resolve<<<1, 1024, 0, stream>>>(K, W.list, W.total, 0, 0, 0, 0, pre, npre, out, cap, o, cr, p, eta,
+                                          W.blocked, budget, res, st);
+}
+
+void launch_ksp_apply(const KspDev& K, const KspNucleus* list, int n, double* o, double* cr, double* p, double* eta,
+                      KspWork& W, DevBudget* budget, KspResult* res, Status* st, cudaStream_t stream) {
+    if (n <= 0) return;
+    k_ksp_resolve<<<1, 1024, 0, stream>>>(K, W.list, W.total, 2, 0, 0, 0, list, n, nullptr, 0, o, cr, p, eta,
+                                          W.blocked, budget, res, st);
 }
 
 }  // namespace nicr

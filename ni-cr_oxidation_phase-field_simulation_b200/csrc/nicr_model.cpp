@@ -48,13 +48,25 @@ T* Model::dalloc_t(size_t n) {
     return p;
 }
 
-Model::Model(const nicr_config& cfg) : c(cfg), dim(cfg.dim) {
+Model::Model(const nicr_config& cfg, const SlabSpec* slab) : c(cfg), dim(cfg.dim) {
     if (dim != 2 && dim != 3) throw Error(NICR_ERR_INVALID_ARG, "dim must be 2 or 3");
     if (dim == 3 && (c.nx < 3 || c.ny < 3 || c.nz < 3 || c.nx > INT_MAX - 2 || c.ny > INT_MAX - 2 || c.nz > INT_MAX - 2))
         throw Error(NICR_ERR_INVALID_ARG, "3D grid dimensions must lie in [3, INT_MAX-2].");
     if (dim == 2 && (c.nx < 3 || c.ny < 3))
         throw Error(NICR_ERR_INVALID_ARG, "Invalid parameter bounds (Ksp nucleation period must be >= dt).");
     if (dim == 2) c.nz = 1;
+    int hlo = 0, hhi = 0;
+    if (slab) {
+        if (dim != 3) throw Error(NICR_ERR_INVALID_ARG, "the slab form is 3D only");
+        const SlabSpec& q = *slab;
+        if (q.halo < 2 || q.x0 < 0 || q.x1 > c.nx || q.x1 - q.x0 < q.halo || (q.x0 > 0 && q.x0 < q.halo) ||
+            (q.x1 < c.nx && c.nx - q.x1 < q.halo))
+            throw Error(NICR_ERR_INVALID_ARG, "slab planes must be at least the halo width and within the domain");
+        is_slab = true;
+        hlo = q.x0 > 0 ? q.halo : 0;
+        hhi = q.x1 < c.nx ? q.halo : 0;
+        x_off = q.x0 - hlo;
+    }
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
         throw Error(NICR_ERR_NO_DEVICE, "no CUDA device is available");
@@ -62,7 +74,7 @@ Model::Model(const nicr_config& cfg) : c(cfg), dim(cfg.dim) {
     check_cuda(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate");
 
     g.dim = dim;
-    g.nx = c.nx;
+    g.nx = is_slab ? slab->x1 - slab->x0 + hlo + hhi : c.nx;
     g.na = dim == 3 ? c.ny : 1;
     g.nb = dim == 3 ? c.nz : c.ny;
     g.pb = (g.nb + 7) / 8 * 8;
@@ -107,11 +119,20 @@ Model::Model(const nicr_config& cfg) : c(cfg), dim(cfg.dim) {
     sp.o_on = c.oxygen_diffusion ? 1 : 0;
     sp.grains = c.grains ? 1 : 0;
     sp.phi_eta = has_eta ? 1 : 0;
-    sp.inlet = (c.bc == NICR_BC_CONCENTRATION && c.oxygen_diffusion) ? 1 : 0;
+    // the inlet layer is domain plane 0 (a slab above it only reads it)
+    sp.inlet = (c.bc == NICR_BC_CONCENTRATION && c.oxygen_diffusion && x_off == 0) ? 1 : 0;
     if (c.precision != NICR_FP64 && c.precision != NICR_FP64_FAST)
         throw Error(NICR_ERR_INVALID_ARG, "precision must be NICR_FP64 or NICR_FP64_FAST");
     sp.fast = c.precision == NICR_FP64_FAST ? 1 : 0;
-    sp.xchunk = choose_xchunk(g);
+    whole_domain_range(sp);
+    if (is_slab) {
+        sp.x_lo = hlo;
+        sp.x_hi = hlo + (slab->x1 - slab->x0);
+        sp.cell_off = (long long)x_off * g.na * g.nb;
+        sp.key_ncells = (long long)c.nx * g.na * g.nb;
+        sp.err_slot = 0;
+    }
+    sp.xchunk = choose_xchunk(own_grid());
 
     try {
         const size_t ns = (size_t)g.nstore;
@@ -131,13 +152,13 @@ Model::Model(const nicr_config& cfg) : c(cfg), dim(cfg.dim) {
         red_out = dalloc_t<StepPartial>(1);
         check_cuda(cudaMallocHost(&h_st, sizeof(Status)), "cudaMallocHost");
         check_cuda(cudaMemsetAsync(bud, 0, sizeof(DevBudget), stream), "memset");
-        Status s0{ERR_NONE, 0, 0, -1, 0};
+        Status s0{ERR_NONE, 0, 0, -1, 0, {ERR_NONE, ERR_NONE}};
         *h_st = s0;
         check_cuda(cudaMemcpyAsync(st, h_st, sizeof(Status), cudaMemcpyHostToDevice, stream), "memcpy");
 
         voronoi();
-        InitParams I{};
-        I.g = g; I.bulk_cr = c.bulk_cr; I.layer_o = c.layer_o; I.inlet_layer = c.bc == NICR_BC_CONCENTRATION;
+        InitParams I = init_params();
+        I.bulk_cr = c.bulk_cr; I.layer_o = c.layer_o; I.inlet_layer = c.bc == NICR_BC_CONCENTRATION;
         launch_init_fields(I, o_[0], cr_[0], p_[0], stream);
         if (dim == 2) check_cuda(cudaMemcpyAsync(gb_initial, gb_[0], ns * 8, cudaMemcpyDeviceToDevice, stream), "memcpy");
         reset_inventory();
@@ -211,7 +232,7 @@ void Model::voronoi() {
         seeds.push_back(0.5 * c.nx);
         seeds.push_back(0.5 * c.ny);
         if (dim == 3) seeds.push_back(0.5 * c.nz);
-        volumes.push_back(dim == 3 ? (long long)(c.nx * c.ny * c.nz) : (long long)(c.nx * c.ny));
+        volumes.push_back(is_slab ? own_grid().ncells : dim == 3 ? (long long)(c.nx * c.ny * c.nz) : (long long)(c.nx * c.ny));
         std::vector<double> ones((size_t)g.ncells, 1.);
         copy_in(grain, ones.data());
         check_cuda(cudaMemsetAsync(gb_[0], 0, ns * 8, stream), "memset");
@@ -288,8 +309,8 @@ void Model::voronoi() {
         double* d_db = gb_[0];
         check_cuda(cudaMemcpyAsync(d_seeds, seeds.data(), seeds.size() * 8, cudaMemcpyHostToDevice, stream), "H2D");
         check_cuda(cudaMemsetAsync(d_vol, 0, ng * sizeof(int), stream), "memset");
-        InitParams I{};
-        I.g = g; I.ng = ng; I.nxd = c.nx; I.nyd = c.ny; I.nzd = c.nz;
+        InitParams I = init_params();
+        I.ng = ng; I.nxd = c.nx; I.nyd = c.ny; I.nzd = c.nz;
         launch_voronoi3(I, d_seeds, grain, d_db, d_vol, stream);
         std::vector<int> vol(ng);
         check_cuda(cudaMemcpyAsync(vol.data(), d_vol, ng * sizeof(int), cudaMemcpyDeviceToHost, stream), "D2H");
@@ -356,8 +377,26 @@ void Model::voronoi2d_host(std::vector<double>& grain_h, std::vector<double>& gb
     for (int k = 0; k < ng; ++k) volumes[k] = vol[k];
 }
 
+Grid Model::own_grid() const {
+    Grid o = g;
+    o.nx = sp.x_hi - sp.x_lo;
+    o.ncells = (long long)o.nx * g.na * g.nb;
+    o.nstore = (long long)o.nx * g.plane;
+    return o;
+}
+
+InitParams Model::init_params() const {
+    InitParams I{};
+    I.g = g;
+    I.x_off = x_off;
+    I.x_lo = sp.x_lo;
+    I.x_hi = sp.x_hi;
+    return I;
+}
+
 void Model::reset_inventory() {
-    launch_diagnostics(g, o_[cur], cr_[cur], p_[cur], diag_part, nullptr, diag_out, stream);
+    const long long off = own_offset();
+    launch_diagnostics(own_grid(), o_[cur] + off, cr_[cur] + off, p_[cur] + off, diag_part, nullptr, diag_out, stream);
     DiagOut d;
     check_cuda(cudaMemcpyAsync(&d, diag_out, sizeof d, cudaMemcpyDeviceToHost, stream), "D2H");
     sync();
@@ -378,8 +417,7 @@ void Model::init_center_seed() {
     if (r >= 0.5 * (double(mn) - 1.))
         throw Error(NICR_ERR_INVALID_ARG, dim == 3 ? "Center seed is too large: --radius-grid must be less than (min(nx,ny,nz)-1)/2."
                                                    : "Center seed is too large: --radius-grid must be less than (min(nx,ny)-1)/2.");
-    InitParams I{};
-    I.g = g;
+    InitParams I = init_params();
     int nb = 0;
     launch_center_seed(I, x, y, z, r, 0, o_[cur], cr_[cur], p_[cur], nullptr, partials, stream, &nb);
     launch_reduce_partials(partials, nb, red_out, stream);
@@ -389,10 +427,11 @@ void Model::init_center_seed() {
     check_cuda(cudaMemcpyAsync(&b, bud, sizeof b, cudaMemcpyDeviceToHost, stream), "D2H");
     sync();
     center_seed_cells = (int)s.clipped;
-    if (center_seed_cells == 0) throw Error(NICR_ERR_INVALID_ARG, "Center seed covers no cell centres: increase --radius-grid.");
+    // a slab may hold none of the seed; its group checks the total
+    if (center_seed_cells == 0 && !is_slab) throw Error(NICR_ERR_INVALID_ARG, "Center seed covers no cell centres: increase --radius-grid.");
     b.v[0][0] = s.s[0][0]; b.v[0][1] = s.s[0][1];
     b.v[1][0] = s.s[1][0]; b.v[1][1] = s.s[1][1];
-    b.nuclei += 1;
+    if (x_off == 0) b.nuclei += 1;   // counted once, by the slab holding domain plane 0
     check_cuda(cudaMemcpyAsync(bud, &b, sizeof b, cudaMemcpyHostToDevice, stream), "H2D");
     sync();
 }
@@ -415,8 +454,8 @@ void Model::init_eta() {
     if (dim == 3) {
         double* d_seeds = dalloc(seeds.size());
         check_cuda(cudaMemcpyAsync(d_seeds, seeds.data(), seeds.size() * 8, cudaMemcpyHostToDevice, stream), "H2D");
-        InitParams I{};
-        I.g = g; I.ng = ng; I.nxd = c.nx; I.nyd = c.ny; I.nzd = c.nz;
+        InitParams I = init_params();
+        I.ng = ng; I.nxd = c.nx; I.nyd = c.ny; I.nzd = c.nz;
         launch_eta_dist3(I, d_seeds, grain, eta_[0], stream);
         for (int q = 0; q < ng; ++q) copy_out(eta_[0] + (size_t)q * ns, d.data() + (size_t)q * n);
         cudaFree(d_seeds);
@@ -523,6 +562,9 @@ void Model::setup_ksp() {
     kd.ball = d_ball; kd.n_ball = nball;
     kd.full_ball = nball;
     kd.box_half = B;
+    kd.x_off = x_off;
+    kd.x_lo = sp.x_lo;
+    kd.x_hi = sp.x_hi;
     kw.flag = dalloc_t<unsigned char>((size_t)g.ncells);
     kw.blocked = dalloc_t<unsigned char>((size_t)g.ncells);
     kw.counts = dalloc_t<int>(ksp_compact_blocks(g.ncells) + 1);
@@ -536,18 +578,29 @@ void Model::setup_ksp() {
 // ------------------------------------------------------------------ fields
 static bool is_state_field(int f) { return f == NICR_FIELD_O || f == NICR_FIELD_CR || f == NICR_FIELD_PHI || f == NICR_FIELD_ETA; }
 
-void Model::set_field(int field, int index, const double* host) {
+double* Model::state_ptr(int field, int index) {
     if (!is_state_field(field)) throw Error(NICR_ERR_INVALID_ARG, "only O, CR, PHI and ETA can be set");
-    double* d = nullptr;
-    if (field == NICR_FIELD_O) d = o_[cur];
-    else if (field == NICR_FIELD_CR) d = cr_[cur];
-    else if (field == NICR_FIELD_PHI) d = p_[cur];
-    else {
-        if (index < 0 || index >= neta) throw Error(NICR_ERR_INVALID_ARG, "eta index out of range");
-        d = eta_[ecur] + (size_t)index * g.nstore;
-    }
-    copy_in(d, host);
+    if (field == NICR_FIELD_O) return o_[cur];
+    if (field == NICR_FIELD_CR) return cr_[cur];
+    if (field == NICR_FIELD_PHI) return p_[cur];
+    if (index < 0 || index >= neta) throw Error(NICR_ERR_INVALID_ARG, "eta index out of range");
+    return eta_[ecur] + (size_t)index * g.nstore;
+}
+
+void Model::set_field(int field, int index, const double* host) {
+    copy_in(state_ptr(field, index), host);
     eta_dirty = true;  // any edit invalidates the frozen-eta cache (3S:347-349)
+}
+
+void Model::copy_planes_out(const double* d, double* host, int x_begin, int count) {
+    check_cuda(cudaMemcpy2DAsync(host, (size_t)g.nb * 8, d + (size_t)x_begin * g.plane, (size_t)g.pb * 8,
+                                 (size_t)g.nb * 8, (size_t)count * g.na, cudaMemcpyDeviceToHost, stream), "D2H");
+    sync();
+}
+void Model::copy_planes_in(double* d, const double* host, int x_begin, int count) {
+    check_cuda(cudaMemcpy2DAsync(d + (size_t)x_begin * g.plane, (size_t)g.pb * 8, host, (size_t)g.nb * 8,
+                                 (size_t)g.nb * 8, (size_t)count * g.na, cudaMemcpyHostToDevice, stream), "H2D");
+    sync();
 }
 
 void Model::refresh() {
@@ -562,7 +615,7 @@ void Model::refresh() {
     check_cuda(cudaGetLastError(), "refresh");
 }
 
-void Model::get_field(int field, int index, double* host) {
+const double* Model::field_ptr(int field, int index) {
     const double* d = nullptr;
     switch (field) {
         case NICR_FIELD_O: d = o_[cur]; break;
@@ -600,8 +653,10 @@ void Model::get_field(int field, int index, double* host) {
             break;
         default: throw Error(NICR_ERR_INVALID_ARG, "unknown field");
     }
-    copy_out(d, host);
+    return d;
 }
+
+void Model::get_field(int field, int index, double* host) { copy_out(field_ptr(field, index), host); }
 
 // ------------------------------------------------------------------ stepping
 void Model::reset_status() {
@@ -611,6 +666,7 @@ void Model::reset_status() {
     h_st->timeout = 0;
     h_st->failed_step = -1;
     h_st->steps_done = steps_done;
+    h_st->slot_err[0] = h_st->slot_err[1] = ERR_NONE;
     check_cuda(cudaMemcpyAsync(st, h_st, sizeof(Status), cudaMemcpyHostToDevice, stream), "H2D");
 }
 
@@ -736,11 +792,17 @@ std::string Model::describe_failure(unsigned long long key, int nxt) {
         const int row = (int)(r % g.na);
         i = (int)(r / g.na) + 1;
         if (dim == 3) { j = row + 1; k = col + 1; } else { j = col + 1; k = 0; }
-        return (long long)(i - 1) * g.plane + (long long)row * g.pb + col;
+        return (long long)(i - 1 - x_off) * g.plane + (long long)row * g.pb + col;
+    };
+    // a slab describes only failures in its own planes (its group asks the owner)
+    auto owned = [&](long long cell) {
+        const long long xi = cell / ((long long)g.na * g.nb) - x_off;
+        return xi >= sp.x_lo && xi < sp.x_hi;
     };
     int i, j, k;
     if (key < ERR_ETA_BASE) {
         const long long cell = (long long)(key / 4);
+        if (!owned(cell)) return std::string();
         if (key % 4 == 0) return "Nonfinite trial field: reduce dt / inspect the model; no update accepted.";
         const long long idx = coords(cell, i, j, k);
         double v[3];
@@ -755,8 +817,9 @@ std::string Model::describe_failure(unsigned long long key, int nxt) {
         return msg.str();
     }
     const unsigned long long q = key - ERR_ETA_BASE;
-    const int gi = (int)(q / (unsigned long long)g.ncells);
-    const long long idx = coords((long long)(q % (unsigned long long)g.ncells), i, j, k);
+    const int gi = (int)(q / (unsigned long long)sp.key_ncells);
+    if (!owned((long long)(q % (unsigned long long)sp.key_ncells))) return std::string();
+    const long long idx = coords((long long)(q % (unsigned long long)sp.key_ncells), i, j, k);
     double v;
     check_cuda(cudaMemcpyAsync(&v, eta_[ecur ^ 1] + (size_t)gi * g.nstore + idx, 8, cudaMemcpyDeviceToHost, stream), "D2H");
     sync();
@@ -885,6 +948,7 @@ void Model::launch_step_pair() {
 }
 
 int Model::step(int nsteps, int* completed) {
+    if (is_slab) throw Error(NICR_ERR_STATE, "a slab is advanced by its slab group");
     if (completed) *completed = 0;
     if (nsteps <= 0) return NICR_OK;
     RunPlan r;
@@ -903,6 +967,7 @@ int Model::step(int nsteps, int* completed) {
 }
 
 int Model::run(int nsteps, int* completed) {
+    if (is_slab) throw Error(NICR_ERR_STATE, "a slab is advanced by its slab group");
     if (completed) *completed = 0;
     if (nsteps <= 0) return NICR_OK;
     RunPlan r;
@@ -920,6 +985,33 @@ int Model::run(int nsteps, int* completed) {
         }
     }
     return run_end(r, completed);
+}
+
+int Model::slab_launch() {
+    prepare_step();
+    StepParams P = sp;
+    P.err_slot = cur;   // one error word per buffer parity: consecutive steps alternate
+    int nb = 0;
+    size_t e = prof_begin();
+    launch_step_main(P, o_[cur], cr_[cur], p_[cur], gb_[gcur], has_eta ? s2_[gcur] : nullptr, o_[cur ^ 1],
+                     cr_[cur ^ 1], p_[cur ^ 1], partials, st, stream, &nb);
+    prof_end(K_STEP_MAIN, e, 1);
+    if (advance_eta) {
+        e = prof_begin();
+        launch_eta_update(P, neta, eta_[ecur], s2_[gcur], p_[cur], eta_[ecur ^ 1], gb_[gcur ^ 1], s2_[gcur ^ 1], st, stream);
+        prof_end(K_ETA_UPDATE, e, 1);
+    }
+    return nb;
+}
+
+void Model::slab_commit(int nblocks, const SlabPeers& peers) {
+    SlabPeers q = peers;
+    q.slot = cur;
+    const size_t e = prof_begin();
+    launch_step_finalize_slab(partials, nblocks, bud, st, q, stream);
+    prof_end(K_FINALIZE, e, 1);
+    cur ^= 1;
+    if (advance_eta) { ecur ^= 1; gcur ^= 1; }
 }
 
 void Model::adopt_stream(cudaStream_t s) {
@@ -977,7 +1069,8 @@ void Model::budget(nicr_budget* out) {
 }
 
 void Model::diagnostics(nicr_diagnostics* d) {
-    launch_diagnostics(g, o_[cur], cr_[cur], p_[cur], diag_part, nullptr, diag_out, stream);
+    const long long off = own_offset();
+    launch_diagnostics(own_grid(), o_[cur] + off, cr_[cur] + off, p_[cur] + off, diag_part, nullptr, diag_out, stream);
     DiagOut r;
     check_cuda(cudaMemcpyAsync(&r, diag_out, sizeof r, cudaMemcpyDeviceToHost, stream), "D2H");
     sync();

@@ -24,11 +24,21 @@ struct Error : std::runtime_error {
 };
 
 void check_cuda(cudaError_t e, const char* what);
+
+// An X slab of a larger 3D domain (the slab form, nicr_slabs.cpp): the model
+// owns domain planes [x0, x1) and stores them with up to `halo` neighbour
+// planes below and above (clipped to the domain), which its group refreshes
+// from the neighbouring slabs; every stored plane is initialised like the
+// whole domain's, so the halos start consistent.
+struct SlabSpec {
+    int x0 = 0, x1 = 0, halo = 0;
+};
+class SlabGroup;
 int run_self_test(int dim);   // --self-test (nicr_selftest.cpp)
 
 class Model {
 public:
-    explicit Model(const nicr_config& cfg);
+    explicit Model(const nicr_config& cfg, const SlabSpec* slab = nullptr);
     ~Model();
     Model(const Model&) = delete;
     Model& operator=(const Model&) = delete;
@@ -47,6 +57,9 @@ public:
     double next_nucleation;
     long long steps_done = 0;          // accepted steps (host view)
     std::string last_error;
+    // slab form: stored plane 0 is domain plane x_off; own planes [sp.x_lo, sp.x_hi)
+    bool is_slab = false;
+    int x_off = 0;
 
     cudaStream_t stream = nullptr;
     bool owns_stream = true;
@@ -122,6 +135,19 @@ public:
     void run_pre_step(RunPlan& r, int s);
     int run_end(RunPlan& r, int* completed);
 
+    // The own planes as a grid of their own (a whole domain: g) and their
+    // offset in the stored arrays, for reductions over owned cells.
+    Grid own_grid() const;
+    long long own_offset() const { return (long long)sp.x_lo * g.plane; }
+    InitParams init_params() const;
+    // Device array of a field for reading (materialising mu/M, the mask or the
+    // eta cache first), and of a state field for writing.
+    const double* field_ptr(int field, int index);
+    double* state_ptr(int field, int index);
+    // Host copies of stored planes [x_begin, x_begin + count) of device array d.
+    void copy_planes_out(const double* d, double* host, int x_begin, int count);
+    void copy_planes_in(double* d, const double* host, int x_begin, int count);
+
     // raw device pointers of the current state (for tests, bench, writers)
     double* d_o() const { return o_[cur]; }
     double* d_cr() const { return cr_[cur]; }
@@ -139,6 +165,12 @@ public:
     void ensure_mask() { if (has_eta && (eta_dirty || dim == 2)) eta_mask_now(); }
 
 private:
+    friend class SlabGroup;
+    // slab form: the step kernels of one step into the trial buffers (no
+    // commit; returns the step kernel's partial count), and the commit that
+    // agrees with the other slabs on the step's outcome, then flips parity
+    int slab_launch();
+    void slab_commit(int nblocks, const SlabPeers& peers);
     StepParams sp{};
     size_t dev_bytes = 0;
     // state (ping-pong)

@@ -48,6 +48,7 @@ __global__ void k_status_clear(nicr::Status* st) {
     st->failed = 0;
     st->timeout = 0;
     st->failed_step = -1;
+    st->slot_err[0] = st->slot_err[1] = nicr::ERR_NONE;
 }
 
 // Reduces the per-CTA partials in block order (deterministic) into the
@@ -139,6 +140,7 @@ nicr::StepParams params_for(const nicr_config& c) {
     sp.inlet = (c.bc == NICR_BC_CONCENTRATION && c.oxygen_diffusion) ? 1 : 0;
     sp.fast = c.precision == NICR_FP64_FAST ? 1 : 0;
     sp.xchunk = choose_xchunk(g);
+    whole_domain_range(sp);
     return sp;
 }
 

@@ -116,6 +116,59 @@ __global__ void k_step_finalize(const StepPartial* __restrict__ partials, int nb
     finalize_body(partials, nblocks, budget, st, accept_mode);
 }
 
+// Slab commit: the same reduction; the step's outcome is the minimum over
+// every slab's error word of this step. The words are read with volatile
+// loads (L2, or the owning GPU's memory for a peer slab) after the stream
+// has waited for every slab's step kernels, so all slabs decide alike.
+__global__ void k_step_finalize_slab(const StepPartial* __restrict__ partials, int nblocks, DevBudget* budget,
+                                     Status* st, const SlabPeers peers) {
+    __shared__ DD sdd[32 * 5];
+    __shared__ long long scnt[32];
+    if (st->failed) return;
+    DD acc[5] = {{0., 0.}, {0., 0.}, {0., 0.}, {0., 0.}, {0., 0.}};
+    long long clipped = 0;
+    for (int b = threadIdx.x; b < nblocks; b += blockDim.x) {
+        for (int q = 0; q < 5; ++q) acc[q] = dd_add(acc[q], DD{partials[b].s[q][0], partials[b].s[q][1]});
+        clipped += partials[b].clipped;
+    }
+    block_reduce_dd<5>(acc, clipped, sdd, scnt);
+    if (threadIdx.x == 0) {
+        unsigned long long key = ERR_NONE;
+        for (int j = 0; j < peers.n; ++j) {
+            const volatile unsigned long long* w = &peers.st[j]->slot_err[peers.slot];
+            const unsigned long long v = *w;
+            key = v < key ? v : key;
+        }
+        if (key != ERR_NONE) {
+            st->err_key = key;
+            st->failed = 1;
+            st->failed_step = st->steps_done;
+            return;
+        }
+        for (int q = 0; q < 5; ++q) {
+            DD b{budget->v[2 + q][0], budget->v[2 + q][1]};
+            b = dd_add(b, acc[q]);
+            budget->v[2 + q][0] = b.hi;
+            budget->v[2 + q][1] = b.lo;
+        }
+        budget->clipped += clipped;
+        st->steps_done += 1;
+    }
+}
+
+// Strided runs of double pairs: blockIdx.y picks the segment, the CTAs of a
+// row of blocks stride over its rows x n doubles.
+__global__ void k_copy_segments(const CopyList L, const Status* st) {
+    if (st && st->failed) return;
+    const CopySeg& S = L.s[blockIdx.y];
+    const long long pairs = S.n / 2, total = pairs * S.rows;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total; q += (long long)gridDim.x * blockDim.x) {
+        const long long r = q / pairs, c = 2 * (q - r * pairs);
+        const double2 v = *reinterpret_cast<const double2*>(S.src + r * S.src_pitch + c);
+        *reinterpret_cast<double2*>(S.dst + r * S.dst_pitch + c) = v;
+    }
+}
+
 // Batched commit: block b commits domain b (same arithmetic as k_step_finalize).
 __global__ void k_finalize_batch(const __grid_constant__ FinalizeBatch B) {
     const FinalizeDomain& d = B.d[blockIdx.x];
@@ -254,6 +307,20 @@ void launch_eta_update(const StepParams& P, int neta, const double* eta, const d
 void launch_step_finalize(const StepPartial* partials, int nblocks, DevBudget* budget, Status* st, int accept_mode,
                           cudaStream_t stream) {
     k_step_finalize<<<1, 256, 0, stream>>>(partials, nblocks, budget, st, accept_mode);
+}
+
+void launch_step_finalize_slab(const StepPartial* partials, int nblocks, DevBudget* budget, Status* st,
+                               const SlabPeers& peers, cudaStream_t stream) {
+    k_step_finalize_slab<<<1, 256, 0, stream>>>(partials, nblocks, budget, st, peers);
+}
+
+void launch_copy_segments(const CopyList& L, const Status* st, cudaStream_t stream) {
+    if (L.count <= 0) return;
+    long long most = 0;
+    for (int i = 0; i < L.count; ++i) most = std::max(most, L.s[i].n / 2 * L.s[i].rows);
+    const long long want = (most + 255) / 256;
+    const int bx = (int)std::max(1LL, std::min(want, 148LL * 4));
+    k_copy_segments<<<dim3(bx, L.count), 256, 0, stream>>>(L, st);
 }
 
 void launch_finalize_batch(const FinalizeDomain* doms, int n, cudaStream_t stream) {

@@ -97,11 +97,19 @@ __device__ __forceinline__ double fdiv(double a, const DivC& d) {
     return xdiv(a, d);
 }
 
+// The error word a launch with parameters P reports its first failing trial to.
+__device__ __forceinline__ unsigned long long* err_word(const StepParams& P, Status* st) {
+    return P.err_slot < 0 ? &st->err_key : &st->slot_err[P.err_slot];
+}
+
 struct CenterVals {
     double o, cr, p, hh, muO, muCr, mo, mc;   // hh = h(p), reused by Ck
 };
 
-template <int DIM, int TA, int TB, bool FAST>
+// SLAB instances update the plane range [P.x_lo, P.x_hi) of a slab's stored
+// planes and report keys with P's offsets to P's error word; the whole-domain
+// instances keep range and keys compile-time.
+template <int DIM, int TA, int TB, bool FAST, bool SLAB = false>
 struct StepKernel {
     using T = Tile<DIM, TA, TB>;
 
@@ -280,8 +288,8 @@ struct StepKernel {
         const Grid& g = P.g;
         const int ta = DIM == 3 ? threadIdx.y : 0, tb = threadIdx.x;
         const int a0 = DIM == 3 ? by * TA : 0, b0 = bx * TB;
-        const int i0 = bz * P.xchunk;
-        const int i1 = min(g.nx, i0 + P.xchunk);
+        const int i0 = (SLAB ? P.x_lo : 0) + bz * P.xchunk;
+        const int i1 = min(SLAB ? P.x_hi : g.nx, i0 + P.xchunk);
         const int row = a0 + ta, col = b0 + tb;
         const bool active = (DIM == 3 ? row < g.na : true) && col < g.nb;
         const Offs offs = make_offs(g, a0, b0);
@@ -393,7 +401,7 @@ struct StepKernel {
                 const int bp = T::i1(ta, tb + 1), bm = T::i1(ta, tb - 1);
                 const int ap = T::i1(ta + 1, tb), am = T::i1(ta - 1, tb);
                 const long long gidx = (long long)u * g.plane + (long long)row * g.pb + col;
-                const long long cell = ((long long)u * g.na + row) * g.nb + col;  // reference loop order
+                const long long cell = ((long long)u * g.na + row) * g.nb + col + (SLAB ? P.cell_off : 0);  // reference loop order
 
                 // x faces: the right face of u is the left face of u+1 (same expression)
                 const double rightO = fdiv<FAST>(-.5 * (C.mo + L.mo) * (L.muO - C.muO), P.v_dx);
@@ -483,7 +491,7 @@ struct StepKernel {
             C = L;
             s2u = s2n;
         }
-        if (errkey != ERR_NONE) atomicMin(&st->err_key, errkey);
+        if (errkey != ERR_NONE) atomicMin(SLAB ? err_word(P, st) : &st->err_key, errkey);
         block_reduce_dd<5>(acc, clipped, sdd, scnt);
         if (threadIdx.x == 0 && threadIdx.y == 0) {
             StepPartial& out = partials[blin];
@@ -493,13 +501,13 @@ struct StepKernel {
     }
 };
 
-template <int DIM, int TA, int TB, int MINB, bool FAST>
+template <int DIM, int TA, int TB, int MINB, bool FAST, bool SLAB = false>
 __global__ void __launch_bounds__(TA * TB, MINB)
 k_step_main(const StepParams P, const double* __restrict__ o, const double* __restrict__ cr,
             const double* __restrict__ p, const double* __restrict__ gb, const double* __restrict__ s2,
             double* __restrict__ on, double* __restrict__ crn, double* __restrict__ pn,
             StepPartial* __restrict__ partials, Status* st) {
-    StepKernel<DIM, TA, TB, FAST>::run(P, o, cr, p, gb, s2, on, crn, pn, partials, st, blockIdx.x, blockIdx.y,
+    StepKernel<DIM, TA, TB, FAST, SLAB>::run(P, o, cr, p, gb, s2, on, crn, pn, partials, st, blockIdx.x, blockIdx.y,
                                        blockIdx.z, blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z));
 }
 
@@ -509,7 +517,7 @@ constexpr int TA2 = 1, TB2 = 128;   // 2D tile: 128 columns
 template <int DIM, int TA, int TB>
 dim3 step_grid(const StepParams& P) {
     const Grid& g = P.g;
-    return dim3((g.nb + TB - 1) / TB, DIM == 3 ? (g.na + TA - 1) / TA : 1, (g.nx + P.xchunk - 1) / P.xchunk);
+    return dim3((g.nb + TB - 1) / TB, DIM == 3 ? (g.na + TA - 1) / TA : 1, (P.x_hi - P.x_lo + P.xchunk - 1) / P.xchunk);
 }
 
 // eta_trial (3S:514-526): v = eta - (dt*L_eta)*(deta - K*lap(eta)); must lie in
@@ -523,7 +531,7 @@ __device__ __forceinline__ void eta_cell(const StepParams& P, int neta, const do
                                          unsigned long long& errkey) {
     const Grid& g = P.g;
     const long long idx = (long long)x * g.plane + (long long)row * g.pb + col;
-    const long long cell = ((long long)x * g.na + row) * g.nb + col;
+    const long long cell = ((long long)x * g.na + row) * g.nb + col + P.cell_off;
     const long long ixm = x > 0 ? idx - g.plane : idx, ixp = x < g.nx - 1 ? idx + g.plane : idx;
     const long long rbase = (long long)x * g.plane;
     const long long ibm = rbase + (long long)row * g.pb + (col == 0 ? g.nb - 1 : col - 1);
@@ -549,7 +557,7 @@ __device__ __forceinline__ void eta_cell(const StepParams& P, int neta, const do
         const double force = grain_deta(ec, S, phi, P.eta_W, P.eta_A) - P.eta_K * lap;
         const double v = ec - P.dt_etaL * force;
         if (!isfinite(v) || v < -1.e-12 || v > 1. + 1.e-12)
-            errkey = min(errkey, ERR_ETA_BASE + (unsigned long long)q * (unsigned long long)g.ncells + (unsigned long long)cell);
+            errkey = min(errkey, ERR_ETA_BASE + (unsigned long long)q * (unsigned long long)P.key_ncells + (unsigned long long)cell);
         eta_next[(long long)q * g.nstore + idx] = v;
         const double sq = v * v;
         pairs += Sn * sq;
@@ -573,8 +581,8 @@ __global__ void __launch_bounds__(256, 5) k_eta_update(const StepParams P, int n
     const int row = DIM == 3 ? blockIdx.y * blockDim.y + threadIdx.y : 0;
     if (col >= g.nb || row >= g.na) return;
     unsigned long long errkey = ERR_NONE;
-    eta_cell<DIM, FAST>(P, neta, eta, s2, p, eta_next, gb_next, s2_next, blockIdx.z, row, col, errkey);
-    if (errkey != ERR_NONE) atomicMin(&st->err_key, errkey);
+    eta_cell<DIM, FAST>(P, neta, eta, s2, p, eta_next, gb_next, s2_next, P.x_lo + blockIdx.z, row, col, errkey);
+    if (errkey != ERR_NONE) atomicMin(err_word(P, st), errkey);
 }
 
 // X-marching form of the eta update for a compile-time number of fields N:
@@ -584,8 +592,11 @@ __global__ void __launch_bounds__(256, 5) k_eta_update(const StepParams P, int n
 // the neighbouring threads' own loads). All N loads of the next plane are
 // issued before the arithmetic of the current plane.
 // NCAP is the register capacity; the first n <= NCAP fields are updated (the
-// stand-alone kernel instantiates NCAP = n, so the guards fold away).
-template <int DIM, bool FAST, int NCAP>
+// stand-alone kernel instantiates NCAP = n, so the guards fold away). SLAB
+// instances take the plane range and key offsets from P; the whole-domain
+// instances keep them compile-time (the runtime range cost this kernel's
+// schedule 85% at 128 registers).
+template <int DIM, bool FAST, int NCAP, bool SLAB = false>
 __device__ __forceinline__ void eta_march_body(const StepParams& P, int n, const double* __restrict__ eta,
                                                const double* __restrict__ p, double* __restrict__ eta_next,
                                                double* __restrict__ gb_next, double* __restrict__ s2_next,
@@ -595,7 +606,7 @@ __device__ __forceinline__ void eta_march_body(const StepParams& P, int n, const
     const int col = bx * blockDim.x + threadIdx.x;
     const int row = DIM == 3 ? by * blockDim.y + threadIdx.y : 0;
     if (col >= g.nb || row >= g.na) return;
-    const int i0 = bz * P.xchunk, i1 = min(g.nx, i0 + P.xchunk);
+    const int i0 = (SLAB ? P.x_lo : 0) + bz * P.xchunk, i1 = min(SLAB ? P.x_hi : g.nx, i0 + P.xchunk);
     const long long rc = (long long)row * g.pb + col;
     const long long cbm = (long long)row * g.pb + (col == 0 ? g.nb - 1 : col - 1);
     const long long cbp = (long long)row * g.pb + (col == g.nb - 1 ? 0 : col + 1);
@@ -627,7 +638,7 @@ __device__ __forceinline__ void eta_march_body(const StepParams& P, int n, const
 #pragma unroll
         for (int q = 0; q < NCAP; ++q)
             if (q < n) S += ec[q] * ec[q];
-        const long long cell = ((long long)x * g.na + row) * g.nb + col;
+        const long long cell = ((long long)x * g.na + row) * g.nb + col + (SLAB ? P.cell_off : 0);
         double Sn = 0., pairs = 0.;
 #pragma unroll
         for (int q = 0; q < NCAP; ++q) {
@@ -645,7 +656,7 @@ __device__ __forceinline__ void eta_march_body(const StepParams& P, int n, const
             const double force = grain_deta(c0, S, phi, P.eta_W, P.eta_A) - P.eta_K * lap;
             const double v = c0 - P.dt_etaL * force;
             if (!isfinite(v) || v < -1.e-12 || v > 1. + 1.e-12)
-                errkey = min(errkey, ERR_ETA_BASE + (unsigned long long)q * (unsigned long long)g.ncells + (unsigned long long)cell);
+                errkey = min(errkey, ERR_ETA_BASE + (unsigned long long)q * (unsigned long long)(SLAB ? P.key_ncells : g.ncells) + (unsigned long long)cell);
             eta_next[(long long)q * g.nstore + base + rc] = v;
             const double sq = v * v;
             pairs += Sn * sq;
@@ -657,17 +668,17 @@ __device__ __forceinline__ void eta_march_body(const StepParams& P, int n, const
         for (int q = 0; q < NCAP; ++q)
             if (q < n) { ep[q] = ec[q]; ec[q] = en[q]; }
     }
-    if (errkey != ERR_NONE) atomicMin(&st->err_key, errkey);
+    if (errkey != ERR_NONE) atomicMin(SLAB ? err_word(P, st) : &st->err_key, errkey);
 }
 
 // 2 CTAs/SM stated in the bounds: the register count stays <= 128 either way,
 // but the schedule compiled for it measured 15% faster on B200 (0.58 vs 0.69
 // ms at 256^3 with 8 fields, same box); bounds for 3 CTAs/SM spill and lose.
-template <int DIM, bool FAST, int N>
+template <int DIM, bool FAST, int N, bool SLAB = false>
 __global__ void __launch_bounds__(256, 2)
 k_eta_march(const StepParams P, const double* __restrict__ eta, const double* __restrict__ p,
             double* __restrict__ eta_next, double* __restrict__ gb_next, double* __restrict__ s2_next, Status* st) {
-    eta_march_body<DIM, FAST, N>(P, N, eta, p, eta_next, gb_next, s2_next, st, blockIdx.x, blockIdx.y, blockIdx.z);
+    eta_march_body<DIM, FAST, N, SLAB>(P, N, eta, p, eta_next, gb_next, s2_next, st, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 template <int DIM, bool FAST, int N>
@@ -675,8 +686,11 @@ static void launch_eta_march(const StepParams& P, const double* eta, const doubl
                              double* gb_next, double* s2_next, Status* st, cudaStream_t stream) {
     const Grid& g = P.g;
     if (DIM == 3) {
-        const dim3 grid((g.nb + 31) / 32, (g.na + 7) / 8, (g.nx + P.xchunk - 1) / P.xchunk);
-        k_eta_march<3, FAST, N><<<grid, dim3(32, 8), 0, stream>>>(P, eta, p, eta_next, gb_next, s2_next, st);
+        const dim3 grid((g.nb + 31) / 32, (g.na + 7) / 8, (P.x_hi - P.x_lo + P.xchunk - 1) / P.xchunk);
+        if (P.err_slot >= 0)   // an X slab (3D only)
+            k_eta_march<3, FAST, N, true><<<grid, dim3(32, 8), 0, stream>>>(P, eta, p, eta_next, gb_next, s2_next, st);
+        else
+            k_eta_march<3, FAST, N><<<grid, dim3(32, 8), 0, stream>>>(P, eta, p, eta_next, gb_next, s2_next, st);
     } else {
         const dim3 grid((g.nb + 127) / 128, 1, (g.nx + P.xchunk - 1) / P.xchunk);
         k_eta_march<2, FAST, N><<<grid, dim3(128, 1), 0, stream>>>(P, eta, p, eta_next, gb_next, s2_next, st);
@@ -1079,10 +1093,16 @@ static void launch_step3(const StepParams& P, const double* o, const double* cr,
                          const double* s2, double* on, double* crn, double* pn, StepPartial* partials, Status* st,
                          cudaStream_t stream, int* nblocks_out) {
     using T = Tile<3, TA3, TB3>;
-    ensure_smem_attr((const void*)k_step_main<3, TA3, TB3, MINB, FAST>, (int)T::SMEM_BYTES);
     const dim3 grid = step_grid<3, TA3, TB3>(P);
-    k_step_main<3, TA3, TB3, MINB, FAST><<<grid, dim3(TB3, TA3), T::SMEM_BYTES, stream>>>(P, o, cr, p, gb, s2, on, crn,
-                                                                                         pn, partials, st);
+    if (P.err_slot >= 0) {   // an X slab
+        ensure_smem_attr((const void*)k_step_main<3, TA3, TB3, MINB, FAST, true>, (int)T::SMEM_BYTES);
+        k_step_main<3, TA3, TB3, MINB, FAST, true><<<grid, dim3(TB3, TA3), T::SMEM_BYTES, stream>>>(
+            P, o, cr, p, gb, s2, on, crn, pn, partials, st);
+    } else {
+        ensure_smem_attr((const void*)k_step_main<3, TA3, TB3, MINB, FAST>, (int)T::SMEM_BYTES);
+        k_step_main<3, TA3, TB3, MINB, FAST><<<grid, dim3(TB3, TA3), T::SMEM_BYTES, stream>>>(P, o, cr, p, gb, s2, on,
+                                                                                             crn, pn, partials, st);
+    }
     if (nblocks_out) *nblocks_out = (int)(grid.x * grid.y * grid.z);
 }
 
@@ -1120,7 +1140,8 @@ static void launch_eta_form(const StepParams& P, int neta, const double* eta, co
         march = e ? (e[0] == 'm' ? 1 : 0) : -2;
         tma = (e && e[0] == 't') ? 1 : 0;
     }
-    if (tma && launch_eta_tma<FAST>(neta, P, eta, p, eta_next, gb_next, s2_next, st, stream)) return;
+    const bool slab = P.err_slot >= 0;   // X slabs use the march or the per-cell kernel
+    if (tma && !slab && launch_eta_tma<FAST>(neta, P, eta, p, eta_next, gb_next, s2_next, st, stream)) return;
     if (march == 1 || (march == -2 && FAST)) {
         const bool done = g.dim == 3 ? eta_march_dispatch<3, FAST>(neta, P, eta, p, eta_next, gb_next, s2_next, st, stream)
                                      : eta_march_dispatch<2, FAST>(neta, P, eta, p, eta_next, gb_next, s2_next, st, stream);
@@ -1129,14 +1150,14 @@ static void launch_eta_form(const StepParams& P, int neta, const double* eta, co
     if (g.dim == 3) {
         constexpr int TA = 8, TB = 32, S1 = (TA + 2) * (TB + 2);
         const size_t smem = (size_t)3 * neta * S1 * sizeof(double) + S1 * sizeof(int);
-        if (!simple && smem <= 200 * 1024) {
+        if (!simple && !slab && smem <= 200 * 1024) {
             ensure_smem_attr((const void*)k_eta_stream<3, TA, TB, FAST>, 200 * 1024);
             const dim3 grid((g.nb + TB - 1) / TB, (g.na + TA - 1) / TA, (g.nx + P.xchunk - 1) / P.xchunk);
             k_eta_stream<3, TA, TB, FAST><<<grid, dim3(TB, TA), smem, stream>>>(P, neta, eta, p, eta_next, gb_next, s2_next, st);
             return;
         }
         const dim3 block(32, 8);
-        const dim3 grid((g.nb + 31) / 32, (g.na + 7) / 8, g.nx);
+        const dim3 grid((g.nb + 31) / 32, (g.na + 7) / 8, P.x_hi - P.x_lo);
         k_eta_update<3, FAST><<<grid, block, 0, stream>>>(P, neta, eta, s2, p, eta_next, gb_next, s2_next, st);
     } else {
         constexpr int TB = 128, S1 = TB + 2;

@@ -123,6 +123,27 @@ def lib():
     L.nicr_batch_stream.restype = ctypes.c_void_p
     L.nicr_kernel_launches.argtypes = [H]
     L.nicr_kernel_launches.restype = ctypes.c_longlong
+    L.nicr_slabs_create.argtypes = [ctypes.POINTER(NicrConfig), ctypes.c_int, ip, ctypes.POINTER(H)]
+    L.nicr_slabs_destroy.argtypes = [H]
+    L.nicr_slabs_destroy.restype = None
+    L.nicr_slabs_count.argtypes = [H]
+    L.nicr_slabs_info.argtypes = [H, ctypes.c_int, ip, ip, ip, ip]
+    L.nicr_slabs_step.argtypes = [H, ctypes.c_int, ip]
+    L.nicr_slabs_run.argtypes = [H, ctypes.c_int, ip]
+    L.nicr_slabs_nucleate.argtypes = [H, ip]
+    L.nicr_slabs_get_field.argtypes = [H, ctypes.c_int, ctypes.c_int, dp]
+    L.nicr_slabs_set_field.argtypes = [H, ctypes.c_int, ctypes.c_int, dp]
+    L.nicr_slabs_reset_inventory.argtypes = [H]
+    L.nicr_slabs_get_budget.argtypes = [H, ctypes.POINTER(NicrBudget)]
+    L.nicr_slabs_get_diagnostics.argtypes = [H, ctypes.POINTER(NicrDiagnostics)]
+    L.nicr_slabs_steps_done.argtypes = [H]
+    L.nicr_slabs_steps_done.restype = ctypes.c_longlong
+    L.nicr_slabs_kernel_launches.argtypes = [H]
+    L.nicr_slabs_kernel_launches.restype = ctypes.c_longlong
+    L.nicr_slabs_stream.argtypes = [H, ctypes.c_int]
+    L.nicr_slabs_stream.restype = ctypes.c_void_p
+    L.nicr_slabs_last_error.argtypes = [H]
+    L.nicr_slabs_last_error.restype = ctypes.c_char_p
     _lib = L
     return L
 
@@ -435,6 +456,130 @@ class Batch:
         return lib().nicr_batch_stream(self.b) or 0
 
 
+class Slabs:
+    """One 3D domain split along X into slabs (nicr_slabs_*), slab i on GPU
+    devices[i] (several slabs may share a GPU). Fields, budgets and
+    diagnostics are whole-domain, as a Solver's."""
+
+    def __init__(self, cfg: NicrConfig, nslabs: int, devices=None):
+        self.cfg = cfg
+        self.s = ctypes.c_void_p()
+        dev = None
+        if devices is not None:
+            devices = list(devices)
+            if len(devices) != nslabs:
+                raise ValueError("one device per slab")
+            dev = (ctypes.c_int * nslabs)(*devices)
+        rc = lib().nicr_slabs_create(ctypes.byref(cfg), nslabs, dev, ctypes.byref(self.s))
+        if rc != 0:
+            raise NicrError(rc, lib().nicr_slabs_last_error(None).decode())
+        self.shape = (cfg.nx, cfg.ny, cfg.nz)
+        self.n = int(np.prod(self.shape))
+
+    def close(self):
+        if getattr(self, "s", None) and self.s.value:
+            lib().nicr_slabs_destroy(self.s)
+            self.s = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, rc: int):
+        if rc != 0:
+            raise NicrError(rc, self.last_error)
+        return rc
+
+    @property
+    def last_error(self) -> str:
+        return lib().nicr_slabs_last_error(self.s).decode()
+
+    def __len__(self):
+        return lib().nicr_slabs_count(self.s)
+
+    def slab(self, i: int) -> dict:
+        """Domain planes [x0, x1) of slab i, its device and the halo width."""
+        v = [ctypes.c_int(0) for _ in range(4)]
+        self._check(lib().nicr_slabs_info(self.s, i, *[ctypes.byref(q) for q in v]))
+        return {"x0": v[0].value, "x1": v[1].value, "device": v[2].value, "halo": v[3].value}
+
+    def get(self, name: str, index: int = 0, out: np.ndarray | None = None) -> np.ndarray:
+        if name.startswith("eta") and name[3:].isdigit():
+            index, name = int(name[3:]) - 1, "eta"
+        if out is None:
+            out = np.empty(self.n)
+        elif out.dtype != np.float64 or out.size != self.n or not out.flags["C_CONTIGUOUS"]:
+            raise ValueError("out must be a contiguous float64 array with one value per cell")
+        self._check(lib().nicr_slabs_get_field(self.s, FIELD[name], index, _dp(out)))
+        return out.reshape(self.shape)
+
+    def set(self, name: str, arr, index: int = 0):
+        if name.startswith("eta") and name[3:].isdigit():
+            index, name = int(name[3:]) - 1, "eta"
+        a = np.ascontiguousarray(arr, dtype=np.float64).ravel()
+        if a.size != self.n:
+            raise ValueError(f"field has {a.size} values, grid has {self.n}")
+        self._check(lib().nicr_slabs_set_field(self.s, FIELD[name], index, _dp(a)))
+
+    def reset_inventory(self):
+        self._check(lib().nicr_slabs_reset_inventory(self.s))
+
+    def step(self, n: int = 1, check: bool = True):
+        done = ctypes.c_int(0)
+        rc = lib().nicr_slabs_step(self.s, n, ctypes.byref(done))
+        if check:
+            self._check(rc)
+        return rc, done.value
+
+    def run(self, n: int, check: bool = True):
+        done = ctypes.c_int(0)
+        rc = lib().nicr_slabs_run(self.s, n, ctypes.byref(done))
+        if check:
+            self._check(rc)
+        return rc, done.value
+
+    def nucleate(self) -> int:
+        k = ctypes.c_int(0)
+        self._check(lib().nicr_slabs_nucleate(self.s, ctypes.byref(k)))
+        return k.value
+
+    def budget(self) -> dict:
+        b = NicrBudget()
+        self._check(lib().nicr_slabs_get_budget(self.s, ctypes.byref(b)))
+        d = {n: (getattr(b, n)[0], getattr(b, n)[1]) for n in
+             ("nucO", "nucCr", "ckO", "ckCr", "clipO", "clipCr", "bcO", "bcCr", "initialO", "initialCr")}
+        d["nuclei"], d["clipped"] = int(b.nuclei), int(b.clipped)
+        return d
+
+    def diagnostics(self) -> dict:
+        d = NicrDiagnostics()
+        self._check(lib().nicr_slabs_get_diagnostics(self.s, ctypes.byref(d)))
+        out = {n: (getattr(d, n)[0], getattr(d, n)[1]) for n in ("sum_O", "sum_Cr", "sum_phi", "sum_h")}
+        for n in ("min_O", "max_O", "min_Cr", "max_Cr", "min_Ni", "min_phi", "max_phi"):
+            out[n] = getattr(d, n)
+        return out
+
+    @property
+    def steps_done(self) -> int:
+        return int(lib().nicr_slabs_steps_done(self.s))
+
+    @property
+    def kernel_launches(self) -> int:
+        return int(lib().nicr_slabs_kernel_launches(self.s))
+
+    def stream(self, i: int) -> int:
+        """The CUDA stream slab i enqueues on."""
+        return lib().nicr_slabs_stream(self.s, i) or 0
+
+
 def main(dim: int, argv: list[str]) -> int:
     """Runs the solver program (the reference's run()) with argv."""
     args = ["nicr%dd" % dim] + list(argv)
@@ -442,5 +587,5 @@ def main(dim: int, argv: list[str]) -> int:
     return lib().nicr_main(dim, len(args), arr)
 
 
-__all__ = ["Solver", "NicrError", "NicrConfig", "make_config", "default_config", "c_default_config", "parse_args",
+__all__ = ["Solver", "Batch", "Slabs", "NicrError", "NicrConfig", "make_config", "default_config", "c_default_config", "parse_args",
            "config_to_flags", "main", "lib", "library_path", "BC", "CK", "BOUNDS", "NUCLEATION", "FIELD"]
