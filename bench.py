@@ -50,12 +50,21 @@ def grain_diameter_for(n_grains: int, shape) -> float:
     return (6.0 * v / (math.pi * n_grains)) ** (1.0 / 3.0)
 
 
-def workload_config(size: int, neta: int, device: int = 0, seed: int = 2):
+SEEDS = 64   # Voronoi seeds of the workload's tessellation, coloured into the eta fields
+
+
+def workload_config(size: int, neta: int, device: int = 0, seed: int = 2, coloured: bool = True):
+    """The 256^3 evolving-grain workload: a 64-seed Voronoi tessellation (seed
+    2) coloured into neta eta fields with 2-cell tanh boundaries (eta_colours).
+    coloured=False gives the reference's own form of the same per-cell work,
+    neta seeds with one eta each, for the reference program, which cannot
+    colour grains."""
     from nicr import make_config
     shape = (size, size, size)
+    kw = dict(grain_diameter_grid=grain_diameter_for(SEEDS, shape), eta_colours=neta) if coloured else \
+        dict(grain_diameter_grid=grain_diameter_for(neta, shape))
     return make_config(3, nx=size, ny=size, nz=size, grains=1, grain_evolution=1, random_seed=seed,
-                       grain_diameter_grid=grain_diameter_for(neta, shape), bc="concentration", ck="legacy",
-                       bounds="legacy", nucleation="ksp", device=device)
+                       bc="concentration", ck="legacy", bounds="legacy", nucleation="ksp", device=device, **kw)
 
 
 def algorithmic_bytes(kernel: str, neta: int, fast: bool) -> int:
@@ -157,7 +166,7 @@ def time_reference(size: int, neta: int, steps: int, ranks: int, budget_s: float
     exe = reference_exe(threads=ranks > 1)
     if exe is None:
         return None
-    cfg = workload_config(size, neta)
+    cfg = workload_config(size, neta, coloured=False)
     flags = config_to_flags(cfg)
     base = [str(exe)] + ([str(ranks)] if ranks > 1 else []) + flags + ["--"]
     with tempfile.TemporaryDirectory() as td:
@@ -187,8 +196,10 @@ def reference_arm(args, rank: int, world: int):
             "ms_per_step": 1e3 * sec / n, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic (reference initial state of the same workload)",
             "impl": "reference",
-            "config": {"workload": f"3D {args.size}^3, {args.neta} evolving eta, bc=concentration, Ksp on, "
-                                   f"legacy Ck, bounds=legacy", "cells": args.size ** 3},
+            "config": {"workload": f"3D {args.size}^3, {args.neta} evolving eta ({args.neta} Voronoi seeds, one eta "
+                                   f"each: the reference cannot colour a 64-seed tessellation into {args.neta} eta; "
+                                   f"the same fields and per-cell work), bc=concentration, Ksp on, legacy Ck, "
+                                   f"bounds=legacy", "cells": args.size ** 3},
             "cpu_baseline": {"value": val, "unit": UNIT, "cores": ranks, "kind": "reference",
                              "sample": f"{n} timed steps of the full {args.size}^3 domain after 1 warm-up step, "
                                        f"{ranks} thread-emulated MPI ranks (reference tests/mpi_threads.h)"},
@@ -626,8 +637,9 @@ def main():
         "error_vs_plain": {"linf_rel_max": err, "fields": "o, cr, phi, eta_1..N",
                            "steps": args.warmup + args.steps, "bound": 1e-4, "per_field": per_field,
                            "oxide_front_max_cells": front},
-        "data": "synthetic (seeded Cr noise, Voronoi seed 2); inputs ~3 GB > L2, no flush needed",
-        "config": {"workload": f"3D {args.size}^3, {args.neta} evolving eta (Voronoi seed 2), Cr 0.25+-0.01, "
+        "data": "synthetic (seeded Cr noise, 64-seed Voronoi tessellation of seed 2); inputs ~3 GB > L2, no flush needed",
+        "config": {"workload": f"3D {args.size}^3, {args.neta} evolving eta coloured from a {SEEDS}-seed Voronoi "
+                               f"tessellation (seed 2) with 2-cell tanh boundaries, Cr 0.25+-0.01, "
                                f"bc=concentration, Ksp on, legacy Ck, bounds=legacy",
                    "cells": n, "parallelism": f"independent domains x{world}", "l2": "inputs larger than L2"},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",

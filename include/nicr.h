@@ -80,7 +80,13 @@ typedef struct nicr_config {
     int device;                   /* CUDA device ordinal                        */
     int checkpoint_every;         /* programs: write out/checkpoint.bin every N
                                      steps (0: never); no reference counterpart */
-    int reserved[5];
+    int eta_colours;              /* 3D evolving grains: 0 = one eta per Voronoi
+                                     grain (the reference, 3S:469-494); K > 0 =
+                                     the grains coloured into K eta fields, no
+                                     two face-adjacent grains sharing one where
+                                     K colours allow, with tanh profiles across
+                                     the boundaries; no reference counterpart */
+    int reserved[4];
 } nicr_config;
 
 /* Fills the reference defaults for dim 2 or 3 (Config{} at 2D:39 / 3S:43). */

@@ -78,7 +78,7 @@ std::string config_mismatch(const nicr_config& a, const nicr_config& b) {
     NICR_SAME(nucleation_period) NICR_SAME(mu_res) NICR_SAME(surface_c_ref) NICR_SAME(bc) NICR_SAME(ck)
     NICR_SAME(bounds) NICR_SAME(nucleation) NICR_SAME(grains) NICR_SAME(oxygen_diffusion) NICR_SAME(grain_evolution)
     NICR_SAME(frozen_eta_cache) NICR_SAME(eta_W) NICR_SAME(eta_kappa) NICR_SAME(eta_L) NICR_SAME(eta_oxide_penalty)
-    NICR_SAME(ksp) NICR_SAME(bulk_cr) NICR_SAME(layer_o)
+    NICR_SAME(ksp) NICR_SAME(bulk_cr) NICR_SAME(layer_o) NICR_SAME(eta_colours)
 #undef NICR_SAME
     return "";
 }

@@ -49,6 +49,8 @@ std::string help_text(int dim) {
          "Extensions (defaults reproduce the fixed reference constants): --ksp v --bulk-cr v --layer-o v\n"
          "--precision fp64|fp64-fast (fp64: bit-identical to the reference; fp64-fast: reciprocal divisions)\n"
          "--checkpoint-every N (write <out>/checkpoint.bin every N steps) --restart FILE (continue from a checkpoint)\n";
+    if (dim == 3)
+        s += "--eta-colours K (evolving grains: colour the Voronoi grains into K eta fields with tanh boundaries)\n";
     return s;
 }
 
@@ -124,6 +126,12 @@ void parse_into(nicr_config& c, int dim, int argc, const char* const* argv, std:
             if (used != v.size() || n < 0 || n > INT_MAX)
                 throw std::runtime_error("--checkpoint-every expects a nonnegative integer.");
             c.checkpoint_every = (int)n;
+        }
+        else if (a == "--eta-colours" && dim == 3) {
+            size_t used = 0;
+            const long long n = std::stoll(v, &used);
+            if (used != v.size() || n < 0 || n > 4096) throw std::runtime_error("--eta-colours expects an integer in [0, 4096].");
+            c.eta_colours = (int)n;
         }
         else if (a == "--precision") {
             if (v == "fp64") c.precision = NICR_FP64;

@@ -57,7 +57,7 @@ __device__ __forceinline__ double competitor_distance(const double* s, int g, in
 }
 
 __global__ void k_voronoi3(const InitParams I, const double* __restrict__ seeds, double* grain, double* dbout,
-                           int* volumes) {
+                           int* volumes, int* competitor) {
     extern __shared__ double ss[];
     for (int q = threadIdx.x; q < 3 * I.ng; q += blockDim.x) ss[q] = seeds[q];
     __syncthreads();
@@ -76,11 +76,17 @@ __global__ void k_voronoi3(const InitParams I, const double* __restrict__ seeds,
             if (rr < rbest) { rbest = rr; owner = s; oY = y + yy; oZ = z + zz; }
         }
         double db = CUDART_INF;
+        int near = -1;   // the first competitor attaining db
         for (int s = 0; s < I.ng; ++s)
-            if (s != owner) db = smin(db, competitor_distance(ss, s, owner, x, y, z, oY, oZ, rbest, ny, nz));
+            if (s != owner) {
+                const double d = competitor_distance(ss, s, owner, x, y, z, oY, oZ, rbest, ny, nz);
+                if (d < db) near = s;
+                db = smin(db, d);
+            }
         const long long idx = (long long)xi * g.plane + (long long)row * g.pb + col;
         grain[idx] = owner + 1;
         dbout[idx] = db;
+        if (competitor) competitor[idx] = near;
         if (xi >= I.x_lo && xi < I.x_hi) atomicAdd(volumes + owner, 1);
     }
 }
@@ -104,6 +110,28 @@ __global__ void k_eta_dist3(const InitParams I, const double* __restrict__ seeds
         for (int s = 0; s < I.ng; ++s)
             eta[(long long)s * g.nstore + idx] =
                 s == owner ? -1. : competitor_distance(ss, s, owner, x, y, z, oy, oz, rbest, ny, nz);
+    }
+}
+
+// Face adjacency of the Voronoi grains over the stored cells: adj[a*ng+b] = 1
+// when a cell of grain a and its +X (stored planes only), +Y or +Z neighbour
+// (periodic) belongs to grain b != a.
+__global__ void k_grain_adjacency(const InitParams I, const double* __restrict__ grain, unsigned char* adj) {
+    const Grid& g = I.g;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < g.ncells; c += (long long)gridDim.x * blockDim.x) {
+        int xi, row, col;
+        decode(g, c, xi, row, col);
+        const long long idx = (long long)xi * g.plane + (long long)row * g.pb + col;
+        const int a = (int)grain[idx] - 1;
+        int nb[3];
+        nb[0] = xi + 1 < g.nx ? (int)grain[idx + g.plane] - 1 : a;
+        nb[1] = (int)grain[(long long)xi * g.plane + (long long)(row + 1 == g.na ? 0 : row + 1) * g.pb + col] - 1;
+        nb[2] = (int)grain[(long long)xi * g.plane + (long long)row * g.pb + (col + 1 == g.nb ? 0 : col + 1)] - 1;
+        for (int q = 0; q < 3; ++q)
+            if (nb[q] != a) {
+                adj[(long long)a * I.ng + nb[q]] = 1;
+                adj[(long long)nb[q] * I.ng + a] = 1;
+            }
     }
 }
 
@@ -411,10 +439,13 @@ void launch_init_fields(const InitParams& I, double* o, double* cr, double* p, c
     k_init_fields<<<grid_for(I.g.ncells, 256, 148 * 16), 256, 0, stream>>>(I, o, cr, p);
 }
 void launch_voronoi3(const InitParams& I, const double* seeds, double* grain, double* db, int* volumes,
-                     cudaStream_t stream) {
+                     int* competitor, cudaStream_t stream) {
     const size_t sm = (size_t)3 * I.ng * sizeof(double);
     if (sm > 48 * 1024) cudaFuncSetAttribute(k_voronoi3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    k_voronoi3<<<grid_for(I.g.ncells, 128, 148 * 32), 128, sm, stream>>>(I, seeds, grain, db, volumes);
+    k_voronoi3<<<grid_for(I.g.ncells, 128, 148 * 32), 128, sm, stream>>>(I, seeds, grain, db, volumes, competitor);
+}
+void launch_grain_adjacency(const InitParams& I, const double* grain, unsigned char* adj, cudaStream_t stream) {
+    k_grain_adjacency<<<grid_for(I.g.ncells, 256, 148 * 16), 256, 0, stream>>>(I, grain, adj);
 }
 void launch_eta_dist3(const InitParams& I, const double* seeds, const double* grain, double* eta, cudaStream_t stream) {
     const size_t sm = (size_t)3 * I.ng * sizeof(double);

@@ -219,9 +219,12 @@ struct InitParams {
 };
 void launch_init_fields(const InitParams& I, double* o, double* cr, double* p, cudaStream_t stream);
 // 3D Voronoi labels (first nearest seed under minimum image) and the distance
-// to the nearest bisector (3S:450-466). seeds: x,y,z per seed.
+// to the nearest bisector (3S:450-466). seeds: x,y,z per seed. competitor
+// (may be null) receives the 0-based seed of the nearest bisector (-1: none).
 void launch_voronoi3(const InitParams& I, const double* seeds, double* grain, double* db,
-                     int* volumes, cudaStream_t stream);
+                     int* volumes, int* competitor, cudaStream_t stream);
+// Face adjacency of the grains (ng x ng bytes, set to 1 for adjacent pairs)
+void launch_grain_adjacency(const InitParams& I, const double* grain, unsigned char* adj, cudaStream_t stream);
 // 3D eta initial weights: per competitor g, the bisector distance (3S:469-494);
 // the owner's slot receives -1. Output layout eta[g*nstore + idx].
 void launch_eta_dist3(const InitParams& I, const double* seeds, const double* grain, double* eta,

@@ -164,10 +164,22 @@ Model::Model(const nicr_config& cfg, const SlabSpec* slab) : c(cfg), dim(cfg.dim
         reset_inventory();
         if (c.nucleation == NICR_NUC_CENTER) init_center_seed();
         if (has_eta) {
-            if ((int)(seeds.size() / dim) > c.max_eta_fields)
+            const int nfields = c.eta_colours > 0 ? c.eta_colours : (int)(seeds.size() / dim);
+            if (nfields > c.max_eta_fields)
                 throw Error(NICR_ERR_INVALID_ARG, dim == 3 ? "Too many eta fields; check --max-eta-fields and memory."
                                                            : "Too many eta fields. Increase --max-eta-fields only after checking memory, or use --grain-evolution off.");
-            init_eta();
+            if (c.eta_colours > 0) {
+                if (dim != 3) throw Error(NICR_ERR_INVALID_ARG, "--eta-colours is 3D only");
+                grain_adjacency();
+                alloc_eta(c.eta_colours);
+                // a slab sees part of the adjacency: its group colours the union
+                if (!is_slab) {
+                    seed_colour = colour_grains(adjacency, (int)(seeds.size() / 3), c.eta_colours);
+                    init_eta_coloured();
+                }
+            } else {
+                init_eta();
+            }
             if (dim == 3) grain_retained = false;
         }
         if (c.nucleation == NICR_NUC_KSP) setup_ksp();
@@ -245,7 +257,7 @@ void Model::voronoi() {
         if (!std::isfinite(ng_real) || ng_real > volume + .5) throw Error(NICR_ERR_INVALID_ARG, "Too many Voronoi sites for this grid.");
         ng = std::max(1, int(std::llround(ng_real)));
         if (ng > volume) throw Error(NICR_ERR_INVALID_ARG, "Too many Voronoi sites for this grid.");
-        if (has_eta && ng > c.max_eta_fields)
+        if (has_eta && c.eta_colours <= 0 && ng > c.max_eta_fields)
             throw Error(NICR_ERR_INVALID_ARG, "3D grain count exceeds --max-eta-fields; increase grain diameter or check memory before increasing the limit.");
     } else {
         const double domain_area = double(c.nx) * c.ny;
@@ -307,14 +319,25 @@ void Model::voronoi() {
         double* d_seeds = dalloc(seeds.size());
         int* d_vol = dalloc_t<int>(ng);
         double* d_db = gb_[0];
+        const bool coloured = has_eta && c.eta_colours > 0;
+        int* d_comp = coloured ? dalloc_t<int>(ns) : nullptr;
         check_cuda(cudaMemcpyAsync(d_seeds, seeds.data(), seeds.size() * 8, cudaMemcpyHostToDevice, stream), "H2D");
         check_cuda(cudaMemsetAsync(d_vol, 0, ng * sizeof(int), stream), "memset");
         InitParams I = init_params();
         I.ng = ng; I.nxd = c.nx; I.nyd = c.ny; I.nzd = c.nz;
-        launch_voronoi3(I, d_seeds, grain, d_db, d_vol, stream);
+        launch_voronoi3(I, d_seeds, grain, d_db, d_vol, d_comp, stream);
         std::vector<int> vol(ng);
         check_cuda(cudaMemcpyAsync(vol.data(), d_vol, ng * sizeof(int), cudaMemcpyDeviceToHost, stream), "D2H");
         copy_out(d_db, gb_h.data());
+        if (coloured) {
+            init_db = gb_h;
+            init_comp.resize((size_t)g.ncells);
+            check_cuda(cudaMemcpy2DAsync(init_comp.data(), (size_t)g.nb * sizeof(int), d_comp, (size_t)g.pb * sizeof(int),
+                                         (size_t)g.nb * sizeof(int), (size_t)g.nx * g.na, cudaMemcpyDeviceToHost, stream), "D2H");
+            sync();
+            cudaFree(d_comp);
+            dev_bytes -= ns * sizeof(int);
+        }
         for (int q = 0; q < ng; ++q) volumes[q] = vol[q];
         cudaFree(d_seeds);
         cudaFree(d_vol);
@@ -434,6 +457,92 @@ void Model::init_center_seed() {
     if (x_off == 0) b.nuclei += 1;   // counted once, by the slab holding domain plane 0
     check_cuda(cudaMemcpyAsync(bud, &b, sizeof b, cudaMemcpyHostToDevice, stream), "H2D");
     sync();
+}
+
+void Model::alloc_eta(int n) {
+    neta = n;
+    const size_t ns = (size_t)g.nstore;
+    eta_[0] = dalloc(ns * n);
+    check_cuda(cudaMemsetAsync(eta_[0], 0, ns * n * 8, stream), "memset");
+    if (advance_eta) eta_[1] = dalloc(ns * n);
+    eta_dirty = true;
+}
+
+void Model::grain_adjacency() {
+    const int ng = (int)(seeds.size() / 3);
+    unsigned char* d_adj = dalloc_t<unsigned char>((size_t)ng * ng);
+    check_cuda(cudaMemsetAsync(d_adj, 0, (size_t)ng * ng, stream), "memset");
+    InitParams I = init_params();
+    I.ng = ng;
+    launch_grain_adjacency(I, grain, d_adj, stream);
+    adjacency.assign((size_t)ng * ng, 0);
+    check_cuda(cudaMemcpyAsync(adjacency.data(), d_adj, adjacency.size(), cudaMemcpyDeviceToHost, stream), "D2H");
+    sync();
+    cudaFree(d_adj);
+    dev_bytes -= (size_t)ng * ng;
+}
+
+std::vector<int> colour_grains(const std::vector<unsigned char>& adj, int ng, int k) {
+    std::vector<int> colour((size_t)ng, -1), degree((size_t)ng, 0);
+    for (int a = 0; a < ng; ++a)
+        for (int b = 0; b < ng; ++b) degree[(size_t)a] += adj[(size_t)a * ng + b] != 0;
+    std::vector<int> count((size_t)k);
+    for (int step = 0; step < ng; ++step) {
+        int v = -1, vsat = -1;
+        for (int a = 0; a < ng; ++a) {
+            if (colour[(size_t)a] >= 0) continue;
+            std::vector<char> seen((size_t)k, 0);
+            int sat = 0;
+            for (int b = 0; b < ng; ++b) {
+                const int cb = colour[(size_t)b];
+                if (adj[(size_t)a * ng + b] && cb >= 0 && !seen[(size_t)cb]) { seen[(size_t)cb] = 1; ++sat; }
+            }
+            if (v < 0 || sat > vsat || (sat == vsat && degree[(size_t)a] > degree[(size_t)v])) { v = a; vsat = sat; }
+        }
+        std::fill(count.begin(), count.end(), 0);
+        for (int b = 0; b < ng; ++b)
+            if (adj[(size_t)v * ng + b] && colour[(size_t)b] >= 0) ++count[(size_t)colour[(size_t)b]];
+        int best = 0;
+        for (int q = 1; q < k; ++q)
+            if (count[(size_t)q] < count[(size_t)best]) best = q;
+        colour[(size_t)v] = best;   // the lowest free colour, else the least used among neighbours
+    }
+    return colour;
+}
+
+// Coloured eta (extension, eta_colours = K): every cell of grain a, whose
+// nearest Voronoi bisector (distance d cells) faces grain b, gets
+// eta[colour(a)] = (1 - h(phi)) (1 + tanh d) / 2 and eta[colour(b)] =
+// (1 - h(phi)) (1 - tanh d) / 2: the two values meet at 1/2 on the bisector
+// and the boundary is about 2 cells wide (10-90%: 2.2 cells). When a and b
+// share a colour (or a is the only grain), eta[colour(a)] = 1 - h(phi).
+// Every other field is 0. tanh is the host C library's.
+void Model::init_eta_coloured() {
+    const long long n = g.ncells;
+    std::vector<double> ph((size_t)n), grain_h((size_t)n);
+    copy_out(p_[cur], ph.data());
+    copy_out(grain, grain_h.data());
+    std::vector<double> eta_h((size_t)n * neta, 0.);
+    parallel_for(n, [&](long long b, long long e) {
+        for (long long q = b; q < e; ++q) {
+            const int owner = int(grain_h[(size_t)q]) - 1, comp = init_comp[(size_t)q];
+            const int ca = seed_colour[(size_t)owner];
+            const double metal = 1. - h(ph[(size_t)q]);
+            if (comp < 0 || seed_colour[(size_t)comp] == ca) {
+                eta_h[(size_t)ca * n + q] = metal;
+                continue;
+            }
+            const double t = std::tanh(init_db[(size_t)q]);
+            eta_h[(size_t)ca * n + q] = metal * (0.5 * (1. + t));
+            eta_h[(size_t)seed_colour[(size_t)comp] * n + q] = metal * (0.5 * (1. - t));
+        }
+    });
+    for (int q = 0; q < neta; ++q) copy_in(eta_[0] + (size_t)q * g.nstore, eta_h.data() + (size_t)q * n);
+    init_db.clear();
+    init_db.shrink_to_fit();
+    init_comp.clear();
+    init_comp.shrink_to_fit();
+    eta_dirty = true;
 }
 
 // initialize_eta (3S:469-494, 2D:293-327): weights exp(-d/ell) normalised,

@@ -34,6 +34,13 @@ struct SlabSpec {
     int x0 = 0, x1 = 0, halo = 0;
 };
 class SlabGroup;
+
+// Colours ng grains with k colours from their face adjacency (adj: ng x ng
+// bytes): DSatur order (most distinct neighbour colours, then most
+// neighbours, then lowest index), each grain taking the lowest colour no
+// coloured neighbour has, or when all k are taken the colour fewest coloured
+// neighbours have (lowest first). Deterministic; returns one colour per grain.
+std::vector<int> colour_grains(const std::vector<unsigned char>& adj, int ng, int k);
 int run_self_test(int dim);   // --self-test (nicr_selftest.cpp)
 
 class Model {
@@ -235,6 +242,16 @@ private:
     void voronoi2d_host(std::vector<double>& grain_h, std::vector<double>& gb_h);
     void init_center_seed();
     void init_eta();
+    // eta_colours > 0: the grains' face adjacency over the stored cells, the
+    // colour of each grain, and the eta fields from the colours (kept from
+    // voronoi(): the nearest-bisector distance and competitor of every cell)
+    void grain_adjacency();
+    void alloc_eta(int n);
+    void init_eta_coloured();
+    std::vector<unsigned char> adjacency;
+    std::vector<int> seed_colour;
+    std::vector<double> init_db;
+    std::vector<int> init_comp;
     void setup_ksp();
     void enqueue_step();
     void reset_status();

@@ -593,6 +593,8 @@ void metadata(Model& m, const std::string& out) {
           << "\neta_mask_integrated_width_m=" << 8. * ec.ell / 3. << "\neta_transport_scale=" << ec.scale
           << "\neta_planar_GB_energy_model_units=" << std::sqrt(2. * ec.K * c.eta_W) / 3.
           << "\neta_planar_geometric_mobility_model_units=" << 3. * c.eta_L * ec.ell << "\n";
+        if (c.eta_colours > 0)   // extension: grains coloured into eta fields
+            f << "eta_init=coloured_voronoi_tanh_boundaries\neta_colours=" << c.eta_colours << "\n";
     }
     if (c.nucleation == NICR_NUC_CENTER)
         f << "initial_oxide_center_x_m=" << 0.5 * c.nx * c.dx << "\ninitial_oxide_center_y_m=" << 0.5 * c.ny * c.dy

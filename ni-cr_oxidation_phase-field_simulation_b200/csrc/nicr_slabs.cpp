@@ -139,6 +139,20 @@ SlabGroup::SlabGroup(const nicr_config& cfg, int n, const int* devices) : c(cfg)
             q.halo = halo;
             m.push_back(std::make_unique<Model>(cs, &q));
         }
+        if (m[0]->has_eta && c.eta_colours > 0) {
+            // every face between two planes lies in some slab's stored planes:
+            // the union of the slabs' adjacencies is the domain's
+            std::vector<unsigned char> adj = m[0]->adjacency;
+            for (auto& q : m)
+                for (size_t i = 0; i < adj.size(); ++i) adj[i] = adj[i] | q->adjacency[i];
+            const std::vector<int> colours = colour_grains(adj, (int)(m[0]->seeds.size() / 3), c.eta_colours);
+            for (int s = 0; s < n; ++s) {
+                on(s);
+                m[(size_t)s]->seed_colour = colours;
+                m[(size_t)s]->init_eta_coloured();
+                m[(size_t)s]->eta_mask_now();
+            }
+        }
         if (c.nucleation == NICR_NUC_CENTER) {
             long long cells = 0;
             for (auto& q : m) cells += q->center_seed_cells;

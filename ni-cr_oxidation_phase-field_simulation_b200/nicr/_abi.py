@@ -55,7 +55,8 @@ class NicrConfig(ctypes.Structure):
         ("precision", ctypes.c_int),
         ("device", ctypes.c_int),
         ("checkpoint_every", ctypes.c_int),
-        ("reserved", ctypes.c_int * 5),
+        ("eta_colours", ctypes.c_int),
+        ("reserved", ctypes.c_int * 4),
     ]
 
 
