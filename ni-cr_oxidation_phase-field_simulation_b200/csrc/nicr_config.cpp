@@ -50,7 +50,8 @@ std::string help_text(int dim) {
          "--precision fp64|fp64-fast (fp64: bit-identical to the reference; fp64-fast: reciprocal divisions)\n"
          "--checkpoint-every N (write <out>/checkpoint.bin every N steps) --restart FILE (continue from a checkpoint)\n";
     if (dim == 3)
-        s += "--eta-colours K (evolving grains: colour the Voronoi grains into K eta fields with tanh boundaries)\n";
+        s += "--eta-colours K (evolving grains: colour the Voronoi grains into K eta fields with tanh boundaries)\n"
+             "--slabs N [--slab-devices a,b,...] (the domain split along X over N slabs/GPUs; VTI output only)\n";
     return s;
 }
 

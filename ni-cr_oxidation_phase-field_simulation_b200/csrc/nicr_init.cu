@@ -340,7 +340,7 @@ __global__ void k_grain_scalar(const GrainParams G, const double* __restrict__ e
         for (int q = 0; q < G.neta; ++q) {
             const double* e = eta + (long long)q * g.nstore;
             const double ec = e[idx];
-            if (xi < g.nx - 1) { const double t = (e[ixp] - ec) / G.dx; density += .5 * G.K * (t * t); }
+            if (xi < g.nx - 1 || G.x_above) { const double t = (e[ixp] - ec) / G.dx; density += .5 * G.K * (t * t); }
             if (G.dim == 3) {
                 { const double t = (e[iap] - ec) / G.da; density += .5 * G.K * (t * t); }
                 { const double t = (e[ibp] - ec) / G.db; density += .5 * G.K * (t * t); }

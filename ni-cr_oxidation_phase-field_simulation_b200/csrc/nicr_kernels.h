@@ -251,6 +251,8 @@ struct GrainParams {
     int dim, neta;
     double dx, da, db, K, W, A;
     const double* pairs;   // 2D: eta_pairs of the last mask (2D:337); unused in 3D
+    int x_above;           // the plane after g's last one is stored and in the domain (an X slab
+                           // below another): the last plane keeps its +X gradient term
 };
 struct GrainOut {
     double lo, hi, slo, shi, gbmax;

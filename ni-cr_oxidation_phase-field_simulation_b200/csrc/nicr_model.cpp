@@ -1206,12 +1206,18 @@ void Model::grain_stats(nicr_grain_stats* out, long long* cells, double* amount)
         g_amount = dalloc((size_t)neta * 2);
         g_cells = dalloc_t<long long>((size_t)neta);
     }
+    // the own planes (a whole domain: all); eta fields keep their stored stride
     GrainParams G{};
-    G.g = g; G.dim = dim; G.neta = neta;
+    G.g = own_grid();
+    G.g.nstore = g.nstore;
+    G.dim = dim; G.neta = neta;
     G.dx = c.dx; G.da = c.dy; G.db = dim == 3 ? c.dz : c.dy;
     G.K = ec.K; G.W = c.eta_W; G.A = ec.A;
     G.pairs = pairs;
-    launch_grain_stats(G, eta_[ecur], s2_[gcur], p_[cur], gb_[gcur], gw, g_out, g_amount, g_cells, stream);
+    G.x_above = x_off + sp.x_hi < c.nx ? 1 : 0;
+    const long long off = own_offset();
+    launch_grain_stats(G, eta_[ecur] + off, s2_[gcur] + off, p_[cur] + off, gb_[gcur] + off, gw, g_out, g_amount,
+                       g_cells, stream);
     GrainOut r;
     check_cuda(cudaMemcpyAsync(&r, g_out, sizeof r, cudaMemcpyDeviceToHost, stream), "D2H");
     if (cells) check_cuda(cudaMemcpyAsync(cells, g_cells, (size_t)neta * sizeof(long long), cudaMemcpyDeviceToHost, stream), "D2H");

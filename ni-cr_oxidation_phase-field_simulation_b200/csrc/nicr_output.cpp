@@ -29,6 +29,7 @@
 
 #include "../../include/nicr.h"
 #include "nicr_model.h"
+#include "nicr_slabs.h"
 
 
 namespace fs = std::filesystem;
@@ -416,25 +417,51 @@ void write_visualization(Model& m, const std::string& stem, bool async = false) 
 }
 
 // ------------------------------------------------------------------ CSV rows
-std::string log_row(Model& m, int n) {
-    nicr_diagnostics d;
-    m.diagnostics(&d);
-    nicr_budget b;
-    m.budget(&b);
-    const auto& c = m.c;
+// One diagnostics.csv row from the diagnostics and budget values (3S:963-977)
+std::string log_row(const nicr_config& c, int dim, const nicr_diagnostics& d, const nicr_budget& b, int n) {
     const long double so = ld(d.sum_O), sc = ld(d.sum_Cr), po = ld(d.sum_phi), sumH = ld(d.sum_h);
     const long double ro = so - ld(b.initialO) - ld(b.bcO) - ld(b.nucO) - ld(b.ckO) - ld(b.clipO);
     const long double rc = sc - ld(b.initialCr) - ld(b.bcCr) - ld(b.nucCr) - ld(b.ckCr) - ld(b.clipCr);
-    const int cells = m.dim == 3 ? c.nx * c.ny * c.nz : c.nx * c.ny;
+    const int cells = dim == 3 ? c.nx * c.ny * c.nz : c.nx * c.ny;
     std::ostringstream f;
     f << std::setprecision(17) << n << "," << n * c.dt << "," << so << "," << sc << "," << po / cells << ","
       << ld(b.bcO) << "," << ld(b.nucO) << "," << ld(b.nucCr) << "," << ld(b.ckO) << "," << ld(b.ckCr) << ","
       << ld(b.clipO) << "," << ld(b.clipCr) << "," << ro << "," << rc << "," << b.nuclei << "," << b.clipped << ","
       << d.min_O << "," << d.max_O << "," << d.min_Cr << "," << d.max_Cr << "," << d.min_Ni << "," << d.min_phi << ","
       << d.max_phi;
-    if (m.dim == 3) f << "," << sumH / cells << "," << sumH * c.dx * c.dy * c.dz;
+    if (dim == 3) f << "," << sumH / cells << "," << sumH * c.dx * c.dy * c.dz;
     f << "\n";
     return f.str();
+}
+
+std::string log_row(Model& m, int n) {
+    nicr_diagnostics d;
+    m.diagnostics(&d);
+    nicr_budget b;
+    m.budget(&b);
+    return log_row(m.c, m.dim, d, b, n);
+}
+
+// grain_diagnostics.csv and grain_history.csv rows from the grain statistics
+// (Model::grain_log, 3S:566-590)
+void grain_rows(const nicr_config& c, int dim, int neta, const nicr_grain_stats& s, const std::vector<long long>& cells,
+                const std::vector<double>& amount, int n, std::string& diag, std::string& history) {
+    const int ncell = dim == 3 ? c.nx * c.ny * c.nz : c.nx * c.ny;
+    std::ostringstream f, h;
+    f << std::setprecision(17) << n << "," << n * c.dt << "," << s.min_eta << "," << s.max_eta << "," << s.min_s2 << ","
+      << s.max_s2 << "," << ld(s.sum_s2) / ncell << "," << s.alive << "," << s.unassigned << ",";
+    if (dim == 3) f << ld(s.mask) * c.dx * c.dy * c.dz;
+    else f << ld(s.mask) * c.dx * c.dy;
+    f << "," << s.gb_max << "," << ld(s.energy) << "\n";
+    for (int g = 0; g < neta; ++g) {
+        const long double a = (long double)amount[2 * g] + (long double)amount[2 * g + 1];
+        h << std::setprecision(17) << n << "," << n * c.dt << "," << g + 1 << "," << cells[(size_t)g] << "," << a << ",";
+        if (dim == 3) h << a * c.dx * c.dy * c.dz;
+        else h << a * c.dx * c.dy;
+        h << "\n";
+    }
+    diag = f.str();
+    history = h.str();
 }
 
 void grain_rows(Model& m, int n, std::string& diag, std::string& history) {
@@ -445,33 +472,51 @@ void grain_rows(Model& m, int n, std::string& diag, std::string& history) {
     std::vector<long long> cells((size_t)m.neta);
     std::vector<double> amount((size_t)m.neta * 2);
     m.grain_stats(&s, cells.data(), amount.data());
-    const auto& c = m.c;
-    const int ncell = m.dim == 3 ? c.nx * c.ny * c.nz : c.nx * c.ny;
-    const long double vol = m.dim == 3 ? (long double)1 : 1;
-    (void)vol;
-    std::ostringstream f, h;
-    f << std::setprecision(17) << n << "," << n * c.dt << "," << s.min_eta << "," << s.max_eta << "," << s.min_s2 << ","
-      << s.max_s2 << "," << ld(s.sum_s2) / ncell << "," << s.alive << "," << s.unassigned << ",";
-    if (m.dim == 3) f << ld(s.mask) * c.dx * c.dy * c.dz;
-    else f << ld(s.mask) * c.dx * c.dy;
-    f << "," << s.gb_max << "," << ld(s.energy) << "\n";
-    for (int g = 0; g < m.neta; ++g) {
-        const long double a = (long double)amount[2 * g] + (long double)amount[2 * g + 1];
-        h << std::setprecision(17) << n << "," << n * c.dt << "," << g + 1 << "," << cells[(size_t)g] << "," << a << ",";
-        if (m.dim == 3) h << a * c.dx * c.dy * c.dz;
-        else h << a * c.dx * c.dy;
-        h << "\n";
-    }
-    diag = f.str();
-    history = h.str();
+    grain_rows(m.c, m.dim, m.neta, s, cells, amount, n, diag, history);
 }
 
 // ------------------------------------------------------------------ metadata
-void metadata(Model& m, const std::string& out) {
+// What parameters.txt and grains.csv need of a domain (a Model, or a slab
+// group's totals).
+struct MetaView {
+    nicr_config c;
+    nicr::EtaCoef ec;
+    int dim = 3;
+    bool has_eta = false;
+    int neta = 0;
+    int center_seed_cells = 0;
+    std::vector<double> seeds;
+    std::vector<long long> volumes;
+    size_t bytes = 0;
+    std::string backend = "execution_backend=cuda_sm100a_single_gpu\n";
+    size_t device_bytes() const { return bytes; }
+};
+
+MetaView meta_of(const Model& m) {
+    MetaView v;
+    v.c = m.c; v.ec = m.ec; v.dim = m.dim; v.has_eta = m.has_eta; v.neta = m.neta;
+    v.center_seed_cells = m.center_seed_cells; v.seeds = m.seeds; v.volumes = m.volumes; v.bytes = m.device_bytes();
+    return v;
+}
+
+MetaView meta_of(const nicr::SlabGroup& g) {
+    MetaView v = meta_of(*g.m[0]);
+    v.center_seed_cells = 0;
+    std::fill(v.volumes.begin(), v.volumes.end(), 0);
+    for (auto& q : g.m) {
+        v.center_seed_cells += q->center_seed_cells;
+        for (size_t k = 0; k < v.volumes.size(); ++k) v.volumes[k] += q->volumes[k];
+    }
+    v.bytes = g.device_bytes();
+    v.backend = "execution_backend=cuda_sm100a_x_slabs_" + std::to_string(g.m.size()) + "\n";
+    return v;
+}
+
+void metadata(const MetaView& m, const std::string& out) {
     const auto& c = m.c;
     const nicr::EtaCoef ec = m.ec;
     const double pi = nicr::PI;
-    const std::string backend = "execution_backend=cuda_sm100a_single_gpu\n";
+    const std::string& backend = m.backend;
     std::ofstream f(out + "/parameters.txt");
     auto onoff = [](bool b) { return b ? "on" : "off"; };
     const char* bc = c.bc == NICR_BC_MU ? "mu" : c.bc == NICR_BC_CLOSED ? "closed" : "concentration";
@@ -640,21 +685,157 @@ void copy_out(char* buf, size_t len, const std::string& s) {
 int self_test(int dim) { return nicr::run_self_test(dim); }
 
 // ------------------------------------------------------------------ run()
+// The program over a slab group (--slabs N [--slab-devices a,b,...]): the
+// domain split along X over N slabs, slab i on GPU a_i (default: GPU i modulo
+// the GPUs present). The same files as the single-GPU program: diagnostics,
+// grain statistics and VTI frames are whole-domain values gathered from the
+// slabs; parameters.txt names the slab backend and the summed device memory.
+// Checkpoints and ASCII VTK frames are not written in this form.
+int run_program_slabs(const nicr_config& c, int dim, const std::string& dir, int slabs, const std::string& devs,
+                      const std::string& restart) {
+    try {
+        if (dim != 3) throw std::runtime_error("--slabs needs the 3D program.");
+        if (!restart.empty() || c.checkpoint_every > 0)
+            throw std::runtime_error("--slabs does not write or read checkpoints.");
+        if (!c.output_vti) throw std::runtime_error("--slabs writes VTI frames only (--output-format vti).");
+        int count = 0;
+        if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) throw std::runtime_error("no CUDA device is available");
+        std::vector<int> dev;
+        if (!devs.empty()) {
+            std::stringstream ss(devs);
+            std::string item;
+            while (std::getline(ss, item, ',')) dev.push_back(std::stoi(item));
+            if (slabs == 1) slabs = (int)dev.size();
+            if ((int)dev.size() != slabs) throw std::runtime_error("--slab-devices needs one device per slab.");
+        } else {
+            for (int s = 0; s < slabs; ++s) dev.push_back((c.device + s) % count);
+        }
+        if (fs::exists(dir) && !fs::is_empty(dir)) throw std::runtime_error("Output directory is not empty; choose a new --out.");
+        fs::create_directories(dir);
+        nicr::SlabGroup g(c, slabs, dev.data());
+        const bool has_eta = g.m[0]->has_eta;
+        const int neta = g.m[0]->neta;
+        metadata(meta_of(g), dir);
+        std::ofstream log(dir + "/diagnostics.csv"), gd, gh;
+        if (!log) throw std::runtime_error("Cannot open diagnostics.csv");
+        log << "step,time_s,sum_O,sum_Cr,mean_phi,O_boundary,O_seed,Cr_seed,O_Ck,Cr_Ck,O_clipping,Cr_clipping,"
+               "O_budget_residual,Cr_budget_residual,nuclei,clipped_cells,min_O,max_O,min_Cr,max_Cr,min_Ni,min_phi,max_phi"
+               ",mean_h_phi,oxide_volume_m3\n";
+        if (has_eta) {
+            gd.open(dir + "/grain_diagnostics.csv");
+            gh.open(dir + "/grain_history.csv");
+            if (!gd || !gh) throw std::runtime_error("Cannot open grain diagnostics.");
+            gd << "step,time_s,min_eta,max_eta,min_sum_eta2,max_sum_eta2,mean_sum_eta2,grains_with_metal_cells,"
+                  "unassigned_metal_cells,integrated_active_GB_m3,max_GB_mask,grain_energy_model_units\n";
+            gh << "step,time_s,grain_id,dominant_metal_cells,weighted_metal_volume_cells,weighted_metal_volume_m3\n";
+        }
+        auto do_log = [&](int n) {
+            nicr_diagnostics d;
+            g.diagnostics(&d);
+            nicr_budget b;
+            g.budget(&b);
+            log << log_row(c, dim, d, b, n);
+            if (has_eta) {
+                nicr_grain_stats st;
+                std::vector<long long> cells((size_t)neta);
+                std::vector<double> amount((size_t)neta * 2);
+                g.grain_stats(&st, cells.data(), amount.data());
+                std::string a, bb;
+                grain_rows(c, dim, neta, st, cells, amount, n, a, bb);
+                gd << a;
+                gh << bb;
+            }
+        };
+        auto frame = [&](const std::string& path) {
+            std::vector<unsigned char> arrays;
+            const bool f64 = c.output_float64 != 0;
+            const unsigned r = g.vti_arrays(arrays, f64);
+            if (r) {
+                int arr = 0;
+                while (!(r & (1u << arr))) ++arr;
+                throw nicr::Error(NICR_ERR_IO, std::string("VTI ") + NAMES3[(size_t)arr] +
+                                                   " exceeds output type range; use --output-precision float64.");
+            }
+            compose_vti(c, arrays.data(), f64, path);
+        };
+        do_log(0);
+        frame(dir + "/fields_0.vti");
+        std::cout << "EXECUTION BACKEND: CUDA sm_100a, the domain split along X over " << slabs << " slabs.\n";
+        std::cout << "MPI processes: 1 (slabs on GPUs";
+        for (int d : dev) std::cout << " " << d;
+        std::cout << ")\n";
+        std::cout << "Output: vti, " << (c.output_float64 ? "float64" : "float32") << "; zlib level=" << c.compression_level
+                  << "; frozen-eta cache=" << (c.frozen_eta_cache ? "on" : "off") << ".\n";
+        std::cout << "Version " << VERSION3 << "; grains=" << (c.grains ? "on" : "off")
+                  << "; oxygen_diffusion=" << (c.oxygen_diffusion ? "on" : "off") << "; nucleation="
+                  << (c.nucleation == NICR_NUC_CENTER ? "center" : c.nucleation == NICR_NUC_OFF ? "off" : "ksp") << "; "
+                  << g.m[0]->seeds.size() / 3 << " grain(s).\n";
+        int last = 0, n = 0;
+        try {
+            while (n < c.steps) {
+                int next = std::min(c.steps, (n / 1000 + 1) * 1000);
+                next = std::min(next, (n / c.output_every + 1) * c.output_every);
+                int done = 0;
+                const int r = g.advance(next - n, true, &done);
+                last = n + done;
+                if (r != NICR_OK) throw nicr::Error(r, g.err);
+                n = next;
+                if (n % 1000 == 0 || n == c.steps)
+                    std::cout << "step " << n << "/" << c.steps << " (" << 100.0 * n / c.steps << "%), time=" << n * c.dt
+                              << " s" << std::endl;
+                if (n % c.output_every == 0 || n == c.steps) {
+                    do_log(n);
+                    log.flush();
+                    if (!log) throw std::runtime_error("Diagnostics write failed.");
+                    if (has_eta) {
+                        gd.flush();
+                        gh.flush();
+                        if (!gd || !gh) throw std::runtime_error("Grain diagnostics write failed.");
+                    }
+                    frame(dir + "/fields_" + std::to_string(n) + ".vti");
+                }
+            }
+        } catch (const std::exception& e) {
+            std::ofstream stop(dir + "/STOPPED.txt");
+            stop << "Last accepted time step: " << last << "\n" << e.what() << "\n";
+            frame(dir + "/state_at_failure.vti");
+            throw;
+        }
+        std::cout << "Finished " << last << " steps. Output: " << dir << "\n";
+        return 0;
+    } catch (const std::exception& e) {
+        std::cerr << "ERROR: " << e.what() << "\n";
+        return 1;
+    }
+}
+
 int run_program(int dim, int argc, const char* const* argv) {
     nicr_config c;
     std::vector<char> out(4096), err(16384);
     int self = 0;
     // --restart FILE is a program-level flag (the state to continue from); the
     // rest is the configuration
-    std::string restart;
+    std::string restart, slab_devices;
+    int slabs = 1;
     std::vector<const char*> args;
     for (int q = 0; q < argc; ++q) {
-        if (q > 0 && std::string(argv[q]) == "--restart") {
+        const std::string a = q > 0 ? argv[q] : "";
+        if (a == "--restart" || a == "--slabs" || a == "--slab-devices") {
             if (q + 1 >= argc) {
-                std::cerr << "ERROR: Missing value for --restart\n";
+                std::cerr << "ERROR: Missing value for " << a << "\n";
                 return 1;
             }
-            restart = argv[++q];
+            const std::string v = argv[++q];
+            if (a == "--restart") restart = v;
+            else if (a == "--slab-devices") slab_devices = v;
+            else {
+                size_t used = 0;
+                try { slabs = std::stoi(v, &used); } catch (...) { used = 0; }
+                if (used != v.size() || slabs < 1 || slabs > nicr::kMaxSlabs) {
+                    std::cerr << "ERROR: --slabs expects an integer in [1, 16].\n";
+                    return 1;
+                }
+            }
             continue;
         }
         args.push_back(argv[q]);
@@ -672,13 +853,14 @@ int run_program(int dim, int argc, const char* const* argv) {
     }
     if (self) return self_test(dim);
     const std::string dir = out.data();
+    if (slabs > 1 || !slab_devices.empty()) return run_program_slabs(c, dim, dir, slabs, slab_devices, restart);
     try {
         if (fs::exists(dir) && !fs::is_empty(dir)) throw std::runtime_error("Output directory is not empty; choose a new --out.");
         fs::create_directories(dir);
         Model m(c);
         if (!restart.empty()) m.load_state(restart);
         const int start = (int)m.steps_done;
-        metadata(m, dir);
+        metadata(meta_of(m), dir);
         std::ofstream log(dir + "/diagnostics.csv"), gd, gh;
         if (!log) throw std::runtime_error("Cannot open diagnostics.csv");
         log << "step,time_s,sum_O,sum_Cr,mean_phi,O_boundary,O_seed,Cr_seed,O_Ck,Cr_Ck,O_clipping,Cr_clipping,"
@@ -797,7 +979,7 @@ int nicr_output_wait(nicr_handle* h) {
     return guarded(h, [&](Model& m) { output_wait(m); });
 }
 int nicr_write_metadata(nicr_handle* h, const char* out_dir) {
-    return guarded(h, [&](Model& m) { metadata(m, out_dir); });
+    return guarded(h, [&](Model& m) { metadata(meta_of(m), out_dir); });
 }
 int nicr_format_log_row(nicr_handle* h, int n, char* buf, size_t len) {
     return guarded(h, [&](Model& m) { copy_out(buf, len, log_row(m, n)); });

@@ -27,53 +27,16 @@
 // cells differently); budgets are the sums of the slabs' double-double budgets.
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <memory>
 #include <new>
 #include <string>
 #include <vector>
 
 #include "../../include/nicr.h"
-#include "nicr_model.h"
+#include "nicr_slabs.h"
 
 namespace nicr {
-
-class SlabGroup {
-public:
-    SlabGroup(const nicr_config& cfg, int n, const int* devices);
-    ~SlabGroup();
-    SlabGroup(const SlabGroup&) = delete;
-    SlabGroup& operator=(const SlabGroup&) = delete;
-
-    nicr_config c;
-    int halo = 2;
-    std::vector<std::unique_ptr<Model>> m;
-    std::vector<int> x0, x1, dev;
-    std::string err;
-
-    int advance(int nsteps, bool schedule, int* completed);
-    int nucleate(int* nuclei);
-    void get_field(int field, int index, double* host);
-    void set_field(int field, int index, const double* host);
-    void reset_inventory();
-    void budget(nicr_budget* b);
-    void diagnostics(nicr_diagnostics* d);
-    long long launches() const;
-
-private:
-    std::vector<cudaEvent_t> ev_done, ev_push;
-    bool pushed = false;
-    SlabPeers peers{};
-    std::vector<KspNucleus*> d_pre, d_out;
-    int cap = 1 << 16;                 // nuclei per slab and scan
-    long long copies = 0;              // halo copy launches
-
-    void on(int s) const { check_cuda(cudaSetDevice(dev[(size_t)s]), "cudaSetDevice"); }
-    void one_step();
-    void push(int s, bool step_fields, int p_width);
-    void sync_all();
-    bool any_failed();
-    int scan();
-};
 
 namespace {
 // the halo width: the step's stencil reach (2 planes of o and cr), or the
@@ -471,6 +434,90 @@ void SlabGroup::diagnostics(nicr_diagnostics* out) {
         out->min_Ni = pick_min(out->min_Ni, d.min_Ni);
         out->min_phi = pick_min(out->min_phi, d.min_phi); out->max_phi = pick_max(out->max_phi, d.max_phi);
     }
+}
+
+void SlabGroup::grain_stats(nicr_grain_stats* out, long long* cells, double* amount) {
+    const int neta = m[0]->neta;
+    std::vector<long long> cs((size_t)neta);
+    std::vector<double> am((size_t)neta * 2);
+    std::vector<long long> tc((size_t)neta, 0);
+    std::vector<double> ta((size_t)neta * 2, 0.);
+    for (int s = 0; s < (int)m.size(); ++s) {
+        on(s);
+        nicr_grain_stats g;
+        m[(size_t)s]->grain_stats(&g, cs.data(), am.data());
+        for (int q = 0; q < neta; ++q) {
+            tc[(size_t)q] += cs[(size_t)q];
+            put(&ta[2 * (size_t)q], dd_add(dd(&ta[2 * (size_t)q]), dd(&am[2 * (size_t)q])));
+        }
+        if (s == 0) { *out = g; continue; }
+        out->min_eta = pick_min(out->min_eta, g.min_eta);
+        out->max_eta = pick_max(out->max_eta, g.max_eta);
+        out->min_s2 = pick_min(out->min_s2, g.min_s2);
+        out->max_s2 = pick_max(out->max_s2, g.max_s2);
+        put(out->sum_s2, dd_add(dd(out->sum_s2), dd(g.sum_s2)));
+        put(out->mask, dd_add(dd(out->mask), dd(g.mask)));
+        put(out->energy, dd_add(dd(out->energy), dd(g.energy)));
+        out->gb_max = pick_max(out->gb_max, g.gb_max);
+        out->unassigned += g.unassigned;
+    }
+    out->alive = 0;
+    for (long long v : tc) out->alive += v > 0;
+    if (cells) std::copy(tc.begin(), tc.end(), cells);
+    if (amount) std::copy(ta.begin(), ta.end(), amount);
+}
+
+unsigned SlabGroup::vti_arrays(std::vector<unsigned char>& out, bool f64) {
+    const size_t esz = f64 ? 8 : 4;
+    const long long ny = c.ny, nz = c.nz, nx = c.nx, n = nx * ny * nz;
+    out.resize(7 * (size_t)n * esz);
+    unsigned range = 0;
+    std::vector<unsigned char> part;
+    for (int s = 0; s < (int)m.size(); ++s) {
+        Model& a = *m[(size_t)s];
+        on(s);
+        a.refresh();
+        a.ensure_mask();
+        VtiArgs v{};
+        v.g = a.own_grid();
+        v.g.nstore = a.g.nstore;   // eta fields keep their stored stride
+        const long long off = a.own_offset(), ns = v.g.ncells, nxs = v.g.nx;
+        v.has_eta = a.has_eta ? 1 : 0;
+        v.neta = a.neta;
+        v.p = a.d_p() + off; v.o = a.d_o() + off; v.cr = a.d_cr() + off;
+        v.muO = a.d_mu_o() + off; v.muCr = a.d_mu_cr() + off;
+        v.gb = a.d_gb() + off;
+        v.grain = a.grain_retained ? a.d_grain() + off : nullptr;
+        v.eta = a.has_eta ? a.d_eta(0) + off : nullptr;
+        if (!a.has_eta && !v.grain) throw Error(NICR_ERR_STATE, "grain map missing for grain_sum");
+        void* d_out = nullptr;
+        unsigned* d_range = nullptr;
+        check_cuda(cudaMalloc(&d_out, 7 * (size_t)ns * esz), "cudaMalloc (VTI arrays)");
+        check_cuda(cudaMalloc(&d_range, sizeof(unsigned)), "cudaMalloc");
+        check_cuda(cudaMemsetAsync(d_range, 0, sizeof(unsigned), a.stream), "memset");
+        launch_vti_arrays(v, d_out, f64, d_range, a.stream);
+        part.resize(7 * (size_t)ns * esz);
+        unsigned r = 0;
+        check_cuda(cudaMemcpyAsync(part.data(), d_out, part.size(), cudaMemcpyDeviceToHost, a.stream), "D2H");
+        check_cuda(cudaMemcpyAsync(&r, d_range, sizeof r, cudaMemcpyDeviceToHost, a.stream), "D2H");
+        a.sync();
+        cudaFree(d_out);
+        cudaFree(d_range);
+        check_cuda(cudaGetLastError(), "VTI arrays");
+        range |= r;
+        // the slab's X-fastest rows are the [x0, x1) pieces of the domain's rows
+        for (int arr = 0; arr < 7; ++arr)
+            for (long long row = 0; row < ny * nz; ++row)
+                std::memcpy(out.data() + ((size_t)arr * n + (size_t)row * nx + x0[(size_t)s]) * esz,
+                            part.data() + ((size_t)arr * ns + (size_t)row * nxs) * esz, (size_t)nxs * esz);
+    }
+    return range;
+}
+
+size_t SlabGroup::device_bytes() const {
+    size_t b = 0;
+    for (auto& q : m) b += q->device_bytes();
+    return b;
 }
 
 }  // namespace nicr

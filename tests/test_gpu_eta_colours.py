@@ -46,6 +46,7 @@ def nearest_bisector(seeds, owner, shape):
     oy, oz = y + yy, z + zz
     db = np.full(shape, np.inf)
     comp = np.full(shape, -1)
+    np.seterr(invalid="ignore", divide="ignore")   # sep == 0 for the owner's own images: masked below
     for s in range(ng):
         d = np.full(shape, np.inf)
         for im in (-1, 0, 1):

@@ -1,6 +1,6 @@
 """Parity at the benchmark's full size: 3D 256^3 with 8 evolving eta (the
-bench.py workload: Voronoi seed 2, Cr 0.25 +- 0.01, O inlet, Ksp, legacy Ck
-and bounds). The tile/X-chunk decomposition, the CTA count and the per-CTA
+bench.py workload: 64 Voronoi seeds of seed 2 coloured into 8 eta, Cr 0.25
++- 0.01, O inlet, Ksp, legacy Ck and bounds). The tile/X-chunk decomposition, the CTA count and the per-CTA
 budget partials at this size are the ones the benchmark times, so the drop-in
 form is checked bit for bit against the oracle here, and the reciprocal form
 for run-to-run determinism and its deviation from the drop-in form."""
@@ -33,11 +33,14 @@ def make_solver(precision):
 
 
 def test_full_size_drop_in_matches_oracle(require_gpu):
+    """The oracle has no coloured initialisation; stepping needs the state
+    alone, so it is built with 8 seeds (8 eta) and given the handle's
+    coloured initial state."""
     sol = make_solver(0)
-    orc = Oracle(bench.workload_config(SIZE, NETA, device=0, seed=2))
+    orc = Oracle(bench.workload_config(SIZE, NETA, device=0, seed=2, coloured=False))
     assert orc.neta == NETA
-    eta = np.array([orc.get(f"eta{g + 1}") for g in range(NETA)])
-    orc.set_fields(orc.get("o"), bench_inputs(orc.shape, orc.get("cr")[0]), orc.get("p"), eta)
+    eta = np.array([sol.get("eta", g) for g in range(NETA)])
+    orc.set_fields(sol.get("o"), sol.get("cr"), sol.get("p"), eta)
     orc.reset_inventory()
     rc, done = orc.run(3)
     assert rc == 0 and done == 3
