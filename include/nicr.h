@@ -338,6 +338,7 @@ typedef struct nicr_slabs nicr_slabs;
 int nicr_slabs_create(const nicr_config* cfg, int nslabs, const int* devices, nicr_slabs** out);
 void nicr_slabs_destroy(nicr_slabs* s);
 int nicr_slabs_count(const nicr_slabs* s);
+int nicr_slabs_n_eta(const nicr_slabs* s);      /* eta fields of the domain */
 /* domain planes [*x0, *x1) of slab i, its device and the halo width */
 int nicr_slabs_info(const nicr_slabs* s, int i, int* x0, int* x1, int* device, int* halo);
 int nicr_slabs_step(nicr_slabs* s, int nsteps, int* completed);
@@ -348,6 +349,10 @@ int nicr_slabs_set_field(nicr_slabs* s, int field, int index, const double* host
 int nicr_slabs_reset_inventory(nicr_slabs* s);
 int nicr_slabs_get_budget(nicr_slabs* s, nicr_budget* b);
 int nicr_slabs_get_diagnostics(nicr_slabs* s, nicr_diagnostics* d);
+/* nicr_get_grain_stats over the whole domain (cells, amount: n_eta entries) */
+int nicr_slabs_get_grain_stats(nicr_slabs* s, nicr_grain_stats* st, long long* cells, double* amount);
+/* nicr_write_vti of the whole domain: the same file a single handle writes */
+int nicr_slabs_write_vti(nicr_slabs* s, const char* path);
 long long nicr_slabs_steps_done(const nicr_slabs* s);
 long long nicr_slabs_kernel_launches(const nicr_slabs* s);
 /* stream (a cudaStream_t) slab i enqueues on */

@@ -957,6 +957,30 @@ int run_program(int dim, int argc, const char* const* argv) {
 // ------------------------------------------------------------------ C-ABI
 extern "C" {
 
+int nicr_slabs_write_vti(nicr_slabs* s, const char* path) {
+    nicr::SlabGroup* g = nicr_slabs_group(s);
+    if (!g || !path) return NICR_ERR_INVALID_ARG;
+    try {
+        std::vector<unsigned char> arrays;
+        const bool f64 = g->c.output_float64 != 0;
+        const unsigned r = g->vti_arrays(arrays, f64);
+        if (r) {
+            int arr = 0;
+            while (!(r & (1u << arr))) ++arr;
+            throw nicr::Error(NICR_ERR_IO, std::string("VTI ") + NAMES3[(size_t)arr] +
+                                               " exceeds output type range; use --output-precision float64.");
+        }
+        compose_vti(g->c, arrays.data(), f64, path);
+        return NICR_OK;
+    } catch (const nicr::Error& e) {
+        nicr_slabs_set_error(s, e.what());
+        return e.code;
+    } catch (const std::exception& e) {
+        nicr_slabs_set_error(s, e.what());
+        return NICR_ERR_IO;
+    }
+}
+
 int nicr_write_vtk(nicr_handle* h, const char* path) {
     return guarded(h, [&](Model& m) {
         if (m.dim == 2) write_vtk2(m, path);

@@ -548,6 +548,12 @@ int slabs_guarded(nicr_slabs* h, F&& f) {
 }
 }  // namespace
 
+// For nicr_slabs_write_vti, defined with the VTI writer (nicr_output.cpp)
+nicr::SlabGroup* nicr_slabs_group(nicr_slabs* h) { return h ? h->g.get() : nullptr; }
+void nicr_slabs_set_error(nicr_slabs* h, const std::string& e) {
+    if (h && h->g) h->g->err = e;
+}
+
 extern "C" {
 
 int nicr_slabs_create(const nicr_config* cfg, int nslabs, const int* devices, nicr_slabs** out) {
@@ -579,6 +585,8 @@ int nicr_slabs_create(const nicr_config* cfg, int nslabs, const int* devices, ni
 void nicr_slabs_destroy(nicr_slabs* h) { delete h; }
 
 int nicr_slabs_count(const nicr_slabs* h) { return h && h->g ? (int)h->g->m.size() : 0; }
+
+int nicr_slabs_n_eta(const nicr_slabs* h) { return h && h->g ? h->g->m[0]->neta : 0; }
 
 int nicr_slabs_info(const nicr_slabs* h, int slab, int* x0, int* x1, int* device, int* halo) {
     if (!h || !h->g || slab < 0 || slab >= (int)h->g->m.size()) return NICR_ERR_INVALID_ARG;
@@ -623,6 +631,15 @@ int nicr_slabs_get_budget(nicr_slabs* h, nicr_budget* b) {
 int nicr_slabs_get_diagnostics(nicr_slabs* h, nicr_diagnostics* d) {
     if (!d) return NICR_ERR_INVALID_ARG;
     return slabs_guarded(h, [&](nicr::SlabGroup& g) { g.diagnostics(d); return NICR_OK; });
+}
+
+int nicr_slabs_get_grain_stats(nicr_slabs* h, nicr_grain_stats* st, long long* cells, double* amount) {
+    if (!st) return NICR_ERR_INVALID_ARG;
+    return slabs_guarded(h, [&](nicr::SlabGroup& g) {
+        if (!g.m[0]->has_eta) throw nicr::Error(NICR_ERR_STATE, "grain statistics exist only with evolving grains");
+        g.grain_stats(st, cells, amount);
+        return NICR_OK;
+    });
 }
 
 long long nicr_slabs_steps_done(const nicr_slabs* h) { return h && h->g ? h->g->m[0]->steps_done : 0; }

@@ -56,3 +56,8 @@ private:
 };
 
 }  // namespace nicr
+
+// The group behind a C-ABI slab handle, and its last-error setter (for the
+// entry points defined with the output code).
+nicr::SlabGroup* nicr_slabs_group(nicr_slabs* h);
+void nicr_slabs_set_error(nicr_slabs* h, const std::string& e);

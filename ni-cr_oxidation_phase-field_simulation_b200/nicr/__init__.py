@@ -140,6 +140,9 @@ def lib():
     L.nicr_slabs_steps_done.restype = ctypes.c_longlong
     L.nicr_slabs_kernel_launches.argtypes = [H]
     L.nicr_slabs_kernel_launches.restype = ctypes.c_longlong
+    L.nicr_slabs_get_grain_stats.argtypes = [H, ctypes.POINTER(NicrGrainStats), ctypes.POINTER(ctypes.c_longlong), dp]
+    L.nicr_slabs_write_vti.argtypes = [H, ctypes.c_char_p]
+    L.nicr_slabs_n_eta.argtypes = [H]
     L.nicr_slabs_stream.argtypes = [H, ctypes.c_int]
     L.nicr_slabs_stream.restype = ctypes.c_void_p
     L.nicr_slabs_last_error.argtypes = [H]
@@ -566,6 +569,30 @@ class Slabs:
         for n in ("min_O", "max_O", "min_Cr", "max_Cr", "min_Ni", "min_phi", "max_phi"):
             out[n] = getattr(d, n)
         return out
+
+    def grain_stats(self):
+        """nicr_slabs_get_grain_stats, in the form Solver.grain_stats returns."""
+        ne = max(1, self.n_eta)
+        s = NicrGrainStats()
+        cells = np.zeros(ne, dtype=np.int64)
+        amount = np.zeros(2 * ne)
+        self._check(lib().nicr_slabs_get_grain_stats(self.s, ctypes.byref(s),
+                                                     cells.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong)),
+                                                     _dp(amount)))
+        out = {n: getattr(s, n) for n in ("min_eta", "max_eta", "min_s2", "max_s2", "gb_max")}
+        for n in ("sum_s2", "mask", "energy"):
+            out[n] = (getattr(s, n)[0], getattr(s, n)[1])
+        out["alive"], out["unassigned"] = int(s.alive), int(s.unassigned)
+        out["cells"] = cells[: self.n_eta]
+        out["amount"] = amount[: 2 * self.n_eta].reshape(-1, 2)
+        return out
+
+    def write_vti(self, path):
+        self._check(lib().nicr_slabs_write_vti(self.s, str(path).encode()))
+
+    @property
+    def n_eta(self) -> int:
+        return int(lib().nicr_slabs_n_eta(self.s))
 
     @property
     def steps_done(self) -> int:

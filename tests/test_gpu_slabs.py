@@ -211,3 +211,27 @@ def test_128cube_8eta_two_slabs(require_gpu, precision):
                 assert dev <= 1e-13, (f, dev)
             assert_budget(s.budget(), solo.budget(), rtol=1e-12)
     solo.close()
+
+
+def test_grain_stats_and_vti_match(require_gpu, tmp_path):
+    """nicr_slabs_get_grain_stats and nicr_slabs_write_vti give a single
+    handle's values and file (grain statistics sum per slab: 1e-13)."""
+    cfg = grains_cfg(eta_colours=5)
+    solo = nicr.Solver(cfg)
+    with nicr.Slabs(cfg, 3) as s:
+        assert s.n_eta == solo.n_eta == 5
+        inject(solo, 6, 5)
+        inject(s, 6, 5)
+        s.run(11)
+        solo.run(11)
+        a, b = s.grain_stats(), solo.grain_stats()
+        for k in ("min_eta", "max_eta", "min_s2", "max_s2", "gb_max", "alive", "unassigned"):
+            assert a[k] == b[k], k
+        for k in ("sum_s2", "mask", "energy"):
+            assert abs(sum(a[k]) - sum(b[k])) <= 1e-13 * (1 + abs(sum(b[k]))), k
+        assert (a["cells"] == b["cells"]).all()
+        assert np.allclose(a["amount"].sum(axis=1), b["amount"].sum(axis=1), rtol=1e-13, atol=0)
+        s.write_vti(tmp_path / "slabs.vti")
+        solo.write_vti(tmp_path / "solo.vti")
+        assert (tmp_path / "slabs.vti").read_bytes() == (tmp_path / "solo.vti").read_bytes()
+    solo.close()
