@@ -359,6 +359,53 @@ long long nicr_slabs_kernel_launches(const nicr_slabs* s);
 void* nicr_slabs_stream(const nicr_slabs* s, int i);
 const char* nicr_slabs_last_error(const nicr_slabs* s);
 
+/* Slab form with one process per GPU: a handle holding slab `index` of the
+ * domain split along X into nslabs slabs (the partition and halo width of
+ * nicr_slabs_create), initialised like the whole domain's planes. The caller
+ * communicates between the ranks (the python package's slab_ranks module does
+ * it over torch.distributed with NCCL), per step:
+ *   nicr_slab_launch    the step kernels, then this step's agreement word
+ *                       (nicr_slab_agree_word: an int64 on the device,
+ *                       INT64_MAX when every trial passed, else the failing
+ *                       cell's key in whole-domain order)
+ *   MIN all-reduce of the agreement words over the ranks, in place
+ *   nicr_slab_commit    commit with the reduced word (all ranks accept or
+ *                       reject alike), flip the buffer parity
+ *   halo exchange: each rank sends nicr_slab_region(which = 0 / 1) planes
+ *   to the rank below / above and receives into which = 2 / 3: o and cr two
+ *   planes deep, phi one, and with evolving grains gb and every eta one.
+ * Batches of steps: nicr_slab_begin(n, schedule), per step s
+ * nicr_slab_scan_due(s) (a Ksp scan is due before step s: exchange phi
+ * `halo` planes deep, nicr_slab_scan_candidates on every rank, then
+ * nicr_slab_scan_resolve rank after rank in X order with the nuclei the
+ * lower ranks accepted in this scan as `pre` (KspNucleus: x, y, z, full;
+ * nicr_slab_box_half cells of reach), then nicr_slab_scan_apply with the
+ * nuclei of the higher ranks) and nicr_slab_note_step(s, scanned), then
+ * nicr_slab_end(enqueued, &completed): the status and rollback of nicr_run
+ * (only the rank owning the failing cell has its message). The coloured
+ * initialisation (eta_colours) needs the ranks' adjacencies OR-reduced:
+ * nicr_slab_adjacency (ng x ng bytes), nicr_colour_grains, then
+ * nicr_slab_set_colours on every rank. The other calls of this header
+ * (fields, budget, diagnostics) see the slab's stored planes / own planes. */
+int nicr_slab_create(const nicr_config* cfg, int nslabs, int index, nicr_handle** out);
+int nicr_slab_info(const nicr_handle* h, int* x0, int* x1, int* x_lo, int* x_hi, int* stored, int* halo);
+int nicr_slab_region(nicr_handle* h, int field, int index, int which, int width, void** ptr, long long* count);
+int nicr_slab_adjacency(nicr_handle* h, unsigned char* adj);
+int nicr_colour_grains(const unsigned char* adj, int ng, int k, int* colours);
+int nicr_slab_set_colours(nicr_handle* h, const int* colours);
+int nicr_slab_begin(nicr_handle* h, int nsteps, int schedule);
+int nicr_slab_scan_due(nicr_handle* h, int s);
+int nicr_slab_note_step(nicr_handle* h, int s, int scanned);
+int nicr_slab_failed(nicr_handle* h, int* failed);
+int nicr_slab_launch(nicr_handle* h);
+void* nicr_slab_agree_word(nicr_handle* h);
+int nicr_slab_commit(nicr_handle* h);
+int nicr_slab_end(nicr_handle* h, int enqueued, int* completed);
+int nicr_slab_scan_candidates(nicr_handle* h);
+int nicr_slab_scan_resolve(nicr_handle* h, const int* pre, int npre, int* out, int cap, int* nout, int* nuclei);
+int nicr_slab_scan_apply(nicr_handle* h, const int* list, int n);
+int nicr_slab_box_half(const nicr_handle* h);
+
 /* The solver program: the reference's run()/main() for dim 2 or 3
  * (2D:1161-1246, 3S:1309-1395), argv as the reference's executable takes it.
  * Returns the process exit code. */

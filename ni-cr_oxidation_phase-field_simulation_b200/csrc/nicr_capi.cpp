@@ -11,6 +11,12 @@
 
 namespace {
 thread_local std::string g_create_error;
+}  // namespace
+
+// the message nicr_last_error(NULL) returns after a failed creation
+void nicr::set_create_error(const std::string& e) { g_create_error = e; }
+
+namespace {
 
 template <class Fn>
 int guarded(nicr_handle* h, Fn fn) {

@@ -183,6 +183,13 @@ struct SlabPeers {
 };
 void launch_step_finalize_slab(const StepPartial* partials, int nblocks, DevBudget* budget, Status* st,
                                const SlabPeers& peers, cudaStream_t stream);
+// One process per slab: the slab's error word of the step (slot) as a signed
+// agreement word (kAgreeNone when every trial passed, else the key), which
+// the ranks reduce with a MIN collective; the commit then reads the result.
+constexpr long long kAgreeNone = 0x7fffffffffffffffLL;
+void launch_agree_word(const Status* st, int slot, long long* agree, cudaStream_t stream);
+void launch_step_finalize_agreed(const StepPartial* partials, int nblocks, DevBudget* budget, Status* st,
+                                 const long long* agreed, cudaStream_t stream);
 // Copies up to kCopySegs strided runs of doubles (rows x n, 16-byte aligned
 // addresses and counts of whole double pairs) in one launch; destinations may
 // be another GPU's memory (peer access enabled): the halo exchange of the

@@ -202,7 +202,7 @@ void Model::release() {
     double* bufs[] = {o_[0], o_[1], cr_[0], cr_[1], p_[0], p_[1], gb_[0], gb_[1], s2_[0], s2_[1], eta_[0], eta_[1],
                       grain, pairs, gb_initial, muO, muCr, mo, mc};
     for (double* b : bufs) if (b) cudaFree(b);
-    void* others[] = {partials, st, bud, diag_part, diag_out, red_out, kres, d_shadow, d_ball, d_hyp,
+    void* others[] = {partials, st, bud, diag_part, diag_out, red_out, kres, d_shadow, d_ball, d_hyp, agree,
                       kw.flag, kw.blocked, kw.counts, kw.list, kw.total, gw.cells, gw.parts, gw.amount_parts,
                       g_out, g_amount, g_cells};
     for (void* b : others) if (b) cudaFree(b);
@@ -216,7 +216,7 @@ void Model::release() {
     std::memset(gb_, 0, sizeof gb_); std::memset(s2_, 0, sizeof s2_); std::memset(eta_, 0, sizeof eta_);
     grain = pairs = gb_initial = muO = muCr = mo = mc = nullptr;
     partials = nullptr; st = nullptr; bud = nullptr; diag_part = diag_out = nullptr; red_out = nullptr; kres = nullptr;
-    d_shadow = d_ball = nullptr; d_hyp = nullptr; kw = KspWork{}; h_st = nullptr; stream = nullptr;
+    d_shadow = d_ball = nullptr; d_hyp = nullptr; kw = KspWork{}; h_st = nullptr; stream = nullptr; agree = nullptr;
     gw = GrainWork{}; g_out = nullptr; g_amount = nullptr; g_cells = nullptr;
 }
 
@@ -1118,6 +1118,26 @@ void Model::slab_commit(int nblocks, const SlabPeers& peers) {
     q.slot = cur;
     const size_t e = prof_begin();
     launch_step_finalize_slab(partials, nblocks, bud, st, q, stream);
+    prof_end(K_FINALIZE, e, 1);
+    cur ^= 1;
+    if (advance_eta) { ecur ^= 1; gcur ^= 1; }
+}
+
+long long* Model::d_agree() {
+    if (!agree) agree = dalloc_t<long long>(1);
+    return agree;
+}
+
+void Model::rank_launch() {
+    const int parity = cur;
+    rank_nb = slab_launch();
+    launch_agree_word(st, parity, d_agree(), stream);
+    launches += 1;
+}
+
+void Model::rank_commit() {
+    const size_t e = prof_begin();
+    launch_step_finalize_agreed(partials, rank_nb, bud, st, d_agree(), stream);
     prof_end(K_FINALIZE, e, 1);
     cur ^= 1;
     if (advance_eta) { ecur ^= 1; gcur ^= 1; }

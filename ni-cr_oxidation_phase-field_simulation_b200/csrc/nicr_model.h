@@ -24,6 +24,8 @@ struct Error : std::runtime_error {
 };
 
 void check_cuda(cudaError_t e, const char* what);
+// The message nicr_last_error(NULL) returns after a failed creation.
+void set_create_error(const std::string& e);
 
 // An X slab of a larger 3D domain (the slab form, nicr_slabs.cpp): the model
 // owns domain planes [x0, x1) and stores them with up to `halo` neighbour
@@ -34,6 +36,7 @@ struct SlabSpec {
     int x0 = 0, x1 = 0, halo = 0;
 };
 class SlabGroup;
+class SlabRank;
 
 // Colours ng grains with k colours from their face adjacency (adj: ng x ng
 // bytes): DSatur order (most distinct neighbour colours, then most
@@ -171,8 +174,20 @@ public:
     void fetch(const double* d, double* host) { copy_out(d, host); }
     void ensure_mask() { if (has_eta && (eta_dirty || dim == 2)) eta_mask_now(); }
 
+    // One process per slab (nicr_slab_* in nicr_slab_rank.cpp): the step
+    // kernels plus this step's signed agreement word (d_agree(), which the
+    // ranks reduce with a MIN collective), then the commit that reads the
+    // reduced word and flips parity.
+    void rank_launch();
+    void rank_commit();
+    long long* d_agree();
+    RunPlan rank_plan;
+
 private:
     friend class SlabGroup;
+    friend class SlabRank;
+    int rank_nb = 0;
+    long long* agree = nullptr;
     // slab form: the step kernels of one step into the trial buffers (no
     // commit; returns the step kernel's partial count), and the commit that
     // agrees with the other slabs on the step's outcome, then flips parity

@@ -61,24 +61,33 @@ double pick_max(double a, double b) {
 }
 }  // namespace
 
-SlabGroup::SlabGroup(const nicr_config& cfg, int n, const int* devices) : c(cfg) {
+SlabSpec slab_partition(const nicr_config& c, int n, int index) {
     if (c.dim != 3) throw Error(NICR_ERR_INVALID_ARG, "the slab form is 3D only");
     if (n < 1 || n > kMaxSlabs) throw Error(NICR_ERR_INVALID_ARG, "between 1 and 16 slabs");
+    if (index < 0 || index >= n) throw Error(NICR_ERR_INVALID_ARG, "slab index out of range");
+    SlabSpec q;
+    q.halo = halo_for(c);
+    const int base = c.nx / n, rem = c.nx % n;
+    if (base < q.halo)
+        throw Error(NICR_ERR_INVALID_ARG, "each slab needs at least " + std::to_string(q.halo) + " planes along X");
+    q.x0 = index * base + std::min(index, rem);
+    q.x1 = q.x0 + base + (index < rem ? 1 : 0);
+    return q;
+}
+
+SlabGroup::SlabGroup(const nicr_config& cfg, int n, const int* devices) : c(cfg) {
     int count = 0;
     if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) throw Error(NICR_ERR_NO_DEVICE, "no CUDA device is available");
-    halo = halo_for(c);
-    const int base = c.nx / n, rem = c.nx % n;
-    if (base < halo)
-        throw Error(NICR_ERR_INVALID_ARG, "each slab needs at least " + std::to_string(halo) + " planes along X");
-    int x = 0;
     for (int s = 0; s < n; ++s) {
+        const SlabSpec q = slab_partition(c, n, s);
+        halo = q.halo;
         const int d = devices ? devices[s] : c.device;
         if (d < 0 || d >= count) throw Error(NICR_ERR_NO_DEVICE, "no CUDA device " + std::to_string(d));
         dev.push_back(d);
-        x0.push_back(x);
-        x += base + (s < rem ? 1 : 0);
-        x1.push_back(x);
+        x0.push_back(q.x0);
+        x1.push_back(q.x1);
     }
+    if (n < 1) throw Error(NICR_ERR_INVALID_ARG, "between 1 and 16 slabs");
     // every slab reads every other slab's error words, and neighbours store
     // into each other's halos: peer access between all devices in use
     for (int a : dev)

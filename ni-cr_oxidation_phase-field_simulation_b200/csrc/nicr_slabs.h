@@ -10,6 +10,11 @@
 
 namespace nicr {
 
+// Slab `index` of a domain split along X into n near-equal slabs (the first
+// nx mod n slabs one plane longer) and the halo width: 2, or ceil(radius +
+// gap) with Ksp nucleation (the reach of the pre-scan test).
+SlabSpec slab_partition(const nicr_config& c, int n, int index);
+
 class SlabGroup {
 public:
     SlabGroup(const nicr_config& cfg, int n, const int* devices);

@@ -116,12 +116,12 @@ __global__ void k_step_finalize(const StepPartial* __restrict__ partials, int nb
     finalize_body(partials, nblocks, budget, st, accept_mode);
 }
 
-// Slab commit: the same reduction; the step's outcome is the minimum over
-// every slab's error word of this step. The words are read with volatile
-// loads (L2, or the owning GPU's memory for a peer slab) after the stream
-// has waited for every slab's step kernels, so all slabs decide alike.
-__global__ void k_step_finalize_slab(const StepPartial* __restrict__ partials, int nblocks, DevBudget* budget,
-                                     Status* st, const SlabPeers peers) {
+// Slab commit: the same reduction; the step's outcome is the failing-trial
+// key key_of() returns (thread 0, after every slab's step kernels completed),
+// so all slabs decide alike.
+template <class KeyFn>
+__device__ void slab_finalize(const StepPartial* __restrict__ partials, int nblocks, DevBudget* budget, Status* st,
+                              KeyFn key_of) {
     __shared__ DD sdd[32 * 5];
     __shared__ long long scnt[32];
     if (st->failed) return;
@@ -133,12 +133,7 @@ __global__ void k_step_finalize_slab(const StepPartial* __restrict__ partials, i
     }
     block_reduce_dd<5>(acc, clipped, sdd, scnt);
     if (threadIdx.x == 0) {
-        unsigned long long key = ERR_NONE;
-        for (int j = 0; j < peers.n; ++j) {
-            const volatile unsigned long long* w = &peers.st[j]->slot_err[peers.slot];
-            const unsigned long long v = *w;
-            key = v < key ? v : key;
-        }
+        const unsigned long long key = key_of();
         if (key != ERR_NONE) {
             st->err_key = key;
             st->failed = 1;
@@ -154,6 +149,37 @@ __global__ void k_step_finalize_slab(const StepPartial* __restrict__ partials, i
         budget->clipped += clipped;
         st->steps_done += 1;
     }
+}
+
+// One process: the minimum over every slab's error word of this step, read
+// with volatile loads (L2, or the owning GPU's memory for a peer slab).
+__global__ void k_step_finalize_slab(const StepPartial* __restrict__ partials, int nblocks, DevBudget* budget,
+                                     Status* st, const SlabPeers peers) {
+    slab_finalize(partials, nblocks, budget, st, [&]() {
+        unsigned long long key = ERR_NONE;
+        for (int j = 0; j < peers.n; ++j) {
+            const volatile unsigned long long* w = &peers.st[j]->slot_err[peers.slot];
+            const unsigned long long v = *w;
+            key = v < key ? v : key;
+        }
+        return key;
+    });
+}
+
+// One process per slab: the word the ranks reduced with a MIN collective
+// (kAgreeNone: every trial passed).
+__global__ void k_step_finalize_agreed(const StepPartial* __restrict__ partials, int nblocks, DevBudget* budget,
+                                       Status* st, const long long* agreed) {
+    slab_finalize(partials, nblocks, budget, st, [&]() {
+        const long long v = *(const volatile long long*)agreed;
+        return v == kAgreeNone ? ERR_NONE : (unsigned long long)v;
+    });
+}
+
+// The signed agreement word of this step from the slab's error word.
+__global__ void k_agree_word(const Status* st, int slot, long long* agree) {
+    const unsigned long long k = st->slot_err[slot];
+    *agree = k == ERR_NONE ? kAgreeNone : (long long)k;
 }
 
 // Strided runs of double pairs: blockIdx.y picks the segment, the CTAs of a
@@ -312,6 +338,15 @@ void launch_step_finalize(const StepPartial* partials, int nblocks, DevBudget* b
 void launch_step_finalize_slab(const StepPartial* partials, int nblocks, DevBudget* budget, Status* st,
                                const SlabPeers& peers, cudaStream_t stream) {
     k_step_finalize_slab<<<1, 256, 0, stream>>>(partials, nblocks, budget, st, peers);
+}
+
+void launch_step_finalize_agreed(const StepPartial* partials, int nblocks, DevBudget* budget, Status* st,
+                                 const long long* agreed, cudaStream_t stream) {
+    k_step_finalize_agreed<<<1, 256, 0, stream>>>(partials, nblocks, budget, st, agreed);
+}
+
+void launch_agree_word(const Status* st, int slot, long long* agree, cudaStream_t stream) {
+    k_agree_word<<<1, 1, 0, stream>>>(st, slot, agree);
 }
 
 void launch_copy_segments(const CopyList& L, const Status* st, cudaStream_t stream) {

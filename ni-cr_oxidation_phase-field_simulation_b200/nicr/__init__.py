@@ -145,6 +145,27 @@ def lib():
     L.nicr_slabs_n_eta.argtypes = [H]
     L.nicr_slabs_stream.argtypes = [H, ctypes.c_int]
     L.nicr_slabs_stream.restype = ctypes.c_void_p
+    vp = ctypes.POINTER(ctypes.c_void_p)
+    L.nicr_slab_create.argtypes = [ctypes.POINTER(NicrConfig), ctypes.c_int, ctypes.c_int, ctypes.POINTER(H)]
+    L.nicr_slab_info.argtypes = [H, ip, ip, ip, ip, ip, ip]
+    L.nicr_slab_region.argtypes = [H, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp,
+                                   ctypes.POINTER(ctypes.c_longlong)]
+    L.nicr_slab_adjacency.argtypes = [H, ctypes.POINTER(ctypes.c_ubyte)]
+    L.nicr_colour_grains.argtypes = [ctypes.POINTER(ctypes.c_ubyte), ctypes.c_int, ctypes.c_int, ip]
+    L.nicr_slab_set_colours.argtypes = [H, ip]
+    L.nicr_slab_begin.argtypes = [H, ctypes.c_int, ctypes.c_int]
+    L.nicr_slab_scan_due.argtypes = [H, ctypes.c_int]
+    L.nicr_slab_note_step.argtypes = [H, ctypes.c_int, ctypes.c_int]
+    L.nicr_slab_failed.argtypes = [H, ip]
+    L.nicr_slab_launch.argtypes = [H]
+    L.nicr_slab_agree_word.argtypes = [H]
+    L.nicr_slab_agree_word.restype = ctypes.c_void_p
+    L.nicr_slab_commit.argtypes = [H]
+    L.nicr_slab_end.argtypes = [H, ctypes.c_int, ip]
+    L.nicr_slab_scan_candidates.argtypes = [H]
+    L.nicr_slab_scan_resolve.argtypes = [H, ip, ctypes.c_int, ip, ctypes.c_int, ip, ip]
+    L.nicr_slab_scan_apply.argtypes = [H, ip, ctypes.c_int]
+    L.nicr_slab_box_half.argtypes = [H]
     L.nicr_slabs_last_error.argtypes = [H]
     L.nicr_slabs_last_error.restype = ctypes.c_char_p
     _lib = L
