@@ -117,3 +117,63 @@ def test_ranks_rejected_trial(require_gpu):
     for r in ranks:
         r.close()
     solo.close()
+
+
+def _nccl_rank(port, q):
+    import os
+    import sys
+    import torch
+    import torch.distributed as dist
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path.insert(0, os.path.join(root, "ni-cr_oxidation_phase-field_simulation_b200"))
+    sys.path.insert(0, os.path.join(root, "tests"))
+    import nicr
+    from nicr.slab_ranks import SlabRank, TorchComm, advance, gather_budget, gather_field
+    from parity import smooth_fields
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    torch.cuda.set_device(0)
+    dist.init_process_group("nccl", rank=0, world_size=1, device_id=torch.device("cuda", 0))
+    try:
+        cfg = cfg_for()
+        r = SlabRank(cfg, 1, 0)
+        solo = nicr.Solver(cfg)
+        o, cr, p, eta = smooth_fields(solo.shape, solo.n_eta, seed=5)
+        for name, arr in (("o", o), ("cr", cr), ("p", p)):
+            solo.set(name, arr)
+            r.set_domain(name, arr)
+        for g, e in enumerate(eta):
+            solo.set("eta", e, g)
+            r.set_domain("eta", e, g)
+        solo.reset_inventory()
+        r.reset_inventory()
+        comm = TorchComm(r)
+        out = [advance(comm, n) for n in (7, 6)]
+        for n in (7, 6):
+            solo.run(n)
+        same = all(np.array_equal(gather_field(comm, f).view(np.int64), solo.get(f).view(np.int64))
+                   for f in ("o", "cr", "p", "gb"))
+        q.put((out, same, gather_budget(comm)["nuclei"], solo.budget()["nuclei"]))
+        r.close()
+        solo.close()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_torchcomm_over_nccl_single_rank(require_gpu):
+    """TorchComm over NCCL (a world of one rank on this GPU): the MIN
+    all-reduce on the library's agreement word and the stream ordering of
+    the collectives with the library's kernels."""
+    import socket
+    import torch.multiprocessing as mp
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    p = ctx.Process(target=_nccl_rank, args=(port, q))
+    p.start()
+    out, same, n1, n2 = q.get(timeout=300)
+    p.join(timeout=120)
+    assert p.exitcode == 0
+    assert [o[:2] for o in out] == [(0, 7), (0, 6)] and same and n1 == n2 > 0
