@@ -405,6 +405,64 @@ def slabs_workload(args) -> int:
     return 0
 
 
+def slab_ranks_workload(args, rank: int, world: int, local: int) -> int:
+    """One domain split along X over the ranks (one per GPU, the slab form of
+    nicr.slab_ranks over torch.distributed with NCCL): the bench workload's
+    configuration and initial state, --warmup steps, then --steps steps on the
+    run() schedule between CUDA events on each rank's library stream, the
+    maximum over ranks. Strong scaling: the domain is the same for every N.
+    At N = 1 the rate against the single handle is the protocol's cost (one
+    host loop per step, the agreement all-reduce, no halo)."""
+    import socket
+    from datetime import timedelta
+    import torch
+    import torch.distributed as dist
+    import nicr
+    from nicr.slab_ranks import SlabRank, TorchComm, advance
+    torch.cuda.set_device(local)
+    if "MASTER_ADDR" not in os.environ:
+        os.environ["MASTER_ADDR"] = "127.0.0.1"
+        with socket.socket() as sk:
+            sk.bind(("127.0.0.1", 0))
+            os.environ["MASTER_PORT"] = str(sk.getsockname()[1])
+    dist.init_process_group("nccl", rank=rank, world_size=world, timeout=timedelta(seconds=300),
+                            device_id=torch.device("cuda", local))
+    try:
+        cfg = workload_config(args.size, args.neta, device=local, seed=2)
+        cfg.precision = 1
+        slab = SlabRank(cfg, world, rank)
+        comm = TorchComm(slab)
+        shape = (args.size,) * 3
+        cr = 0.25 + np.random.default_rng(2).uniform(-0.01, 0.01, size=shape)
+        inlet = slab.own("cr")[0] if slab.x0 == 0 else None
+        inlet = comm.broadcast(inlet, src=0)
+        cr[0] = inlet
+        slab.set_domain("cr", cr)
+        slab.reset_inventory()
+        advance(comm, args.warmup)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        dist.barrier()
+        torch.cuda.synchronize()
+        e0.record(slab.stream)
+        rc, done, msg = advance(comm, args.steps)
+        e1.record(slab.stream)
+        torch.cuda.synchronize()
+        ms = torch.tensor([e0.elapsed_time(e1)], device=slab.device)
+        dist.all_reduce(ms, op=dist.ReduceOp.MAX)
+        if rank == 0:
+            cells = args.size ** 3
+            print(json.dumps({"workload": "slab-ranks", "config": f"3D {args.size}^3 split over {world} rank(s), "
+                                                                  f"{args.neta} evolving eta, fp64-fast, Ksp",
+                              "unit": "Mcell-updates/s", "n_gpus": world, "steps": args.steps, "status": rc,
+                              "value": cells * args.steps / (float(ms.item()) * 1e-3) / 1e6,
+                              "ms_per_step": float(ms.item()) / args.steps, "scaling": "strong",
+                              "halo": slab.halo}))
+        slab.close()
+    finally:
+        dist.destroy_process_group()
+    return 0
+
+
 def accuracy_workload(args) -> int:
     """The reciprocal form against the drop-in form on the bench workload over a
     long run (the run() schedule, Ksp scans included): per-field relative L-inf
@@ -464,11 +522,13 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-budget", type=float, default=60.0, help="seconds of CPU stepping for the reference")
     ap.add_argument("--slab-devices", default="", help="--workload slabs: comma-separated device per slab")
-    ap.add_argument("--workload", choices=["step", "output", "sweep", "small", "accuracy", "slabs"], default="step",
+    ap.add_argument("--workload", choices=["step", "output", "sweep", "small", "accuracy", "slabs", "slab-ranks"],
+                    default="step",
                     help="step: the headline line (default); output: VTI frame cost and overlap with stepping; "
                          "sweep: 64 uneven domains advanced as one batch; small: step rate of the small configs; "
                          "accuracy: the fast form against the drop-in form over --steps (5000 by default here); "
-                         "slabs: the domain split along X into slabs against one handle")
+                         "slabs: the domain split along X into slabs against one handle; "
+                         "slab-ranks: the domain split over the torchrun ranks (one slab per GPU)")
     ap.add_argument("--precision", type=int, default=0, help="arithmetic form of --workload sweep (0 drop-in, 1 fast)")
     args = ap.parse_args()
     if args.e2e_steps <= 0:
@@ -490,6 +550,8 @@ def main():
         return accuracy_workload(args)
     if args.workload == "slabs":
         return slabs_workload(args)
+    if args.workload == "slab-ranks":
+        return slab_ranks_workload(args, rank, world, local)
 
     import torch
     import torch.distributed as dist
