@@ -41,7 +41,7 @@ sys.path.insert(0, str(PKG))
 
 METRIC = "Mcell-updates/s at 256^3 vs plain FP64 GPU path at ≤1e-4 L∞ err; % HBM peak"
 UNIT = "Mcell-updates/s"
-KERNELS = ["step_main", "eta_update", "step_finalize", "eta_mask", "ksp_scan", "refresh", "diagnostics"]
+KERNELS = ["step_main", "eta_update", "step_finalize", "eta_mask", "ksp_scan", "refresh", "diagnostics", "step_eta"]
 
 
 def grain_diameter_for(n_grains: int, shape) -> float:
@@ -77,6 +77,8 @@ def algorithmic_bytes(kernel: str, neta: int, fast: bool) -> int:
         return (2 * neta + (3 if fast else 4)) * 8
     if kernel == "eta_mask":       # r: eta_1..N  w: gb eta_s2
         return (neta + 2) * 8
+    if kernel == "step_eta":       # the two in one launch (reciprocal form)
+        return algorithmic_bytes("step_main", neta, fast) + algorithmic_bytes("eta_update", neta, fast)
     return 0
 
 

@@ -418,7 +418,8 @@ void* nicr_stream(nicr_handle* h);
  * enabled, CUDA events bracket every kernel launch on the handle's stream;
  * nicr_profile_read returns the accumulated device time and launch count of
  * one kernel (0 step_main, 1 eta_update, 2 step_finalize, 3 eta_mask,
- * 4 ksp_scan, 5 refresh, 6 diagnostics). nicr_kernel_launches counts every
+ * 4 ksp_scan, 5 refresh, 6 diagnostics, 7 step_eta: the step kernel and the
+ * eta update in one launch, reciprocal form). nicr_kernel_launches counts every
  * kernel the handle has launched since creation. */
 int nicr_profile(nicr_handle* h, int enable);
 int nicr_profile_read(nicr_handle* h, int kernel, double* total_ms, long long* launches);

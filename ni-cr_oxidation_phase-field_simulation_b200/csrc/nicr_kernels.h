@@ -146,6 +146,18 @@ struct StepBatch {
 int launch_step_batch(BatchDomain* doms, int n, cudaStream_t stream);
 void launch_batch_group_fast(StepBatch& B, int nblocks, int dim, cudaStream_t stream);
 
+// One launch for the step kernel and the eta update of one step (reciprocal
+// form, 3D, 1..16 eta fields): the two are independent within a step, and
+// their CTAs share the SMs (see k_step_eta). ticket: one word of device
+// memory, zeroed by the launcher before each launch. Returns false (nothing
+// launched) when the form does not apply; nblocks_out receives the step
+// kernel's partial-sum count.
+bool launch_step_eta_fast(const StepParams& P, int neta, const double* o, const double* cr, const double* p,
+                          const double* gb, const double* s2, double* on, double* crn, double* pn,
+                          StepPartial* partials, const double* eta, double* eta_next, double* gb_next,
+                          double* s2_next, unsigned* ticket, Status* st, cudaStream_t stream, int* nblocks_out);
+void step_eta_prepare_fast(const StepParams& P, int neta);
+
 struct FinalizeDomain {
     const StepPartial* partials;
     int nblocks, pad;

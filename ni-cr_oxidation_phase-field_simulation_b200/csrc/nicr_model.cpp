@@ -202,7 +202,7 @@ void Model::release() {
     double* bufs[] = {o_[0], o_[1], cr_[0], cr_[1], p_[0], p_[1], gb_[0], gb_[1], s2_[0], s2_[1], eta_[0], eta_[1],
                       grain, pairs, gb_initial, muO, muCr, mo, mc};
     for (double* b : bufs) if (b) cudaFree(b);
-    void* others[] = {partials, st, bud, diag_part, diag_out, red_out, kres, d_shadow, d_ball, d_hyp, agree,
+    void* others[] = {partials, st, bud, diag_part, diag_out, red_out, kres, d_shadow, d_ball, d_hyp, agree, ticket,
                       kw.flag, kw.blocked, kw.counts, kw.list, kw.total, gw.cells, gw.parts, gw.amount_parts,
                       g_out, g_amount, g_cells};
     for (void* b : others) if (b) cudaFree(b);
@@ -216,7 +216,7 @@ void Model::release() {
     std::memset(gb_, 0, sizeof gb_); std::memset(s2_, 0, sizeof s2_); std::memset(eta_, 0, sizeof eta_);
     grain = pairs = gb_initial = muO = muCr = mo = mc = nullptr;
     partials = nullptr; st = nullptr; bud = nullptr; diag_part = diag_out = nullptr; red_out = nullptr; kres = nullptr;
-    d_shadow = d_ball = nullptr; d_hyp = nullptr; kw = KspWork{}; h_st = nullptr; stream = nullptr; agree = nullptr;
+    d_shadow = d_ball = nullptr; d_hyp = nullptr; kw = KspWork{}; h_st = nullptr; stream = nullptr; agree = nullptr; ticket = nullptr;
     gw = GrainWork{}; g_out = nullptr; g_amount = nullptr; g_cells = nullptr;
 }
 
@@ -883,10 +883,33 @@ void Model::complete_step(int nb, bool finalize) {
     if (advance_eta) { ecur ^= 1; gcur ^= 1; }
 }
 
+bool Model::fused_step() const {
+    static int v = -1;
+    if (v < 0) {
+        const char* e = getenv("NICR_FUSED");
+        v = (e && e[0] == '1') ? 1 : 0;
+    }
+    return v == 1 && sp.fast && dim == 3 && advance_eta && !is_slab && neta >= 1 && neta <= 16;
+}
+
 void Model::enqueue_step() {
     prepare_step();
     const BatchDomain d = step_desc();
     int nb = 0;
+    if (fused_step()) {
+        if (!ticket) ticket = dalloc_t<unsigned>(1);
+        size_t e = prof_begin();
+        launch_step_eta_fast(sp, neta, d.o, d.cr, d.p, d.gb, d.s2, d.on, d.crn, d.pn, partials, eta_[ecur],
+                             eta_[ecur ^ 1], gb_[gcur ^ 1], s2_[gcur ^ 1], ticket, st, stream, &nb);
+        prof_end(K_STEP_ETA, e, 1);
+        e = prof_begin();
+        launch_step_finalize(partials, nb, bud, st, 0, stream);
+        prof_end(K_FINALIZE, e, 1);
+        cur ^= 1;
+        ecur ^= 1;
+        gcur ^= 1;
+        return;
+    }
     const size_t e = prof_begin();
     launch_step_main(sp, d.o, d.cr, d.p, d.gb, d.s2, d.on, d.crn, d.pn, partials, st, stream, &nb);
     prof_end(K_STEP_MAIN, e, 1);
@@ -1038,6 +1061,10 @@ void Model::launch_step_pair() {
             if (!q.exec) { pg = &q; break; }
         if (!pg) throw Error(NICR_ERR_STATE, "step graph slots exhausted");
         step_kernels_prepare(sp);
+        if (fused_step()) {
+            if (!ticket) ticket = dalloc_t<unsigned>(1);
+            step_eta_prepare_fast(sp, neta);   // kernel attributes outside the capture
+        }
         const long long l0 = launches;
         cudaGraph_t graph = nullptr;
         check_cuda(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
@@ -1260,7 +1287,7 @@ void Model::grain_stats(nicr_grain_stats* out, long long* cells, double* amount)
 // ------------------------------------------------------------------ measurement hooks
 const char* Model::kernel_name(int k) {
     static const char* names[K_COUNT] = {"step_main", "eta_update", "step_finalize", "eta_mask", "ksp_scan",
-                                         "refresh", "diagnostics"};
+                                         "refresh", "diagnostics", "step_eta"};
     return (k >= 0 && k < K_COUNT) ? names[k] : "?";
 }
 

@@ -21,6 +21,18 @@ void launch_eta_update_fast(const StepParams& P, int neta, const double* eta, co
     launch_eta_form<true>(P, neta, eta, s2, p, eta_next, gb_next, s2_next, st, stream);
 }
 
+bool launch_step_eta_fast(const StepParams& P, int neta, const double* o, const double* cr, const double* p,
+                          const double* gb, const double* s2, double* on, double* crn, double* pn,
+                          StepPartial* partials, const double* eta, double* eta_next, double* gb_next,
+                          double* s2_next, unsigned* ticket, Status* st, cudaStream_t stream, int* nblocks_out) {
+    return launch_step_eta_form<true>(P, neta, o, cr, p, gb, s2, on, crn, pn, partials, eta, eta_next, gb_next,
+                                      s2_next, ticket, st, stream, nblocks_out);
+}
+
+void step_eta_prepare_fast(const StepParams& P, int neta) {
+    if (P.g.dim == 3) step_eta_prepare<true>(neta);
+}
+
 void launch_batch_group_fast(StepBatch& B, int nblocks, int dim, cudaStream_t stream) {
     if (dim == 3) launch_batch_group<3, TA3, TB3, 2, true>(B, nblocks, stream);
     else launch_batch_group<2, TA2, TB2, 4, true>(B, nblocks, stream);

@@ -697,6 +697,112 @@ static void launch_eta_march(const StepParams& P, const double* eta, const doubl
     }
 }
 
+// Horizontal fusion of the step kernel and the eta march (3D): within a step
+// the two are independent (the step kernel reads o, cr, phi, gb, eta_s2 and
+// writes the trial o, cr, phi; the eta update reads eta and the current phi
+// and writes the next eta, gb, eta_s2), and the step kernel is bound by FP64
+// issue while the march waits on HBM. Each CTA draws a ticket and takes the
+// step tile or the eta column block the ticket names; the tickets alternate
+// between the two kinds while both last, so the SMs run both kinds at once
+// and their pipes overlap. The CTAs compute what the separate kernels compute
+// (the same bodies; step partial sums at the step kernel's block index).
+// Opt-in (NICR_FUSED=1): at 256^3 with 8 fields it measured 1.122 ms per step
+// against 1.129 ms for the two launches. Both kernels hold 2 CTAs/SM at 128
+// registers and each is bound by the latency its own warps hide; an SM that
+// runs one CTA of each gives each kind half the warps, which costs about what
+// the overlap gains.
+struct FusedStep {
+    int n_step, n_eta;     // CTAs of each kind
+    int gx_s, gy_s;        // step grid (x, y; z = X chunks)
+    int gx_e, gy_e;        // eta march grid (x, y; z = X chunks)
+    unsigned* ticket;      // zero at launch
+};
+template <bool FAST, int N>
+__global__ void __launch_bounds__(TA3 * TB3, 2)
+k_step_eta(const StepParams P, const FusedStep F, const double* __restrict__ o, const double* __restrict__ cr,
+           const double* __restrict__ p, const double* __restrict__ gb, const double* __restrict__ s2,
+           double* __restrict__ on, double* __restrict__ crn, double* __restrict__ pn,
+           StepPartial* __restrict__ partials, const double* __restrict__ eta, double* __restrict__ eta_next,
+           double* __restrict__ gb_next, double* __restrict__ s2_next, Status* st) {
+    __shared__ int s_ticket;
+    if (threadIdx.x == 0 && threadIdx.y == 0) s_ticket = (int)atomicAdd(F.ticket, 1u);
+    __syncthreads();
+    const int t = s_ticket, pairs = min(F.n_step, F.n_eta);
+    int role, idx;
+    if (t < 2 * pairs) {
+        role = t & 1;
+        idx = t >> 1;
+    } else {
+        role = F.n_step > F.n_eta ? 0 : 1;
+        idx = pairs + (t - 2 * pairs);
+    }
+    if (role == 0) {
+        const int bx = idx % F.gx_s, r = idx / F.gx_s;
+        StepKernel<3, TA3, TB3, FAST>::run(P, o, cr, p, gb, s2, on, crn, pn, partials, st, bx, r % F.gy_s,
+                                           r / F.gy_s, idx);
+    } else {
+        const int bx = idx % F.gx_e, r = idx / F.gx_e;
+        eta_march_body<3, FAST, N>(P, N, eta, p, eta_next, gb_next, s2_next, st, bx, r % F.gy_e, r / F.gy_e);
+    }
+}
+
+template <bool FAST, int N>
+static void launch_step_eta_n(const StepParams& P, const double* o, const double* cr, const double* p,
+                              const double* gb, const double* s2, double* on, double* crn, double* pn,
+                              StepPartial* partials, const double* eta, double* eta_next, double* gb_next,
+                              double* s2_next, unsigned* ticket, Status* st, cudaStream_t stream, int* nblocks_out) {
+    using T = Tile<3, TA3, TB3>;
+    const Grid& g = P.g;
+    const dim3 gs = step_grid<3, TA3, TB3>(P);
+    const dim3 ge((g.nb + 31) / 32, (g.na + 7) / 8, (P.x_hi - P.x_lo + P.xchunk - 1) / P.xchunk);
+    FusedStep F;
+    F.gx_s = (int)gs.x; F.gy_s = (int)gs.y; F.n_step = (int)(gs.x * gs.y * gs.z);
+    F.gx_e = (int)ge.x; F.gy_e = (int)ge.y; F.n_eta = (int)(ge.x * ge.y * ge.z);
+    F.ticket = ticket;
+    ensure_smem_attr((const void*)k_step_eta<FAST, N>, (int)T::SMEM_BYTES);
+    cudaMemsetAsync(ticket, 0, sizeof(unsigned), stream);
+    k_step_eta<FAST, N><<<F.n_step + F.n_eta, dim3(TB3, TA3), T::SMEM_BYTES, stream>>>(
+        P, F, o, cr, p, gb, s2, on, crn, pn, partials, eta, eta_next, gb_next, s2_next, st);
+    if (nblocks_out) *nblocks_out = F.n_step;
+}
+
+template <bool FAST>
+static void step_eta_prepare(int neta) {
+    using T = Tile<3, TA3, TB3>;
+    switch (neta) {
+#define NICR_FUSED_PREP(n) \
+    case n: ensure_smem_attr((const void*)k_step_eta<FAST, n>, (int)T::SMEM_BYTES); break;
+        NICR_FUSED_PREP(1) NICR_FUSED_PREP(2) NICR_FUSED_PREP(3) NICR_FUSED_PREP(4) NICR_FUSED_PREP(5)
+        NICR_FUSED_PREP(6) NICR_FUSED_PREP(7) NICR_FUSED_PREP(8) NICR_FUSED_PREP(9) NICR_FUSED_PREP(10)
+        NICR_FUSED_PREP(11) NICR_FUSED_PREP(12) NICR_FUSED_PREP(13) NICR_FUSED_PREP(14) NICR_FUSED_PREP(15)
+        NICR_FUSED_PREP(16)
+#undef NICR_FUSED_PREP
+        default: break;
+    }
+}
+
+template <bool FAST>
+static bool launch_step_eta_form(const StepParams& P, int neta, const double* o, const double* cr, const double* p,
+                                 const double* gb, const double* s2, double* on, double* crn, double* pn,
+                                 StepPartial* partials, const double* eta, double* eta_next, double* gb_next,
+                                 double* s2_next, unsigned* ticket, Status* st, cudaStream_t stream,
+                                 int* nblocks_out) {
+    if (P.g.dim != 3 || P.err_slot >= 0) return false;
+    switch (neta) {
+#define NICR_FUSED_CASE(n)                                                                                   \
+    case n:                                                                                                  \
+        launch_step_eta_n<FAST, n>(P, o, cr, p, gb, s2, on, crn, pn, partials, eta, eta_next, gb_next, s2_next, \
+                                   ticket, st, stream, nblocks_out);                                         \
+        return true;
+        NICR_FUSED_CASE(1) NICR_FUSED_CASE(2) NICR_FUSED_CASE(3) NICR_FUSED_CASE(4) NICR_FUSED_CASE(5)
+        NICR_FUSED_CASE(6) NICR_FUSED_CASE(7) NICR_FUSED_CASE(8) NICR_FUSED_CASE(9) NICR_FUSED_CASE(10)
+        NICR_FUSED_CASE(11) NICR_FUSED_CASE(12) NICR_FUSED_CASE(13) NICR_FUSED_CASE(14) NICR_FUSED_CASE(15)
+        NICR_FUSED_CASE(16)
+#undef NICR_FUSED_CASE
+        default: return false;
+    }
+}
+
 // Dispatch to the compile-time field counts 1..16; false when N is larger.
 template <int DIM, bool FAST>
 static bool eta_march_dispatch(int neta, const StepParams& P, const double* eta, const double* p, double* eta_next,
