@@ -59,7 +59,7 @@ FUSED_CHILD = textwrap.dedent("""
     sys.path.insert(0, root + "/ni-cr_oxidation_phase-field_simulation_b200"); sys.path.insert(0, root + "/tests")
     import nicr
     from parity import smooth_fields
-    cfg = nicr.make_config(3, nx=48, ny=32, nz=64, grains=1, grain_evolution=1, grain_diameter_grid=20.,
+    cfg = nicr.make_config(3, nx=48, ny=32, nz=64, grains=1, grain_evolution=1, grain_diameter_grid=28.,
                            bounds="legacy", bc="concentration", nucleation="ksp", dt=1e-12, radius_grid=2.5,
                            nucleation_period=5e-12, precision=1)
     sol = nicr.Solver(cfg)
