@@ -67,3 +67,45 @@ def test_version_strings():
     with pytest.raises(nicr.NicrError) as e:
         nicr.parse_args(2, ["--version"])
     assert e.value.message.strip() == "mpi-eta-v1"
+
+
+def _dsatur(adj, k):
+    """DSatur as nicr_colour_grains states it: most distinct coloured
+    neighbour colours, then most neighbours, then lowest index; the lowest
+    colour no coloured neighbour has, else the one fewest of them have."""
+    ng = len(adj)
+    colour = [-1] * ng
+    degree = [int(sum(row)) for row in adj]
+    for _ in range(ng):
+        best, bsat = -1, -1
+        for a in range(ng):
+            if colour[a] >= 0:
+                continue
+            sat = len({colour[b] for b in range(ng) if adj[a][b] and colour[b] >= 0})
+            if best < 0 or sat > bsat or (sat == bsat and degree[a] > degree[best]):
+                best, bsat = a, sat
+        count = [0] * k
+        for b in range(ng):
+            if adj[best][b] and colour[b] >= 0:
+                count[colour[b]] += 1
+        colour[best] = min(range(k), key=lambda q: (count[q], q))
+    return colour
+
+
+@pytest.mark.parametrize("ng,density,k", [(12, 0.3, 4), (40, 0.25, 8), (64, 0.12, 8), (30, 0.6, 5), (1, 0.0, 3)])
+def test_colour_grains_is_dsatur(ng, density, k):
+    """The grain colouring of the coloured eta initialisation (host code, no
+    GPU): DSatur with the stated tie rules on random symmetric graphs."""
+    import ctypes
+    import numpy as np
+    L = nicr.lib()
+    rng = np.random.default_rng(ng * 7 + k)
+    upper = np.triu(rng.random((ng, ng)) < density, 1)
+    adj = (upper | upper.T).astype(np.uint8)
+    out = np.zeros(ng, dtype=np.int32)
+    rc = L.nicr_colour_grains(adj.ctypes.data_as(ctypes.POINTER(ctypes.c_ubyte)), ng, k,
+                              out.ctypes.data_as(ctypes.POINTER(ctypes.c_int)))
+    assert rc == 0
+    assert out.tolist() == _dsatur(adj.tolist(), k)
+    if k >= ng:
+        assert not any(adj[a, b] and out[a] == out[b] for a in range(ng) for b in range(ng))
