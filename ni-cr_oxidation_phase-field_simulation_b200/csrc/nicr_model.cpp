@@ -1033,11 +1033,11 @@ bool Model::ksp_due(const RunPlan& r, int s) const {
     return double(n) * c.dt + 1.e-12 * c.nucleation_period >= r.next;
 }
 
-// Step-pair graphs. Replaying a captured pair of steps costs one host launch
+// Step graphs. Replaying a captured run of 2..16 steps costs one host launch
 // instead of two or three per step, which decides the step rate of small
-// domains (a 2D 128^2 step is a few microseconds of GPU work). A pair returns
-// the buffer parity to where it started, so one graph per starting parity
-// serves every pair; the kernels read their run constants from their
+// domains (a 2D 128^2 step is a few microseconds of GPU work). An even run
+// returns the buffer parity to where it started, so one graph per length and
+// starting parity serves every run; the kernels read their run constants from their
 // parameters and the batch-stop flag from device memory, both unchanged
 // between replays. Not used while profiling (the per-kernel events) or when
 // NICR_GRAPHS=0.
@@ -1050,9 +1050,9 @@ bool Model::graphs_enabled() const {
     return v == 1 && !prof_on;
 }
 
-void Model::launch_step_pair() {
+void Model::launch_step_group(int n) {
     prepare_step();   // a stale eta mask is rebuilt outside the graph
-    const int key = cur | (ecur << 1) | (gcur << 2);
+    const int key = cur | (ecur << 1) | (gcur << 2) | (n << 3);
     PairGraph* pg = nullptr;
     for (auto& q : pair_graphs)
         if (q.exec && q.key == key) pg = &q;
@@ -1068,8 +1068,7 @@ void Model::launch_step_pair() {
         const long long l0 = launches;
         cudaGraph_t graph = nullptr;
         check_cuda(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
-        enqueue_step();
-        enqueue_step();
+        for (int q = 0; q < n; ++q) enqueue_step();
         check_cuda(cudaStreamEndCapture(stream, &graph), "cudaStreamEndCapture");
         const cudaError_t e = cudaGraphInstantiate(&pg->exec, graph, 0);
         cudaGraphDestroy(graph);
@@ -1077,10 +1076,23 @@ void Model::launch_step_pair() {
         pg->key = key;
         pg->kernels = launches - l0;
         launches = l0;   // nothing ran while capturing; each replay counts them
-        // the two captured enqueue_step calls toggled the parity twice: back at key
+        // the captured enqueue_step calls toggled the parity an even number of times: back at key
     }
     check_cuda(cudaGraphLaunch(pg->exec, stream), "cudaGraphLaunch");
     launches += pg->kernels;
+}
+
+// The longest captured run (16, 8, 4 or 2 steps) that starts at step s of
+// plan r, fits in the batch and has no Ksp scan due after its first step;
+// 1 when none does (a plain launch).
+int Model::group_length(const RunPlan& r, int s, int nsteps) const {
+    for (int g : {16, 8, 4, 2}) {
+        if (s + g > nsteps) continue;
+        bool ok = true;
+        for (int j = 1; j < g && ok; ++j) ok = !ksp_due(r, s + j);
+        if (ok) return g;
+    }
+    return 1;
 }
 
 int Model::step(int nsteps, int* completed) {
@@ -1091,13 +1103,10 @@ int Model::step(int nsteps, int* completed) {
     run_begin(r, nsteps, false);
     const bool graphs = graphs_enabled();
     for (int s = 0; s < nsteps;) {
-        if (graphs && s + 1 < nsteps) {
-            launch_step_pair();
-            s += 2;
-        } else {
-            enqueue_step();
-            ++s;
-        }
+        const int g = graphs ? group_length(r, s, nsteps) : 1;
+        if (g > 1) launch_step_group(g);
+        else enqueue_step();
+        s += g;
     }
     return run_end(r, completed);
 }
@@ -1111,14 +1120,11 @@ int Model::run(int nsteps, int* completed) {
     const bool graphs = graphs_enabled();
     for (int s = 0; s < nsteps;) {
         run_pre_step(r, s);
-        if (graphs && s + 1 < nsteps && !ksp_due(r, s + 1)) {
-            launch_step_pair();
-            run_pre_step(r, s + 1);   // no scan is due: records the schedule entry only
-            s += 2;
-        } else {
-            enqueue_step();
-            ++s;
-        }
+        const int g = graphs ? group_length(r, s, nsteps) : 1;
+        if (g > 1) launch_step_group(g);
+        else enqueue_step();
+        for (int j = 1; j < g; ++j) run_pre_step(r, s + j);   // no scan is due: schedule entries only
+        s += g;
     }
     return run_end(r, completed);
 }

@@ -247,14 +247,16 @@ private:
     size_t prof_begin();
     void prof_end(int k, size_t e0, int kernels);
 
-    // captured step pairs, one per starting buffer parity (cur, ecur, gcur)
+    // captured runs of 2, 4, 8 or 16 steps, one per length and starting
+    // buffer parity (cur, ecur, gcur)
     struct PairGraph {
         cudaGraphExec_t exec = nullptr;
         int key = 0;
         long long kernels = 0;
     };
-    PairGraph pair_graphs[8];
-    void launch_step_pair();
+    PairGraph pair_graphs[32];
+    void launch_step_group(int nsteps);
+    int group_length(const RunPlan& r, int s, int nsteps) const;
 
     void release();
     double* dalloc(size_t n);
