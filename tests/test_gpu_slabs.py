@@ -235,3 +235,24 @@ def test_grain_stats_and_vti_match(require_gpu, tmp_path):
         solo.write_vti(tmp_path / "solo.vti")
         assert (tmp_path / "slabs.vti").read_bytes() == (tmp_path / "solo.vti").read_bytes()
     solo.close()
+
+
+@pytest.mark.parametrize("kw", [dict(bc="mu", ck="off"), dict(bc="closed"), dict(oxygen_diffusion=0),
+                                dict(grains=0, nucleation="center", radius_grid=6.0),
+                                dict(grain_evolution=0, bounds="stop")],
+                         ids=["bc-mu-ck-off", "bc-closed", "o-off", "single-crystal-centre", "static-stop"])
+def test_slab_modes(require_gpu, kw):
+    """The boundary and physics modes around the seams: the mu boundary's
+    surface flux (slab 0 only), closed boundaries, O transport off, a single
+    crystal whose centre seed spans slabs, static grains with bounds=stop."""
+    cfg = grains_cfg(**kw)
+    solo = nicr.Solver(cfg)
+    with nicr.Slabs(cfg, 3) as s:
+        inject(solo, 8, solo.n_eta)
+        inject(s, 8, solo.n_eta)
+        for chunk in (5, 6):
+            rc, done = s.run(chunk, check=False)
+            rc1, done1 = solo.run(chunk, check=False)
+            assert (rc, done) == (rc1, done1)
+        assert_same(s, solo, solo.n_eta, str(kw))
+    solo.close()
