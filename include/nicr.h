@@ -406,6 +406,20 @@ int nicr_slab_scan_resolve(nicr_handle* h, const int* pre, int npre, int* out, i
 int nicr_slab_scan_apply(nicr_handle* h, const int* list, int n);
 int nicr_slab_box_half(const nicr_handle* h);
 
+/* Learned surrogate building blocks (no counterpart in the reference): 3x3x3
+ * convolutions, stride 1, zero padding 1, on the BF16 tensor cores with FP32
+ * accumulation, on device pointers and the caller's CUDA stream. x: NDHWC
+ * BF16 (n, d, h, w, cin); w: BF16 [cout][27][cin], tap = (dz+1)*9 +
+ * (dy+1)*3 + (dx+1); y, dw: FP32. n*d*h*w a multiple of 64; cin and cout
+ * multiples of 16. nicr_conv3d_fwd: y[v][co] = sum x[v+off(tap)][ci]
+ * w[co][tap][ci]. nicr_conv3d_wgrad: dw[co][tap][ci] = sum_v dy[v][co]
+ * x[v+off(tap)][ci] (dy: BF16 NDHWC with cout channels). The data gradient
+ * is nicr_conv3d_fwd of dy with w'[ci][tap][co] = w[co][26-tap][ci]. */
+int nicr_conv3d_fwd(const void* x, const void* w, float* y, int n, int d, int h, int w_, int cin, int cout,
+                    void* stream);
+int nicr_conv3d_wgrad(const void* x, const void* dy, float* dw, int n, int d, int h, int w_, int cin, int cout,
+                      void* stream);
+
 /* The solver program: the reference's run()/main() for dim 2 or 3
  * (2D:1161-1246, 3S:1309-1395), argv as the reference's executable takes it.
  * Returns the process exit code. */

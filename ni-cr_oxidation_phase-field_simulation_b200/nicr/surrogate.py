@@ -1,0 +1,398 @@
+"""The learned surrogate, first stage: a 3-level 3D U-Net over the fields
+(c_O, c_Cr, phi, GB indicator) that predicts the state K steps ahead, trained
+on trajectories the solver itself generates. Every convolution runs on the
+library's BF16 tensor-core kernels (nicr_conv3d_fwd for the forward pass and
+the data gradient, nicr_conv3d_wgrad for the weight gradient; FP32
+accumulation); the elementwise parts (bias, ReLU, pooling, upsampling, skip
+concatenation, the loss and the optimiser) are torch operations on the same
+stream. Activations are channels-last (NDHWC) BF16; the weights' master copy
+is FP32. JumpStepper applies the trained network to a Solver: each jump is
+accepted only if the FP64 mass budget holds and a short plain re-check
+agrees, otherwise the plain steps run.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+FIELDS = ("o", "cr", "p", "gb")
+PAD = 16   # channels are padded to a multiple of 16 for the tensor-core tiles
+
+
+def _lib():
+    import ctypes
+    from . import lib
+    L = lib()
+    if not getattr(L, "_conv_bound", False):
+        vp, i = ctypes.c_void_p, ctypes.c_int
+        for f in ("nicr_conv3d_fwd", "nicr_conv3d_wgrad"):
+            getattr(L, f).argtypes = [vp, vp, vp, i, i, i, i, i, i, vp]
+        L._conv_bound = True
+    return L
+
+
+def _check(rc, what):
+    if rc != 0:
+        raise RuntimeError(f"{what} failed with status {rc}")
+
+
+def conv3d_raw(x, w_bf16):
+    """y = conv(x, w): x (n, d, h, w, cin) BF16, w (cout, 27, cin) BF16 -> FP32."""
+    import torch
+    n, d, h, wd, cin = x.shape
+    cout = w_bf16.shape[0]
+    y = torch.empty((n, d, h, wd, cout), dtype=torch.float32, device=x.device)
+    _check(_lib().nicr_conv3d_fwd(x.data_ptr(), w_bf16.data_ptr(), y.data_ptr(), n, d, h, wd, cin, cout,
+                                  torch.cuda.current_stream(x.device).cuda_stream), "nicr_conv3d_fwd")
+    return y
+
+
+def conv3d_wgrad_raw(x, dy):
+    """dw[co][tap][ci] = sum_v dy[v][co] x[v + off(tap)][ci] (FP32)."""
+    import torch
+    n, d, h, wd, cin = x.shape
+    cout = dy.shape[-1]
+    dw = torch.empty((cout, 27, cin), dtype=torch.float32, device=x.device)
+    _check(_lib().nicr_conv3d_wgrad(x.data_ptr(), dy.data_ptr(), dw.data_ptr(), n, d, h, wd, cin, cout,
+                                    torch.cuda.current_stream(x.device).cuda_stream), "nicr_conv3d_wgrad")
+    return dw
+
+
+def _make_fn():
+    import torch
+
+    class Conv3dFn(torch.autograd.Function):
+        """3x3x3 convolution on the library's kernels; x BF16 NDHWC, w FP32
+        master weights (cast to BF16 for the tensor cores)."""
+
+        @staticmethod
+        def forward(ctx, x, w):
+            xb = x.contiguous()
+            wb = w.to(torch.bfloat16).contiguous()
+            ctx.save_for_backward(xb, wb)
+            return conv3d_raw(xb, wb)
+
+        @staticmethod
+        def backward(ctx, gy):
+            xb, wb = ctx.saved_tensors
+            gyb = gy.to(torch.bfloat16).contiguous()
+            # data gradient: the forward convolution of dy with w'[ci][tap][co] = w[co][26 - tap][ci]
+            wt = wb.flip(1).permute(2, 1, 0).contiguous()
+            gx = conv3d_raw(gyb, wt).to(xb.dtype)
+            gw = conv3d_wgrad_raw(xb, gyb)
+            return gx, gw
+
+    return Conv3dFn
+
+
+_FN = None
+
+
+def conv3d(x, w):
+    global _FN
+    if _FN is None:
+        _FN = _make_fn()
+    return _FN.apply(x, w)
+
+
+def _module_classes():
+    import torch
+    import torch.nn as nn
+
+    class Conv(nn.Module):
+        def __init__(self, cin, cout, relu=True):
+            super().__init__()
+            self.w = nn.Parameter(torch.randn(cout, 27, cin) * math.sqrt(2.0 / (27 * cin)))
+            self.b = nn.Parameter(torch.zeros(cout))
+            self.relu = relu
+
+        def forward(self, x):
+            y = conv3d(x, self.w) + self.b
+            return (torch.relu(y) if self.relu else y).to(torch.bfloat16)
+
+    def pool(x):   # 2x2x2 average, NDHWC
+        n, d, h, w, c = x.shape
+        return x.float().view(n, d // 2, 2, h // 2, 2, w // 2, 2, c).mean(dim=(2, 4, 6)).to(torch.bfloat16)
+
+    def up(x):     # nearest 2x, NDHWC
+        return x.repeat_interleave(2, 1).repeat_interleave(2, 2).repeat_interleave(2, 3)
+
+    class UNet3d(nn.Module):
+        """3 levels, `base` channels at full resolution (x2 per level)."""
+
+        def __init__(self, fields: int = 4, base: int = 32):
+            super().__init__()
+            c1, c2, c3 = base, 2 * base, 4 * base
+            self.fields = fields
+            self.enc1 = nn.Sequential(Conv(PAD, c1), Conv(c1, c1))
+            self.enc2 = nn.Sequential(Conv(c1, c2), Conv(c2, c2))
+            self.mid = nn.Sequential(Conv(c2, c3), Conv(c3, c3))
+            self.dec2 = nn.Sequential(Conv(c3 + c2, c2), Conv(c2, c2))
+            self.dec1 = nn.Sequential(Conv(c2 + c1, c1), Conv(c1, c1))
+            self.head = Conv(c1, PAD, relu=False)
+
+        def forward(self, x):
+            """x: (n, d, h, w, fields) FP32, normalised -> the predicted change (same shape)."""
+            pad = torch.zeros(x.shape[:-1] + (PAD - x.shape[-1],), dtype=x.dtype, device=x.device)
+            h0 = torch.cat([x, pad], dim=-1).to(torch.bfloat16)
+            e1 = self.enc1(h0)
+            e2 = self.enc2(pool(e1))
+            m = self.mid(pool(e2))
+            d2 = self.dec2(torch.cat([up(m), e2], dim=-1))
+            d1 = self.dec1(torch.cat([up(d2), e1], dim=-1))
+            return self.head(d1).float()[..., : self.fields]
+
+    return Conv, UNet3d
+
+
+def unet(fields: int = 4, base: int = 32):
+    return _module_classes()[1](fields, base)
+
+
+# ------------------------------------------------------------------ data
+def trajectory_configs(n: int, size: int, first_seed: int = 100, **kw):
+    """Static-Voronoi runs with the batching form's parameter draws (bulk Cr
+    U[0.15, 0.30], O supply U[0.5, 1.0] x the default layerO, Ksp log-uniform
+    over a decade around the default, 8-32 grains), one seed per run; kw
+    overrides other configuration fields."""
+    from . import default_config, make_config
+    d0 = default_config(3)
+    out = []
+    for k in range(n):
+        rng = np.random.default_rng(first_seed + k)
+        grains = int(rng.integers(8, 33))
+        d = (6.0 * size ** 3 / (math.pi * grains)) ** (1.0 / 3.0)
+        out.append(make_config(3, nx=size, ny=size, nz=size, grains=1, grain_evolution=0,
+                               grain_diameter_grid=d, random_seed=first_seed + k, bc="concentration",
+                               bounds="legacy", nucleation="ksp", bulk_cr=float(rng.uniform(0.15, 0.30)),
+                               layer_o=d0.layer_o * float(rng.uniform(0.5, 1.0)),
+                               ksp=d0.ksp * 10.0 ** float(rng.uniform(-1.0, 1.0)), **kw))
+    return out
+
+
+def trajectories(cfgs, steps: int, every: int, device: int = 0):
+    """Snapshots (fields o, cr, p, gb) of each run every `every` steps:
+    a tensor (runs, steps // every + 1, size, size, size, 4) on the GPU."""
+    import torch
+    from . import Solver
+    runs = []
+    for c in cfgs:
+        c.device = device
+        s = Solver(c)
+        snaps = []
+        for t in range(steps // every + 1):
+            if t:
+                s.run(every)
+            snaps.append(np.stack([s.get(f) for f in FIELDS], axis=-1))
+        s.close()
+        runs.append(torch.tensor(np.stack(snaps), dtype=torch.float32, device=f"cuda:{device}"))
+    return torch.stack(runs)
+
+
+class Normaliser:
+    """Per-field shift/scale of the states and of their K-step changes."""
+
+    def __init__(self, snaps, k: int):
+        flat = snaps.reshape(-1, snaps.shape[-1])
+        self.mu, self.sd = flat.mean(0), flat.std(0).clamp_min(1e-12)
+        delta = (snaps[:, k:] - snaps[:, :-k]).reshape(-1, snaps.shape[-1])
+        self.dsd = delta.std(0).clamp_min(1e-12)
+        self.k = k
+
+    def inputs(self, x):
+        return (x - self.mu) / self.sd
+
+    def target(self, x0, x1):
+        return (x1 - x0) / self.dsd
+
+    def apply(self, x0, pred):
+        return x0 + pred * self.dsd
+
+
+def train(model, snaps, k: int, iters: int = 200, batch: int = 2, lr: float = 2e-3, seed: int = 0):
+    """Adam on MSE of the normalised K-step change; returns (normaliser, losses)."""
+    import torch
+    torch.manual_seed(seed)
+    norm = Normaliser(snaps, k)
+    x0 = snaps[:, :-k].reshape((-1,) + snaps.shape[2:])
+    x1 = snaps[:, k:].reshape((-1,) + snaps.shape[2:])
+    opt = torch.optim.Adam(model.parameters(), lr=lr)
+    g = torch.Generator(device="cpu").manual_seed(seed)
+    losses = []
+    for _ in range(iters):
+        idx = torch.randint(0, x0.shape[0], (batch,), generator=g)
+        a, b = x0[idx], x1[idx]
+        loss = torch.mean((model(norm.inputs(a)) - norm.target(a, b)) ** 2)
+        opt.zero_grad()
+        loss.backward()
+        opt.step()
+        losses.append(loss.item())
+    return norm, losses
+
+
+def predict(model, norm, x0, chunk: int = 4):
+    """The network's state K steps after x0 (n, d, h, w, fields), FP32."""
+    import torch
+    out = []
+    with torch.no_grad():
+        for i in range(0, x0.shape[0], chunk):
+            a = x0[i:i + chunk]
+            out.append(norm.apply(a, model(norm.inputs(a))))
+    return torch.cat(out)
+
+
+def relative_errors(model, norm, snaps, k: int):
+    """Relative L2 error of the K-step change predicted by the network, by
+    persistence (no change: 1 by definition) and by linear extrapolation of
+    the previous K steps, over the fields that change (c_O, c_Cr, phi)."""
+    import torch
+    x0 = snaps[:, k:-k].reshape((-1,) + snaps.shape[2:])
+    xm = snaps[:, :-2 * k].reshape((-1,) + snaps.shape[2:])
+    x1 = snaps[:, 2 * k:].reshape((-1,) + snaps.shape[2:])
+    f = slice(0, 3)
+    ref = torch.linalg.vector_norm(((x1 - x0) / norm.dsd)[..., f])
+    pred = predict(model, norm, x0)
+    e = lambda y: float(torch.linalg.vector_norm(((y - x1) / norm.dsd)[..., f]) / ref)
+    return {"network": e(pred), "persistence": e(x0), "linear": e(2 * x0 - xm)}
+
+
+# ------------------------------------------------------------------ jumps
+class JumpStepper:
+    """Advances a Solver by plain steps and surrogate jumps of K steps.
+
+    A jump is tried only where no Ksp scan falls inside it. It runs: `probe`
+    plain steps (which measure the per-step change and the FP64 rate of
+    change of total O and Cr), the network's proposal for K steps ahead, the
+    mass-budget gate, and `probe` plain re-check steps from the proposal.
+
+    Mass budget: the proposal's change of total O and of total Cr must equal
+    K x the measured FP64 rate up to a correction c x |change| per cell with
+    |c| <= mass_tol; the correction is then applied, so the accepted state
+    carries exactly the extrapolated budget (summed in FP64), and the amounts
+    a jump adds are kept in `ledger` so that the solver's budget still
+    closes. Re-check: the per-step change of the re-check steps may be at
+    most recheck_factor x that of the probe steps (an off-manifold proposal
+    relaxes fast in its first plain steps). A jump failing either gate is
+    rolled back from a checkpoint and K plain steps run instead.
+
+    The stepper keeps the simulated clock itself: the solver's own step
+    counter does not see jumps, so plain stepping uses nicr_step and the Ksp
+    scans fire here (before the step whose physical time reaches the next
+    scan time, as nicr_run fires them).
+    """
+
+    def __init__(self, solver, model, norm, k: int, probe: int = 2, mass_tol: float = 0.05,
+                 recheck_factor: float = 4.0, workdir=None):
+        import tempfile
+        from . import NUCLEATION
+        self.s, self.model, self.norm, self.k, self.probe = solver, model, norm, k, probe
+        self.mass_tol, self.recheck_factor = mass_tol, recheck_factor
+        c = solver.cfg
+        self.dt, self.period = c.dt, c.nucleation_period
+        self.ksp = c.nucleation == NUCLEATION["ksp"]
+        self.t = int(solver.info().steps_done)
+        self.next_scan = self.period
+        while self._due(self.t):
+            self.next_scan += self.period
+        self._tmp = tempfile.TemporaryDirectory(dir=workdir)
+        self.ckpt = f"{self._tmp.name}/jump.ckpt"
+        self.ledger = {"o": 0.0, "cr": 0.0}
+        self.counts = {"accepted": 0, "rejected_mass": 0, "rejected_recheck": 0, "plain_steps": 0,
+                       "jumped_steps": 0, "scans": 0}
+
+    def _due(self, t: int) -> bool:
+        """A scan fires before step t + 1."""
+        return self.ksp and (t + 1) * self.dt + 1e-12 * self.period >= self.next_scan
+
+    def _steps_free(self) -> int:
+        """Steps that can run before the next scan."""
+        if not self.ksp:
+            return 1 << 60
+        m = 0
+        while not self._due(self.t + m):
+            m += 1
+        return m
+
+    def plain(self, n: int):
+        while n > 0:
+            if self._due(self.t):
+                self.s.nucleate()
+                self.counts["scans"] += 1
+                self.next_scan += self.period
+                self._step(1)
+                n -= 1
+                continue
+            m = min(n, self._steps_free())
+            self._step(m)
+            n -= m
+
+    def _step(self, m: int):
+        self.s.step(m)
+        self.t += m
+        self.counts["plain_steps"] += m
+
+    def _state(self):
+        import torch
+        x = np.stack([self.s.get(f) for f in FIELDS], axis=-1)
+        return torch.from_numpy(x).cuda()
+
+    def _change(self, a, b):
+        import torch
+        return float(torch.linalg.vector_norm(((b - a) / self.norm.dsd.double())[..., :3]))
+
+    def advance(self, n: int):
+        """n simulated steps; returns the counts."""
+        end = self.t + n
+        span = self.k + 2 * self.probe
+        while self.t < end:
+            left = end - self.t
+            free = self._steps_free()
+            if self.model is None or left < span or free < span:
+                self.plain(left if self.model is None else min(left, free + 1))
+                continue
+            self.s.save(self.ckpt)
+            t0, counts0 = self.t, dict(self.counts)
+            xa = self._state()
+            self.plain(self.probe)
+            xb = self._state()
+            rate = {f: float((xb[..., i] - xa[..., i]).sum()) / self.probe for i, f in ((0, "o"), (1, "cr"))}
+            pre = self._change(xa, xb) / self.probe
+            prop = predict(self.model, self.norm, xb[None].float())[0].double()
+            prop[..., 3] = xb[..., 3]
+            ok = True
+            for i, f in ((0, "o"), (1, "cr")):
+                d = prop[..., i] - xb[..., i]
+                want = self.k * rate[f]
+                mag = float(d.abs().sum())
+                c = (want - float(d.sum())) / mag if mag > 0 else 0.0
+                if abs(c) > self.mass_tol:
+                    ok = False
+                    break
+                prop[..., i] = xb[..., i] + d + c * d.abs()
+            if not ok:
+                self.counts["rejected_mass"] += 1
+                self.plain(self.k + self.probe)
+                continue
+            jumped = {f: float((prop[..., i] - xb[..., i]).sum()) for i, f in ((0, "o"), (1, "cr"))}
+            host = prop.cpu().numpy()
+            for i, f in enumerate(("o", "cr", "p")):
+                self.s.set(f, host[..., i])
+            self.s.invalidate_eta_cache()
+            self.t += self.k
+            self.plain(self.probe)
+            post = self._change(prop, self._state()) / self.probe
+            if post <= self.recheck_factor * pre:
+                self.counts["accepted"] += 1
+                self.counts["jumped_steps"] += self.k
+                for f in ("o", "cr"):
+                    self.ledger[f] += jumped[f]
+                continue
+            self.s.load(self.ckpt)
+            self.t, self.counts = t0, counts0
+            self.counts["rejected_recheck"] += 1
+            self.plain(self.k + 2 * self.probe)
+        return dict(self.counts)
+
+    def close(self):
+        self._tmp.cleanup()

@@ -1,0 +1,98 @@
+"""The surrogate's BF16 tensor-core convolutions (nicr_conv3d_fwd,
+nicr_conv3d_wgrad) and their autograd wrapper against torch's conv3d in FP64
+on the CPU, on BF16-representable inputs. Bound: FP32 accumulation, so each
+output may differ from the FP64 value by at most 1e-4 x the same sum taken
+over absolute values (a wrong tap, channel or voxel gives errors of order 1)."""
+import pytest
+import torch
+
+import conv_ref
+from nicr import surrogate
+
+pytestmark = pytest.mark.gpu
+
+SHAPES = [(2, 4, 8, 8, 16, 48), (1, 8, 8, 8, 32, 64), (1, 6, 4, 16, 48, 16), (2, 16, 16, 16, 16, 32),
+          (1, 8, 8, 8, 96, 128)]
+TOL = 1e-4
+
+
+def inputs(shape, seed):
+    n, d, h, w, ci, co = shape
+    g = torch.Generator().manual_seed(seed)
+    x = conv_ref.bf16_rounded((n, d, h, w, ci), g)
+    wt = conv_ref.bf16_rounded((co, 27, ci), g, 0.2)
+    dy = conv_ref.bf16_rounded((n, d, h, w, co), g)
+    return x, wt, dy
+
+
+def within(got, ref, bound, label):
+    err = (got.double().cpu() - ref).abs()
+    worst = float((err / (bound + 1e-300)).max())
+    assert worst <= TOL, f"{label}: error {worst:.3g} x the absolute-value bound"
+
+
+@pytest.mark.parametrize("shape", SHAPES)
+def test_forward(require_gpu, shape):
+    x, wt, _ = inputs(shape, 1)
+    y = surrogate.conv3d_raw(x.cuda().bfloat16(), wt.cuda().bfloat16())
+    torch.cuda.synchronize()
+    within(y, conv_ref.conv3d(x, wt), conv_ref.conv3d(x.abs(), wt.abs()), "forward")
+
+
+@pytest.mark.parametrize("shape", SHAPES)
+def test_data_gradient(require_gpu, shape):
+    x, wt, dy = inputs(shape, 2)
+    dx_ref, _ = conv_ref.grads(x, wt, dy)
+    wf = conv_ref.dgrad_weights(wt)
+    dx = surrogate.conv3d_raw(dy.cuda().bfloat16(), wf.cuda().bfloat16())
+    within(dx, dx_ref, conv_ref.conv3d(dy.abs(), wf.abs()), "data gradient")
+
+
+@pytest.mark.parametrize("shape", SHAPES)
+def test_weight_gradient(require_gpu, shape):
+    x, wt, dy = inputs(shape, 3)
+    _, dw_ref = conv_ref.grads(x, wt, dy)
+    _, dw_abs = conv_ref.grads(x.abs(), wt, dy.abs())
+    dw = surrogate.conv3d_wgrad_raw(x.cuda().bfloat16(), dy.cuda().bfloat16())
+    within(dw, dw_ref, dw_abs, "weight gradient")
+
+
+def test_autograd_wrapper(require_gpu):
+    """Conv3dFn's gradients: dw in FP32, dx rounded to the input's BF16."""
+    x, wt, dy = inputs((1, 8, 8, 8, 32, 48), 4)
+    dx_ref, dw_ref = conv_ref.grads(x, wt, dy)
+    xg = x.cuda().bfloat16().requires_grad_(True)
+    wg = wt.cuda().requires_grad_(True)
+    y = surrogate.conv3d(xg, wg)
+    (y * dy.cuda()).sum().backward()
+    _, dw_abs = conv_ref.grads(x.abs(), wt, dy.abs())
+    within(wg.grad, dw_ref, dw_abs, "autograd dw")
+    rel = float((xg.grad.double().cpu() - dx_ref).abs().max() / dx_ref.abs().max())
+    assert rel < 8e-3
+
+
+def test_rejects_misaligned_shapes(require_gpu):
+    x = torch.zeros((1, 3, 3, 3, 16), dtype=torch.bfloat16, device="cuda")
+    w = torch.zeros((16, 27, 16), dtype=torch.bfloat16, device="cuda")
+    with pytest.raises(RuntimeError):
+        surrogate.conv3d_raw(x, w)
+
+
+def test_unet_gradients_finite_and_descend(require_gpu):
+    """One U-Net on random inputs: every parameter receives a finite gradient
+    from the library's kernels, and a few Adam steps reduce the loss."""
+    torch.manual_seed(0)
+    net = surrogate.unet(4, 16).cuda()
+    x = torch.randn(2, 16, 16, 16, 4, device="cuda")
+    target = torch.tanh(x.roll(1, 1)) * 0.5
+    opt = torch.optim.Adam(net.parameters(), lr=2e-3)
+    losses = []
+    for _ in range(30):
+        loss = torch.mean((net(x) - target) ** 2)
+        opt.zero_grad()
+        loss.backward()
+        for p in net.parameters():
+            assert p.grad is not None and torch.isfinite(p.grad).all()
+        opt.step()
+        losses.append(loss.item())
+    assert losses[-1] < 0.7 * losses[0]

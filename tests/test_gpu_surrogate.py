@@ -1,0 +1,93 @@
+"""The learned surrogate end to end on one GPU: trajectories from the solver
+(32^3 static Voronoi, Ksp, parameters drawn per seed), a 3D U-Net trained by
+the library's BF16 convolution kernels, its K-step prediction on a held-out
+seed against persistence and linear extrapolation, and JumpStepper against
+the plain solver (the plain run is the oracle that reports the surrogate's
+error)."""
+import time
+
+import numpy as np
+import pytest
+
+import nicr
+from nicr import surrogate
+
+pytestmark = pytest.mark.gpu
+
+SIZE, STEPS, EVERY, KS = 32, 256, 8, 2   # K = KS x EVERY = 16 steps
+
+
+@pytest.fixture(scope="module")
+def trained(require_gpu):
+    import torch
+    cfgs = surrogate.trajectory_configs(5, SIZE, first_seed=100)
+    t0 = time.perf_counter()
+    snaps = surrogate.trajectories(cfgs, STEPS, EVERY)
+    t1 = time.perf_counter()
+    torch.manual_seed(0)
+    net = surrogate.unet(4, 16).cuda()
+    norm, losses = surrogate.train(net, snaps[:4], KS, iters=400, batch=4)
+    torch.cuda.synchronize()
+    t2 = time.perf_counter()
+    print(f"\ntrajectories {t1 - t0:.1f} s, training {t2 - t1:.1f} s, loss {np.mean(losses[:20]):.4g} -> "
+          f"{np.mean(losses[-20:]):.4g}")
+    return net, norm, losses, snaps, cfgs
+
+
+def test_training_reduces_loss(trained):
+    _, _, losses, _, _ = trained
+    assert np.mean(losses[-20:]) < 0.5 * np.mean(losses[:20])
+
+
+def test_network_beats_persistence_on_held_out_seed(trained):
+    net, norm, _, snaps, _ = trained
+    e = surrogate.relative_errors(net, norm, snaps[4:], KS)
+    print("\nheld-out relative L2 error of the K-step change:", e)
+    assert e["persistence"] == pytest.approx(1.0)
+    assert e["network"] < 0.7
+
+
+def test_stepper_without_network_is_the_plain_run(require_gpu):
+    """Plain stepping with the stepper's own Ksp clock reproduces nicr_run
+    bit for bit across several scans."""
+    cfg = surrogate.trajectory_configs(1, 24, first_seed=7, nucleation_period=4e-9)[0]
+    a, b = nicr.Solver(cfg), nicr.Solver(cfg)
+    st = surrogate.JumpStepper(a, None, None, 16)
+    st.advance(37)
+    st.advance(60)
+    b.run(97)
+    assert st.counts["scans"] == 4 and st.counts["plain_steps"] == 97
+    for f in ("o", "cr", "p"):
+        assert np.array_equal(a.get(f).view(np.int64), b.get(f).view(np.int64)), f
+    assert a.budget()["nuclei"] == b.budget()["nuclei"]
+    st.close()
+    a.close()
+    b.close()
+
+
+def test_jumps_against_plain_solver(trained):
+    net, norm, _, _, cfgs = trained
+    cfg = cfgs[4]
+    jump, plain = nicr.Solver(cfg), nicr.Solver(cfg)
+    jump.run(32)
+    plain.run(32)
+    st = surrogate.JumpStepper(jump, net, norm, KS * EVERY)
+    t0 = time.perf_counter()
+    counts = st.advance(192)
+    t1 = time.perf_counter()
+    plain.run(192)
+    err = {f: float(np.abs(jump.get(f) - plain.get(f)).max() / max(np.abs(plain.get(f)).max(), 1e-300))
+           for f in ("o", "cr", "p")}
+    print(f"\njump stepper: {counts}, {t1 - t0:.2f} s; relative Linf error vs the plain run: {err}; "
+          f"ledger {st.ledger}")
+    tried = counts["accepted"] + counts["rejected_mass"] + counts["rejected_recheck"]
+    assert tried >= 1
+    assert counts["plain_steps"] + counts["jumped_steps"] == 192
+    if counts["accepted"] == 0:
+        for f in ("o", "cr", "p"):
+            assert np.array_equal(jump.get(f).view(np.int64), plain.get(f).view(np.int64)), f
+    else:
+        assert max(err.values()) < 0.05
+    st.close()
+    jump.close()
+    plain.close()
