@@ -171,90 +171,113 @@ def trajectory_configs(n: int, size: int, first_seed: int = 100, **kw):
     return out
 
 
-def trajectories(cfgs, steps: int, every: int, device: int = 0):
-    """Snapshots (fields o, cr, p, gb) of each run every `every` steps:
-    a tensor (runs, steps // every + 1, size, size, size, 4) on the GPU."""
+def trajectories(cfgs, steps: int, every: int, probe: int = 2, device: int = 0):
+    """States (fields o, cr, p, gb) of each run at steps every, 2 every, ...,
+    and their per-step rates over the `probe` steps before each: tensors
+    x, r of shape (runs, steps // every, size, size, size, 4) on the GPU."""
     import torch
     from . import Solver
-    runs = []
+    xs, rs = [], []
     for c in cfgs:
         c.device = device
         s = Solver(c)
-        snaps = []
-        for t in range(steps // every + 1):
-            if t:
-                s.run(every)
-            snaps.append(np.stack([s.get(f) for f in FIELDS], axis=-1))
+        state = lambda: np.stack([s.get(f) for f in FIELDS], axis=-1)
+        x, r = [], []
+        for _ in range(steps // every):
+            s.run(every - probe)
+            a = state()
+            s.run(probe)
+            b = state()
+            x.append(b)
+            r.append((b - a) / probe)
         s.close()
-        runs.append(torch.tensor(np.stack(snaps), dtype=torch.float32, device=f"cuda:{device}"))
-    return torch.stack(runs)
+        xs.append(torch.tensor(np.stack(x), dtype=torch.float32, device=f"cuda:{device}"))
+        rs.append(torch.tensor(np.stack(r), dtype=torch.float32, device=f"cuda:{device}"))
+    return torch.stack(xs), torch.stack(rs)
 
 
 class Normaliser:
-    """Per-field shift/scale of the states and of their K-step changes."""
+    """Per-field scales: of the states (mu, sd), of the per-step rates (rsd),
+    of the K-step changes (csd) and of the network's target, the K-step
+    change minus K x the rate (dsd). K counts steps; k counts samples."""
 
-    def __init__(self, snaps, k: int):
-        flat = snaps.reshape(-1, snaps.shape[-1])
+    def __init__(self, x, r, k: int, steps_k: int):
+        f = x.shape[-1]
+        flat = x.reshape(-1, f)
         self.mu, self.sd = flat.mean(0), flat.std(0).clamp_min(1e-12)
-        delta = (snaps[:, k:] - snaps[:, :-k]).reshape(-1, snaps.shape[-1])
-        self.dsd = delta.std(0).clamp_min(1e-12)
-        self.k = k
+        self.rsd = r.reshape(-1, f).std(0).clamp_min(1e-30)
+        d = x[:, k:] - x[:, :-k]
+        self.csd = d.reshape(-1, f).std(0).clamp_min(1e-30)
+        self.dsd = (d - steps_k * r[:, :-k]).reshape(-1, f).std(0).clamp_min(1e-30)
+        self.steps_k = steps_k
 
-    def inputs(self, x):
-        return (x - self.mu) / self.sd
+    def inputs(self, x, r):
+        import torch
+        return torch.cat([(x - self.mu) / self.sd, r / self.rsd], dim=-1)
 
-    def target(self, x0, x1):
-        return (x1 - x0) / self.dsd
+    def target(self, x0, r0, x1):
+        return (x1 - x0 - self.steps_k * r0) / self.dsd
 
-    def apply(self, x0, pred):
-        return x0 + pred * self.dsd
+    def apply(self, x0, r0, pred):
+        return x0 + self.steps_k * r0 + pred * self.dsd
 
 
-def train(model, snaps, k: int, iters: int = 200, batch: int = 2, lr: float = 2e-3, seed: int = 0):
-    """Adam on MSE of the normalised K-step change; returns (normaliser, losses)."""
+def _pairs(x, r, k):
+    f = x.shape[2:]
+    return x[:, :-k].reshape((-1,) + f), r[:, :-k].reshape((-1,) + f), x[:, k:].reshape((-1,) + f)
+
+
+def train(model, x, r, k: int, steps_k: int, iters: int = 200, batch: int = 2, lr: float = 2e-3, seed: int = 0):
+    """Adam (cosine-decayed rate) on the MSE of the normalised target over
+    sample pairs k apart (steps_k steps); returns (normaliser, losses)."""
     import torch
     torch.manual_seed(seed)
-    norm = Normaliser(snaps, k)
-    x0 = snaps[:, :-k].reshape((-1,) + snaps.shape[2:])
-    x1 = snaps[:, k:].reshape((-1,) + snaps.shape[2:])
+    norm = Normaliser(x, r, k, steps_k)
+    x0, r0, x1 = _pairs(x, r, k)
     opt = torch.optim.Adam(model.parameters(), lr=lr)
+    sched = torch.optim.lr_scheduler.CosineAnnealingLR(opt, iters)
     g = torch.Generator(device="cpu").manual_seed(seed)
     losses = []
     for _ in range(iters):
         idx = torch.randint(0, x0.shape[0], (batch,), generator=g)
-        a, b = x0[idx], x1[idx]
-        loss = torch.mean((model(norm.inputs(a)) - norm.target(a, b)) ** 2)
+        a, ra, b = x0[idx], r0[idx], x1[idx]
+        loss = torch.mean((model(norm.inputs(a, ra)) - norm.target(a, ra, b)) ** 2)
         opt.zero_grad()
         loss.backward()
         opt.step()
+        sched.step()
         losses.append(loss.item())
     return norm, losses
 
 
-def predict(model, norm, x0, chunk: int = 4):
-    """The network's state K steps after x0 (n, d, h, w, fields), FP32."""
+def predict(model, norm, x0, r0, chunk: int = 4):
+    """The network's state K steps after x0 with rates r0 (n, d, h, w, fields)."""
     import torch
     out = []
     with torch.no_grad():
         for i in range(0, x0.shape[0], chunk):
-            a = x0[i:i + chunk]
-            out.append(norm.apply(a, model(norm.inputs(a))))
+            a, ra = x0[i:i + chunk], r0[i:i + chunk]
+            out.append(norm.apply(a, ra, model(norm.inputs(a, ra))))
     return torch.cat(out)
 
 
-def relative_errors(model, norm, snaps, k: int):
-    """Relative L2 error of the K-step change predicted by the network, by
-    persistence (no change: 1 by definition) and by linear extrapolation of
-    the previous K steps, over the fields that change (c_O, c_Cr, phi)."""
+def relative_errors(model, norm, x, r, k: int):
+    """Relative L2 error of the K-step change (each field scaled by the
+    spread of its change; c_O, c_Cr and phi) predicted by the network, by
+    persistence (no change: 1 by definition), by extrapolation of the
+    current rate (x + K r: the network's starting point) and by linear
+    extrapolation of the previous K steps (2 x_t - x_{t-K})."""
     import torch
-    x0 = snaps[:, k:-k].reshape((-1,) + snaps.shape[2:])
-    xm = snaps[:, :-2 * k].reshape((-1,) + snaps.shape[2:])
-    x1 = snaps[:, 2 * k:].reshape((-1,) + snaps.shape[2:])
-    f = slice(0, 3)
-    ref = torch.linalg.vector_norm(((x1 - x0) / norm.dsd)[..., f])
-    pred = predict(model, norm, x0)
-    e = lambda y: float(torch.linalg.vector_norm(((y - x1) / norm.dsd)[..., f]) / ref)
-    return {"network": e(pred), "persistence": e(x0), "linear": e(2 * x0 - xm)}
+    f = x.shape[2:]
+    x0 = x[:, k:-k].reshape((-1,) + f)
+    r0 = r[:, k:-k].reshape((-1,) + f)
+    xm = x[:, :-2 * k].reshape((-1,) + f)
+    x1 = x[:, 2 * k:].reshape((-1,) + f)
+    c = slice(0, 3)
+    ref = torch.linalg.vector_norm(((x1 - x0) / norm.csd)[..., c])
+    e = lambda y: float(torch.linalg.vector_norm(((y - x1) / norm.csd)[..., c]) / ref)
+    return {"network": e(predict(model, norm, x0, r0)), "persistence": e(x0), "rate": e(x0 + norm.steps_k * r0),
+            "linear": e(2 * x0 - xm)}
 
 
 # ------------------------------------------------------------------ jumps
@@ -286,6 +309,8 @@ class JumpStepper:
                  recheck_factor: float = 4.0, workdir=None):
         import tempfile
         from . import NUCLEATION
+        if norm is not None and norm.steps_k != k:
+            raise ValueError(f"the network predicts {norm.steps_k} steps ahead, not {k}")
         self.s, self.model, self.norm, self.k, self.probe = solver, model, norm, k, probe
         self.mass_tol, self.recheck_factor = mass_tol, recheck_factor
         c = solver.cfg
@@ -339,7 +364,7 @@ class JumpStepper:
 
     def _change(self, a, b):
         import torch
-        return float(torch.linalg.vector_norm(((b - a) / self.norm.dsd.double())[..., :3]))
+        return float(torch.linalg.vector_norm(((b - a) / self.norm.csd.double())[..., :3]))
 
     def advance(self, n: int):
         """n simulated steps; returns the counts."""
@@ -356,9 +381,10 @@ class JumpStepper:
             xa = self._state()
             self.plain(self.probe)
             xb = self._state()
-            rate = {f: float((xb[..., i] - xa[..., i]).sum()) / self.probe for i, f in ((0, "o"), (1, "cr"))}
+            rb = (xb - xa) / self.probe
+            rate = {f: float(rb[..., i].sum()) for i, f in ((0, "o"), (1, "cr"))}
             pre = self._change(xa, xb) / self.probe
-            prop = predict(self.model, self.norm, xb[None].float())[0].double()
+            prop = predict(self.model, self.norm, xb[None].float(), rb[None].float())[0].double()
             prop[..., 3] = xb[..., 3]
             ok = True
             for i, f in ((0, "o"), (1, "cr")):
