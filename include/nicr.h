@@ -414,11 +414,18 @@ int nicr_slab_box_half(const nicr_handle* h);
  * multiples of 16. nicr_conv3d_fwd: y[v][co] = sum x[v+off(tap)][ci]
  * w[co][tap][ci]. nicr_conv3d_wgrad: dw[co][tap][ci] = sum_v dy[v][co]
  * x[v+off(tap)][ci] (dy: BF16 NDHWC with cout channels). The data gradient
- * is nicr_conv3d_fwd of dy with w'[ci][tap][co] = w[co][26-tap][ci]. */
+ * is nicr_conv3d_fwd of dy with w'[ci][tap][co] = w[co][26-tap][ci].
+ * nicr_conv3d_fwd runs on tcgen05.mma (accumulator in TMEM);
+ * nicr_conv3d_fwd_mma_sync is the same convolution on the warp-level MMA
+ * instructions. nicr_conv3d_error copies and clears the flag the tcgen05
+ * kernel sets when one of its bounded waits gives up (synchronous). */
 int nicr_conv3d_fwd(const void* x, const void* w, float* y, int n, int d, int h, int w_, int cin, int cout,
                     void* stream);
+int nicr_conv3d_fwd_mma_sync(const void* x, const void* w, float* y, int n, int d, int h, int w_, int cin, int cout,
+                             void* stream);
 int nicr_conv3d_wgrad(const void* x, const void* dy, float* dw, int n, int d, int h, int w_, int cin, int cout,
                       void* stream);
+int nicr_conv3d_error(int* flag);
 
 /* The solver program: the reference's run()/main() for dim 2 or 3
  * (2D:1161-1246, 3S:1309-1395), argv as the reference's executable takes it.

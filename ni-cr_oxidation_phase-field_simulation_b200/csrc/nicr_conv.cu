@@ -10,9 +10,10 @@
 //            (off(26 - tap) = -off(tap)); the caller transposes the weights
 //   wgrad    dw[co][tap][ci] = sum_v dy[v][co] * x[v + off(tap)][ci]
 //            (GEMM per tap: M = Cout, N = Cin, K = voxels, split over CTAs)
-// This first form uses the warp-level WMMA tensor-core instructions (16x16x16
-// BF16 tiles staged through shared memory with plain 16-byte loads); the
-// tcgen05/TMEM form is the next step for these GEMMs.
+// The forward (and so the data gradient) runs on tcgen05.mma with the
+// accumulator in TMEM (k_conv3d_fwd_tc); the weight gradient and the
+// reference forward nicr_conv3d_fwd_mma_sync use the warp-level WMMA
+// instructions (16x16x16 BF16 tiles staged through shared memory).
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <mma.h>
@@ -127,6 +128,176 @@ __global__ void __launch_bounds__(128) k_conv3d_wgrad(const __nv_bfloat16* __res
     }
 }
 
+// ---------------------------------------------------------------- tcgen05
+// Forward on the 5th-generation tensor cores: CTA of 4 warps = 128 voxels x
+// N output channels (N <= 256), accumulator in TMEM (128 lanes x N FP32
+// columns). The K loop runs over 27 taps x Cin/KC chunks; each chunk (stage)
+// is gathered by all threads with zero-filling 16-byte cp.async into the
+// no-swizzle K-major canonical layout (8-row x 16-byte core matrices; chunk
+// (row r, 16-byte column kc) at byte kc*ROWS*16 + r*16, so SBO = 128 B between
+// 8-row groups and LBO = ROWS*16 B between the two K halves of an MMA), and
+// one thread issues its KC/16 tcgen05.mma (M=128, N, K=16; BF16 in, FP32
+// accumulate) and commits them to the stage's mbarrier. Four stages, loads
+// run two chunks ahead. Every mbarrier wait is bounded: on timeout the CTA
+// records the error, stops issuing work, waits (bounded) for its MMAs and
+// frees its TMEM.
+constexpr int TC_M = 128, TC_STAGES = 4, TC_AHEAD = 2;
+constexpr long long TC_SPIN = 1LL << 22;
+
+__device__ int g_conv_error;   // non-zero after a timed-out wait
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ uint64_t umma_sdesc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);   // version 1, no swizzle
+}
+
+// kind::f16 instruction descriptor: FP32 accumulator, BF16 A and B, both K-major
+__host__ __device__ constexpr uint32_t umma_idesc(int m, int n) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(m >> 4) << 24);
+}
+
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, bool valid) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(src), "r"(valid ? 16 : 0));
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+    for (long long i = 0; i < TC_SPIN; ++i) {
+        uint32_t done;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+__global__ void __launch_bounds__(128) k_conv3d_fwd_tc(const __nv_bfloat16* __restrict__ x,
+                                                        const __nv_bfloat16* __restrict__ wt, float* __restrict__ y,
+                                                        const Vol V, int cin, int cout, int kc_elems, int tmem_cols) {
+    extern __shared__ __align__(1024) unsigned char tc_smem[];
+    const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+    const long long M = V.voxels();
+    const long long v0 = (long long)blockIdx.x * TC_M;
+    const int n0 = blockIdx.y * 256;
+    const int N = min(256, cout - n0);
+    const int kcols = kc_elems / 8;                      // 16-byte columns per chunk
+    const uint32_t a_bytes = TC_M * kc_elems * 2, b_bytes = (uint32_t)N * kc_elems * 2;
+    const uint32_t stage_bytes = (a_bytes + b_bytes + 1023) & ~1023u;
+    unsigned char* stages = tc_smem;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(tc_smem + TC_STAGES * stage_bytes);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + TC_STAGES);
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(tmem_cols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (t == 0) {
+        for (int s = 0; s < TC_STAGES; ++s)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bars + s)));
+        asm volatile("fence.mbarrier_init.release.cluster;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+
+    const int chunks_per_tap = cin / kc_elems;
+    const int iters = 27 * chunks_per_tap;
+    const uint32_t idesc = umma_idesc(TC_M, N);
+    const bool row_ok = v0 + t < M;
+
+    auto load = [&](int it) {
+        const int tap = it / chunks_per_tap, c0 = (it % chunks_per_tap) * kc_elems;
+        const uint32_t base = smem_u32(stages + (it % TC_STAGES) * stage_bytes);
+        const long long src = row_ok ? shifted(V, v0 + t, tap) : -1;
+        const __nv_bfloat16* a_src = src >= 0 ? x + src * cin + c0 : x;
+        for (int kc = 0; kc < kcols; ++kc)   // A: thread t owns voxel row t
+            cp_async16(base + (uint32_t)(kc * TC_M + t) * 16, a_src + (src >= 0 ? kc * 8 : 0), src >= 0);
+        for (int q = t; q < kcols * N; q += 128) {   // B: chunk q = kc * N + co
+            const int kc = q / N, co = q % N;
+            cp_async16(base + a_bytes + (uint32_t)q * 16, wt + ((long long)(n0 + co) * 27 + tap) * cin + c0 + kc * 8, true);
+        }
+    };
+
+    for (int it = 0; it < TC_AHEAD && it < iters; ++it) {
+        load(it);
+        asm volatile("cp.async.commit_group;");
+    }
+    bool ok = true;
+    int committed = 0;   // chunks whose MMAs have been issued and committed
+    for (int it = 0; it < iters; ++it) {
+        const int ahead = it + TC_AHEAD;
+        if (ahead < iters) {
+            // the stage of chunk `ahead` last held chunk ahead - STAGES: its MMAs must have finished
+            if (ahead >= TC_STAGES)
+                ok = mbar_wait(smem_u32(bars + ahead % TC_STAGES), (uint32_t)((ahead / TC_STAGES - 1) & 1));
+            if (__syncthreads_or(!ok)) break;
+            load(ahead);
+        }
+        asm volatile("cp.async.commit_group;");
+        asm volatile("cp.async.wait_group %0;" ::"n"(TC_AHEAD));
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (t == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t base = smem_u32(stages + (it % TC_STAGES) * stage_bytes);
+            for (int k = 0; k < kc_elems / 16; ++k) {
+                const uint64_t ad = umma_sdesc(base + k * 2 * TC_M * 16, TC_M * 16, 128);
+                const uint64_t bd = umma_sdesc(base + a_bytes + k * 2 * N * 16, N * 16, 128);
+                const uint32_t acc = (it > 0 || k > 0) ? 1u : 0u;
+                asm volatile(
+                    "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                    " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
+                    "l"(ad), "l"(bd), "r"(idesc), "r"(acc));
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                smem_u32(bars + it % TC_STAGES)));
+        }
+        committed = it + 1;
+    }
+    asm volatile("cp.async.wait_all;");
+    // the last commit covers every MMA issued before it (also after a timeout,
+    // so that no MMA is in flight when the TMEM is freed)
+    if (committed > 0) {
+        const int last = committed - 1;
+        const bool done = mbar_wait(smem_u32(bars + last % TC_STAGES), (uint32_t)((last / TC_STAGES) & 1));
+        ok = ok && done;
+    }
+    ok = !__syncthreads_or(!ok);
+    if (ok) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const bool store = v0 + warp * 32 + lane < M;
+        float* out = y + (v0 + warp * 32 + lane) * cout + n0;
+        for (int c = 0; c < N; c += 16) {
+            uint32_t r[16];
+            const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c;
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+                : "r"(taddr));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (store)
+                for (int j = 0; j < 16; j += 4)
+                    *reinterpret_cast<float4*>(out + c + j) =
+                        make_float4(__uint_as_float(r[j]), __uint_as_float(r[j + 1]), __uint_as_float(r[j + 2]),
+                                    __uint_as_float(r[j + 3]));
+        }
+    } else if (t == 0) {
+        atomicExch(&g_conv_error, 1);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(tmem_cols));
+}
+
 int check_args(long long voxels, int cin, int cout) {
     if (voxels <= 0 || voxels % 64 != 0 || cin <= 0 || cin % 16 != 0 || cout <= 0 || cout % 16 != 0)
         return NICR_ERR_INVALID_ARG;
@@ -139,6 +310,29 @@ extern "C" {
 
 int nicr_conv3d_fwd(const void* x, const void* w, float* y, int n, int d, int h, int w_, int cin, int cout,
                     void* stream) {
+    const Vol V{n, d, h, w_};
+    const int rc = check_args(V.voxels(), cin, cout);
+    if (rc != NICR_OK || !x || !w || !y) return rc != NICR_OK ? rc : NICR_ERR_INVALID_ARG;
+    const int cmax = cout < 256 ? cout : 256;
+    int kc = 64;   // channels per chunk: the largest of 64, 48, 32, 16 dividing Cin
+    while (cin % kc != 0) kc -= 16;
+    const size_t stage = ((size_t)(TC_M + cmax) * kc * 2 + 1023) / 1024 * 1024;
+    int cols = 32;   // TMEM columns: a power of two >= N
+    while (cols < cmax) cols <<= 1;
+    // at least cols x 400 bytes of shared memory per CTA, so that the CTAs
+    // resident on one SM never ask for more than its 512 TMEM columns
+    size_t smem = TC_STAGES * stage + 64;
+    if (smem < (size_t)cols * 400) smem = (size_t)cols * 400;
+    if (cudaFuncSetAttribute(k_conv3d_fwd_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return NICR_ERR_CUDA;
+    const dim3 grid((unsigned)((V.voxels() + TC_M - 1) / TC_M), (unsigned)((cout + 255) / 256));
+    k_conv3d_fwd_tc<<<grid, 128, smem, static_cast<cudaStream_t>(stream)>>>(
+        static_cast<const __nv_bfloat16*>(x), static_cast<const __nv_bfloat16*>(w), y, V, cin, cout, kc, cols);
+    return cudaGetLastError() == cudaSuccess ? NICR_OK : NICR_ERR_CUDA;
+}
+
+int nicr_conv3d_fwd_mma_sync(const void* x, const void* w, float* y, int n, int d, int h, int w_, int cin, int cout,
+                             void* stream) {
     const Vol V{n, d, h, w_};
     const int rc = check_args(V.voxels(), cin, cout);
     if (rc != NICR_OK || !x || !w || !y) return rc != NICR_OK ? rc : NICR_ERR_INVALID_ARG;
@@ -166,6 +360,15 @@ int nicr_conv3d_wgrad(const void* x, const void* dy, float* dw, int n, int d, in
     k_conv3d_wgrad<<<grid, 128, 0, s>>>(static_cast<const __nv_bfloat16*>(x), static_cast<const __nv_bfloat16*>(dy), dw,
                                         V, cin, cout, slice);
     return cudaGetLastError() == cudaSuccess ? NICR_OK : NICR_ERR_CUDA;
+}
+
+int nicr_conv3d_error(int* flag) {
+    if (!flag) return NICR_ERR_INVALID_ARG;
+    const int zero = 0;
+    if (cudaMemcpyFromSymbol(flag, g_conv_error, sizeof(int)) != cudaSuccess ||
+        cudaMemcpyToSymbol(g_conv_error, &zero, sizeof(int)) != cudaSuccess)
+        return NICR_ERR_CUDA;
+    return NICR_OK;
 }
 
 }  // extern "C"

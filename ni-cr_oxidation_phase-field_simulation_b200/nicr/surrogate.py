@@ -26,8 +26,9 @@ def _lib():
     L = lib()
     if not getattr(L, "_conv_bound", False):
         vp, i = ctypes.c_void_p, ctypes.c_int
-        for f in ("nicr_conv3d_fwd", "nicr_conv3d_wgrad"):
+        for f in ("nicr_conv3d_fwd", "nicr_conv3d_fwd_mma_sync", "nicr_conv3d_wgrad"):
             getattr(L, f).argtypes = [vp, vp, vp, i, i, i, i, i, i, vp]
+        L.nicr_conv3d_error.argtypes = [ctypes.POINTER(ctypes.c_int)]
         L._conv_bound = True
     return L
 
@@ -37,15 +38,25 @@ def _check(rc, what):
         raise RuntimeError(f"{what} failed with status {rc}")
 
 
-def conv3d_raw(x, w_bf16):
-    """y = conv(x, w): x (n, d, h, w, cin) BF16, w (cout, 27, cin) BF16 -> FP32."""
+def conv3d_raw(x, w_bf16, form: str = "tcgen05"):
+    """y = conv(x, w): x (n, d, h, w, cin) BF16, w (cout, 27, cin) BF16 -> FP32.
+    form "tcgen05" (nicr_conv3d_fwd) or "mma_sync" (nicr_conv3d_fwd_mma_sync)."""
     import torch
     n, d, h, wd, cin = x.shape
     cout = w_bf16.shape[0]
     y = torch.empty((n, d, h, wd, cout), dtype=torch.float32, device=x.device)
-    _check(_lib().nicr_conv3d_fwd(x.data_ptr(), w_bf16.data_ptr(), y.data_ptr(), n, d, h, wd, cin, cout,
-                                  torch.cuda.current_stream(x.device).cuda_stream), "nicr_conv3d_fwd")
+    f = {"tcgen05": "nicr_conv3d_fwd", "mma_sync": "nicr_conv3d_fwd_mma_sync"}[form]
+    _check(getattr(_lib(), f)(x.data_ptr(), w_bf16.data_ptr(), y.data_ptr(), n, d, h, wd, cin, cout,
+                              torch.cuda.current_stream(x.device).cuda_stream), f)
     return y
+
+
+def conv_error() -> int:
+    """The tcgen05 kernel's timeout flag (synchronous; cleared by the read)."""
+    import ctypes
+    flag = ctypes.c_int(0)
+    _check(_lib().nicr_conv3d_error(ctypes.byref(flag)), "nicr_conv3d_error")
+    return flag.value
 
 
 def conv3d_wgrad_raw(x, dy):

@@ -11,8 +11,11 @@ from nicr import surrogate
 
 pytestmark = pytest.mark.gpu
 
+# (n, d, h, w, cin, cout): chunks of 64/48/32/16 channels, a partial
+# 128-voxel tile (64 voxels), two output-channel tiles (cout 272 = 256 + 16)
 SHAPES = [(2, 4, 8, 8, 16, 48), (1, 8, 8, 8, 32, 64), (1, 6, 4, 16, 48, 16), (2, 16, 16, 16, 16, 32),
-          (1, 8, 8, 8, 96, 128)]
+          (1, 8, 8, 8, 96, 128), (1, 4, 4, 4, 16, 16), (1, 4, 8, 8, 32, 272), (1, 4, 4, 8, 80, 32),
+          (1, 8, 8, 8, 64, 256)]
 TOL = 1e-4
 
 
@@ -31,12 +34,14 @@ def within(got, ref, bound, label):
     assert worst <= TOL, f"{label}: error {worst:.3g} x the absolute-value bound"
 
 
+@pytest.mark.parametrize("form", ["tcgen05", "mma_sync"])
 @pytest.mark.parametrize("shape", SHAPES)
-def test_forward(require_gpu, shape):
+def test_forward(require_gpu, shape, form):
     x, wt, _ = inputs(shape, 1)
-    y = surrogate.conv3d_raw(x.cuda().bfloat16(), wt.cuda().bfloat16())
+    y = surrogate.conv3d_raw(x.cuda().bfloat16(), wt.cuda().bfloat16(), form)
     torch.cuda.synchronize()
-    within(y, conv_ref.conv3d(x, wt), conv_ref.conv3d(x.abs(), wt.abs()), "forward")
+    within(y, conv_ref.conv3d(x, wt), conv_ref.conv3d(x.abs(), wt.abs()), f"forward ({form})")
+    assert surrogate.conv_error() == 0
 
 
 @pytest.mark.parametrize("shape", SHAPES)
