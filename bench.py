@@ -354,6 +354,92 @@ def small_workload(args) -> int:
     return 0
 
 
+def surrogate_workload(args) -> int:
+    """The learned surrogate's kernels at 128^3: (1) the 3x3x3 convolutions of
+    the U-Net's layers (base 16 channels: 16->16 and 48->16 at 128^3, 96->32
+    at 64^3, 64->64 at 32^3, plus 64->256 at 64^3 as a wide case) through
+    nicr_conv3d_fwd (tcgen05, TMA-staged), nicr_conv3d_fwd_gather (tcgen05,
+    cp.async-gathered) and nicr_conv3d_fwd_mma_sync, and the weight
+    gradient, each timed with CUDA events over 10 launches after 3 warm-up
+    launches; (2) one U-Net forward (a jump proposal) at 128^3 and one
+    training step at 64^3 (batch 2); (3) the plain FP64 step at 128^3 (32
+    static grains), for the break-even K of a jump. FLOPs = 2 x 27 x Cin x Cout
+    per voxel (zero-padding taps counted)."""
+    import torch
+    import nicr
+    from nicr import surrogate
+    dev = torch.device("cuda", 0)
+    peak, peak_kind = (1590.0, "fallback")
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        peak, peak_kind = float(json.loads(p.read_text())["bf16_tflops"]), "measured"
+
+    def timed(f, reps=10):
+        for _ in range(3):
+            f()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(reps):
+            f()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    layers = [("enc1 16->16 @128^3", 128, 16, 16), ("dec1 48->16 @128^3", 128, 48, 16),
+              ("dec2 96->32 @64^3", 64, 96, 32), ("mid 64->64 @32^3", 32, 64, 64), ("wide 64->256 @64^3", 64, 64, 256)]
+    clocks = ClockSampler(0)
+    clocks.start()
+    rows = []
+    g = torch.Generator(device=dev).manual_seed(0)
+    for name, s, ci, co in layers:
+        x = torch.randn((1, s, s, s, ci), device=dev, generator=g).bfloat16()
+        w = (torch.randn((co, 27, ci), device=dev, generator=g) * 0.05).bfloat16()
+        dy = torch.randn((1, s, s, s, co), device=dev, generator=g).bfloat16()
+        flops = 2.0 * 27 * ci * co * s ** 3
+        r = {"layer": name}
+        for form in ("tcgen05", "gather", "mma_sync"):
+            ms = timed(lambda: surrogate.conv3d_raw(x, w, form))
+            r[f"fwd_{form}_ms"] = ms
+            r[f"fwd_{form}_tflops"] = flops / ms / 1e9
+        ms = timed(lambda: surrogate.conv3d_wgrad_raw(x, dy))
+        r["wgrad_ms"], r["wgrad_tflops"] = ms, flops / ms / 1e9
+        rows.append(r)
+        del x, w, dy
+    err = surrogate.conv_error()
+    torch.manual_seed(0)
+    net = surrogate.unet(4, 16).to(dev)
+    xin = torch.randn((1, 128, 128, 128, 8), device=dev)
+    with torch.no_grad():
+        fwd_ms = timed(lambda: net(xin), reps=5)
+    xt = torch.randn((2, 64, 64, 64, 8), device=dev)
+    opt = torch.optim.Adam(net.parameters(), lr=1e-3)
+
+    def train_step():
+        loss = torch.mean(net(xt) ** 2)
+        opt.zero_grad()
+        loss.backward()
+        opt.step()
+    train_ms = timed(train_step, reps=5)
+    cl = clocks.stop()
+    cfg = nicr.make_config(3, nx=128, ny=128, nz=128, grains=1, grain_diameter_grid=50., random_seed=1, bounds="legacy")
+    sol = nicr.Solver(cfg)
+    sol.run(20)
+    plain_ms = timed(lambda: sol.run(16), reps=5) / 16
+    sol.close()
+    best = max(rows, key=lambda r: r["fwd_tcgen05_tflops"])
+    out = {"workload": "surrogate", "metric": "surrogate conv3d forward TFLOP/s (BF16 in, FP32 accumulate)",
+           "unit": "TFLOP/s", "value": best["fwd_tcgen05_tflops"], "dtype": "bf16",
+           "roofline": {"bound": "tensor", "kernel": "k_conv3d_fwd_tma", "layer": best["layer"],
+                        "achieved": best["fwd_tcgen05_tflops"], "peak": peak, "unit": "TFLOP/s",
+                        "frac": best["fwd_tcgen05_tflops"] / peak, "peak_kind": peak_kind},
+           "layers": rows, "unet_forward_128cube_ms": fwd_ms, "train_step_64cube_batch2_ms": train_ms,
+           "plain_fp64_step_128cube_ms": plain_ms,
+           "break_even_k": fwd_ms / plain_ms, "conv_error_flag": err, "clocks": cl, "data": "synthetic"}
+    print(json.dumps(out))
+    return 0
+
+
 def slabs_workload(args) -> int:
     """The slab form (one domain split along X, nicr_slabs_*) on the bench
     workload: 256^3, 8 evolving eta, reciprocal form, Ksp on, the same initial
@@ -524,13 +610,15 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-budget", type=float, default=60.0, help="seconds of CPU stepping for the reference")
     ap.add_argument("--slab-devices", default="", help="--workload slabs: comma-separated device per slab")
-    ap.add_argument("--workload", choices=["step", "output", "sweep", "small", "accuracy", "slabs", "slab-ranks"],
+    ap.add_argument("--workload", choices=["step", "output", "sweep", "small", "accuracy", "slabs", "slab-ranks",
+                                           "surrogate"],
                     default="step",
                     help="step: the headline line (default); output: VTI frame cost and overlap with stepping; "
                          "sweep: 64 uneven domains advanced as one batch; small: step rate of the small configs; "
                          "accuracy: the fast form against the drop-in form over --steps (5000 by default here); "
                          "slabs: the domain split along X into slabs against one handle; "
-                         "slab-ranks: the domain split over the torchrun ranks (one slab per GPU)")
+                         "slab-ranks: the domain split over the torchrun ranks (one slab per GPU); "
+                         "surrogate: the learned surrogate's convolution kernels and U-Net at 128^3")
     ap.add_argument("--precision", type=int, default=0, help="arithmetic form of --workload sweep (0 drop-in, 1 fast)")
     args = ap.parse_args()
     if args.e2e_steps <= 0:
@@ -554,6 +642,8 @@ def main():
         return slabs_workload(args)
     if args.workload == "slab-ranks":
         return slab_ranks_workload(args, rank, world, local)
+    if args.workload == "surrogate":
+        return surrogate_workload(args)
 
     import torch
     import torch.distributed as dist

@@ -415,12 +415,19 @@ int nicr_slab_box_half(const nicr_handle* h);
  * w[co][tap][ci]. nicr_conv3d_wgrad: dw[co][tap][ci] = sum_v dy[v][co]
  * x[v+off(tap)][ci] (dy: BF16 NDHWC with cout channels). The data gradient
  * is nicr_conv3d_fwd of dy with w'[ci][tap][co] = w[co][26-tap][ci].
- * nicr_conv3d_fwd runs on tcgen05.mma (accumulator in TMEM);
- * nicr_conv3d_fwd_mma_sync is the same convolution on the warp-level MMA
- * instructions. nicr_conv3d_error copies and clears the flag the tcgen05
- * kernel sets when one of its bounded waits gives up (synchronous). */
+ * nicr_conv3d_fwd runs on tcgen05.mma (accumulator in TMEM) with TMA-staged
+ * operands (nicr_conv3d_fwd_tma, which returns NICR_ERR_INVALID_ARG when the
+ * driver refuses its tensor maps) and otherwise with cp.async-gathered ones
+ * (nicr_conv3d_fwd_gather); nicr_conv3d_fwd_mma_sync is the same
+ * convolution on the warp-level MMA instructions. nicr_conv3d_error copies
+ * and clears the flag the tcgen05 kernels set when one of their bounded
+ * waits gives up (synchronous). */
 int nicr_conv3d_fwd(const void* x, const void* w, float* y, int n, int d, int h, int w_, int cin, int cout,
                     void* stream);
+int nicr_conv3d_fwd_tma(const void* x, const void* w, float* y, int n, int d, int h, int w_, int cin, int cout,
+                        void* stream);
+int nicr_conv3d_fwd_gather(const void* x, const void* w, float* y, int n, int d, int h, int w_, int cin, int cout,
+                           void* stream);
 int nicr_conv3d_fwd_mma_sync(const void* x, const void* w, float* y, int n, int d, int h, int w_, int cin, int cout,
                              void* stream);
 int nicr_conv3d_wgrad(const void* x, const void* dy, float* dw, int n, int d, int h, int w_, int cin, int cout,

@@ -11,11 +11,15 @@
 //   wgrad    dw[co][tap][ci] = sum_v dy[v][co] * x[v + off(tap)][ci]
 //            (GEMM per tap: M = Cout, N = Cin, K = voxels, split over CTAs)
 // The forward (and so the data gradient) runs on tcgen05.mma with the
-// accumulator in TMEM (k_conv3d_fwd_tc); the weight gradient and the
-// reference forward nicr_conv3d_fwd_mma_sync use the warp-level WMMA
-// instructions (16x16x16 BF16 tiles staged through shared memory).
+// accumulator in TMEM, its operands staged by TMA (k_conv3d_fwd_tma) or, where
+// the driver refuses the tensor maps, gathered with cp.async
+// (k_conv3d_fwd_tc); the weight gradient and the reference forward
+// nicr_conv3d_fwd_mma_sync use the warp-level WMMA instructions (16x16x16
+// BF16 tiles staged through shared memory).
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 #include <mma.h>
 
 #include "../../include/nicr.h"
@@ -298,6 +302,219 @@ __global__ void __launch_bounds__(128) k_conv3d_fwd_tc(const __nv_bfloat16* __re
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(tmem_cols));
 }
 
+// ---------------------------------------------------------------- tcgen05 + TMA
+// The forward with both operands staged by the tensor memory accelerator.
+// Output tile: Wt x Ht voxels of one (batch, z) plane (Wt * Ht = 128 rows of
+// the MMA) x N output channels. Per chunk (tap, KC channels):
+//   A = the 5D box {KC, Wt, Ht, 1, 1} of x at (c0, x0+dx, y0+dy, z+dz, b):
+//       out-of-range coordinates read zeros, which is the convolution's zero
+//       padding, so every tap is a plain coordinate offset;
+//   B = the 3D box {KC, 1, N} of w at (c0, tap, n0).
+// Both land K-major with the swizzle matching KC (64 -> 128 B, 32 -> 64 B,
+// 16 -> 32 B rows), the canonical layouts tcgen05.mma reads (8-row groups
+// SBO = 8 rows apart; K steps of 16 advance the start address by 32 B).
+// Warp 0 lane 0 issues the loads (full barrier: expect_tx), warp 1 lane 0
+// the MMAs (stage freed through its empty barrier by tcgen05.commit), all
+// four warps the epilogue. Waits are bounded as in k_conv3d_fwd_tc.
+struct TmaConv {
+    int kc, swz_bytes, stages, wt, ht, tiles_x, tiles_y, cols;
+    uint32_t a_bytes, b_bytes, stage_bytes;
+    size_t smem;
+};
+
+__device__ __forceinline__ uint64_t umma_sdesc_sw(uint32_t saddr, uint32_t row_bytes) {
+    const uint64_t layout = row_bytes == 128 ? 2 : row_bytes == 64 ? 4 : 6;   // SWIZZLE_128B / 64B / 32B
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | (1ull << 16) |                 // LBO unused (1)
+           ((uint64_t)(((8 * row_bytes) >> 4) & 0x3FFFu) << 32) | (1ull << 46) | (layout << 61);
+}
+
+__device__ __forceinline__ void mbar_expect(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void tma_5d(uint32_t dst, const CUtensorMap* map, int c0, int c1, int c2, int c3, int c4,
+                                       uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.5d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5, %6}], "
+        "[%7];" ::"r"(dst),
+        "l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4), "r"(bar)
+        : "memory");
+}
+
+__device__ __forceinline__ void tma_3d(uint32_t dst, const CUtensorMap* map, int c0, int c1, int c2, uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(
+            dst),
+        "l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(bar)
+        : "memory");
+}
+
+__global__ void __launch_bounds__(128) k_conv3d_fwd_tma(const __grid_constant__ CUtensorMap xmap,
+                                                         const __grid_constant__ CUtensorMap wmap, float* __restrict__ y,
+                                                         const Vol V, int cin, int cout, const TmaConv C) {
+    extern __shared__ unsigned char tma_smem_raw[];
+    const uint32_t raw = smem_u32(tma_smem_raw);
+    const uint32_t base = (raw + 1023u) & ~1023u;   // swizzled stages start on 1024-byte boundaries
+    unsigned char* gen = tma_smem_raw + (base - raw);
+    const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+    const int S = C.stages;
+    uint64_t* full = reinterpret_cast<uint64_t*>(gen + S * C.stage_bytes);
+    uint64_t* empty = full + S;
+    uint64_t* acc_full = empty + S;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acc_full + 1);
+    int* failed = reinterpret_cast<int*>(tmem_slot + 1);
+    int* issued = failed + 1;     // chunks whose loads were issued
+    int* consumed = failed + 2;   // chunks whose loads the MMA thread saw land
+
+    long long tile = blockIdx.x;
+    const int tx = (int)(tile % C.tiles_x);
+    tile /= C.tiles_x;
+    const int ty = (int)(tile % C.tiles_y);
+    tile /= C.tiles_y;
+    const int z = (int)(tile % V.d);
+    const int b = (int)(tile / V.d);
+    const int x0 = tx * C.wt, y0 = ty * C.ht;
+    const int n0 = blockIdx.y * 256;
+    const int N = min(256, cout - n0);
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(C.cols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (t == 32) {
+        for (int s = 0; s < 2 * S + 1; ++s) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(full + s)));
+        asm volatile("fence.mbarrier_init.release.cluster;");
+        *failed = *issued = *consumed = 0;
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+
+    const int chunks_per_tap = cin / C.kc;
+    const int iters = 27 * chunks_per_tap;
+    if (t == 0) {   // producer
+        asm volatile("prefetch.tensormap [%0];" ::"l"(&xmap) : "memory");
+        asm volatile("prefetch.tensormap [%0];" ::"l"(&wmap) : "memory");
+        for (int it = 0; it < iters; ++it) {
+            const int s = it % S;
+            if (it >= S && !mbar_wait(smem_u32(empty + s), (uint32_t)((it / S - 1) & 1))) {
+                atomicExch(failed, 1);
+                break;
+            }
+            const int tap = it / chunks_per_tap, c0 = (it % chunks_per_tap) * C.kc;
+            const uint32_t st = base + s * C.stage_bytes;
+            // the boxes' full bytes arrive, zero-filled parts included
+            mbar_expect(smem_u32(full + s), C.a_bytes + C.b_bytes);
+            tma_5d(st, &xmap, c0, x0 + tap % 3 - 1, y0 + (tap / 3) % 3 - 1, z + tap / 9 - 1, b, smem_u32(full + s));
+            tma_3d(st + C.a_bytes, &wmap, c0, tap, n0, smem_u32(full + s));
+            *issued = it + 1;
+        }
+    } else if (t == 32) {   // MMA issuer
+        const uint32_t idesc = umma_idesc(TC_M, N);
+        const uint32_t row = (uint32_t)C.swz_bytes;
+        int it = 0;
+        for (; it < iters; ++it) {
+            const int s = it % S;
+            if (!mbar_wait(smem_u32(full + s), (uint32_t)((it / S) & 1))) {
+                atomicExch(failed, 1);
+                break;
+            }
+            *consumed = it + 1;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t st = base + s * C.stage_bytes;
+            for (int k = 0; k < C.kc / 16; ++k) {
+                const uint64_t ad = umma_sdesc_sw(st + k * 32, row);
+                const uint64_t bd = umma_sdesc_sw(st + C.a_bytes + k * 32, row);
+                const uint32_t acc = (it > 0 || k > 0) ? 1u : 0u;
+                asm volatile(
+                    "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                    " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
+                    "l"(ad), "l"(bd), "r"(idesc), "r"(acc));
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                smem_u32(empty + s)));
+        }
+        // arrives once every MMA issued so far has completed (also after a timeout)
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+            smem_u32(acc_full)));
+    }
+    __syncwarp();
+    bool ok = mbar_wait(smem_u32(acc_full), 0);
+    __syncthreads();
+    ok = ok && *failed == 0;
+    if (!__syncthreads_or(!ok)) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const int r = warp * 32 + lane;
+        const int yy = y0 + r / C.wt, xx = x0 + r % C.wt;
+        const bool store = yy < V.h && xx < V.w;
+        float* out = y + ((((long long)b * V.d + z) * V.h + yy) * V.w + xx) * cout + n0;
+        for (int c = 0; c < N; c += 16) {
+            uint32_t q[16];
+            const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c;
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+                : "=r"(q[0]), "=r"(q[1]), "=r"(q[2]), "=r"(q[3]), "=r"(q[4]), "=r"(q[5]), "=r"(q[6]), "=r"(q[7]),
+                  "=r"(q[8]), "=r"(q[9]), "=r"(q[10]), "=r"(q[11]), "=r"(q[12]), "=r"(q[13]), "=r"(q[14]), "=r"(q[15])
+                : "r"(taddr));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (store)
+                for (int j = 0; j < 16; j += 4)
+                    *reinterpret_cast<float4*>(out + c + j) =
+                        make_float4(__uint_as_float(q[j]), __uint_as_float(q[j + 1]), __uint_as_float(q[j + 2]),
+                                    __uint_as_float(q[j + 3]));
+        }
+    } else if (t == 0) {
+        atomicExch(&g_conv_error, 1);
+        // loads still in flight land in this CTA's shared memory: wait (bounded) for the issued ones
+        for (int it = *consumed; it < *issued; ++it) mbar_wait(smem_u32(full + it % S), (uint32_t)((it / S) & 1));
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(C.cols));
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (the
+// library links the CUDA runtime statically and not libcuda).
+PFN_cuTensorMapEncodeTiled_v12000 conv_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+    }
+    return fn;
+}
+
+TmaConv tma_conv_plan(const Vol& V, int cin, int cout) {
+    TmaConv C{};
+    C.kc = cin % 64 == 0 ? 64 : cin % 32 == 0 ? 32 : 16;
+    C.swz_bytes = C.kc * 2;
+    C.wt = 1;
+    while (C.wt < V.w && C.wt < TC_M) C.wt <<= 1;
+    C.ht = TC_M / C.wt;
+    C.tiles_x = (V.w + C.wt - 1) / C.wt;
+    C.tiles_y = (V.h + C.ht - 1) / C.ht;
+    const int cmax = cout < 256 ? cout : 256;
+    C.cols = 32;
+    while (C.cols < cmax) C.cols <<= 1;
+    C.a_bytes = (uint32_t)TC_M * C.kc * 2;
+    C.b_bytes = (uint32_t)cmax * C.kc * 2;
+    C.stage_bytes = (C.a_bytes + C.b_bytes + 1023u) & ~1023u;
+    C.stages = (int)((200u * 1024u) / C.stage_bytes);
+    if (C.stages > 8) C.stages = 8;
+    // barriers (2 per stage + 1), the TMEM address and the failure flag, and
+    // 1 KB to align the stages; at least cols x 400 bytes (TMEM per SM)
+    C.smem = (size_t)C.stages * C.stage_bytes + (2 * C.stages + 1) * 8 + 16 + 1024;
+    if (C.smem < (size_t)C.cols * 400) C.smem = (size_t)C.cols * 400;
+    return C;
+}
+
 int check_args(long long voxels, int cin, int cout) {
     if (voxels <= 0 || voxels % 64 != 0 || cin <= 0 || cin % 16 != 0 || cout <= 0 || cout % 16 != 0)
         return NICR_ERR_INVALID_ARG;
@@ -308,8 +525,56 @@ int check_args(long long voxels, int cin, int cout) {
 
 extern "C" {
 
+int nicr_conv3d_fwd_tma(const void* x, const void* w, float* y, int n, int d, int h, int w_, int cin, int cout,
+                        void* stream) {
+    const Vol V{n, d, h, w_};
+    const int rc = check_args(V.voxels(), cin, cout);
+    if (rc != NICR_OK || !x || !w || !y) return rc != NICR_OK ? rc : NICR_ERR_INVALID_ARG;
+    const auto enc = conv_map_encoder();
+    if (!enc) return NICR_ERR_CUDA;
+    const TmaConv C = tma_conv_plan(V, cin, cout);
+    const CUtensorMapSwizzle swz = C.kc == 64 ? CU_TENSOR_MAP_SWIZZLE_128B
+                                   : C.kc == 32 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_32B;
+    const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
+    CUtensorMap xmap, wmap;
+    {   // x: (c, w, h, d, n), boxes {KC, Wt, Ht, 1, 1}
+        const cuuint64_t dims[5] = {(cuuint64_t)cin, (cuuint64_t)w_, (cuuint64_t)h, (cuuint64_t)d, (cuuint64_t)n};
+        const cuuint64_t str[4] = {(cuuint64_t)cin * 2, (cuuint64_t)w_ * cin * 2, (cuuint64_t)h * w_ * cin * 2,
+                                   (cuuint64_t)d * h * w_ * cin * 2};
+        const cuuint32_t box[5] = {(cuuint32_t)C.kc, (cuuint32_t)C.wt, (cuuint32_t)C.ht, 1, 1};
+        if (enc(&xmap, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<void*>(x), dims, str, box, estr,
+                CU_TENSOR_MAP_INTERLEAVE_NONE, swz, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+            return NICR_ERR_INVALID_ARG;
+    }
+    {   // w: (ci, tap, co), boxes {KC, 1, min(cout, 256)}
+        const cuuint64_t dims[3] = {(cuuint64_t)cin, 27, (cuuint64_t)cout};
+        const cuuint64_t str[2] = {(cuuint64_t)cin * 2, (cuuint64_t)27 * cin * 2};
+        const cuuint32_t box[3] = {(cuuint32_t)C.kc, 1, (cuuint32_t)(cout < 256 ? cout : 256)};
+        if (enc(&wmap, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<void*>(w), dims, str, box, estr,
+                CU_TENSOR_MAP_INTERLEAVE_NONE, swz, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+            return NICR_ERR_INVALID_ARG;
+    }
+    if (cudaFuncSetAttribute(k_conv3d_fwd_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C.smem) != cudaSuccess)
+        return NICR_ERR_CUDA;
+    const long long tiles = (long long)C.tiles_x * C.tiles_y * d * n;
+    const dim3 grid((unsigned)tiles, (unsigned)((cout + 255) / 256));
+    k_conv3d_fwd_tma<<<grid, 128, C.smem, static_cast<cudaStream_t>(stream)>>>(xmap, wmap, y, V, cin, cout, C);
+    return cudaGetLastError() == cudaSuccess ? NICR_OK : NICR_ERR_CUDA;
+}
+
 int nicr_conv3d_fwd(const void* x, const void* w, float* y, int n, int d, int h, int w_, int cin, int cout,
                     void* stream) {
+    const int rc = nicr_conv3d_fwd_tma(x, w, y, n, d, h, w_, cin, cout, stream);
+    if (rc != NICR_ERR_INVALID_ARG || check_args((long long)n * d * h * w_, cin, cout) != NICR_OK || !x || !w || !y)
+        return rc;
+    // a tensor map the driver refused: the gathering form
+    return nicr_conv3d_fwd_gather(x, w, y, n, d, h, w_, cin, cout, stream);
+}
+
+int nicr_conv3d_fwd_gather(const void* x, const void* w, float* y, int n, int d, int h, int w_, int cin, int cout,
+                           void* stream) {
     const Vol V{n, d, h, w_};
     const int rc = check_args(V.voxels(), cin, cout);
     if (rc != NICR_OK || !x || !w || !y) return rc != NICR_OK ? rc : NICR_ERR_INVALID_ARG;

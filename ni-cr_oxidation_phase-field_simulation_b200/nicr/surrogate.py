@@ -26,7 +26,8 @@ def _lib():
     L = lib()
     if not getattr(L, "_conv_bound", False):
         vp, i = ctypes.c_void_p, ctypes.c_int
-        for f in ("nicr_conv3d_fwd", "nicr_conv3d_fwd_mma_sync", "nicr_conv3d_wgrad"):
+        for f in ("nicr_conv3d_fwd", "nicr_conv3d_fwd_tma", "nicr_conv3d_fwd_gather", "nicr_conv3d_fwd_mma_sync",
+                  "nicr_conv3d_wgrad"):
             getattr(L, f).argtypes = [vp, vp, vp, i, i, i, i, i, i, vp]
         L.nicr_conv3d_error.argtypes = [ctypes.POINTER(ctypes.c_int)]
         L._conv_bound = True
@@ -40,12 +41,14 @@ def _check(rc, what):
 
 def conv3d_raw(x, w_bf16, form: str = "tcgen05"):
     """y = conv(x, w): x (n, d, h, w, cin) BF16, w (cout, 27, cin) BF16 -> FP32.
-    form "tcgen05" (nicr_conv3d_fwd) or "mma_sync" (nicr_conv3d_fwd_mma_sync)."""
+    form: "tcgen05" (nicr_conv3d_fwd: TMA-staged, else gathered), "tma",
+    "gather" (the two tcgen05 forms alone) or "mma_sync"."""
     import torch
     n, d, h, wd, cin = x.shape
     cout = w_bf16.shape[0]
     y = torch.empty((n, d, h, wd, cout), dtype=torch.float32, device=x.device)
-    f = {"tcgen05": "nicr_conv3d_fwd", "mma_sync": "nicr_conv3d_fwd_mma_sync"}[form]
+    f = {"tcgen05": "nicr_conv3d_fwd", "tma": "nicr_conv3d_fwd_tma", "gather": "nicr_conv3d_fwd_gather",
+         "mma_sync": "nicr_conv3d_fwd_mma_sync"}[form]
     _check(getattr(_lib(), f)(x.data_ptr(), w_bf16.data_ptr(), y.data_ptr(), n, d, h, wd, cin, cout,
                               torch.cuda.current_stream(x.device).cuda_stream), f)
     return y

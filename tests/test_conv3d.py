@@ -45,6 +45,7 @@ def test_conv_abi_rejects_shapes():
     err = nicr._abi.ERR_INVALID_ARG
     for n, d, h, w, ci, co in ((1, 3, 3, 3, 16, 16), (1, 4, 4, 4, 8, 16), (1, 4, 4, 4, 16, 24), (0, 4, 4, 4, 16, 16)):
         assert L.nicr_conv3d_fwd(1, 1, 1, n, d, h, w, ci, co, None) == err
-        assert L.nicr_conv3d_fwd_mma_sync(1, 1, 1, n, d, h, w, ci, co, None) == err
+        for f in ("nicr_conv3d_fwd_mma_sync", "nicr_conv3d_fwd_tma", "nicr_conv3d_fwd_gather"):
+            assert getattr(L, f)(1, 1, 1, n, d, h, w, ci, co, None) == err
         assert L.nicr_conv3d_wgrad(1, 1, 1, n, d, h, w, ci, co, None) == err
     assert L.nicr_conv3d_fwd(None, 1, 1, 1, 4, 4, 4, 16, 16, None) == err

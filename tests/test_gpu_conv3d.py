@@ -34,7 +34,7 @@ def within(got, ref, bound, label):
     assert worst <= TOL, f"{label}: error {worst:.3g} x the absolute-value bound"
 
 
-@pytest.mark.parametrize("form", ["tcgen05", "mma_sync"])
+@pytest.mark.parametrize("form", ["tcgen05", "tma", "gather", "mma_sync"])
 @pytest.mark.parametrize("shape", SHAPES)
 def test_forward(require_gpu, shape, form):
     x, wt, _ = inputs(shape, 1)
