@@ -506,7 +506,11 @@ TmaConv tma_conv_plan(const Vol& V, int cin, int cout) {
     C.a_bytes = (uint32_t)TC_M * C.kc * 2;
     C.b_bytes = (uint32_t)cmax * C.kc * 2;
     C.stage_bytes = (C.a_bytes + C.b_bytes + 1023u) & ~1023u;
-    C.stages = (int)((200u * 1024u) / C.stage_bytes);
+    // about 72 KB of stages (at least 2): two or three CTAs share an SM, so one
+    // CTA's epilogue overlaps another's main loop (64->256 at 64^3: 1029
+    // TFLOP/s, against 808 with 200 KB and one CTA per SM)
+    C.stages = (int)((72u * 1024u) / C.stage_bytes);
+    if (C.stages < 2) C.stages = 2;
     if (C.stages > 8) C.stages = 8;
     // barriers (2 per stage + 1), the TMEM address and the failure flag, and
     // 1 KB to align the stages; at least cols x 400 bytes (TMEM per SM)
