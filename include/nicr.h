@@ -419,7 +419,10 @@ int nicr_slab_box_half(const nicr_handle* h);
  * operands (nicr_conv3d_fwd_tma, which returns NICR_ERR_INVALID_ARG when the
  * driver refuses its tensor maps) and otherwise with cp.async-gathered ones
  * (nicr_conv3d_fwd_gather); nicr_conv3d_fwd_mma_sync is the same
- * convolution on the warp-level MMA instructions. nicr_conv3d_error copies
+ * convolution on the warp-level MMA instructions. nicr_conv3d_wgrad runs on
+ * tcgen05.mma with TMA-staged operands (nicr_conv3d_wgrad_tma: Cout 16, 32,
+ * 64 or a multiple of 128, else NICR_ERR_INVALID_ARG) and otherwise on the
+ * warp-level instructions (nicr_conv3d_wgrad_mma_sync). nicr_conv3d_error copies
  * and clears the flag the tcgen05 kernels set when one of their bounded
  * waits gives up (synchronous). */
 int nicr_conv3d_fwd(const void* x, const void* w, float* y, int n, int d, int h, int w_, int cin, int cout,
@@ -432,6 +435,10 @@ int nicr_conv3d_fwd_mma_sync(const void* x, const void* w, float* y, int n, int 
                              void* stream);
 int nicr_conv3d_wgrad(const void* x, const void* dy, float* dw, int n, int d, int h, int w_, int cin, int cout,
                       void* stream);
+int nicr_conv3d_wgrad_tma(const void* x, const void* dy, float* dw, int n, int d, int h, int w_, int cin, int cout,
+                          void* stream);
+int nicr_conv3d_wgrad_mma_sync(const void* x, const void* dy, float* dw, int n, int d, int h, int w_, int cin, int cout,
+                               void* stream);
 int nicr_conv3d_error(int* flag);
 
 /* The solver program: the reference's run()/main() for dim 2 or 3

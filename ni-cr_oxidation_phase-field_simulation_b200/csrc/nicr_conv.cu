@@ -9,13 +9,14 @@
 //   dgrad    dx = forward(dy, w') with w'[ci][tap][co] = w[co][26-tap][ci]
 //            (off(26 - tap) = -off(tap)); the caller transposes the weights
 //   wgrad    dw[co][tap][ci] = sum_v dy[v][co] * x[v + off(tap)][ci]
-//            (GEMM per tap: M = Cout, N = Cin, K = voxels, split over CTAs)
+//            (GEMM: M = (tap, Cout), N = Cin, K = voxels, split over CTAs)
 // The forward (and so the data gradient) runs on tcgen05.mma with the
 // accumulator in TMEM, its operands staged by TMA (k_conv3d_fwd_tma) or, where
 // the driver refuses the tensor maps, gathered with cp.async
-// (k_conv3d_fwd_tc); the weight gradient and the reference forward
-// nicr_conv3d_fwd_mma_sync use the warp-level WMMA instructions (16x16x16
-// BF16 tiles staged through shared memory).
+// (k_conv3d_fwd_tc); the weight gradient runs on tcgen05.mma with TMA-staged
+// operands (k_conv3d_wgrad_tma) for Cout 16, 32, 64 or multiples of 128. The
+// warp-level WMMA forms (16x16x16 BF16 tiles staged through shared memory)
+// stay as reference forms and as the weight gradient of other Cout.
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
@@ -519,6 +520,219 @@ TmaConv tma_conv_plan(const Vol& V, int cin, int cout) {
     return C;
 }
 
+// ---------------------------------------------------------------- weight gradient, tcgen05 + TMA
+// dw[co][tap][ci] = sum_u dy[u - off(tap)][co] * x[u][ci] (u runs over the
+// voxels of x; dy is zero outside the grid): one GEMM with M = (tap, co)
+// rows, N = ci, K = voxels. An M tile holds 128/Cout taps of all Cout
+// channels (Cout 16, 32 or 64) or 128 channels of one tap (Cout a multiple of
+// 128); K advances by tiles of 64 voxels (Wt x Ht of one (batch, z) plane) and
+// is split over CTAs, which add their partial sums to dw with FP32 atomics.
+// Per K tile: A = for each tap of the M tile, the box {Ws_a, Wt, Ht, 1, 1} of
+// dy at (co0, x0-dx, y0-dy, z-dz, b) (zero fill = zero outside); B = the
+// boxes {Ws_b, Wt, Ht, 1, 1} of x at (ci0, x0, y0, z, b). Both land MN-major
+// (rows = the 64 voxels, each row Ws channels), with the swizzle of Ws
+// (64 -> 128 B, 32 -> 64 B, 16 -> 32 B): 8-row groups SBO = 8 rows apart, the
+// blocks of Ws channels LBO = one box apart; an MMA (K = 16) takes two
+// 8-row groups.
+struct TmaWgrad {
+    int wsa, wsb, taps_per_m, m_tiles, co_blocks, n_tiles, wt, ht, tiles_x, tiles_y, ktiles, parts, per_part,
+        stages, cols;
+    uint32_t a_box, b_box, a_bytes, b_bytes, stage_bytes;
+    size_t smem;
+};
+
+constexpr int WG_K = 64;   // voxels per K tile
+
+__device__ __forceinline__ uint64_t umma_sdesc_mn(uint32_t saddr, uint32_t row_bytes, uint32_t lbo) {
+    const uint64_t layout = row_bytes == 128 ? 2 : row_bytes == 64 ? 4 : 6;
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)(((8 * row_bytes) >> 4) & 0x3FFFu) << 32) | (1ull << 46) | (layout << 61);
+}
+
+__global__ void __launch_bounds__(128) k_conv3d_wgrad_tma(const __grid_constant__ CUtensorMap dymap,
+                                                           const __grid_constant__ CUtensorMap xmap, float* __restrict__ dw,
+                                                           const Vol V, int cin, int cout, const TmaWgrad G) {
+    extern __shared__ unsigned char wg_smem_raw[];
+    const uint32_t raw = smem_u32(wg_smem_raw);
+    const uint32_t base = (raw + 1023u) & ~1023u;
+    unsigned char* gen = wg_smem_raw + (base - raw);
+    const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+    const int S = G.stages;
+    uint64_t* full = reinterpret_cast<uint64_t*>(gen + S * G.stage_bytes);
+    uint64_t* empty = full + S;
+    uint64_t* acc_full = empty + S;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acc_full + 1);
+    int* failed = reinterpret_cast<int*>(tmem_slot + 1);
+    int* issued = failed + 1;
+    int* consumed = failed + 2;
+
+    const int part = blockIdx.x, mt = blockIdx.y, n0 = blockIdx.z * 256;
+    const int N = min(256, cin - n0);
+    // M tile: taps tap0 .. tap0 + taps_per_m - 1 (those < 27) of channels co0 .. co0 + mrows / taps - 1
+    const int tap0 = G.co_blocks > 1 ? mt / G.co_blocks : mt * G.taps_per_m;
+    const int co0 = G.co_blocks > 1 ? (mt % G.co_blocks) * 128 : 0;
+    const int ntaps = G.co_blocks > 1 ? 1 : min(G.taps_per_m, 27 - tap0);
+    const int co_rows = G.co_blocks > 1 ? 128 : cout;   // M rows per tap
+    const int a_boxes_per_tap = co_rows / G.wsa;
+    const int b_boxes = N / G.wsb;
+    const int k_begin = part * G.per_part, k_end = min(G.ktiles, k_begin + G.per_part);
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(G.cols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (t == 32) {
+        for (int s = 0; s < 2 * S + 1; ++s) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(full + s)));
+        asm volatile("fence.mbarrier_init.release.cluster;");
+        *failed = *issued = *consumed = 0;
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+    const int iters = k_end - k_begin;
+
+    if (t == 0) {   // producer
+        asm volatile("prefetch.tensormap [%0];" ::"l"(&dymap) : "memory");
+        asm volatile("prefetch.tensormap [%0];" ::"l"(&xmap) : "memory");
+        for (int it = 0; it < iters; ++it) {
+            const int s = it % S;
+            if (it >= S && !mbar_wait(smem_u32(empty + s), (uint32_t)((it / S - 1) & 1))) {
+                atomicExch(failed, 1);
+                break;
+            }
+            long long kt = k_begin + it;
+            const int tx = (int)(kt % G.tiles_x);
+            kt /= G.tiles_x;
+            const int ty = (int)(kt % G.tiles_y);
+            kt /= G.tiles_y;
+            const int z = (int)(kt % V.d), b = (int)(kt / V.d);
+            const int x0 = tx * G.wt, y0 = ty * G.ht;
+            const uint32_t st = base + s * G.stage_bytes, bar = smem_u32(full + s);
+            mbar_expect(bar, (uint32_t)(ntaps * a_boxes_per_tap) * G.a_box + (uint32_t)b_boxes * G.b_box);
+            for (int q = 0; q < ntaps; ++q) {
+                const int tap = tap0 + q;
+                for (int j = 0; j < a_boxes_per_tap; ++j)
+                    tma_5d(st + (uint32_t)(q * a_boxes_per_tap + j) * G.a_box, &dymap, co0 + j * G.wsa,
+                           x0 - (tap % 3 - 1), y0 - ((tap / 3) % 3 - 1), z - (tap / 9 - 1), b, bar);
+            }
+            for (int j = 0; j < b_boxes; ++j)
+                tma_5d(st + G.a_bytes + (uint32_t)j * G.b_box, &xmap, n0 + j * G.wsb, x0, y0, z, b, bar);
+            *issued = it + 1;
+        }
+    } else if (t == 32) {   // MMA issuer
+        const uint32_t idesc = umma_idesc(TC_M, N) | (1u << 15) | (1u << 16);   // A and B MN-major
+        const uint32_t ra = (uint32_t)G.wsa * 2, rb = (uint32_t)G.wsb * 2;
+        for (int it = 0; it < iters; ++it) {
+            const int s = it % S;
+            if (!mbar_wait(smem_u32(full + s), (uint32_t)((it / S) & 1))) {
+                atomicExch(failed, 1);
+                break;
+            }
+            *consumed = it + 1;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t st = base + s * G.stage_bytes;
+            for (int k = 0; k < WG_K / 16; ++k) {   // two 8-row groups per MMA
+                const uint64_t ad = umma_sdesc_mn(st + k * 16 * ra, ra, G.a_box);
+                const uint64_t bd = umma_sdesc_mn(st + G.a_bytes + k * 16 * rb, rb, G.b_box);
+                const uint32_t acc = (it > 0 || k > 0) ? 1u : 0u;
+                asm volatile(
+                    "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                    " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
+                    "l"(ad), "l"(bd), "r"(idesc), "r"(acc));
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                smem_u32(empty + s)));
+        }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+            smem_u32(acc_full)));
+    }
+    __syncwarp();
+    bool ok = iters > 0 ? mbar_wait(smem_u32(acc_full), 0) : true;
+    __syncthreads();
+    ok = ok && *failed == 0;
+    if (!__syncthreads_or(!ok)) {
+        if (iters > 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const int r = warp * 32 + lane;   // M row = (tap, co)
+            const int q = r / co_rows, co = co0 + r % co_rows;
+            const bool store = q < ntaps;
+            float* out = dw + ((long long)co * 27 + tap0 + q) * cin + n0;
+            for (int c = 0; c < N; c += 16) {
+                uint32_t v[16];
+                const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c;
+                asm volatile(
+                    "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+                    : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                      "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+                    : "r"(taddr));
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                if (store)
+                    for (int j = 0; j < 16; j += 4)
+                        atomicAdd(reinterpret_cast<float4*>(out + c + j),
+                                  make_float4(__uint_as_float(v[j]), __uint_as_float(v[j + 1]), __uint_as_float(v[j + 2]),
+                                              __uint_as_float(v[j + 3])));
+            }
+        }
+    } else if (t == 0) {
+        atomicExch(&g_conv_error, 1);
+        for (int it = *consumed; it < *issued; ++it) mbar_wait(smem_u32(full + it % S), (uint32_t)((it / S) & 1));
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(G.cols));
+}
+
+// The plan, or false when the shapes are outside the TMA form (Cout not 16,
+// 32, 64 or a multiple of 128).
+bool tma_wgrad_plan(const Vol& V, int cin, int cout, TmaWgrad& G) {
+    G = TmaWgrad{};
+    if (cout == 16 || cout == 32 || cout == 64) {
+        G.wsa = cout;
+        G.taps_per_m = TC_M / cout;
+        G.co_blocks = 1;
+        G.m_tiles = (27 + G.taps_per_m - 1) / G.taps_per_m;
+    } else if (cout % 128 == 0) {
+        G.wsa = 64;
+        G.taps_per_m = 1;
+        G.co_blocks = cout / 128;
+        G.m_tiles = 27 * G.co_blocks;
+    } else {
+        return false;
+    }
+    G.wsb = cin % 64 == 0 ? 64 : cin % 32 == 0 ? 32 : 16;
+    G.n_tiles = (cin + 255) / 256;
+    const int nmax = cin < 256 ? cin : 256;
+    G.wt = 1;
+    while (G.wt < V.w && G.wt < WG_K) G.wt <<= 1;
+    G.ht = WG_K / G.wt;
+    G.tiles_x = (V.w + G.wt - 1) / G.wt;
+    G.tiles_y = (V.h + G.ht - 1) / G.ht;
+    G.ktiles = G.tiles_x * G.tiles_y * V.d * V.n;
+    // enough CTAs for about 8 per SM, each with at least 16 K tiles
+    const long long mn = (long long)G.m_tiles * G.n_tiles;
+    long long parts = (148LL * 8 + mn - 1) / mn;
+    const long long most = (G.ktiles + 15) / 16;
+    if (parts > most) parts = most;
+    if (parts < 1) parts = 1;
+    G.per_part = (int)((G.ktiles + parts - 1) / parts);
+    G.parts = (G.ktiles + G.per_part - 1) / G.per_part;
+    G.cols = 32;
+    while (G.cols < nmax) G.cols <<= 1;
+    G.a_box = (uint32_t)WG_K * G.wsa * 2;
+    G.b_box = (uint32_t)WG_K * G.wsb * 2;
+    G.a_bytes = (uint32_t)TC_M * WG_K * 2;
+    G.b_bytes = (uint32_t)nmax * WG_K * 2;
+    G.stage_bytes = (G.a_bytes + G.b_bytes + 1023u) & ~1023u;
+    G.stages = (int)((72u * 1024u) / G.stage_bytes);
+    if (G.stages < 2) G.stages = 2;
+    if (G.stages > 8) G.stages = 8;
+    G.smem = (size_t)G.stages * G.stage_bytes + (2 * G.stages + 1) * 8 + 16 + 1024;
+    if (G.smem < (size_t)G.cols * 400) G.smem = (size_t)G.cols * 400;
+    return true;
+}
+
 int check_args(long long voxels, int cin, int cout) {
     if (voxels <= 0 || voxels % 64 != 0 || cin <= 0 || cin % 16 != 0 || cout <= 0 || cout % 16 != 0)
         return NICR_ERR_INVALID_ARG;
@@ -611,8 +825,52 @@ int nicr_conv3d_fwd_mma_sync(const void* x, const void* w, float* y, int n, int 
     return cudaGetLastError() == cudaSuccess ? NICR_OK : NICR_ERR_CUDA;
 }
 
+int nicr_conv3d_wgrad_tma(const void* x, const void* dy, float* dw, int n, int d, int h, int w_, int cin, int cout,
+                          void* stream) {
+    const Vol V{n, d, h, w_};
+    const int rc = check_args(V.voxels(), cin, cout);
+    if (rc != NICR_OK || !x || !dy || !dw) return rc != NICR_OK ? rc : NICR_ERR_INVALID_ARG;
+    TmaWgrad G;
+    if (!tma_wgrad_plan(V, cin, cout, G)) return NICR_ERR_INVALID_ARG;
+    const auto enc = conv_map_encoder();
+    if (!enc) return NICR_ERR_CUDA;
+    auto swz = [](int ws) {
+        return ws == 64 ? CU_TENSOR_MAP_SWIZZLE_128B : ws == 32 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_32B;
+    };
+    const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
+    CUtensorMap dymap, xmap;
+    // (c, w, h, d, n) views of dy (Cout channels) and x (Cin channels), boxes {Ws, Wt, Ht, 1, 1}
+    auto encode = [&](CUtensorMap* m, const void* p, int c, int ws) {
+        const cuuint64_t dims[5] = {(cuuint64_t)c, (cuuint64_t)w_, (cuuint64_t)h, (cuuint64_t)d, (cuuint64_t)n};
+        const cuuint64_t str[4] = {(cuuint64_t)c * 2, (cuuint64_t)w_ * c * 2, (cuuint64_t)h * w_ * c * 2,
+                                   (cuuint64_t)d * h * w_ * c * 2};
+        const cuuint32_t box[5] = {(cuuint32_t)ws, (cuuint32_t)G.wt, (cuuint32_t)G.ht, 1, 1};
+        return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<void*>(p), dims, str, box, estr,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, swz(ws), CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+    };
+    if (!encode(&dymap, dy, cout, G.wsa) || !encode(&xmap, x, cin, G.wsb)) return NICR_ERR_INVALID_ARG;
+    if (cudaFuncSetAttribute(k_conv3d_wgrad_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G.smem) !=
+        cudaSuccess)
+        return NICR_ERR_CUDA;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (cudaMemsetAsync(dw, 0, sizeof(float) * (size_t)cout * 27 * cin, s) != cudaSuccess) return NICR_ERR_CUDA;
+    const dim3 grid((unsigned)G.parts, (unsigned)G.m_tiles, (unsigned)G.n_tiles);
+    k_conv3d_wgrad_tma<<<grid, 128, G.smem, s>>>(dymap, xmap, dw, V, cin, cout, G);
+    return cudaGetLastError() == cudaSuccess ? NICR_OK : NICR_ERR_CUDA;
+}
+
 int nicr_conv3d_wgrad(const void* x, const void* dy, float* dw, int n, int d, int h, int w_, int cin, int cout,
                       void* stream) {
+    const int rc = nicr_conv3d_wgrad_tma(x, dy, dw, n, d, h, w_, cin, cout, stream);
+    if (rc != NICR_ERR_INVALID_ARG || check_args((long long)n * d * h * w_, cin, cout) != NICR_OK || !x || !dy || !dw)
+        return rc;
+    // Cout outside the TMA form, or tensor maps the driver refused
+    return nicr_conv3d_wgrad_mma_sync(x, dy, dw, n, d, h, w_, cin, cout, stream);
+}
+
+int nicr_conv3d_wgrad_mma_sync(const void* x, const void* dy, float* dw, int n, int d, int h, int w_, int cin, int cout,
+                               void* stream) {
     const Vol V{n, d, h, w_};
     const int rc = check_args(V.voxels(), cin, cout);
     if (rc != NICR_OK || !x || !dy || !dw) return rc != NICR_OK ? rc : NICR_ERR_INVALID_ARG;

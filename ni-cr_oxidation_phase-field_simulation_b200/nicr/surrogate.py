@@ -27,7 +27,7 @@ def _lib():
     if not getattr(L, "_conv_bound", False):
         vp, i = ctypes.c_void_p, ctypes.c_int
         for f in ("nicr_conv3d_fwd", "nicr_conv3d_fwd_tma", "nicr_conv3d_fwd_gather", "nicr_conv3d_fwd_mma_sync",
-                  "nicr_conv3d_wgrad"):
+                  "nicr_conv3d_wgrad", "nicr_conv3d_wgrad_tma", "nicr_conv3d_wgrad_mma_sync"):
             getattr(L, f).argtypes = [vp, vp, vp, i, i, i, i, i, i, vp]
         L.nicr_conv3d_error.argtypes = [ctypes.POINTER(ctypes.c_int)]
         L._conv_bound = True
@@ -62,14 +62,17 @@ def conv_error() -> int:
     return flag.value
 
 
-def conv3d_wgrad_raw(x, dy):
-    """dw[co][tap][ci] = sum_v dy[v][co] x[v + off(tap)][ci] (FP32)."""
+def conv3d_wgrad_raw(x, dy, form: str = "tcgen05"):
+    """dw[co][tap][ci] = sum_v dy[v][co] x[v + off(tap)][ci] (FP32). form:
+    "tcgen05" (nicr_conv3d_wgrad: TMA-staged where Cout allows, else WMMA),
+    "tma" or "mma_sync" alone."""
     import torch
     n, d, h, wd, cin = x.shape
     cout = dy.shape[-1]
     dw = torch.empty((cout, 27, cin), dtype=torch.float32, device=x.device)
-    _check(_lib().nicr_conv3d_wgrad(x.data_ptr(), dy.data_ptr(), dw.data_ptr(), n, d, h, wd, cin, cout,
-                                    torch.cuda.current_stream(x.device).cuda_stream), "nicr_conv3d_wgrad")
+    f = {"tcgen05": "nicr_conv3d_wgrad", "tma": "nicr_conv3d_wgrad_tma", "mma_sync": "nicr_conv3d_wgrad_mma_sync"}[form]
+    _check(getattr(_lib(), f)(x.data_ptr(), dy.data_ptr(), dw.data_ptr(), n, d, h, wd, cin, cout,
+                              torch.cuda.current_stream(x.device).cuda_stream), f)
     return dw
 
 

@@ -47,5 +47,6 @@ def test_conv_abi_rejects_shapes():
         assert L.nicr_conv3d_fwd(1, 1, 1, n, d, h, w, ci, co, None) == err
         for f in ("nicr_conv3d_fwd_mma_sync", "nicr_conv3d_fwd_tma", "nicr_conv3d_fwd_gather"):
             assert getattr(L, f)(1, 1, 1, n, d, h, w, ci, co, None) == err
-        assert L.nicr_conv3d_wgrad(1, 1, 1, n, d, h, w, ci, co, None) == err
+        for f in ("nicr_conv3d_wgrad", "nicr_conv3d_wgrad_tma", "nicr_conv3d_wgrad_mma_sync"):
+            assert getattr(L, f)(1, 1, 1, n, d, h, w, ci, co, None) == err
     assert L.nicr_conv3d_fwd(None, 1, 1, 1, 4, 4, 4, 16, 16, None) == err

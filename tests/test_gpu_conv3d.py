@@ -53,13 +53,23 @@ def test_data_gradient(require_gpu, shape):
     within(dx, dx_ref, conv_ref.conv3d(dy.abs(), wf.abs()), "data gradient")
 
 
+TMA_WGRAD_COUT = (16, 32, 64, 128, 256)
+
+
+@pytest.mark.parametrize("form", ["tcgen05", "tma", "mma_sync"])
 @pytest.mark.parametrize("shape", SHAPES)
-def test_weight_gradient(require_gpu, shape):
+def test_weight_gradient(require_gpu, shape, form):
     x, wt, dy = inputs(shape, 3)
+    xb, dyb = x.cuda().bfloat16(), dy.cuda().bfloat16()
+    if form == "tma" and shape[-1] not in TMA_WGRAD_COUT:
+        with pytest.raises(RuntimeError):
+            surrogate.conv3d_wgrad_raw(xb, dyb, form)
+        return
     _, dw_ref = conv_ref.grads(x, wt, dy)
     _, dw_abs = conv_ref.grads(x.abs(), wt, dy.abs())
-    dw = surrogate.conv3d_wgrad_raw(x.cuda().bfloat16(), dy.cuda().bfloat16())
-    within(dw, dw_ref, dw_abs, "weight gradient")
+    dw = surrogate.conv3d_wgrad_raw(xb, dyb, form)
+    within(dw, dw_ref, dw_abs, f"weight gradient ({form})")
+    assert surrogate.conv_error() == 0
 
 
 def test_autograd_wrapper(require_gpu):
