@@ -427,6 +427,7 @@ def surrogate_workload(args) -> int:
     sol.run(20)
     plain_ms = timed(lambda: sol.run(16), reps=5) / 16
     sol.close()
+    jumps = None if args.no_jumps else surrogate_jumps(dev)
     best = max(rows, key=lambda r: r["fwd_tcgen05_tflops"])
     out = {"workload": "surrogate", "metric": "surrogate conv3d forward TFLOP/s (BF16 in, FP32 accumulate)",
            "unit": "TFLOP/s", "value": best["fwd_tcgen05_tflops"], "dtype": "bf16",
@@ -435,9 +436,62 @@ def surrogate_workload(args) -> int:
                         "frac": best["fwd_tcgen05_tflops"] / peak, "peak_kind": peak_kind},
            "layers": rows, "unet_forward_128cube_ms": fwd_ms, "train_step_64cube_batch2_ms": train_ms,
            "plain_fp64_step_128cube_ms": plain_ms,
-           "break_even_k": fwd_ms / plain_ms, "conv_error_flag": err, "clocks": cl, "data": "synthetic"}
+           "break_even_k": fwd_ms / plain_ms, "jumps": jumps, "conv_error_flag": err, "clocks": cl,
+           "data": "synthetic"}
     print(json.dumps(out))
     return 0
+
+
+def surrogate_jumps(dev, size=128, every=32, ks=2, steps=1024, iters=1200):
+    """The surrogate against the plain FP64 path at size^3 (static Voronoi,
+    Ksp, parameters drawn per seed): trajectories of seeds 100-103 (`steps`
+    steps, a sample every `every`), a U-Net (base 16) trained `iters` Adam
+    steps to jump K = ks x every steps, then seed 104 advanced `steps` steps
+    by JumpStepper (mass gate 5% and 25%) and by nicr_run from the same state
+    after 64 plain steps; wall clock of each (synchronised), counts, the
+    gates' values per trial, and the relative L-inf error of the jump runs
+    against the plain run."""
+    import torch
+    import nicr
+    from nicr import surrogate
+    cfgs = surrogate.trajectory_configs(5, size, first_seed=100)
+    t0 = time.perf_counter()
+    x, r = surrogate.trajectories(cfgs[:4], steps, every)
+    t1 = time.perf_counter()
+    torch.manual_seed(0)
+    net = surrogate.unet(4, 16).to(dev)
+    norm, losses = surrogate.train(net, x, r, ks, ks * every, iters=iters, batch=1)
+    torch.cuda.synchronize()
+    t2 = time.perf_counter()
+    del x, r
+    plain = nicr.Solver(cfgs[4])
+    plain.run(64)
+    torch.cuda.synchronize()
+    t3 = time.perf_counter()
+    plain.run(steps)
+    torch.cuda.synchronize()
+    plain_s = time.perf_counter() - t3
+    out = {"size": size, "k": ks * every, "steps": steps, "trajectory_s": t1 - t0, "train_s": t2 - t1,
+           "train_iters": iters, "loss_first20": float(np.mean(losses[:20])),
+           "loss_last20": float(np.mean(losses[-20:])), "plain_wall_s": plain_s, "runs": []}
+    for tol in (0.05, 0.25):
+        jump = nicr.Solver(cfgs[4])
+        jump.run(64)
+        st = surrogate.JumpStepper(jump, net, norm, ks * every, mass_tol=tol)
+        torch.cuda.synchronize()
+        t4 = time.perf_counter()
+        counts = st.advance(steps)
+        torch.cuda.synchronize()
+        jump_s = time.perf_counter() - t4
+        err = {f: float(np.abs(jump.get(f) - plain.get(f)).max() / max(np.abs(plain.get(f)).max(), 1e-300))
+               for f in ("o", "cr")}
+        out["runs"].append({"mass_tol": tol, "counts": counts, "jump_wall_s": jump_s,
+                            "simulated_time_per_wall_s_ratio": plain_s / jump_s, "rel_linf_vs_plain": err,
+                            "gates": [[round(a, 4), round(b, 4), None if c is None else round(c, 3)]
+                                      for a, b, c in st.gates]})
+        jump.close()
+    plain.close()
+    return out
 
 
 def slabs_workload(args) -> int:
@@ -620,6 +674,7 @@ def main():
                          "slab-ranks: the domain split over the torchrun ranks (one slab per GPU); "
                          "surrogate: the learned surrogate's convolution kernels and U-Net at 128^3")
     ap.add_argument("--precision", type=int, default=0, help="arithmetic form of --workload sweep (0 drop-in, 1 fast)")
+    ap.add_argument("--no-jumps", action="store_true", help="--workload surrogate: kernels only, no training and jump runs")
     args = ap.parse_args()
     if args.e2e_steps <= 0:
         args.e2e_steps = args.steps

@@ -150,6 +150,16 @@ int nicr_get_seeds(const nicr_handle* h, double* xyz, long long* volumes);
  * M_*). Host buffers in pinned memory transfer at full PCIe speed. */
 int nicr_set_field(nicr_handle* h, int field, int index, const double* host);
 int nicr_get_field(nicr_handle* h, int field, int index, double* host);
+/* Device view of one field of the current state (no copy; no counterpart in
+ * the reference): *ptr points at cell (0, 0, 0) and cell (i, j, k) of the
+ * nx x ny x nz grid (2D: nx x 1 x ny) is (*ptr)[(i * ny + j) * pitch + k],
+ * FP64. The view is valid until the next step, nucleation, load or field
+ * write of the handle (steps alternate buffers); the handle's stream has no
+ * work pending when it returns. writable = 1 (O, CR, PHI, ETA only) marks
+ * the frozen-eta cache stale as nicr_set_field does; the caller then writes
+ * through the view before the next call on the handle, on a stream ordered
+ * with the handle's (nicr_stream). Whole-domain handles only. */
+int nicr_field_device(nicr_handle* h, int field, int index, int writable, void** ptr, long long* pitch);
 
 /* Model::refresh (3S:597-620): materialises mu_O, mu_Cr, M_O, M_Cr (and the
  * eta mask) for output. Steps do not need it; they fuse it on chip. */

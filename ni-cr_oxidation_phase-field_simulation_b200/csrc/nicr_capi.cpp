@@ -138,6 +138,22 @@ int nicr_tune(nicr_handle* h, int reps, int* xchunk, int* minb) {
 int nicr_refresh(nicr_handle* h) {
     return guarded(h, [&](nicr::Model& m) { m.refresh(); m.sync(); return (int)NICR_OK; });
 }
+int nicr_field_device(nicr_handle* h, int field, int index, int writable, void** ptr, long long* pitch) {
+    return guarded(h, [&](nicr::Model& m) {
+        if (!ptr || !pitch) return (int)NICR_ERR_INVALID_ARG;
+        if (m.is_slab) throw nicr::Error(NICR_ERR_STATE, "device views are of whole-domain handles (slabs: nicr_slab_region)");
+        if (writable) {
+            *ptr = m.state_ptr(field, index);
+            m.invalidate_eta_cache();   // as after nicr_set_field
+        } else {
+            *ptr = const_cast<double*>(m.field_ptr(field, index));   // may materialise the eta mask
+        }
+        m.sync();
+        *pitch = m.g.pb;
+        return (int)NICR_OK;
+    });
+}
+
 int nicr_invalidate_eta_cache(nicr_handle* h) {
     return guarded(h, [&](nicr::Model& m) { m.invalidate_eta_cache(); return (int)NICR_OK; });
 }

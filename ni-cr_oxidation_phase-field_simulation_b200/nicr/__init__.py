@@ -103,6 +103,8 @@ def lib():
     L.nicr_main.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_char_p)]
     L.nicr_stream.argtypes = [H]
     L.nicr_stream.restype = ctypes.c_void_p
+    L.nicr_field_device.argtypes = [H, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p),
+                                    ctypes.POINTER(ctypes.c_longlong)]
     L.nicr_tune.argtypes = [H, ctypes.c_int, ip, ip]
     L.nicr_batch_tune.argtypes = [H, ctypes.c_int, ip]
     L.nicr_save_state.argtypes = [H, ctypes.c_char_p]
@@ -193,6 +195,14 @@ def parse_args(dim: int, argv: list[str]):
 
 def _dp(a: np.ndarray):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+class _DeviceArray:
+    """__cuda_array_interface__ of an FP64 device array owned by a handle."""
+
+    def __init__(self, ptr: int, shape, strides):
+        self.__cuda_array_interface__ = {"shape": tuple(shape), "strides": tuple(strides), "typestr": "<f8",
+                                         "data": (ptr, False), "version": 3, "stream": None}
 
 
 class Solver:
@@ -405,6 +415,25 @@ class Solver:
 
     def stream(self) -> int:
         return lib().nicr_stream(self.h) or 0
+
+    def device_view(self, name: str, index: int = 0, writable: bool = False):
+        """The field's device storage as a torch tensor (no copy), shaped like
+        get(): valid until the next call that steps, nucleates, loads or sets
+        fields (nicr_field_device). writable=True for o, cr, p and eta; the
+        caller synchronises its stream before the next call on the handle."""
+        import torch
+        if name.startswith("eta") and name[3:].isdigit():
+            index, name = int(name[3:]) - 1, "eta"
+        ptr, pitch = ctypes.c_void_p(), ctypes.c_longlong()
+        self._check(lib().nicr_field_device(self.h, FIELD[name], index, int(writable), ctypes.byref(ptr),
+                                            ctypes.byref(pitch)))
+        i = self.info()
+        rows = i.ny if i.dim == 3 else 1
+        cols = i.nz if i.dim == 3 else i.ny
+        # torch takes no read-only CUDA arrays: a read view must not be written
+        view = _DeviceArray(ptr.value, (i.nx, rows, cols), (rows * pitch.value * 8, pitch.value * 8, 8))
+        t = torch.as_tensor(view, device=f"cuda:{self.cfg.device}")
+        return t if i.dim == 3 else t[:, 0, :]
 
 
 class Batch:

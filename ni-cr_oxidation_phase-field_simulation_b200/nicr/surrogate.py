@@ -191,25 +191,26 @@ def trajectory_configs(n: int, size: int, first_seed: int = 100, **kw):
 def trajectories(cfgs, steps: int, every: int, probe: int = 2, device: int = 0):
     """States (fields o, cr, p, gb) of each run at steps every, 2 every, ...,
     and their per-step rates over the `probe` steps before each: tensors
-    x, r of shape (runs, steps // every, size, size, size, 4) on the GPU."""
+    x, r of shape (runs, steps // every, size, size, size, 4), FP32 on the
+    GPU (read in place through Solver.device_view)."""
     import torch
     from . import Solver
     xs, rs = [], []
     for c in cfgs:
         c.device = device
         s = Solver(c)
-        state = lambda: np.stack([s.get(f) for f in FIELDS], axis=-1)
+        state = lambda: torch.stack([s.device_view(f) for f in FIELDS], dim=-1)
         x, r = [], []
         for _ in range(steps // every):
             s.run(every - probe)
             a = state()
             s.run(probe)
             b = state()
-            x.append(b)
-            r.append((b - a) / probe)
+            x.append(b.float())
+            r.append(((b - a) / probe).float())
         s.close()
-        xs.append(torch.tensor(np.stack(x), dtype=torch.float32, device=f"cuda:{device}"))
-        rs.append(torch.tensor(np.stack(r), dtype=torch.float32, device=f"cuda:{device}"))
+        xs.append(torch.stack(x))
+        rs.append(torch.stack(r))
     return torch.stack(xs), torch.stack(rs)
 
 
@@ -299,35 +300,41 @@ def relative_errors(model, norm, x, r, k: int):
 
 # ------------------------------------------------------------------ jumps
 class JumpStepper:
-    """Advances a Solver by plain steps and surrogate jumps of K steps.
+    """Advances a Solver by plain steps and surrogate jumps of K steps, with
+    the state read and written in place on the GPU (Solver.device_view).
 
     A jump is tried only where no Ksp scan falls inside it. It runs: `probe`
-    plain steps (which measure the per-step change and the FP64 rate of
-    change of total O and Cr), the network's proposal for K steps ahead, the
-    mass-budget gate, and `probe` plain re-check steps from the proposal.
+    plain steps (which measure the per-step rate of every field and the FP64
+    rate of change of total O and Cr), the network's proposal for K steps
+    ahead, the mass-budget gate, and `probe` plain re-check steps from the
+    proposal.
 
     Mass budget: the proposal's change of total O and of total Cr must equal
     K x the measured FP64 rate up to a correction c x |change| per cell with
     |c| <= mass_tol; the correction is then applied, so the accepted state
-    carries exactly the extrapolated budget (summed in FP64), and the amounts
-    a jump adds are kept in `ledger` so that the solver's budget still
-    closes. Re-check: the per-step change of the re-check steps may be at
-    most recheck_factor x that of the probe steps (an off-manifold proposal
-    relaxes fast in its first plain steps). A jump failing either gate is
-    rolled back from a checkpoint and K plain steps run instead.
+    carries exactly the extrapolated budget (summed in FP64). Re-check: the
+    per-step change of the re-check steps may be at most recheck_factor x
+    that of the probe steps (an off-manifold proposal relaxes fast in its
+    first plain steps). A jump failing either gate is rolled back to the
+    state before it (device copies of c_O, c_Cr, phi) and K plain steps run
+    instead. `ledger` holds what the solver's budget does not see: the
+    amounts of accepted jumps, less the budget increments of re-check steps
+    that were rolled back.
 
     The stepper keeps the simulated clock itself: the solver's own step
     counter does not see jumps, so plain stepping uses nicr_step and the Ksp
     scans fire here (before the step whose physical time reaches the next
-    scan time, as nicr_run fires them).
+    scan time, as nicr_run fires them). Grains must be static (the jump
+    leaves eta as it is).
     """
 
     def __init__(self, solver, model, norm, k: int, probe: int = 2, mass_tol: float = 0.05,
-                 recheck_factor: float = 4.0, workdir=None):
-        import tempfile
+                 recheck_factor: float = 4.0):
         from . import NUCLEATION
         if norm is not None and norm.steps_k != k:
             raise ValueError(f"the network predicts {norm.steps_k} steps ahead, not {k}")
+        if model is not None and solver.cfg.grain_evolution:
+            raise ValueError("jumps leave eta unchanged: static grains only")
         self.s, self.model, self.norm, self.k, self.probe = solver, model, norm, k, probe
         self.mass_tol, self.recheck_factor = mass_tol, recheck_factor
         c = solver.cfg
@@ -337,11 +344,10 @@ class JumpStepper:
         self.next_scan = self.period
         while self._due(self.t):
             self.next_scan += self.period
-        self._tmp = tempfile.TemporaryDirectory(dir=workdir)
-        self.ckpt = f"{self._tmp.name}/jump.ckpt"
         self.ledger = {"o": 0.0, "cr": 0.0}
         self.counts = {"accepted": 0, "rejected_mass": 0, "rejected_recheck": 0, "plain_steps": 0,
                        "jumped_steps": 0, "scans": 0}
+        self.gates = []   # per trial: (c for O, c for Cr, re-check ratio post / pre or None)
 
     def _due(self, t: int) -> bool:
         """A scan fires before step t + 1."""
@@ -375,13 +381,26 @@ class JumpStepper:
         self.counts["plain_steps"] += m
 
     def _state(self):
+        """(nx, ny, nz, 4) FP64 copy of o, cr, p, gb on the GPU."""
         import torch
-        x = np.stack([self.s.get(f) for f in FIELDS], axis=-1)
-        return torch.from_numpy(x).cuda()
+        return torch.stack([self.s.device_view(f) for f in FIELDS], dim=-1)
+
+    def _write(self, x):
+        import torch
+        for i, f in enumerate(("o", "cr", "p")):
+            self.s.device_view(f, writable=True).copy_(x[..., i])
+        torch.cuda.current_stream().synchronize()
 
     def _change(self, a, b):
         import torch
         return float(torch.linalg.vector_norm(((b - a) / self.norm.csd.double())[..., :3]))
+
+    def _budget_total(self):
+        """Amounts of O and Cr the solver's budget has recorded (inlet,
+        nucleation, Ck and clipping terms)."""
+        b = self.s.budget()
+        species = {"o": "O", "cr": "Cr"}
+        return {f: sum(b[n + sp][0] + b[n + sp][1] for n in ("bc", "nuc", "ck", "clip")) for f, sp in species.items()}
 
     def advance(self, n: int):
         """n simulated steps; returns the counts."""
@@ -393,7 +412,6 @@ class JumpStepper:
             if self.model is None or left < span or free < span:
                 self.plain(left if self.model is None else min(left, free + 1))
                 continue
-            self.s.save(self.ckpt)
             t0, counts0 = self.t, dict(self.counts)
             xa = self._state()
             self.plain(self.probe)
@@ -403,39 +421,42 @@ class JumpStepper:
             pre = self._change(xa, xb) / self.probe
             prop = predict(self.model, self.norm, xb[None].float(), rb[None].float())[0].double()
             prop[..., 3] = xb[..., 3]
-            ok = True
+            cs = []
             for i, f in ((0, "o"), (1, "cr")):
                 d = prop[..., i] - xb[..., i]
                 want = self.k * rate[f]
                 mag = float(d.abs().sum())
-                c = (want - float(d.sum())) / mag if mag > 0 else 0.0
-                if abs(c) > self.mass_tol:
-                    ok = False
-                    break
-                prop[..., i] = xb[..., i] + d + c * d.abs()
-            if not ok:
+                cs.append((want - float(d.sum())) / mag if mag > 0 else 0.0)
+            if max(abs(c) for c in cs) > self.mass_tol:
+                self.gates.append((cs[0], cs[1], None))
                 self.counts["rejected_mass"] += 1
                 self.plain(self.k + self.probe)
                 continue
+            for i, c in enumerate(cs):
+                d = prop[..., i] - xb[..., i]
+                prop[..., i] = xb[..., i] + d + c * d.abs()
             jumped = {f: float((prop[..., i] - xb[..., i]).sum()) for i, f in ((0, "o"), (1, "cr"))}
-            host = prop.cpu().numpy()
-            for i, f in enumerate(("o", "cr", "p")):
-                self.s.set(f, host[..., i])
-            self.s.invalidate_eta_cache()
+            self._write(prop)
+            b0 = self._budget_total()
             self.t += self.k
             self.plain(self.probe)
             post = self._change(prop, self._state()) / self.probe
+            self.gates.append((cs[0], cs[1], post / pre if pre > 0 else float("inf")))
             if post <= self.recheck_factor * pre:
                 self.counts["accepted"] += 1
                 self.counts["jumped_steps"] += self.k
                 for f in ("o", "cr"):
                     self.ledger[f] += jumped[f]
                 continue
-            self.s.load(self.ckpt)
-            self.t, self.counts = t0, counts0
+            b1 = self._budget_total()
+            self._write(xb)
+            for f in ("o", "cr"):
+                self.ledger[f] -= b1[f] - b0[f]
+            self.t, self.counts = t0 + self.probe, counts0
+            self.counts["plain_steps"] += self.probe
             self.counts["rejected_recheck"] += 1
-            self.plain(self.k + 2 * self.probe)
+            self.plain(self.k + self.probe)
         return dict(self.counts)
 
     def close(self):
-        self._tmp.cleanup()
+        pass

@@ -94,3 +94,51 @@ def test_jumps_against_plain_solver(trained):
     st.close()
     jump.close()
     plain.close()
+
+
+@pytest.mark.parametrize("gate", ["mass", "recheck"])
+def test_rejected_jumps_leave_the_plain_run(trained, gate):
+    """Every jump rejected (mass_tol < 0, or recheck_factor 0): the state is
+    the plain run's bit for bit, and the ledger takes back the budget of the
+    rolled-back re-check steps."""
+    net, norm, _, _, cfgs = trained
+    cfg = cfgs[4]
+    jump, plain = nicr.Solver(cfg), nicr.Solver(cfg)
+    jump.run(32)
+    plain.run(32)
+    kw = {"mass_tol": -1.0} if gate == "mass" else {"recheck_factor": 0.0}
+    st = surrogate.JumpStepper(jump, net, norm, KS * EVERY, **kw)
+    counts = st.advance(100)
+    plain.run(100)
+    assert counts["accepted"] == 0 and counts["plain_steps"] == 100
+    assert counts["rejected_mass"] + counts["rejected_recheck"] >= 4 and counts[f"rejected_{gate}"] >= 1
+    for f in ("o", "cr", "p"):
+        assert np.array_equal(jump.get(f).view(np.int64), plain.get(f).view(np.int64)), f
+    a, b = st._budget_total(), surrogate.JumpStepper(plain, None, None, KS * EVERY)._budget_total()
+    for f in ("o", "cr"):
+        assert a[f] + st.ledger[f] == pytest.approx(b[f], rel=1e-12, abs=1e-18)
+    jump.close()
+    plain.close()
+
+
+def test_device_view_round_trip(require_gpu):
+    """Solver.device_view reads the state in place and a write through a
+    writable view is what the next step sees (as nicr_set_field)."""
+    import torch
+    cfg = surrogate.trajectory_configs(1, 24, first_seed=9)[0]
+    a, b = nicr.Solver(cfg), nicr.Solver(cfg)
+    a.run(5)
+    b.run(5)
+    for f in ("o", "cr", "p", "gb"):
+        assert np.array_equal(a.device_view(f).cpu().numpy(), a.get(f))
+    o = a.get("o")
+    o[3:6, 4:9, 2:7] *= 1.01
+    a.device_view("o", writable=True).copy_(torch.from_numpy(o).cuda())
+    torch.cuda.synchronize()
+    b.set("o", o)
+    a.step(7)
+    b.step(7)
+    for f in ("o", "cr", "p"):
+        assert np.array_equal(a.get(f).view(np.int64), b.get(f).view(np.int64)), f
+    a.close()
+    b.close()
