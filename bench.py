@@ -494,6 +494,56 @@ def surrogate_jumps(dev, size=128, every=32, ks=2, steps=1024, iters=1200):
     return out
 
 
+def surrogate_train_workload(args, rank: int, world: int, local: int) -> int:
+    """Data-parallel training of the surrogate (one process per GPU under
+    torchrun, NCCL): every rank generates its own 64^3 trajectories (2 seeds
+    per rank, 256 steps, a sample every 16) and trains the U-Net (base 16,
+    K = 32) on them with batches of 2 per rank, gradients all-reduced every
+    step (weak scaling). --warmup untimed, then --steps timed training steps
+    (CUDA events, max over ranks); value = samples per second of the job."""
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    group = None
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+        group = dist.group.WORLD
+    from nicr import surrogate
+    cfgs = surrogate.trajectory_configs(2, 64, first_seed=100 + 2 * rank)
+    for c in cfgs:
+        c.device = local
+    x, r = surrogate.trajectories(cfgs, 256, 16, device=local)
+    torch.manual_seed(0)
+    net = surrogate.unet(4, 16).cuda()
+    batch = 2
+    surrogate.train(net, x, r, 2, 32, iters=max(3, args.warmup), batch=batch, group=group)
+    if group is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    norm, losses = surrogate.train(net, x, r, 2, 32, iters=args.steps, batch=batch, group=group)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = torch.tensor([e0.elapsed_time(e1)], device="cuda")
+    if group is not None:
+        dist.all_reduce(ms, op=dist.ReduceOp.MAX)
+        dist.barrier()
+    t = float(ms) / 1000.0
+    if rank == 0:
+        print(json.dumps({"workload": "surrogate-train", "metric": "surrogate training samples/s (64^3, U-Net base 16)",
+                          "value": world * batch * args.steps / t, "unit": "samples/s", "n_gpus": world,
+                          "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * t / args.steps,
+                          "scaling": "weak", "dtype": "bf16", "data": "synthetic (solver trajectories)",
+                          "loss_first": losses[0], "loss_last": losses[-1],
+                          "config": {"workload": "surrogate-train", "size": 64, "batch_per_rank": batch, "k": 32,
+                                     "parallelism": f"dp{world}"}}))
+    if group is not None:
+        dist.destroy_process_group()
+    return 0
+
+
 def slabs_workload(args) -> int:
     """The slab form (one domain split along X, nicr_slabs_*) on the bench
     workload: 256^3, 8 evolving eta, reciprocal form, Ksp on, the same initial
@@ -665,14 +715,15 @@ def main():
     ap.add_argument("--ref-budget", type=float, default=60.0, help="seconds of CPU stepping for the reference")
     ap.add_argument("--slab-devices", default="", help="--workload slabs: comma-separated device per slab")
     ap.add_argument("--workload", choices=["step", "output", "sweep", "small", "accuracy", "slabs", "slab-ranks",
-                                           "surrogate"],
+                                           "surrogate", "surrogate-train"],
                     default="step",
                     help="step: the headline line (default); output: VTI frame cost and overlap with stepping; "
                          "sweep: 64 uneven domains advanced as one batch; small: step rate of the small configs; "
                          "accuracy: the fast form against the drop-in form over --steps (5000 by default here); "
                          "slabs: the domain split along X into slabs against one handle; "
                          "slab-ranks: the domain split over the torchrun ranks (one slab per GPU); "
-                         "surrogate: the learned surrogate's convolution kernels and U-Net at 128^3")
+                         "surrogate: the learned surrogate's convolution kernels and U-Net at 128^3; "
+                         "surrogate-train: data-parallel training of the surrogate over the torchrun ranks")
     ap.add_argument("--precision", type=int, default=0, help="arithmetic form of --workload sweep (0 drop-in, 1 fast)")
     ap.add_argument("--no-jumps", action="store_true", help="--workload surrogate: kernels only, no training and jump runs")
     args = ap.parse_args()
@@ -699,6 +750,8 @@ def main():
         return slab_ranks_workload(args, rank, world, local)
     if args.workload == "surrogate":
         return surrogate_workload(args)
+    if args.workload == "surrogate-train":
+        return surrogate_train_workload(args, rank, world, local)
 
     import torch
     import torch.distributed as dist

@@ -214,19 +214,35 @@ def trajectories(cfgs, steps: int, every: int, probe: int = 2, device: int = 0):
     return torch.stack(xs), torch.stack(rs)
 
 
+def _moments(v, group):
+    """(mean, std) per field of v (..., fields) over every rank of group
+    (sums of v and v^2 in FP64 all-reduced; population std)."""
+    import torch
+    f = v.shape[-1]
+    flat = v.reshape(-1, f).double()
+    m = torch.stack([flat.sum(0), (flat * flat).sum(0),
+                     torch.full((f,), float(flat.shape[0]), dtype=torch.float64, device=v.device)])
+    if group is not None:
+        import torch.distributed as dist
+        dist.all_reduce(m, group=group)
+    mean = m[0] / m[2]
+    var = (m[1] / m[2] - mean * mean).clamp_min(0.0)
+    return mean.to(v.dtype), var.sqrt().to(v.dtype)
+
+
 class Normaliser:
     """Per-field scales: of the states (mu, sd), of the per-step rates (rsd),
     of the K-step changes (csd) and of the network's target, the K-step
-    change minus K x the rate (dsd). K counts steps; k counts samples."""
+    change minus K x the rate (dsd). K counts steps; k counts samples. With
+    a process group the moments are those of every rank's samples."""
 
-    def __init__(self, x, r, k: int, steps_k: int):
-        f = x.shape[-1]
-        flat = x.reshape(-1, f)
-        self.mu, self.sd = flat.mean(0), flat.std(0).clamp_min(1e-12)
-        self.rsd = r.reshape(-1, f).std(0).clamp_min(1e-30)
+    def __init__(self, x, r, k: int, steps_k: int, group=None):
         d = x[:, k:] - x[:, :-k]
-        self.csd = d.reshape(-1, f).std(0).clamp_min(1e-30)
-        self.dsd = (d - steps_k * r[:, :-k]).reshape(-1, f).std(0).clamp_min(1e-30)
+        self.mu, sd = _moments(x, group)
+        self.sd = sd.clamp_min(1e-12)
+        self.rsd = _moments(r, group)[1].clamp_min(1e-30)
+        self.csd = _moments(d, group)[1].clamp_min(1e-30)
+        self.dsd = _moments(d - steps_k * r[:, :-k], group)[1].clamp_min(1e-30)
         self.steps_k = steps_k
 
     def inputs(self, x, r):
@@ -245,16 +261,44 @@ def _pairs(x, r, k):
     return x[:, :-k].reshape((-1,) + f), r[:, :-k].reshape((-1,) + f), x[:, k:].reshape((-1,) + f)
 
 
-def train(model, x, r, k: int, steps_k: int, iters: int = 200, batch: int = 2, lr: float = 2e-3, seed: int = 0):
+def allreduce_gradients(model, group):
+    """Averages the gradients over the ranks of group: one flat bucket, one
+    all-reduce (NCCL on GPUs, gloo on the CPU)."""
+    import torch
+    import torch.distributed as dist
+    grads = [p.grad for p in model.parameters() if p.grad is not None]
+    flat = torch.cat([g.reshape(-1) for g in grads])
+    dist.all_reduce(flat, group=group)
+    flat /= dist.get_world_size(group)
+    o = 0
+    for g in grads:
+        g.copy_(flat[o:o + g.numel()].view_as(g))
+        o += g.numel()
+
+
+def train(model, x, r, k: int, steps_k: int, iters: int = 200, batch: int = 2, lr: float = 2e-3, seed: int = 0,
+          group=None):
     """Adam (cosine-decayed rate) on the MSE of the normalised target over
-    sample pairs k apart (steps_k steps); returns (normaliser, losses)."""
+    sample pairs k apart (steps_k steps); returns (normaliser, losses).
+
+    Data parallel with a process group: each rank passes its own
+    trajectories (its share of the seeds), draws its own batches, and the
+    gradients are averaged over the ranks before every optimiser step
+    (allreduce_gradients), after rank 0's initial weights were broadcast; all
+    ranks then hold the same weights. The losses are each rank's own."""
     import torch
     torch.manual_seed(seed)
-    norm = Normaliser(x, r, k, steps_k)
+    rank = 0
+    if group is not None:
+        import torch.distributed as dist
+        rank = dist.get_rank(group)
+        for p in model.parameters():
+            dist.broadcast(p.data, src=dist.get_global_rank(group, 0), group=group)
+    norm = Normaliser(x, r, k, steps_k, group)
     x0, r0, x1 = _pairs(x, r, k)
     opt = torch.optim.Adam(model.parameters(), lr=lr)
     sched = torch.optim.lr_scheduler.CosineAnnealingLR(opt, iters)
-    g = torch.Generator(device="cpu").manual_seed(seed)
+    g = torch.Generator(device="cpu").manual_seed(seed + 1000003 * rank)
     losses = []
     for _ in range(iters):
         idx = torch.randint(0, x0.shape[0], (batch,), generator=g)
@@ -262,6 +306,8 @@ def train(model, x, r, k: int, steps_k: int, iters: int = 200, batch: int = 2, l
         loss = torch.mean((model(norm.inputs(a, ra)) - norm.target(a, ra, b)) ** 2)
         opt.zero_grad()
         loss.backward()
+        if group is not None:
+            allreduce_gradients(model, group)
         opt.step()
         sched.step()
         losses.append(loss.item())

@@ -142,3 +142,44 @@ def test_device_view_round_trip(require_gpu):
         assert np.array_equal(a.get(f).view(np.int64), b.get(f).view(np.int64)), f
     a.close()
     b.close()
+
+
+def _nccl_train(port, q):
+    import os
+    import sys
+    import torch
+    import torch.distributed as dist
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path.insert(0, os.path.join(root, "ni-cr_oxidation_phase-field_simulation_b200"))
+    from nicr import surrogate
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    torch.cuda.set_device(0)
+    dist.init_process_group("nccl", rank=0, world_size=1, device_id=torch.device("cuda", 0))
+    try:
+        x, r = surrogate.trajectories(surrogate.trajectory_configs(2, 16, first_seed=100), 64, 8)
+        torch.manual_seed(0)
+        net = surrogate.unet(4, 16).cuda()
+        norm, losses = surrogate.train(net, x, r, 2, 16, iters=20, batch=2, group=dist.group.WORLD)
+        ok = all(torch.isfinite(p).all() for p in net.parameters())
+        q.put((ok, losses[0], losses[-1], surrogate.conv_error()))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_data_parallel_training_over_nccl_single_rank(require_gpu):
+    """train() with an NCCL group (a world of one rank on this GPU): the
+    broadcast, the moment and gradient all-reduces on the library's kernels'
+    stream order; the multi-rank host logic is tested over gloo on the CPU."""
+    import socket
+    import torch.multiprocessing as mp
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    p = ctx.Process(target=_nccl_train, args=(port, q))
+    p.start()
+    ok, first, last, err = q.get(timeout=300)
+    p.join(timeout=120)
+    assert p.exitcode == 0 and ok and err == 0 and last < first
