@@ -350,9 +350,15 @@ __device__ __forceinline__ void tma_3d(uint32_t dst, const CUtensorMap* map, int
         : "memory");
 }
 
+// Epilogue options of the TMA forward (act): bias added per output channel
+// when `bias` is given, then ACT_RELU, and the result stored as BF16 with
+// ACT_BF16 (else FP32).
+constexpr int ACT_RELU = 1, ACT_BF16 = 2;
+
 __global__ void __launch_bounds__(128) k_conv3d_fwd_tma(const __grid_constant__ CUtensorMap xmap,
-                                                         const __grid_constant__ CUtensorMap wmap, float* __restrict__ y,
-                                                         const Vol V, int cin, int cout, const TmaConv C) {
+                                                         const __grid_constant__ CUtensorMap wmap, void* __restrict__ y,
+                                                         const float* __restrict__ bias, int act, const Vol V, int cin,
+                                                         int cout, const TmaConv C) {
     extern __shared__ unsigned char tma_smem_raw[];
     const uint32_t raw = smem_u32(tma_smem_raw);
     const uint32_t base = (raw + 1023u) & ~1023u;   // swizzled stages start on 1024-byte boundaries
@@ -450,7 +456,7 @@ __global__ void __launch_bounds__(128) k_conv3d_fwd_tma(const __grid_constant__ 
         const int r = warp * 32 + lane;
         const int yy = y0 + r / C.wt, xx = x0 + r % C.wt;
         const bool store = yy < V.h && xx < V.w;
-        float* out = y + ((((long long)b * V.d + z) * V.h + yy) * V.w + xx) * cout + n0;
+        const long long o0 = ((((long long)b * V.d + z) * V.h + yy) * V.w + xx) * cout + n0;
         for (int c = 0; c < N; c += 16) {
             uint32_t q[16];
             const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c;
@@ -460,11 +466,35 @@ __global__ void __launch_bounds__(128) k_conv3d_fwd_tma(const __grid_constant__ 
                   "=r"(q[8]), "=r"(q[9]), "=r"(q[10]), "=r"(q[11]), "=r"(q[12]), "=r"(q[13]), "=r"(q[14]), "=r"(q[15])
                 : "r"(taddr));
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-            if (store)
+            float v[16];
+#pragma unroll
+            for (int j = 0; j < 16; j += 4) {
+                const float4 bj = bias ? *reinterpret_cast<const float4*>(bias + n0 + c + j) : make_float4(0.f, 0.f, 0.f, 0.f);
+                v[j] = __uint_as_float(q[j]) + bj.x;
+                v[j + 1] = __uint_as_float(q[j + 1]) + bj.y;
+                v[j + 2] = __uint_as_float(q[j + 2]) + bj.z;
+                v[j + 3] = __uint_as_float(q[j + 3]) + bj.w;
+            }
+            if (act & ACT_RELU) {
+#pragma unroll
+                for (int j = 0; j < 16; ++j) v[j] = fmaxf(v[j], 0.f);
+            }
+            if (!store) continue;
+            if (act & ACT_BF16) {
+                uint32_t h[8];
+#pragma unroll
+                for (int j = 0; j < 8; ++j)
+                    h[j] = (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(v[2 * j])) |
+                           ((uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(v[2 * j + 1])) << 16);
+                uint4* out = reinterpret_cast<uint4*>(static_cast<__nv_bfloat16*>(y) + o0 + c);
+                out[0] = make_uint4(h[0], h[1], h[2], h[3]);
+                out[1] = make_uint4(h[4], h[5], h[6], h[7]);
+            } else {
+                float* out = static_cast<float*>(y) + o0 + c;
+#pragma unroll
                 for (int j = 0; j < 16; j += 4)
-                    *reinterpret_cast<float4*>(out + c + j) =
-                        make_float4(__uint_as_float(q[j]), __uint_as_float(q[j + 1]), __uint_as_float(q[j + 2]),
-                                    __uint_as_float(q[j + 3]));
+                    *reinterpret_cast<float4*>(out + j) = make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]);
+            }
         }
     } else if (t == 0) {
         atomicExch(&g_conv_error, 1);
@@ -745,9 +775,15 @@ extern "C" {
 
 int nicr_conv3d_fwd_tma(const void* x, const void* w, float* y, int n, int d, int h, int w_, int cin, int cout,
                         void* stream) {
+    return nicr_conv3d_fwd_act(x, w, nullptr, 0, y, n, d, h, w_, cin, cout, stream);
+}
+
+int nicr_conv3d_fwd_act(const void* x, const void* w, const float* bias, int act, void* y, int n, int d, int h, int w_,
+                        int cin, int cout, void* stream) {
     const Vol V{n, d, h, w_};
     const int rc = check_args(V.voxels(), cin, cout);
-    if (rc != NICR_OK || !x || !w || !y) return rc != NICR_OK ? rc : NICR_ERR_INVALID_ARG;
+    if (rc != NICR_OK || !x || !w || !y || (act & ~(ACT_RELU | ACT_BF16)) != 0)
+        return rc != NICR_OK ? rc : NICR_ERR_INVALID_ARG;
     const auto enc = conv_map_encoder();
     if (!enc) return NICR_ERR_CUDA;
     const TmaConv C = tma_conv_plan(V, cin, cout);
@@ -778,7 +814,8 @@ int nicr_conv3d_fwd_tma(const void* x, const void* w, float* y, int n, int d, in
         return NICR_ERR_CUDA;
     const long long tiles = (long long)C.tiles_x * C.tiles_y * d * n;
     const dim3 grid((unsigned)tiles, (unsigned)((cout + 255) / 256));
-    k_conv3d_fwd_tma<<<grid, 128, C.smem, static_cast<cudaStream_t>(stream)>>>(xmap, wmap, y, V, cin, cout, C);
+    k_conv3d_fwd_tma<<<grid, 128, C.smem, static_cast<cudaStream_t>(stream)>>>(xmap, wmap, y, bias, act, V, cin,
+                                                                                   cout, C);
     return cudaGetLastError() == cudaSuccess ? NICR_OK : NICR_ERR_CUDA;
 }
 

@@ -29,6 +29,7 @@ def _lib():
         for f in ("nicr_conv3d_fwd", "nicr_conv3d_fwd_tma", "nicr_conv3d_fwd_gather", "nicr_conv3d_fwd_mma_sync",
                   "nicr_conv3d_wgrad", "nicr_conv3d_wgrad_tma", "nicr_conv3d_wgrad_mma_sync"):
             getattr(L, f).argtypes = [vp, vp, vp, i, i, i, i, i, i, vp]
+        L.nicr_conv3d_fwd_act.argtypes = [vp, vp, vp, i, vp, i, i, i, i, i, i, vp]
         L.nicr_conv3d_error.argtypes = [ctypes.POINTER(ctypes.c_int)]
         L._conv_bound = True
     return L
@@ -51,6 +52,22 @@ def conv3d_raw(x, w_bf16, form: str = "tcgen05"):
          "mma_sync": "nicr_conv3d_fwd_mma_sync"}[form]
     _check(getattr(_lib(), f)(x.data_ptr(), w_bf16.data_ptr(), y.data_ptr(), n, d, h, wd, cin, cout,
                               torch.cuda.current_stream(x.device).cuda_stream), f)
+    return y
+
+
+def conv3d_act_raw(x, w_bf16, bias, relu: bool, out_bf16: bool):
+    """act(conv(x, w) + bias) in the TMA forward's epilogue (nicr_conv3d_fwd_act):
+    BF16 when out_bf16 else FP32; None where the TMA form is unavailable."""
+    import torch
+    n, d, h, wd, cin = x.shape
+    cout = w_bf16.shape[0]
+    y = torch.empty((n, d, h, wd, cout), dtype=torch.bfloat16 if out_bf16 else torch.float32, device=x.device)
+    rc = _lib().nicr_conv3d_fwd_act(x.data_ptr(), w_bf16.data_ptr(), bias.data_ptr() if bias is not None else None,
+                                    (1 if relu else 0) | (2 if out_bf16 else 0), y.data_ptr(), n, d, h, wd, cin, cout,
+                                    torch.cuda.current_stream(x.device).cuda_stream)
+    if rc == 1:   # NICR_ERR_INVALID_ARG: shapes valid (checked by the caller's layer sizes) but no tensor map
+        return None
+    _check(rc, "nicr_conv3d_fwd_act")
     return y
 
 
@@ -100,17 +117,60 @@ def _make_fn():
             gw = conv3d_wgrad_raw(xb, gyb)
             return gx, gw
 
-    return Conv3dFn
+    class ConvActFn(torch.autograd.Function):
+        """act(conv(x, w) + b) with the bias, the ReLU and the BF16 store in
+        the convolution's epilogue; the backward masks the gradient with the
+        stored activation (y > 0), sums it for the bias and runs the data and
+        weight gradients on the library's kernels."""
+
+        @staticmethod
+        def forward(ctx, x, w, b, relu, out_bf16):
+            xb = x.contiguous()
+            wb = w.to(torch.bfloat16).contiguous()
+            bf = b.float().contiguous()
+            y = conv3d_act_raw(xb, wb, bf, relu, out_bf16)
+            if y is None:
+                y = conv3d_raw(xb, wb) + bf
+                y = torch.relu(y) if relu else y
+                y = y.to(torch.bfloat16) if out_bf16 else y
+            ctx.relu = relu
+            ctx.save_for_backward(xb, wb, y if relu else None)
+            return y
+
+        @staticmethod
+        def backward(ctx, gy):
+            xb, wb, y = ctx.saved_tensors
+            g = gy.float()
+            if ctx.relu:
+                g = g * (y > 0)
+            gb = g.sum(dim=tuple(range(g.dim() - 1)))
+            gyb = g.to(torch.bfloat16).contiguous()
+            wt = wb.flip(1).permute(2, 1, 0).contiguous()
+            gx = conv3d_raw(gyb, wt).to(xb.dtype)
+            gw = conv3d_wgrad_raw(xb, gyb)
+            return gx, gw, gb, None, None
+
+    return Conv3dFn, ConvActFn
 
 
 _FN = None
 
 
-def conv3d(x, w):
+def _fns():
     global _FN
     if _FN is None:
         _FN = _make_fn()
-    return _FN.apply(x, w)
+    return _FN
+
+
+def conv3d(x, w):
+    return _fns()[0].apply(x, w)
+
+
+def conv3d_act(x, w, b, relu: bool = True, out_bf16: bool = True):
+    """act(conv(x, w) + b): x BF16 NDHWC, w FP32 [Cout][27][Cin], b FP32
+    [Cout]; BF16 result when out_bf16, else FP32."""
+    return _fns()[1].apply(x, w, b, relu, out_bf16)
 
 
 def _module_classes():
@@ -125,8 +185,8 @@ def _module_classes():
             self.relu = relu
 
         def forward(self, x):
-            y = conv3d(x, self.w) + self.b
-            return (torch.relu(y) if self.relu else y).to(torch.bfloat16)
+            # hidden layers: ReLU, BF16 activations; the head: FP32 output
+            return conv3d_act(x, self.w, self.b, self.relu, out_bf16=self.relu)
 
     def pool(x):   # 2x2x2 average, NDHWC
         n, d, h, w, c = x.shape

@@ -86,6 +86,36 @@ def test_autograd_wrapper(require_gpu):
     assert rel < 8e-3
 
 
+@pytest.mark.parametrize("relu,out_bf16", [(True, True), (False, False), (True, False)])
+def test_fused_bias_activation(require_gpu, relu, out_bf16):
+    """conv3d_act: y = act(conv(x, w) + b) from the epilogue, and its
+    gradients (ReLU mask from the stored activation, bias = sum of dy)
+    against torch's FP64 autograd on the CPU."""
+    x, wt, dy = inputs((1, 8, 8, 8, 32, 48), 5)
+    b = conv_ref.bf16_rounded((48,), torch.Generator().manual_seed(6), 0.3)
+    xd, wd, bd = x.double().requires_grad_(True), wt.double().requires_grad_(True), b.double().requires_grad_(True)
+    yd = conv_ref.conv3d(xd, wd) + bd
+    yd = torch.relu(yd) if relu else yd
+    (yd * dy.double()).sum().backward()
+    xg = x.cuda().bfloat16().requires_grad_(True)
+    wg = wt.cuda().requires_grad_(True)
+    bg = b.cuda().requires_grad_(True)
+    y = surrogate.conv3d_act(xg, wg, bg, relu, out_bf16)
+    assert y.dtype == (torch.bfloat16 if out_bf16 else torch.float32)
+    bound = conv_ref.conv3d(x.abs(), wt.abs()) + b.abs().double()
+    err = (y.double().cpu() - yd.detach()).abs()
+    # FP32 accumulation, then (BF16 output) one rounding to 8 significant bits
+    tol = 1e-4 * bound + (yd.detach().abs() * 2.0 ** -8 * 1.01 if out_bf16 else 0.0)
+    assert bool((err <= tol).all())
+    (y.float() * dy.cuda()).sum().backward()
+    assert surrogate.conv_error() == 0
+    for got, ref, name in ((wg.grad, wd.grad, "w"), (bg.grad, bd.grad, "b")):
+        rel = float((got.double().cpu() - ref).abs().max() / ref.abs().max())
+        assert rel < 2e-2, name   # the masked gradient is rounded to BF16 before the kernels
+    rel = float((xg.grad.double().cpu() - xd.grad).abs().max() / xd.grad.abs().max())
+    assert rel < 2e-2
+
+
 def test_rejects_misaligned_shapes(require_gpu):
     x = torch.zeros((1, 3, 3, 3, 16), dtype=torch.bfloat16, device="cuda")
     w = torch.zeros((16, 27, 16), dtype=torch.bfloat16, device="cuda")
