@@ -439,11 +439,16 @@ int nicr_conv3d_fwd(const void* x, const void* w, float* y, int n, int d, int h,
                     void* stream);
 int nicr_conv3d_fwd_tma(const void* x, const void* w, float* y, int n, int d, int h, int w_, int cin, int cout,
                         void* stream);
-/* The TMA forward with its epilogue fused: y = act(conv(x, w) + bias), bias
- * FP32 [cout] or NULL, act bit 1 = ReLU, bit 2 = store BF16 (else FP32).
- * NICR_ERR_INVALID_ARG where nicr_conv3d_fwd_tma would return it. */
+/* The tcgen05 forward with its epilogue fused: y = act(conv(x, w) + bias),
+ * bias FP32 [cout] or NULL, act bit 1 = ReLU, bit 2 = store BF16 (else
+ * FP32). NICR_ERR_INVALID_ARG where nicr_conv3d_fwd_tma would return it. */
 int nicr_conv3d_fwd_act(const void* x, const void* w, const float* bias, int act, void* y, int n, int d, int h, int w_,
                         int cin, int cout, void* stream);
+/* The same from a staged halo block (Cout <= 64 and rows of at least 128
+ * voxels, else NICR_ERR_INVALID_ARG); nicr_conv3d_fwd_act and
+ * nicr_conv3d_fwd use it for Cout <= 32, where it is the faster form. */
+int nicr_conv3d_fwd_halo(const void* x, const void* w, const float* bias, int act, void* y, int n, int d, int h, int w_,
+                         int cin, int cout, void* stream);
 int nicr_conv3d_fwd_gather(const void* x, const void* w, float* y, int n, int d, int h, int w_, int cin, int cout,
                            void* stream);
 int nicr_conv3d_fwd_mma_sync(const void* x, const void* w, float* y, int n, int d, int h, int w_, int cin, int cout,

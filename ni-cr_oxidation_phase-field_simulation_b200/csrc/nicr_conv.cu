@@ -550,6 +550,192 @@ TmaConv tma_conv_plan(const Vol& V, int cin, int cout) {
     return C;
 }
 
+// ---------------------------------------------------------------- forward from a halo block
+// For narrow outputs (Cout <= 64) on rows of at least 128 voxels: the
+// output tile is 128 consecutive voxels of one x row (b, z, y, x0..x0+127).
+// Per chunk of 16 input channels, two TMA boxes {8, 130, 3, 3, 1} of x at
+// (c0 + 8 kc, x0 - 1, y - 1, z - 1, b) bring the whole 3 x 3 x 130 halo block
+// into shared memory in the no-swizzle K-major layout, one plane per 8
+// channels: row (line, xr) at byte (line * 130 + xr) * 16, line = (dz+1)*3 +
+// (dy+1). The A operand of tap (dz, dy, dx) is then the 128 rows starting at
+// line * 130 + dx + 1: a descriptor whose start address moves by 16 bytes per
+// row (SBO 128 B between 8-row groups, LBO = one plane between the two K
+// halves), so x is staged once per chunk instead of once per tap. The
+// chunk's weights for all 27 taps are copied by all threads into
+// [tap][kc][co][16 B] (LBO = Cout * 16 B). Zero fill outside the grid is the
+// padding. Stages: one per chunk in flight (two when Cin > 16).
+constexpr int HB_ROWS = 130, HB_LINES = 9;
+
+struct HaloConv {
+    int chunks, stages, cols, tiles_x;
+    uint32_t a_box, a_plane, a_bytes, b_bytes, stage_bytes;   // a_plane: a_box rounded up to 128 bytes
+    size_t smem;
+};
+
+__global__ void __launch_bounds__(128) k_conv3d_fwd_halo(const __grid_constant__ CUtensorMap xmap,
+                                                          const __nv_bfloat16* __restrict__ wt, void* __restrict__ y,
+                                                          const float* __restrict__ bias, int act, const Vol V, int cin,
+                                                          int cout, const HaloConv H) {
+    extern __shared__ unsigned char hb_smem_raw[];
+    const uint32_t raw = smem_u32(hb_smem_raw);
+    const uint32_t base = (raw + 1023u) & ~1023u;
+    unsigned char* gen = hb_smem_raw + (base - raw);
+    const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+    const int S = H.stages;
+    uint64_t* full = reinterpret_cast<uint64_t*>(gen + S * H.stage_bytes);
+    uint64_t* empty = full + S;
+    uint64_t* acc_full = empty + S;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acc_full + 1);
+
+    long long tile = blockIdx.x;
+    const int tx = (int)(tile % H.tiles_x);
+    tile /= H.tiles_x;
+    const int yv = (int)(tile % V.h);
+    tile /= V.h;
+    const int z = (int)(tile % V.d), b = (int)(tile / V.d);
+    const int x0 = tx * TC_M;
+    const int N = cout;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(H.cols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (t == 0) {
+        for (int s = 0; s < 2 * S + 1; ++s) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(full + s)));
+        asm volatile("fence.mbarrier_init.release.cluster;");
+        asm volatile("prefetch.tensormap [%0];" ::"l"(&xmap) : "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+    const uint32_t idesc = umma_idesc(TC_M, N);
+
+    bool ok = true;
+    int committed = 0;
+    for (int c = 0; c < H.chunks; ++c) {
+        const int s = c % S;
+        const uint32_t st = base + s * H.stage_bytes;
+        // the stage last held chunk c - S: its MMAs must have finished
+        if (c >= S) ok = mbar_wait(smem_u32(empty + s), (uint32_t)((c / S - 1) & 1));
+        if (__syncthreads_or(!ok)) break;
+        if (t == 0) {
+            mbar_expect(smem_u32(full + s), 2 * H.a_box);
+            for (int kc = 0; kc < 2; ++kc)
+                tma_5d(st + kc * H.a_plane, &xmap, c * 16 + kc * 8, x0 - 1, yv - 1, z - 1, b, smem_u32(full + s));
+        }
+        // weights of the chunk: [tap][kc][co][8 channels]
+        for (int q = t; q < 27 * 2 * N; q += 128) {
+            const int co = q % N, kc = (q / N) % 2, tap = q / (2 * N);
+            cp_async16(st + H.a_bytes + (uint32_t)q * 16, wt + ((long long)co * 27 + tap) * cin + c * 16 + kc * 8, true);
+        }
+        asm volatile("cp.async.commit_group;");
+        asm volatile("cp.async.wait_group 0;");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (t == 0) {
+            ok = mbar_wait(smem_u32(full + s), (uint32_t)((c / S) & 1));
+            if (ok) {
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                for (int tap = 0; tap < 27; ++tap) {
+                    const uint32_t row = (uint32_t)((tap / 3) * HB_ROWS + tap % 3);
+                    const uint64_t ad = umma_sdesc(st + row * 16, H.a_plane, 128);
+                    const uint64_t bd = umma_sdesc(st + H.a_bytes + (uint32_t)(tap * 2 * N) * 16, (uint32_t)N * 16, 128);
+                    const uint32_t accum = (c > 0 || tap > 0) ? 1u : 0u;
+                    asm volatile(
+                        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                        " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
+                        "l"(ad), "l"(bd), "r"(idesc), "r"(accum));
+                }
+                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                    smem_u32(empty + s)));
+            }
+        }
+        if (__syncthreads_or(!ok)) break;
+        committed = c + 1;
+    }
+    if (t == 0) asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                     smem_u32(acc_full)));
+    if (committed > 0 || !ok) {
+        const bool done = mbar_wait(smem_u32(acc_full), 0);
+        ok = ok && done;
+    }
+    ok = !__syncthreads_or(!ok);
+    if (ok) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const int r = warp * 32 + lane;
+        const int xx = x0 + r;
+        const bool store = xx < V.w;
+        const long long o0 = ((((long long)b * V.d + z) * V.h + yv) * V.w + xx) * cout;
+        for (int c = 0; c < N; c += 16) {
+            uint32_t q[16];
+            const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c;
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+                : "=r"(q[0]), "=r"(q[1]), "=r"(q[2]), "=r"(q[3]), "=r"(q[4]), "=r"(q[5]), "=r"(q[6]), "=r"(q[7]),
+                  "=r"(q[8]), "=r"(q[9]), "=r"(q[10]), "=r"(q[11]), "=r"(q[12]), "=r"(q[13]), "=r"(q[14]), "=r"(q[15])
+                : "r"(taddr));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            float v[16];
+#pragma unroll
+            for (int j = 0; j < 16; j += 4) {
+                const float4 bj = bias ? *reinterpret_cast<const float4*>(bias + c + j) : make_float4(0.f, 0.f, 0.f, 0.f);
+                v[j] = __uint_as_float(q[j]) + bj.x;
+                v[j + 1] = __uint_as_float(q[j + 1]) + bj.y;
+                v[j + 2] = __uint_as_float(q[j + 2]) + bj.z;
+                v[j + 3] = __uint_as_float(q[j + 3]) + bj.w;
+            }
+            if (act & ACT_RELU) {
+#pragma unroll
+                for (int j = 0; j < 16; ++j) v[j] = fmaxf(v[j], 0.f);
+            }
+            if (!store) continue;
+            if (act & ACT_BF16) {
+                uint32_t hh[8];
+#pragma unroll
+                for (int j = 0; j < 8; ++j)
+                    hh[j] = (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(v[2 * j])) |
+                            ((uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(v[2 * j + 1])) << 16);
+                uint4* out = reinterpret_cast<uint4*>(static_cast<__nv_bfloat16*>(y) + o0 + c);
+                out[0] = make_uint4(hh[0], hh[1], hh[2], hh[3]);
+                out[1] = make_uint4(hh[4], hh[5], hh[6], hh[7]);
+            } else {
+                float* out = static_cast<float*>(y) + o0 + c;
+#pragma unroll
+                for (int j = 0; j < 16; j += 4)
+                    *reinterpret_cast<float4*>(out + j) = make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]);
+            }
+        }
+    } else if (t == 0) {
+        atomicExch(&g_conv_error, 1);
+        // a chunk's loads may still be in flight: wait (bounded) for the last issued one
+        if (committed < H.chunks) mbar_wait(smem_u32(full + committed % S), (uint32_t)((committed / S) & 1));
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(H.cols));
+}
+
+// The halo-block plan, or false outside its shapes (Cout <= 64, W >= 128).
+bool halo_plan(const Vol& V, int cin, int cout, HaloConv& H) {
+    if (cout > 64 || V.w < TC_M || cin % 16 != 0) return false;
+    H = HaloConv{};
+    H.chunks = cin / 16;
+    H.stages = H.chunks > 1 ? 2 : 1;
+    H.cols = 32;
+    while (H.cols < cout) H.cols <<= 1;
+    H.tiles_x = (V.w + TC_M - 1) / TC_M;
+    H.a_box = (uint32_t)HB_LINES * HB_ROWS * 16;
+    H.a_plane = (H.a_box + 127u) & ~127u;
+    H.a_bytes = 2 * H.a_plane;
+    H.b_bytes = (uint32_t)27 * 2 * cout * 16;
+    H.stage_bytes = (H.a_bytes + H.b_bytes + 1023u) & ~1023u;
+    H.smem = (size_t)H.stages * H.stage_bytes + (2 * H.stages + 1) * 8 + 8 + 1024;
+    if (H.smem < (size_t)H.cols * 400) H.smem = (size_t)H.cols * 400;
+    return true;
+}
+
 // ---------------------------------------------------------------- weight gradient, tcgen05 + TMA
 // dw[co][tap][ci] = sum_u dy[u - off(tap)][co] * x[u][ci] (u runs over the
 // voxels of x; dy is zero outside the grid): one GEMM with M = (tap, co)
@@ -763,6 +949,9 @@ bool tma_wgrad_plan(const Vol& V, int cin, int cout, TmaWgrad& G) {
     return true;
 }
 
+int launch_fwd_tma(const void* x, const void* w, const float* bias, int act, void* y, int n, int d, int h, int w_,
+                   int cin, int cout, void* stream);
+
 int check_args(long long voxels, int cin, int cout) {
     if (voxels <= 0 || voxels % 64 != 0 || cin <= 0 || cin % 16 != 0 || cout <= 0 || cout % 16 != 0)
         return NICR_ERR_INVALID_ARG;
@@ -775,11 +964,54 @@ extern "C" {
 
 int nicr_conv3d_fwd_tma(const void* x, const void* w, float* y, int n, int d, int h, int w_, int cin, int cout,
                         void* stream) {
-    return nicr_conv3d_fwd_act(x, w, nullptr, 0, y, n, d, h, w_, cin, cout, stream);
+    return launch_fwd_tma(x, w, nullptr, 0, y, n, d, h, w_, cin, cout, stream);
 }
 
 int nicr_conv3d_fwd_act(const void* x, const void* w, const float* bias, int act, void* y, int n, int d, int h, int w_,
                         int cin, int cout, void* stream) {
+    // the halo block wins for narrow outputs (16->16 at 128^3: 143 against 90
+    // TFLOP/s) and loses from Cout 64 on (64->64 at 128^3: 214 against 677)
+    HaloConv H;
+    if (cout <= 32 && halo_plan(Vol{n, d, h, w_}, cin, cout, H)) {
+        const int rc = nicr_conv3d_fwd_halo(x, w, bias, act, y, n, d, h, w_, cin, cout, stream);
+        if (rc != NICR_ERR_INVALID_ARG) return rc;
+    }
+    return launch_fwd_tma(x, w, bias, act, y, n, d, h, w_, cin, cout, stream);
+}
+
+int nicr_conv3d_fwd_halo(const void* x, const void* w, const float* bias, int act, void* y, int n, int d, int h, int w_,
+                         int cin, int cout, void* stream) {
+    const Vol V{n, d, h, w_};
+    const int rc = check_args(V.voxels(), cin, cout);
+    HaloConv H;
+    if (rc != NICR_OK || !x || !w || !y || (act & ~(ACT_RELU | ACT_BF16)) != 0 || !halo_plan(V, cin, cout, H))
+        return rc != NICR_OK ? rc : NICR_ERR_INVALID_ARG;
+    const auto enc = conv_map_encoder();
+    if (!enc) return NICR_ERR_CUDA;
+    CUtensorMap xmap;
+    const cuuint64_t dims[5] = {(cuuint64_t)cin, (cuuint64_t)w_, (cuuint64_t)h, (cuuint64_t)d, (cuuint64_t)n};
+    const cuuint64_t str[4] = {(cuuint64_t)cin * 2, (cuuint64_t)w_ * cin * 2, (cuuint64_t)h * w_ * cin * 2,
+                               (cuuint64_t)d * h * w_ * cin * 2};
+    const cuuint32_t box[5] = {8, HB_ROWS, 3, 3, 1};
+    const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
+    if (enc(&xmap, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<void*>(x), dims, str, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return NICR_ERR_INVALID_ARG;
+    if (cudaFuncSetAttribute(k_conv3d_fwd_halo, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)H.smem) != cudaSuccess)
+        return NICR_ERR_CUDA;
+    const long long tiles = (long long)H.tiles_x * h * d * n;
+    k_conv3d_fwd_halo<<<(unsigned)tiles, 128, H.smem, static_cast<cudaStream_t>(stream)>>>(
+        xmap, static_cast<const __nv_bfloat16*>(w), y, bias, act, V, cin, cout, H);
+    return cudaGetLastError() == cudaSuccess ? NICR_OK : NICR_ERR_CUDA;
+}
+
+}  // extern "C"
+
+namespace {
+
+int launch_fwd_tma(const void* x, const void* w, const float* bias, int act, void* y, int n, int d, int h, int w_,
+                   int cin, int cout, void* stream) {
     const Vol V{n, d, h, w_};
     const int rc = check_args(V.voxels(), cin, cout);
     if (rc != NICR_OK || !x || !w || !y || (act & ~(ACT_RELU | ACT_BF16)) != 0)
@@ -819,9 +1051,13 @@ int nicr_conv3d_fwd_act(const void* x, const void* w, const float* bias, int act
     return cudaGetLastError() == cudaSuccess ? NICR_OK : NICR_ERR_CUDA;
 }
 
+}  // namespace
+
+extern "C" {
+
 int nicr_conv3d_fwd(const void* x, const void* w, float* y, int n, int d, int h, int w_, int cin, int cout,
                     void* stream) {
-    const int rc = nicr_conv3d_fwd_tma(x, w, y, n, d, h, w_, cin, cout, stream);
+    const int rc = nicr_conv3d_fwd_act(x, w, nullptr, 0, y, n, d, h, w_, cin, cout, stream);
     if (rc != NICR_ERR_INVALID_ARG || check_args((long long)n * d * h * w_, cin, cout) != NICR_OK || !x || !w || !y)
         return rc;
     // a tensor map the driver refused: the gathering form

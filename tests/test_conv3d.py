@@ -50,3 +50,7 @@ def test_conv_abi_rejects_shapes():
         for f in ("nicr_conv3d_wgrad", "nicr_conv3d_wgrad_tma", "nicr_conv3d_wgrad_mma_sync"):
             assert getattr(L, f)(1, 1, 1, n, d, h, w, ci, co, None) == err
     assert L.nicr_conv3d_fwd(None, 1, 1, 1, 4, 4, 4, 16, 16, None) == err
+    # the halo-block form: Cout <= 64 and rows of at least 128 voxels
+    assert L.nicr_conv3d_fwd_halo(1, 1, None, 0, 1, 1, 4, 4, 64, 16, 16, None) == err
+    assert L.nicr_conv3d_fwd_halo(1, 1, None, 0, 1, 1, 1, 1, 128, 16, 128, None) == err
+    assert L.nicr_conv3d_fwd_act(1, 1, None, 4, 1, 1, 1, 1, 128, 16, 16, None) == err   # unknown act bit

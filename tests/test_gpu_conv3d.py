@@ -13,9 +13,12 @@ pytestmark = pytest.mark.gpu
 
 # (n, d, h, w, cin, cout): chunks of 64/48/32/16 channels, a partial
 # 128-voxel tile (64 voxels), two output-channel tiles (cout 272 = 256 + 16)
+# and rows of 128 voxels or more (the halo-block form: one x tile, a partial
+# second x tile, 1 to 4 chunks of 16 input channels)
 SHAPES = [(2, 4, 8, 8, 16, 48), (1, 8, 8, 8, 32, 64), (1, 6, 4, 16, 48, 16), (2, 16, 16, 16, 16, 32),
           (1, 8, 8, 8, 96, 128), (1, 4, 4, 4, 16, 16), (1, 4, 8, 8, 32, 272), (1, 4, 4, 8, 80, 32),
-          (1, 8, 8, 8, 64, 256)]
+          (1, 8, 8, 8, 64, 256), (1, 3, 4, 128, 16, 16), (1, 2, 3, 160, 48, 32), (1, 2, 4, 136, 64, 48)]
+HALO = lambda shape: shape[3] >= 128 and shape[5] <= 64
 TOL = 1e-4
 
 
@@ -34,10 +37,14 @@ def within(got, ref, bound, label):
     assert worst <= TOL, f"{label}: error {worst:.3g} x the absolute-value bound"
 
 
-@pytest.mark.parametrize("form", ["tcgen05", "tma", "gather", "mma_sync"])
+@pytest.mark.parametrize("form", ["tcgen05", "halo", "tma", "gather", "mma_sync"])
 @pytest.mark.parametrize("shape", SHAPES)
 def test_forward(require_gpu, shape, form):
     x, wt, _ = inputs(shape, 1)
+    if form == "halo" and not HALO(shape):
+        with pytest.raises(RuntimeError):
+            surrogate.conv3d_raw(x.cuda().bfloat16(), wt.cuda().bfloat16(), form)
+        return
     y = surrogate.conv3d_raw(x.cuda().bfloat16(), wt.cuda().bfloat16(), form)
     torch.cuda.synchronize()
     within(y, conv_ref.conv3d(x, wt), conv_ref.conv3d(x.abs(), wt.abs()), f"forward ({form})")
@@ -86,12 +93,13 @@ def test_autograd_wrapper(require_gpu):
     assert rel < 8e-3
 
 
+@pytest.mark.parametrize("shape", [(1, 8, 8, 8, 32, 48), (1, 2, 3, 128, 32, 48)])
 @pytest.mark.parametrize("relu,out_bf16", [(True, True), (False, False), (True, False)])
-def test_fused_bias_activation(require_gpu, relu, out_bf16):
-    """conv3d_act: y = act(conv(x, w) + b) from the epilogue, and its
-    gradients (ReLU mask from the stored activation, bias = sum of dy)
-    against torch's FP64 autograd on the CPU."""
-    x, wt, dy = inputs((1, 8, 8, 8, 32, 48), 5)
+def test_fused_bias_activation(require_gpu, relu, out_bf16, shape):
+    """conv3d_act: y = act(conv(x, w) + b) from the epilogue (TMA form at W = 8,
+    halo-block form at W = 128), and its gradients (ReLU mask from the stored
+    activation, bias = sum of dy) against torch's FP64 autograd on the CPU."""
+    x, wt, dy = inputs(shape, 5)
     b = conv_ref.bf16_rounded((48,), torch.Generator().manual_seed(6), 0.3)
     xd, wd, bd = x.double().requires_grad_(True), wt.double().requires_grad_(True), b.double().requires_grad_(True)
     yd = conv_ref.conv3d(xd, wd) + bd
