@@ -433,6 +433,10 @@ class JumpStepper:
     amounts of accepted jumps, less the budget increments of re-check steps
     that were rolled back.
 
+    With backoff, f consecutive rejections are followed by min(2^(f-1), 8)
+    spans of plain steps before the next trial (the inlet transient, where
+    the mass gate fails, costs fewer proposals).
+
     The stepper keeps the simulated clock itself: the solver's own step
     counter does not see jumps, so plain stepping uses nicr_step and the Ksp
     scans fire here (before the step whose physical time reaches the next
@@ -441,7 +445,7 @@ class JumpStepper:
     """
 
     def __init__(self, solver, model, norm, k: int, probe: int = 2, mass_tol: float = 0.05,
-                 recheck_factor: float = 4.0):
+                 recheck_factor: float = 4.0, backoff: bool = False):
         from . import NUCLEATION
         if norm is not None and norm.steps_k != k:
             raise ValueError(f"the network predicts {norm.steps_k} steps ahead, not {k}")
@@ -460,6 +464,8 @@ class JumpStepper:
         self.counts = {"accepted": 0, "rejected_mass": 0, "rejected_recheck": 0, "plain_steps": 0,
                        "jumped_steps": 0, "scans": 0}
         self.gates = []   # per trial: (c for O, c for Cr, re-check ratio post / pre or None)
+        # backoff: after f consecutive rejections, min(2^(f-1), 8) spans of plain steps before the next trial
+        self.backoff, self.fails, self.skip = backoff, 0, 0
 
     def _due(self, t: int) -> bool:
         """A scan fires before step t + 1."""
@@ -524,6 +530,10 @@ class JumpStepper:
             if self.model is None or left < span or free < span:
                 self.plain(left if self.model is None else min(left, free + 1))
                 continue
+            if self.skip > 0:
+                self.skip -= 1
+                self.plain(span)
+                continue
             t0, counts0 = self.t, dict(self.counts)
             xa = self._state()
             self.plain(self.probe)
@@ -542,6 +552,7 @@ class JumpStepper:
             if max(abs(c) for c in cs) > self.mass_tol:
                 self.gates.append((cs[0], cs[1], None))
                 self.counts["rejected_mass"] += 1
+                self._rejected()
                 self.plain(self.k + self.probe)
                 continue
             for i, c in enumerate(cs):
@@ -555,6 +566,7 @@ class JumpStepper:
             post = self._change(prop, self._state()) / self.probe
             self.gates.append((cs[0], cs[1], post / pre if pre > 0 else float("inf")))
             if post <= self.recheck_factor * pre:
+                self.fails = 0
                 self.counts["accepted"] += 1
                 self.counts["jumped_steps"] += self.k
                 for f in ("o", "cr"):
@@ -567,8 +579,14 @@ class JumpStepper:
             self.t, self.counts = t0 + self.probe, counts0
             self.counts["plain_steps"] += self.probe
             self.counts["rejected_recheck"] += 1
+            self._rejected()
             self.plain(self.k + self.probe)
         return dict(self.counts)
+
+    def _rejected(self):
+        self.fails += 1
+        if self.backoff:
+            self.skip = min(2 ** (self.fails - 1), 8)
 
     def close(self):
         pass
