@@ -149,3 +149,33 @@ def test_unet_gradients_finite_and_descend(require_gpu):
         opt.step()
         losses.append(loss.item())
     assert losses[-1] < 0.7 * losses[0]
+
+
+def _random_shapes(count, seed):
+    """Seeded shapes over the forms' cases: batches, degenerate d or h of 1,
+    rows below, at and above 128 voxels (not multiples of 128), channel
+    counts 16..96 and Cout up to 80; voxel counts multiples of 64."""
+    import random
+    rnd = random.Random(seed)
+    out = []
+    while len(out) < count:
+        n, d, h = rnd.choice([1, 2]), rnd.choice([1, 2, 3, 5]), rnd.choice([1, 2, 4, 6])
+        w = rnd.choice([8, 16, 24, 64, 128, 136, 200, 256])
+        ci, co = rnd.choice([16, 32, 48, 64, 96]), rnd.choice([16, 32, 48, 64, 80])
+        if (n * d * h * w) % 64 == 0 and n * d * h * w <= 8192:
+            out.append((n, d, h, w, ci, co))
+    return out
+
+
+@pytest.mark.parametrize("shape", _random_shapes(14, 11))
+def test_random_shapes_every_form(require_gpu, shape):
+    x, wt, dy = inputs(shape, 9)
+    ref, bound = conv_ref.conv3d(x, wt), conv_ref.conv3d(x.abs(), wt.abs())
+    xb, wb, dyb = x.cuda().bfloat16(), wt.cuda().bfloat16(), dy.cuda().bfloat16()
+    forms = ["tcgen05", "tma", "gather"] + (["halo"] if HALO(shape) else [])
+    for form in forms:
+        within(surrogate.conv3d_raw(xb, wb, form), ref, bound, f"forward ({form}) {shape}")
+    _, dw_ref = conv_ref.grads(x, wt, dy)
+    _, dw_abs = conv_ref.grads(x.abs(), wt, dy.abs())
+    within(surrogate.conv3d_wgrad_raw(xb, dyb), dw_ref, dw_abs, f"weight gradient {shape}")
+    assert surrogate.conv_error() == 0
