@@ -446,9 +446,16 @@ int nicr_conv3d_fwd_act(const void* x, const void* w, const float* bias, int act
                         int cin, int cout, void* stream);
 /* The same from a staged halo block (Cout <= 64 and rows of at least 128
  * voxels, else NICR_ERR_INVALID_ARG); nicr_conv3d_fwd_act and
- * nicr_conv3d_fwd use it for Cout <= 32, where it is the faster form. */
+ * nicr_conv3d_fwd use it for Cout <= 32 with Cin x Cout <= 768, where it is
+ * the faster form. */
 int nicr_conv3d_fwd_halo(const void* x, const void* w, const float* bias, int act, void* y, int n, int d, int h, int w_,
                          int cin, int cout, void* stream);
+/* The halo-block forward marching along y (a CTA keeps its input lines and
+ * weights on chip between output lines): Cin <= 48, Cout <= 32 and rows of
+ * at least 128 voxels, else NICR_ERR_INVALID_ARG; nicr_conv3d_fwd_act and
+ * nicr_conv3d_fwd use it for Cin 16, where it is the fastest form. */
+int nicr_conv3d_fwd_march(const void* x, const void* w, const float* bias, int act, void* y, int n, int d, int h,
+                          int w_, int cin, int cout, void* stream);
 int nicr_conv3d_fwd_gather(const void* x, const void* w, float* y, int n, int d, int h, int w_, int cin, int cout,
                            void* stream);
 int nicr_conv3d_fwd_mma_sync(const void* x, const void* w, float* y, int n, int d, int h, int w_, int cin, int cout,

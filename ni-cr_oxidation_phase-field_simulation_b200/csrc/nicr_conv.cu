@@ -736,6 +736,221 @@ bool halo_plan(const Vol& V, int cin, int cout, HaloConv& H) {
     return true;
 }
 
+// ---------------------------------------------------------------- forward marching along y
+// The halo-block forward with the block kept between output lines: a CTA
+// owns x tile x0..x0+127 of plane (b, z) and output lines y0..y1-1. Input
+// line L (y index; the three z lines z-1..z+1 of it) sits in ring slot L % 4
+// as one TMA box {8, 130, 1, 3, 1} per 8 channels ([slot][kc][dz][130 rows]
+// [16 B], each box padded to 128 bytes), so a new output line loads 3 input
+// lines instead of 9. All weights ([chunk][tap][kc][co][16 B]) are staged
+// once per CTA. Two TMEM accumulators: in iteration y the MMAs of line y run
+// while the four warps store line y-1; then line y+2 is loaded into the slot
+// of line y-2, whose last reader (the MMAs of line y-1) has finished.
+// Applies to Cin <= 48, Cout <= 32 on rows of at least 128 voxels.
+struct MarchConv {
+    int kcp, cols, tiles_x, ysplit, lines;   // 8-channel planes, TMEM columns, x tiles, y ranges, lines per CTA
+    uint32_t box, plane, slot, w_bytes, w_off;
+    size_t smem;
+};
+
+__global__ void __launch_bounds__(128) k_conv3d_fwd_march(const __grid_constant__ CUtensorMap xmap,
+                                                           const __nv_bfloat16* __restrict__ wt, void* __restrict__ y,
+                                                           const float* __restrict__ bias, int act, const Vol V, int cin,
+                                                           int cout, const MarchConv M) {
+    extern __shared__ unsigned char mc_smem_raw[];
+    const uint32_t raw = smem_u32(mc_smem_raw);
+    const uint32_t base = (raw + 1023u) & ~1023u;
+    unsigned char* gen = mc_smem_raw + (base - raw);
+    const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+    uint64_t* full = reinterpret_cast<uint64_t*>(gen + M.w_off + M.w_bytes);   // 4 slots
+    uint64_t* accf = full + 4;                                                 // 2 accumulators
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(accf + 2);
+
+    long long blk = blockIdx.x;
+    const int tx = (int)(blk % M.tiles_x);
+    blk /= M.tiles_x;
+    const int ys = (int)(blk % M.ysplit);
+    blk /= M.ysplit;
+    const int z = (int)(blk % V.d), b = (int)(blk / V.d);
+    const int x0 = tx * TC_M, N = cout;
+    const int y0 = ys * M.lines, y1 = min(V.h, y0 + M.lines);
+    const int chunks = cin / 16;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(M.cols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    // input line L into its slot (thread 0); k = L - (y0 - 1) counts the loads of this CTA
+    auto load_line = [&](int L) {
+        const uint32_t sl = (uint32_t)(L - (y0 - 1)) % 4u;
+        mbar_expect(smem_u32(full + sl), (uint32_t)M.kcp * M.box);
+        for (int kc = 0; kc < M.kcp; ++kc)
+            tma_5d(base + sl * M.slot + kc * M.plane, &xmap, kc * 8, x0 - 1, L, z - 1, b, smem_u32(full + sl));
+    };
+    if (t == 0) {
+        for (int s = 0; s < 6; ++s) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(full + s)));
+        asm volatile("fence.mbarrier_init.release.cluster;");
+        asm volatile("prefetch.tensormap [%0];" ::"l"(&xmap) : "memory");
+        for (int L = y0 - 1; L <= y0 + 1; ++L) load_line(L);
+    }
+    // all weights: [chunk][tap][kc][co][8 channels]
+    for (int q = t; q < chunks * 27 * 2 * N; q += 128) {
+        const int co = q % N, kc = (q / N) % 2, tap = (q / (2 * N)) % 27, c = q / (54 * N);
+        cp_async16(base + M.w_off + (uint32_t)q * 16, wt + ((long long)co * 27 + tap) * cin + c * 16 + kc * 8, true);
+    }
+    asm volatile("cp.async.commit_group;");
+    asm volatile("cp.async.wait_group 0;");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+    const uint32_t idesc = umma_idesc(TC_M, N);
+
+    // stores output line yo from accumulator j % 2 (j = yo - y0) after its MMAs completed
+    auto epilogue = [&](int yo) -> bool {
+        const int j = yo - y0;
+        const bool done = mbar_wait(smem_u32(accf + (j & 1)), (uint32_t)((j >> 1) & 1));
+        if (__syncthreads_or(!done)) return false;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const int r = warp * 32 + lane;
+        const int xx = x0 + r;
+        const bool store = xx < V.w;
+        const long long o0 = ((((long long)b * V.d + z) * V.h + yo) * V.w + xx) * cout;
+        for (int c = 0; c < N; c += 16) {
+            uint32_t q[16];
+            const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)((j & 1) * N + c);
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+                : "=r"(q[0]), "=r"(q[1]), "=r"(q[2]), "=r"(q[3]), "=r"(q[4]), "=r"(q[5]), "=r"(q[6]), "=r"(q[7]),
+                  "=r"(q[8]), "=r"(q[9]), "=r"(q[10]), "=r"(q[11]), "=r"(q[12]), "=r"(q[13]), "=r"(q[14]), "=r"(q[15])
+                : "r"(taddr));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            float v[16];
+#pragma unroll
+            for (int jj = 0; jj < 16; jj += 4) {
+                const float4 bj = bias ? *reinterpret_cast<const float4*>(bias + c + jj) : make_float4(0.f, 0.f, 0.f, 0.f);
+                v[jj] = __uint_as_float(q[jj]) + bj.x;
+                v[jj + 1] = __uint_as_float(q[jj + 1]) + bj.y;
+                v[jj + 2] = __uint_as_float(q[jj + 2]) + bj.z;
+                v[jj + 3] = __uint_as_float(q[jj + 3]) + bj.w;
+            }
+            if (act & ACT_RELU) {
+#pragma unroll
+                for (int jj = 0; jj < 16; ++jj) v[jj] = fmaxf(v[jj], 0.f);
+            }
+            if (!store) continue;
+            if (act & ACT_BF16) {
+                uint32_t hh[8];
+#pragma unroll
+                for (int jj = 0; jj < 8; ++jj)
+                    hh[jj] = (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(v[2 * jj])) |
+                             ((uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(v[2 * jj + 1])) << 16);
+                uint4* out = reinterpret_cast<uint4*>(static_cast<__nv_bfloat16*>(y) + o0 + c);
+                out[0] = make_uint4(hh[0], hh[1], hh[2], hh[3]);
+                out[1] = make_uint4(hh[4], hh[5], hh[6], hh[7]);
+            } else {
+                float* out = static_cast<float*>(y) + o0 + c;
+#pragma unroll
+                for (int jj = 0; jj < 16; jj += 4)
+                    *reinterpret_cast<float4*>(out + jj) = make_float4(v[jj], v[jj + 1], v[jj + 2], v[jj + 3]);
+            }
+        }
+        // the accumulator is read: the MMAs of line yo + 2 may overwrite it
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+        return true;
+    };
+
+    bool ok = true;
+    int issued = 0;   // output lines whose MMAs were issued
+    for (int yo = y0; yo < y1 && ok; ++yo) {
+        if (t == 0) {
+            // lines yo-1 and yo landed in earlier iterations (or the prologue); wait for yo + 1
+            for (int L = (yo == y0 ? yo - 1 : yo + 1); L <= yo + 1 && ok; ++L) {
+                const int k = L - (y0 - 1);
+                ok = mbar_wait(smem_u32(full + (k & 3)), (uint32_t)((k >> 2) & 1));
+            }
+            if (ok) {
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const int j = yo - y0;
+                const uint32_t dacc = tmem + (uint32_t)((j & 1) * N);
+                int first = 1;
+                for (int c = 0; c < chunks; ++c)
+                    for (int tap = 0; tap < 27; ++tap) {
+                        const int L = yo + (tap / 3) % 3 - 1, dz = tap / 9;   // input line and its z line
+                        const uint32_t sl = (uint32_t)(L - (y0 - 1)) % 4u;
+                        const uint32_t a = base + sl * M.slot + (uint32_t)(2 * c) * M.plane +
+                                           (uint32_t)(dz * HB_ROWS + tap % 3) * 16;
+                        const uint64_t ad = umma_sdesc(a, M.plane, 128);
+                        const uint64_t bd =
+                            umma_sdesc(base + M.w_off + (uint32_t)((c * 27 + tap) * 2 * N) * 16, (uint32_t)N * 16, 128);
+                        const uint32_t accum = first ? 0u : 1u;
+                        first = 0;
+                        asm volatile(
+                            "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                            " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(dacc),
+                            "l"(ad), "l"(bd), "r"(idesc), "r"(accum));
+                    }
+                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                    smem_u32(accf + (j & 1))));
+            }
+        }
+        if (__syncthreads_or(!ok)) {
+            ok = false;
+            break;
+        }
+        issued = yo - y0 + 1;
+        // line yo - 1 out while the MMAs of line yo run
+        if (yo > y0 && !epilogue(yo - 1)) {
+            ok = false;
+            break;
+        }
+        // the MMAs of line yo - 1 are complete: line yo - 2's slot takes line yo + 2
+        if (t == 0 && yo + 2 <= y1) load_line(yo + 2);
+    }
+    if (ok && issued > 0) ok = epilogue(y0 + issued - 1);
+    if (!ok && t == 0) {
+        atomicExch(&g_conv_error, 1);
+        // wait (bounded) for the issued MMAs and the loads in flight
+        if (issued > 0) mbar_wait(smem_u32(accf + ((issued - 1) & 1)), (uint32_t)(((issued - 1) >> 1) & 1));
+        const int last = min(y1, y0 + issued + 1);
+        for (int L = max(y0 - 1, last - 3); L <= last; ++L) {
+            const int k = L - (y0 - 1);
+            mbar_wait(smem_u32(full + (k & 3)), (uint32_t)((k >> 2) & 1));
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(M.cols));
+}
+
+// The y-march plan, or false outside its shapes.
+bool march_plan(const Vol& V, int cin, int cout, MarchConv& M) {
+    if (cout > 32 || cin > 48 || V.w < TC_M || cin % 16 != 0) return false;
+    M = MarchConv{};
+    M.kcp = cin / 8;
+    M.cols = 32;
+    while (M.cols < 2 * cout) M.cols <<= 1;
+    M.tiles_x = (V.w + TC_M - 1) / TC_M;
+    M.box = 3u * HB_ROWS * 16;
+    M.plane = (M.box + 127u) & ~127u;
+    M.slot = (uint32_t)M.kcp * M.plane;
+    M.w_off = 4 * M.slot;
+    M.w_bytes = (uint32_t)27 * cin * cout * 2;
+    // y ranges: about 2 waves of 148 SMs x 2 CTAs, at least 8 lines each
+    const long long planes = (long long)M.tiles_x * V.d * V.n;
+    long long split = (148LL * 4 + planes - 1) / planes;
+    if (split > (V.h + 7) / 8) split = (V.h + 7) / 8;
+    if (split < 1) split = 1;
+    M.lines = (int)((V.h + split - 1) / split);
+    M.ysplit = (V.h + M.lines - 1) / M.lines;
+    M.smem = (size_t)M.w_off + M.w_bytes + 6 * 8 + 8 + 1024;
+    if (M.smem < (size_t)M.cols * 400) M.smem = (size_t)M.cols * 400;
+    return M.smem <= 227u * 1024u;
+}
+
 // ---------------------------------------------------------------- weight gradient, tcgen05 + TMA
 // dw[co][tap][ci] = sum_u dy[u - off(tap)][co] * x[u][ci] (u runs over the
 // voxels of x; dy is zero outside the grid): one GEMM with M = (tap, co)
@@ -969,10 +1184,16 @@ int nicr_conv3d_fwd_tma(const void* x, const void* w, float* y, int n, int d, in
 
 int nicr_conv3d_fwd_act(const void* x, const void* w, const float* bias, int act, void* y, int n, int d, int h, int w_,
                         int cin, int cout, void* stream) {
-    // the halo block wins for narrow outputs (16->16 at 128^3: 143 against 90
-    // TFLOP/s) and loses from Cout 64 on (64->64 at 128^3: 214 against 677)
+    // measured at 128^3 (TFLOP/s): march / halo block / per-tap TMA
+    //   16->16 170 / 145 / 91, 16->32 238 / 167 / 135, 48->16 128 / 138 / 104,
+    //   32->32 200 / 131 / 225, 64->64 - / 214 / 677
+    MarchConv M;
+    if (cin == 16 && march_plan(Vol{n, d, h, w_}, cin, cout, M)) {
+        const int rc = nicr_conv3d_fwd_march(x, w, bias, act, y, n, d, h, w_, cin, cout, stream);
+        if (rc != NICR_ERR_INVALID_ARG) return rc;
+    }
     HaloConv H;
-    if (cout <= 32 && halo_plan(Vol{n, d, h, w_}, cin, cout, H)) {
+    if (cout <= 32 && cin * cout <= 768 && halo_plan(Vol{n, d, h, w_}, cin, cout, H)) {
         const int rc = nicr_conv3d_fwd_halo(x, w, bias, act, y, n, d, h, w_, cin, cout, stream);
         if (rc != NICR_ERR_INVALID_ARG) return rc;
     }
@@ -1003,6 +1224,33 @@ int nicr_conv3d_fwd_halo(const void* x, const void* w, const float* bias, int ac
     const long long tiles = (long long)H.tiles_x * h * d * n;
     k_conv3d_fwd_halo<<<(unsigned)tiles, 128, H.smem, static_cast<cudaStream_t>(stream)>>>(
         xmap, static_cast<const __nv_bfloat16*>(w), y, bias, act, V, cin, cout, H);
+    return cudaGetLastError() == cudaSuccess ? NICR_OK : NICR_ERR_CUDA;
+}
+
+int nicr_conv3d_fwd_march(const void* x, const void* w, const float* bias, int act, void* y, int n, int d, int h,
+                          int w_, int cin, int cout, void* stream) {
+    const Vol V{n, d, h, w_};
+    const int rc = check_args(V.voxels(), cin, cout);
+    MarchConv M;
+    if (rc != NICR_OK || !x || !w || !y || (act & ~(ACT_RELU | ACT_BF16)) != 0 || !march_plan(V, cin, cout, M))
+        return rc != NICR_OK ? rc : NICR_ERR_INVALID_ARG;
+    const auto enc = conv_map_encoder();
+    if (!enc) return NICR_ERR_CUDA;
+    CUtensorMap xmap;
+    const cuuint64_t dims[5] = {(cuuint64_t)cin, (cuuint64_t)w_, (cuuint64_t)h, (cuuint64_t)d, (cuuint64_t)n};
+    const cuuint64_t str[4] = {(cuuint64_t)cin * 2, (cuuint64_t)w_ * cin * 2, (cuuint64_t)h * w_ * cin * 2,
+                               (cuuint64_t)d * h * w_ * cin * 2};
+    const cuuint32_t box[5] = {8, HB_ROWS, 1, 3, 1};
+    const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
+    if (enc(&xmap, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<void*>(x), dims, str, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return NICR_ERR_INVALID_ARG;
+    if (cudaFuncSetAttribute(k_conv3d_fwd_march, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)M.smem) != cudaSuccess)
+        return NICR_ERR_CUDA;
+    const long long blocks = (long long)M.tiles_x * M.ysplit * d * n;
+    k_conv3d_fwd_march<<<(unsigned)blocks, 128, M.smem, static_cast<cudaStream_t>(stream)>>>(
+        xmap, static_cast<const __nv_bfloat16*>(w), y, bias, act, V, cin, cout, M);
     return cudaGetLastError() == cudaSuccess ? NICR_OK : NICR_ERR_CUDA;
 }
 

@@ -31,6 +31,7 @@ def _lib():
             getattr(L, f).argtypes = [vp, vp, vp, i, i, i, i, i, i, vp]
         L.nicr_conv3d_fwd_act.argtypes = [vp, vp, vp, i, vp, i, i, i, i, i, i, vp]
         L.nicr_conv3d_fwd_halo.argtypes = [vp, vp, vp, i, vp, i, i, i, i, i, i, vp]
+        L.nicr_conv3d_fwd_march.argtypes = [vp, vp, vp, i, vp, i, i, i, i, i, i, vp]
         L.nicr_conv3d_error.argtypes = [ctypes.POINTER(ctypes.c_int)]
         L._conv_bound = True
     return L
@@ -43,17 +44,18 @@ def _check(rc, what):
 
 def conv3d_raw(x, w_bf16, form: str = "tcgen05"):
     """y = conv(x, w): x (n, d, h, w, cin) BF16, w (cout, 27, cin) BF16 -> FP32.
-    form: "tcgen05" (nicr_conv3d_fwd: halo block, TMA-staged or gathered as
-    the shapes allow), "halo", "tma", "gather" (the tcgen05 forms alone) or
-    "mma_sync"."""
+    form: "tcgen05" (nicr_conv3d_fwd: y-march, halo block, TMA-staged or
+    gathered as the shapes allow), "march", "halo", "tma", "gather" (the
+    tcgen05 forms alone) or "mma_sync"."""
     import torch
     n, d, h, wd, cin = x.shape
     cout = w_bf16.shape[0]
     y = torch.empty((n, d, h, wd, cout), dtype=torch.float32, device=x.device)
     stream = torch.cuda.current_stream(x.device).cuda_stream
-    if form == "halo":
-        _check(_lib().nicr_conv3d_fwd_halo(x.data_ptr(), w_bf16.data_ptr(), None, 0, y.data_ptr(), n, d, h, wd, cin,
-                                           cout, stream), "nicr_conv3d_fwd_halo")
+    if form in ("halo", "march"):
+        f = f"nicr_conv3d_fwd_{form}"
+        _check(getattr(_lib(), f)(x.data_ptr(), w_bf16.data_ptr(), None, 0, y.data_ptr(), n, d, h, wd, cin, cout,
+                                  stream), f)
         return y
     f = {"tcgen05": "nicr_conv3d_fwd", "tma": "nicr_conv3d_fwd_tma", "gather": "nicr_conv3d_fwd_gather",
          "mma_sync": "nicr_conv3d_fwd_mma_sync"}[form]

@@ -54,3 +54,7 @@ def test_conv_abi_rejects_shapes():
     assert L.nicr_conv3d_fwd_halo(1, 1, None, 0, 1, 1, 4, 4, 64, 16, 16, None) == err
     assert L.nicr_conv3d_fwd_halo(1, 1, None, 0, 1, 1, 1, 1, 128, 16, 128, None) == err
     assert L.nicr_conv3d_fwd_act(1, 1, None, 4, 1, 1, 1, 1, 128, 16, 16, None) == err   # unknown act bit
+    # the y-march form: Cin <= 48, Cout <= 32, rows of at least 128 voxels
+    assert L.nicr_conv3d_fwd_march(1, 1, None, 0, 1, 1, 1, 1, 128, 64, 16, None) == err
+    assert L.nicr_conv3d_fwd_march(1, 1, None, 0, 1, 1, 1, 1, 128, 16, 48, None) == err
+    assert L.nicr_conv3d_fwd_march(1, 1, None, 0, 1, 1, 1, 4, 64, 16, 16, None) == err

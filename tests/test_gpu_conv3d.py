@@ -17,8 +17,13 @@ pytestmark = pytest.mark.gpu
 # second x tile, 1 to 4 chunks of 16 input channels)
 SHAPES = [(2, 4, 8, 8, 16, 48), (1, 8, 8, 8, 32, 64), (1, 6, 4, 16, 48, 16), (2, 16, 16, 16, 16, 32),
           (1, 8, 8, 8, 96, 128), (1, 4, 4, 4, 16, 16), (1, 4, 8, 8, 32, 272), (1, 4, 4, 8, 80, 32),
-          (1, 8, 8, 8, 64, 256), (1, 3, 4, 128, 16, 16), (1, 2, 3, 160, 48, 32), (1, 2, 4, 136, 64, 48)]
+          (1, 8, 8, 8, 64, 256), (1, 3, 4, 128, 16, 16), (1, 2, 3, 160, 48, 32), (1, 2, 4, 136, 64, 48),
+          (1, 3, 20, 128, 16, 16), (2, 2, 16, 200, 32, 32), (1, 2, 1, 128, 48, 16)]
 HALO = lambda shape: shape[3] >= 128 and shape[5] <= 64
+# the y-march form: Cin <= 48, Cout <= 32, rows >= 128, and its shared memory (27 x Cin x Cout x 2 B of
+# weights beside 4 x Cin/8 input planes) within a CTA's
+MARCH = lambda shape: (shape[3] >= 128 and shape[4] <= 48 and shape[5] <= 32 and
+                       4 * (shape[4] // 8) * 6272 + 27 * shape[4] * shape[5] * 2 + 1080 <= 227 * 1024)
 TOL = 1e-4
 
 
@@ -37,11 +42,11 @@ def within(got, ref, bound, label):
     assert worst <= TOL, f"{label}: error {worst:.3g} x the absolute-value bound"
 
 
-@pytest.mark.parametrize("form", ["tcgen05", "halo", "tma", "gather", "mma_sync"])
+@pytest.mark.parametrize("form", ["tcgen05", "march", "halo", "tma", "gather", "mma_sync"])
 @pytest.mark.parametrize("shape", SHAPES)
 def test_forward(require_gpu, shape, form):
     x, wt, _ = inputs(shape, 1)
-    if form == "halo" and not HALO(shape):
+    if (form == "halo" and not HALO(shape)) or (form == "march" and not MARCH(shape)):
         with pytest.raises(RuntimeError):
             surrogate.conv3d_raw(x.cuda().bfloat16(), wt.cuda().bfloat16(), form)
         return
@@ -93,14 +98,14 @@ def test_autograd_wrapper(require_gpu):
     assert rel < 8e-3
 
 
-@pytest.mark.parametrize("shape", [(1, 8, 8, 8, 32, 48), (1, 2, 3, 128, 32, 48)])
+@pytest.mark.parametrize("shape", [(1, 8, 8, 8, 32, 48), (1, 2, 3, 128, 32, 48), (1, 2, 12, 128, 32, 32)])
 @pytest.mark.parametrize("relu,out_bf16", [(True, True), (False, False), (True, False)])
 def test_fused_bias_activation(require_gpu, relu, out_bf16, shape):
     """conv3d_act: y = act(conv(x, w) + b) from the epilogue (TMA form at W = 8,
-    halo-block form at W = 128), and its gradients (ReLU mask from the stored
+    halo-block form at W = 128 with Cout 48, y-march with Cout 32), and its gradients (ReLU mask from the stored
     activation, bias = sum of dy) against torch's FP64 autograd on the CPU."""
     x, wt, dy = inputs(shape, 5)
-    b = conv_ref.bf16_rounded((48,), torch.Generator().manual_seed(6), 0.3)
+    b = conv_ref.bf16_rounded((shape[5],), torch.Generator().manual_seed(6), 0.3)
     xd, wd, bd = x.double().requires_grad_(True), wt.double().requires_grad_(True), b.double().requires_grad_(True)
     yd = conv_ref.conv3d(xd, wd) + bd
     yd = torch.relu(yd) if relu else yd
@@ -172,7 +177,7 @@ def test_random_shapes_every_form(require_gpu, shape):
     x, wt, dy = inputs(shape, 9)
     ref, bound = conv_ref.conv3d(x, wt), conv_ref.conv3d(x.abs(), wt.abs())
     xb, wb, dyb = x.cuda().bfloat16(), wt.cuda().bfloat16(), dy.cuda().bfloat16()
-    forms = ["tcgen05", "tma", "gather"] + (["halo"] if HALO(shape) else [])
+    forms = ["tcgen05", "tma", "gather"] + (["halo"] if HALO(shape) else []) + (["march"] if MARCH(shape) else [])
     for form in forms:
         within(surrogate.conv3d_raw(xb, wb, form), ref, bound, f"forward ({form}) {shape}")
     _, dw_ref = conv_ref.grads(x, wt, dy)
