@@ -957,12 +957,12 @@ bool march_plan(const Vol& V, int cin, int cout, MarchConv& M) {
 // voxels of x; dy is zero outside the grid): one GEMM with M = (tap, co)
 // rows, N = ci, K = voxels. An M tile holds 128/Cout taps of all Cout
 // channels (Cout 16, 32 or 64) or 128 channels of one tap (Cout a multiple of
-// 128); K advances by tiles of 64 voxels (Wt x Ht of one (batch, z) plane) and
+// 128); K advances by tiles of WG_K voxels (Wt x Ht of one (batch, z) plane) and
 // is split over CTAs, which add their partial sums to dw with FP32 atomics.
 // Per K tile: A = for each tap of the M tile, the box {Ws_a, Wt, Ht, 1, 1} of
 // dy at (co0, x0-dx, y0-dy, z-dz, b) (zero fill = zero outside); B = the
 // boxes {Ws_b, Wt, Ht, 1, 1} of x at (ci0, x0, y0, z, b). Both land MN-major
-// (rows = the 64 voxels, each row Ws channels), with the swizzle of Ws
+// (rows = the WG_K voxels, each row Ws channels), with the swizzle of Ws
 // (64 -> 128 B, 32 -> 64 B, 16 -> 32 B): 8-row groups SBO = 8 rows apart, the
 // blocks of Ws channels LBO = one box apart; an MMA (K = 16) takes two
 // 8-row groups.
@@ -973,7 +973,10 @@ struct TmaWgrad {
     size_t smem;
 };
 
-constexpr int WG_K = 64;   // voxels per K tile
+// voxels per K tile; measured (TFLOP/s) 64 / 128 / 256 voxels: 16->16 at 128^3
+// 58 / 97 / 78, 48->16 164 / 220 / 210, 64->64 at 32^3 180 / 254 / 277,
+// 96->32 at 64^3 328 / 261 / 413, 64->256 at 64^3 451 / 537 / 461
+constexpr int WG_K = 128;
 
 __device__ __forceinline__ uint64_t umma_sdesc_mn(uint32_t saddr, uint32_t row_bytes, uint32_t lbo) {
     const uint64_t layout = row_bytes == 128 ? 2 : row_bytes == 64 ? 4 : 6;
