@@ -412,6 +412,14 @@ def surrogate_workload(args) -> int:
     xin = torch.randn((1, 128, 128, 128, 8), device=dev)
     with torch.no_grad():
         fwd_ms = timed(lambda: net(xin), reps=5)
+    # the whole proposal (normalisation, U-Net, un-normalisation) replayed as one CUDA graph
+    norm0 = surrogate.Normaliser(torch.randn((1, 3, 8, 8, 8, 4), device=dev), torch.randn((1, 3, 8, 8, 8, 4), device=dev),
+                                 1, 16)
+    gp = surrogate.GraphPredictor(net, norm0, (1, 128, 128, 128, 4), dev)
+    x4, r4 = torch.randn((1, 128, 128, 128, 4), device=dev), torch.randn((1, 128, 128, 128, 4), device=dev)
+    eager_ms = timed(lambda: surrogate.predict(net, norm0, x4, r4), reps=5)
+    graph_ms = timed(lambda: gp(x4, r4), reps=5)
+    del gp
     xt = torch.randn((2, 64, 64, 64, 8), device=dev)
     opt = torch.optim.Adam(net.parameters(), lr=1e-3)
 
@@ -434,7 +442,8 @@ def surrogate_workload(args) -> int:
            "roofline": {"bound": "tensor", "kernel": "k_conv3d_fwd_tma", "layer": best["layer"],
                         "achieved": best["fwd_tcgen05_tflops"], "peak": peak, "unit": "TFLOP/s",
                         "frac": best["fwd_tcgen05_tflops"] / peak, "peak_kind": peak_kind},
-           "layers": rows, "unet_forward_128cube_ms": fwd_ms, "train_step_64cube_batch2_ms": train_ms,
+           "layers": rows, "unet_forward_128cube_ms": fwd_ms, "proposal_128cube_ms": {"eager": eager_ms, "graph": graph_ms},
+           "train_step_64cube_batch2_ms": train_ms,
            "plain_fp64_step_128cube_ms": plain_ms,
            "break_even_k": fwd_ms / plain_ms, "jumps": jumps, "conv_error_flag": err, "clocks": cl,
            "data": "synthetic"}

@@ -183,3 +183,16 @@ def test_data_parallel_training_over_nccl_single_rank(require_gpu):
     ok, first, last, err = q.get(timeout=300)
     p.join(timeout=120)
     assert p.exitcode == 0 and ok and err == 0 and last < first
+
+
+def test_graph_predictor_matches_eager(trained):
+    """The proposal replayed as a CUDA graph equals the eager one bit for bit,
+    for new inputs written into its static buffers."""
+    import torch
+    net, norm, _, (x, r), _ = trained
+    gp = surrogate.GraphPredictor(net, norm, (1,) + tuple(x.shape[2:]), x.device)
+    for i in (3, 7):
+        x0, r0 = x[4:, i].contiguous(), r[4:, i].contiguous()
+        eager = surrogate.predict(net, norm, x0, r0)
+        assert torch.equal(gp(x0, r0), eager)
+    assert surrogate.conv_error() == 0
