@@ -3,18 +3,22 @@
 // implicit GEMMs on the BF16 tensor cores with FP32 accumulation.
 //
 // Layout: activations NDHWC, BF16, channels a multiple of 16; weights
-// [Cout][27][Cin] BF16 (tap = (dz+1)*9 + (dy+1)*3 + (dx+1)); outputs FP32.
+// [Cout][27][Cin] BF16 (tap = (dz+1)*9 + (dy+1)*3 + (dx+1)); outputs FP32
+// (or, through the fused epilogue, act(y + bias) in BF16).
 //   forward  y[v][co]  = sum_{tap,ci} x[v + off(tap)][ci] * w[co][tap][ci]
-//            (GEMM: M = voxels, N = Cout, K = 27*Cin; A gathered per tap)
+//            (GEMM: M = voxels, N = Cout, K = 27*Cin)
 //   dgrad    dx = forward(dy, w') with w'[ci][tap][co] = w[co][26-tap][ci]
 //            (off(26 - tap) = -off(tap)); the caller transposes the weights
 //   wgrad    dw[co][tap][ci] = sum_v dy[v][co] * x[v + off(tap)][ci]
 //            (GEMM: M = (tap, Cout), N = Cin, K = voxels, split over CTAs)
-// The forward (and so the data gradient) runs on tcgen05.mma with the
-// accumulator in TMEM, its operands staged by TMA (k_conv3d_fwd_tma) or, where
-// the driver refuses the tensor maps, gathered with cp.async
-// (k_conv3d_fwd_tc); the weight gradient runs on tcgen05.mma with TMA-staged
-// operands (k_conv3d_wgrad_tma) for Cout 16, 32, 64 or multiples of 128. The
+// Every tcgen05 form keeps its accumulator in TMEM. Forward forms, chosen by
+// shape in nicr_conv3d_fwd_act from measured rates:
+//   k_conv3d_fwd_march  Cin 16, rows >= 128: halo lines kept on chip along y
+//   k_conv3d_fwd_halo   narrow outputs, rows >= 128: one halo block per chunk
+//   k_conv3d_fwd_tma    everything else: per-tap TMA boxes
+//   k_conv3d_fwd_tc     where the driver refuses a tensor map: cp.async gathers
+// The weight gradient runs on tcgen05.mma with TMA-staged operands
+// (k_conv3d_wgrad_tma) for Cout 16, 32, 64 or multiples of 128. The
 // warp-level WMMA forms (16x16x16 BF16 tiles staged through shared memory)
 // stay as reference forms and as the weight gradient of other Cout.
 #include <cuda.h>
