@@ -196,3 +196,21 @@ def test_graph_predictor_matches_eager(trained):
         eager = surrogate.predict(net, norm, x0, r0)
         assert torch.equal(gp(x0, r0), eager)
     assert surrogate.conv_error() == 0
+
+
+def test_stepper_with_graph_proposals_matches_eager(trained):
+    """JumpStepper(graphs=True) replays its proposals as a CUDA graph: same
+    gates, same counts and the same fields bit for bit as eager proposals."""
+    net, norm, _, _, cfgs = trained
+    runs = []
+    for graphs in (False, True):
+        s = nicr.Solver(cfgs[4])
+        s.run(32)
+        st = surrogate.JumpStepper(s, net, norm, KS * EVERY, mass_tol=0.25, graphs=graphs)
+        counts = st.advance(96)
+        runs.append((counts, st.gates, [s.get(f) for f in ("o", "cr", "p")]))
+        s.close()
+    (c0, g0, f0), (c1, g1, f1) = runs
+    assert c0 == c1 and g0 == g1
+    for a, b in zip(f0, f1):
+        assert np.array_equal(a.view(np.int64), b.view(np.int64))
