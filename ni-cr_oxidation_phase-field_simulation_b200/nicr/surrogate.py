@@ -101,6 +101,16 @@ def conv3d_wgrad_raw(x, dy, form: str = "tcgen05"):
     return dw
 
 
+def _data_gradient(gyb, wt, dtype):
+    """dx = conv(dy, w'), stored by the epilogue in the input's BF16 where it can."""
+    import torch
+    if dtype == torch.bfloat16:
+        gx = conv3d_act_raw(gyb, wt, None, False, True)
+        if gx is not None:
+            return gx
+    return conv3d_raw(gyb, wt).to(dtype)
+
+
 def _make_fn():
     import torch
 
@@ -121,7 +131,7 @@ def _make_fn():
             gyb = gy.to(torch.bfloat16).contiguous()
             # data gradient: the forward convolution of dy with w'[ci][tap][co] = w[co][26 - tap][ci]
             wt = wb.flip(1).permute(2, 1, 0).contiguous()
-            gx = conv3d_raw(gyb, wt).to(xb.dtype)
+            gx = _data_gradient(gyb, wt, xb.dtype)
             gw = conv3d_wgrad_raw(xb, gyb)
             return gx, gw
 
@@ -154,7 +164,7 @@ def _make_fn():
             gb = g.sum(dim=tuple(range(g.dim() - 1)))
             gyb = g.to(torch.bfloat16).contiguous()
             wt = wb.flip(1).permute(2, 1, 0).contiguous()
-            gx = conv3d_raw(gyb, wt).to(xb.dtype)
+            gx = _data_gradient(gyb, wt, xb.dtype)
             gw = conv3d_wgrad_raw(xb, gyb)
             return gx, gw, gb, None, None
 
