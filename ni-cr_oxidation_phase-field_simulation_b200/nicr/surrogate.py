@@ -1,14 +1,15 @@
-"""The learned surrogate, first stage: a 3-level 3D U-Net over the fields
-(c_O, c_Cr, phi, GB indicator) that predicts the state K steps ahead, trained
-on trajectories the solver itself generates. Every convolution runs on the
-library's BF16 tensor-core kernels (nicr_conv3d_fwd for the forward pass and
-the data gradient, nicr_conv3d_wgrad for the weight gradient; FP32
-accumulation); the elementwise parts (bias, ReLU, pooling, upsampling, skip
-concatenation, the loss and the optimiser) are torch operations on the same
-stream. Activations are channels-last (NDHWC) BF16; the weights' master copy
-is FP32. JumpStepper applies the trained network to a Solver: each jump is
-accepted only if the FP64 mass budget holds and a short plain re-check
-agrees, otherwise the plain steps run.
+"""The learned surrogate: a 3-level 3D U-Net over the fields (c_O, c_Cr,
+phi, GB indicator) and their per-step rates that predicts the state K steps
+ahead, trained on trajectories the solver itself generates. Every
+convolution runs on the library's BF16 tcgen05 kernels with FP32
+accumulation: nicr_conv3d_fwd_act for the forward pass (bias, ReLU and the
+BF16 store in its epilogue) and the data gradient, nicr_conv3d_wgrad for the
+weight gradient. Pooling, upsampling, skip concatenation, the loss and the
+optimiser are torch operations on the same stream. Activations are
+channels-last (NDHWC) BF16; the weights' master copy is FP32. train() runs
+data parallel over a process group (NCCL). JumpStepper applies the trained
+network to a Solver: each jump is accepted only if the FP64 mass budget
+holds and a short plain re-check agrees, otherwise the plain steps run.
 """
 from __future__ import annotations
 
