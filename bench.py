@@ -456,7 +456,8 @@ def surrogate_jumps(dev, size=128, every=32, ks=2, steps=1024, iters=1200):
     Ksp, parameters drawn per seed): trajectories of seeds 100-103 (`steps`
     steps, a sample every `every`), a U-Net (base 16) trained `iters` Adam
     steps to jump K = ks x every steps, then seed 104 advanced `steps` steps
-    by JumpStepper (mass gate 5%, 25%, and 5% with backoff) and by nicr_run from the same state
+    by JumpStepper (mass gate 5%, 25%, 5% with backoff; linear and geometric budget
+    extrapolation) and by nicr_run from the same state
     after 64 plain steps; wall clock of each (synchronised), counts, the
     gates' values per trial, and the relative L-inf error of the jump runs
     against the plain run."""
@@ -483,10 +484,11 @@ def surrogate_jumps(dev, size=128, every=32, ks=2, steps=1024, iters=1200):
     out = {"size": size, "k": ks * every, "steps": steps, "trajectory_s": t1 - t0, "train_s": t2 - t1,
            "train_iters": iters, "loss_first20": float(np.mean(losses[:20])),
            "loss_last20": float(np.mean(losses[-20:])), "plain_wall_s": plain_s, "runs": []}
-    for tol, backoff in ((0.05, False), (0.25, False), (0.05, True)):
+    for tol, backoff, budget in ((0.05, False, "linear"), (0.25, False, "linear"), (0.05, True, "linear"),
+                                 (0.05, False, "geometric"), (0.05, True, "geometric")):
         jump = nicr.Solver(cfgs[4])
         jump.run(64)
-        st = surrogate.JumpStepper(jump, net, norm, ks * every, mass_tol=tol, backoff=backoff)
+        st = surrogate.JumpStepper(jump, net, norm, ks * every, mass_tol=tol, backoff=backoff, budget=budget)
         torch.cuda.synchronize()
         t4 = time.perf_counter()
         counts = st.advance(steps)
@@ -494,7 +496,8 @@ def surrogate_jumps(dev, size=128, every=32, ks=2, steps=1024, iters=1200):
         jump_s = time.perf_counter() - t4
         err = {f: float(np.abs(jump.get(f) - plain.get(f)).max() / max(np.abs(plain.get(f)).max(), 1e-300))
                for f in ("o", "cr")}
-        out["runs"].append({"mass_tol": tol, "backoff": backoff, "counts": counts, "jump_wall_s": jump_s,
+        out["runs"].append({"mass_tol": tol, "backoff": backoff, "budget": budget, "counts": counts,
+                            "jump_wall_s": jump_s,
                             "simulated_time_per_wall_s_ratio": plain_s / jump_s, "rel_linf_vs_plain": err,
                             "gates": [[round(a, 4), round(b, 4), None if c is None else round(c, 3)]
                                       for a, b, c in st.gates]})

@@ -463,9 +463,11 @@ class JumpStepper:
     proposal.
 
     Mass budget: the proposal's change of total O and of total Cr must equal
-    K x the measured FP64 rate up to a correction c x |change| per cell with
-    |c| <= mass_tol; the correction is then applied, so the accepted state
-    carries exactly the extrapolated budget (summed in FP64). Re-check: the
+    the change extrapolated from the probe steps' FP64 totals (K x their mean
+    rate, or with budget="geometric" a decaying rate summed over K steps) up
+    to a correction c x |change| per cell with |c| <= mass_tol; the
+    correction is then applied, so the accepted state carries exactly the
+    extrapolated budget (summed in FP64). Re-check: the
     per-step change of the re-check steps may be at most recheck_factor x
     that of the probe steps (an off-manifold proposal relaxes fast in its
     first plain steps). A jump failing either gate is rolled back to the
@@ -486,7 +488,8 @@ class JumpStepper:
     """
 
     def __init__(self, solver, model, norm, k: int, probe: int = 2, mass_tol: float = 0.05,
-                 recheck_factor: float = 4.0, backoff: bool = False, graphs: bool = False):
+                 recheck_factor: float = 4.0, backoff: bool = False, graphs: bool = False,
+                 budget: str = "linear"):
         from . import NUCLEATION
         if norm is not None and norm.steps_k != k:
             raise ValueError(f"the network predicts {norm.steps_k} steps ahead, not {k}")
@@ -494,6 +497,9 @@ class JumpStepper:
             raise ValueError("jumps leave eta unchanged: static grains only")
         self.s, self.model, self.norm, self.k, self.probe = solver, model, norm, k, probe
         self.mass_tol, self.recheck_factor = mass_tol, recheck_factor
+        if budget not in ("linear", "geometric"):
+            raise ValueError(budget)
+        self.budget = budget
         c = solver.cfg
         self.dt, self.period = c.dt, c.nucleation_period
         self.ksp = c.nucleation == NUCLEATION["ksp"]
@@ -560,6 +566,26 @@ class JumpStepper:
             self.s.device_view(f, writable=True).copy_(x[..., i])
         torch.cuda.current_stream().synchronize()
 
+    def _totals(self, x):
+        """FP64 totals of O and Cr (of x, or of the solver's current state)."""
+        if x is None:
+            return tuple(float(self.s.device_view(f).sum()) for f in ("o", "cr"))
+        return float(x[..., 0].sum()), float(x[..., 1].sum())
+
+    def _expected_change(self, t):
+        """The change of a total over the next K steps from its values over
+        the probe steps: K x the mean rate (budget="linear"), or, with
+        budget="geometric" and a rate that keeps its sign and decays between
+        the last two probe steps (ratio q), r q + r q^2 + ... + r q^K."""
+        r = [b - a for a, b in zip(t, t[1:])]
+        mean = (t[-1] - t[0]) / (len(t) - 1)
+        if self.budget != "geometric" or len(r) < 2 or r[-2] == 0.0:
+            return self.k * mean
+        q = r[-1] / r[-2]
+        if not 0.0 < q < 1.0:
+            return self.k * mean
+        return r[-1] * q * (1.0 - q ** self.k) / (1.0 - q)
+
     def _change(self, a, b):
         import torch
         return float(torch.linalg.vector_norm(((b - a) / self.norm.csd.double())[..., :3]))
@@ -587,17 +613,19 @@ class JumpStepper:
                 continue
             t0, counts0 = self.t, dict(self.counts)
             xa = self._state()
-            self.plain(self.probe)
+            totals = [self._totals(xa)]
+            for _ in range(self.probe):
+                self.plain(1)
+                totals.append(self._totals(None))
             xb = self._state()
             rb = (xb - xa) / self.probe
-            rate = {f: float(rb[..., i].sum()) for i, f in ((0, "o"), (1, "cr"))}
             pre = self._change(xa, xb) / self.probe
             prop = self._predict(xb[None].float(), rb[None].float())[0].double()
             prop[..., 3] = xb[..., 3]
             cs = []
             for i, f in ((0, "o"), (1, "cr")):
                 d = prop[..., i] - xb[..., i]
-                want = self.k * rate[f]
+                want = self._expected_change([t[i] for t in totals])
                 mag = float(d.abs().sum())
                 cs.append((want - float(d.sum())) / mag if mag > 0 else 0.0)
             if max(abs(c) for c in cs) > self.mass_tol:
