@@ -27,6 +27,10 @@
 #include <cudaTypedefs.h>
 #include <mma.h>
 
+#include <map>
+#include <mutex>
+#include <utility>
+
 #include "../../include/nicr.h"
 
 namespace {
@@ -1175,6 +1179,23 @@ bool tma_wgrad_plan(const Vol& V, int cin, int cout, TmaWgrad& G) {
 int launch_fwd_tma(const void* x, const void* w, const float* bias, int act, void* y, int n, int d, int h, int w_,
                    int cin, int cout, void* stream);
 
+// Raises a kernel's dynamic shared-memory limit when a launch needs more than
+// was set before on this device (the attribute call costs microseconds, the
+// small layers' kernels tens of them).
+int ensure_smem(const void* kernel, size_t bytes) {
+    static std::mutex mu;
+    static std::map<std::pair<const void*, int>, size_t> done;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return NICR_ERR_CUDA;
+    std::lock_guard<std::mutex> lock(mu);
+    size_t& cur = done[{kernel, dev}];
+    if (bytes <= cur) return NICR_OK;
+    if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) != cudaSuccess)
+        return NICR_ERR_CUDA;
+    cur = bytes;
+    return NICR_OK;
+}
+
 int check_args(long long voxels, int cin, int cout) {
     if (voxels <= 0 || voxels % 64 != 0 || cin <= 0 || cin % 16 != 0 || cout <= 0 || cout % 16 != 0)
         return NICR_ERR_INVALID_ARG;
@@ -1227,7 +1248,7 @@ int nicr_conv3d_fwd_halo(const void* x, const void* w, const float* bias, int ac
             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
         return NICR_ERR_INVALID_ARG;
-    if (cudaFuncSetAttribute(k_conv3d_fwd_halo, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)H.smem) != cudaSuccess)
+    if (ensure_smem((const void*)k_conv3d_fwd_halo, H.smem) != NICR_OK)
         return NICR_ERR_CUDA;
     const long long tiles = (long long)H.tiles_x * h * d * n;
     k_conv3d_fwd_halo<<<(unsigned)tiles, 128, H.smem, static_cast<cudaStream_t>(stream)>>>(
@@ -1254,7 +1275,7 @@ int nicr_conv3d_fwd_march(const void* x, const void* w, const float* bias, int a
             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
         return NICR_ERR_INVALID_ARG;
-    if (cudaFuncSetAttribute(k_conv3d_fwd_march, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)M.smem) != cudaSuccess)
+    if (ensure_smem((const void*)k_conv3d_fwd_march, M.smem) != NICR_OK)
         return NICR_ERR_CUDA;
     const long long blocks = (long long)M.tiles_x * M.ysplit * d * n;
     k_conv3d_fwd_march<<<(unsigned)blocks, 128, M.smem, static_cast<cudaStream_t>(stream)>>>(
@@ -1298,7 +1319,7 @@ int launch_fwd_tma(const void* x, const void* w, const float* bias, int act, voi
                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
             return NICR_ERR_INVALID_ARG;
     }
-    if (cudaFuncSetAttribute(k_conv3d_fwd_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C.smem) != cudaSuccess)
+    if (ensure_smem((const void*)k_conv3d_fwd_tma, C.smem) != NICR_OK)
         return NICR_ERR_CUDA;
     const long long tiles = (long long)C.tiles_x * C.tiles_y * d * n;
     const dim3 grid((unsigned)tiles, (unsigned)((cout + 255) / 256));
@@ -1335,7 +1356,7 @@ int nicr_conv3d_fwd_gather(const void* x, const void* w, float* y, int n, int d,
     // resident on one SM never ask for more than its 512 TMEM columns
     size_t smem = TC_STAGES * stage + 64;
     if (smem < (size_t)cols * 400) smem = (size_t)cols * 400;
-    if (cudaFuncSetAttribute(k_conv3d_fwd_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    if (ensure_smem((const void*)k_conv3d_fwd_tc, smem) != NICR_OK)
         return NICR_ERR_CUDA;
     const dim3 grid((unsigned)((V.voxels() + TC_M - 1) / TC_M), (unsigned)((cout + 255) / 256));
     k_conv3d_fwd_tc<<<grid, 128, smem, static_cast<cudaStream_t>(stream)>>>(
@@ -1379,8 +1400,7 @@ int nicr_conv3d_wgrad_tma(const void* x, const void* dy, float* dw, int n, int d
                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
     };
     if (!encode(&dymap, dy, cout, G.wsa) || !encode(&xmap, x, cin, G.wsb)) return NICR_ERR_INVALID_ARG;
-    if (cudaFuncSetAttribute(k_conv3d_wgrad_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G.smem) !=
-        cudaSuccess)
+    if (ensure_smem((const void*)k_conv3d_wgrad_tma, G.smem) != NICR_OK)
         return NICR_ERR_CUDA;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     if (cudaMemsetAsync(dw, 0, sizeof(float) * (size_t)cout * 27 * cin, s) != cudaSuccess) return NICR_ERR_CUDA;
