@@ -965,26 +965,26 @@ bool march_plan(const Vol& V, int cin, int cout, MarchConv& M) {
 // voxels of x; dy is zero outside the grid): one GEMM with M = (tap, co)
 // rows, N = ci, K = voxels. An M tile holds 128/Cout taps of all Cout
 // channels (Cout 16, 32 or 64) or 128 channels of one tap (Cout a multiple of
-// 128); K advances by tiles of WG_K voxels (Wt x Ht of one (batch, z) plane) and
+// 128); K advances by tiles of kt voxels (Wt x Ht of one (batch, z) plane) and
 // is split over CTAs, which add their partial sums to dw with FP32 atomics.
 // Per K tile: A = for each tap of the M tile, the box {Ws_a, Wt, Ht, 1, 1} of
 // dy at (co0, x0-dx, y0-dy, z-dz, b) (zero fill = zero outside); B = the
 // boxes {Ws_b, Wt, Ht, 1, 1} of x at (ci0, x0, y0, z, b). Both land MN-major
-// (rows = the WG_K voxels, each row Ws channels), with the swizzle of Ws
+// (rows = the kt voxels, each row Ws channels), with the swizzle of Ws
 // (64 -> 128 B, 32 -> 64 B, 16 -> 32 B): 8-row groups SBO = 8 rows apart, the
 // blocks of Ws channels LBO = one box apart; an MMA (K = 16) takes two
 // 8-row groups.
 struct TmaWgrad {
-    int wsa, wsb, taps_per_m, m_tiles, co_blocks, n_tiles, wt, ht, tiles_x, tiles_y, ktiles, parts, per_part,
+    int kt, wsa, wsb, taps_per_m, m_tiles, co_blocks, n_tiles, wt, ht, tiles_x, tiles_y, ktiles, parts, per_part,
         stages, cols;
     uint32_t a_box, b_box, a_bytes, b_bytes, stage_bytes;
     size_t smem;
 };
 
-// voxels per K tile; measured (TFLOP/s) 64 / 128 / 256 voxels: 16->16 at 128^3
-// 58 / 97 / 78, 48->16 164 / 220 / 210, 64->64 at 32^3 180 / 254 / 277,
-// 96->32 at 64^3 328 / 261 / 413, 64->256 at 64^3 451 / 537 / 461
-constexpr int WG_K = 128;
+// voxels per K tile (kt); measured (TFLOP/s) 64 / 128 / 256 voxels: 16->16 at
+// 128^3 58 / 97 / 78, 48->16 164 / 220 / 210, 64->64 at 32^3 180 / 254 / 277,
+// 96->32 at 64^3 328 / 261 / 413, 64->256 at 64^3 451 / 537 / 461: 256 for
+// Cin >= 96 with Cout <= 64 (when the stages fit), else 128
 
 __device__ __forceinline__ uint64_t umma_sdesc_mn(uint32_t saddr, uint32_t row_bytes, uint32_t lbo) {
     const uint64_t layout = row_bytes == 128 ? 2 : row_bytes == 64 ? 4 : 6;
@@ -1076,7 +1076,7 @@ __global__ void __launch_bounds__(128) k_conv3d_wgrad_tma(const __grid_constant_
             *consumed = it + 1;
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const uint32_t st = base + s * G.stage_bytes;
-            for (int k = 0; k < WG_K / 16; ++k) {   // two 8-row groups per MMA
+            for (int k = 0; k < G.kt / 16; ++k) {   // two 8-row groups per MMA
                 const uint64_t ad = umma_sdesc_mn(st + k * 16 * ra, ra, G.a_box);
                 const uint64_t bd = umma_sdesc_mn(st + G.a_bytes + k * 16 * rb, rb, G.b_box);
                 const uint32_t acc = (it > 0 || k > 0) ? 1u : 0u;
@@ -1127,6 +1127,8 @@ __global__ void __launch_bounds__(128) k_conv3d_wgrad_tma(const __grid_constant_
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(G.cols));
 }
 
+bool tma_wgrad_tiles(const Vol& V, int cin, TmaWgrad& G);
+
 // The plan, or false when the shapes are outside the TMA form (Cout not 16,
 // 32, 64 or a multiple of 128).
 bool tma_wgrad_plan(const Vol& V, int cin, int cout, TmaWgrad& G) {
@@ -1146,10 +1148,19 @@ bool tma_wgrad_plan(const Vol& V, int cin, int cout, TmaWgrad& G) {
     }
     G.wsb = cin % 64 == 0 ? 64 : cin % 32 == 0 ? 32 : 16;
     G.n_tiles = (cin + 255) / 256;
+    for (int kt : {cin >= 96 && cout <= 64 ? 256 : 128, 128}) {
+        G.kt = kt;
+        if (tma_wgrad_tiles(V, cin, G)) return true;
+    }
+    return false;
+}
+
+// The K tiling and stages of plan G for its kt; false when they do not fit.
+bool tma_wgrad_tiles(const Vol& V, int cin, TmaWgrad& G) {
     const int nmax = cin < 256 ? cin : 256;
     G.wt = 1;
-    while (G.wt < V.w && G.wt < WG_K) G.wt <<= 1;
-    G.ht = WG_K / G.wt;
+    while (G.wt < V.w && G.wt < G.kt) G.wt <<= 1;
+    G.ht = G.kt / G.wt;
     G.tiles_x = (V.w + G.wt - 1) / G.wt;
     G.tiles_y = (V.h + G.ht - 1) / G.ht;
     G.ktiles = G.tiles_x * G.tiles_y * V.d * V.n;
@@ -1163,17 +1174,17 @@ bool tma_wgrad_plan(const Vol& V, int cin, int cout, TmaWgrad& G) {
     G.parts = (G.ktiles + G.per_part - 1) / G.per_part;
     G.cols = 32;
     while (G.cols < nmax) G.cols <<= 1;
-    G.a_box = (uint32_t)WG_K * G.wsa * 2;
-    G.b_box = (uint32_t)WG_K * G.wsb * 2;
-    G.a_bytes = (uint32_t)TC_M * WG_K * 2;
-    G.b_bytes = (uint32_t)nmax * WG_K * 2;
+    G.a_box = (uint32_t)G.kt * G.wsa * 2;
+    G.b_box = (uint32_t)G.kt * G.wsb * 2;
+    G.a_bytes = (uint32_t)TC_M * G.kt * 2;
+    G.b_bytes = (uint32_t)nmax * G.kt * 2;
     G.stage_bytes = (G.a_bytes + G.b_bytes + 1023u) & ~1023u;
     G.stages = (int)((72u * 1024u) / G.stage_bytes);
     if (G.stages < 2) G.stages = 2;
     if (G.stages > 8) G.stages = 8;
     G.smem = (size_t)G.stages * G.stage_bytes + (2 * G.stages + 1) * 8 + 16 + 1024;
     if (G.smem < (size_t)G.cols * 400) G.smem = (size_t)G.cols * 400;
-    return true;
+    return G.smem <= 227u * 1024u;
 }
 
 int launch_fwd_tma(const void* x, const void* w, const float* bias, int act, void* y, int n, int d, int h, int w_,
