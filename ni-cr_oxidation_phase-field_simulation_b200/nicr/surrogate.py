@@ -564,7 +564,8 @@ class JumpStepper:
         import torch
         for i, f in enumerate(("o", "cr", "p")):
             self.s.device_view(f, writable=True).copy_(x[..., i])
-        torch.cuda.current_stream().synchronize()
+        if x.is_cuda:   # the next library call runs on the solver's stream
+            torch.cuda.current_stream(x.device).synchronize()
 
     def _totals(self, x):
         """FP64 totals of O and Cr (of x, or of the solver's current state)."""
