@@ -214,3 +214,28 @@ def test_stepper_with_graph_proposals_matches_eager(trained):
     assert c0 == c1 and g0 == g1
     for a, b in zip(f0, f1):
         assert np.array_equal(a.view(np.int64), b.view(np.int64))
+
+
+def test_device_view_2d(require_gpu):
+    """2D handles: the view is (nx, ny), equal to get(), and a write is what
+    the next step sees."""
+    import torch
+    cfg = nicr.make_config(2, nx=48, ny=40, grains=0, nucleation="center", radius_grid=4.0, bc="concentration",
+                           ck="legacy", bounds="legacy")
+    a, b = nicr.Solver(cfg), nicr.Solver(cfg)
+    a.run(3)
+    b.run(3)
+    for f in ("o", "cr", "p"):
+        v = a.device_view(f)
+        assert tuple(v.shape) == a.get(f).shape and np.array_equal(v.cpu().numpy(), a.get(f))
+    cr = a.get("cr")
+    cr[10:20, 5:15] += 1e-3
+    a.device_view("cr", writable=True).copy_(torch.from_numpy(cr).cuda())
+    torch.cuda.synchronize()
+    b.set("cr", cr)
+    a.step(5)
+    b.step(5)
+    for f in ("o", "cr", "p"):
+        assert np.array_equal(a.get(f).view(np.int64), b.get(f).view(np.int64)), f
+    a.close()
+    b.close()
