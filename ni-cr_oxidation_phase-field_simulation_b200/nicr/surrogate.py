@@ -220,7 +220,7 @@ def _module_classes():
         def __init__(self, fields: int = 4, base: int = 32):
             super().__init__()
             c1, c2, c3 = base, 2 * base, 4 * base
-            self.fields = fields
+            self.fields, self.base = fields, base
             self.enc1 = nn.Sequential(Conv(PAD, c1), Conv(c1, c1))
             self.enc2 = nn.Sequential(Conv(c1, c2), Conv(c2, c2))
             self.mid = nn.Sequential(Conv(c2, c3), Conv(c3, c3))
@@ -244,6 +244,35 @@ def _module_classes():
 
 def unet(fields: int = 4, base: int = 32):
     return _module_classes()[1](fields, base)
+
+
+_NORM_KEYS = ("mu", "sd", "rsd", "csd", "dsd")
+
+
+def save_model(path, model, norm, **meta):
+    """A trained surrogate in one file: the U-Net's shape and weights, the
+    normaliser (K in steps and the per-field scales) and caller metadata
+    (e.g. the training configurations), for JumpStepper runs in other
+    processes."""
+    import torch
+    torch.save({"fields": model.fields, "base": model.base,
+                "weights": {k: v.detach().cpu() for k, v in model.state_dict().items()},
+                "steps_k": norm.steps_k, "norm": {k: getattr(norm, k).detach().cpu() for k in _NORM_KEYS},
+                "meta": meta}, str(path))
+
+
+def load_model(path, device="cuda"):
+    """(model, normaliser, metadata) from save_model, on `device`."""
+    import torch
+    d = torch.load(str(path), map_location="cpu", weights_only=True)
+    model = unet(d["fields"], d["base"])
+    model.load_state_dict(d["weights"])
+    model.to(device)
+    norm = Normaliser.__new__(Normaliser)
+    for k in _NORM_KEYS:
+        setattr(norm, k, d["norm"][k].to(device))
+    norm.steps_k = int(d["steps_k"])
+    return model, norm, d["meta"]
 
 
 # ------------------------------------------------------------------ data

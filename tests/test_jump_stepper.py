@@ -126,3 +126,21 @@ def test_expected_change_models():
     assert st._expected_change([0.0, 1.0, 1.5]) == pytest.approx(7.5)
     with pytest.raises(ValueError):
         surrogate.JumpStepper(a, None, None, 10, budget="cubic")
+
+
+def test_save_and_load_model(tmp_path):
+    """save_model / load_model: the U-Net's shape and weights, the normaliser
+    and the metadata round-trip exactly (on the CPU)."""
+    torch.manual_seed(1)
+    net = surrogate.unet(4, 16)
+    x = torch.randn((1, 4, 8, 8, 8, 4))
+    norm = surrogate.Normaliser(x, torch.randn_like(x) * 0.1, 2, 16)
+    surrogate.save_model(tmp_path / "s.pt", net, norm, seeds=[100, 101])
+    net2, norm2, meta = surrogate.load_model(tmp_path / "s.pt", device="cpu")
+    assert meta == {"seeds": [100, 101]} and net2.base == 16 and net2.fields == 4 and norm2.steps_k == 16
+    for (k, a), (k2, b) in zip(net.state_dict().items(), net2.state_dict().items()):
+        assert k == k2 and torch.equal(a, b)
+    for k in ("mu", "sd", "rsd", "csd", "dsd"):
+        assert torch.equal(getattr(norm, k), getattr(norm2, k))
+    xi, ri = x[0, :1], x[0, :1] * 0.1
+    assert torch.equal(norm.inputs(xi, ri), norm2.inputs(xi, ri))
