@@ -239,3 +239,14 @@ def test_device_view_2d(require_gpu):
         assert np.array_equal(a.get(f).view(np.int64), b.get(f).view(np.int64)), f
     a.close()
     b.close()
+
+
+def test_reloaded_model_predicts_alike(trained, tmp_path):
+    """A trained surrogate saved and loaded on the GPU proposes the same
+    states bit for bit."""
+    import torch
+    net, norm, _, (x, r), _ = trained
+    surrogate.save_model(tmp_path / "s.pt", net, norm)
+    net2, norm2, _ = surrogate.load_model(tmp_path / "s.pt", device="cuda")
+    x0, r0 = x[4:, 5].contiguous(), r[4:, 5].contiguous()
+    assert torch.equal(surrogate.predict(net, norm, x0, r0), surrogate.predict(net2, norm2, x0, r0))
