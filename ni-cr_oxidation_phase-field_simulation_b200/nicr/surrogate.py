@@ -303,6 +303,8 @@ def trajectories(cfgs, steps: int, every: int, probe: int = 2, device: int = 0):
     GPU (read in place through Solver.device_view)."""
     import torch
     from . import Solver
+    if every <= probe or probe < 1 or steps < every:
+        raise ValueError(f"need 1 <= probe < every <= steps (probe {probe}, every {every}, steps {steps})")
     xs, rs = [], []
     for c in cfgs:
         c.device = device
@@ -395,6 +397,8 @@ def train(model, x, r, k: int, steps_k: int, iters: int = 200, batch: int = 2, l
     (allreduce_gradients), after rank 0's initial weights were broadcast; all
     ranks then hold the same weights. The losses are each rank's own."""
     import torch
+    if not 1 <= k < x.shape[1] or tuple(r.shape) != tuple(x.shape):
+        raise ValueError(f"need 1 <= k < samples per run ({x.shape[1]}) and rates shaped like the states")
     torch.manual_seed(seed)
     rank = 0
     if group is not None:
@@ -520,6 +524,8 @@ class JumpStepper:
                  recheck_factor: float = 4.0, backoff: bool = False, graphs: bool = False,
                  budget: str = "linear"):
         from . import NUCLEATION
+        if k < 1 or probe < 2:
+            raise ValueError("need K >= 1 and at least 2 probe steps")
         if norm is not None and norm.steps_k != k:
             raise ValueError(f"the network predicts {norm.steps_k} steps ahead, not {k}")
         if model is not None and solver.cfg.grain_evolution:

@@ -144,3 +144,19 @@ def test_save_and_load_model(tmp_path):
         assert torch.equal(getattr(norm, k), getattr(norm2, k))
     xi, ri = x[0, :1], x[0, :1] * 0.1
     assert torch.equal(norm.inputs(xi, ri), norm2.inputs(xi, ri))
+
+
+def test_argument_checks():
+    x = torch.zeros((1, 3, 4, 4, 4, 4))
+    net = surrogate.unet(4, 16)
+    with pytest.raises(ValueError):
+        surrogate.train(net, x, x, 3, 16)          # k must leave pairs
+    with pytest.raises(ValueError):
+        surrogate.train(net, x, x[:, :2], 1, 16)   # rates shaped like the states
+    with pytest.raises(ValueError):
+        surrogate.trajectories([], 64, 2, probe=2)
+    a = FakeSolver()
+    with pytest.raises(ValueError):
+        surrogate.JumpStepper(a, None, None, 8, probe=1)
+    with pytest.raises(ValueError):
+        surrogate.JumpStepper(a, zero_model, norm_for(a, 8), 16)   # K of the network
