@@ -232,26 +232,38 @@ int nicr_format_log_row(nicr_handle* h, int n, char* buf, size_t len);
 int nicr_format_grain_rows(nicr_handle* h, int n, char* diag, size_t diag_len,
                            char* history, size_t history_len);
 
-/* One FP64 step of c_O, c_Cr and phi on caller-owned device memory, for
- * callers that must not allocate device memory (a coupling code that owns all
- * of HBM through its own pool, or code running where the CUDA memory API may
- * not be called). No counterpart in the reference, which has no GPU.
+/* One step of c_O, c_Cr and phi on caller-owned device memory, for callers
+ * that must not allocate device memory (a coupling code that owns all of HBM
+ * through its own pool, or code running where the CUDA memory API may not be
+ * called). No counterpart in the reference, which has no GPU.
+ *
+ * The arithmetic form is cfg->precision: NICR_FP64 (the drop-in form,
+ * bit-identical to the reference) or NICR_FP64_FAST (the reciprocal form);
+ * any other value returns NICR_ERR_INVALID_ARG, as nicr_create does.
  *
  * It allocates nothing: o, cr, p (inputs) and o_next, cr_next, p_next
  * (outputs) are packed device arrays in interior order (X slowest, column
  * pitch nz in 3D and ny in 2D); gb is the grain-boundary mask when grains are
  * on, eta_s2 the sum of eta^2 when eta evolves. The step's scratch lives in a
  * file-scope device array of the library (about 768 KB per GPU, held until
- * exit) that serves step grids of up to 8192 CTAs (every 3D grid with
- * ny*nz <= 2^21 cells per X plane); larger grids return NICR_ERR_INVALID_ARG
- * before touching the device. The first call on a device resolves the array's
- * device address, so make it before any stream capture. Every call shares the
- * array and clears its status word first; calls that overlap on the GPU race
- * on it. The kernels are enqueued on `stream` (a cudaStream_t, NULL for the
- * legacy default stream) and write *result (device memory) asynchronously:
- * trial_key == ~0 when every trial was accepted; otherwise the trial buffers
- * hold a rejected step (key/4 = first failing cell in reference order, key%4:
- * 0 nonfinite, 1 out of bounds) and must not be swapped in. */
+ * exit) that holds the partial sums of at most 8192 CTAs of the step kernel.
+ * The call lengthens the X chunk (planes per CTA) until the grid fits, so it
+ * serves every grid with at most 8192 step tiles per X plane (3D:
+ * ceil(ny/8)*ceil(nz/32) <= 8192; 2D: ceil(ny/128) <= 8192); larger grids
+ * return NICR_ERR_INVALID_ARG before touching the device. The fields do not
+ * depend on the chunk; the budget increments may differ from the handle
+ * API's in the last bits (~1e-16 relative). The first call on a device
+ * resolves the array's device address, so make it before any stream capture.
+ * Every call shares the array and clears its status word first; calls that
+ * overlap on the GPU race on it. If a CUDA error is already pending on the
+ * calling thread, the call enqueues nothing, leaves that error in place and
+ * returns NICR_ERR_CUDA; otherwise it reads and clears only the launch errors
+ * of its own kernels. The kernels are enqueued on `stream` (a cudaStream_t,
+ * NULL for the legacy default stream) and write *result (device memory)
+ * asynchronously: trial_key == ~0 when every trial was accepted; otherwise
+ * the trial buffers hold a rejected step (key/4 = first failing cell in
+ * reference order, key%4: 0 nonfinite, 1 out of bounds) and must not be
+ * swapped in. */
 typedef struct nicr_step_result {
     double ckO[2], ckCr[2], clipO[2], clipCr[2], bcO[2];  /* budget increments (hi, lo) */
     long long clipped;                                     /* cells clipped this step     */

@@ -1,5 +1,7 @@
-// nicr_step_noalloc: one FP64 step of c_O, c_Cr and phi on caller-owned
-// device arrays, for callers that must not allocate device memory.
+// nicr_step_noalloc: one step of c_O, c_Cr and phi on caller-owned device
+// arrays, in the FP64 form the configuration selects (the bit-identical
+// drop-in form or the reciprocal form), for callers that must not allocate
+// device memory.
 //
 // Who needs it: codes that embed the step inside their own time loop and own
 // every byte of device memory through their own pool (a coupled multiphysics
@@ -17,6 +19,7 @@
 // race on the array and must be serialised by the caller.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <mutex>
 
 #include "../../include/nicr.h"
@@ -25,9 +28,11 @@
 
 namespace {
 
-// Largest step grid the scratch array serves: 8192 CTAs of the step kernel
-// (3D tiles of 8 rows x 32 columns over >= 16 X planes, 2D tiles of 128
-// columns), e.g. every 3D grid with ny*nz <= 2^21 cells per X plane.
+// Largest step grid the scratch array serves: 8192 CTAs of the step kernel.
+// params_for lengthens the X chunk (planes per CTA) until the grid fits, so
+// every grid with at most 8192 step tiles per X plane is served (3D tiles of
+// 8 rows x 32 columns: ceil(ny/8)*ceil(nz/32) <= 8192; 2D tiles of 128
+// columns: ceil(ny/128) <= 8192).
 constexpr int kMaxCtas = 8192;
 struct Scratch {
     nicr::Status status;
@@ -141,6 +146,9 @@ nicr::StepParams params_for(const nicr_config& c) {
     sp.fast = c.precision == NICR_FP64_FAST ? 1 : 0;
     sp.xchunk = choose_xchunk(g);
     whole_domain_range(sp);
+    // Longer X chunks mean fewer CTAs; the fields do not depend on the chunk
+    // (budget partial sums group differently, ~1e-16 relative).
+    while (step_main_blocks(sp) > kMaxCtas && sp.xchunk < g.nx) sp.xchunk = std::min(g.nx, 2 * sp.xchunk);
     return sp;
 }
 
@@ -151,12 +159,18 @@ extern "C" int nicr_step_noalloc(const nicr_config* cfg, const double* o, const 
                                  double* p_next, nicr_step_result* result, void* stream) {
     if (!cfg || (cfg->dim != 2 && cfg->dim != 3) || cfg->nx < 3 || cfg->ny < 3 || (cfg->dim == 3 && cfg->nz < 3))
         return NICR_ERR_INVALID_ARG;
+    // the same arithmetic forms as nicr_create accepts
+    if (cfg->precision != NICR_FP64 && cfg->precision != NICR_FP64_FAST) return NICR_ERR_INVALID_ARG;
     const nicr::StepParams sp = params_for(*cfg);
     // reject sizes beyond the scratch array before touching the device
     if (nicr::step_main_blocks(sp) > kMaxCtas) return NICR_ERR_INVALID_ARG;
     if (!o || !cr || !p || !o_next || !cr_next || !p_next || !result) return NICR_ERR_INVALID_ARG;
     if (cfg->grains && !gb) return NICR_ERR_INVALID_ARG;
     if (cfg->grain_evolution && cfg->grains && !eta_s2) return NICR_ERR_INVALID_ARG;
+    // An error already pending on this thread belongs to the caller's earlier
+    // work: leave it in place for the caller and enqueue nothing. Past this
+    // point every launch error read (and cleared) below is this call's own.
+    if (cudaPeekAtLastError() != cudaSuccess) return NICR_ERR_CUDA;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return NICR_ERR_NO_DEVICE;
     Scratch* s = nullptr;

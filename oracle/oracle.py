@@ -30,8 +30,11 @@ REF_DIR = HERE / "_ref"
 
 
 def build(quiet: bool = True) -> None:
-    """Builds the oracle library (and oracle/_ref when the reference is present)."""
-    out = subprocess.run(["make", "-C", str(HERE), "all"], capture_output=True, text=True)
+    """Builds the oracle library (and oracle/_ref when NICR_REF_DIR names the
+    reference sources)."""
+    import os
+    out = subprocess.run(["make", "-C", str(HERE), "all", f"REF={os.environ.get('NICR_REF_DIR', '')}"],
+                         capture_output=True, text=True)
     if out.returncode != 0:
         raise RuntimeError("oracle build failed:\n" + out.stdout + out.stderr)
     if not quiet:

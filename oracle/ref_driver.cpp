@@ -93,7 +93,21 @@ static std::vector<double> interior(const Model& m, const Field& a) {
     return v;
 }
 
+static void dump_model(Model& m, const std::string& path);
+
+// Over several ranks (the thread-per-rank build) the state is first gathered
+// into the root's snapshot model, as the reference's own output does
+// (gather_state); the budget is then the ranks' reduced budget.
 static void dump(Model& m, const std::string& path) {
+    if (m.domain.size > 1) {
+        m.gather_state();
+        if (m.domain.rank == 0) dump_model(*m.snapshot, path);
+        return;
+    }
+    dump_model(m, path);
+}
+
+static void dump_model(Model& m, const std::string& path) {
     m.refresh();
     Writer w(path);
     w.f64("o", interior(m, m.o));

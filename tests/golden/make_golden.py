@@ -18,6 +18,16 @@ built (`make -C oracle`). It writes:
   hashes of the last frame's arrays cast to Float32/Float64 for the VTI payload).
 * verify_mpi_2d.json: the five cases of mpi2d/tests/verify_mpi.py:57-75 with the
   SHA-256 of every VTK frame (output every 250 steps) and the diagnostics rows.
+* long_runs.json: the specification's workloads run on the reference's run()
+  schedule (golden_cases.LONG_CASES): 128^3 with 32 static grains for 2000
+  steps (plain and supersaturated), and 256^3 with 8 evolving eta for one
+  nucleation period. Per case: SHA-256 of every field, the budget, nuclei and
+  clipped cells. The thread-per-rank reference build (oracle/_ref/*_threads)
+  runs them on all host cores; its fields equal the single-process build's.
+
+Usage: make_golden.py --ref <reference source dir> [--only NAME ...]
+(the reference sources are needed for the stored example; oracle/_ref must
+be built with `make -C oracle REF=<dir>`).
 
 Inputs are drawn from numpy's PCG64 (bit-reproducible), so tests regenerate
 them instead of storing them.
@@ -36,9 +46,8 @@ ROOT = HERE.parent.parent
 sys.path.insert(0, str(ROOT / "oracle"))
 sys.path.insert(0, str(ROOT / "tests"))
 from oracle import make_config, run_reference, REF_DIR  # noqa: E402
-from golden_cases import MODES, regression_cases, regression_inputs, regression_commands  # noqa: E402
-
-REFERENCE = Path("/root/reference")
+from golden_cases import (MODES, LONG_CASES, long_inputs, regression_cases, regression_inputs,  # noqa: E402
+                          regression_commands)
 
 
 def sha(a) -> str:
@@ -69,8 +78,8 @@ def file_sha(p: Path) -> str:
     return hashlib.sha256(p.read_bytes()).hexdigest()
 
 
-def example_center():
-    src = REFERENCE / "mpi2d" / "example_center"
+def example_center(reference: Path):
+    src = reference / "mpi2d" / "example_center"
     args = ["--nx", "61", "--ny", "61", "--grain-evolution", "on", "--eta-output", "all", "--seed", "2001",
             "--left-edge-sites", "2", "--nucleation", "center", "--radius-grid", "5.5", "--bc", "closed",
             "--ck", "off", "--bounds", "legacy", "--dt", "1e-12", "--steps", "500", "--output-every", "500"]
@@ -153,14 +162,63 @@ def cli_3d():
     return out
 
 
+def long_runs(names, threads):
+    import os
+    path = HERE / "long_runs.json"
+    out = json.loads(path.read_text()) if path.exists() else {}
+    for name in names:
+        case = LONG_CASES[name]
+        cfg = make_config(3, **case["config"])
+        d0 = run_reference(cfg, ["dump"], threads=threads, timeout=3600)["dumps"][0]
+        shape = (cfg.nx, cfg.ny, cfg.nz)
+        o, cr, p = long_inputs(case, d0["o"].reshape(shape), d0["cr"].reshape(shape), d0["p"].reshape(shape))
+        n_eta = int(d0["n_eta"][0])
+        inj = {"o": o, "cr": cr, "p": p, "eta": [d0[f"eta{g + 1}"].reshape(shape) for g in range(n_eta)]}
+        cmds = ["reset_inventory"]
+        if case["stamp"]:
+            cmds.append(["stamp"] + list(case["stamp"]))
+        cmds += [["time_run", case["steps"]], "dump"]
+        res = run_reference(cfg, cmds, inject=inj, threads=threads, timeout=4 * 3600)
+        if "REJECTED" in res["stdout"]:
+            raise RuntimeError(f"{name}: the reference rejected a step: {res['stdout']}")
+        d = res["dumps"][-1]
+        fields = {k: sha(d[k]) for k in ("o", "cr", "p", "muO", "muCr", "mo", "mc", "gb")}
+        for g in range(n_eta):
+            fields[f"eta{g + 1}"] = sha(d[f"eta{g + 1}"])
+        if n_eta:
+            fields["eta_s2"] = sha(d["eta_s2"])
+        names_b = ("nucO", "nucCr", "ckO", "ckCr", "clipO", "clipCr", "bcO", "bcCr")
+        out[name] = {"config": case["config"], "steps": case["steps"], "fields": fields,
+                     "budget": {n: [float(x) for x in d["budget"][q]] for q, n in enumerate(names_b)},
+                     "nuclei": int(d["counts"][0]), "clipped": int(d["counts"][1]),
+                     "reference_ranks": threads or 1, "stdout": res["stdout"].strip().splitlines()}
+        path.write_text(json.dumps(out, indent=1) + "\n")
+        print(name, "nuclei", out[name]["nuclei"], "clipped", out[name]["clipped"], res["stdout"].strip())
+
+
 def main():
+    import argparse
+    import os
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ref", type=Path, required=True, help="directory holding the reference sources")
+    ap.add_argument("--only", nargs="*", help="fixture groups: regression example verify cli or a LONG_CASES name")
+    ap.add_argument("--threads", type=int, default=os.cpu_count() or 1, help="reference ranks for the long runs")
+    a = ap.parse_args()
     if not (REF_DIR / "ref3d").exists():
-        raise SystemExit("oracle/_ref is not built (make -C oracle)")
-    (HERE / "regression_3d.json").write_text(json.dumps(regression(3), indent=1) + "\n")
-    (HERE / "regression_2d.json").write_text(json.dumps(regression(2), indent=1) + "\n")
-    (HERE / "example_center_2d.json").write_text(json.dumps(example_center(), indent=1) + "\n")
-    (HERE / "verify_mpi_2d.json").write_text(json.dumps(verify_mpi_2d(), indent=1) + "\n")
-    (HERE / "cli_3d.json").write_text(json.dumps(cli_3d(), indent=1) + "\n")
+        raise SystemExit("oracle/_ref is not built (make -C oracle REF=<dir>)")
+    want = set(a.only or ["regression", "example", "verify", "cli"] + list(LONG_CASES))
+    if "regression" in want:
+        (HERE / "regression_3d.json").write_text(json.dumps(regression(3), indent=1) + "\n")
+        (HERE / "regression_2d.json").write_text(json.dumps(regression(2), indent=1) + "\n")
+    if "example" in want:
+        (HERE / "example_center_2d.json").write_text(json.dumps(example_center(a.ref), indent=1) + "\n")
+    if "verify" in want:
+        (HERE / "verify_mpi_2d.json").write_text(json.dumps(verify_mpi_2d(), indent=1) + "\n")
+    if "cli" in want:
+        (HERE / "cli_3d.json").write_text(json.dumps(cli_3d(), indent=1) + "\n")
+    long_names = [n for n in LONG_CASES if n in want]
+    if long_names:
+        long_runs(long_names, a.threads if a.threads > 1 else 0)
     print("golden fixtures written to", HERE)
 
 

@@ -109,3 +109,37 @@ def test_colour_grains_is_dsatur(ng, density, k):
     assert out.tolist() == _dsatur(adj.tolist(), k)
     if k >= ng:
         assert not any(adj[a, b] and out[a] == out[b] for a in range(ng) for b in range(ng))
+
+
+def _noalloc():
+    f = nicr.lib().nicr_step_noalloc
+    f.argtypes = [ctypes.POINTER(nicr.NicrConfig)] + [ctypes.c_void_p] * 10
+    f.restype = ctypes.c_int
+    return f
+
+
+def _no_gpu():
+    from conftest import gpu_available
+    return not gpu_available()
+
+
+@pytest.mark.skipif(not _no_gpu(), reason="passes placeholder pointers; runs only where no GPU can be reached")
+@pytest.mark.parametrize("precision", [2, -1, 7])
+def test_noalloc_rejects_unknown_precision_before_the_device(precision):
+    """nicr_step_noalloc accepts the forms nicr_create accepts (NICR_FP64 and
+    NICR_FP64_FAST) and rejects others before any CUDA call. Non-null
+    placeholder pointers get the call past its null checks: without the
+    precision check it would reach the (absent) device and return
+    NICR_ERR_NO_DEVICE or NICR_ERR_CUDA instead."""
+    cfg = nicr.make_config(3, nx=16, ny=16, nz=32, grains=0, nucleation="off", precision=precision)
+    ptrs = [ctypes.c_void_p(256 * (k + 1)) for k in range(10)]
+    assert _noalloc()(ctypes.byref(cfg), *ptrs) == _abi.ERR_INVALID_ARG
+    cfg.precision = 1
+    assert _noalloc()(ctypes.byref(cfg), *ptrs) in (_abi.ERR_NO_DEVICE, _abi.ERR_CUDA)
+
+
+def test_noalloc_rejects_too_many_tiles_before_the_device():
+    """More than 8192 step tiles per X plane (3D: ceil(ny/8)*ceil(nz/32)) do
+    not fit the scratch array at any X chunk: rejected before any CUDA call."""
+    cfg = nicr.make_config(3, nx=4, ny=8 * 129, nz=32 * 64, grains=0, nucleation="off")
+    assert _noalloc()(ctypes.byref(cfg), *([None] * 10)) == _abi.ERR_INVALID_ARG

@@ -3,7 +3,11 @@ cudaMalloc (they own all device memory, or run where the CUDA memory API may
 not be used). The test allocates the caller-side arrays itself (as such a
 caller would, from its own pool) and checks two calls in a row against the
 handle API's nicr_step: fields bit-identical, budget increments within the
-suite's budget tolerance (1e-13 relative). Collected last on purpose."""
+suite's budget tolerance (1e-13 relative). Covered: the drop-in and the
+reciprocal form, no grains, static grains and evolving eta (the caller passes
+gb and eta_s2 of the current eta), and a grid with long X and small planes
+whose default X chunk would exceed the scratch array (the call lengthens the
+chunk). Collected last on purpose."""
 import ctypes
 
 import numpy as np
@@ -28,31 +32,49 @@ def entry():
     return f
 
 
-@pytest.mark.parametrize("dim,mode,bc", [(3, "static", "mu"), (3, "single", "concentration"), (2, "static", "concentration")])
-def test_noalloc_matches_handle_step_twice(require_gpu, dim, mode, bc):
+CASES = [
+    # dim, grain mode, bc, precision, shape
+    (3, "static", "mu", 0, (37, 21, 45)),
+    (3, "single", "concentration", 0, (37, 21, 45)),
+    (2, "static", "concentration", 0, (53, 70)),
+    (3, "evolving", "mu", 0, (29, 24, 33)),
+    (3, "evolving", "concentration", 1, (29, 24, 33)),
+    (3, "static", "mu", 1, (37, 21, 45)),
+    (2, "evolving", "mu", 1, (53, 70)),
+    # 120 x 320 planes are 150 step tiles; the default chunk of 16 planes gives
+    # 8250 CTAs, more than the scratch array holds
+    (3, "static", "concentration", 0, (872, 120, 320)),
+]
+
+
+@pytest.mark.parametrize("dim,mode,bc,precision,shape", CASES)
+def test_noalloc_matches_handle_step_twice(require_gpu, dim, mode, bc, precision, shape):
     import torch
-    shape = (37, 21, 45) if dim == 3 else (53, 70)
-    kw = dict(nx=shape[0], ny=shape[1], grains=1 if mode == "static" else 0, grain_diameter_grid=12.,
-              bc=bc, ck="legacy", bounds="legacy", nucleation="off", dt=1e-12)
+    kw = dict(nx=shape[0], ny=shape[1], grains=0 if mode == "single" else 1, grain_diameter_grid=12.,
+              grain_evolution=1 if mode == "evolving" else 0, bc=bc, ck="legacy", bounds="legacy",
+              nucleation="off", dt=1e-12, precision=precision)
     if dim == 3:
         kw["nz"] = shape[2]
     cfg = nicr.make_config(dim, **kw)
     sol = nicr.Solver(cfg)
-    o, cr, p, _ = smooth_fields(shape, 0, seed=5)
+    neta = sol.neta if mode == "evolving" else 0
+    o, cr, p, eta = smooth_fields(shape, neta, seed=5)
     p = 0.02 * (1 + np.cos(np.indices(shape).sum(axis=0) * 0.3))   # some interface cells
-    sol.set_fields(o, cr, p)
+    sol.set_fields(o, cr, p, eta if neta else None)
     dev = torch.device("cuda", 0)
-    cur = [torch.from_numpy(np.ascontiguousarray(sol.get(f))).to(dev) for f in ("o", "cr", "p")]
-    gb = torch.from_numpy(np.ascontiguousarray(sol.get("gb"))).to(dev)
-    nxt = [torch.empty_like(t) for t in cur]
-    res = torch.zeros(ctypes.sizeof(StepResult), dtype=torch.uint8, device=dev)
     f = entry()
+    res = torch.zeros(ctypes.sizeof(StepResult), dtype=torch.uint8, device=dev)
     b0 = sol.budget()
     totals = {n: 0.0 for n in ("ckO", "ckCr", "clipO", "clipCr", "bcO")}
     clipped = 0
+    cur = [torch.from_numpy(np.ascontiguousarray(sol.get(n))).to(dev) for n in ("o", "cr", "p")]
+    nxt = [torch.empty_like(t) for t in cur]
     for call in range(2):
+        # the caller's mask inputs of this step: gb, and eta_s2 when eta evolves
+        gb = torch.from_numpy(np.ascontiguousarray(sol.get("gb"))).to(dev)
+        s2 = torch.from_numpy(np.ascontiguousarray(sol.get("eta_s2"))).to(dev) if neta else None
         torch.cuda.synchronize()
-        rc = f(ctypes.byref(cfg), *(t.data_ptr() for t in cur), gb.data_ptr(), None,
+        rc = f(ctypes.byref(cfg), *(t.data_ptr() for t in cur), gb.data_ptr(), s2.data_ptr() if neta else None,
                *(t.data_ptr() for t in nxt), res.data_ptr(), None)
         assert rc == 0
         torch.cuda.synchronize()
@@ -74,6 +96,6 @@ def test_noalloc_matches_handle_step_twice(require_gpu, dim, mode, bc):
 
 
 def test_noalloc_rejects_grids_beyond_its_scratch(require_gpu):
-    cfg = nicr.make_config(3, nx=64, ny=4096, nz=4096, grains=0, nucleation="off")
+    cfg = nicr.make_config(3, nx=64, ny=4096, nz=4096 * 64, grains=0, nucleation="off")
     rc = entry()(ctypes.byref(cfg), *([None] * 10))
     assert rc == nicr._abi.ERR_INVALID_ARG
