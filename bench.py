@@ -41,7 +41,8 @@ sys.path.insert(0, str(PKG))
 
 METRIC = "Mcell-updates/s at 256^3 vs plain FP64 GPU path at ≤1e-4 L∞ err; % HBM peak"
 UNIT = "Mcell-updates/s"
-KERNELS = ["step_main", "eta_update", "step_finalize", "eta_mask", "ksp_scan", "refresh", "diagnostics", "step_eta"]
+KERNELS = ["step_main", "eta_update", "step_finalize", "eta_mask", "ksp_scan", "refresh", "diagnostics", "step_eta",
+           "step_fused"]
 
 
 def grain_diameter_for(n_grains: int, shape) -> float:
@@ -79,6 +80,8 @@ def algorithmic_bytes(kernel: str, neta: int, fast: bool) -> int:
         return (neta + 2) * 8
     if kernel == "step_eta":       # the two in one launch (reciprocal form)
         return algorithmic_bytes("step_main", neta, fast) + algorithmic_bytes("eta_update", neta, fast)
+    if kernel == "step_fused":     # one pass: r/w o cr p eta_1..N (S and gb rebuilt on chip)
+        return (6 + 2 * neta) * 8
     return 0
 
 

@@ -493,7 +493,8 @@ void* nicr_stream(nicr_handle* h);
  * nicr_profile_read returns the accumulated device time and launch count of
  * one kernel (0 step_main, 1 eta_update, 2 step_finalize, 3 eta_mask,
  * 4 ksp_scan, 5 refresh, 6 diagnostics, 7 step_eta: the step kernel and the
- * eta update in one launch, reciprocal form). nicr_kernel_launches counts every
+ * eta update in one launch, reciprocal form; 8 step_fused: the one-pass step
+ * of 3D grids with evolving eta). nicr_kernel_launches counts every
  * kernel the handle has launched since creation. */
 int nicr_profile(nicr_handle* h, int enable);
 int nicr_profile_read(nicr_handle* h, int kernel, double* total_ms, long long* launches);

@@ -103,6 +103,8 @@ int step_main_blocks(const StepParams& P);
 // Planes per CTA along X for grid g (step and eta kernels), and one chunk for
 // the n domains of a batch. NICR_XCHUNK forces a chunk for tuning runs.
 int choose_xchunk(const Grid& g);
+// The same choice for the one-pass step (16 x 32 tiles, one CTA per SM).
+int choose_xchunk_fused(const Grid& g);
 int choose_xchunk_batch(const Grid* grids, int n);
 // The chunks the choosers consider for a largest X extent nxmax: nxmax halved
 // repeatedly and the powers of two below it, longest first.
@@ -157,6 +159,25 @@ bool launch_step_eta_fast(const StepParams& P, int neta, const double* o, const 
                           StepPartial* partials, const double* eta, double* eta_next, double* gb_next,
                           double* s2_next, unsigned* ticket, Status* st, cudaStream_t stream, int* nblocks_out);
 void step_eta_prepare_fast(const StepParams& P, int neta);
+
+// One HBM pass per step (3D, evolving eta): the step kernel and the eta
+// update fused into one X march with the eta planes staged by TMA and S / gb
+// rebuilt on chip (k_step_fused, nicr_step_fused.cuh). It reads o, cr, p and
+// the n eta fields and writes the trial o, cr, p and eta; gb and eta_s2 are
+// neither read nor written. Applies to 1 <= n <= 8 fields, rows a multiple of
+// 16 and columns a multiple of 32 (step_fused_applies); the launchers return
+// false and launch nothing otherwise. The drop-in form is bit-identical to
+// the two-kernel form.
+bool step_fused_applies(const Grid& g, int neta);
+bool launch_step_fused(const StepParams& P, int neta, const double* o, const double* cr, const double* p,
+                       const double* eta, double* on, double* crn, double* pn, double* eta_next,
+                       StepPartial* partials, Status* st, cudaStream_t stream, int* nblocks_out);
+bool launch_step_fused_fast(const StepParams& P, int neta, const double* o, const double* cr, const double* p,
+                            const double* eta, double* on, double* crn, double* pn, double* eta_next,
+                            StepPartial* partials, Status* st, cudaStream_t stream, int* nblocks_out);
+// kernel attributes of the fused step, set outside any stream capture
+void step_fused_prepare(const StepParams& P, int neta);
+void step_fused_prepare_fast(const StepParams& P, int neta);
 
 struct FinalizeDomain {
     const StepPartial* partials;

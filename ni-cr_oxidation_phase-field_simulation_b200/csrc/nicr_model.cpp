@@ -184,6 +184,8 @@ Model::Model(const nicr_config& cfg, const SlabSpec* slab) : c(cfg), dim(cfg.dim
         }
         if (c.nucleation == NICR_NUC_KSP) setup_ksp();
         if (has_eta) eta_mask_now();
+        // the one-pass step runs one 16 x 32 tile per SM: its own chunk choice
+        if (onepass_step()) set_xchunk(choose_xchunk_fused(g));
         check_cuda(cudaStreamSynchronize(stream), "init");
         check_cuda(cudaGetLastError(), "init kernels");
     } catch (...) {
@@ -800,15 +802,16 @@ void Model::launch_trial_eta() {
 }
 
 void Model::launch_trial_kernels() {
-    const BatchDomain d = step_desc();
     int nb = 0;
+    if (onepass_step() && launch_onepass(&nb)) return;
+    const BatchDomain d = step_desc();
     launch_step_main(sp, d.o, d.cr, d.p, d.gb, d.s2, d.on, d.crn, d.pn, partials, st, stream, &nb);
     launch_trial_eta();
 }
 
 void Model::tune(int reps, int* xchunk, int* minb) {
     reps = std::max(1, reps);
-    prepare_step();
+    if (!onepass_step()) prepare_step();
     reset_status();   // trial kernels of a failing state must not stop the timing runs
     cudaEvent_t e0, e1;
     check_cuda(cudaEventCreate(&e0), "cudaEventCreate");
@@ -821,6 +824,7 @@ void Model::tune(int reps, int* xchunk, int* minb) {
         for (int mb : minbs) {
             sp.minb = mb;
             step_kernels_prepare(sp);
+            if (onepass_step()) step_fused_prepare(sp, neta);
             launch_trial_kernels();   // warm-up
             check_cuda(cudaEventRecord(e0, stream), "cudaEventRecord");
             for (int r = 0; r < reps; ++r) launch_trial_kernels();
@@ -892,10 +896,43 @@ bool Model::fused_step() const {
     return v == 1 && sp.fast && dim == 3 && advance_eta && !is_slab && neta >= 1 && neta <= 16;
 }
 
+bool Model::onepass_step() const {
+    static int v = -1;
+    if (v < 0) {
+        const char* e = getenv("NICR_STEP_FORM");
+        v = (e && e[0] == 's') ? 0 : 1;
+    }
+    return v == 1 && !onepass_failed && dim == 3 && advance_eta && !is_slab && !fused_step() &&
+           step_fused_applies(g, neta);
+}
+
+bool Model::launch_onepass(int* nb) {
+    const size_t e = prof_begin();
+    if (!launch_step_fused(sp, neta, o_[cur], cr_[cur], p_[cur], eta_[ecur], o_[cur ^ 1], cr_[cur ^ 1], p_[cur ^ 1],
+                           eta_[ecur ^ 1], partials, st, stream, nb)) {
+        onepass_failed = true;
+        return false;
+    }
+    prof_end(K_STEP_FUSED, e, 1);
+    return true;
+}
+
 void Model::enqueue_step() {
+    int nb = 0;
+    if (onepass_step()) {
+        if (launch_onepass(&nb)) {
+            const size_t e = prof_begin();
+            launch_step_finalize(partials, nb, bud, st, 0, stream);
+            prof_end(K_FINALIZE, e, 1);
+            cur ^= 1;
+            ecur ^= 1;
+            gcur ^= 1;
+            eta_dirty = true;   // gb and eta_s2 were not written: rebuilt from eta when read
+            return;
+        }
+    }
     prepare_step();
     const BatchDomain d = step_desc();
-    int nb = 0;
     if (fused_step()) {
         if (!ticket) ticket = dalloc_t<unsigned>(1);
         size_t e = prof_begin();
@@ -1051,7 +1088,7 @@ bool Model::graphs_enabled() const {
 }
 
 void Model::launch_step_group(int n) {
-    prepare_step();   // a stale eta mask is rebuilt outside the graph
+    if (!onepass_step()) prepare_step();   // a stale eta mask is rebuilt outside the graph
     const int key = cur | (ecur << 1) | (gcur << 2) | (n << 3);
     PairGraph* pg = nullptr;
     for (auto& q : pair_graphs)
@@ -1061,6 +1098,7 @@ void Model::launch_step_group(int n) {
             if (!q.exec) { pg = &q; break; }
         if (!pg) throw Error(NICR_ERR_STATE, "step graph slots exhausted");
         step_kernels_prepare(sp);
+        if (onepass_step()) step_fused_prepare(sp, neta);   // kernel attributes outside the capture
         if (fused_step()) {
             if (!ticket) ticket = dalloc_t<unsigned>(1);
             step_eta_prepare_fast(sp, neta);   // kernel attributes outside the capture
@@ -1293,7 +1331,7 @@ void Model::grain_stats(nicr_grain_stats* out, long long* cells, double* amount)
 // ------------------------------------------------------------------ measurement hooks
 const char* Model::kernel_name(int k) {
     static const char* names[K_COUNT] = {"step_main", "eta_update", "step_finalize", "eta_mask", "ksp_scan",
-                                         "refresh", "diagnostics", "step_eta"};
+                                         "refresh", "diagnostics", "step_eta", "step_fused"};
     return (k >= 0 && k < K_COUNT) ? names[k] : "?";
 }
 

@@ -101,7 +101,8 @@ public:
 
     // measurement hooks: CUDA events around every kernel launch (when enabled)
     // and a count of the kernels this model launched
-    enum Kern { K_STEP_MAIN, K_ETA_UPDATE, K_FINALIZE, K_ETA_MASK, K_KSP, K_REFRESH, K_DIAG, K_STEP_ETA, K_COUNT };
+    enum Kern { K_STEP_MAIN, K_ETA_UPDATE, K_FINALIZE, K_ETA_MASK, K_KSP, K_REFRESH, K_DIAG, K_STEP_ETA,
+                K_STEP_FUSED, K_COUNT };
     static const char* kernel_name(int k);
     void profile_enable(bool on);
     void profile_collect();
@@ -187,6 +188,15 @@ public:
     // reciprocal form, 3D, 1..16 evolving eta fields; opt-in, NICR_FUSED=1:
     // measured 1.122 vs 1.129 ms per step at 256^3 with 8 fields)
     bool fused_step() const;
+    // One HBM pass per step (k_step_fused: 3D, 1..8 evolving eta fields, rows
+    // a multiple of 16, columns of 32): the default for the grids it serves;
+    // NICR_STEP_FORM=split selects the two-kernel form (A/B runs and tests).
+    // The pass rebuilds S and gb from eta on chip and writes neither, so the
+    // handle's gb / eta_s2 arrays go stale (eta_dirty) and are rebuilt when read.
+    bool onepass_step() const;
+    bool onepass_failed = false;   // the launcher refused (buffer alignment): split form from then on
+    // one step in the one-pass form into the trial buffers; false when it cannot launch
+    bool launch_onepass(int* nb);
 
 private:
     friend class SlabGroup;

@@ -18,6 +18,7 @@
 // Neumann copies in X for o, cr, phi, gb and for the computed mu and M
 // (refresh copies mu(1) into the ghost, 3S:613-615), periodic rows/columns.
 #include "nicr_step_impl.cuh"
+#include "nicr_step_fused.cuh"
 
 namespace nicr {
 
@@ -256,6 +257,19 @@ int choose_xchunk(const Grid& g) {
     return choose_xchunk_batch(&g, 1);
 }
 
+int choose_xchunk_fused(const Grid& g) {
+    if (forced_xchunk() > 0) return std::min(forced_xchunk(), g.nx);
+    const long long tiles = (long long)(g.na / FTA) * (g.nb / FTB), slots = 148;
+    int best = g.nx;
+    long long best_cost = -1;
+    for (int c : xchunk_candidates(g.nx)) {
+        const long long ctas = tiles * ((g.nx + c - 1) / c);
+        const long long cost = ((ctas + slots - 1) / slots) * (c + 2);
+        if (best_cost < 0 || cost < best_cost) { best_cost = cost; best = c; }
+    }
+    return best;
+}
+
 // One chunk for all domains of a batch: the same cost with the CTAs of every
 // domain sharing the waves (chunks above a domain's nx clamp to it).
 std::vector<int> xchunk_candidates(int nxmax) {
@@ -313,6 +327,23 @@ void launch_step_main(const StepParams& P, const double* o, const double* cr, co
                       cudaStream_t stream, int* nblocks_out) {
     if (P.fast) launch_step_main_fast(P, o, cr, p, gb, s2, on, crn, pn, partials, st, stream, nblocks_out);
     else launch_step_form<false>(P, o, cr, p, gb, s2, on, crn, pn, partials, st, stream, nblocks_out);
+}
+
+bool step_fused_applies(const Grid& g, int neta) { return fused_step_applies(g, neta); }
+
+bool launch_step_fused(const StepParams& P, int neta, const double* o, const double* cr, const double* p,
+                       const double* eta, double* on, double* crn, double* pn, double* eta_next,
+                       StepPartial* partials, Status* st, cudaStream_t stream, int* nblocks_out) {
+    if (P.fast)
+        return launch_step_fused_fast(P, neta, o, cr, p, eta, on, crn, pn, eta_next, partials, st, stream,
+                                      nblocks_out);
+    return launch_step_fused_form<false>(P, neta, o, cr, p, eta, on, crn, pn, eta_next, partials, st, stream,
+                                         nblocks_out);
+}
+
+void step_fused_prepare(const StepParams& P, int neta) {
+    if (P.fast) step_fused_prepare_fast(P, neta);
+    else if (fused_step_applies(P.g, neta)) step_fused_prepare<false>(neta);
 }
 
 void launch_eta_mask(const StepParams& P, int neta, const double* eta, double* gb, double* s2, double* pairs,

@@ -7,6 +7,7 @@
 // in both kernels on B200. The kernels are the shared templates of
 // nicr_step_impl.cuh, instantiated with FAST = true.
 #include "nicr_step_impl.cuh"
+#include "nicr_step_fused.cuh"
 
 namespace nicr {
 
@@ -27,6 +28,17 @@ bool launch_step_eta_fast(const StepParams& P, int neta, const double* o, const 
                           double* s2_next, unsigned* ticket, Status* st, cudaStream_t stream, int* nblocks_out) {
     return launch_step_eta_form<true>(P, neta, o, cr, p, gb, s2, on, crn, pn, partials, eta, eta_next, gb_next,
                                       s2_next, ticket, st, stream, nblocks_out);
+}
+
+bool launch_step_fused_fast(const StepParams& P, int neta, const double* o, const double* cr, const double* p,
+                            const double* eta, double* on, double* crn, double* pn, double* eta_next,
+                            StepPartial* partials, Status* st, cudaStream_t stream, int* nblocks_out) {
+    return launch_step_fused_form<true>(P, neta, o, cr, p, eta, on, crn, pn, eta_next, partials, st, stream,
+                                        nblocks_out);
+}
+
+void step_fused_prepare_fast(const StepParams& P, int neta) {
+    if (fused_step_applies(P.g, neta)) step_fused_prepare<true>(neta);
 }
 
 void step_eta_prepare_fast(const StepParams& P, int neta) {

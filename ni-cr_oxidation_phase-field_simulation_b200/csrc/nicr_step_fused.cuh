@@ -1,0 +1,496 @@
+// One HBM pass per step in 3D with evolving eta: the step kernel and the eta
+// update fused into one X march (the reference's refresh + step + eta_trial,
+// 3S:597-620, 3S:761-826, 3S:514-526, with rebuild_eta_mask 3S:495-507 done
+// on chip). Included by nicr_step_impl.cuh users after the shared templates.
+//
+// Per CTA: a 16 x 32 tile (512 threads, one CTA per SM) marching along its X
+// chunk. o, cr and phi are staged as in k_step_main (register prefetch into
+// shared-memory rings). The N eta fields of each plane are staged by TMA
+// (cp.async.bulk.tensor, nine boxes: the tile, the two wrapped halo rows, the
+// two 2-column halo strips and the four corners, all N fields at once) into a
+// three-plane ring whose slots complete on mbarriers; the copy of plane x+2
+// is issued at the top of the iteration that updates plane x-1+1... one plane
+// ahead of its use. From the staged plane of the lead plane x every thread
+// rebuilds S = sum eta^2 and the GB mask gb = scale*min(1,16*pairs) at its own
+// point and, for the first 100 threads, at one halo-ring point, in
+// rebuild_eta_mask's order, so the mobilities of the lead plane need no gb
+// array and the phi force no eta_s2 array. The eta update of plane u reads
+// its centre and in-plane neighbours from the slot of plane u, the +X value
+// from the slot of plane u+1 and the -X value from registers (each thread's
+// own column of plane u-1, kept from the previous iteration).
+//
+// HBM traffic per cell and step: o, cr, phi and the N eta read once and
+// written once: (6 + 2N) * 8 bytes (176 at N = 8), against (6 + 2N) * 8 + 40
+// for the two-kernel form, which writes and re-reads gb and eta_s2 and reads
+// phi twice. The handle's gb and eta_s2 arrays are not written; the model
+// rebuilds them (k_eta_mask) when something reads them.
+//
+// Shared memory at N = 8: 105.6 KB of step staging + 3 x 41.5 KB of eta
+// slots = 225 KB, so N <= 8 and one CTA per SM. Grids: rows a multiple of 16,
+// columns a multiple of 32 (whole tiles, so every TMA box and its x
+// coordinate, b0, b0 - 2, b0 + 32, nb - 2 or 0, is a multiple of two doubles).
+// Every mbarrier wait is bounded; a wait that runs out sets st->timeout and
+// the CTA leaves after a bounded wait for its own copies in flight.
+#pragma once
+
+namespace nicr {
+namespace {
+
+constexpr int FTA = 16, FTB = 32;    // fused tile: 16 rows x 32 columns
+constexpr int kFusedMaxEta = 8;
+
+template <int N>
+struct FusedLayout {
+    static constexpr int TA = FTA, TB = FTB, NT = TA * TB;
+    // eta slot regions (doubles), each a 128-byte multiple: tile [N][TA][TB],
+    // top and bottom halo rows [N][TB], left and right strips [N][TA][2]
+    // (columns b0-2, b0-1 and b0+32, b0+33), four corners [N][2]
+    static constexpr int INT = N * NT, ROW = N * TB, COL = N * TA * 2, CRN = ((2 * N + 15) / 16) * 16;
+    static constexpr int O_TOP = INT, O_BOT = O_TOP + ROW, O_LFT = O_BOT + ROW, O_RGT = O_LFT + COL;
+    static constexpr int O_TL = O_RGT + COL, O_TR = O_TL + CRN, O_BL = O_TR + CRN, O_BR = O_BL + CRN;
+    static constexpr int SLOT = O_BR + CRN;
+    static constexpr unsigned TX_BYTES = (unsigned)(INT + 2 * ROW + 2 * COL + 4 * 2 * N) * 8u;
+    static constexpr int RING = 3;
+    using T = Tile<3, TA, TB>;
+    static constexpr size_t STEP_BYTES = (T::SMEM_BYTES + 127) / 128 * 128;
+    static constexpr size_t BYTES = STEP_BYTES + 128 + (size_t)RING * SLOT * 8;
+    static_assert(STEP_BYTES % 128 == 0 && SLOT % 16 == 0, "eta slots must stay 128-byte aligned");
+};
+
+__device__ __forceinline__ void tma_load_4d_c(void* dst, const CUtensorMap* map, int x, int y, int z,
+                                              unsigned long long* bar) {
+    tma_load_4d(dst, map, x, y, z, 0, bar);
+}
+
+// Offset and field stride of a point of the tile + halo ring within an eta slot.
+template <int N>
+__device__ __forceinline__ void eta_slot_point(int a, int b, int& off, int& stride) {
+    using L = FusedLayout<N>;
+    constexpr int TA = L::TA, TB = L::TB;
+    if (a >= 0 && a < TA && b >= 0 && b < TB) { off = a * TB + b; stride = L::NT; return; }
+    if (b >= 0 && b < TB) { off = (a < 0 ? L::O_TOP : L::O_BOT) + b; stride = TB; return; }
+    if (a >= 0 && a < TA) { off = (b < 0 ? L::O_LFT + a * 2 + 1 : L::O_RGT + a * 2); stride = 2 * TA; return; }
+    if (a < 0) off = b < 0 ? L::O_TL + 1 : L::O_TR;
+    else off = b < 0 ? L::O_BL + 1 : L::O_BR;
+    stride = 2;
+}
+
+template <bool FAST, int N>
+struct OnePassStep {
+    using L = FusedLayout<N>;
+    using T = typename L::T;
+    using SK = StepKernel<3, FTA, FTB, FAST>;
+    static constexpr int TA = FTA, TB = FTB, NT = L::NT;
+
+    // S and the GB mask of one point from a staged eta plane (rebuild_eta_mask order)
+    __device__ static double mask_at(const StepParams& P, const double* slot, int off, int stride, double& S) {
+        double s = 0., pairs = 0.;
+#pragma unroll
+        for (int q = 0; q < N; ++q) {
+            const double e = slot[off + q * stride];
+            const double sq = e * e;
+            pairs += s * sq;
+            s += sq;
+        }
+        S = s;
+        return P.eta_scale * smin(1., 16. * pairs);
+    }
+
+    // o, cr at plane xoc (radius 2) and phi at plane xp (radius 1) into registers
+    __device__ static void fetch_ocp(const StepParams& P, const double* __restrict__ o, const double* __restrict__ cr,
+                                     const double* __restrict__ p, int xoc, int xp, const typename SK::Offs& f,
+                                     typename SK::Prefetch& r) {
+        const Grid& g = P.g;
+        const int xo = xoc < 0 ? 0 : (xoc > g.nx - 1 ? g.nx - 1 : xoc);
+        const int xq = xp < 0 ? 0 : (xp > g.nx - 1 ? g.nx - 1 : xp);
+        const bool inlet = P.inlet && xo == 0;
+        const long long bo = (long long)xo * g.plane, bq = (long long)xq * g.plane;
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            if (f.o2[k] >= 0) {
+                r.o[k] = inlet ? P.layer_o : __ldg(o + bo + f.o2[k]);
+                r.cr[k] = __ldg(cr + bo + f.o2[k]);
+            }
+            if (f.o1[k] >= 0) r.p[k] = __ldg(p + bq + f.o1[k]);
+        }
+    }
+
+    __device__ static void run(const StepParams& P, const CUtensorMap* m_int, const CUtensorMap* m_row,
+                               const CUtensorMap* m_col, const CUtensorMap* m_crn, const double* __restrict__ o,
+                               const double* __restrict__ cr, const double* __restrict__ p, double* __restrict__ on,
+                               double* __restrict__ crn, double* __restrict__ pn, double* __restrict__ eta_next,
+                               StepPartial* __restrict__ partials, Status* st) {
+        extern __shared__ __align__(128) unsigned char fused_smem[];
+        __shared__ unsigned long long bars[L::RING];
+        double* smem = reinterpret_cast<double*>(fused_smem);
+        double* so = smem;                 // 4 slots x S2
+        double* scr = so + 4 * T::S2;      // 4 slots x S2
+        double* sp = scr + 4 * T::S2;      // 3 slots x S1
+        double* smuO = sp + 3 * T::S1;     // 2 slots x S1
+        double* smuCr = smuO + 2 * T::S1;
+        double* smo = smuCr + 2 * T::S1;
+        double* smc = smo + 2 * T::S1;
+        DD* sdd = reinterpret_cast<DD*>(smc + 2 * T::S1);
+        long long* scnt = reinterpret_cast<long long*>(sdd + 32 * 5);
+        double* ering = reinterpret_cast<double*>(
+            ((unsigned long long)(fused_smem + L::STEP_BYTES) + 127ull) & ~127ull);
+
+        if (st->failed) return;   // a previous step of this batch was rejected
+
+        const Grid& g = P.g;
+        const int ta = threadIdx.y, tb = threadIdx.x, tid = tb + TB * ta;
+        const int a0 = blockIdx.y * TA, b0 = blockIdx.x * TB;
+        const int i0 = blockIdx.z * P.xchunk, i1 = min(g.nx, i0 + P.xchunk);
+        const int row = a0 + ta, col = b0 + tb;
+        const typename SK::Offs offs = SK::make_offs(g, a0, b0);
+
+        // ---- eta staging: plane q (clamped to [0, nx-1], the Neumann ghosts)
+        // lives in slot (q - i0 + 1) % 3; planes i0-1 .. i1 are staged once each
+        const int ytop = a0 == 0 ? g.na - 1 : a0 - 1, ybot = a0 + TA == g.na ? 0 : a0 + TA;
+        const int xl = b0 == 0 ? g.nb - 2 : b0 - 2, xr = b0 + TB == g.nb ? 0 : b0 + TB;
+        auto eslot = [&](int q) { return ering + (size_t)((q - i0 + 1) % L::RING) * L::SLOT; };
+        auto issue = [&](int q) {   // one thread
+            const int xg = q < 0 ? 0 : (q > g.nx - 1 ? g.nx - 1 : q);
+            double* s = eslot(q);
+            unsigned long long* bar = &bars[(q - i0 + 1) % L::RING];
+            asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+            mbar_expect_tx(bar, L::TX_BYTES);
+            tma_load_4d_c(s, m_int, b0, a0, xg, bar);
+            tma_load_4d_c(s + L::O_TOP, m_row, b0, ytop, xg, bar);
+            tma_load_4d_c(s + L::O_BOT, m_row, b0, ybot, xg, bar);
+            tma_load_4d_c(s + L::O_LFT, m_col, xl, a0, xg, bar);
+            tma_load_4d_c(s + L::O_RGT, m_col, xr, a0, xg, bar);
+            tma_load_4d_c(s + L::O_TL, m_crn, xl, ytop, xg, bar);
+            tma_load_4d_c(s + L::O_TR, m_crn, xr, ytop, xg, bar);
+            tma_load_4d_c(s + L::O_BL, m_crn, xl, ybot, xg, bar);
+            tma_load_4d_c(s + L::O_BR, m_crn, xr, ybot, xg, bar);
+        };
+        bool ok = true;
+        auto wait = [&](int q) {
+            const int k = q - i0 + 1;
+            const unsigned parity = (unsigned)((k / L::RING) & 1);
+            unsigned long long* bar = &bars[k % L::RING];
+            for (long long it = 0; ok && !mbar_try_wait(bar, parity); ++it)
+                if (it > kTmaWaitLimit) ok = false;
+        };
+        if (tid == 0) {
+            for (int r = 0; r < L::RING; ++r) mbar_init(&bars[r], 1);
+            asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+        }
+        __syncthreads();
+        int issued = i0 + 1;   // last plane whose copy was issued
+        if (tid == 0)
+            for (int q = i0 - 1; q <= i0 + 1; ++q) issue(q);
+
+        // per-thread positions in an eta slot: own point and its four in-plane
+        // neighbours; the halo-ring point of the first S1 - NT threads
+        const int e_own = ta * TB + tb;
+        int am_o, am_s, ap_o, ap_s, bm_o, bm_s, bp_o, bp_s;
+        eta_slot_point<N>(ta - 1, tb, am_o, am_s);
+        eta_slot_point<N>(ta + 1, tb, ap_o, ap_s);
+        eta_slot_point<N>(ta, tb - 1, bm_o, bm_s);
+        eta_slot_point<N>(ta, tb + 1, bp_o, bp_s);
+        int ring_o = 0, ring_s = 0;
+        if (offs.gl[1] >= 0) {
+            int a, b;
+            SK::ring_point(tid, a, b);
+            eta_slot_point<N>(a, b, ring_o, ring_s);
+        }
+
+        DD acc[5] = {{0., 0.}, {0., 0.}, {0., 0.}, {0., 0.}, {0., 0.}};  // ckO ckCr clipO clipCr bcO
+        long long clipped = 0;
+        unsigned long long errkey = ERR_NONE;
+
+        auto slot3 = [](int w) { return ((w % 3) + 3) % 3; };
+        auto oslot = [&](int w) { return so + (w & 3) * T::S2; };
+        auto cslot = [&](int w) { return scr + (w & 3) * T::S2; };
+        auto pslot = [&](int x) { return sp + slot3(x) * T::S1; };
+
+        // the lead plane x over the tile + radius-1 halo; S and gb of the own
+        // point are returned for the update of plane x in the next iteration
+        auto lead = [&](int x, double& S_own, double& gb_own) -> CenterVals {
+            const double* es = eslot(x);
+            double gbl[2];
+            gbl[0] = mask_at(P, es, e_own, NT, S_own);
+            gb_own = gbl[0];
+            const double *som = oslot(x - 1), *so0 = oslot(x), *sop = oslot(x + 1);
+            const double *scm = cslot(x - 1), *sc0 = cslot(x), *scp = cslot(x + 1);
+            const double* spx = pslot(x);
+            double* mO = smuO + (x & 1) * T::S1;
+            double* mC = smuCr + (x & 1) * T::S1;
+            double* mo_ = smo + (x & 1) * T::S1;
+            double* mc_ = smc + (x & 1) * T::S1;
+            CenterVals own = SK::lead_point(P, nullptr, som, so0, sop, scm, sc0, scp, spx, mO, mC, mo_, mc_, ta, tb,
+                                            gbl[0]);
+            if (offs.gl[1] >= 0) {
+                double Sr;
+                gbl[1] = mask_at(P, es, ring_o, ring_s, Sr);
+                int a, b;
+                SK::ring_point(tid, a, b);
+                SK::lead_point(P, nullptr, som, so0, sop, scm, sc0, scp, spx, mO, mC, mo_, mc_, a, b, gbl[1]);
+            }
+            return own;
+        };
+
+        CenterVals C, Lv;
+        double pP, FxO, FxCr;
+        double s2u, gbu;          // S and gb of the own point of the update plane
+        double ep[N];             // own column of eta at plane u - 1
+        // ---- prologue: centre values of the first update plane and its left x-face flux
+        if (i0 == 0) {
+            SK::load_oc(P, o, cr, -1, oslot(-1), cslot(-1), offs);
+            SK::load_oc(P, o, cr, 0, oslot(0), cslot(0), offs);
+            SK::load_oc(P, o, cr, 1, oslot(1), cslot(1), offs);
+            SK::load_p(P, p, 0, pslot(0), offs);
+            wait(-1);
+            wait(0);
+            __syncthreads();
+            C = lead(0, s2u, gbu);
+            __syncthreads();
+            const double muOg = (P.bc == 1 && P.o_on) ? 2. * P.mu_res - C.muO : C.muO;
+            FxO = fdiv<FAST>(-.5 * (C.mo + C.mo) * (C.muO - muOg), P.v_dx);
+            FxCr = fdiv<FAST>(-.5 * (C.mc + C.mc) * (C.muCr - C.muCr), P.v_dx);
+            pP = C.p;
+        } else {
+            SK::load_oc(P, o, cr, i0 - 2, oslot(i0 - 2), cslot(i0 - 2), offs);
+            SK::load_oc(P, o, cr, i0 - 1, oslot(i0 - 1), cslot(i0 - 1), offs);
+            SK::load_oc(P, o, cr, i0, oslot(i0), cslot(i0), offs);
+            SK::load_p(P, p, i0 - 1, pslot(i0 - 1), offs);
+            wait(i0 - 1);
+            __syncthreads();
+            double Sm, gbm;
+            const CenterVals Pv = lead(i0 - 1, Sm, gbm);
+            SK::load_oc(P, o, cr, i0 + 1, oslot(i0 + 1), cslot(i0 + 1), offs);
+            SK::load_p(P, p, i0, pslot(i0), offs);
+            wait(i0);
+            __syncthreads();
+            C = lead(i0, s2u, gbu);
+            __syncthreads();
+            FxO = fdiv<FAST>(-.5 * (Pv.mo + C.mo) * (C.muO - Pv.muO), P.v_dx);
+            FxCr = fdiv<FAST>(-.5 * (Pv.mc + C.mc) * (C.muCr - Pv.muCr), P.v_dx);
+            pP = Pv.p;
+        }
+        {
+            const double* es = eslot(i0 - 1);   // plane i0 - 1 (plane 0, the Neumann ghost, when i0 = 0)
+#pragma unroll
+            for (int q = 0; q < N; ++q) ep[q] = es[e_own + q * NT];
+        }
+
+        typename SK::Prefetch pf;
+        if (i0 + 1 <= g.nx - 1) fetch_ocp(P, o, cr, p, i0 + 2, i0 + 1, offs, pf);
+        for (int u = i0; u < i1; ++u) {
+            const int x = u + 1;
+            double s2n = 0., gbn = 0.;
+            if (x <= g.nx - 1) {
+                SK::store(pf, oslot(x + 1), cslot(x + 1), pslot(x), offs);
+                // one barrier per plane: this plane's staging before lead(x); the
+                // previous iteration's reads of the mu/M slot lead(x) overwrites and
+                // of the eta slot the copy of plane u+2 overwrites
+                if (__syncthreads_or(!ok)) break;
+                if (u + 2 <= i1) {
+                    if (tid == 0) issue(u + 2);
+                    issued = u + 2;
+                }
+                if (x + 1 <= g.nx - 1 && u + 1 < i1) fetch_ocp(P, o, cr, p, x + 2, x + 1, offs, pf);
+                wait(x);
+                Lv = lead(x, s2n, gbn);
+            } else {
+                Lv = C;  // ghost plane nx: Neumann copy of plane nx-1 (mu and M copied too)
+                if (__syncthreads_or(!ok)) break;
+                wait(x);   // plane nx: the clamped copy of plane nx-1 (the eta +X ghost)
+            }
+            {
+                const double* mO = smuO + (u & 1) * T::S1;
+                const double* mC = smuCr + (u & 1) * T::S1;
+                const double* mo_ = smo + (u & 1) * T::S1;
+                const double* mc_ = smc + (u & 1) * T::S1;
+                const double* spu = pslot(u);
+                const int c1 = T::i1(ta, tb);
+                const int bp = T::i1(ta, tb + 1), bm = T::i1(ta, tb - 1);
+                const int ap = T::i1(ta + 1, tb), am = T::i1(ta - 1, tb);
+                const long long gidx = (long long)u * g.plane + (long long)row * g.pb + col;
+                const long long cell = ((long long)u * g.na + row) * g.nb + col;   // reference loop order
+
+                const double rightO = fdiv<FAST>(-.5 * (C.mo + Lv.mo) * (Lv.muO - C.muO), P.v_dx);
+                const double rightCr = fdiv<FAST>(-.5 * (C.mc + Lv.mc) * (Lv.muCr - C.muCr), P.v_dx);
+                double leftO = FxO;
+                if (u == 0 && P.bc == 1) {
+                    // left_flux (3S:621-628): surface-mobility face closure for bc=mu
+                    double lf = 0.;
+                    if (P.o_on) {
+                        const double mf = mobility(P.surface_c_ref, h(C.p), gbu, Phys::bmo, Phys::boo, P.gbm1_o);
+                        lf = fdiv<FAST>(2. * mf * (P.mu_res - C.muO), P.v_dx);
+                    }
+                    leftO = lf;
+                    acc[4] = dd_add(acc[4], fdiv<FAST>(P.dt * lf, P.v_dx));
+                }
+                if (u == 0 && P.inlet) acc[4] = dd_add(acc[4], P.layer_o - __ldg(o + gidx));
+
+                double divO = 0., divCr;
+                {
+                    const double mc0 = mc_[c1], mu0 = mC[c1];
+                    const double front = fdiv<FAST>(-.5 * (mc0 + mc_[bp]) * (mC[bp] - mu0), P.v_db);
+                    const double back = fdiv<FAST>(-.5 * (mc_[bm] + mc0) * (mu0 - mC[bm]), P.v_db);
+                    const double top = fdiv<FAST>(-.5 * (mc0 + mc_[ap]) * (mC[ap] - mu0), P.v_da);
+                    const double bottom = fdiv<FAST>(-.5 * (mc_[am] + mc0) * (mu0 - mC[am]), P.v_da);
+                    divCr = fdiv<FAST>(FxCr - rightCr, P.v_dx) + fdiv<FAST>(bottom - top, P.v_da) + fdiv<FAST>(back - front, P.v_db);
+                }
+                if (P.o_on) {
+                    const double m0 = mo_[c1], mu0 = mO[c1];
+                    const double front = fdiv<FAST>(-.5 * (m0 + mo_[bp]) * (mO[bp] - mu0), P.v_db);
+                    const double back = fdiv<FAST>(-.5 * (mo_[bm] + m0) * (mu0 - mO[bm]), P.v_db);
+                    const double top = fdiv<FAST>(-.5 * (m0 + mo_[ap]) * (mO[ap] - mu0), P.v_da);
+                    const double bottom = fdiv<FAST>(-.5 * (mo_[am] + m0) * (mu0 - mO[am]), P.v_da);
+                    divO = fdiv<FAST>(leftO - rightO, P.v_dx) + fdiv<FAST>(bottom - top, P.v_da) + fdiv<FAST>(back - front, P.v_db);
+                }
+                const double oo = C.o, cc = C.cr, pp = C.p;
+                double onv = P.o_on ? oo + P.dt * divO : oo;
+                double crv = cc + P.dt * divCr;
+                const double lapP = fdiv<FAST>((Lv.p - 2. * pp + pP), P.v_dxdx)
+                                  + fdiv<FAST>((spu[ap] - 2. * pp + spu[am]), P.v_dada)
+                                  + fdiv<FAST>((spu[bp] - 2. * pp + spu[bm]), P.v_dbdb);
+                const double hpv = 30. * pp * pp * (pp - 1.) * (pp - 1.);
+                double fp = Phys::W * (4. * pp * pp * pp - 6. * pp * pp + 2. * pp)
+                          + hpv * (foxide(oo, cc) - fmetal(oo, cc)) - 2. * Phys::kp * lapP;
+                fp += grain_dphi(s2u, pp, P.eta_W, P.eta_A);
+                double pnv = pp - P.dtL * fp;
+                if (P.ck == 0) {
+                    const double hn = h(pnv);
+                    const double dO = fdiv<FAST>(-Phys::ckO * ((Phys::oxideO - onv) * hn - (Phys::oxideO - oo) * C.hh), P.v_dt);
+                    const double dCr = fdiv<FAST>(-Phys::ckCr * ((Phys::oxideCr - crv) * hn - (Phys::oxideCr - cc) * C.hh), P.v_dt);
+                    onv += dO; crv += dCr;
+                    if (dO != 0.) acc[0] = dd_add(acc[0], dO);
+                    if (dCr != 0.) acc[1] = dd_add(acc[1], dCr);
+                }
+                if (!isfinite(onv) || !isfinite(crv) || !isfinite(pnv)) {
+                    errkey = min(errkey, (unsigned long long)cell * 4ull);
+                } else if (P.bounds == 1) {
+                    const double oc = sclamp(onv, 0., 1.), ccr = sclamp(crv, 0., 1.);
+                    const double clO = oc - onv, clCr = ccr - crv;
+                    if (clO != 0.) acc[2] = dd_add(acc[2], clO);
+                    if (clCr != 0.) acc[3] = dd_add(acc[3], clCr);
+                    if (oc != onv || ccr != crv) ++clipped;
+                    onv = oc; crv = ccr;
+                    if (pnv > .99999) pnv = 1.;
+                    if (pnv < 1.e-5) pnv = 0.;
+                } else if (onv < -1.e-12 || crv < -1.e-12 || onv + crv > 1. + 1.e-12 || pnv < -1.e-12 ||
+                           pnv > 1. + 1.e-12) {
+                    errkey = min(errkey, (unsigned long long)cell * 4ull + 1ull);
+                }
+                on[gidx] = onv; crn[gidx] = crv; pn[gidx] = pnv;
+                FxO = rightO; FxCr = rightCr;
+
+                // eta_trial (3S:514-526) at plane u: v = eta - (dt L_eta)(deta - K lap eta)
+                const double* es = eslot(u);
+                const double* en = eslot(u + 1);
+#pragma unroll
+                for (int q = 0; q < N; ++q) {
+                    const double c0 = es[e_own + q * NT];
+                    const double lap = fdiv<FAST>((en[e_own + q * NT] - 2. * c0 + ep[q]), P.v_dxdx)
+                                     + fdiv<FAST>((es[ap_o + q * ap_s] - 2. * c0 + es[am_o + q * am_s]), P.v_dada)
+                                     + fdiv<FAST>((es[bp_o + q * bp_s] - 2. * c0 + es[bm_o + q * bm_s]), P.v_dbdb);
+                    const double force = grain_deta(c0, s2u, pp, P.eta_W, P.eta_A) - P.eta_K * lap;
+                    const double v = c0 - P.dt_etaL * force;
+                    if (!isfinite(v) || v < -1.e-12 || v > 1. + 1.e-12)
+                        errkey = min(errkey, ERR_ETA_BASE + (unsigned long long)q * (unsigned long long)g.ncells +
+                                                 (unsigned long long)cell);
+                    eta_next[(long long)q * g.nstore + gidx] = v;
+                    ep[q] = c0;
+                }
+            }
+            pP = C.p;
+            C = Lv;
+            s2u = s2n;
+            gbu = gbn;
+        }
+        if (__syncthreads_or(!ok)) {
+            // a wait ran out: flag it, give the copies in flight a bounded time to land, leave
+            if (tid == 0) {
+                atomicOr(&st->timeout, 1);
+                for (int q = i0 - 1; q <= issued; ++q) {
+                    const int k = q - i0 + 1;
+                    unsigned long long* bar = &bars[k % L::RING];
+                    for (long long it = 0; it <= kTmaWaitLimit && !mbar_try_wait(bar, (unsigned)((k / L::RING) & 1));
+                         ++it) {
+                    }
+                }
+            }
+            __syncthreads();
+            return;
+        }
+        if (errkey != ERR_NONE) atomicMin(&st->err_key, errkey);
+        block_reduce_dd<5>(acc, clipped, sdd, scnt);
+        if (tid == 0) {
+            StepPartial& out = partials[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)];
+            for (int q = 0; q < 5; ++q) { out.s[q][0] = acc[q].hi; out.s[q][1] = acc[q].lo; }
+            out.clipped = clipped;
+        }
+    }
+};
+
+template <bool FAST, int N>
+__global__ void __launch_bounds__(FTA * FTB, 1)
+k_step_fused(const StepParams P, const __grid_constant__ CUtensorMap m_int, const __grid_constant__ CUtensorMap m_row,
+             const __grid_constant__ CUtensorMap m_col, const __grid_constant__ CUtensorMap m_crn,
+             const double* __restrict__ o, const double* __restrict__ cr, const double* __restrict__ p,
+             double* __restrict__ on, double* __restrict__ crn, double* __restrict__ pn,
+             double* __restrict__ eta_next, StepPartial* __restrict__ partials, Status* st) {
+    OnePassStep<FAST, N>::run(P, &m_int, &m_row, &m_col, &m_crn, o, cr, p, on, crn, pn, eta_next, partials, st);
+}
+
+// Whether the fused step serves grid g with n eta fields (the eta buffer's
+// 16-byte alignment is checked at launch).
+inline bool fused_step_applies(const Grid& g, int n) {
+    return g.dim == 3 && n >= 1 && n <= kFusedMaxEta && g.na % FTA == 0 && g.nb % FTB == 0 && g.nx >= 2;
+}
+
+template <bool FAST, int N>
+static bool launch_step_fused_n(const StepParams& P, const double* o, const double* cr, const double* p,
+                                const double* eta, double* on, double* crn, double* pn, double* eta_next,
+                                StepPartial* partials, Status* st, cudaStream_t stream, int* nblocks_out) {
+    const Grid& g = P.g;
+    CUtensorMap mi, mr, mc, mk;
+    if (!encode_eta_map(&mi, g, N, eta, FTB, FTA) || !encode_eta_map(&mr, g, N, eta, FTB, 1) ||
+        !encode_eta_map(&mc, g, N, eta, 2, FTA) || !encode_eta_map(&mk, g, N, eta, 2, 1))
+        return false;
+    using L = FusedLayout<N>;
+    ensure_smem_attr((const void*)k_step_fused<FAST, N>, (int)L::BYTES);
+    const dim3 grid(g.nb / FTB, g.na / FTA, (g.nx + P.xchunk - 1) / P.xchunk);
+    k_step_fused<FAST, N><<<grid, dim3(FTB, FTA), L::BYTES, stream>>>(P, mi, mr, mc, mk, o, cr, p, on, crn, pn,
+                                                                      eta_next, partials, st);
+    if (nblocks_out) *nblocks_out = (int)(grid.x * grid.y * grid.z);
+    return true;
+}
+
+// Launches the fused step for n eta fields; false (nothing launched) when the
+// grid, the field count or the buffer alignment does not allow it.
+template <bool FAST>
+static bool launch_step_fused_form(const StepParams& P, int n, const double* o, const double* cr, const double* p,
+                                   const double* eta, double* on, double* crn, double* pn, double* eta_next,
+                                   StepPartial* partials, Status* st, cudaStream_t stream, int* nblocks_out) {
+    if (!fused_step_applies(P.g, n) || P.err_slot >= 0) return false;
+    if ((reinterpret_cast<unsigned long long>(eta) & 15ull) != 0) return false;
+    switch (n) {
+#define NICR_FUSED_STEP_CASE(k) \
+    case k: return launch_step_fused_n<FAST, k>(P, o, cr, p, eta, on, crn, pn, eta_next, partials, st, stream, nblocks_out);
+        NICR_FUSED_STEP_CASE(1) NICR_FUSED_STEP_CASE(2) NICR_FUSED_STEP_CASE(3) NICR_FUSED_STEP_CASE(4)
+        NICR_FUSED_STEP_CASE(5) NICR_FUSED_STEP_CASE(6) NICR_FUSED_STEP_CASE(7) NICR_FUSED_STEP_CASE(8)
+#undef NICR_FUSED_STEP_CASE
+        default: return false;
+    }
+}
+
+template <bool FAST>
+static void step_fused_prepare(int n) {
+    switch (n) {
+#define NICR_FUSED_PREP_CASE(k) \
+    case k: ensure_smem_attr((const void*)k_step_fused<FAST, k>, (int)FusedLayout<k>::BYTES); break;
+        NICR_FUSED_PREP_CASE(1) NICR_FUSED_PREP_CASE(2) NICR_FUSED_PREP_CASE(3) NICR_FUSED_PREP_CASE(4)
+        NICR_FUSED_PREP_CASE(5) NICR_FUSED_PREP_CASE(6) NICR_FUSED_PREP_CASE(7) NICR_FUSED_PREP_CASE(8)
+#undef NICR_FUSED_PREP_CASE
+        default: break;
+    }
+}
+
+}  // namespace
+}  // namespace nicr
