@@ -357,6 +357,56 @@ def small_workload(args) -> int:
     return 0
 
 
+def ksp_workload(args) -> int:
+    """Cost of one Ksp scan (Model::nucleate, 3S:752-759) at the benchmark's
+    size, against the stepping it interrupts once per nucleation period (500
+    steps at the default dt): the benchmark state after --warmup + --steps
+    steps (O has entered only the first planes, so few cells pass the point
+    test), and the same grid made supersaturated (O = 0.001 everywhere, as
+    3S:1197 does for its insertion self-test), where every metal cell is a
+    candidate and the ordered resolve inserts many nuclei. CUDA events on the
+    library's stream around nicr_nucleate (which reads its result back)."""
+    import torch
+    import nicr
+    out = {"workload": "ksp", "unit": "ms per scan"}
+    cfg = workload_config(args.size, args.neta, seed=2)
+    cfg.precision = 1
+    sol = nicr.Solver(cfg)
+    cr = 0.25 + np.random.default_rng(2).uniform(-0.01, 0.01, size=sol.shape)
+    cr[0] = sol.get("cr")[0]
+    sol.set("cr", cr)
+    sol.reset_inventory()
+    stream = torch.cuda.ExternalStream(sol.stream())
+    sol.run(max(args.warmup, 1))
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    sol.run(args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    step_ms = e0.elapsed_time(e1) / args.steps
+    out["step_ms"] = step_ms
+    period = int(round(cfg.nucleation_period / cfg.dt))
+    for state in ("bench", "supersaturated"):
+        if state == "supersaturated":
+            sol.set("o", np.full(sol.shape, 0.001))
+        times, nuclei = [], []
+        for rep in range(2):
+            torch.cuda.synchronize()
+            e0.record(stream)
+            k = sol.nucleate()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1))
+            nuclei.append(k)
+        out[state] = {"scan_ms": times, "nuclei": nuclei,
+                      "fraction_of_period": times[0] / (times[0] + period * step_ms),
+                      "period_steps": period}
+    sol.close()
+    print(json.dumps(out))
+    return 0
+
+
 def surrogate_workload(args) -> int:
     """The learned surrogate's kernels at 128^3: (1) the 3x3x3 convolutions of
     the U-Net's layers (base 16 channels: 16->16 and 48->16 at 128^3, 96->32
@@ -730,7 +780,7 @@ def main():
     ap.add_argument("--ref-budget", type=float, default=60.0, help="seconds of CPU stepping for the reference")
     ap.add_argument("--slab-devices", default="", help="--workload slabs: comma-separated device per slab")
     ap.add_argument("--workload", choices=["step", "output", "sweep", "small", "accuracy", "slabs", "slab-ranks",
-                                           "surrogate", "surrogate-train"],
+                                           "surrogate", "surrogate-train", "ksp"],
                     default="step",
                     help="step: the headline line (default); output: VTI frame cost and overlap with stepping; "
                          "sweep: 64 uneven domains advanced as one batch; small: step rate of the small configs; "
@@ -738,7 +788,8 @@ def main():
                          "slabs: the domain split along X into slabs against one handle; "
                          "slab-ranks: the domain split over the torchrun ranks (one slab per GPU); "
                          "surrogate: the learned surrogate's convolution kernels and U-Net at 128^3; "
-                         "surrogate-train: data-parallel training of the surrogate over the torchrun ranks")
+                         "surrogate-train: data-parallel training of the surrogate over the torchrun ranks; "
+                         "ksp: one Ksp scan at 256^3 in the benchmark state and supersaturated")
     ap.add_argument("--precision", type=int, default=0, help="arithmetic form of --workload sweep (0 drop-in, 1 fast)")
     ap.add_argument("--no-jumps", action="store_true", help="--workload surrogate: kernels only, no training and jump runs")
     args = ap.parse_args()
@@ -767,6 +818,8 @@ def main():
         return surrogate_workload(args)
     if args.workload == "surrogate-train":
         return surrogate_train_workload(args, rank, world, local)
+    if args.workload == "ksp":
+        return ksp_workload(args)
 
     import torch
     import torch.distributed as dist

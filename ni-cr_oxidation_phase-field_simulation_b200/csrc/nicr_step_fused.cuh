@@ -407,7 +407,8 @@ struct OnePassStep {
             // a wait ran out: flag it, give the copies in flight a bounded time to land, leave
             if (tid == 0) {
                 atomicOr(&st->timeout, 1);
-                for (int q = i0 - 1; q <= issued; ++q) {
+                // the last copy issued into each slot (earlier phases of a slot have completed)
+                for (int q = max(i0 - 1, issued - (L::RING - 1)); q <= issued; ++q) {
                     const int k = q - i0 + 1;
                     unsigned long long* bar = &bars[k % L::RING];
                     for (long long it = 0; it <= kTmaWaitLimit && !mbar_try_wait(bar, (unsigned)((k / L::RING) & 1));
