@@ -232,8 +232,7 @@ struct OnePassStep {
             return own;
         };
 
-        CenterVals C, Lv;
-        double pP, FxO, FxCr;
+        double pP, FxO, FxCr;   // phi of plane u-1 (own point), left x-face fluxes of plane u
         double s2u, gbu;          // S and gb of the own point of the update plane
         double ep[N];             // own column of eta at plane u - 1
         // ---- prologue: centre values of the first update plane and its left x-face flux
@@ -245,7 +244,7 @@ struct OnePassStep {
             wait(-1);
             wait(0);
             __syncthreads();
-            C = lead(0, s2u, gbu);
+            const CenterVals C = lead(0, s2u, gbu);
             __syncthreads();
             const double muOg = (P.bc == 1 && P.o_on) ? 2. * P.mu_res - C.muO : C.muO;
             FxO = fdiv<FAST>(-.5 * (C.mo + C.mo) * (C.muO - muOg), P.v_dx);
@@ -264,7 +263,7 @@ struct OnePassStep {
             SK::load_p(P, p, i0, pslot(i0), offs);
             wait(i0);
             __syncthreads();
-            C = lead(i0, s2u, gbu);
+            const CenterVals C = lead(i0, s2u, gbu);
             __syncthreads();
             FxO = fdiv<FAST>(-.5 * (Pv.mo + C.mo) * (C.muO - Pv.muO), P.v_dx);
             FxCr = fdiv<FAST>(-.5 * (Pv.mc + C.mc) * (C.muCr - Pv.muCr), P.v_dx);
@@ -293,9 +292,8 @@ struct OnePassStep {
                 }
                 if (x + 1 <= g.nx - 1 && u + 1 < i1) fetch_ocp(P, o, cr, p, x + 2, x + 1, offs, pf);
                 wait(x);
-                Lv = lead(x, s2n, gbn);
+                lead(x, s2n, gbn);
             } else {
-                Lv = C;  // ghost plane nx: Neumann copy of plane nx-1 (mu and M copied too)
                 if (__syncthreads_or(!ok)) break;
                 wait(x);   // plane nx: the clamped copy of plane nx-1 (the eta +X ghost)
             }
@@ -310,6 +308,23 @@ struct OnePassStep {
                 const int ap = T::i1(ta + 1, tb), am = T::i1(ta - 1, tb);
                 const long long gidx = (long long)u * g.plane + (long long)row * g.pb + col;
                 const long long cell = ((long long)u * g.na + row) * g.nb + col;   // reference loop order
+                // Centre (plane u) and lead (plane x) values are read back from
+                // the staging rings rather than carried in registers across the
+                // iteration (the same doubles; fewer live registers). The ghost
+                // plane nx is the Neumann copy of plane nx-1, mu and M included.
+                CenterVals C, Lv;
+                {
+                    const int c2 = T::i2(ta, tb);
+                    C.o = oslot(u)[c2]; C.cr = cslot(u)[c2]; C.p = spu[c1]; C.hh = h(C.p);
+                    C.muO = mO[c1]; C.muCr = mC[c1]; C.mo = mo_[c1]; C.mc = mc_[c1];
+                    if (x <= g.nx - 1) {
+                        const int lx = (x & 1) * T::S1 + c1;
+                        Lv.p = pslot(x)[c1];
+                        Lv.muO = smuO[lx]; Lv.muCr = smuCr[lx]; Lv.mo = smo[lx]; Lv.mc = smc[lx];
+                    } else {
+                        Lv = C;
+                    }
+                }
 
                 const double rightO = fdiv<FAST>(-.5 * (C.mo + Lv.mo) * (Lv.muO - C.muO), P.v_dx);
                 const double rightCr = fdiv<FAST>(-.5 * (C.mc + Lv.mc) * (Lv.muCr - C.muCr), P.v_dx);
@@ -397,9 +412,8 @@ struct OnePassStep {
                     eta_next[(long long)q * g.nstore + gidx] = v;
                     ep[q] = c0;
                 }
+                pP = pp;   // a register: the ring slot of plane u-1 takes plane u+2 next
             }
-            pP = C.p;
-            C = Lv;
             s2u = s2n;
             gbu = gbn;
         }

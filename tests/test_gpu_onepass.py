@@ -122,7 +122,7 @@ def run_child(tmp_path, tag, case, **env):
 
 
 SPLIT_CASES = {
-    "chunk1": ({"NICR_XCHUNK": "1"}, dict(nx=13, ny=32, nz=32, grain_diameter_grid=18.)),
+    "chunk1": ({"NICR_XCHUNK": "1"}, dict(nx=21, ny=32, nz=32, grain_diameter_grid=20.)),
     "chunk3": ({"NICR_XCHUNK": "3"}, dict(nx=29, ny=16, nz=64, grain_diameter_grid=19.)),
     "chunk7": ({"NICR_XCHUNK": "7"}, dict(nx=45, ny=32, nz=32, grain_diameter_grid=22.)),
 }
