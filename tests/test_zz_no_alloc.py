@@ -57,7 +57,7 @@ def test_noalloc_matches_handle_step_twice(require_gpu, dim, mode, bc, precision
         kw["nz"] = shape[2]
     cfg = nicr.make_config(dim, **kw)
     sol = nicr.Solver(cfg)
-    neta = sol.neta if mode == "evolving" else 0
+    neta = sol.n_eta if mode == "evolving" else 0
     o, cr, p, eta = smooth_fields(shape, neta, seed=5)
     p = 0.02 * (1 + np.cos(np.indices(shape).sum(axis=0) * 0.3))   # some interface cells
     sol.set_fields(o, cr, p, eta if neta else None)
