@@ -56,11 +56,18 @@ __device__ __forceinline__ double competitor_distance(const double* s, int g, in
     return db;
 }
 
+// STAGED: the seed table is copied to shared memory (when it fits, up to
+// ~8,500 seeds); otherwise the threads read it from global memory (L1/L2).
+template <bool STAGED>
 __global__ void k_voronoi3(const InitParams I, const double* __restrict__ seeds, double* grain, double* dbout,
                            int* volumes, int* competitor) {
-    extern __shared__ double ss[];
-    for (int q = threadIdx.x; q < 3 * I.ng; q += blockDim.x) ss[q] = seeds[q];
-    __syncthreads();
+    extern __shared__ double seed_smem[];
+    const double* ss = seeds;
+    if (STAGED) {
+        for (int q = threadIdx.x; q < 3 * I.ng; q += blockDim.x) seed_smem[q] = seeds[q];
+        __syncthreads();
+        ss = seed_smem;
+    }
     const Grid& g = I.g;
     const int ny = g.na, nz = g.nb;
     for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < g.ncells; c += (long long)gridDim.x * blockDim.x) {
@@ -91,11 +98,16 @@ __global__ void k_voronoi3(const InitParams I, const double* __restrict__ seeds,
     }
 }
 
+template <bool STAGED>
 __global__ void k_eta_dist3(const InitParams I, const double* __restrict__ seeds, const double* __restrict__ grain,
                             double* eta) {
-    extern __shared__ double ss[];
-    for (int q = threadIdx.x; q < 3 * I.ng; q += blockDim.x) ss[q] = seeds[q];
-    __syncthreads();
+    extern __shared__ double seed_smem[];
+    const double* ss = seeds;
+    if (STAGED) {
+        for (int q = threadIdx.x; q < 3 * I.ng; q += blockDim.x) seed_smem[q] = seeds[q];
+        __syncthreads();
+        ss = seed_smem;
+    }
     const Grid& g = I.g;
     const int ny = g.na, nz = g.nb;
     for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < g.ncells; c += (long long)gridDim.x * blockDim.x) {
@@ -438,19 +450,30 @@ int grid_for(long long n, int threads, int cap) {
 void launch_init_fields(const InitParams& I, double* o, double* cr, double* p, cudaStream_t stream) {
     k_init_fields<<<grid_for(I.g.ncells, 256, 148 * 16), 256, 0, stream>>>(I, o, cr, p);
 }
+// Seed tables larger than this are read from global memory (200 KB: ~8,500 seeds).
+constexpr size_t kSeedSmemMax = 200 * 1024;
+
 void launch_voronoi3(const InitParams& I, const double* seeds, double* grain, double* db, int* volumes,
                      int* competitor, cudaStream_t stream) {
     const size_t sm = (size_t)3 * I.ng * sizeof(double);
-    if (sm > 48 * 1024) cudaFuncSetAttribute(k_voronoi3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    k_voronoi3<<<grid_for(I.g.ncells, 128, 148 * 32), 128, sm, stream>>>(I, seeds, grain, db, volumes, competitor);
+    if (sm > kSeedSmemMax) {
+        k_voronoi3<false><<<grid_for(I.g.ncells, 128, 148 * 32), 128, 0, stream>>>(I, seeds, grain, db, volumes, competitor);
+        return;
+    }
+    if (sm > 48 * 1024) cudaFuncSetAttribute(k_voronoi3<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k_voronoi3<true><<<grid_for(I.g.ncells, 128, 148 * 32), 128, sm, stream>>>(I, seeds, grain, db, volumes, competitor);
 }
 void launch_grain_adjacency(const InitParams& I, const double* grain, unsigned char* adj, cudaStream_t stream) {
     k_grain_adjacency<<<grid_for(I.g.ncells, 256, 148 * 16), 256, 0, stream>>>(I, grain, adj);
 }
 void launch_eta_dist3(const InitParams& I, const double* seeds, const double* grain, double* eta, cudaStream_t stream) {
     const size_t sm = (size_t)3 * I.ng * sizeof(double);
-    if (sm > 48 * 1024) cudaFuncSetAttribute(k_eta_dist3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    k_eta_dist3<<<grid_for(I.g.ncells, 128, 148 * 32), 128, sm, stream>>>(I, seeds, grain, eta);
+    if (sm > kSeedSmemMax) {
+        k_eta_dist3<false><<<grid_for(I.g.ncells, 128, 148 * 32), 128, 0, stream>>>(I, seeds, grain, eta);
+        return;
+    }
+    if (sm > 48 * 1024) cudaFuncSetAttribute(k_eta_dist3<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k_eta_dist3<true><<<grid_for(I.g.ncells, 128, 148 * 32), 128, sm, stream>>>(I, seeds, grain, eta);
 }
 void launch_center_seed(const InitParams& I, double cx, double cy, double cz, double r, int neta, double* o,
                         double* cr, double* p, double* eta, StepPartial* partials, cudaStream_t stream,

@@ -50,7 +50,9 @@ CASES = [
 @pytest.mark.parametrize("dim,mode,bc,precision,shape", CASES)
 def test_noalloc_matches_handle_step_twice(require_gpu, dim, mode, bc, precision, shape):
     import torch
-    kw = dict(nx=shape[0], ny=shape[1], grains=0 if mode == "single" else 1, grain_diameter_grid=12.,
+    # ~300 grains on the long grid (the Voronoi initialisation is O(cells x grains))
+    diameter = 12. if np.prod(shape) < 1e6 else 60.
+    kw = dict(nx=shape[0], ny=shape[1], grains=0 if mode == "single" else 1, grain_diameter_grid=diameter,
               grain_evolution=1 if mode == "evolving" else 0, bc=bc, ck="legacy", bounds="legacy",
               nucleation="off", dt=1e-12, precision=precision)
     if dim == 3:
