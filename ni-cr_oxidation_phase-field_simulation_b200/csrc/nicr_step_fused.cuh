@@ -6,11 +6,14 @@
 // Per CTA: a 16 x 32 tile (512 threads, one CTA per SM) marching along its X
 // chunk. o, cr and phi are staged as in k_step_main (register prefetch into
 // shared-memory rings). The N eta fields of each plane are staged by TMA
-// (cp.async.bulk.tensor, nine boxes: the tile, the two wrapped halo rows, the
-// two 2-column halo strips and the four corners, all N fields at once) into a
-// three-plane ring whose slots complete on mbarriers; the copy of plane x+2
-// is issued at the top of the iteration that updates plane x-1+1... one plane
-// ahead of its use. From the staged plane of the lead plane x every thread
+// (cp.async.bulk.tensor, five boxes per field: the tile, the two wrapped halo
+// rows and the two 2-column halo strips, issued by one lane per field) into a
+// three-plane ring whose slots complete on mbarriers; the four halo corners of
+// each field (4N values) are copied by 4N threads. Each field's tile and halo
+// form one block at a fixed stride, so every stencil read is a shared load at
+// a per-thread base plus a compile-time offset. The copy of plane u+2 is
+// issued at the top of the iteration that updates plane u, one plane ahead of
+// its use. From the staged plane of the lead plane x every thread
 // rebuilds S = sum eta^2 and the GB mask gb = scale*min(1,16*pairs) at its own
 // point and, for the first 100 threads, at one halo-ring point, in
 // rebuild_eta_mask's order, so the mobilities of the lead plane need no gb
@@ -25,8 +28,8 @@
 // phi twice. The handle's gb and eta_s2 arrays are not written; the model
 // rebuilds them (k_eta_mask) when something reads them.
 //
-// Shared memory at N = 8: 105.6 KB of step staging + 3 x 41.5 KB of eta
-// slots = 225 KB, so N <= 8 and one CTA per SM. Grids: rows a multiple of 16,
+// Shared memory at N = 8: 102.8 KB of step staging + 3 x 42 KB of eta slots
+// = 226 KB, so N <= 8 and one CTA per SM. Grids: rows a multiple of 16,
 // columns a multiple of 32 (whole tiles, so every TMA box and its x
 // coordinate, b0, b0 - 2, b0 + 32, nb - 2 or 0, is a multiple of two doubles).
 // Every mbarrier wait is bounded; a wait that runs out sets st->timeout and
@@ -42,37 +45,34 @@ constexpr int kFusedMaxEta = 8;
 template <int N>
 struct FusedLayout {
     static constexpr int TA = FTA, TB = FTB, NT = TA * TB;
-    // eta slot regions (doubles), each a 128-byte multiple: tile [N][TA][TB],
-    // top and bottom halo rows [N][TB], left and right strips [N][TA][2]
-    // (columns b0-2, b0-1 and b0+32, b0+33), four corners [N][2]
-    static constexpr int INT = N * NT, ROW = N * TB, COL = N * TA * 2, CRN = ((2 * N + 15) / 16) * 16;
-    static constexpr int O_TOP = INT, O_BOT = O_TOP + ROW, O_LFT = O_BOT + ROW, O_RGT = O_LFT + COL;
-    static constexpr int O_TL = O_RGT + COL, O_TR = O_TL + CRN, O_BL = O_TR + CRN, O_BR = O_BL + CRN;
-    static constexpr int SLOT = O_BR + CRN;
-    static constexpr unsigned TX_BYTES = (unsigned)(INT + 2 * ROW + 2 * COL + 4 * 2 * N) * 8u;
+    // One field's block in an eta slot (doubles; the four TMA regions start on
+    // 128-byte boundaries): tile [TA][TB], top and bottom halo rows [TB], left
+    // and right strips [TA][2] (columns b0-2, b0-1 and b0+32, b0+33), the four
+    // corners (-1,-1), (-1,TB), (TA,-1), (TA,TB); FS doubles per field.
+    static constexpr int O_TOP = NT, O_BOT = O_TOP + TB, O_LFT = O_BOT + TB, O_RGT = O_LFT + 2 * TA;
+    static constexpr int O_CRN = O_RGT + 2 * TA;
+    static constexpr int FS = (O_CRN + 4 + 15) / 16 * 16;
+    static constexpr int SLOT = N * FS;
+    static constexpr unsigned TX_BYTES = (unsigned)N * (NT + 2 * TB + 4 * TA) * 8u;   // the TMA boxes of a slot
     static constexpr int RING = 3;
     using T = Tile<3, TA, TB>;
-    static constexpr size_t STEP_BYTES = (T::SMEM_BYTES + 127) / 128 * 128;
+    // step staging (T::SMEM_DOUBLES) + the block reduction's scratch (32 warps x 5 DD + counts)
+    static constexpr size_t STEP_BYTES = ((size_t)T::SMEM_DOUBLES * 8 + 32 * (5 * 16 + 8) + 127) / 128 * 128;
     static constexpr size_t BYTES = STEP_BYTES + 128 + (size_t)RING * SLOT * 8;
-    static_assert(STEP_BYTES % 128 == 0 && SLOT % 16 == 0, "eta slots must stay 128-byte aligned");
+    static_assert(O_TOP % 16 == 0 && O_BOT % 16 == 0 && O_LFT % 16 == 0 && O_RGT % 16 == 0 && FS % 16 == 0,
+                  "TMA destinations must stay 128-byte aligned");
 };
 
-__device__ __forceinline__ void tma_load_4d_c(void* dst, const CUtensorMap* map, int x, int y, int z,
-                                              unsigned long long* bar) {
-    tma_load_4d(dst, map, x, y, z, 0, bar);
-}
-
-// Offset and field stride of a point of the tile + halo ring within an eta slot.
+// Offset of a point of the tile + halo ring within a field's block of an eta
+// slot (field q of the slot at q * FS from it).
 template <int N>
-__device__ __forceinline__ void eta_slot_point(int a, int b, int& off, int& stride) {
+__device__ __forceinline__ int eta_slot_point(int a, int b) {
     using L = FusedLayout<N>;
     constexpr int TA = L::TA, TB = L::TB;
-    if (a >= 0 && a < TA && b >= 0 && b < TB) { off = a * TB + b; stride = L::NT; return; }
-    if (b >= 0 && b < TB) { off = (a < 0 ? L::O_TOP : L::O_BOT) + b; stride = TB; return; }
-    if (a >= 0 && a < TA) { off = (b < 0 ? L::O_LFT + a * 2 + 1 : L::O_RGT + a * 2); stride = 2 * TA; return; }
-    if (a < 0) off = b < 0 ? L::O_TL + 1 : L::O_TR;
-    else off = b < 0 ? L::O_BL + 1 : L::O_BR;
-    stride = 2;
+    if (a >= 0 && a < TA && b >= 0 && b < TB) return a * TB + b;
+    if (b >= 0 && b < TB) return (a < 0 ? L::O_TOP : L::O_BOT) + b;
+    if (a >= 0 && a < TA) return b < 0 ? L::O_LFT + a * 2 + 1 : L::O_RGT + a * 2;
+    return L::O_CRN + (a < 0 ? 0 : 2) + (b < 0 ? 0 : 1);
 }
 
 template <bool FAST, int N>
@@ -83,11 +83,11 @@ struct OnePassStep {
     static constexpr int TA = FTA, TB = FTB, NT = L::NT;
 
     // S and the GB mask of one point from a staged eta plane (rebuild_eta_mask order)
-    __device__ static double mask_at(const StepParams& P, const double* slot, int off, int stride, double& S) {
+    __device__ static double mask_at(const StepParams& P, const double* slot, int off, double& S) {
         double s = 0., pairs = 0.;
 #pragma unroll
         for (int q = 0; q < N; ++q) {
-            const double e = slot[off + q * stride];
+            const double e = slot[off + q * L::FS];
             const double sq = e * e;
             pairs += s * sq;
             s += sq;
@@ -116,7 +116,7 @@ struct OnePassStep {
     }
 
     __device__ static void run(const StepParams& P, const CUtensorMap* m_int, const CUtensorMap* m_row,
-                               const CUtensorMap* m_col, const CUtensorMap* m_crn, const double* __restrict__ o,
+                               const CUtensorMap* m_col, const double* __restrict__ eta, const double* __restrict__ o,
                                const double* __restrict__ cr, const double* __restrict__ p, double* __restrict__ on,
                                double* __restrict__ crn, double* __restrict__ pn, double* __restrict__ eta_next,
                                StepPartial* __restrict__ partials, Status* st) {
@@ -132,8 +132,10 @@ struct OnePassStep {
         double* smc = smo + 2 * T::S1;
         DD* sdd = reinterpret_cast<DD*>(smc + 2 * T::S1);
         long long* scnt = reinterpret_cast<long long*>(sdd + 32 * 5);
+        // the eta ring on a 128-byte boundary (an offset from the shared array, so
+        // the compiler keeps shared-memory addressing)
         double* ering = reinterpret_cast<double*>(
-            ((unsigned long long)(fused_smem + L::STEP_BYTES) + 127ull) & ~127ull);
+            fused_smem + L::STEP_BYTES + ((128u - (smem_u32(fused_smem + L::STEP_BYTES) & 127u)) & 127u));
 
         if (st->failed) return;   // a previous step of this batch was rejected
 
@@ -149,21 +151,33 @@ struct OnePassStep {
         const int ytop = a0 == 0 ? g.na - 1 : a0 - 1, ybot = a0 + TA == g.na ? 0 : a0 + TA;
         const int xl = b0 == 0 ? g.nb - 2 : b0 - 2, xr = b0 + TB == g.nb ? 0 : b0 + TB;
         auto eslot = [&](int q) { return ering + (size_t)((q - i0 + 1) % L::RING) * L::SLOT; };
-        auto issue = [&](int q) {   // one thread
+        // warp 0: lane 0 registers the slot's bytes on its mbarrier, then lane
+        // q < N copies field q's five boxes; threads 32 .. 32 + 4N - 1 copy the
+        // corners (plain loads and stores, ordered by the next barrier)
+        auto issue = [&](int q) {
             const int xg = q < 0 ? 0 : (q > g.nx - 1 ? g.nx - 1 : q);
             double* s = eslot(q);
-            unsigned long long* bar = &bars[(q - i0 + 1) % L::RING];
-            asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-            mbar_expect_tx(bar, L::TX_BYTES);
-            tma_load_4d_c(s, m_int, b0, a0, xg, bar);
-            tma_load_4d_c(s + L::O_TOP, m_row, b0, ytop, xg, bar);
-            tma_load_4d_c(s + L::O_BOT, m_row, b0, ybot, xg, bar);
-            tma_load_4d_c(s + L::O_LFT, m_col, xl, a0, xg, bar);
-            tma_load_4d_c(s + L::O_RGT, m_col, xr, a0, xg, bar);
-            tma_load_4d_c(s + L::O_TL, m_crn, xl, ytop, xg, bar);
-            tma_load_4d_c(s + L::O_TR, m_crn, xr, ytop, xg, bar);
-            tma_load_4d_c(s + L::O_BL, m_crn, xl, ybot, xg, bar);
-            tma_load_4d_c(s + L::O_BR, m_crn, xr, ybot, xg, bar);
+            if (tid < 32) {
+                unsigned long long* bar = &bars[(q - i0 + 1) % L::RING];
+                if (tid == 0) {
+                    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+                    mbar_expect_tx(bar, L::TX_BYTES);
+                }
+                __syncwarp();
+                if (tid < N) {
+                    double* f = s + tid * L::FS;
+                    tma_load_4d(f, m_int, b0, a0, xg, tid, bar);
+                    tma_load_4d(f + L::O_TOP, m_row, b0, ytop, xg, tid, bar);
+                    tma_load_4d(f + L::O_BOT, m_row, b0, ybot, xg, tid, bar);
+                    tma_load_4d(f + L::O_LFT, m_col, xl, a0, xg, tid, bar);
+                    tma_load_4d(f + L::O_RGT, m_col, xr, a0, xg, tid, bar);
+                }
+            } else if (tid < 32 + 4 * N) {
+                const int c = tid - 32, f = c >> 2, k = c & 3;
+                const int yy = k < 2 ? ytop : ybot, zz = (k & 1) ? xr : xl + 1;
+                s[f * L::FS + L::O_CRN + k] =
+                    __ldg(eta + (long long)f * g.nstore + (long long)xg * g.plane + (long long)yy * g.pb + zz);
+            }
         };
         bool ok = true;
         auto wait = [&](int q) {
@@ -179,22 +193,19 @@ struct OnePassStep {
         }
         __syncthreads();
         int issued = i0 + 1;   // last plane whose copy was issued
-        if (tid == 0)
-            for (int q = i0 - 1; q <= i0 + 1; ++q) issue(q);
+        for (int q = i0 - 1; q <= i0 + 1; ++q) issue(q);
+        __syncthreads();   // the corner stores of the first three planes
 
         // per-thread positions in an eta slot: own point and its four in-plane
         // neighbours; the halo-ring point of the first S1 - NT threads
         const int e_own = ta * TB + tb;
-        int am_o, am_s, ap_o, ap_s, bm_o, bm_s, bp_o, bp_s;
-        eta_slot_point<N>(ta - 1, tb, am_o, am_s);
-        eta_slot_point<N>(ta + 1, tb, ap_o, ap_s);
-        eta_slot_point<N>(ta, tb - 1, bm_o, bm_s);
-        eta_slot_point<N>(ta, tb + 1, bp_o, bp_s);
-        int ring_o = 0, ring_s = 0;
+        const int am_o = eta_slot_point<N>(ta - 1, tb), ap_o = eta_slot_point<N>(ta + 1, tb);
+        const int bm_o = eta_slot_point<N>(ta, tb - 1), bp_o = eta_slot_point<N>(ta, tb + 1);
+        int ring_o = 0;
         if (offs.gl[1] >= 0) {
             int a, b;
             SK::ring_point(tid, a, b);
-            eta_slot_point<N>(a, b, ring_o, ring_s);
+            ring_o = eta_slot_point<N>(a, b);
         }
 
         DD acc[5] = {{0., 0.}, {0., 0.}, {0., 0.}, {0., 0.}, {0., 0.}};  // ckO ckCr clipO clipCr bcO
@@ -211,7 +222,7 @@ struct OnePassStep {
         auto lead = [&](int x, double& S_own, double& gb_own) -> CenterVals {
             const double* es = eslot(x);
             double gbl[2];
-            gbl[0] = mask_at(P, es, e_own, NT, S_own);
+            gbl[0] = mask_at(P, es, e_own, S_own);
             gb_own = gbl[0];
             const double *som = oslot(x - 1), *so0 = oslot(x), *sop = oslot(x + 1);
             const double *scm = cslot(x - 1), *sc0 = cslot(x), *scp = cslot(x + 1);
@@ -224,7 +235,7 @@ struct OnePassStep {
                                             gbl[0]);
             if (offs.gl[1] >= 0) {
                 double Sr;
-                gbl[1] = mask_at(P, es, ring_o, ring_s, Sr);
+                gbl[1] = mask_at(P, es, ring_o, Sr);
                 int a, b;
                 SK::ring_point(tid, a, b);
                 SK::lead_point(P, nullptr, som, so0, sop, scm, sc0, scp, spx, mO, mC, mo_, mc_, a, b, gbl[1]);
@@ -272,7 +283,7 @@ struct OnePassStep {
         {
             const double* es = eslot(i0 - 1);   // plane i0 - 1 (plane 0, the Neumann ghost, when i0 = 0)
 #pragma unroll
-            for (int q = 0; q < N; ++q) ep[q] = es[e_own + q * NT];
+            for (int q = 0; q < N; ++q) ep[q] = es[e_own + q * L::FS];
         }
 
         typename SK::Prefetch pf;
@@ -287,7 +298,7 @@ struct OnePassStep {
                 // of the eta slot the copy of plane u+2 overwrites
                 if (__syncthreads_or(!ok)) break;
                 if (u + 2 <= i1) {
-                    if (tid == 0) issue(u + 2);
+                    issue(u + 2);
                     issued = u + 2;
                 }
                 if (x + 1 <= g.nx - 1 && u + 1 < i1) fetch_ocp(P, o, cr, p, x + 2, x + 1, offs, pf);
@@ -400,10 +411,11 @@ struct OnePassStep {
                 const double* en = eslot(u + 1);
 #pragma unroll
                 for (int q = 0; q < N; ++q) {
-                    const double c0 = es[e_own + q * NT];
-                    const double lap = fdiv<FAST>((en[e_own + q * NT] - 2. * c0 + ep[q]), P.v_dxdx)
-                                     + fdiv<FAST>((es[ap_o + q * ap_s] - 2. * c0 + es[am_o + q * am_s]), P.v_dada)
-                                     + fdiv<FAST>((es[bp_o + q * bp_s] - 2. * c0 + es[bm_o + q * bm_s]), P.v_dbdb);
+                    const int fq = q * L::FS;
+                    const double c0 = es[e_own + fq];
+                    const double lap = fdiv<FAST>((en[e_own + fq] - 2. * c0 + ep[q]), P.v_dxdx)
+                                     + fdiv<FAST>((es[ap_o + fq] - 2. * c0 + es[am_o + fq]), P.v_dada)
+                                     + fdiv<FAST>((es[bp_o + fq] - 2. * c0 + es[bm_o + fq]), P.v_dbdb);
                     const double force = grain_deta(c0, s2u, pp, P.eta_W, P.eta_A) - P.eta_K * lap;
                     const double v = c0 - P.dt_etaL * force;
                     if (!isfinite(v) || v < -1.e-12 || v > 1. + 1.e-12)
@@ -446,11 +458,11 @@ struct OnePassStep {
 template <bool FAST, int N>
 __global__ void __launch_bounds__(FTA * FTB, 1)
 k_step_fused(const StepParams P, const __grid_constant__ CUtensorMap m_int, const __grid_constant__ CUtensorMap m_row,
-             const __grid_constant__ CUtensorMap m_col, const __grid_constant__ CUtensorMap m_crn,
+             const __grid_constant__ CUtensorMap m_col, const double* __restrict__ eta,
              const double* __restrict__ o, const double* __restrict__ cr, const double* __restrict__ p,
              double* __restrict__ on, double* __restrict__ crn, double* __restrict__ pn,
              double* __restrict__ eta_next, StepPartial* __restrict__ partials, Status* st) {
-    OnePassStep<FAST, N>::run(P, &m_int, &m_row, &m_col, &m_crn, o, cr, p, on, crn, pn, eta_next, partials, st);
+    OnePassStep<FAST, N>::run(P, &m_int, &m_row, &m_col, eta, o, cr, p, on, crn, pn, eta_next, partials, st);
 }
 
 // Whether the fused step serves grid g with n eta fields (the eta buffer's
@@ -464,14 +476,14 @@ static bool launch_step_fused_n(const StepParams& P, const double* o, const doub
                                 const double* eta, double* on, double* crn, double* pn, double* eta_next,
                                 StepPartial* partials, Status* st, cudaStream_t stream, int* nblocks_out) {
     const Grid& g = P.g;
-    CUtensorMap mi, mr, mc, mk;
-    if (!encode_eta_map(&mi, g, N, eta, FTB, FTA) || !encode_eta_map(&mr, g, N, eta, FTB, 1) ||
-        !encode_eta_map(&mc, g, N, eta, 2, FTA) || !encode_eta_map(&mk, g, N, eta, 2, 1))
+    CUtensorMap mi, mr, mc;
+    if (!encode_eta_map(&mi, g, N, eta, FTB, FTA, 1) || !encode_eta_map(&mr, g, N, eta, FTB, 1, 1) ||
+        !encode_eta_map(&mc, g, N, eta, 2, FTA, 1))
         return false;
     using L = FusedLayout<N>;
     ensure_smem_attr((const void*)k_step_fused<FAST, N>, (int)L::BYTES);
     const dim3 grid(g.nb / FTB, g.na / FTA, (g.nx + P.xchunk - 1) / P.xchunk);
-    k_step_fused<FAST, N><<<grid, dim3(FTB, FTA), L::BYTES, stream>>>(P, mi, mr, mc, mk, o, cr, p, on, crn, pn,
+    k_step_fused<FAST, N><<<grid, dim3(FTB, FTA), L::BYTES, stream>>>(P, mi, mr, mc, eta, o, cr, p, on, crn, pn,
                                                                       eta_next, partials, st);
     if (nblocks_out) *nblocks_out = (int)(grid.x * grid.y * grid.z);
     return true;

@@ -1016,13 +1016,14 @@ static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
 }
 
 // The N eta fields of one buffer as a 4D tensor (columns, rows, planes,
-// fields), boxes of bx x by x 1 x N.
-static bool encode_eta_map(CUtensorMap* m, const Grid& g, int n, const double* eta, unsigned bx, unsigned by) {
+// fields), boxes of bx x by x 1 x bw (bw = N: every field at once).
+static bool encode_eta_map(CUtensorMap* m, const Grid& g, int n, const double* eta, unsigned bx, unsigned by,
+                           unsigned bw) {
     const auto enc = tensor_map_encoder();
     if (!enc) return false;
     const cuuint64_t dims[4] = {(cuuint64_t)g.nb, (cuuint64_t)g.na, (cuuint64_t)g.nx, (cuuint64_t)n};
     const cuuint64_t strides[3] = {(cuuint64_t)g.pb * 8, (cuuint64_t)g.plane * 8, (cuuint64_t)g.nstore * 8};
-    const cuuint32_t box[4] = {bx, by, 1, (cuuint32_t)n};
+    const cuuint32_t box[4] = {bx, by, 1, bw};
     const cuuint32_t estr[4] = {1, 1, 1, 1};
     return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, const_cast<double*>(eta), dims, strides, box, estr,
                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
@@ -1035,8 +1036,8 @@ static bool launch_eta_tma_n(const StepParams& P, const double* eta, const doubl
                              double* gb_next, double* s2_next, Status* st, cudaStream_t stream) {
     const Grid& g = P.g;
     CUtensorMap mi, mr, mc;
-    if (!encode_eta_map(&mi, g, N, eta, 32, 8) || !encode_eta_map(&mr, g, N, eta, 32, 1) ||
-        !encode_eta_map(&mc, g, N, eta, 2, 8))
+    if (!encode_eta_map(&mi, g, N, eta, 32, 8, N) || !encode_eta_map(&mr, g, N, eta, 32, 1, N) ||
+        !encode_eta_map(&mc, g, N, eta, 2, 8, N))
         return false;
     const size_t smem = TmaStage<N>::SMEM;
     ensure_smem_attr((const void*)k_eta_tma<FAST, N>, (int)smem);
