@@ -7,11 +7,11 @@
 // chunk. o, cr and phi are staged as in k_step_main (register prefetch into
 // shared-memory rings). The N eta fields of each plane are staged by TMA
 // (cp.async.bulk.tensor, five boxes per field: the tile, the two wrapped halo
-// rows and the two 2-column halo strips, issued by one lane per field) into a
-// three-plane ring whose slots complete on mbarriers; the four halo corners of
-// each field (4N values) are copied by 4N threads. Each field's tile and halo
-// form one block at a fixed stride, so every stencil read is a shared load at
-// a per-thread base plus a compile-time offset. The copy of plane u+2 is
+// rows and the two 2-column halo strips, issued by one lane per field, and
+// four corner boxes of all fields) into a three-plane ring whose slots
+// complete on mbarriers. Each field's tile and halo form one block at a fixed
+// stride, so every stencil read is a shared load at a per-thread base plus a
+// compile-time offset. The copy of plane u+2 is
 // issued at the top of the iteration that updates plane u, one plane ahead of
 // its use. From the staged plane of the lead plane x every thread
 // rebuilds S = sum eta^2 and the GB mask gb = scale*min(1,16*pairs) at its own
@@ -39,40 +39,51 @@
 namespace nicr {
 namespace {
 
+// A field stride known at compile time (the own point's), converting like an int.
+template <int S>
+struct ConstStride {
+    __device__ __forceinline__ operator int() const { return S; }
+};
+
 constexpr int FTA = 16, FTB = 32;    // fused tile: 16 rows x 32 columns
 constexpr int kFusedMaxEta = 8;
 
 template <int N>
 struct FusedLayout {
     static constexpr int TA = FTA, TB = FTB, NT = TA * TB;
-    // One field's block in an eta slot (doubles; the four TMA regions start on
-    // 128-byte boundaries): tile [TA][TB], top and bottom halo rows [TB], left
-    // and right strips [TA][2] (columns b0-2, b0-1 and b0+32, b0+33), the four
-    // corners (-1,-1), (-1,TB), (TA,-1), (TA,TB); FS doubles per field.
+    // One field's block in an eta slot (doubles; every TMA region starts on a
+    // 128-byte boundary): tile [TA][TB], top and bottom halo rows [TB], left
+    // and right strips [TA][2] (columns b0-2, b0-1 and b0+32, b0+33); FS
+    // doubles per field. After the N blocks, the corners (-1,-1), (-1,TB),
+    // (TA,-1), (TA,TB) of all fields, one [N][2] box each (columns as the
+    // strips), CP doubles apart.
     static constexpr int O_TOP = NT, O_BOT = O_TOP + TB, O_LFT = O_BOT + TB, O_RGT = O_LFT + 2 * TA;
-    static constexpr int O_CRN = O_RGT + 2 * TA;
-    static constexpr int FS = (O_CRN + 4 + 15) / 16 * 16;
-    static constexpr int SLOT = N * FS;
-    static constexpr unsigned TX_BYTES = (unsigned)N * (NT + 2 * TB + 4 * TA) * 8u;   // the TMA boxes of a slot
+    static constexpr int FS = O_RGT + 2 * TA;
+    static constexpr int CP = (2 * N + 15) / 16 * 16;
+    static constexpr int O_CRN = N * FS;
+    static constexpr int SLOT = O_CRN + 4 * CP;
+    static constexpr unsigned TX_BYTES = (unsigned)N * (NT + 2 * TB + 4 * TA + 8) * 8u;   // the TMA boxes of a slot
     static constexpr int RING = 3;
     using T = Tile<3, TA, TB>;
     // step staging (T::SMEM_DOUBLES) + the block reduction's scratch (32 warps x 5 DD + counts)
     static constexpr size_t STEP_BYTES = ((size_t)T::SMEM_DOUBLES * 8 + 32 * (5 * 16 + 8) + 127) / 128 * 128;
     static constexpr size_t BYTES = STEP_BYTES + 128 + (size_t)RING * SLOT * 8;
-    static_assert(O_TOP % 16 == 0 && O_BOT % 16 == 0 && O_LFT % 16 == 0 && O_RGT % 16 == 0 && FS % 16 == 0,
-                  "TMA destinations must stay 128-byte aligned");
+    static_assert(O_TOP % 16 == 0 && O_BOT % 16 == 0 && O_LFT % 16 == 0 && O_RGT % 16 == 0 && FS % 16 == 0 &&
+                  CP % 16 == 0, "TMA destinations must stay 128-byte aligned");
 };
 
-// Offset of a point of the tile + halo ring within a field's block of an eta
-// slot (field q of the slot at q * FS from it).
+// Offset of a point of the tile + halo ring in an eta slot, field 0; field q
+// lies stride * q further (FS, or 2 for the corners).
 template <int N>
-__device__ __forceinline__ int eta_slot_point(int a, int b) {
+__device__ __forceinline__ int eta_slot_point(int a, int b, int& stride) {
     using L = FusedLayout<N>;
     constexpr int TA = L::TA, TB = L::TB;
+    stride = L::FS;
     if (a >= 0 && a < TA && b >= 0 && b < TB) return a * TB + b;
     if (b >= 0 && b < TB) return (a < 0 ? L::O_TOP : L::O_BOT) + b;
     if (a >= 0 && a < TA) return b < 0 ? L::O_LFT + a * 2 + 1 : L::O_RGT + a * 2;
-    return L::O_CRN + (a < 0 ? 0 : 2) + (b < 0 ? 0 : 1);
+    stride = 2;
+    return L::O_CRN + ((a < 0 ? 0 : 2) + (b < 0 ? 0 : 1)) * L::CP + (b < 0 ? 1 : 0);
 }
 
 template <bool FAST, int N>
@@ -83,11 +94,12 @@ struct OnePassStep {
     static constexpr int TA = FTA, TB = FTB, NT = L::NT;
 
     // S and the GB mask of one point from a staged eta plane (rebuild_eta_mask order)
-    __device__ static double mask_at(const StepParams& P, const double* slot, int off, double& S) {
+    template <typename Stride>
+    __device__ static double mask_at(const StepParams& P, const double* slot, int off, Stride stride, double& S) {
         double s = 0., pairs = 0.;
 #pragma unroll
         for (int q = 0; q < N; ++q) {
-            const double e = slot[off + q * L::FS];
+            const double e = slot[off + q * stride];
             const double sq = e * e;
             pairs += s * sq;
             s += sq;
@@ -116,7 +128,7 @@ struct OnePassStep {
     }
 
     __device__ static void run(const StepParams& P, const CUtensorMap* m_int, const CUtensorMap* m_row,
-                               const CUtensorMap* m_col, const double* __restrict__ eta, const double* __restrict__ o,
+                               const CUtensorMap* m_col, const CUtensorMap* m_crn, const double* __restrict__ o,
                                const double* __restrict__ cr, const double* __restrict__ p, double* __restrict__ on,
                                double* __restrict__ crn, double* __restrict__ pn, double* __restrict__ eta_next,
                                StepPartial* __restrict__ partials, Status* st) {
@@ -151,32 +163,29 @@ struct OnePassStep {
         const int ytop = a0 == 0 ? g.na - 1 : a0 - 1, ybot = a0 + TA == g.na ? 0 : a0 + TA;
         const int xl = b0 == 0 ? g.nb - 2 : b0 - 2, xr = b0 + TB == g.nb ? 0 : b0 + TB;
         auto eslot = [&](int q) { return ering + (size_t)((q - i0 + 1) % L::RING) * L::SLOT; };
-        // warp 0: lane 0 registers the slot's bytes on its mbarrier, then lane
-        // q < N copies field q's five boxes; threads 32 .. 32 + 4N - 1 copy the
-        // corners (plain loads and stores, ordered by the next barrier)
+        // the last warp: lane 0 registers the slot's bytes on its mbarrier, then
+        // lane q < N copies field q's five boxes and lanes N .. N+3 the corners
         auto issue = [&](int q) {
+            const int lane = tid - (NT - 32);
+            if (lane < 0) return;
             const int xg = q < 0 ? 0 : (q > g.nx - 1 ? g.nx - 1 : q);
             double* s = eslot(q);
-            if (tid < 32) {
-                unsigned long long* bar = &bars[(q - i0 + 1) % L::RING];
-                if (tid == 0) {
-                    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-                    mbar_expect_tx(bar, L::TX_BYTES);
-                }
-                __syncwarp();
-                if (tid < N) {
-                    double* f = s + tid * L::FS;
-                    tma_load_4d(f, m_int, b0, a0, xg, tid, bar);
-                    tma_load_4d(f + L::O_TOP, m_row, b0, ytop, xg, tid, bar);
-                    tma_load_4d(f + L::O_BOT, m_row, b0, ybot, xg, tid, bar);
-                    tma_load_4d(f + L::O_LFT, m_col, xl, a0, xg, tid, bar);
-                    tma_load_4d(f + L::O_RGT, m_col, xr, a0, xg, tid, bar);
-                }
-            } else if (tid < 32 + 4 * N) {
-                const int c = tid - 32, f = c >> 2, k = c & 3;
-                const int yy = k < 2 ? ytop : ybot, zz = (k & 1) ? xr : xl + 1;
-                s[f * L::FS + L::O_CRN + k] =
-                    __ldg(eta + (long long)f * g.nstore + (long long)xg * g.plane + (long long)yy * g.pb + zz);
+            unsigned long long* bar = &bars[(q - i0 + 1) % L::RING];
+            if (lane == 0) {
+                asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+                mbar_expect_tx(bar, L::TX_BYTES);
+            }
+            __syncwarp();
+            if (lane < N) {
+                double* f = s + lane * L::FS;
+                tma_load_4d(f, m_int, b0, a0, xg, lane, bar);
+                tma_load_4d(f + L::O_TOP, m_row, b0, ytop, xg, lane, bar);
+                tma_load_4d(f + L::O_BOT, m_row, b0, ybot, xg, lane, bar);
+                tma_load_4d(f + L::O_LFT, m_col, xl, a0, xg, lane, bar);
+                tma_load_4d(f + L::O_RGT, m_col, xr, a0, xg, lane, bar);
+            } else if (lane < N + 4) {
+                const int k = lane - N;
+                tma_load_4d(s + L::O_CRN + k * L::CP, m_crn, (k & 1) ? xr : xl, k < 2 ? ytop : ybot, xg, 0, bar);
             }
         };
         bool ok = true;
@@ -194,18 +203,18 @@ struct OnePassStep {
         __syncthreads();
         int issued = i0 + 1;   // last plane whose copy was issued
         for (int q = i0 - 1; q <= i0 + 1; ++q) issue(q);
-        __syncthreads();   // the corner stores of the first three planes
 
         // per-thread positions in an eta slot: own point and its four in-plane
         // neighbours; the halo-ring point of the first S1 - NT threads
         const int e_own = ta * TB + tb;
-        const int am_o = eta_slot_point<N>(ta - 1, tb), ap_o = eta_slot_point<N>(ta + 1, tb);
-        const int bm_o = eta_slot_point<N>(ta, tb - 1), bp_o = eta_slot_point<N>(ta, tb + 1);
-        int ring_o = 0;
+        int unused;
+        const int am_o = eta_slot_point<N>(ta - 1, tb, unused), ap_o = eta_slot_point<N>(ta + 1, tb, unused);
+        const int bm_o = eta_slot_point<N>(ta, tb - 1, unused), bp_o = eta_slot_point<N>(ta, tb + 1, unused);
+        int ring_o = 0, ring_s = L::FS;
         if (offs.gl[1] >= 0) {
             int a, b;
             SK::ring_point(tid, a, b);
-            ring_o = eta_slot_point<N>(a, b);
+            ring_o = eta_slot_point<N>(a, b, ring_s);
         }
 
         DD acc[5] = {{0., 0.}, {0., 0.}, {0., 0.}, {0., 0.}, {0., 0.}};  // ckO ckCr clipO clipCr bcO
@@ -222,7 +231,7 @@ struct OnePassStep {
         auto lead = [&](int x, double& S_own, double& gb_own) -> CenterVals {
             const double* es = eslot(x);
             double gbl[2];
-            gbl[0] = mask_at(P, es, e_own, S_own);
+            gbl[0] = mask_at(P, es, e_own, ConstStride<L::FS>(), S_own);
             gb_own = gbl[0];
             const double *som = oslot(x - 1), *so0 = oslot(x), *sop = oslot(x + 1);
             const double *scm = cslot(x - 1), *sc0 = cslot(x), *scp = cslot(x + 1);
@@ -235,7 +244,7 @@ struct OnePassStep {
                                             gbl[0]);
             if (offs.gl[1] >= 0) {
                 double Sr;
-                gbl[1] = mask_at(P, es, ring_o, Sr);
+                gbl[1] = mask_at(P, es, ring_o, ring_s, Sr);
                 int a, b;
                 SK::ring_point(tid, a, b);
                 SK::lead_point(P, nullptr, som, so0, sop, scm, sc0, scp, spx, mO, mC, mo_, mc_, a, b, gbl[1]);
@@ -318,7 +327,8 @@ struct OnePassStep {
                 const int bp = T::i1(ta, tb + 1), bm = T::i1(ta, tb - 1);
                 const int ap = T::i1(ta + 1, tb), am = T::i1(ta - 1, tb);
                 const long long gidx = (long long)u * g.plane + (long long)row * g.pb + col;
-                const long long cell = ((long long)u * g.na + row) * g.nb + col;   // reference loop order
+                // the cell's index in reference loop order, for failing-trial keys only
+                auto cell_of = [&]() { return ((long long)u * g.na + row) * g.nb + col; };
                 // Centre (plane u) and lead (plane x) values are read back from
                 // the staging rings rather than carried in registers across the
                 // iteration (the same doubles; fewer live registers). The ghost
@@ -389,7 +399,7 @@ struct OnePassStep {
                     if (dCr != 0.) acc[1] = dd_add(acc[1], dCr);
                 }
                 if (!isfinite(onv) || !isfinite(crv) || !isfinite(pnv)) {
-                    errkey = min(errkey, (unsigned long long)cell * 4ull);
+                    errkey = min(errkey, (unsigned long long)cell_of() * 4ull);
                 } else if (P.bounds == 1) {
                     const double oc = sclamp(onv, 0., 1.), ccr = sclamp(crv, 0., 1.);
                     const double clO = oc - onv, clCr = ccr - crv;
@@ -401,7 +411,7 @@ struct OnePassStep {
                     if (pnv < 1.e-5) pnv = 0.;
                 } else if (onv < -1.e-12 || crv < -1.e-12 || onv + crv > 1. + 1.e-12 || pnv < -1.e-12 ||
                            pnv > 1. + 1.e-12) {
-                    errkey = min(errkey, (unsigned long long)cell * 4ull + 1ull);
+                    errkey = min(errkey, (unsigned long long)cell_of() * 4ull + 1ull);
                 }
                 on[gidx] = onv; crn[gidx] = crv; pn[gidx] = pnv;
                 FxO = rightO; FxCr = rightCr;
@@ -409,6 +419,7 @@ struct OnePassStep {
                 // eta_trial (3S:514-526) at plane u: v = eta - (dt L_eta)(deta - K lap eta)
                 const double* es = eslot(u);
                 const double* en = eslot(u + 1);
+                double* edst = eta_next + gidx;
 #pragma unroll
                 for (int q = 0; q < N; ++q) {
                     const int fq = q * L::FS;
@@ -420,8 +431,9 @@ struct OnePassStep {
                     const double v = c0 - P.dt_etaL * force;
                     if (!isfinite(v) || v < -1.e-12 || v > 1. + 1.e-12)
                         errkey = min(errkey, ERR_ETA_BASE + (unsigned long long)q * (unsigned long long)g.ncells +
-                                                 (unsigned long long)cell);
-                    eta_next[(long long)q * g.nstore + gidx] = v;
+                                                 (unsigned long long)cell_of());
+                    *edst = v;
+                    edst += g.nstore;
                     ep[q] = c0;
                 }
                 pP = pp;   // a register: the ring slot of plane u-1 takes plane u+2 next
@@ -458,11 +470,11 @@ struct OnePassStep {
 template <bool FAST, int N>
 __global__ void __launch_bounds__(FTA * FTB, 1)
 k_step_fused(const StepParams P, const __grid_constant__ CUtensorMap m_int, const __grid_constant__ CUtensorMap m_row,
-             const __grid_constant__ CUtensorMap m_col, const double* __restrict__ eta,
+             const __grid_constant__ CUtensorMap m_col, const __grid_constant__ CUtensorMap m_crn,
              const double* __restrict__ o, const double* __restrict__ cr, const double* __restrict__ p,
              double* __restrict__ on, double* __restrict__ crn, double* __restrict__ pn,
              double* __restrict__ eta_next, StepPartial* __restrict__ partials, Status* st) {
-    OnePassStep<FAST, N>::run(P, &m_int, &m_row, &m_col, eta, o, cr, p, on, crn, pn, eta_next, partials, st);
+    OnePassStep<FAST, N>::run(P, &m_int, &m_row, &m_col, &m_crn, o, cr, p, on, crn, pn, eta_next, partials, st);
 }
 
 // Whether the fused step serves grid g with n eta fields (the eta buffer's
@@ -476,14 +488,14 @@ static bool launch_step_fused_n(const StepParams& P, const double* o, const doub
                                 const double* eta, double* on, double* crn, double* pn, double* eta_next,
                                 StepPartial* partials, Status* st, cudaStream_t stream, int* nblocks_out) {
     const Grid& g = P.g;
-    CUtensorMap mi, mr, mc;
+    CUtensorMap mi, mr, mc, mk;
     if (!encode_eta_map(&mi, g, N, eta, FTB, FTA, 1) || !encode_eta_map(&mr, g, N, eta, FTB, 1, 1) ||
-        !encode_eta_map(&mc, g, N, eta, 2, FTA, 1))
+        !encode_eta_map(&mc, g, N, eta, 2, FTA, 1) || !encode_eta_map(&mk, g, N, eta, 2, 1, N))
         return false;
     using L = FusedLayout<N>;
     ensure_smem_attr((const void*)k_step_fused<FAST, N>, (int)L::BYTES);
     const dim3 grid(g.nb / FTB, g.na / FTA, (g.nx + P.xchunk - 1) / P.xchunk);
-    k_step_fused<FAST, N><<<grid, dim3(FTB, FTA), L::BYTES, stream>>>(P, mi, mr, mc, eta, o, cr, p, on, crn, pn,
+    k_step_fused<FAST, N><<<grid, dim3(FTB, FTA), L::BYTES, stream>>>(P, mi, mr, mc, mk, o, cr, p, on, crn, pn,
                                                                       eta_next, partials, st);
     if (nblocks_out) *nblocks_out = (int)(grid.x * grid.y * grid.z);
     return true;
