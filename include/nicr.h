@@ -86,8 +86,20 @@ typedef struct nicr_config {
                                      two face-adjacent grains sharing one where
                                      K colours allow, with tanh profiles across
                                      the boundaries; no reference counterpart */
-    int reserved[4];
+    int step_form;                /* 3D evolving grains (no reference
+                                     counterpart): NICR_STEP_AUTO, NICR_STEP_ONEPASS
+                                     (one HBM pass: the step and the eta update in
+                                     one kernel, where the grid allows it) or
+                                     NICR_STEP_SPLIT (two kernels); the fields are
+                                     the same bit for bit in the drop-in form */
+    int reserved[3];
 } nicr_config;
+
+/* nicr_config.step_form. AUTO takes the one-pass kernel for the reciprocal
+ * form (NICR_FP64_FAST) and the two kernels for the drop-in form, the faster
+ * of each on B200; the environment variable NICR_STEP_FORM=onepass|split
+ * overrides every handle of the process (benchmarks). */
+enum { NICR_STEP_AUTO = 0, NICR_STEP_ONEPASS = 1, NICR_STEP_SPLIT = 2 };
 
 /* Fills the reference defaults for dim 2 or 3 (Config{} at 2D:39 / 3S:43). */
 void nicr_config_default(nicr_config* cfg, int dim);

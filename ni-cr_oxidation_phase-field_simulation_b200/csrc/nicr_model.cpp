@@ -897,12 +897,14 @@ bool Model::fused_step() const {
 }
 
 bool Model::onepass_step() const {
-    static int v = -1;
-    if (v < 0) {
+    static int env = -1;   // NICR_STEP_FORM: 1 onepass, 2 split, 0 unset
+    if (env < 0) {
         const char* e = getenv("NICR_STEP_FORM");
-        v = (e && e[0] == 's') ? 0 : 1;
+        env = (e && e[0] == 'o') ? NICR_STEP_ONEPASS : (e && e[0] == 's') ? NICR_STEP_SPLIT : 0;
     }
-    return v == 1 && !onepass_failed && dim == 3 && advance_eta && !is_slab && !fused_step() &&
+    const int form = env ? env : c.step_form;
+    const bool want = form == NICR_STEP_ONEPASS || (form == NICR_STEP_AUTO && sp.fast);
+    return want && !onepass_failed && dim == 3 && advance_eta && !is_slab && !fused_step() &&
            step_fused_applies(g, neta);
 }
 

@@ -189,8 +189,9 @@ public:
     // measured 1.122 vs 1.129 ms per step at 256^3 with 8 fields)
     bool fused_step() const;
     // One HBM pass per step (k_step_fused: 3D, 1..8 evolving eta fields, rows
-    // a multiple of 16, columns of 32): the default for the grids it serves;
-    // NICR_STEP_FORM=split selects the two-kernel form (A/B runs and tests).
+    // a multiple of 16, columns of 32) where nicr_config.step_form asks for it
+    // (AUTO: the reciprocal form only); NICR_STEP_FORM=onepass|split overrides
+    // every handle (A/B runs).
     // The pass rebuilds S and gb from eta on chip and writes neither, so the
     // handle's gb / eta_s2 arrays go stale (eta_dirty) and are rebuilt when read.
     bool onepass_step() const;

@@ -56,7 +56,8 @@ class NicrConfig(ctypes.Structure):
         ("device", ctypes.c_int),
         ("checkpoint_every", ctypes.c_int),
         ("eta_colours", ctypes.c_int),
-        ("reserved", ctypes.c_int * 4),
+        ("step_form", ctypes.c_int),
+        ("reserved", ctypes.c_int * 3),
     ]
 
 

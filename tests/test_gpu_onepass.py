@@ -7,6 +7,9 @@ columns a multiple of 32).
   wrap of every halo box onto the tile itself), several tiles, 1 to 8 eta
   fields, the three boundary conditions, O off, Ck on and off, a stamp across
   both periodic seams and Ksp scans, graph-replayed runs.
+The handles ask for the one-pass form (nicr_config.step_form = 1); the
+default (AUTO) takes it for the reciprocal form only.
+
 * Against the two-kernel form (NICR_STEP_FORM=split) in child processes,
   with forced X chunks of 1, 3 and 7 planes (chunk prologues, chunk ends at
   the ghost plane): drop-in fields bit-identical, reciprocal form within
@@ -36,7 +39,7 @@ STEP_FUSED = 8   # nicr_profile_read kernel index of the one-pass step
 
 def cfg_for(shape, **kw):
     base = dict(nx=shape[0], ny=shape[1], nz=shape[2], grains=1, grain_evolution=1, bounds="legacy",
-                nucleation="ksp", dt=1e-12, radius_grid=2.5)
+                nucleation="ksp", dt=1e-12, radius_grid=2.5, step_form=1)
     base.update(kw)
     return make_config(3, **base)
 
@@ -133,10 +136,10 @@ SPLIT_CASES = {
 def test_onepass_matches_two_kernel_form(require_gpu, tmp_path, name, precision):
     env, shape = SPLIT_CASES[name]
     cfg = dict(shape, grains=1, grain_evolution=1, bounds="legacy", bc="mu", ck="legacy", nucleation="ksp",
-               dt=1e-12, radius_grid=2.5, nucleation_period=6e-12, precision=precision)
+               dt=1e-12, radius_grid=2.5, nucleation_period=6e-12, precision=precision, step_form=1)
     case = {"cfg": cfg, "steps": 24}
     a, ja = run_child(tmp_path, "onepass", case, **env)
-    b, jb = run_child(tmp_path, "split", case, NICR_STEP_FORM="split", **env)
+    b, jb = run_child(tmp_path, "split", case, NICR_STEP_FORM="split", **env)   # overrides step_form
     assert ja["fused"] == 24 and jb["fused"] == 0
     assert ja["rcs"] == jb["rcs"] and ja["nuclei"] == jb["nuclei"] and ja["clipped"] == jb["clipped"]
     assert jb["nuclei"] > 0
