@@ -16,6 +16,7 @@
 // Distances are integer-valued: 3D compares sqrt(D) < r + gap with IEEE sqrt
 // like the reference; 2D uses the reference's C-library hypot, tabulated on
 // the host for the integer offsets that occur.
+#include <cmath>
 #include <cuda_runtime.h>
 #include "nicr_kernels.h"
 #include "nicr_ksp.h"
@@ -109,6 +110,88 @@ __global__ void k_ksp_candidates(const KspDev K, const double* __restrict__ o, c
             const int x = xi + K.x_off + 1;
             if (g.dim == 3) f = valid_prescan(K, p, x, row + 1, col + 1) ? 1 : 0;
             else f = valid_prescan(K, p, x, col + 1, 0) ? 1 : 0;
+        }
+        flag[c] = f;
+    }
+}
+
+// 3D pre-scan test by an exact, separable bounded distance transform instead
+// of a search of the (2 reach + 1)^3 exclusion box per candidate (whose cost
+// grows with the number of candidates: a supersaturated 256^3 grid has 16.7M).
+// valid_prescan rejects a candidate when some cell with phi > .01 lies in its
+// box (|di| <= reach in x within [1, nx]; |dj|, |dk| <= reach periodic) at
+// sqrt(di^2 + dj^2 + dk^2) < r + gap, with dj, dk minimum-image offsets. The
+// least di^2 + dj^2 + dk^2 over the box's occupied cells is computed in three
+// passes (z, then y, then x), each the minimum over the axis' offsets of
+// offset^2 plus the previous pass' value. Offsets that wrap a short axis twice
+// only add larger copies of the minimum-image distance, so the minimum is the
+// reference's; the distances are integers, so sqrt of the exact minimum
+// decides as the reference's first hit does.
+constexpr int kEdtInf = 1 << 29;
+
+__device__ __forceinline__ int wrap_axis(int v, int n) { v %= n; return v < 0 ? v + n : v; }
+
+__global__ void k_ksp_edt_z(const KspDev K, const double* __restrict__ p, int* __restrict__ dz2, int R, Status* st) {
+    if (st->failed) return;
+    const Grid& g = K.g;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < g.ncells; c += (long long)gridDim.x * blockDim.x) {
+        const int col = (int)(c % g.nb);
+        const long long r = c / g.nb;
+        const int row = (int)(r % g.na);
+        const int xi = (int)(r / g.na);
+        const double* base = p + (long long)xi * g.plane + (long long)row * g.pb;
+        int best = kEdtInf;
+        for (int d = -R; d <= R; ++d)
+            if (__ldg(base + wrap_axis(col + d, g.nb)) > .01) best = min(best, d * d);
+        dz2[c] = best;
+    }
+}
+
+__global__ void k_ksp_edt_y(const KspDev K, const int* __restrict__ dz2, int* __restrict__ dyz2, int R, Status* st) {
+    if (st->failed) return;
+    const Grid& g = K.g;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < g.ncells; c += (long long)gridDim.x * blockDim.x) {
+        const int col = (int)(c % g.nb);
+        const long long r = c / g.nb;
+        const int row = (int)(r % g.na);
+        const long long xi = r / g.na;
+        int best = kEdtInf;
+        for (int d = -R; d <= R; ++d) {
+            const int v = __ldg(dz2 + (xi * g.na + wrap_axis(row + d, g.na)) * g.nb + col);
+            if (v < kEdtInf) best = min(best, v + d * d);
+        }
+        dyz2[c] = best;
+    }
+}
+
+// The x pass with the point test (phi <= .01, o*cr > Ksp, own plane, the
+// reference's x-range test): the candidate flags.
+__global__ void k_ksp_candidates_edt(const KspDev K, const double* __restrict__ o, const double* __restrict__ cr,
+                                     const double* __restrict__ p, const int* __restrict__ dyz2, int R,
+                                     unsigned char* __restrict__ flag, Status* st) {
+    if (st->failed) return;
+    const Grid& g = K.g;
+    const double limit = K.radius + K.gap;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < g.ncells; c += (long long)gridDim.x * blockDim.x) {
+        const int col = (int)(c % g.nb);
+        const long long r = c / g.nb;
+        const int row = (int)(r % g.na);
+        const int xi = (int)(r / g.na);
+        const long long idx = (long long)xi * g.plane + (long long)row * g.pb + col;
+        unsigned char f = 0;
+        const double pv = __ldg(p + idx);
+        if (xi >= K.x_lo && xi < K.x_hi && pv <= .01 && __ldg(o + idx) * __ldg(cr + idx) > K.ksp) {
+            const int x = xi + K.x_off + 1;
+            if (!(x - K.radius < 5. || x + K.radius > (double)(K.nx - 3))) {
+                int best = kEdtInf;
+                for (int d = -R; d <= R; ++d) {
+                    const int xd = x + d, li = xd - 1 - K.x_off;
+                    if (xd < 1 || xd > K.nx || li < 0 || li >= g.nx) continue;
+                    const int v = __ldg(dyz2 + ((long long)li * g.na + row) * g.nb + col);
+                    if (v < kEdtInf) best = min(best, v + d * d);
+                }
+                f = (best < kEdtInf && sqrt((double)best) < limit) ? 0 : 1;
+            }
         }
         flag[c] = f;
     }
@@ -297,6 +380,7 @@ __global__ void __launch_bounds__(1024) k_ksp_resolve(const KspDev K, const long
     if (st->failed) return;
     __shared__ long long s_cand;
     __shared__ int s_next;
+    __shared__ int s_first[32];
     __shared__ DD s_dd[32][2];
     __shared__ int s_cnt[32];
     const Grid& g = K.g;
@@ -312,37 +396,47 @@ __global__ void __launch_bounds__(1024) k_ksp_resolve(const KspDev K, const long
     }
     const int n = mode == 2 ? 0 : (forced ? 1 : *total);
     int pos = 0, accepted = 0, last_cells = 0, listed = 0;
+    const int nw = (int)(blockDim.x >> 5);
     while (mode != 2) {
-        // warp 0 finds the next accepted candidate from pos (32 at a time)
-        if (w == 0) {
-            int found = -1;
-            while (pos < n && found < 0) {
-                const int q = pos + lane;
+        // the whole CTA looks at the next blockDim.x candidates from pos; the
+        // first (lowest index) that is neither excluded nor stamped since the
+        // pre-scan is the next nucleus
+        int found = -1;
+        if (forced) {
+            found = pos < n ? 0 : -1;
+        } else {
+            while (pos < n) {
+                const int q = pos + tid;
                 bool ok = false;
-                long long cq = 0;
                 if (q < n) {
-                    if (forced) ok = true;
-                    else {
-                        cq = list[q];
-                        const int col = (int)(cq % g.nb);
-                        const long long rr = cq / g.nb;
-                        const int row = (int)(rr % g.na);
-                        const int xi = (int)(rr / g.na);
-                        const long long idx = (long long)xi * g.plane + (long long)row * g.pb + col;
-                        ok = !blocked[cq] && p[idx] <= .01;
-                    }
+                    const long long cq = list[q];
+                    const int col = (int)(cq % g.nb);
+                    const long long rr = cq / g.nb;
+                    const int row = (int)(rr % g.na);
+                    const int xi = (int)(rr / g.na);
+                    const long long idx = (long long)xi * g.plane + (long long)row * g.pb + col;
+                    ok = !blocked[cq] && p[idx] <= .01;
                 }
                 const unsigned b = __ballot_sync(0xffffffffu, ok);
-                if (b) found = pos + __ffs(b) - 1;
-                else pos += 32;
-            }
-            if (lane == 0) {
-                s_next = found;
-                s_cand = found >= 0 ? (forced ? -1 : list[found]) : -1;
+                if (lane == 0) s_first[w] = b ? w * 32 + __ffs(b) - 1 : 0x7fffffff;
+                __syncthreads();
+                if (w == 0) {
+                    int v = lane < nw ? s_first[lane] : 0x7fffffff;
+                    for (int off = 16; off > 0; off >>= 1) v = min(v, __shfl_down_sync(0xffffffffu, v, off));
+                    if (lane == 0) s_next = v;
+                }
+                __syncthreads();
+                const int first = s_next;
+                __syncthreads();   // s_first and s_next are rewritten in the next round
+                if (first != 0x7fffffff) {
+                    found = pos + first;
+                    break;
+                }
+                pos += (int)blockDim.x;
             }
         }
+        if (tid == 0) s_cand = found >= 0 ? (forced ? -1 : list[found]) : -1;
         __syncthreads();
-        const int found = s_next;
         if (found < 0) break;
         pos = found + 1;
         int x, y, z = 0;
@@ -411,7 +505,20 @@ void launch_ksp_candidates(const KspDev& K, const double* o, const double* cr, c
                            Status* st, cudaStream_t stream) {
     const long long n = K.g.ncells;
     cudaMemsetAsync(W.blocked, 0, (size_t)n, stream);
-    k_ksp_candidates<<<cgrid(n, 128, 148 * 64), 128, 0, stream>>>(K, o, cr, p, W.flag, st);
+    if (K.g.dim == 3) {
+        // the two distance arrays live in the candidate list's storage (8 bytes
+        // per cell), which the compaction below overwrites afterwards
+        int* dz2 = reinterpret_cast<int*>(W.list);
+        int* dyz2 = dz2 + n;
+        const double limit = K.radius + K.gap;
+        auto reach = [&](int m) { return limit >= m ? m : (int)std::ceil(limit); };
+        const int blocks = cgrid(n, 256, 148 * 16);
+        k_ksp_edt_z<<<blocks, 256, 0, stream>>>(K, p, dz2, reach(K.nz), st);
+        k_ksp_edt_y<<<blocks, 256, 0, stream>>>(K, dz2, dyz2, reach(K.ny), st);
+        k_ksp_candidates_edt<<<blocks, 256, 0, stream>>>(K, o, cr, p, dyz2, reach(K.nx), W.flag, st);
+    } else {
+        k_ksp_candidates<<<cgrid(n, 128, 148 * 64), 128, 0, stream>>>(K, o, cr, p, W.flag, st);
+    }
     const int nb = ksp_compact_blocks(n);
     k_ksp_count<<<nb, CBLK, 0, stream>>>(W.flag, n, W.counts);
     k_ksp_write<<<nb, CBLK, 0, stream>>>(W.flag, n, W.counts, W.list, W.total, nb);
