@@ -147,6 +147,23 @@ struct StepBatch {
 // returns the number of launches
 int launch_step_batch(BatchDomain* doms, int n, cudaStream_t stream);
 void launch_batch_group_fast(StepBatch& B, int nblocks, int dim, cudaStream_t stream);
+// The batched step of any number of domains of one dimensionality and form
+// in one launch, its descriptors in device memory: table holds two entries
+// per domain (buffer parity 0, then 1), block0 the first block of each
+// domain (nblocks in all); bit d of parity selects domain d's entry. Each
+// block copies its domain's parameters to shared memory and runs the CTA the
+// single-domain launch would run.
+constexpr int kBatchParityWords = 16;   // up to 512 domains
+struct BatchTableLaunch {
+    const BatchDomain* table;
+    const int* block0;
+    int n, nblocks;
+    unsigned parity[kBatchParityWords];
+};
+void launch_step_batch_table(const BatchTableLaunch& L, int dim, bool fast, cudaStream_t stream);
+void launch_step_batch_table_fast(const BatchTableLaunch& L, int dim, cudaStream_t stream);
+// step_grid of P's kernel: (x, y) blocks per X chunk and the total block count
+void step_grid_dims(const StepParams& P, int* gx, int* gy, int* nblocks);
 
 // One launch for the step kernel and the eta update of one step (reciprocal
 // form, 3D, 1..16 eta fields): the two are independent within a step, and

@@ -398,6 +398,19 @@ void launch_finalize_batch(const FinalizeDomain* doms, int n, cudaStream_t strea
     }
 }
 
+void launch_step_batch_table(const BatchTableLaunch& L, int dim, bool fast, cudaStream_t stream) {
+    if (fast) launch_step_batch_table_fast(L, dim, stream);
+    else if (dim == 3) launch_batch_table<3, TA3, TB3, 2, false>(L, stream);
+    else launch_batch_table<2, TA2, TB2, 4, false>(L, stream);
+}
+
+void step_grid_dims(const StepParams& P, int* gx, int* gy, int* nblocks) {
+    const dim3 grid = P.g.dim == 3 ? step_grid<3, TA3, TB3>(P) : step_grid<2, TA2, TB2>(P);
+    *gx = (int)grid.x;
+    *gy = (int)grid.y;
+    *nblocks = (int)(grid.x * grid.y * grid.z);
+}
+
 int launch_step_batch(BatchDomain* doms, int n, cudaStream_t stream) {
     int launches = 0;
     int i = 0;

@@ -269,7 +269,7 @@ struct StepKernel {
         return v;
     }
 
-    __device__ static void run(const StepParams P, const double* __restrict__ o, const double* __restrict__ cr,
+    __device__ static void run(const StepParams& P, const double* __restrict__ o, const double* __restrict__ cr,
                                const double* __restrict__ p, const double* __restrict__ gb,
                                const double* __restrict__ s2, double* __restrict__ on,
                                double* __restrict__ crn, double* __restrict__ pn,
@@ -1170,6 +1170,43 @@ __global__ void __launch_bounds__(TA * TB, MINB) k_step_batch(const __grid_const
     const int bx = t % D.gx, r = t / D.gx, by = r % D.gy, bz = r / D.gy;
     StepKernel<DIM, TA, TB, FAST>::run(D.sp, D.o, D.cr, D.p, D.gb, D.s2, D.on, D.crn, D.pn, D.partials, D.st, bx, by,
                                        bz, t);
+}
+
+// Batched step with device-resident descriptors (BatchTableLaunch).
+template <int DIM, int TA, int TB, int MINB, bool FAST>
+__global__ void __launch_bounds__(TA * TB, MINB) k_step_batch_table(const BatchTableLaunch L) {
+    __shared__ StepParams sP;
+    __shared__ int s_dom;
+    const int tid = threadIdx.x + blockDim.x * threadIdx.y, nth = blockDim.x * blockDim.y;
+    if (tid == 0) {
+        int lo = 0, hi = L.n - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (__ldg(L.block0 + mid) <= (int)blockIdx.x) lo = mid;
+            else hi = mid - 1;
+        }
+        s_dom = lo;
+    }
+    __syncthreads();
+    const int d = s_dom;
+    const BatchDomain* D = L.table + 2 * d + ((L.parity[d >> 5] >> (d & 31)) & 1u);
+    {
+        const unsigned* src = reinterpret_cast<const unsigned*>(&D->sp);
+        unsigned* dst = reinterpret_cast<unsigned*>(&sP);
+        for (int q = tid; q < (int)(sizeof(StepParams) / 4); q += nth) dst[q] = __ldg(src + q);
+    }
+    __syncthreads();
+    const int t = (int)blockIdx.x - D->block0;
+    const int bx = t % D->gx, r = t / D->gx, by = r % D->gy, bz = r / D->gy;
+    StepKernel<DIM, TA, TB, FAST>::run(sP, D->o, D->cr, D->p, D->gb, D->s2, D->on, D->crn, D->pn, D->partials, D->st,
+                                       bx, by, bz, t);
+}
+
+template <int DIM, int TA, int TB, int MINB, bool FAST>
+static void launch_batch_table(const BatchTableLaunch& L, cudaStream_t stream) {
+    using T = Tile<DIM, TA, TB>;
+    ensure_smem_attr((const void*)k_step_batch_table<DIM, TA, TB, MINB, FAST>, (int)T::SMEM_BYTES);
+    k_step_batch_table<DIM, TA, TB, MINB, FAST><<<L.nblocks, dim3(TB, TA), T::SMEM_BYTES, stream>>>(L);
 }
 
 }  // namespace
