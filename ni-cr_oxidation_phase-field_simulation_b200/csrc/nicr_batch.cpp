@@ -21,20 +21,8 @@ struct nicr_batch {
     std::string err;
     long long launches = 0;   // batch-level launches (grouped step + finalize)
 
-    // Device-resident step descriptors: one launch for all domains when they
-    // share dimensionality and arithmetic form (else one launch per group of
-    // kBatchMax in the kernel's parameter space). Rebuilt when a domain's X
-    // chunk or partial-sum buffer changes.
-    nicr::BatchDomain* d_table = nullptr;
-    int* d_block0 = nullptr;
-    std::vector<int> table_nblocks;
-    std::vector<std::pair<int, const void*>> table_key;   // per domain: X chunk, partials
-    int table_total = 0;
-
     ~nicr_batch() {
         if (stream) cudaStreamSynchronize(stream);
-        if (d_table) cudaFree(d_table);
-        if (d_block0) cudaFree(d_block0);
         for (auto& q : graphs)
             if (q.exec) cudaGraphExecDestroy(q.exec);
         for (nicr_handle* h : doms) {
@@ -57,77 +45,14 @@ struct nicr_batch {
     };
     std::vector<PairGraph> graphs;
 
-    // Whether the one-launch path serves the batch now; (re)builds the device
-    // table when needed. Not called during a stream capture.
-    bool table_ready() {
-        const int n = (int)doms.size();
-        if (n > nicr::kBatchParityWords * 32) return false;
-        const nicr::StepParams s0 = doms[0]->m->params();
-        for (auto* h : doms) {
-            const nicr::StepParams sp = h->m->params();
-            if (sp.g.dim != s0.g.dim || sp.fast != s0.fast || !h->m->parity_linked()) return false;
-        }
-        bool fresh = d_table && (int)table_key.size() == n;
-        for (int i = 0; fresh && i < n; ++i)
-            fresh = table_key[i] == std::make_pair(doms[i]->m->params().xchunk,
-                                                   static_cast<const void*>(doms[i]->m->partials_ptr()));
-        if (fresh) return true;
-        std::vector<nicr::BatchDomain> t((size_t)2 * n);
-        std::vector<int> b0((size_t)n);
-        table_nblocks.assign((size_t)n, 0);
-        table_key.assign((size_t)n, {0, nullptr});
-        int total = 0;
-        for (int i = 0; i < n; ++i) {
-            nicr::Model& m = *doms[i]->m;
-            int gx = 0, gy = 0, nb = 0;
-            nicr::step_grid_dims(m.params(), &gx, &gy, &nb);
-            for (int q = 0; q < 2; ++q) {
-                nicr::BatchDomain d = m.step_desc_parity(q);
-                d.gx = gx; d.gy = gy; d.block0 = total; d.nblocks = nb;
-                t[(size_t)2 * i + q] = d;
-            }
-            b0[i] = total;
-            table_nblocks[i] = nb;
-            table_key[i] = {m.params().xchunk, static_cast<const void*>(m.partials_ptr())};
-            total += nb;
-        }
-        nicr::check_cuda(cudaStreamSynchronize(stream), "sync");
-        if (!d_table) {
-            nicr::check_cuda(cudaMalloc(&d_table, sizeof(nicr::BatchDomain) * 2 * n), "cudaMalloc (batch table)");
-            nicr::check_cuda(cudaMalloc(&d_block0, sizeof(int) * n), "cudaMalloc (batch table)");
-        }
-        nicr::check_cuda(cudaMemcpy(d_table, t.data(), sizeof(nicr::BatchDomain) * 2 * n, cudaMemcpyHostToDevice), "H2D");
-        nicr::check_cuda(cudaMemcpy(d_block0, b0.data(), sizeof(int) * n, cudaMemcpyHostToDevice), "H2D");
-        table_total = total;
-        return true;
-    }
-    bool use_table = false;   // set per advance/tune call by table_ready()
-
     void enqueue_step(std::vector<nicr::BatchDomain>& descs, std::vector<nicr::FinalizeDomain>& fins) {
         const int n = (int)doms.size();
-        if (use_table) {
-            nicr::BatchTableLaunch L{};
-            L.table = d_table;
-            L.block0 = d_block0;
-            L.n = n;
-            L.nblocks = table_total;
-            for (int i = 0; i < n; ++i) {
-                nicr::Model& m = *doms[i]->m;
-                m.prepare_step();
-                if (m.parity_key() & 1) L.parity[i >> 5] |= 1u << (i & 31);
-                descs[i].nblocks = table_nblocks[i];
-            }
-            const nicr::StepParams s0 = doms[0]->m->params();
-            nicr::launch_step_batch_table(L, s0.g.dim, s0.fast != 0, stream);
-            launches += 1;
-        } else {
-            for (int i = 0; i < n; ++i) {
-                nicr::Model& m = *doms[i]->m;
-                m.prepare_step();
-                descs[i] = m.step_desc();
-            }
-            launches += nicr::launch_step_batch(descs.data(), n, stream);
+        for (int i = 0; i < n; ++i) {
+            nicr::Model& m = *doms[i]->m;
+            m.prepare_step();
+            descs[i] = m.step_desc();
         }
+        launches += nicr::launch_step_batch(descs.data(), n, stream);
         for (int i = 0; i < n; ++i) {
             nicr::Model& m = *doms[i]->m;
             m.complete_step(descs[i].nblocks, false);
@@ -236,7 +161,6 @@ struct nicr_batch {
         std::vector<nicr::Model::RunPlan> plans((size_t)n);
         std::vector<nicr::BatchDomain> descs((size_t)n);
         std::vector<nicr::FinalizeDomain> fins((size_t)n);
-        use_table = table_ready();
         for (int i = 0; i < n; ++i) doms[i]->m->run_begin(plans[i], nsteps, schedule);
         const bool use_graphs = doms[0]->m->graphs_enabled();
         for (int s = 0; s < nsteps;) {

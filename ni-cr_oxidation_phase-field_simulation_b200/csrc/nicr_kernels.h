@@ -144,26 +144,32 @@ struct StepBatch {
     int n, pad;
     BatchDomain d[kBatchMax];
 };
-// returns the number of launches
-int launch_step_batch(BatchDomain* doms, int n, cudaStream_t stream);
-void launch_batch_group_fast(StepBatch& B, int nblocks, int dim, cudaStream_t stream);
-// The batched step of any number of domains of one dimensionality and form
-// in one launch, its descriptors in device memory: table holds two entries
-// per domain (buffer parity 0, then 1), block0 the first block of each
-// domain (nblocks in all); bit d of parity selects domain d's entry. Each
-// block copies its domain's parameters to shared memory and runs the CTA the
-// single-domain launch would run.
-constexpr int kBatchParityWords = 16;   // up to 512 domains
-struct BatchTableLaunch {
-    const BatchDomain* table;
-    const int* block0;
-    int n, nblocks;
-    unsigned parity[kBatchParityWords];
+// Compact form of a batch whose domains share every step parameter except
+// the grid, the inlet value and the plane/key ranges that follow from the
+// grid (a parameter sweep over sizes, O supply, Cr and Ksp, which the step
+// kernel does not read): the shared parameters once, ~170 bytes per domain,
+// so one launch serves up to kBatchSlimMax domains.
+struct BatchSlim {
+    Grid g;
+    double layer_o;
+    long long key_ncells;
+    int x_hi, inlet, gx, gy, block0, pad;
+    const double *o, *cr, *p, *gb, *s2;
+    double *on, *crn, *pn;
+    StepPartial* partials;
+    Status* st;
 };
-void launch_step_batch_table(const BatchTableLaunch& L, int dim, bool fast, cudaStream_t stream);
-void launch_step_batch_table_fast(const BatchTableLaunch& L, int dim, cudaStream_t stream);
-// step_grid of P's kernel: (x, y) blocks per X chunk and the total block count
-void step_grid_dims(const StepParams& P, int* gx, int* gy, int* nblocks);
+constexpr int kBatchSlimMax = 160;   // 160 x 168 bytes + the shared parameters: < 27.5 KB of kernel parameters
+struct StepBatchSlim {
+    StepParams base;
+    int n, pad;
+    BatchSlim d[kBatchSlimMax];
+};
+// returns the number of launches: one for the whole batch in the compact
+// form when it applies, else one per group of kBatchMax domains
+int launch_step_batch(BatchDomain* doms, int n, cudaStream_t stream);
+void launch_batch_slim_fast(const StepBatchSlim& B, int nblocks, int dim, cudaStream_t stream);
+void launch_batch_group_fast(StepBatch& B, int nblocks, int dim, cudaStream_t stream);
 
 // One launch for the step kernel and the eta update of one step (reciprocal
 // form, 3D, 1..16 eta fields): the two are independent within a step, and

@@ -863,19 +863,6 @@ BatchDomain Model::step_desc() const {
     return d;
 }
 
-BatchDomain Model::step_desc_parity(int parity) const {
-    BatchDomain d{};
-    const int gpar = advance_eta ? parity : gcur;
-    d.sp = sp;
-    d.o = o_[parity]; d.cr = cr_[parity]; d.p = p_[parity];
-    d.gb = gb_[gpar];
-    d.s2 = has_eta ? s2_[gpar] : nullptr;
-    d.on = o_[parity ^ 1]; d.crn = cr_[parity ^ 1]; d.pn = p_[parity ^ 1];
-    d.partials = partials;
-    d.st = st;
-    return d;
-}
-
 FinalizeDomain Model::finalize_desc(int nb) const {
     FinalizeDomain f{};
     f.partials = partials;

@@ -135,13 +135,6 @@ public:
     void launch_trial_eta();
     void prepare_step();
     BatchDomain step_desc() const;
-    // step_desc() as if the buffer parity were `parity` (the eta-mask parity
-    // following it when eta evolves): the batch's device-resident descriptors
-    BatchDomain step_desc_parity(int parity) const;
-    // whether the eta-mask parity follows the buffer parity (always, unless
-    // some path flipped one without the other)
-    bool parity_linked() const { return !advance_eta || gcur == cur; }
-    const StepPartial* partials_ptr() const { return partials; }
     FinalizeDomain finalize_desc(int nblocks) const;
     void complete_step(int nblocks, bool finalize);
     // step-pair graphs: whether they are used, whether step s of plan r

@@ -17,6 +17,8 @@
 // form, nicr_step_fast.cu the reciprocal form. Ghost semantics:
 // Neumann copies in X for o, cr, phi, gb and for the computed mu and M
 // (refresh copies mu(1) into the ghost, 3S:613-615), periodic rows/columns.
+#include <cstring>
+
 #include "nicr_step_impl.cuh"
 #include "nicr_step_fused.cuh"
 
@@ -398,20 +400,62 @@ void launch_finalize_batch(const FinalizeDomain* doms, int n, cudaStream_t strea
     }
 }
 
-void launch_step_batch_table(const BatchTableLaunch& L, int dim, bool fast, cudaStream_t stream) {
-    if (fast) launch_step_batch_table_fast(L, dim, stream);
-    else if (dim == 3) launch_batch_table<3, TA3, TB3, 2, false>(L, stream);
-    else launch_batch_table<2, TA2, TB2, 4, false>(L, stream);
+// The shared part of a domain's parameters: everything but what BatchSlim carries.
+static StepParams slim_base(StepParams sp) {
+    sp.g = Grid{};
+    sp.layer_o = 0.;
+    sp.inlet = 0;
+    sp.x_hi = 0;
+    sp.key_ncells = 0;
+    return sp;
 }
 
-void step_grid_dims(const StepParams& P, int* gx, int* gy, int* nblocks) {
-    const dim3 grid = P.g.dim == 3 ? step_grid<3, TA3, TB3>(P) : step_grid<2, TA2, TB2>(P);
-    *gx = (int)grid.x;
-    *gy = (int)grid.y;
-    *nblocks = (int)(grid.x * grid.y * grid.z);
+// One compact launch for the whole batch when every domain has the same
+// dimensionality, form and shared parameters (compared bytewise: the model's
+// parameter blocks are value-initialised, padding included); false otherwise.
+static bool launch_step_batch_slim(BatchDomain* doms, int n, cudaStream_t stream) {
+    if (n > kBatchSlimMax) return false;
+    static StepBatchSlim B;   // host staging of the kernel parameters (~27 KB)
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lock(mu);
+    B.base = doms[0].sp;
+    const StepParams ref = slim_base(doms[0].sp);
+    for (int i = 0; i < n; ++i) {
+        const StepParams b = slim_base(doms[i].sp);
+        if (std::memcmp(&b, &ref, sizeof(StepParams)) != 0 || doms[i].sp.x_lo != 0 || doms[i].sp.err_slot >= 0)
+            return false;
+    }
+    const int dim = doms[0].sp.g.dim, fast = doms[0].sp.fast;
+    B.n = n;
+    int nb = 0;
+    for (int i = 0; i < n; ++i) {
+        const BatchDomain& d = doms[i];
+        const dim3 grid = dim == 3 ? step_grid<3, TA3, TB3>(d.sp) : step_grid<2, TA2, TB2>(d.sp);
+        BatchSlim& s = B.d[i];
+        s.g = d.sp.g;
+        s.layer_o = d.sp.layer_o;
+        s.key_ncells = d.sp.key_ncells;
+        s.x_hi = d.sp.x_hi;
+        s.inlet = d.sp.inlet;
+        s.gx = (int)grid.x;
+        s.gy = (int)grid.y;
+        s.block0 = nb;
+        s.pad = 0;
+        s.o = d.o; s.cr = d.cr; s.p = d.p; s.gb = d.gb; s.s2 = d.s2;
+        s.on = d.on; s.crn = d.crn; s.pn = d.pn;
+        s.partials = d.partials;
+        s.st = d.st;
+        doms[i].nblocks = (int)(grid.x * grid.y * grid.z);
+        nb += doms[i].nblocks;
+    }
+    if (fast) launch_batch_slim_fast(B, nb, dim, stream);
+    else if (dim == 3) launch_batch_slim<3, TA3, TB3, 2, false>(B, nb, stream);
+    else launch_batch_slim<2, TA2, TB2, 4, false>(B, nb, stream);
+    return true;
 }
 
 int launch_step_batch(BatchDomain* doms, int n, cudaStream_t stream) {
+    if (launch_step_batch_slim(doms, n, stream)) return 1;
     int launches = 0;
     int i = 0;
     while (i < n) {

@@ -45,9 +45,9 @@ void step_eta_prepare_fast(const StepParams& P, int neta) {
     if (P.g.dim == 3) step_eta_prepare<true>(neta);
 }
 
-void launch_step_batch_table_fast(const BatchTableLaunch& L, int dim, cudaStream_t stream) {
-    if (dim == 3) launch_batch_table<3, TA3, TB3, 2, true>(L, stream);
-    else launch_batch_table<2, TA2, TB2, 4, true>(L, stream);
+void launch_batch_slim_fast(const StepBatchSlim& B, int nblocks, int dim, cudaStream_t stream) {
+    if (dim == 3) launch_batch_slim<3, TA3, TB3, 2, true>(B, nblocks, stream);
+    else launch_batch_slim<2, TA2, TB2, 4, true>(B, nblocks, stream);
 }
 
 void launch_batch_group_fast(StepBatch& B, int nblocks, int dim, cudaStream_t stream) {

@@ -269,7 +269,7 @@ struct StepKernel {
         return v;
     }
 
-    __device__ static void run(const StepParams& P, const double* __restrict__ o, const double* __restrict__ cr,
+    __device__ static void run(const StepParams P, const double* __restrict__ o, const double* __restrict__ cr,
                                const double* __restrict__ p, const double* __restrict__ gb,
                                const double* __restrict__ s2, double* __restrict__ on,
                                double* __restrict__ crn, double* __restrict__ pn,
@@ -1157,6 +1157,29 @@ k_eta_stream(const StepParams P, int neta, const double* __restrict__ eta, const
 // is <= b and runs exactly the CTA (bx, by, bz) the single-domain launch would
 // run, with the same partial-sum slot, so every domain's result is identical
 // to its own nicr_step.
+// The compact batch: the block's domain's parameters are the shared ones with
+// the domain's grid, inlet value and ranges.
+template <int DIM, int TA, int TB, int MINB, bool FAST>
+__global__ void __launch_bounds__(TA * TB, MINB) k_step_batch_slim(const __grid_constant__ StepBatchSlim B) {
+    int lo = 0, hi = B.n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (B.d[mid].block0 <= (int)blockIdx.x) lo = mid;
+        else hi = mid - 1;
+    }
+    const BatchSlim& D = B.d[lo];
+    StepParams P = B.base;
+    P.g = D.g;
+    P.layer_o = D.layer_o;
+    P.inlet = D.inlet;
+    P.x_hi = D.x_hi;
+    P.key_ncells = D.key_ncells;
+    const int t = (int)blockIdx.x - D.block0;
+    const int bx = t % D.gx, r = t / D.gx, by = r % D.gy, bz = r / D.gy;
+    StepKernel<DIM, TA, TB, FAST>::run(P, D.o, D.cr, D.p, D.gb, D.s2, D.on, D.crn, D.pn, D.partials, D.st, bx, by,
+                                       bz, t);
+}
+
 template <int DIM, int TA, int TB, int MINB, bool FAST>
 __global__ void __launch_bounds__(TA * TB, MINB) k_step_batch(const __grid_constant__ StepBatch B) {
     int lo = 0, hi = B.n - 1;
@@ -1170,43 +1193,6 @@ __global__ void __launch_bounds__(TA * TB, MINB) k_step_batch(const __grid_const
     const int bx = t % D.gx, r = t / D.gx, by = r % D.gy, bz = r / D.gy;
     StepKernel<DIM, TA, TB, FAST>::run(D.sp, D.o, D.cr, D.p, D.gb, D.s2, D.on, D.crn, D.pn, D.partials, D.st, bx, by,
                                        bz, t);
-}
-
-// Batched step with device-resident descriptors (BatchTableLaunch).
-template <int DIM, int TA, int TB, int MINB, bool FAST>
-__global__ void __launch_bounds__(TA * TB, MINB) k_step_batch_table(const BatchTableLaunch L) {
-    __shared__ StepParams sP;
-    __shared__ int s_dom;
-    const int tid = threadIdx.x + blockDim.x * threadIdx.y, nth = blockDim.x * blockDim.y;
-    if (tid == 0) {
-        int lo = 0, hi = L.n - 1;
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (__ldg(L.block0 + mid) <= (int)blockIdx.x) lo = mid;
-            else hi = mid - 1;
-        }
-        s_dom = lo;
-    }
-    __syncthreads();
-    const int d = s_dom;
-    const BatchDomain* D = L.table + 2 * d + ((L.parity[d >> 5] >> (d & 31)) & 1u);
-    {
-        const unsigned* src = reinterpret_cast<const unsigned*>(&D->sp);
-        unsigned* dst = reinterpret_cast<unsigned*>(&sP);
-        for (int q = tid; q < (int)(sizeof(StepParams) / 4); q += nth) dst[q] = __ldg(src + q);
-    }
-    __syncthreads();
-    const int t = (int)blockIdx.x - D->block0;
-    const int bx = t % D->gx, r = t / D->gx, by = r % D->gy, bz = r / D->gy;
-    StepKernel<DIM, TA, TB, FAST>::run(sP, D->o, D->cr, D->p, D->gb, D->s2, D->on, D->crn, D->pn, D->partials, D->st,
-                                       bx, by, bz, t);
-}
-
-template <int DIM, int TA, int TB, int MINB, bool FAST>
-static void launch_batch_table(const BatchTableLaunch& L, cudaStream_t stream) {
-    using T = Tile<DIM, TA, TB>;
-    ensure_smem_attr((const void*)k_step_batch_table<DIM, TA, TB, MINB, FAST>, (int)T::SMEM_BYTES);
-    k_step_batch_table<DIM, TA, TB, MINB, FAST><<<L.nblocks, dim3(TB, TA), T::SMEM_BYTES, stream>>>(L);
 }
 
 }  // namespace
@@ -1316,6 +1302,13 @@ static void launch_eta_form(const StepParams& P, int neta, const double* eta, co
         const dim3 grid((g.nb + 127) / 128, 1, g.nx);
         k_eta_update<2, FAST><<<grid, block, 0, stream>>>(P, neta, eta, s2, p, eta_next, gb_next, s2_next, st);
     }
+}
+
+template <int DIM, int TA, int TB, int MINB, bool FAST>
+static void launch_batch_slim(const StepBatchSlim& B, int nblocks, cudaStream_t stream) {
+    using T = Tile<DIM, TA, TB>;
+    ensure_smem_attr((const void*)k_step_batch_slim<DIM, TA, TB, MINB, FAST>, (int)T::SMEM_BYTES);
+    k_step_batch_slim<DIM, TA, TB, MINB, FAST><<<nblocks, dim3(TB, TA), T::SMEM_BYTES, stream>>>(B);
 }
 
 template <int DIM, int TA, int TB, int MINB, bool FAST>
