@@ -303,6 +303,22 @@ def sweep_workload(args, rank: int, world: int, local: int) -> int:
             "config": {"workload": "64 domains, edges in {32,48,64,80,96}, static grains 8-32, Ksp on (seed 3)",
                        "cells": total, "domains_this_rank": len(part)},
             "gpu_launches": b.kernel_launches - l0, "status": rc}
+    # mass-budget residuals of every domain (the reference's log(), 3S:963-967):
+    # O and Cr now minus the initial inventory and every booked change, relative
+    # to the inventory; the totals are double-double sums over the domain
+    res_o, res_cr = [], []
+    for d in b.domains:
+        bud, dg = d.budget(), d.diagnostics()
+        so = dg["sum_O"][0] + dg["sum_O"][1]
+        sc = dg["sum_Cr"][0] + dg["sum_Cr"][1]
+        io, ic = sum(bud["initialO"]), sum(bud["initialCr"])
+        ro = so - io - sum(bud["bcO"]) - sum(bud["nucO"]) - sum(bud["ckO"]) - sum(bud["clipO"])
+        rc_ = sc - ic - sum(bud["bcCr"]) - sum(bud["nucCr"]) - sum(bud["ckCr"]) - sum(bud["clipCr"])
+        res_o.append(abs(ro) / max(abs(so), 1e-300))
+        res_cr.append(abs(rc_) / max(abs(sc), 1e-300))
+    line["budget_residual"] = {"max_rel_O": max(res_o), "max_rel_Cr": max(res_cr),
+                               "nuclei": sum(d.budget()["nuclei"] for d in b.domains),
+                               "note": "per domain |sum - initial - bc - nuc - ck - clip| / |sum| after warmup + steps"}
     b.close()
     if rank == 0:
         print(json.dumps(line))
