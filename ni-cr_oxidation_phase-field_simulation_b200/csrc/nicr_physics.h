@@ -125,20 +125,24 @@ __device__ __forceinline__ double xdiv(double a, const DivC& d) {
 #elif defined(NICR_DIV_IEEE)
     return __ddiv_rn(a, d.b);
 #else
+    // Computed without branches; one (rarely taken) branch picks the IEEE
+    // division when neither the zero rule nor the certificate applies.
     const long long ab = __double_as_longlong(a);
     const int ea = (int)((ab >> 52) & 0x7FF);
+    const double q0 = __dmul_rn(a, d.rb);
+    const double r0 = __fma_rn(-q0, d.b, a);
+    const double q1 = __fma_rn(r0, d.rb, q0);
+    const double r1 = __fma_rn(-q1, d.b, a);
+    const long long qb = __double_as_longlong(q1);
+    const int eq = (int)((qb >> 52) & 0x7FF);
+    // 2^(1076 - eq) = 1 / (ulp(q1) / 2); meaningful when a is in range, which
+    // the certificate requires (the quotient's exponent then lies in [63, 1983])
+    const double scale = __longlong_as_double((long long)((unsigned long long)(2099 - eq) << 52));
     // +-0 / b is an exactly signed zero, which a * RN(1/b) reproduces
-    if (d.fast && (ab << 1) == 0) return __dmul_rn(a, d.rb);
-    if (d.fast && ea >= 123 && ea <= 1923) {
-        const double q0 = __dmul_rn(a, d.rb);
-        const double r0 = __fma_rn(-q0, d.b, a);
-        const double q1 = __fma_rn(r0, d.rb, q0);
-        const double r1 = __fma_rn(-q1, d.b, a);
-        const long long qb = __double_as_longlong(q1);
-        const int eq = (int)((qb >> 52) & 0x7FF);
-        const double scale = __longlong_as_double((long long)(2099 - eq) << 52);
-        if ((qb & 0x000FFFFFFFFFFFFFLL) != 0 && __dmul_rn(fabs(r1), scale) < fabs(d.b)) return q1;
-    }
+    const bool zero = (ab << 1) == 0;
+    const bool cert = ea >= 123 && ea <= 1923 && (qb & 0x000FFFFFFFFFFFFFLL) != 0 &&
+                      __dmul_rn(fabs(r1), scale) < fabs(d.b);
+    if (d.fast && (zero || cert)) return zero ? q0 : q1;
 #if defined(NICR_DIV_INLINE_FALLBACK)
     return __ddiv_rn(a, d.b);
 #else
