@@ -125,11 +125,14 @@ __device__ __forceinline__ double xdiv(double a, const DivC& d) {
 #elif defined(NICR_DIV_IEEE)
     return __ddiv_rn(a, d.b);
 #else
-    // Computed without branches; one (rarely taken) branch picks the IEEE
-    // division when neither the zero rule nor the certificate applies.
+    // Zeros (common: the Laplacian of a uniform region) return at once; the
+    // rest is computed without branches, and one rarely taken branch picks
+    // the IEEE division when the certificate fails.
     const long long ab = __double_as_longlong(a);
     const int ea = (int)((ab >> 52) & 0x7FF);
     const double q0 = __dmul_rn(a, d.rb);
+    // +-0 / b is an exactly signed zero, which a * RN(1/b) reproduces
+    if (d.fast && (ab << 1) == 0) return q0;
     const double r0 = __fma_rn(-q0, d.b, a);
     const double q1 = __fma_rn(r0, d.rb, q0);
     const double r1 = __fma_rn(-q1, d.b, a);
@@ -138,11 +141,9 @@ __device__ __forceinline__ double xdiv(double a, const DivC& d) {
     // 2^(1076 - eq) = 1 / (ulp(q1) / 2); meaningful when a is in range, which
     // the certificate requires (the quotient's exponent then lies in [63, 1983])
     const double scale = __longlong_as_double((long long)((unsigned long long)(2099 - eq) << 52));
-    // +-0 / b is an exactly signed zero, which a * RN(1/b) reproduces
-    const bool zero = (ab << 1) == 0;
     const bool cert = ea >= 123 && ea <= 1923 && (qb & 0x000FFFFFFFFFFFFFLL) != 0 &&
                       __dmul_rn(fabs(r1), scale) < fabs(d.b);
-    if (d.fast && (zero || cert)) return zero ? q0 : q1;
+    if (d.fast && cert) return q1;
 #if defined(NICR_DIV_INLINE_FALLBACK)
     return __ddiv_rn(a, d.b);
 #else
