@@ -575,6 +575,105 @@ def surrogate_jumps(dev, size=128, every=32, ks=2, steps=1024, iters=1200):
     return out
 
 
+def surrogate_spec_workload(args) -> int:
+    """The learned surrogate at its specified configuration: 3D 128^3 static
+    Voronoi runs with the batching form's parameter draws, a 3-level U-Net
+    with 32 base channels (BF16 weights and activations, FP32 accumulation),
+    trained on 200 solver trajectories (seeds 100-299, 4000 steps each, two
+    (t, t + 64) pairs drawn per run) to jump K = 64 steps; evaluated on
+    held-out seeds 300-301: the relative L2 error of the 64-step change
+    (network against rate extrapolation and persistence), and jump runs of
+    1024 steps (mass gates 5% and 25%) against plain stepping in both
+    arithmetic forms, with the relative L-inf error against the plain drop-in
+    run. Trajectories and timed runs use the reciprocal form."""
+    import torch
+    import nicr
+    from nicr import surrogate
+    dev = torch.device("cuda", 0)
+    size, K, runs, steps = 128, 64, args.spec_runs, 4000
+    out = {"workload": "surrogate-spec", "size": size, "k": K, "base": 32, "trajectories": runs,
+           "trajectory_steps": steps}
+    cfgs = surrogate.trajectory_configs(runs, size, first_seed=100, precision=1)
+    t0 = time.perf_counter()
+    x, r = surrogate.pair_samples(cfgs, steps, K, per_run=2, seed=7)
+    torch.cuda.synchronize()
+    out["samples"] = int(x.shape[0])
+    out["sample_s"] = time.perf_counter() - t0
+    torch.manual_seed(0)
+    net = surrogate.unet(4, 32).to(dev)
+    t0 = time.perf_counter()
+    norm, losses = surrogate.train(net, x, r, 1, K, iters=args.spec_iters, batch=1, lr=1e-3)
+    torch.cuda.synchronize()
+    out["train_s"] = time.perf_counter() - t0
+    out["train_iters"] = args.spec_iters
+    out["loss_first50"] = float(np.mean(losses[:50]))
+    out["loss_last50"] = float(np.mean(losses[-50:]))
+    del x, r
+    torch.cuda.empty_cache()
+    # the U-Net proposal at 128^3 (forward, eager)
+    probe_x = torch.zeros((1, size, size, size, 4), device=dev)
+    with torch.no_grad():
+        for _ in range(3):
+            surrogate.predict(net, norm, probe_x, probe_x)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(10):
+            surrogate.predict(net, norm, probe_x, probe_x)
+        torch.cuda.synchronize()
+    out["proposal_ms"] = (time.perf_counter() - t0) / 10 * 1e3
+    held = surrogate.trajectory_configs(2, size, first_seed=300, precision=1)
+    hx, hr = surrogate.pair_samples(held, steps, K, per_run=4, seed=11)
+    with torch.no_grad():
+        pred = surrogate.predict(net, norm, hx[:, 0], hr[:, 0], chunk=1)
+    x0, x1, r0 = hx[:, 0], hx[:, 1], hr[:, 0]
+    ref = lambda f: torch.linalg.vector_norm(((x1 - x0) / norm.csd)[..., f])
+    err = lambda y, f: float(torch.linalg.vector_norm(((y - x1) / norm.csd)[..., f]) / ref(f))
+    out["heldout_rel_l2"] = {name: {"network": err(pred, i), "rate": err(x0 + K * r0, i), "persistence": 1.0}
+                             for i, name in enumerate(("o", "cr", "phi"))}
+    out["heldout_rel_linf"] = {name: float((pred[..., i] - x1[..., i]).abs().max() / x1[..., i].abs().max())
+                               for i, name in enumerate(("o", "cr", "phi"))}
+    del hx, hr, pred
+    torch.cuda.empty_cache()
+    # jump runs against plain stepping of the same held-out seed
+    n = 1024
+    runs_out = []
+    base_cfg = held[0]
+
+    def timed_plain(precision):
+        c = surrogate.trajectory_configs(1, size, first_seed=300, precision=precision)[0]
+        s = nicr.Solver(c)
+        s.run(256)
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        s.run(n)
+        torch.cuda.synchronize()
+        return s, time.perf_counter() - t
+    plain_exact, t_exact = timed_plain(0)
+    plain_fast, t_fast = timed_plain(1)
+    out["plain_wall_s"] = {"fp64": t_exact, "fp64-fast": t_fast}
+    for tol in (0.05, 0.25):
+        c = surrogate.trajectory_configs(1, size, first_seed=300, precision=1)[0]
+        j = nicr.Solver(c)
+        j.run(256)
+        st = surrogate.JumpStepper(j, net, norm, K, mass_tol=tol)
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        counts = st.advance(n)
+        torch.cuda.synchronize()
+        tj = time.perf_counter() - t
+        e = {f: float(np.abs(j.get(f) - plain_exact.get(f)).max() / max(np.abs(plain_exact.get(f)).max(), 1e-300))
+             for f in ("o", "cr", "p")}
+        runs_out.append({"mass_tol": tol, "counts": counts, "wall_s": tj,
+                         "speed_vs_plain_fp64": t_exact / tj, "speed_vs_plain_fast": t_fast / tj,
+                         "rel_linf_vs_plain_fp64": e})
+        j.close()
+    plain_exact.close()
+    plain_fast.close()
+    out["jumps"] = runs_out
+    print(json.dumps(out))
+    return 0
+
+
 def surrogate_train_workload(args, rank: int, world: int, local: int) -> int:
     """Data-parallel training of the surrogate (one process per GPU under
     torchrun, NCCL): every rank generates its own 64^3 trajectories (2 seeds
@@ -796,7 +895,7 @@ def main():
     ap.add_argument("--ref-budget", type=float, default=60.0, help="seconds of CPU stepping for the reference")
     ap.add_argument("--slab-devices", default="", help="--workload slabs: comma-separated device per slab")
     ap.add_argument("--workload", choices=["step", "output", "sweep", "small", "accuracy", "slabs", "slab-ranks",
-                                           "surrogate", "surrogate-train", "ksp"],
+                                           "surrogate", "surrogate-train", "surrogate-spec", "ksp"],
                     default="step",
                     help="step: the headline line (default); output: VTI frame cost and overlap with stepping; "
                          "sweep: 64 uneven domains advanced as one batch; small: step rate of the small configs; "
@@ -805,9 +904,12 @@ def main():
                          "slab-ranks: the domain split over the torchrun ranks (one slab per GPU); "
                          "surrogate: the learned surrogate's convolution kernels and U-Net at 128^3; "
                          "surrogate-train: data-parallel training of the surrogate over the torchrun ranks; "
-                         "ksp: one Ksp scan at 256^3 in the benchmark state and supersaturated")
+                         "ksp: one Ksp scan at 256^3 in the benchmark state and supersaturated; "
+                         "surrogate-spec: the surrogate at its specified configuration (base 32, 200 runs, K 64)")
     ap.add_argument("--precision", type=int, default=0, help="arithmetic form of --workload sweep (0 drop-in, 1 fast)")
     ap.add_argument("--no-jumps", action="store_true", help="--workload surrogate: kernels only, no training and jump runs")
+    ap.add_argument("--spec-runs", type=int, default=200, help="--workload surrogate-spec: training trajectories")
+    ap.add_argument("--spec-iters", type=int, default=3000, help="--workload surrogate-spec: Adam steps")
     args = ap.parse_args()
     if args.e2e_steps <= 0:
         args.e2e_steps = args.steps
@@ -836,6 +938,8 @@ def main():
         return surrogate_train_workload(args, rank, world, local)
     if args.workload == "ksp":
         return ksp_workload(args)
+    if args.workload == "surrogate-spec":
+        return surrogate_spec_workload(args)
 
     import torch
     import torch.distributed as dist

@@ -324,14 +324,55 @@ def trajectories(cfgs, steps: int, every: int, probe: int = 2, device: int = 0):
     return torch.stack(xs), torch.stack(rs)
 
 
+def pair_samples(cfgs, steps: int, k_steps: int, per_run: int = 2, probe: int = 2, seed: int = 0,
+                 device: int = 0):
+    """Training pairs from long runs: for each configuration, `per_run`
+    times t drawn uniformly (seeded) in [4 * k_steps, steps - k_steps], the
+    state at t with its per-step rates over the `probe` steps before, and the
+    state k_steps later. Returns x, r of shape (runs * per_run, 2, size,
+    size, size, 4) FP32 on the GPU, sample 0 at t and sample 1 at t + k_steps,
+    for train(..., k=1, steps_k=k_steps)."""
+    import torch
+    from . import Solver
+    rng = np.random.default_rng(seed)
+    xs, rs = [], []
+    for c in cfgs:
+        c.device = device
+        s = Solver(c)
+        state = lambda: torch.stack([s.device_view(f) for f in FIELDS], dim=-1)
+        times = sorted(int(t) for t in rng.integers(4 * k_steps, steps - k_steps + 1, size=per_run))
+        done = 0
+        for t in times:
+            if t - probe > done:
+                s.run(t - probe - done)
+            a = state().float()
+            s.run(probe)
+            b = state().float()
+            rate = (b - a) / probe
+            s.run(k_steps)
+            c1 = state().float()
+            s.run(probe)
+            rate1 = (state().float() - c1) / probe
+            done = t + k_steps + probe
+            xs.append(torch.stack([b, c1]))
+            rs.append(torch.stack([rate, rate1]))
+            del a
+        s.close()
+    return torch.stack(xs), torch.stack(rs)
+
+
 def _moments(v, group):
     """(mean, std) per field of v (..., fields) over every rank of group
-    (sums of v and v^2 in FP64 all-reduced; population std)."""
+    (sums of v and v^2 in FP64 all-reduced; population std). Summed in
+    slices of the leading dimension, so large sample sets need no FP64 copy."""
     import torch
     f = v.shape[-1]
-    flat = v.reshape(-1, f).double()
-    m = torch.stack([flat.sum(0), (flat * flat).sum(0),
-                     torch.full((f,), float(flat.shape[0]), dtype=torch.float64, device=v.device)])
+    m = torch.zeros((3, f), dtype=torch.float64, device=v.device)
+    for i in range(v.shape[0]):
+        flat = v[i].reshape(-1, f).double()
+        m[0] += flat.sum(0)
+        m[1] += (flat * flat).sum(0)
+        m[2] += float(flat.shape[0])
     if group is not None:
         import torch.distributed as dist
         dist.all_reduce(m, group=group)
