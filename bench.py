@@ -628,9 +628,13 @@ def surrogate_spec_workload(args) -> int:
     x0, x1, r0 = hx[:, 0], hx[:, 1], hr[:, 0]
     ref = lambda f: torch.linalg.vector_norm(((x1 - x0) / norm.csd)[..., f])
     err = lambda y, f: float(torch.linalg.vector_norm(((y - x1) / norm.csd)[..., f]) / ref(f))
-    out["heldout_rel_l2"] = {name: {"network": err(pred, i), "rate": err(x0 + K * r0, i), "persistence": 1.0}
+    # phi does not change where no oxide forms: such a field has no relative error (None)
+    moved = lambda i: float(ref(i)) > 0.0
+    out["heldout_rel_l2"] = {name: ({"network": err(pred, i), "rate": err(x0 + K * r0, i), "persistence": 1.0}
+                                    if moved(i) else None)
                              for i, name in enumerate(("o", "cr", "phi"))}
-    out["heldout_rel_linf"] = {name: float((pred[..., i] - x1[..., i]).abs().max() / x1[..., i].abs().max())
+    out["heldout_rel_linf"] = {name: (float((pred[..., i] - x1[..., i]).abs().max() / x1[..., i].abs().max())
+                                      if moved(i) else None)
                                for i, name in enumerate(("o", "cr", "phi"))}
     del hx, hr, pred
     torch.cuda.empty_cache()
