@@ -416,26 +416,33 @@ struct OnePassStep {
                 on[gidx] = onv; crn[gidx] = crv; pn[gidx] = pnv;
                 FxO = rightO; FxCr = rightCr;
 
-                // eta_trial (3S:514-526) at plane u: v = eta - (dt L_eta)(deta - K lap eta)
-                const double* es = eslot(u);
-                const double* en = eslot(u + 1);
-                double* edst = eta_next + gidx;
+                // eta_trial (3S:514-526) at plane u: v = eta - (dt L_eta)(deta - K lap eta);
+                // the fields failing the range test are collected as bits and keyed
+                // once (the first field in reference order)
+                {
+                    const double* es = eslot(u);
+                    const double* en = eslot(u + 1);
+                    double* edst = eta_next + gidx;
+                    unsigned ebad = 0;
 #pragma unroll
-                for (int q = 0; q < N; ++q) {
-                    const int fq = q * L::FS;
-                    const double c0 = es[e_own + fq];
-                    const double lap = fdiv<FAST>((en[e_own + fq] - 2. * c0 + ep[q]), P.v_dxdx)
-                                     + fdiv<FAST>((es[ap_o + fq] - 2. * c0 + es[am_o + fq]), P.v_dada)
-                                     + fdiv<FAST>((es[bp_o + fq] - 2. * c0 + es[bm_o + fq]), P.v_dbdb);
-                    const double force = grain_deta(c0, s2u, pp, P.eta_W, P.eta_A) - P.eta_K * lap;
-                    const double v = c0 - P.dt_etaL * force;
-                    if (!isfinite(v) || v < -1.e-12 || v > 1. + 1.e-12)
-                        errkey = min(errkey, ERR_ETA_BASE + (unsigned long long)q * (unsigned long long)g.ncells +
-                                                 (unsigned long long)cell_of());
-                    *edst = v;
-                    edst += g.nstore;
-                    ep[q] = c0;
+                    for (int q = 0; q < N; ++q) {
+                        const int fq = q * L::FS;
+                        const double c0 = es[e_own + fq];
+                        const double lap = fdiv<FAST>((en[e_own + fq] - 2. * c0 + ep[q]), P.v_dxdx)
+                                         + fdiv<FAST>((es[ap_o + fq] - 2. * c0 + es[am_o + fq]), P.v_dada)
+                                         + fdiv<FAST>((es[bp_o + fq] - 2. * c0 + es[bm_o + fq]), P.v_dbdb);
+                        const double force = grain_deta(c0, s2u, C.p, P.eta_W, P.eta_A) - P.eta_K * lap;
+                        const double v = c0 - P.dt_etaL * force;
+                        ebad |= (!isfinite(v) || v < -1.e-12 || v > 1. + 1.e-12) ? (1u << q) : 0u;
+                        *edst = v;
+                        edst += g.nstore;
+                        ep[q] = c0;
+                    }
+                    if (ebad)
+                        errkey = min(errkey, ERR_ETA_BASE + (unsigned long long)(__ffs(ebad) - 1) *
+                                                 (unsigned long long)g.ncells + (unsigned long long)cell_of());
                 }
+
                 pP = pp;   // a register: the ring slot of plane u-1 takes plane u+2 next
             }
             s2u = s2n;
