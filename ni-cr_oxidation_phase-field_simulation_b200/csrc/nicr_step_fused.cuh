@@ -390,31 +390,46 @@ struct OnePassStep {
                           + hpv * (foxide(oo, cc) - fmetal(oo, cc)) - 2. * Phys::kp * lapP;
                 fp += grain_dphi(s2u, pp, P.eta_W, P.eta_A);
                 double pnv = pp - P.dtL * fp;
+                // Ck, the trial test and the clamps without data-dependent branches
+                // (so the scheduler sees one block); the rare bookkeeping (budget
+                // terms of changed cells, failure keys) is one branch after the stores
+                double dO = 0., dCr = 0.;
                 if (P.ck == 0) {
                     const double hn = h(pnv);
-                    const double dO = fdiv<FAST>(-Phys::ckO * ((Phys::oxideO - onv) * hn - (Phys::oxideO - oo) * C.hh), P.v_dt);
-                    const double dCr = fdiv<FAST>(-Phys::ckCr * ((Phys::oxideCr - crv) * hn - (Phys::oxideCr - cc) * C.hh), P.v_dt);
+                    dO = fdiv<FAST>(-Phys::ckO * ((Phys::oxideO - onv) * hn - (Phys::oxideO - oo) * C.hh), P.v_dt);
+                    dCr = fdiv<FAST>(-Phys::ckCr * ((Phys::oxideCr - crv) * hn - (Phys::oxideCr - cc) * C.hh), P.v_dt);
                     onv += dO; crv += dCr;
-                    if (dO != 0.) acc[0] = dd_add(acc[0], dO);
-                    if (dCr != 0.) acc[1] = dd_add(acc[1], dCr);
                 }
-                if (!isfinite(onv) || !isfinite(crv) || !isfinite(pnv)) {
-                    errkey = min(errkey, (unsigned long long)cell_of() * 4ull);
-                } else if (P.bounds == 1) {
+                const bool nonfinite = !isfinite(onv) || !isfinite(crv) || !isfinite(pnv);
+                double clO = 0., clCr = 0.;
+                bool outside = false;
+                if (P.bounds == 1) {
                     const double oc = sclamp(onv, 0., 1.), ccr = sclamp(crv, 0., 1.);
-                    const double clO = oc - onv, clCr = ccr - crv;
-                    if (clO != 0.) acc[2] = dd_add(acc[2], clO);
-                    if (clCr != 0.) acc[3] = dd_add(acc[3], clCr);
-                    if (oc != onv || ccr != crv) ++clipped;
-                    onv = oc; crv = ccr;
-                    if (pnv > .99999) pnv = 1.;
-                    if (pnv < 1.e-5) pnv = 0.;
-                } else if (onv < -1.e-12 || crv < -1.e-12 || onv + crv > 1. + 1.e-12 || pnv < -1.e-12 ||
-                           pnv > 1. + 1.e-12) {
-                    errkey = min(errkey, (unsigned long long)cell_of() * 4ull + 1ull);
+                    if (!nonfinite) {
+                        clO = oc - onv;
+                        clCr = ccr - crv;
+                        clipped += (oc != onv || ccr != crv) ? 1 : 0;
+                        onv = oc;
+                        crv = ccr;
+                        pnv = pnv > .99999 ? 1. : pnv;
+                        pnv = pnv < 1.e-5 ? 0. : pnv;
+                    }
+                } else {
+                    outside = !nonfinite && (onv < -1.e-12 || crv < -1.e-12 || onv + crv > 1. + 1.e-12 ||
+                                             pnv < -1.e-12 || pnv > 1. + 1.e-12);
                 }
                 on[gidx] = onv; crn[gidx] = crv; pn[gidx] = pnv;
                 FxO = rightO; FxCr = rightCr;
+                if (nonfinite || outside || dO != 0. || dCr != 0. || clO != 0. || clCr != 0.) {
+                    if (nonfinite || outside)
+                        errkey = min(errkey, (unsigned long long)cell_of() * 4ull + (nonfinite ? 0ull : 1ull));
+                    // adding +-0 to a normalised double-double leaves it unchanged,
+                    // so zero increments are skipped
+                    if (dO != 0.) acc[0] = dd_add(acc[0], dO);
+                    if (dCr != 0.) acc[1] = dd_add(acc[1], dCr);
+                    if (clO != 0.) acc[2] = dd_add(acc[2], clO);
+                    if (clCr != 0.) acc[3] = dd_add(acc[3], clCr);
+                }
 
                 // eta_trial (3S:514-526) at plane u: v = eta - (dt L_eta)(deta - K lap eta);
                 // the fields failing the range test are collected as bits and keyed
