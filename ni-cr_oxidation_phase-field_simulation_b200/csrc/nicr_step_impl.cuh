@@ -459,33 +459,45 @@ struct StepKernel {
                           + hpv * (foxide(oo, cc) - fmetal(oo, cc)) - 2. * Phys::kp * lapP;
                 if (P.phi_eta) fp += grain_dphi(s2u, pp, P.eta_W, P.eta_A);
                 double pnv = pp - P.dtL * fp;
+                // Ck, the trial test and the clamps without data-dependent branches
+                // (so the scheduler sees one block); the rare bookkeeping (budget
+                // terms of changed cells, failure keys) is one branch after the stores
+                double dO = 0., dCr = 0.;
                 if (P.ck == 0) {
                     const double hn = h(pnv);
-                    const double dO = fdiv<FAST>(-Phys::ckO * ((Phys::oxideO - onv) * hn - (Phys::oxideO - oo) * C.hh), P.v_dt);
-                    const double dCr = fdiv<FAST>(-Phys::ckCr * ((Phys::oxideCr - crv) * hn - (Phys::oxideCr - cc) * C.hh), P.v_dt);
+                    dO = fdiv<FAST>(-Phys::ckO * ((Phys::oxideO - onv) * hn - (Phys::oxideO - oo) * C.hh), P.v_dt);
+                    dCr = fdiv<FAST>(-Phys::ckCr * ((Phys::oxideCr - crv) * hn - (Phys::oxideCr - cc) * C.hh), P.v_dt);
                     onv += dO; crv += dCr;
+                }
+                const bool nonfinite = !isfinite(onv) || !isfinite(crv) || !isfinite(pnv);
+                double clO = 0., clCr = 0.;
+                bool outside = false;
+                if (P.bounds == 1) {
+                    const double oc = sclamp(onv, 0., 1.), ccr = sclamp(crv, 0., 1.);
+                    if (!nonfinite) {
+                        clO = oc - onv;
+                        clCr = ccr - crv;
+                        clipped += (oc != onv || ccr != crv) ? 1 : 0;
+                        onv = oc;
+                        crv = ccr;
+                        pnv = pnv > .99999 ? 1. : pnv;
+                        pnv = pnv < 1.e-5 ? 0. : pnv;
+                    }
+                } else {
+                    outside = !nonfinite && (onv < -1.e-12 || crv < -1.e-12 || onv + crv > 1. + 1.e-12 ||
+                                             pnv < -1.e-12 || pnv > 1. + 1.e-12);
+                }
+                on[gidx] = onv; crn[gidx] = crv; pn[gidx] = pnv;
+                FxO = rightO; FxCr = rightCr;
+                if (nonfinite || outside || dO != 0. || dCr != 0. || clO != 0. || clCr != 0.) {
+                    if (nonfinite || outside) errkey = min(errkey, (unsigned long long)cell * 4ull + (nonfinite ? 0ull : 1ull));
                     // adding +-0 to a normalised double-double leaves it unchanged,
                     // so zero increments (metal cells: h(pn) == h(p) == 0) are skipped
                     if (dO != 0.) acc[0] = dd_add(acc[0], dO);
                     if (dCr != 0.) acc[1] = dd_add(acc[1], dCr);
-                }
-                if (!isfinite(onv) || !isfinite(crv) || !isfinite(pnv)) {
-                    errkey = min(errkey, (unsigned long long)cell * 4ull);
-                } else if (P.bounds == 1) {
-                    const double oc = sclamp(onv, 0., 1.), ccr = sclamp(crv, 0., 1.);
-                    const double clO = oc - onv, clCr = ccr - crv;
                     if (clO != 0.) acc[2] = dd_add(acc[2], clO);
                     if (clCr != 0.) acc[3] = dd_add(acc[3], clCr);
-                    if (oc != onv || ccr != crv) ++clipped;
-                    onv = oc; crv = ccr;
-                    if (pnv > .99999) pnv = 1.;
-                    if (pnv < 1.e-5) pnv = 0.;
-                } else if (onv < -1.e-12 || crv < -1.e-12 || onv + crv > 1. + 1.e-12 || pnv < -1.e-12 ||
-                           pnv > 1. + 1.e-12) {
-                    errkey = min(errkey, (unsigned long long)cell * 4ull + 1ull);
                 }
-                on[gidx] = onv; crn[gidx] = crv; pn[gidx] = pnv;
-                FxO = rightO; FxCr = rightCr;
             }
             pP = C.p;
             C = L;
@@ -543,6 +555,7 @@ __device__ __forceinline__ void eta_cell(const StepParams& P, int neta, const do
     }
     const double S = __ldg(s2 + idx), phi = __ldg(p + idx);
     double Sn = 0., pairs = 0.;
+    int first_bad = -1;   // the first field failing the range test
     for (int q = 0; q < neta; ++q) {
         const double* e = eta + (long long)q * g.nstore;
         const double ec = __ldg(e + idx);
@@ -556,13 +569,17 @@ __device__ __forceinline__ void eta_cell(const StepParams& P, int neta, const do
                 + fdiv<FAST>((__ldg(e + ibp) - 2. * ec + __ldg(e + ibm)), P.v_dbdb);
         const double force = grain_deta(ec, S, phi, P.eta_W, P.eta_A) - P.eta_K * lap;
         const double v = ec - P.dt_etaL * force;
-        if (!isfinite(v) || v < -1.e-12 || v > 1. + 1.e-12)
-            errkey = min(errkey, ERR_ETA_BASE + (unsigned long long)q * (unsigned long long)P.key_ncells + (unsigned long long)cell);
+        const bool fail = !isfinite(v) || v < -1.e-12 || v > 1. + 1.e-12;
+        first_bad = (fail && first_bad < 0) ? q : first_bad;
         eta_next[(long long)q * g.nstore + idx] = v;
         const double sq = v * v;
         pairs += Sn * sq;
         Sn += sq;
     }
+    // keyed once per cell: the first failing field in reference order
+    if (first_bad >= 0)
+        errkey = min(errkey, ERR_ETA_BASE + (unsigned long long)first_bad * (unsigned long long)P.key_ncells +
+                                 (unsigned long long)cell);
     s2_next[idx] = Sn;
     gb_next[idx] = P.eta_scale * smin(1., 16. * pairs);
 }
@@ -640,6 +657,7 @@ __device__ __forceinline__ void eta_march_body(const StepParams& P, int n, const
             if (q < n) S += ec[q] * ec[q];
         const long long cell = ((long long)x * g.na + row) * g.nb + col + (SLAB ? P.cell_off : 0);
         double Sn = 0., pairs = 0.;
+        unsigned bad = 0;
 #pragma unroll
         for (int q = 0; q < NCAP; ++q) {
             if (q >= n) break;
@@ -655,13 +673,16 @@ __device__ __forceinline__ void eta_march_body(const StepParams& P, int n, const
                     + fdiv<FAST>((__ldg(e + cbp) - 2. * c0 + __ldg(e + cbm)), P.v_dbdb);
             const double force = grain_deta(c0, S, phi, P.eta_W, P.eta_A) - P.eta_K * lap;
             const double v = c0 - P.dt_etaL * force;
-            if (!isfinite(v) || v < -1.e-12 || v > 1. + 1.e-12)
-                errkey = min(errkey, ERR_ETA_BASE + (unsigned long long)q * (unsigned long long)(SLAB ? P.key_ncells : g.ncells) + (unsigned long long)cell);
+            bad |= (!isfinite(v) || v < -1.e-12 || v > 1. + 1.e-12) ? (1u << q) : 0u;
             eta_next[(long long)q * g.nstore + base + rc] = v;
             const double sq = v * v;
             pairs += Sn * sq;
             Sn += sq;
         }
+        // fields failing the range test, keyed once (the first in reference order)
+        if (bad)
+            errkey = min(errkey, ERR_ETA_BASE + (unsigned long long)(__ffs(bad) - 1) *
+                                     (unsigned long long)(SLAB ? P.key_ncells : g.ncells) + (unsigned long long)cell);
         s2_next[base + rc] = Sn;
         gb_next[base + rc] = P.eta_scale * smin(1., 16. * pairs);
 #pragma unroll
