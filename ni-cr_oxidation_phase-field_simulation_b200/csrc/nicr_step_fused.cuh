@@ -86,7 +86,9 @@ __device__ __forceinline__ int eta_slot_point(int a, int b, int& stride) {
     return L::O_CRN + ((a < 0 ? 0 : 2) + (b < 0 ? 0 : 1)) * L::CP + (b < 0 ? 1 : 0);
 }
 
-template <bool FAST, int N>
+// MODE 1: O diffusion on, legacy Ck, legacy bounds (the common setting, the
+// benchmark's): those flags fold at compile time; MODE 0 reads them from P.
+template <bool FAST, int N, int MODE>
 struct OnePassStep {
     using L = FusedLayout<N>;
     using T = typename L::T;
@@ -151,6 +153,9 @@ struct OnePassStep {
 
         if (st->failed) return;   // a previous step of this batch was rejected
 
+        const bool o_on = MODE == 1 ? true : P.o_on != 0;
+        const bool ck_legacy = MODE == 1 ? true : P.ck == 0;
+        const bool bounds_legacy = MODE == 1 ? true : P.bounds == 1;
         const Grid& g = P.g;
         const int ta = threadIdx.y, tb = threadIdx.x, tid = tb + TB * ta;
         const int a0 = blockIdx.y * TA, b0 = blockIdx.x * TB;
@@ -266,10 +271,23 @@ struct OnePassStep {
             __syncthreads();
             const CenterVals C = lead(0, s2u, gbu);
             __syncthreads();
-            const double muOg = (P.bc == 1 && P.o_on) ? 2. * P.mu_res - C.muO : C.muO;
+            const double muOg = (P.bc == 1 && o_on) ? 2. * P.mu_res - C.muO : C.muO;
             FxO = fdiv<FAST>(-.5 * (C.mo + C.mo) * (C.muO - muOg), P.v_dx);
             FxCr = fdiv<FAST>(-.5 * (C.mc + C.mc) * (C.muCr - C.muCr), P.v_dx);
             pP = C.p;
+            // the x = 0 face of plane 0 and the inlet's budget term, here rather
+            // than in the march: left_flux (3S:621-628), the surface-mobility
+            // closure of the O face with bc=mu, replaces the ghost face
+            if (P.bc == 1) {
+                double lf = 0.;
+                if (o_on) {
+                    const double mf = mobility(P.surface_c_ref, h(C.p), gbu, Phys::bmo, Phys::boo, P.gbm1_o);
+                    lf = fdiv<FAST>(2. * mf * (P.mu_res - C.muO), P.v_dx);
+                }
+                FxO = lf;
+                acc[4] = dd_add(acc[4], fdiv<FAST>(P.dt * lf, P.v_dx));
+            }
+            if (P.inlet) acc[4] = dd_add(acc[4], P.layer_o - __ldg(o + (long long)row * g.pb + col));
         } else {
             SK::load_oc(P, o, cr, i0 - 2, oslot(i0 - 2), cslot(i0 - 2), offs);
             SK::load_oc(P, o, cr, i0 - 1, oslot(i0 - 1), cslot(i0 - 1), offs);
@@ -349,18 +367,7 @@ struct OnePassStep {
 
                 const double rightO = fdiv<FAST>(-.5 * (C.mo + Lv.mo) * (Lv.muO - C.muO), P.v_dx);
                 const double rightCr = fdiv<FAST>(-.5 * (C.mc + Lv.mc) * (Lv.muCr - C.muCr), P.v_dx);
-                double leftO = FxO;
-                if (u == 0 && P.bc == 1) {
-                    // left_flux (3S:621-628): surface-mobility face closure for bc=mu
-                    double lf = 0.;
-                    if (P.o_on) {
-                        const double mf = mobility(P.surface_c_ref, h(C.p), gbu, Phys::bmo, Phys::boo, P.gbm1_o);
-                        lf = fdiv<FAST>(2. * mf * (P.mu_res - C.muO), P.v_dx);
-                    }
-                    leftO = lf;
-                    acc[4] = dd_add(acc[4], fdiv<FAST>(P.dt * lf, P.v_dx));
-                }
-                if (u == 0 && P.inlet) acc[4] = dd_add(acc[4], P.layer_o - __ldg(o + gidx));
+                const double leftO = FxO;
 
                 double divO = 0., divCr;
                 {
@@ -371,7 +378,7 @@ struct OnePassStep {
                     const double bottom = fdiv<FAST>(-.5 * (mc_[am] + mc0) * (mu0 - mC[am]), P.v_da);
                     divCr = fdiv<FAST>(FxCr - rightCr, P.v_dx) + fdiv<FAST>(bottom - top, P.v_da) + fdiv<FAST>(back - front, P.v_db);
                 }
-                if (P.o_on) {
+                if (o_on) {
                     const double m0 = mo_[c1], mu0 = mO[c1];
                     const double front = fdiv<FAST>(-.5 * (m0 + mo_[bp]) * (mO[bp] - mu0), P.v_db);
                     const double back = fdiv<FAST>(-.5 * (mo_[bm] + m0) * (mu0 - mO[bm]), P.v_db);
@@ -380,7 +387,7 @@ struct OnePassStep {
                     divO = fdiv<FAST>(leftO - rightO, P.v_dx) + fdiv<FAST>(bottom - top, P.v_da) + fdiv<FAST>(back - front, P.v_db);
                 }
                 const double oo = C.o, cc = C.cr, pp = C.p;
-                double onv = P.o_on ? oo + P.dt * divO : oo;
+                double onv = o_on ? oo + P.dt * divO : oo;
                 double crv = cc + P.dt * divCr;
                 const double lapP = fdiv<FAST>((Lv.p - 2. * pp + pP), P.v_dxdx)
                                   + fdiv<FAST>((spu[ap] - 2. * pp + spu[am]), P.v_dada)
@@ -394,7 +401,7 @@ struct OnePassStep {
                 // (so the scheduler sees one block); the rare bookkeeping (budget
                 // terms of changed cells, failure keys) is one branch after the stores
                 double dO = 0., dCr = 0.;
-                if (P.ck == 0) {
+                if (ck_legacy) {
                     const double hn = h(pnv);
                     dO = fdiv<FAST>(-Phys::ckO * ((Phys::oxideO - onv) * hn - (Phys::oxideO - oo) * C.hh), P.v_dt);
                     dCr = fdiv<FAST>(-Phys::ckCr * ((Phys::oxideCr - crv) * hn - (Phys::oxideCr - cc) * C.hh), P.v_dt);
@@ -403,7 +410,7 @@ struct OnePassStep {
                 const bool nonfinite = !isfinite(onv) || !isfinite(crv) || !isfinite(pnv);
                 double clO = 0., clCr = 0.;
                 bool outside = false;
-                if (P.bounds == 1) {
+                if (bounds_legacy) {
                     const double oc = sclamp(onv, 0., 1.), ccr = sclamp(crv, 0., 1.);
                     if (!nonfinite) {
                         clO = oc - onv;
@@ -489,15 +496,18 @@ struct OnePassStep {
     }
 };
 
-template <bool FAST, int N>
+template <bool FAST, int N, int MODE>
 __global__ void __launch_bounds__(FTA * FTB, 1)
 k_step_fused(const StepParams P, const __grid_constant__ CUtensorMap m_int, const __grid_constant__ CUtensorMap m_row,
              const __grid_constant__ CUtensorMap m_col, const __grid_constant__ CUtensorMap m_crn,
              const double* __restrict__ o, const double* __restrict__ cr, const double* __restrict__ p,
              double* __restrict__ on, double* __restrict__ crn, double* __restrict__ pn,
              double* __restrict__ eta_next, StepPartial* __restrict__ partials, Status* st) {
-    OnePassStep<FAST, N>::run(P, &m_int, &m_row, &m_col, &m_crn, o, cr, p, on, crn, pn, eta_next, partials, st);
+    OnePassStep<FAST, N, MODE>::run(P, &m_int, &m_row, &m_col, &m_crn, o, cr, p, on, crn, pn, eta_next, partials, st);
 }
+
+// The flag combination k_step_fused instantiates with the flags folded (MODE 1).
+inline bool fused_common_mode(const StepParams& P) { return P.o_on && P.ck == 0 && P.bounds == 1; }
 
 // Whether the fused step serves grid g with n eta fields (the eta buffer's
 // 16-byte alignment is checked at launch).
@@ -515,10 +525,16 @@ static bool launch_step_fused_n(const StepParams& P, const double* o, const doub
         !encode_eta_map(&mc, g, N, eta, 2, FTA, 1) || !encode_eta_map(&mk, g, N, eta, 2, 1, N))
         return false;
     using L = FusedLayout<N>;
-    ensure_smem_attr((const void*)k_step_fused<FAST, N>, (int)L::BYTES);
     const dim3 grid(g.nb / FTB, g.na / FTA, (g.nx + P.xchunk - 1) / P.xchunk);
-    k_step_fused<FAST, N><<<grid, dim3(FTB, FTA), L::BYTES, stream>>>(P, mi, mr, mc, mk, o, cr, p, on, crn, pn,
-                                                                      eta_next, partials, st);
+    if (fused_common_mode(P)) {
+        ensure_smem_attr((const void*)k_step_fused<FAST, N, 1>, (int)L::BYTES);
+        k_step_fused<FAST, N, 1><<<grid, dim3(FTB, FTA), L::BYTES, stream>>>(P, mi, mr, mc, mk, o, cr, p, on, crn,
+                                                                            pn, eta_next, partials, st);
+    } else {
+        ensure_smem_attr((const void*)k_step_fused<FAST, N, 0>, (int)L::BYTES);
+        k_step_fused<FAST, N, 0><<<grid, dim3(FTB, FTA), L::BYTES, stream>>>(P, mi, mr, mc, mk, o, cr, p, on, crn,
+                                                                            pn, eta_next, partials, st);
+    }
     if (nblocks_out) *nblocks_out = (int)(grid.x * grid.y * grid.z);
     return true;
 }
@@ -545,7 +561,10 @@ template <bool FAST>
 static void step_fused_prepare(int n) {
     switch (n) {
 #define NICR_FUSED_PREP_CASE(k) \
-    case k: ensure_smem_attr((const void*)k_step_fused<FAST, k>, (int)FusedLayout<k>::BYTES); break;
+    case k:                                                                                  \
+        ensure_smem_attr((const void*)k_step_fused<FAST, k, 0>, (int)FusedLayout<k>::BYTES); \
+        ensure_smem_attr((const void*)k_step_fused<FAST, k, 1>, (int)FusedLayout<k>::BYTES); \
+        break;
         NICR_FUSED_PREP_CASE(1) NICR_FUSED_PREP_CASE(2) NICR_FUSED_PREP_CASE(3) NICR_FUSED_PREP_CASE(4)
         NICR_FUSED_PREP_CASE(5) NICR_FUSED_PREP_CASE(6) NICR_FUSED_PREP_CASE(7) NICR_FUSED_PREP_CASE(8)
 #undef NICR_FUSED_PREP_CASE
