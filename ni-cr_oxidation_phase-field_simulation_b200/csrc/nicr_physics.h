@@ -92,27 +92,43 @@ inline EtaCoef eta_coef(double fwhm, double dx, double W, double kappa, double p
 }
 
 // Division by a run constant b, correctly rounded (bit-identical to a / b).
-// q1 = a*RN(1/b) refined by one FMA residual step is accepted only when an
-// exact FMA residual proves it is the nearest double: |a - q1*b| < |b|*ulp(q1)/2
-// (strict, so ties are excluded; q1 a power of two is excluded because its
-// lower neighbour is closer). The residual is exact whenever q1 is within an
-// ulp of a/b, and when it is not, its rounded value cannot pass the test, so
-// an accepted q1 is always RN(a/b). Zeros return a * RN(1/b), the exactly
-// signed zero. Outside the guarded exponent range (subnormals, infinities,
-// NaNs) the IEEE division is used. The scale factor
-// 2^(53-E) (E = exponent of q1) keeps the comparison free of underflow.
+// The host stores y = RN(1/b) and the double-word reciprocal zh = RD(1/b),
+// zl = RN(1/b - zh) >= 0 (Brisebarre, Muller, Raina, "Accelerating correctly
+// rounded floating-point division when the divisor is known in advance",
+// IEEE Trans. Comput. 53(8), 2004). For b > 0 with 2^-60 <= b <= 2^60 and a
+// numerator of biased exponent 123..1923:
+//   q0 = RN(a*zh + RN(a*zl))   within (1/2 + 2^-51) ulp of a/b,
+//   e  = q0*b - a              exact, because q0 is within one ulp of a/b,
+//   q  = RN(q0 - e*y)          = RN(a/b),
+// the last line being Markstein's correction theorem (IBM J. Res. Dev. 34(1),
+// 1990: q0 within one ulp of a/b and y within half an ulp of 1/b make
+// RN(q0 + r*y), r = a - b*q0, the correctly rounded quotient). The exponent
+// range keeps every intermediate normal and the quotient in [2^-961, 2^961].
+// Zeros come out with the IEEE sign because zl >= 0 and e is formed as
+// q0*b - a (+0 for a = +-0, b > 0). Any other numerator (subnormal, tiny,
+// huge, infinite, NaN) and every numerator of a divisor outside the range
+// take the IEEE division. tests/division_check.c restates this on the host
+// and checks it against IEEE division, near-midpoint quotients included.
 struct DivC {
-    double b, rb;   // divisor and RN(1/b)
-    int fast;       // b normal with 2^-60 <= |b| <= 2^60
-    int pad;
+    double b, rb;      // divisor and y = RN(1/b) (the reciprocal form multiplies by it)
+    double zh, zl;     // RD(1/b) and RN(1/b - RD(1/b))
+    unsigned erange;   // 1801 << 20 when b is in range, else 0 (no numerator passes)
+    unsigned gate;     // 0 when b is in range, else 1 (zeros take the IEEE division too)
 };
 inline DivC make_divc(double b) {
     DivC d;
     d.b = b;
     d.rb = 1.0 / b;
-    const double ab = std::fabs(b);
-    d.fast = (std::isnormal(b) && ab >= std::ldexp(1.0, -60) && ab <= std::ldexp(1.0, 60)) ? 1 : 0;
-    d.pad = 0;
+    d.zh = d.rb;
+    double rem = std::fma(-d.zh, b, 1.0);   // exact: zh is within one ulp of 1/b
+    if (rem < 0.) {
+        d.zh = std::nextafter(d.zh, 0.0);
+        rem = std::fma(-d.zh, b, 1.0);
+    }
+    d.zl = rem / b;
+    const bool in_range = std::isnormal(b) && b > 0. && b >= std::ldexp(1.0, -60) && b <= std::ldexp(1.0, 60);
+    d.erange = in_range ? 0x70900000u : 0u;
+    d.gate = in_range ? 0u : 1u;
     return d;
 }
 #ifdef __CUDACC__
@@ -125,25 +141,12 @@ __device__ __forceinline__ double xdiv(double a, const DivC& d) {
 #elif defined(NICR_DIV_IEEE)
     return __ddiv_rn(a, d.b);
 #else
-    // Zeros (common: the Laplacian of a uniform region) return at once; the
-    // rest is computed without branches, and one rarely taken branch picks
-    // the IEEE division when the certificate fails.
-    const long long ab = __double_as_longlong(a);
-    const int ea = (int)((ab >> 52) & 0x7FF);
-    const double q0 = __dmul_rn(a, d.rb);
-    // +-0 / b is an exactly signed zero, which a * RN(1/b) reproduces
-    if (d.fast && (ab << 1) == 0) return q0;
-    const double r0 = __fma_rn(-q0, d.b, a);
-    const double q1 = __fma_rn(r0, d.rb, q0);
-    const double r1 = __fma_rn(-q1, d.b, a);
-    const long long qb = __double_as_longlong(q1);
-    const int eq = (int)((qb >> 52) & 0x7FF);
-    // 2^(1076 - eq) = 1 / (ulp(q1) / 2); meaningful when a is in range, which
-    // the certificate requires (the quotient's exponent then lies in [63, 1983])
-    const double scale = __longlong_as_double((long long)((unsigned long long)(2099 - eq) << 52));
-    const bool cert = ea >= 123 && ea <= 1923 && (qb & 0x000FFFFFFFFFFFFFLL) != 0 &&
-                      __dmul_rn(fabs(r1), scale) < fabs(d.b);
-    if (d.fast && cert) return q1;
+    const unsigned h = (unsigned)__double2hiint(a) & 0x7FFFFFFFu, lo = (unsigned)__double2loint(a);
+    const double q0 = __fma_rn(a, d.zh, __dmul_rn(a, d.zl));
+    const double e = __fma_rn(q0, d.b, -a);
+    const double q = __fma_rn(-e, d.rb, q0);
+    // biased exponent 123..1923 (h in [123 << 20, 1924 << 20)), or a zero
+    if ((h - 0x07B00000u) < d.erange || (h | lo | d.gate) == 0u) return q;
 #if defined(NICR_DIV_INLINE_FALLBACK)
     return __ddiv_rn(a, d.b);
 #else

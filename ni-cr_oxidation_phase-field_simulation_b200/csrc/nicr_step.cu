@@ -54,16 +54,39 @@ __global__ void k_eta_mask(const StepParams P, int neta, const double* __restric
     }
 }
 
-// Self-check of xdiv on the device: random numerators (all finite bit
-// patterns, and values of typical magnitude) against IEEE division.
+// Self-check of xdiv on the device against IEEE division: random numerators
+// (all finite bit patterns, values of typical magnitude, signed zeros) and,
+// every fifth one, a numerator whose quotient lies within ~2^-104 relative of
+// a rounding midpoint. The latter: b's odd mantissa part B, M = delta / B mod
+// 2^54 for delta in {-3, -1, 1, 3}, kept when M has 54 bits; then
+// B * M = A * 2^54 + delta and A (scaled) / b is next to the midpoint M * 2^-54.
 __global__ void k_check_division(DivC d, long long n, unsigned long long seed, unsigned long long* counts) {
     unsigned long long bad = 0, total = 0;
+    unsigned long long B = ((unsigned long long)__double_as_longlong(d.b) & 0x000FFFFFFFFFFFFFull) | (1ull << 52);
+    while (!(B & 1)) B >>= 1;
+    unsigned long long inv = B;   // Newton's iteration for 1 / B modulo 2^64
+    for (int k = 0; k < 6; ++k) inv *= 2 - B * inv;
+    const unsigned long long m54 = (1ull << 54) - 1;
+    inv &= m54;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
         unsigned long long x = seed ^ (0x9E3779B97F4A7C15ull * (unsigned long long)(i + 1));
         x ^= x >> 33; x *= 0xff51afd7ed558ccdull; x ^= x >> 33; x *= 0xc4ceb9fe1a85ec53ull; x ^= x >> 33;
         double a;
         if (i % 97 == 0) {
             a = (i & 1) ? -0.0 : 0.0;
+        } else if (i % 5 == 1) {
+            const long long delta = ((long long)((x >> 60) & 7) - 4) | 1;
+            const unsigned long long M = ((unsigned long long)delta * inv) & m54;
+            if (!(M >> 53)) continue;
+            // num = B * M - delta as 128 bits (hi:lo); its low 54 bits are zero
+            unsigned long long lo = B * M, hi = __umul64hi(B, M);
+            const unsigned long long dl = (unsigned long long)delta;
+            const unsigned long long nlo = lo - dl;
+            hi -= (delta > 0 && nlo > lo) ? 1ull : 0ull;
+            hi += (delta < 0 && nlo < lo) ? 1ull : 0ull;
+            const unsigned long long A = (hi << 10) | (nlo >> 54);
+            a = ldexp((double)A, (int)((x >> 8) % 1600) - 800);
+            if (x & 1) a = -a;
         } else if (i & 3) {
             const int e = (int)((x >> 56) % 120) - 60;
             a = ldexp((double)(x >> 11) * (1.0 / 9007199254740992.0) + 0.5, e);

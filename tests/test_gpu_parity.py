@@ -142,10 +142,13 @@ def test_run_schedule_with_ksp(require_gpu, dim):
     assert sol.budget()["nuclei"] > 0
 
 
-@pytest.mark.parametrize("b", [1e-16, 1.0000000000000002e-16, 1e-8, 2e-10, 1e-12, 3.3e-9, 0.7, 3.0])
+@pytest.mark.parametrize("b", [1e-16, 1.0000000000000002e-16, 1e-8, 2e-10, 1e-12, 3.3e-9, 0.7, 3.0,
+                               1.9999999999999998, 1.4142135623730951, 2.0 ** -60, 2.0 ** 61, -3.0])
 def test_verified_division_matches_ieee(require_gpu, b):
-    """xdiv (reciprocal + FMA correction + exact residual proof, IEEE fallback)
-    returns exactly a/b on the device for 2^27 seeded numerators per divisor."""
+    """xdiv (double-word reciprocal, one Markstein correction step, IEEE
+    division outside the guarded range) returns exactly a/b on the device for
+    2^27 seeded numerators per divisor, a fifth of them with quotients next to
+    a rounding midpoint; 2^61 and -3 lie outside the guarded divisor range."""
     import ctypes
     L = nicr.lib()
     L.nicr_check_division.argtypes = [ctypes.c_double, ctypes.c_longlong, ctypes.c_ulonglong,
