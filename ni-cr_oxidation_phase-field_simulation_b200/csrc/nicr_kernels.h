@@ -54,7 +54,8 @@ struct DevBudget {
 struct StepPartial {
     double s[5][2];
     long long clipped;
-    long long pad;
+    int redo;   // drop-in form: the CTA's chunk awaits the recomputation kernel
+    int pad;
 };
 
 struct StepParams {
@@ -100,6 +101,9 @@ void launch_step_main(const StepParams& P, const double* o, const double* cr, co
                       const double* gb, const double* s2, double* on, double* crn, double* pn,
                       StepPartial* partials, Status* st, cudaStream_t stream, int* nblocks_out);
 int step_main_blocks(const StepParams& P);
+// kernels launch_step_main launches: the drop-in form adds the recomputation
+// kernel of CTAs whose numerators left the exact-division range
+int step_main_kernels(const StepParams& P);
 // Planes per CTA along X for grid g (step and eta kernels), and one chunk for
 // the n domains of a batch. NICR_XCHUNK forces a chunk for tuning runs.
 int choose_xchunk(const Grid& g);

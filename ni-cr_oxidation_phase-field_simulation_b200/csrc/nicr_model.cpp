@@ -951,7 +951,7 @@ void Model::enqueue_step() {
     }
     const size_t e = prof_begin();
     launch_step_main(sp, d.o, d.cr, d.p, d.gb, d.s2, d.on, d.crn, d.pn, partials, st, stream, &nb);
-    prof_end(K_STEP_MAIN, e, 1);
+    prof_end(K_STEP_MAIN, e, step_main_kernels(sp));
     complete_step(nb, true);
 }
 
@@ -1177,7 +1177,7 @@ int Model::slab_launch() {
     size_t e = prof_begin();
     launch_step_main(P, o_[cur], cr_[cur], p_[cur], gb_[gcur], has_eta ? s2_[gcur] : nullptr, o_[cur ^ 1],
                      cr_[cur ^ 1], p_[cur ^ 1], partials, st, stream, &nb);
-    prof_end(K_STEP_MAIN, e, 1);
+    prof_end(K_STEP_MAIN, e, step_main_kernels(P));
     if (advance_eta) {
         e = prof_begin();
         launch_eta_update(P, neta, eta_[ecur], s2_[gcur], p_[cur], eta_[ecur ^ 1], gb_[gcur ^ 1], s2_[gcur ^ 1], st, stream);

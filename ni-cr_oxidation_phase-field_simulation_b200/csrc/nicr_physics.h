@@ -135,24 +135,23 @@ inline DivC make_divc(double b) {
 // IEEE division kept out of line: it is only the rare fallback, and inlining
 // it at every call site would multiply the kernels' instruction footprint.
 __device__ __noinline__ double ieee_div(double a, double b);
-__device__ __forceinline__ double xdiv(double a, const DivC& d) {
-#if defined(NICR_DIV_RECIP)
-    return __dmul_rn(a, d.rb);
-#elif defined(NICR_DIV_IEEE)
-    return __ddiv_rn(a, d.b);
-#else
+// The exact quotient for numerators in the guarded range; any other numerator
+// sets `bad` (the value returned for it is then not the IEEE quotient), so a
+// caller can test once for a whole group of divisions and recompute the group
+// with IEEE division.
+__device__ __forceinline__ double xdiv_flag(double a, const DivC& d, unsigned& bad) {
     const unsigned h = (unsigned)__double2hiint(a) & 0x7FFFFFFFu, lo = (unsigned)__double2loint(a);
     const double q0 = __fma_rn(a, d.zh, __dmul_rn(a, d.zl));
     const double e = __fma_rn(q0, d.b, -a);
     const double q = __fma_rn(-e, d.rb, q0);
     // biased exponent 123..1923 (h in [123 << 20, 1924 << 20)), or a zero
-    if ((h - 0x07B00000u) < d.erange || (h | lo | d.gate) == 0u) return q;
-#if defined(NICR_DIV_INLINE_FALLBACK)
-    return __ddiv_rn(a, d.b);
-#else
-    return ieee_div(a, d.b);
-#endif
-#endif
+    bad |= ((h - 0x07B00000u) < d.erange || (h | lo | d.gate) == 0u) ? 0u : 1u;
+    return q;
+}
+__device__ __forceinline__ double xdiv(double a, const DivC& d) {
+    unsigned bad = 0;
+    const double q = xdiv_flag(a, d, bad);
+    return bad ? ieee_div(a, d.b) : q;
 }
 #endif
 

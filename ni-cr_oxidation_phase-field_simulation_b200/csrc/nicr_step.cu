@@ -347,6 +347,8 @@ void step_kernels_prepare(const StepParams& P) {
     ensure_smem_attr(k, (int)T::SMEM_BYTES);
 }
 
+int step_main_kernels(const StepParams& P) { return P.fast ? 1 : 2; }
+
 void launch_step_main(const StepParams& P, const double* o, const double* cr, const double* p, const double* gb,
                       const double* s2, double* on, double* crn, double* pn, StepPartial* partials, Status* st,
                       cudaStream_t stream, int* nblocks_out) {

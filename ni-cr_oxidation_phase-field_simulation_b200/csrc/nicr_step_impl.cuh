@@ -97,6 +97,57 @@ __device__ __forceinline__ double fdiv(double a, const DivC& d) {
     return xdiv(a, d);
 }
 
+// Divisions of the cell arithmetic, as policies the shared arithmetic (lead
+// points, cell updates) is written against. DivRun<true>: the reciprocal form.
+// DivRun<false>: the exact quotient for numerators in the guarded range
+// (xdiv_flag), raising `bad` for any other numerator instead of branching, so
+// the march carries no branch or call per division; a CTA that raised it
+// marches its chunk again with DivExact before it publishes anything, so every
+// result is still the IEEE quotient.
+template <bool FAST>
+struct DivRun {
+    const StepParams& P;
+    unsigned& bad;
+    __device__ double q(double v, const DivC& d) const {
+        if (FAST) return __dmul_rn(v, d.rb);
+        return xdiv_flag(v, d, bad);
+    }
+    __device__ double dvx(double v) const { return q(v, P.v_dx); }
+    __device__ double dva(double v) const { return q(v, P.v_da); }
+    __device__ double dvb(double v) const { return q(v, P.v_db); }
+    __device__ double dvxx(double v) const { return q(v, P.v_dxdx); }
+    __device__ double dvaa(double v) const { return q(v, P.v_dada); }
+    __device__ double dvbb(double v) const { return q(v, P.v_dbdb); }
+    __device__ double dvt(double v) const { return q(v, P.v_dt); }
+};
+// exact for every numerator: xdiv, with the IEEE division (an out-of-line
+// call) for numerators outside the guarded range
+struct DivExact {
+    const StepParams& P;
+    unsigned& bad;   // unused: every result is exact
+    __device__ double dvx(double v) const { return xdiv(v, P.v_dx); }
+    __device__ double dva(double v) const { return xdiv(v, P.v_da); }
+    __device__ double dvb(double v) const { return xdiv(v, P.v_db); }
+    __device__ double dvxx(double v) const { return xdiv(v, P.v_dxdx); }
+    __device__ double dvaa(double v) const { return xdiv(v, P.v_dada); }
+    __device__ double dvbb(double v) const { return xdiv(v, P.v_dbdb); }
+    __device__ double dvt(double v) const { return xdiv(v, P.v_dt); }
+};
+// The policy of a march pass: 0 the reciprocal form; 1 the drop-in form's
+// first pass (exact quotients, out-of-range numerators flagged); 2 the drop-in
+// form's recomputation of a CTA whose first pass raised the flag.
+template <int DM> struct DivOf;
+template <> struct DivOf<0> { using T = DivRun<true>; };
+template <> struct DivOf<1> { using T = DivRun<false>; };
+template <> struct DivOf<2> { using T = DivExact; };
+// The scalars the cell arithmetic reads besides the divisors.
+struct CellK {
+    double dt, dtL, eta_W, eta_A, eta_K, dt_etaL, gbm1_o, gbm1_cr;
+};
+__device__ __forceinline__ CellK cell_k(const StepParams& P) {
+    return CellK{P.dt, P.dtL, P.eta_W, P.eta_A, P.eta_K, P.dt_etaL, P.gbm1_o, P.gbm1_cr};
+}
+
 // The error word a launch with parameters P reports its first failing trial to.
 __device__ __forceinline__ unsigned long long* err_word(const StepParams& P, Status* st) {
     return P.err_slot < 0 ? &st->err_key : &st->slot_err[P.err_slot];
@@ -235,26 +286,24 @@ struct StepKernel {
     }
 
     // mu and M at tile point (a,b) of real plane x; writes the mu/M slot.
-    __device__ static CenterVals lead_point(const StepParams& P, const double* __restrict__ gb,
-                                            const double* som, const double* so0, const double* sop,
-                                            const double* scm, const double* sc0, const double* scp,
-                                            const double* sp, double* smuO, double* smuCr, double* smo,
-                                            double* smc, int a, int b, double gbv) {
+    template <class Dv>
+    __device__ static CenterVals lead_core(const Dv& dv, const CellK& k, bool o_on, const double* som,
+                                           const double* so0, const double* sop, const double* scm, const double* sc0,
+                                           const double* scp, const double* sp, double* smuO, double* smuCr,
+                                           double* smo, double* smc, int a, int b, double gbv) {
         const int c2 = T::i2(a, b);
         const double oc = so0[c2], cc = sc0[c2];
         double lapO, lapC;
         if (DIM == 3) {
-            lapO = fdiv<FAST>((sop[c2] - 2. * oc + som[c2]), P.v_dxdx)
-                 + fdiv<FAST>((so0[T::i2(a + 1, b)] - 2. * oc + so0[T::i2(a - 1, b)]), P.v_dada)
-                 + fdiv<FAST>((so0[T::i2(a, b + 1)] - 2. * oc + so0[T::i2(a, b - 1)]), P.v_dbdb);
-            lapC = fdiv<FAST>((scp[c2] - 2. * cc + scm[c2]), P.v_dxdx)
-                 + fdiv<FAST>((sc0[T::i2(a + 1, b)] - 2. * cc + sc0[T::i2(a - 1, b)]), P.v_dada)
-                 + fdiv<FAST>((sc0[T::i2(a, b + 1)] - 2. * cc + sc0[T::i2(a, b - 1)]), P.v_dbdb);
+            lapO = dv.dvxx((sop[c2] - 2. * oc + som[c2]))
+                 + dv.dvaa((so0[T::i2(a + 1, b)] - 2. * oc + so0[T::i2(a - 1, b)]))
+                 + dv.dvbb((so0[T::i2(a, b + 1)] - 2. * oc + so0[T::i2(a, b - 1)]));
+            lapC = dv.dvxx((scp[c2] - 2. * cc + scm[c2]))
+                 + dv.dvaa((sc0[T::i2(a + 1, b)] - 2. * cc + sc0[T::i2(a - 1, b)]))
+                 + dv.dvbb((sc0[T::i2(a, b + 1)] - 2. * cc + sc0[T::i2(a, b - 1)]));
         } else {
-            lapO = fdiv<FAST>((sop[c2] - 2. * oc + som[c2]), P.v_dxdx)
-                 + fdiv<FAST>((so0[T::i2(a, b + 1)] - 2. * oc + so0[T::i2(a, b - 1)]), P.v_dbdb);
-            lapC = fdiv<FAST>((scp[c2] - 2. * cc + scm[c2]), P.v_dxdx)
-                 + fdiv<FAST>((sc0[T::i2(a, b + 1)] - 2. * cc + sc0[T::i2(a, b - 1)]), P.v_dbdb);
+            lapO = dv.dvxx((sop[c2] - 2. * oc + som[c2])) + dv.dvbb((so0[T::i2(a, b + 1)] - 2. * oc + so0[T::i2(a, b - 1)]));
+            lapC = dv.dvxx((scp[c2] - 2. * cc + scm[c2])) + dv.dvbb((sc0[T::i2(a, b + 1)] - 2. * cc + sc0[T::i2(a, b - 1)]));
         }
         const int c1 = T::i1(a, b);
         const double pc = sp[c1];
@@ -263,17 +312,100 @@ struct StepKernel {
         v.o = oc; v.cr = cc; v.p = pc; v.hh = hh;
         v.muO = mu_o_local(oc, cc, hh) - 2. * Phys::ko * lapO;
         v.muCr = mu_cr_local(oc, cc, hh) - 2. * Phys::kc * lapC;
-        v.mo = P.o_on ? mobility(oc, hh, gbv, Phys::bmo, Phys::boo, P.gbm1_o) : 0.;
-        v.mc = mobility(cc, hh, gbv, Phys::bmc, Phys::boc, P.gbm1_cr);
+        v.mo = o_on ? mobility(oc, hh, gbv, Phys::bmo, Phys::boo, k.gbm1_o) : 0.;
+        v.mc = mobility(cc, hh, gbv, Phys::bmc, Phys::boc, k.gbm1_cr);
         smuO[c1] = v.muO; smuCr[c1] = v.muCr; smo[c1] = v.mo; smc[c1] = v.mc;
         return v;
     }
+    // lead_core with the per-division policy of the form (every quotient exact)
+    __device__ static CenterVals lead_point(const StepParams& P, const double* __restrict__ gb,
+                                            const double* som, const double* so0, const double* sop,
+                                            const double* scm, const double* sc0, const double* scp,
+                                            const double* sp, double* smuO, double* smuCr, double* smo,
+                                            double* smc, int a, int b, double gbv) {
+        unsigned bad = 0;
+        typename DivOf<FAST ? 0 : 2>::T dv{P, bad};
+        return lead_core(dv, cell_k(P), P.o_on != 0, som, so0, sop, scm, sc0, scp, sp, smuO, smuCr, smo, smc, a, b,
+                         gbv);
+    }
 
-    __device__ static void run(const StepParams P, const double* __restrict__ o, const double* __restrict__ cr,
-                               const double* __restrict__ p, const double* __restrict__ gb,
-                               const double* __restrict__ s2, double* __restrict__ on,
-                               double* __restrict__ crn, double* __restrict__ pn,
-                               StepPartial* __restrict__ partials, Status* st, int bx, int by, int bz, int blin) {
+    // The flux divergence, phi force and Ck of the cell at (ta, tb) of plane u
+    // (C: plane u, L: plane u+1, pP: phi of plane u-1, leftO/leftCr: its -X
+    // face fluxes), before the trial test and the clamps.
+    struct CoreOut {
+        double onv, crv, pnv, rightO, rightCr, dO, dCr;
+    };
+    template <class Dv>
+    __device__ static CoreOut cell_core(const Dv& dv, const CellK& k, bool o_on, bool ck_legacy, bool phi_eta,
+                                        const CenterVals& C, const CenterVals& L, double pP, double leftO,
+                                        double leftCr, double s2u, const double* mO, const double* mC,
+                                        const double* mo_, const double* mc_, const double* spu, int c1, int bp,
+                                        int bm, int ap, int am) {
+        CoreOut r;
+        // x faces: the right face of u is the left face of u+1 (same expression)
+        r.rightO = dv.dvx(-.5 * (C.mo + L.mo) * (L.muO - C.muO));
+        r.rightCr = dv.dvx(-.5 * (C.mc + L.mc) * (L.muCr - C.muCr));
+        double divO = 0., divCr;
+        {
+            const double mc0 = mc_[c1], mu0 = mC[c1];
+            const double front = dv.dvb(-.5 * (mc0 + mc_[bp]) * (mC[bp] - mu0));
+            const double back = dv.dvb(-.5 * (mc_[bm] + mc0) * (mu0 - mC[bm]));
+            if (DIM == 3) {
+                const double top = dv.dva(-.5 * (mc0 + mc_[ap]) * (mC[ap] - mu0));
+                const double bottom = dv.dva(-.5 * (mc_[am] + mc0) * (mu0 - mC[am]));
+                divCr = dv.dvx(leftCr - r.rightCr) + dv.dva(bottom - top) + dv.dvb(back - front);
+            } else {
+                divCr = dv.dvx(leftCr - r.rightCr) + dv.dvb(back - front);
+            }
+        }
+        if (o_on) {
+            const double m0 = mo_[c1], mu0 = mO[c1];
+            const double front = dv.dvb(-.5 * (m0 + mo_[bp]) * (mO[bp] - mu0));
+            const double back = dv.dvb(-.5 * (mo_[bm] + m0) * (mu0 - mO[bm]));
+            if (DIM == 3) {
+                const double top = dv.dva(-.5 * (m0 + mo_[ap]) * (mO[ap] - mu0));
+                const double bottom = dv.dva(-.5 * (mo_[am] + m0) * (mu0 - mO[am]));
+                divO = dv.dvx(leftO - r.rightO) + dv.dva(bottom - top) + dv.dvb(back - front);
+            } else {
+                divO = dv.dvx(leftO - r.rightO) + dv.dvb(back - front);
+            }
+        }
+        const double oo = C.o, cc = C.cr, pp = C.p;
+        double onv = o_on ? oo + k.dt * divO : oo;
+        double crv = cc + k.dt * divCr;
+        double lapP;
+        if (DIM == 3)
+            lapP = dv.dvxx((L.p - 2. * pp + pP)) + dv.dvaa((spu[ap] - 2. * pp + spu[am]))
+                 + dv.dvbb((spu[bp] - 2. * pp + spu[bm]));
+        else
+            lapP = dv.dvxx((L.p - 2. * pp + pP)) + dv.dvbb((spu[bp] - 2. * pp + spu[bm]));
+        const double hpv = 30. * pp * pp * (pp - 1.) * (pp - 1.);
+        double fp = Phys::W * (4. * pp * pp * pp - 6. * pp * pp + 2. * pp)
+                  + hpv * (foxide(oo, cc) - fmetal(oo, cc)) - 2. * Phys::kp * lapP;
+        if (phi_eta) fp += grain_dphi(s2u, pp, k.eta_W, k.eta_A);
+        r.pnv = pp - k.dtL * fp;
+        r.dO = 0.;
+        r.dCr = 0.;
+        if (ck_legacy) {
+            const double hn = h(r.pnv);
+            r.dO = dv.dvt(-Phys::ckO * ((Phys::oxideO - onv) * hn - (Phys::oxideO - oo) * C.hh));
+            r.dCr = dv.dvt(-Phys::ckCr * ((Phys::oxideCr - crv) * hn - (Phys::oxideCr - cc) * C.hh));
+            onv += r.dO;
+            crv += r.dCr;
+        }
+        r.onv = onv;
+        r.crv = crv;
+        return r;
+    }
+    // One march over the CTA's chunk with the division policy of DM (DivOf).
+    // DM 1 returns true, without publishing its failure keys or budget
+    // partials, when a numerator of the chunk left the guarded range.
+    template <int DM>
+    __device__ static bool run_body(const StepParams& P, const double* __restrict__ o, const double* __restrict__ cr,
+                                    const double* __restrict__ p, const double* __restrict__ gb,
+                                    const double* __restrict__ s2, double* __restrict__ on,
+                                    double* __restrict__ crn, double* __restrict__ pn,
+                                    StepPartial* __restrict__ partials, Status* st, int bx, int by, int bz, int blin) {
         extern __shared__ __align__(16) double smem[];
         double* so = smem;                 // 4 slots x S2
         double* scr = so + 4 * T::S2;      // 4 slots x S2
@@ -298,7 +430,10 @@ struct StepKernel {
         long long clipped = 0;
         unsigned long long errkey = ERR_NONE;
 
-        if (st->failed) return;  // a previous step of this batch was rejected
+        if (st->failed) return false;  // a previous step of this batch was rejected
+        unsigned bad = 0;
+        const typename DivOf<DM>::T dv{P, bad};
+        const CellK kc = cell_k(P);
 
         auto slot3 = [](int w) { return ((w % 3) + 3) % 3; };
         // o/cr ring of 4 planes: the plane staged at the top of an iteration
@@ -317,14 +452,15 @@ struct StepKernel {
             double* mC = smuCr + (x & 1) * T::S1;
             double* mo_ = smo + (x & 1) * T::S1;
             double* mc_ = smc + (x & 1) * T::S1;
-            CenterVals own = lead_point(P, gb, som, so0, sop, scm, sc0, scp, spx, mO, mC, mo_, mc_, ta, tb, gbl[0]);
+            CenterVals own = lead_core(dv, kc, P.o_on != 0, som, so0, sop, scm, sc0, scp, spx, mO, mC, mo_, mc_, ta,
+                                       tb, gbl[0]);
             // halo ring points: one per thread for the first S1-NT threads
             static_assert(T::S1 - T::NT <= T::NT, "ring larger than the CTA");
             const int tid = threadIdx.x + TB * threadIdx.y;
             if (offs.gl[1] >= 0) {
                 int a, b;
                 ring_point(tid, a, b);
-                lead_point(P, gb, som, so0, sop, scm, sc0, scp, spx, mO, mC, mo_, mc_, a, b, gbl[1]);
+                lead_core(dv, kc, P.o_on != 0, som, so0, sop, scm, sc0, scp, spx, mO, mC, mo_, mc_, a, b, gbl[1]);
             }
             return own;
         };
@@ -344,8 +480,8 @@ struct StepKernel {
             __syncthreads();
             // ghost plane -1: copies of plane 0 (3S:187, 3S:613-615, 3S:616-619)
             const double muOg = (P.bc == 1 && P.o_on) ? 2. * P.mu_res - C.muO : C.muO;
-            FxO = fdiv<FAST>(-.5 * (C.mo + C.mo) * (C.muO - muOg), P.v_dx);
-            FxCr = fdiv<FAST>(-.5 * (C.mc + C.mc) * (C.muCr - C.muCr), P.v_dx);
+            FxO = dv.dvx(-.5 * (C.mo + C.mo) * (C.muO - muOg));
+            FxCr = dv.dvx(-.5 * (C.mc + C.mc) * (C.muCr - C.muCr));
             pP = C.p;
         } else {
             load_oc(P, o, cr, i0 - 2, oslot(i0 - 2), cslot(i0 - 2), offs);
@@ -363,8 +499,8 @@ struct StepKernel {
             __syncthreads();
             C = lead(i0, gb0);
             __syncthreads();
-            FxO = fdiv<FAST>(-.5 * (Pv.mo + C.mo) * (C.muO - Pv.muO), P.v_dx);
-            FxCr = fdiv<FAST>(-.5 * (Pv.mc + C.mc) * (C.muCr - Pv.muCr), P.v_dx);
+            FxO = dv.dvx(-.5 * (Pv.mo + C.mo) * (C.muO - Pv.muO));
+            FxCr = dv.dvx(-.5 * (Pv.mc + C.mc) * (C.muCr - Pv.muCr));
             pP = Pv.p;
         }
 
@@ -403,9 +539,6 @@ struct StepKernel {
                 const long long gidx = (long long)u * g.plane + (long long)row * g.pb + col;
                 const long long cell = ((long long)u * g.na + row) * g.nb + col + (SLAB ? P.cell_off : 0);  // reference loop order
 
-                // x faces: the right face of u is the left face of u+1 (same expression)
-                const double rightO = fdiv<FAST>(-.5 * (C.mo + L.mo) * (L.muO - C.muO), P.v_dx);
-                const double rightCr = fdiv<FAST>(-.5 * (C.mc + L.mc) * (L.muCr - C.muCr), P.v_dx);
                 double leftO = FxO;
                 if (u == 0 && P.bc == 1) {
                     // left_flux (3S:621-628): surface-mobility face closure for bc=mu
@@ -413,62 +546,21 @@ struct StepKernel {
                     if (P.o_on) {
                         const double gb0 = P.grains ? __ldg(gb + gidx) : 0.;
                         const double mf = mobility(P.surface_c_ref, h(C.p), gb0, Phys::bmo, Phys::boo, P.gbm1_o);
-                        lf = fdiv<FAST>(2. * mf * (P.mu_res - C.muO), P.v_dx);
+                        lf = dv.dvx(2. * mf * (P.mu_res - C.muO));
                     }
                     leftO = lf;
-                    acc[4] = dd_add(acc[4], fdiv<FAST>(P.dt * lf, P.v_dx));
+                    acc[4] = dd_add(acc[4], dv.dvx(P.dt * lf));
                 }
                 if (u == 0 && P.inlet) acc[4] = dd_add(acc[4], P.layer_o - __ldg(o + gidx));
 
-                double divO = 0., divCr;
-                {
-                    const double mc0 = mc_[c1], mu0 = mC[c1];
-                    const double front = fdiv<FAST>(-.5 * (mc0 + mc_[bp]) * (mC[bp] - mu0), P.v_db);
-                    const double back = fdiv<FAST>(-.5 * (mc_[bm] + mc0) * (mu0 - mC[bm]), P.v_db);
-                    if (DIM == 3) {
-                        const double top = fdiv<FAST>(-.5 * (mc0 + mc_[ap]) * (mC[ap] - mu0), P.v_da);
-                        const double bottom = fdiv<FAST>(-.5 * (mc_[am] + mc0) * (mu0 - mC[am]), P.v_da);
-                        divCr = fdiv<FAST>(FxCr - rightCr, P.v_dx) + fdiv<FAST>(bottom - top, P.v_da) + fdiv<FAST>(back - front, P.v_db);
-                    } else {
-                        divCr = fdiv<FAST>(FxCr - rightCr, P.v_dx) + fdiv<FAST>(back - front, P.v_db);
-                    }
-                }
-                if (P.o_on) {
-                    const double m0 = mo_[c1], mu0 = mO[c1];
-                    const double front = fdiv<FAST>(-.5 * (m0 + mo_[bp]) * (mO[bp] - mu0), P.v_db);
-                    const double back = fdiv<FAST>(-.5 * (mo_[bm] + m0) * (mu0 - mO[bm]), P.v_db);
-                    if (DIM == 3) {
-                        const double top = fdiv<FAST>(-.5 * (m0 + mo_[ap]) * (mO[ap] - mu0), P.v_da);
-                        const double bottom = fdiv<FAST>(-.5 * (mo_[am] + m0) * (mu0 - mO[am]), P.v_da);
-                        divO = fdiv<FAST>(leftO - rightO, P.v_dx) + fdiv<FAST>(bottom - top, P.v_da) + fdiv<FAST>(back - front, P.v_db);
-                    } else {
-                        divO = fdiv<FAST>(leftO - rightO, P.v_dx) + fdiv<FAST>(back - front, P.v_db);
-                    }
-                }
-                const double oo = C.o, cc = C.cr, pp = C.p;
-                double onv = P.o_on ? oo + P.dt * divO : oo;
-                double crv = cc + P.dt * divCr;
-                double lapP;
-                if (DIM == 3)
-                    lapP = fdiv<FAST>((L.p - 2. * pp + pP), P.v_dxdx) + fdiv<FAST>((spu[ap] - 2. * pp + spu[am]), P.v_dada)
-                         + fdiv<FAST>((spu[bp] - 2. * pp + spu[bm]), P.v_dbdb);
-                else
-                    lapP = fdiv<FAST>((L.p - 2. * pp + pP), P.v_dxdx) + fdiv<FAST>((spu[bp] - 2. * pp + spu[bm]), P.v_dbdb);
-                const double hpv = 30. * pp * pp * (pp - 1.) * (pp - 1.);
-                double fp = Phys::W * (4. * pp * pp * pp - 6. * pp * pp + 2. * pp)
-                          + hpv * (foxide(oo, cc) - fmetal(oo, cc)) - 2. * Phys::kp * lapP;
-                if (P.phi_eta) fp += grain_dphi(s2u, pp, P.eta_W, P.eta_A);
-                double pnv = pp - P.dtL * fp;
-                // Ck, the trial test and the clamps without data-dependent branches
-                // (so the scheduler sees one block); the rare bookkeeping (budget
-                // terms of changed cells, failure keys) is one branch after the stores
-                double dO = 0., dCr = 0.;
-                if (P.ck == 0) {
-                    const double hn = h(pnv);
-                    dO = fdiv<FAST>(-Phys::ckO * ((Phys::oxideO - onv) * hn - (Phys::oxideO - oo) * C.hh), P.v_dt);
-                    dCr = fdiv<FAST>(-Phys::ckCr * ((Phys::oxideCr - crv) * hn - (Phys::oxideCr - cc) * C.hh), P.v_dt);
-                    onv += dO; crv += dCr;
-                }
+                // fluxes, phi force and Ck (3S:761-811); the trial test and the
+                // clamps below without data-dependent branches (so the scheduler
+                // sees one block); the rare bookkeeping (budget terms of changed
+                // cells, failure keys) is one branch after the stores
+                const CoreOut R = cell_core(dv, kc, P.o_on != 0, P.ck == 0, P.phi_eta != 0, C, L, pP, leftO, FxCr,
+                                            s2u, mO, mC, mo_, mc_, spu, c1, bp, bm, ap, am);
+                double onv = R.onv, crv = R.crv, pnv = R.pnv;
+                const double dO = R.dO, dCr = R.dCr, rightO = R.rightO, rightCr = R.rightCr;
                 const bool nonfinite = !isfinite(onv) || !isfinite(crv) || !isfinite(pnv);
                 double clO = 0., clCr = 0.;
                 bool outside = false;
@@ -503,12 +595,39 @@ struct StepKernel {
             C = L;
             s2u = s2n;
         }
+        if (DM == 1 && __syncthreads_or(bad != 0)) return true;
         if (errkey != ERR_NONE) atomicMin(SLAB ? err_word(P, st) : &st->err_key, errkey);
         block_reduce_dd<5>(acc, clipped, sdd, scnt);
         if (threadIdx.x == 0 && threadIdx.y == 0) {
             StepPartial& out = partials[blin];
             for (int q = 0; q < 5; ++q) { out.s[q][0] = acc[q].hi; out.s[q][1] = acc[q].lo; }
             out.clipped = clipped;
+            out.redo = 0;
+        }
+        return false;
+    }
+
+    // One CTA's chunk. In the drop-in form a chunk whose numerators left the
+    // guarded range is marched again with every quotient exact (IEEE division
+    // for those), rewriting its trial values, before keys and partials are
+    // published: here (DEFER false), or by k_step_redo after the launch
+    // (DEFER true: the CTA only marks its partial slot), which keeps the
+    // second march and its division calls out of the hot kernel.
+    template <bool DEFER = false>
+    __device__ static void run(const StepParams& P, const double* __restrict__ o, const double* __restrict__ cr,
+                               const double* __restrict__ p, const double* __restrict__ gb,
+                               const double* __restrict__ s2, double* __restrict__ on,
+                               double* __restrict__ crn, double* __restrict__ pn,
+                               StepPartial* __restrict__ partials, Status* st, int bx, int by, int bz, int blin) {
+        if (FAST) {
+            run_body<0>(P, o, cr, p, gb, s2, on, crn, pn, partials, st, bx, by, bz, blin);
+        } else if (run_body<1>(P, o, cr, p, gb, s2, on, crn, pn, partials, st, bx, by, bz, blin)) {
+            if (DEFER) {
+                if (threadIdx.x == 0 && threadIdx.y == 0) partials[blin].redo = 1;
+            } else {
+                __syncthreads();
+                run_body<2>(P, o, cr, p, gb, s2, on, crn, pn, partials, st, bx, by, bz, blin);
+            }
         }
     }
 };
@@ -519,8 +638,28 @@ k_step_main(const StepParams P, const double* __restrict__ o, const double* __re
             const double* __restrict__ p, const double* __restrict__ gb, const double* __restrict__ s2,
             double* __restrict__ on, double* __restrict__ crn, double* __restrict__ pn,
             StepPartial* __restrict__ partials, Status* st) {
-    StepKernel<DIM, TA, TB, FAST, SLAB>::run(P, o, cr, p, gb, s2, on, crn, pn, partials, st, blockIdx.x, blockIdx.y,
-                                       blockIdx.z, blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z));
+    StepKernel<DIM, TA, TB, FAST, SLAB>::template run<true>(P, o, cr, p, gb, s2, on, crn, pn, partials, st, blockIdx.x,
+                                                            blockIdx.y, blockIdx.z,
+                                                            blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z));
+}
+
+// The drop-in form's recomputation of the chunks k_step_main marked (numerators
+// outside the exact-division range, which its march only flags): each CTA
+// takes marked chunks of the step grid (gx x gy x gz CTAs) in turn and marches
+// them with every quotient exact, rewriting trial values, key and partials.
+template <int DIM, int TA, int TB, bool SLAB = false>
+__global__ void __launch_bounds__(TA * TB, 1)
+k_step_redo(const StepParams P, const double* __restrict__ o, const double* __restrict__ cr,
+            const double* __restrict__ p, const double* __restrict__ gb, const double* __restrict__ s2,
+            double* __restrict__ on, double* __restrict__ crn, double* __restrict__ pn,
+            StepPartial* __restrict__ partials, Status* st, int gx, int gy, int nblocks) {
+    for (int blin = blockIdx.x; blin < nblocks; blin += gridDim.x) {
+        if (!partials[blin].redo) continue;   // the same word for the whole CTA
+        __syncthreads();                      // the previous chunk's shared-memory reads are done
+        StepKernel<DIM, TA, TB, false, SLAB>::template run_body<2>(P, o, cr, p, gb, s2, on, crn, pn, partials, st,
+                                                                   blin % gx, (blin / gx) % gy, blin / (gx * gy),
+                                                                   blin);
+    }
 }
 
 constexpr int TA3 = 8, TB3 = 32;    // 3D tile: 8 rows x 32 columns, 256 threads
@@ -613,17 +752,16 @@ __global__ void __launch_bounds__(256, 5) k_eta_update(const StepParams P, int n
 // instances take the plane range and key offsets from P; the whole-domain
 // instances keep them compile-time (the runtime range cost this kernel's
 // schedule 85% at 128 registers).
-template <int DIM, bool FAST, int NCAP, bool SLAB = false>
-__device__ __forceinline__ void eta_march_body(const StepParams& P, int n, const double* __restrict__ eta,
-                                               const double* __restrict__ p, double* __restrict__ eta_next,
-                                               double* __restrict__ gb_next, double* __restrict__ s2_next,
-                                               Status* st, int bx, int by, int bz) {
-    if (st->failed) return;
+// One march of a thread's column with the division policy of DM (DivOf);
+// returns the flag of numerators outside the exact-division range (DM 1).
+template <int DIM, int DM, int NCAP, bool SLAB>
+__device__ __forceinline__ unsigned eta_march_pass(const StepParams& P, int n, const double* __restrict__ eta,
+                                                   const double* __restrict__ p, double* __restrict__ eta_next,
+                                                   double* __restrict__ gb_next, double* __restrict__ s2_next,
+                                                   int row, int col, int i0, int i1, unsigned long long& errkey) {
     const Grid& g = P.g;
-    const int col = bx * blockDim.x + threadIdx.x;
-    const int row = DIM == 3 ? by * blockDim.y + threadIdx.y : 0;
-    if (col >= g.nb || row >= g.na) return;
-    const int i0 = (SLAB ? P.x_lo : 0) + bz * P.xchunk, i1 = min(SLAB ? P.x_hi : g.nx, i0 + P.xchunk);
+    unsigned dbad = 0;
+    const typename DivOf<DM>::T dv{P, dbad};
     const long long rc = (long long)row * g.pb + col;
     const long long cbm = (long long)row * g.pb + (col == 0 ? g.nb - 1 : col - 1);
     const long long cbp = (long long)row * g.pb + (col == g.nb - 1 ? 0 : col + 1);
@@ -643,7 +781,6 @@ __device__ __forceinline__ void eta_march_body(const StepParams& P, int n, const
             }
         }
     }
-    unsigned long long errkey = ERR_NONE;
     for (int x = i0; x < i1; ++x) {
         const long long base = (long long)x * g.plane;
         const long long bnext = (long long)(x < g.nx - 1 ? x + 1 : x) * g.plane;
@@ -665,12 +802,10 @@ __device__ __forceinline__ void eta_march_body(const StepParams& P, int n, const
             const double c0 = ec[q];
             double lap;
             if (DIM == 3)
-                lap = fdiv<FAST>((en[q] - 2. * c0 + ep[q]), P.v_dxdx)
-                    + fdiv<FAST>((__ldg(e + cap) - 2. * c0 + __ldg(e + cam)), P.v_dada)
-                    + fdiv<FAST>((__ldg(e + cbp) - 2. * c0 + __ldg(e + cbm)), P.v_dbdb);
+                lap = dv.dvxx((en[q] - 2. * c0 + ep[q])) + dv.dvaa((__ldg(e + cap) - 2. * c0 + __ldg(e + cam)))
+                    + dv.dvbb((__ldg(e + cbp) - 2. * c0 + __ldg(e + cbm)));
             else
-                lap = fdiv<FAST>((en[q] - 2. * c0 + ep[q]), P.v_dxdx)
-                    + fdiv<FAST>((__ldg(e + cbp) - 2. * c0 + __ldg(e + cbm)), P.v_dbdb);
+                lap = dv.dvxx((en[q] - 2. * c0 + ep[q])) + dv.dvbb((__ldg(e + cbp) - 2. * c0 + __ldg(e + cbm)));
             const double force = grain_deta(c0, S, phi, P.eta_W, P.eta_A) - P.eta_K * lap;
             const double v = c0 - P.dt_etaL * force;
             bad |= (!isfinite(v) || v < -1.e-12 || v > 1. + 1.e-12) ? (1u << q) : 0u;
@@ -688,6 +823,41 @@ __device__ __forceinline__ void eta_march_body(const StepParams& P, int n, const
 #pragma unroll
         for (int q = 0; q < NCAP; ++q)
             if (q < n) { ep[q] = ec[q]; ec[q] = en[q]; }
+    }
+    return dbad;
+}
+
+// X-marching form of the eta update for a compile-time number of fields N:
+// each thread owns one (row, col) column of a chunk of planes and keeps
+// eta(x-1), eta(x), eta(x+1) of its column in registers, so each field value
+// is read from HBM once; the four in-plane neighbours come from L1 (they are
+// the neighbouring threads' own loads). All N loads of the next plane are
+// issued before the arithmetic of the current plane.
+// NCAP is the register capacity; the first n <= NCAP fields are updated (the
+// stand-alone kernel instantiates NCAP = n, so the guards fold away). SLAB
+// instances take the plane range and key offsets from P; the whole-domain
+// instances keep them compile-time (the runtime range cost this kernel's
+// schedule 85% at 128 registers). In the drop-in form a column whose
+// numerators left the exact-division range is marched again with every
+// quotient exact before its key is merged (its trial values rewritten).
+template <int DIM, bool FAST, int NCAP, bool SLAB = false>
+__device__ __forceinline__ void eta_march_body(const StepParams& P, int n, const double* __restrict__ eta,
+                                               const double* __restrict__ p, double* __restrict__ eta_next,
+                                               double* __restrict__ gb_next, double* __restrict__ s2_next,
+                                               Status* st, int bx, int by, int bz) {
+    if (st->failed) return;
+    const Grid& g = P.g;
+    const int col = bx * blockDim.x + threadIdx.x;
+    const int row = DIM == 3 ? by * blockDim.y + threadIdx.y : 0;
+    if (col >= g.nb || row >= g.na) return;
+    const int i0 = (SLAB ? P.x_lo : 0) + bz * P.xchunk, i1 = min(SLAB ? P.x_hi : g.nx, i0 + P.xchunk);
+    unsigned long long errkey = ERR_NONE;
+    if (FAST) {
+        eta_march_pass<DIM, 0, NCAP, SLAB>(P, n, eta, p, eta_next, gb_next, s2_next, row, col, i0, i1, errkey);
+    } else if (eta_march_pass<DIM, 1, NCAP, SLAB>(P, n, eta, p, eta_next, gb_next, s2_next, row, col, i0, i1,
+                                                   errkey)) {
+        errkey = ERR_NONE;
+        eta_march_pass<DIM, 2, NCAP, SLAB>(P, n, eta, p, eta_next, gb_next, s2_next, row, col, i0, i1, errkey);
     }
     if (errkey != ERR_NONE) atomicMin(SLAB ? err_word(P, st) : &st->err_key, errkey);
 }
@@ -1239,22 +1409,37 @@ static int step_minb() {
 }
 static int step_minb_for(const StepParams& P) { return P.minb == 2 || P.minb == 3 ? P.minb : step_minb(); }
 
+// CTAs per SM of the recomputation kernel (its grid strides over the step grid)
+constexpr int kRedoCtasPerSm = 2;
+
 template <int MINB, bool FAST>
 static void launch_step3(const StepParams& P, const double* o, const double* cr, const double* p, const double* gb,
                          const double* s2, double* on, double* crn, double* pn, StepPartial* partials, Status* st,
                          cudaStream_t stream, int* nblocks_out) {
     using T = Tile<3, TA3, TB3>;
     const dim3 grid = step_grid<3, TA3, TB3>(P);
+    const int nblocks = (int)(grid.x * grid.y * grid.z);
+    const int gredo = std::min(nblocks, kRedoCtasPerSm * 148);
     if (P.err_slot >= 0) {   // an X slab
         ensure_smem_attr((const void*)k_step_main<3, TA3, TB3, MINB, FAST, true>, (int)T::SMEM_BYTES);
         k_step_main<3, TA3, TB3, MINB, FAST, true><<<grid, dim3(TB3, TA3), T::SMEM_BYTES, stream>>>(
             P, o, cr, p, gb, s2, on, crn, pn, partials, st);
+        if constexpr (!FAST) {
+            ensure_smem_attr((const void*)k_step_redo<3, TA3, TB3, true>, (int)T::SMEM_BYTES);
+            k_step_redo<3, TA3, TB3, true><<<gredo, dim3(TB3, TA3), T::SMEM_BYTES, stream>>>(
+                P, o, cr, p, gb, s2, on, crn, pn, partials, st, (int)grid.x, (int)grid.y, nblocks);
+        }
     } else {
         ensure_smem_attr((const void*)k_step_main<3, TA3, TB3, MINB, FAST>, (int)T::SMEM_BYTES);
         k_step_main<3, TA3, TB3, MINB, FAST><<<grid, dim3(TB3, TA3), T::SMEM_BYTES, stream>>>(P, o, cr, p, gb, s2, on,
                                                                                              crn, pn, partials, st);
+        if constexpr (!FAST) {
+            ensure_smem_attr((const void*)k_step_redo<3, TA3, TB3>, (int)T::SMEM_BYTES);
+            k_step_redo<3, TA3, TB3><<<gredo, dim3(TB3, TA3), T::SMEM_BYTES, stream>>>(
+                P, o, cr, p, gb, s2, on, crn, pn, partials, st, (int)grid.x, (int)grid.y, nblocks);
+        }
     }
-    if (nblocks_out) *nblocks_out = (int)(grid.x * grid.y * grid.z);
+    if (nblocks_out) *nblocks_out = nblocks;
 }
 
 template <bool FAST>
@@ -1269,7 +1454,12 @@ static void launch_step_form(const StepParams& P, const double* o, const double*
         const dim3 grid = step_grid<2, TA2, TB2>(P);
         k_step_main<2, TA2, TB2, 4, FAST><<<grid, dim3(TB2, TA2), T::SMEM_BYTES, stream>>>(P, o, cr, p, gb, s2, on,
                                                                                           crn, pn, partials, st);
-        if (nblocks_out) *nblocks_out = (int)(grid.x * grid.y * grid.z);
+        const int nblocks = (int)(grid.x * grid.y * grid.z);
+        if constexpr (!FAST)
+            k_step_redo<2, TA2, TB2><<<std::min(nblocks, kRedoCtasPerSm * 148), dim3(TB2, TA2), T::SMEM_BYTES,
+                                       stream>>>(P, o, cr, p, gb, s2, on, crn, pn, partials, st, (int)grid.x,
+                                                 (int)grid.y, nblocks);
+        if (nblocks_out) *nblocks_out = nblocks;
     }
 }
 

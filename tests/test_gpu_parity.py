@@ -176,3 +176,27 @@ def test_fast_form_deviation_from_drop_in(require_gpu, dim, mode):
         a, b = fast.get(n), exact.get(n)
         err = np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300)
         assert err <= 1e-10, (n, err)
+
+
+@pytest.mark.parametrize("dim,mode,step_form", [(2, "static", 0), (3, "static", 0), (3, "evolving", 0),
+                                                (3, "evolving", 1)])
+def test_tiny_and_subnormal_numerators(require_gpu, dim, mode, step_form):
+    """O falling through every magnitude from 1e-3 to below the subnormals along
+    X, and phi from 1e-50 to 1e-110 along the rows (h(phi) down to ~1e-330):
+    flux, Laplacian and Ck numerators leave the exact-division range (biased
+    exponent 123..1923) in most CTAs, whose chunks the drop-in form marches a
+    second time with IEEE division for those; fields stay bit-identical."""
+    shape = SHAPES[dim][1]
+    cfg = cfg_for(dim, shape, bc="concentration", ck="legacy", nucleation="off", step_form=step_form,
+                  **MODES[mode])
+    sol, orc = nicr.Solver(cfg), Oracle(cfg)
+    o, cr, p, eta = smooth_fields(orc.shape, orc.neta, seed=7)
+    idx = np.indices(orc.shape).astype(float)
+    o = o * 10.0 ** (-330.0 * idx[0] / orc.shape[0])
+    p = 10.0 ** (-50.0 - 60.0 * idx[1] / orc.shape[1])
+    orc.set_fields(o, cr, p, np.array(eta) if eta else None)
+    sol.set_fields(o, cr, p, eta if eta else None)
+    for _ in range(6):
+        assert orc.step() == 0, orc.error()
+        sol.step(1)
+    compare_state(sol, orc)
