@@ -95,9 +95,9 @@ typedef struct nicr_config {
     int reserved[3];
 } nicr_config;
 
-/* nicr_config.step_form. AUTO takes the one-pass kernel for the reciprocal
- * form (NICR_FP64_FAST) and the two kernels for the drop-in form, the faster
- * of each on B200; the environment variable NICR_STEP_FORM=onepass|split
+/* nicr_config.step_form. AUTO takes the one-pass kernel wherever the grid
+ * allows it (the faster form in both arithmetic forms on B200) and the two
+ * kernels elsewhere; the environment variable NICR_STEP_FORM=onepass|split
  * overrides every handle of the process (benchmarks). */
 enum { NICR_STEP_AUTO = 0, NICR_STEP_ONEPASS = 1, NICR_STEP_SPLIT = 2 };
 

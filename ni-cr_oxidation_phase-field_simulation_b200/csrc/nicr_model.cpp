@@ -903,7 +903,7 @@ bool Model::onepass_step() const {
         env = (e && e[0] == 'o') ? NICR_STEP_ONEPASS : (e && e[0] == 's') ? NICR_STEP_SPLIT : 0;
     }
     const int form = env ? env : c.step_form;
-    const bool want = form == NICR_STEP_ONEPASS || (form == NICR_STEP_AUTO && sp.fast);
+    const bool want = form != NICR_STEP_SPLIT;
     return want && !onepass_failed && dim == 3 && advance_eta && !is_slab && !fused_step() &&
            step_fused_applies(g, neta);
 }

@@ -95,58 +95,63 @@ inline EtaCoef eta_coef(double fwhm, double dx, double W, double kappa, double p
 // The host stores y = RN(1/b) and the double-word reciprocal zh = RD(1/b),
 // zl = RN(1/b - zh) >= 0 (Brisebarre, Muller, Raina, "Accelerating correctly
 // rounded floating-point division when the divisor is known in advance",
-// IEEE Trans. Comput. 53(8), 2004). For b > 0 with 2^-60 <= b <= 2^60 and a
-// numerator of biased exponent 123..1923:
-//   q0 = RN(a*zh + RN(a*zl))   within (1/2 + 2^-51) ulp of a/b,
-//   e  = q0*b - a              exact, because q0 is within one ulp of a/b,
-//   q  = RN(q0 - e*y)          = RN(a/b),
-// the last line being Markstein's correction theorem (IBM J. Res. Dev. 34(1),
-// 1990: q0 within one ulp of a/b and y within half an ulp of 1/b make
-// RN(q0 + r*y), r = a - b*q0, the correctly rounded quotient). The exponent
-// range keeps every intermediate normal and the quotient in [2^-961, 2^961].
+// IEEE Trans. Comput. 53(8), 2004), the latter two scaled by 2^128. For b > 0
+// with 2^-60 <= b <= 2^60 and a numerator a:
+//   as = a * 2^128                  exact for |a| < 2^895, subnormals included,
+//   q0 = RN(a*zh' + RN(a*zl'))      within (1/2 + 2^-51) ulp of as/b,
+//   e  = q0*b - as                  exact: q0 is within one ulp of as/b, and
+//                                   as/b >= 2^-1006 keeps its bits normal,
+//   qs = RN(q0 - e*y)               = RN(as/b), Markstein's correction theorem
+//                                   (IBM J. Res. Dev. 34(1), 1990: q0 within one
+//                                   ulp, y within half an ulp of 1/b, exact
+//                                   remainder => the correctly rounded quotient),
+//   q  = qs * 2^-128                exact whenever a/b is normal or zero.
+// The scaling keeps tiny numerators (the tails of diffusing fields) exact.
 // Zeros come out with the IEEE sign because zl >= 0 and e is formed as
-// q0*b - a (+0 for a = +-0, b > 0). Any other numerator (subnormal, tiny,
-// huge, infinite, NaN) and every numerator of a divisor outside the range
-// take the IEEE division. tests/division_check.c restates this on the host
-// and checks it against IEEE division, near-midpoint quotients included.
+// q0*b - as. A quotient that is subnormal (qs nonzero below 2^-894, which the
+// final scaling would round a second time), infinite or NaN (infinite, NaN or
+// huge numerators), or any quotient of a divisor outside the range, is
+// flagged. tests/division_check.c restates this on the host and checks it
+// against IEEE division, near-midpoint quotients included.
 struct DivC {
     double b, rb;      // divisor and y = RN(1/b) (the reciprocal form multiplies by it)
-    double zh, zl;     // RD(1/b) and RN(1/b - RD(1/b))
-    unsigned erange;   // 1801 << 20 when b is in range, else 0 (no numerator passes)
-    unsigned gate;     // 0 when b is in range, else 1 (zeros take the IEEE division too)
+    double zh, zl;     // 2^128 RD(1/b) and 2^128 RN(1/b - RD(1/b))
+    unsigned gate;     // 0 when b is in range, else 1 (every quotient flagged)
+    unsigned pad;
 };
 inline DivC make_divc(double b) {
     DivC d;
     d.b = b;
     d.rb = 1.0 / b;
-    d.zh = d.rb;
-    double rem = std::fma(-d.zh, b, 1.0);   // exact: zh is within one ulp of 1/b
+    double zh = d.rb;
+    double rem = std::fma(-zh, b, 1.0);   // exact: zh is within one ulp of 1/b
     if (rem < 0.) {
-        d.zh = std::nextafter(d.zh, 0.0);
-        rem = std::fma(-d.zh, b, 1.0);
+        zh = std::nextafter(zh, 0.0);
+        rem = std::fma(-zh, b, 1.0);
     }
-    d.zl = rem / b;
+    d.zh = std::ldexp(zh, 128);
+    d.zl = std::ldexp(rem / b, 128);
     const bool in_range = std::isnormal(b) && b > 0. && b >= std::ldexp(1.0, -60) && b <= std::ldexp(1.0, 60);
-    d.erange = in_range ? 0x70900000u : 0u;
     d.gate = in_range ? 0u : 1u;
+    d.pad = 0;
     return d;
 }
 #ifdef __CUDACC__
 // IEEE division kept out of line: it is only the rare fallback, and inlining
 // it at every call site would multiply the kernels' instruction footprint.
 __device__ __noinline__ double ieee_div(double a, double b);
-// The exact quotient for numerators in the guarded range; any other numerator
-// sets `bad` (the value returned for it is then not the IEEE quotient), so a
-// caller can test once for a whole group of divisions and recompute the group
-// with IEEE division.
+// The exact quotient; a flagged one (see DivC) sets `bad` (the value returned
+// for it is then not the IEEE quotient), so a caller can test once for a
+// whole group of divisions and recompute the group with IEEE division.
 __device__ __forceinline__ double xdiv_flag(double a, const DivC& d, unsigned& bad) {
-    const unsigned h = (unsigned)__double2hiint(a) & 0x7FFFFFFFu, lo = (unsigned)__double2loint(a);
+    const double as = __dmul_rn(a, 0x1p128);
     const double q0 = __fma_rn(a, d.zh, __dmul_rn(a, d.zl));
-    const double e = __fma_rn(q0, d.b, -a);
-    const double q = __fma_rn(-e, d.rb, q0);
-    // biased exponent 123..1923 (h in [123 << 20, 1924 << 20)), or a zero
-    bad |= ((h - 0x07B00000u) < d.erange || (h | lo | d.gate) == 0u) ? 0u : 1u;
-    return q;
+    const double e = __fma_rn(q0, d.b, -as);
+    const double qs = __fma_rn(-e, d.rb, q0);
+    // |qs| in (0, 2^-894): a subnormal quotient; >= 2^1024: infinite or NaN
+    const unsigned u = (unsigned)__double2hiint(qs) & 0x7FFFFFFFu;
+    bad |= ((u - 1u) < 0x080FFFFFu || u >= 0x7FF00000u || d.gate) ? 1u : 0u;
+    return __dmul_rn(qs, 0x1p-128);
 }
 __device__ __forceinline__ double xdiv(double a, const DivC& d) {
     unsigned bad = 0;

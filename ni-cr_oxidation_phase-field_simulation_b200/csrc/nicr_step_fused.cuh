@@ -129,13 +129,19 @@ struct OnePassStep {
         }
     }
 
-    __device__ static void run(const StepParams& P, const CUtensorMap* m_int, const CUtensorMap* m_row,
-                               const CUtensorMap* m_col, const CUtensorMap* m_crn, const double* __restrict__ o,
-                               const double* __restrict__ cr, const double* __restrict__ p, double* __restrict__ on,
-                               double* __restrict__ crn, double* __restrict__ pn, double* __restrict__ eta_next,
-                               StepPartial* __restrict__ partials, Status* st) {
+    // One march over the CTA's chunk with the division policy of DM (DivOf).
+    // kb offsets the staging ring's plane counter (slot and phase of each
+    // copy), so a second march continues the mbarrier phases of the first;
+    // DM 1 returns true, without publishing keys or partials, when a
+    // numerator of the chunk left the exact-division range.
+    template <int DM>
+    __device__ static bool run_body(const StepParams& P, const CUtensorMap* m_int, const CUtensorMap* m_row,
+                                    const CUtensorMap* m_col, const CUtensorMap* m_crn, const double* __restrict__ o,
+                                    const double* __restrict__ cr, const double* __restrict__ p,
+                                    double* __restrict__ on, double* __restrict__ crn, double* __restrict__ pn,
+                                    double* __restrict__ eta_next, StepPartial* __restrict__ partials, Status* st,
+                                    unsigned long long* bars, int kb) {
         extern __shared__ __align__(128) unsigned char fused_smem[];
-        __shared__ unsigned long long bars[L::RING];
         double* smem = reinterpret_cast<double*>(fused_smem);
         double* so = smem;                 // 4 slots x S2
         double* scr = so + 4 * T::S2;      // 4 slots x S2
@@ -151,7 +157,9 @@ struct OnePassStep {
         double* ering = reinterpret_cast<double*>(
             fused_smem + L::STEP_BYTES + ((128u - (smem_u32(fused_smem + L::STEP_BYTES) & 127u)) & 127u));
 
-        if (st->failed) return;   // a previous step of this batch was rejected
+        if (st->failed) return false;   // a previous step of this batch was rejected
+        unsigned dbad = 0;
+        const typename DivOf<DM>::T dv{P, dbad};
 
         const bool o_on = MODE == 1 ? true : P.o_on != 0;
         const bool ck_legacy = MODE == 1 ? true : P.ck == 0;
@@ -167,7 +175,7 @@ struct OnePassStep {
         // lives in slot (q - i0 + 1) % 3; planes i0-1 .. i1 are staged once each
         const int ytop = a0 == 0 ? g.na - 1 : a0 - 1, ybot = a0 + TA == g.na ? 0 : a0 + TA;
         const int xl = b0 == 0 ? g.nb - 2 : b0 - 2, xr = b0 + TB == g.nb ? 0 : b0 + TB;
-        auto eslot = [&](int q) { return ering + (size_t)((q - i0 + 1) % L::RING) * L::SLOT; };
+        auto eslot = [&](int q) { return ering + (size_t)((q - i0 + 1 + kb) % L::RING) * L::SLOT; };
         // the last warp: lane 0 registers the slot's bytes on its mbarrier, then
         // lane q < N copies field q's five boxes and lanes N .. N+3 the corners
         auto issue = [&](int q) {
@@ -175,7 +183,7 @@ struct OnePassStep {
             if (lane < 0) return;
             const int xg = q < 0 ? 0 : (q > g.nx - 1 ? g.nx - 1 : q);
             double* s = eslot(q);
-            unsigned long long* bar = &bars[(q - i0 + 1) % L::RING];
+            unsigned long long* bar = &bars[(q - i0 + 1 + kb) % L::RING];
             if (lane == 0) {
                 asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
                 mbar_expect_tx(bar, L::TX_BYTES);
@@ -195,13 +203,13 @@ struct OnePassStep {
         };
         bool ok = true;
         auto wait = [&](int q) {
-            const int k = q - i0 + 1;
+            const int k = q - i0 + 1 + kb;
             const unsigned parity = (unsigned)((k / L::RING) & 1);
             unsigned long long* bar = &bars[k % L::RING];
             for (long long it = 0; ok && !mbar_try_wait(bar, parity); ++it)
                 if (it > kTmaWaitLimit) ok = false;
         };
-        if (tid == 0) {
+        if (tid == 0 && kb == 0) {
             for (int r = 0; r < L::RING; ++r) mbar_init(&bars[r], 1);
             asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
         }
@@ -245,14 +253,14 @@ struct OnePassStep {
             double* mC = smuCr + (x & 1) * T::S1;
             double* mo_ = smo + (x & 1) * T::S1;
             double* mc_ = smc + (x & 1) * T::S1;
-            CenterVals own = SK::lead_point(P, nullptr, som, so0, sop, scm, sc0, scp, spx, mO, mC, mo_, mc_, ta, tb,
-                                            gbl[0]);
+            CenterVals own = SK::lead_core(dv, P, o_on, som, so0, sop, scm, sc0, scp, spx, mO, mC, mo_, mc_, ta, tb,
+                                           gbl[0]);
             if (offs.gl[1] >= 0) {
                 double Sr;
                 gbl[1] = mask_at(P, es, ring_o, ring_s, Sr);
                 int a, b;
                 SK::ring_point(tid, a, b);
-                SK::lead_point(P, nullptr, som, so0, sop, scm, sc0, scp, spx, mO, mC, mo_, mc_, a, b, gbl[1]);
+                SK::lead_core(dv, P, o_on, som, so0, sop, scm, sc0, scp, spx, mO, mC, mo_, mc_, a, b, gbl[1]);
             }
             return own;
         };
@@ -272,8 +280,8 @@ struct OnePassStep {
             const CenterVals C = lead(0, s2u, gbu);
             __syncthreads();
             const double muOg = (P.bc == 1 && o_on) ? 2. * P.mu_res - C.muO : C.muO;
-            FxO = fdiv<FAST>(-.5 * (C.mo + C.mo) * (C.muO - muOg), P.v_dx);
-            FxCr = fdiv<FAST>(-.5 * (C.mc + C.mc) * (C.muCr - C.muCr), P.v_dx);
+            FxO = dv.dvx(-.5 * (C.mo + C.mo) * (C.muO - muOg));
+            FxCr = dv.dvx(-.5 * (C.mc + C.mc) * (C.muCr - C.muCr));
             pP = C.p;
             // the x = 0 face of plane 0 and the inlet's budget term, here rather
             // than in the march: left_flux (3S:621-628), the surface-mobility
@@ -282,10 +290,10 @@ struct OnePassStep {
                 double lf = 0.;
                 if (o_on) {
                     const double mf = mobility(P.surface_c_ref, h(C.p), gbu, Phys::bmo, Phys::boo, P.gbm1_o);
-                    lf = fdiv<FAST>(2. * mf * (P.mu_res - C.muO), P.v_dx);
+                    lf = dv.dvx(2. * mf * (P.mu_res - C.muO));
                 }
                 FxO = lf;
-                acc[4] = dd_add(acc[4], fdiv<FAST>(P.dt * lf, P.v_dx));
+                acc[4] = dd_add(acc[4], dv.dvx(P.dt * lf));
             }
             if (P.inlet) acc[4] = dd_add(acc[4], P.layer_o - __ldg(o + (long long)row * g.pb + col));
         } else {
@@ -303,8 +311,8 @@ struct OnePassStep {
             __syncthreads();
             const CenterVals C = lead(i0, s2u, gbu);
             __syncthreads();
-            FxO = fdiv<FAST>(-.5 * (Pv.mo + C.mo) * (C.muO - Pv.muO), P.v_dx);
-            FxCr = fdiv<FAST>(-.5 * (Pv.mc + C.mc) * (C.muCr - Pv.muCr), P.v_dx);
+            FxO = dv.dvx(-.5 * (Pv.mo + C.mo) * (C.muO - Pv.muO));
+            FxCr = dv.dvx(-.5 * (Pv.mc + C.mc) * (C.muCr - Pv.muCr));
             pP = Pv.p;
         }
         {
@@ -365,48 +373,15 @@ struct OnePassStep {
                     }
                 }
 
-                const double rightO = fdiv<FAST>(-.5 * (C.mo + Lv.mo) * (Lv.muO - C.muO), P.v_dx);
-                const double rightCr = fdiv<FAST>(-.5 * (C.mc + Lv.mc) * (Lv.muCr - C.muCr), P.v_dx);
-                const double leftO = FxO;
-
-                double divO = 0., divCr;
-                {
-                    const double mc0 = mc_[c1], mu0 = mC[c1];
-                    const double front = fdiv<FAST>(-.5 * (mc0 + mc_[bp]) * (mC[bp] - mu0), P.v_db);
-                    const double back = fdiv<FAST>(-.5 * (mc_[bm] + mc0) * (mu0 - mC[bm]), P.v_db);
-                    const double top = fdiv<FAST>(-.5 * (mc0 + mc_[ap]) * (mC[ap] - mu0), P.v_da);
-                    const double bottom = fdiv<FAST>(-.5 * (mc_[am] + mc0) * (mu0 - mC[am]), P.v_da);
-                    divCr = fdiv<FAST>(FxCr - rightCr, P.v_dx) + fdiv<FAST>(bottom - top, P.v_da) + fdiv<FAST>(back - front, P.v_db);
-                }
-                if (o_on) {
-                    const double m0 = mo_[c1], mu0 = mO[c1];
-                    const double front = fdiv<FAST>(-.5 * (m0 + mo_[bp]) * (mO[bp] - mu0), P.v_db);
-                    const double back = fdiv<FAST>(-.5 * (mo_[bm] + m0) * (mu0 - mO[bm]), P.v_db);
-                    const double top = fdiv<FAST>(-.5 * (m0 + mo_[ap]) * (mO[ap] - mu0), P.v_da);
-                    const double bottom = fdiv<FAST>(-.5 * (mo_[am] + m0) * (mu0 - mO[am]), P.v_da);
-                    divO = fdiv<FAST>(leftO - rightO, P.v_dx) + fdiv<FAST>(bottom - top, P.v_da) + fdiv<FAST>(back - front, P.v_db);
-                }
-                const double oo = C.o, cc = C.cr, pp = C.p;
-                double onv = o_on ? oo + P.dt * divO : oo;
-                double crv = cc + P.dt * divCr;
-                const double lapP = fdiv<FAST>((Lv.p - 2. * pp + pP), P.v_dxdx)
-                                  + fdiv<FAST>((spu[ap] - 2. * pp + spu[am]), P.v_dada)
-                                  + fdiv<FAST>((spu[bp] - 2. * pp + spu[bm]), P.v_dbdb);
-                const double hpv = 30. * pp * pp * (pp - 1.) * (pp - 1.);
-                double fp = Phys::W * (4. * pp * pp * pp - 6. * pp * pp + 2. * pp)
-                          + hpv * (foxide(oo, cc) - fmetal(oo, cc)) - 2. * Phys::kp * lapP;
-                fp += grain_dphi(s2u, pp, P.eta_W, P.eta_A);
-                double pnv = pp - P.dtL * fp;
-                // Ck, the trial test and the clamps without data-dependent branches
-                // (so the scheduler sees one block); the rare bookkeeping (budget
-                // terms of changed cells, failure keys) is one branch after the stores
-                double dO = 0., dCr = 0.;
-                if (ck_legacy) {
-                    const double hn = h(pnv);
-                    dO = fdiv<FAST>(-Phys::ckO * ((Phys::oxideO - onv) * hn - (Phys::oxideO - oo) * C.hh), P.v_dt);
-                    dCr = fdiv<FAST>(-Phys::ckCr * ((Phys::oxideCr - crv) * hn - (Phys::oxideCr - cc) * C.hh), P.v_dt);
-                    onv += dO; crv += dCr;
-                }
+                // fluxes, phi force and Ck (3S:761-811); the trial test and the
+                // clamps below without data-dependent branches (so the scheduler
+                // sees one block); the rare bookkeeping (budget terms of changed
+                // cells, failure keys) is one branch after the stores
+                const typename SK::CoreOut R = SK::cell_core(dv, P, o_on, ck_legacy, true, C, Lv, pP, FxO, FxCr, s2u,
+                                                             mO, mC, mo_, mc_, spu, c1, bp, bm, ap, am);
+                const double pp = C.p;
+                double onv = R.onv, crv = R.crv, pnv = R.pnv;
+                const double dO = R.dO, dCr = R.dCr, rightO = R.rightO, rightCr = R.rightCr;
                 const bool nonfinite = !isfinite(onv) || !isfinite(crv) || !isfinite(pnv);
                 double clO = 0., clCr = 0.;
                 bool outside = false;
@@ -450,9 +425,9 @@ struct OnePassStep {
                     for (int q = 0; q < N; ++q) {
                         const int fq = q * L::FS;
                         const double c0 = es[e_own + fq];
-                        const double lap = fdiv<FAST>((en[e_own + fq] - 2. * c0 + ep[q]), P.v_dxdx)
-                                         + fdiv<FAST>((es[ap_o + fq] - 2. * c0 + es[am_o + fq]), P.v_dada)
-                                         + fdiv<FAST>((es[bp_o + fq] - 2. * c0 + es[bm_o + fq]), P.v_dbdb);
+                        const double lap = dv.dvxx((en[e_own + fq] - 2. * c0 + ep[q]))
+                                         + dv.dvaa((es[ap_o + fq] - 2. * c0 + es[am_o + fq]))
+                                         + dv.dvbb((es[bp_o + fq] - 2. * c0 + es[bm_o + fq]));
                         const double force = grain_deta(c0, s2u, C.p, P.eta_W, P.eta_A) - P.eta_K * lap;
                         const double v = c0 - P.dt_etaL * force;
                         ebad |= (!isfinite(v) || v < -1.e-12 || v > 1. + 1.e-12) ? (1u << q) : 0u;
@@ -476,7 +451,7 @@ struct OnePassStep {
                 atomicOr(&st->timeout, 1);
                 // the last copy issued into each slot (earlier phases of a slot have completed)
                 for (int q = max(i0 - 1, issued - (L::RING - 1)); q <= issued; ++q) {
-                    const int k = q - i0 + 1;
+                    const int k = q - i0 + 1 + kb;
                     unsigned long long* bar = &bars[k % L::RING];
                     for (long long it = 0; it <= kTmaWaitLimit && !mbar_try_wait(bar, (unsigned)((k / L::RING) & 1));
                          ++it) {
@@ -484,14 +459,41 @@ struct OnePassStep {
                 }
             }
             __syncthreads();
-            return;
+            return false;
         }
+        if (DM == 1 && __syncthreads_or(dbad != 0)) return true;
         if (errkey != ERR_NONE) atomicMin(&st->err_key, errkey);
         block_reduce_dd<5>(acc, clipped, sdd, scnt);
         if (tid == 0) {
             StepPartial& out = partials[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)];
             for (int q = 0; q < 5; ++q) { out.s[q][0] = acc[q].hi; out.s[q][1] = acc[q].lo; }
             out.clipped = clipped;
+            out.redo = 0;
+        }
+        return false;
+    }
+
+    // The CTA's chunk. In the drop-in form a chunk whose numerators left the
+    // exact-division range is marched a second time with every quotient exact
+    // (IEEE division for those), rewriting its trial values, before keys and
+    // partials are published; the second march stages its planes after the
+    // i1 - i0 + 2 copies of the first, all of which the first has waited for.
+    __device__ static void run(const StepParams& P, const CUtensorMap* m_int, const CUtensorMap* m_row,
+                               const CUtensorMap* m_col, const CUtensorMap* m_crn, const double* __restrict__ o,
+                               const double* __restrict__ cr, const double* __restrict__ p, double* __restrict__ on,
+                               double* __restrict__ crn, double* __restrict__ pn, double* __restrict__ eta_next,
+                               StepPartial* __restrict__ partials, Status* st) {
+        // the staging ring's mbarriers: one array for both marches (declared in
+        // a march, each instantiation would have its own)
+        __shared__ unsigned long long bars[L::RING];
+        if (FAST) {
+            run_body<0>(P, m_int, m_row, m_col, m_crn, o, cr, p, on, crn, pn, eta_next, partials, st, bars, 0);
+        } else if (run_body<1>(P, m_int, m_row, m_col, m_crn, o, cr, p, on, crn, pn, eta_next, partials, st, bars,
+                               0)) {
+            const int i0 = blockIdx.z * P.xchunk, i1 = min(P.g.nx, i0 + P.xchunk);
+            __syncthreads();
+            run_body<2>(P, m_int, m_row, m_col, m_crn, o, cr, p, on, crn, pn, eta_next, partials, st, bars,
+                        i1 - i0 + 2);
         }
     }
 };

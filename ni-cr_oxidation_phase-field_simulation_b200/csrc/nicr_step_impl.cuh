@@ -140,14 +140,6 @@ template <int DM> struct DivOf;
 template <> struct DivOf<0> { using T = DivRun<true>; };
 template <> struct DivOf<1> { using T = DivRun<false>; };
 template <> struct DivOf<2> { using T = DivExact; };
-// The scalars the cell arithmetic reads besides the divisors.
-struct CellK {
-    double dt, dtL, eta_W, eta_A, eta_K, dt_etaL, gbm1_o, gbm1_cr;
-};
-__device__ __forceinline__ CellK cell_k(const StepParams& P) {
-    return CellK{P.dt, P.dtL, P.eta_W, P.eta_A, P.eta_K, P.dt_etaL, P.gbm1_o, P.gbm1_cr};
-}
-
 // The error word a launch with parameters P reports its first failing trial to.
 __device__ __forceinline__ unsigned long long* err_word(const StepParams& P, Status* st) {
     return P.err_slot < 0 ? &st->err_key : &st->slot_err[P.err_slot];
@@ -287,7 +279,7 @@ struct StepKernel {
 
     // mu and M at tile point (a,b) of real plane x; writes the mu/M slot.
     template <class Dv>
-    __device__ static CenterVals lead_core(const Dv& dv, const CellK& k, bool o_on, const double* som,
+    __device__ static CenterVals lead_core(const Dv& dv, const StepParams& k, bool o_on, const double* som,
                                            const double* so0, const double* sop, const double* scm, const double* sc0,
                                            const double* scp, const double* sp, double* smuO, double* smuCr,
                                            double* smo, double* smc, int a, int b, double gbv) {
@@ -317,18 +309,6 @@ struct StepKernel {
         smuO[c1] = v.muO; smuCr[c1] = v.muCr; smo[c1] = v.mo; smc[c1] = v.mc;
         return v;
     }
-    // lead_core with the per-division policy of the form (every quotient exact)
-    __device__ static CenterVals lead_point(const StepParams& P, const double* __restrict__ gb,
-                                            const double* som, const double* so0, const double* sop,
-                                            const double* scm, const double* sc0, const double* scp,
-                                            const double* sp, double* smuO, double* smuCr, double* smo,
-                                            double* smc, int a, int b, double gbv) {
-        unsigned bad = 0;
-        typename DivOf<FAST ? 0 : 2>::T dv{P, bad};
-        return lead_core(dv, cell_k(P), P.o_on != 0, som, so0, sop, scm, sc0, scp, sp, smuO, smuCr, smo, smc, a, b,
-                         gbv);
-    }
-
     // The flux divergence, phi force and Ck of the cell at (ta, tb) of plane u
     // (C: plane u, L: plane u+1, pP: phi of plane u-1, leftO/leftCr: its -X
     // face fluxes), before the trial test and the clamps.
@@ -336,7 +316,7 @@ struct StepKernel {
         double onv, crv, pnv, rightO, rightCr, dO, dCr;
     };
     template <class Dv>
-    __device__ static CoreOut cell_core(const Dv& dv, const CellK& k, bool o_on, bool ck_legacy, bool phi_eta,
+    __device__ static CoreOut cell_core(const Dv& dv, const StepParams& k, bool o_on, bool ck_legacy, bool phi_eta,
                                         const CenterVals& C, const CenterVals& L, double pP, double leftO,
                                         double leftCr, double s2u, const double* mO, const double* mC,
                                         const double* mo_, const double* mc_, const double* spu, int c1, int bp,
@@ -433,7 +413,6 @@ struct StepKernel {
         if (st->failed) return false;  // a previous step of this batch was rejected
         unsigned bad = 0;
         const typename DivOf<DM>::T dv{P, bad};
-        const CellK kc = cell_k(P);
 
         auto slot3 = [](int w) { return ((w % 3) + 3) % 3; };
         // o/cr ring of 4 planes: the plane staged at the top of an iteration
@@ -452,7 +431,7 @@ struct StepKernel {
             double* mC = smuCr + (x & 1) * T::S1;
             double* mo_ = smo + (x & 1) * T::S1;
             double* mc_ = smc + (x & 1) * T::S1;
-            CenterVals own = lead_core(dv, kc, P.o_on != 0, som, so0, sop, scm, sc0, scp, spx, mO, mC, mo_, mc_, ta,
+            CenterVals own = lead_core(dv, P, P.o_on != 0, som, so0, sop, scm, sc0, scp, spx, mO, mC, mo_, mc_, ta,
                                        tb, gbl[0]);
             // halo ring points: one per thread for the first S1-NT threads
             static_assert(T::S1 - T::NT <= T::NT, "ring larger than the CTA");
@@ -460,7 +439,7 @@ struct StepKernel {
             if (offs.gl[1] >= 0) {
                 int a, b;
                 ring_point(tid, a, b);
-                lead_core(dv, kc, P.o_on != 0, som, so0, sop, scm, sc0, scp, spx, mO, mC, mo_, mc_, a, b, gbl[1]);
+                lead_core(dv, P, P.o_on != 0, som, so0, sop, scm, sc0, scp, spx, mO, mC, mo_, mc_, a, b, gbl[1]);
             }
             return own;
         };
@@ -557,7 +536,7 @@ struct StepKernel {
                 // clamps below without data-dependent branches (so the scheduler
                 // sees one block); the rare bookkeeping (budget terms of changed
                 // cells, failure keys) is one branch after the stores
-                const CoreOut R = cell_core(dv, kc, P.o_on != 0, P.ck == 0, P.phi_eta != 0, C, L, pP, leftO, FxCr,
+                const CoreOut R = cell_core(dv, P, P.o_on != 0, P.ck == 0, P.phi_eta != 0, C, L, pP, leftO, FxCr,
                                             s2u, mO, mC, mo_, mc_, spu, c1, bp, bm, ap, am);
                 double onv = R.onv, crv = R.crv, pnv = R.pnv;
                 const double dO = R.dO, dCr = R.dCr, rightO = R.rightO, rightCr = R.rightCr;
@@ -674,13 +653,15 @@ dim3 step_grid(const StepParams& P) {
 // eta_trial (3S:514-526): v = eta - (dt*L_eta)*(deta - K*lap(eta)); must lie in
 // [-1e-12, 1+1e-12]. Writes the trial and the mask of the trial values (the
 // next step's gb and eta_s2, identical to rebuild_eta_mask on them).
-template <int DIM, bool FAST>
-__device__ __forceinline__ void eta_cell(const StepParams& P, int neta, const double* __restrict__ eta,
+template <int DIM, int DM>
+__device__ __forceinline__ unsigned eta_cell_pass(const StepParams& P, int neta, const double* __restrict__ eta,
                                          const double* __restrict__ s2, const double* __restrict__ p,
                                          double* __restrict__ eta_next, double* __restrict__ gb_next,
                                          double* __restrict__ s2_next, int x, int row, int col,
                                          unsigned long long& errkey) {
     const Grid& g = P.g;
+    unsigned dbad = 0;
+    const typename DivOf<DM>::T dv{P, dbad};
     const long long idx = (long long)x * g.plane + (long long)row * g.pb + col;
     const long long cell = ((long long)x * g.na + row) * g.nb + col + P.cell_off;
     const long long ixm = x > 0 ? idx - g.plane : idx, ixp = x < g.nx - 1 ? idx + g.plane : idx;
@@ -700,12 +681,10 @@ __device__ __forceinline__ void eta_cell(const StepParams& P, int neta, const do
         const double ec = __ldg(e + idx);
         double lap;
         if (DIM == 3)
-            lap = fdiv<FAST>((__ldg(e + ixp) - 2. * ec + __ldg(e + ixm)), P.v_dxdx)
-                + fdiv<FAST>((__ldg(e + iap) - 2. * ec + __ldg(e + iam)), P.v_dada)
-                + fdiv<FAST>((__ldg(e + ibp) - 2. * ec + __ldg(e + ibm)), P.v_dbdb);
+            lap = dv.dvxx((__ldg(e + ixp) - 2. * ec + __ldg(e + ixm))) + dv.dvaa((__ldg(e + iap) - 2. * ec + __ldg(e + iam)))
+                + dv.dvbb((__ldg(e + ibp) - 2. * ec + __ldg(e + ibm)));
         else
-            lap = fdiv<FAST>((__ldg(e + ixp) - 2. * ec + __ldg(e + ixm)), P.v_dxdx)
-                + fdiv<FAST>((__ldg(e + ibp) - 2. * ec + __ldg(e + ibm)), P.v_dbdb);
+            lap = dv.dvxx((__ldg(e + ixp) - 2. * ec + __ldg(e + ixm))) + dv.dvbb((__ldg(e + ibp) - 2. * ec + __ldg(e + ibm)));
         const double force = grain_deta(ec, S, phi, P.eta_W, P.eta_A) - P.eta_K * lap;
         const double v = ec - P.dt_etaL * force;
         const bool fail = !isfinite(v) || v < -1.e-12 || v > 1. + 1.e-12;
@@ -721,6 +700,28 @@ __device__ __forceinline__ void eta_cell(const StepParams& P, int neta, const do
                                  (unsigned long long)cell);
     s2_next[idx] = Sn;
     gb_next[idx] = P.eta_scale * smin(1., 16. * pairs);
+    return dbad;
+}
+// The cell's eta update with the division policy of the form; in the drop-in
+// form a cell whose numerators left the exact-division range is recomputed
+// with every quotient exact (its values rewritten, its key taken from the
+// recomputation).
+template <int DIM, bool FAST>
+__device__ __forceinline__ void eta_cell(const StepParams& P, int neta, const double* __restrict__ eta,
+                                         const double* __restrict__ s2, const double* __restrict__ p,
+                                         double* __restrict__ eta_next, double* __restrict__ gb_next,
+                                         double* __restrict__ s2_next, int x, int row, int col,
+                                         unsigned long long& errkey) {
+    if (FAST) {
+        eta_cell_pass<DIM, 0>(P, neta, eta, s2, p, eta_next, gb_next, s2_next, x, row, col, errkey);
+        return;
+    }
+    unsigned long long k = ERR_NONE;
+    if (eta_cell_pass<DIM, 1>(P, neta, eta, s2, p, eta_next, gb_next, s2_next, x, row, col, k)) {
+        k = ERR_NONE;
+        eta_cell_pass<DIM, 2>(P, neta, eta, s2, p, eta_next, gb_next, s2_next, x, row, col, k);
+    }
+    errkey = min(errkey, k);
 }
 
 // Bounds for 5 CTAs/SM (<= 51 registers, no spills): the load-latency-bound

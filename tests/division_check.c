@@ -1,30 +1,33 @@
 /* Host restatement of the device's correctly rounded division by a run
- * constant (xdiv in csrc/nicr_physics.h) and an exhaustive-style check of it
- * against IEEE division (x86-64 SSE2 double: correctly rounded).
+ * constant (xdiv_flag in csrc/nicr_physics.h) and an exhaustive-style check
+ * of it against IEEE division (x86-64 SSE2 double: correctly rounded).
  *
- * The method: the host stores y = RN(1/b), zh = RD(1/b) and zl = RN(1/b - zh)
- * (zl >= 0, so zh + zl = 1/b to ~2^-105 relative). For a numerator a with a
- * biased exponent in [123, 1923] (and b > 0, 2^-60 <= b <= 2^60):
- *     q0 = RN(a*zh + RN(a*zl))        within (1/2 + 2^-51) ulp of a/b
- *     e  = RN(q0*b - a)               exact (q0 within one ulp of a/b)
- *     q  = RN(q0 - e*y)               = RN(a/b)
- * the last line being one correction step of Markstein's theorem (IBM J. Res.
- * Dev. 34(1), 1990: q within one ulp of a/b, y within half an ulp of 1/b,
- * exact remainder => RN(q + r*y) = RN(a/b)); the double-word reciprocal for a
- * divisor known in advance follows Brisebarre, Muller and Raina (IEEE Trans.
- * Comput. 53(8), 2004). Zeros keep their sign because e is formed as
- * q0*b - a (never -0 for a = +-0) and zl >= 0. Every other numerator goes to
- * the IEEE division.
+ * The method: the host stores y = RN(1/b) and the double-word reciprocal
+ * zh = RD(1/b), zl = RN(1/b - zh) >= 0, the latter two scaled by 2^128. For
+ * b > 0 with 2^-60 <= b <= 2^60 and any numerator a:
+ *     as = a * 2^128                       exact for |a| < 2^895, subnormals included
+ *     q0 = RN(a*zh' + RN(a*zl'))           within (1/2 + 2^-51) ulp of as/b
+ *     e  = RN(q0*b - as)                   exact (q0 within one ulp; as/b >= 2^-1006)
+ *     qs = RN(q0 - e*y)                    = RN(as/b) (Markstein's correction theorem,
+ *                                           IBM J. Res. Dev. 34(1), 1990)
+ *     q  = qs * 2^-128                     exact when a/b is normal or zero
+ * (the double-word reciprocal of a divisor known in advance: Brisebarre,
+ * Muller, Raina, IEEE Trans. Comput. 53(8), 2004). Zeros keep their sign
+ * (zl >= 0, e formed as q0*b - as). The result is flagged, and the IEEE
+ * division taken, when qs is nonzero below 2^-894 (a subnormal quotient,
+ * which the final scaling would round a second time), infinite or NaN
+ * (infinite, NaN or huge numerators), or the divisor is out of range.
  *
- * Cases: random numerators over the whole guarded range, numerators whose
- * quotient lies within ~2^-104 relative of a rounding midpoint (built with
- * integer arithmetic, below) and their neighbours, signed zeros,
- * subnormals, huge and non-finite numerators; divisors with random
- * mantissas, mantissas of all ones, powers of two, near sqrt(2), and the
- * grid spacings and time steps of the solver's configurations.
+ * Cases: random numerators over the whole exponent range, subnormals among
+ * them, numerators whose quotient lies within ~2^-102 relative of a rounding
+ * midpoint (built with integer arithmetic, below) and their neighbours,
+ * signed zeros, infinities and NaN; divisors with random mantissas, mantissas
+ * of all ones, powers of two, near sqrt(2), above 1, and the grid spacings
+ * and time steps of the solver's configurations.
  *
  * Usage: division_check <cases per divisor> <seed>; prints
- * "checked N mismatches M" and exits 1 on any mismatch. */
+ * "checked N mismatches M fallbacks F near-midpoint H" and exits 1 on any
+ * mismatch. */
 #include <math.h>
 #include <stdint.h>
 #include <stdio.h>
@@ -40,16 +43,17 @@ static divc make(double b) {
     divc d;
     d.b = b;
     d.y = 1.0 / b;
-    d.zh = d.y;
-    double rem = fma(-d.zh, b, 1.0); /* exact: zh within one ulp of 1/b */
+    double zh = d.y;
+    double rem = fma(-zh, b, 1.0); /* exact: zh within one ulp of 1/b */
     if (rem < 0) {
-        d.zh = nextafter(d.zh, 0.0);
-        rem = fma(-d.zh, b, 1.0);
+        zh = nextafter(zh, 0.0);
+        rem = fma(-zh, b, 1.0);
     }
-    d.zl = rem / b;
+    d.zh = ldexp(zh, 128);
+    d.zl = ldexp(rem / b, 128);
     const int fast = isnormal(b) && b > 0 && b >= ldexp(1.0, -60) && b <= ldexp(1.0, 60);
-    d.erange = fast ? 0x70900000u : 0u;
     d.gate = fast ? 0u : 1u;
+    d.erange = 0;
     return d;
 }
 
@@ -64,17 +68,17 @@ static double from_bits(uint64_t u) {
     return x;
 }
 
-/* the device sequence; *fallback set when the numerator leaves the guarded range */
+/* the device sequence; *fallback set when the result is flagged */
 static double xdiv(double a, const divc* d, int* fallback) {
-    const uint64_t u = bits(a);
-    const unsigned h = (unsigned)(u >> 32) & 0x7FFFFFFFu, lo = (unsigned)u;
+    const double as = a * 0x1p128;
     const double t = a * d->zl;
     const double q0 = fma(a, d->zh, t);
-    const double e = fma(q0, d->b, -a);
-    const double q = fma(-e, d->y, q0);
-    const int ok = (h - 0x07B00000u) < d->erange || (h | lo | d->gate) == 0u;
-    *fallback = !ok;
-    return ok ? q : a / d->b;
+    const double e = fma(q0, d->b, -as);
+    const double qs = fma(-e, d->y, q0);
+    const unsigned u = (unsigned)(bits(qs) >> 32) & 0x7FFFFFFFu;
+    const int bad = (u - 1u) < 0x080FFFFFu || u >= 0x7FF00000u || d->gate;
+    *fallback = bad;
+    return bad ? a / d->b : qs * 0x1p-128;
 }
 
 static uint64_t s = 0x243F6A8885A308D3ull;
@@ -99,7 +103,7 @@ static void one(double a, const divc* d) {
     }
 }
 
-/* numerators whose quotient by b lies within ~2^-104 relative of a rounding
+/* numerators whose quotient by b lies within ~2^-102 relative of a rounding
  * midpoint: with b = B * 2^k (B odd), take M = delta / B mod 2^54 for a small
  * odd delta, kept when it has 54 bits (M odd, 2^53 <= M < 2^54); then
  * B * M = A * 2^54 + delta with A < B <= 2^53, and a = A (scaled) gives
@@ -118,13 +122,13 @@ static void near_midpoints(const divc* d, int n) {
     while (!(B & 1)) B >>= 1;
     const uint64_t inv = inverse_mod_2_54(B), mask = (1ull << 54) - 1;
     for (int i = 0; i < n; ++i) {
-        const long long delta = ((long long)(rnd() % 8) - 4) | 1;   /* -3, -1, 1, 3 */
+        const long long delta = ((long long)(rnd() % 32) - 16) | 1;   /* odd, -15 .. 15 */
         const uint64_t M = ((uint64_t)delta * inv) & mask;
         if (!(M >> 53)) continue;
         const __int128 num = (__int128)((unsigned __int128)B * M) - delta;
         if (num <= 0 || (num & ((((__int128)1) << 54) - 1)) != 0) continue;
         const uint64_t A = (uint64_t)(num >> 54);
-        const double a = ldexp((double)A, (int)(rnd() % 1600) - 800);
+        const double a = ldexp((double)A, (int)(rnd() % 2000) - 1100);
         ++hard;
         one(a, d);
         one(-a, d);
@@ -149,8 +153,11 @@ static void run_divisor(double b, long long n) {
         case 2: /* differences of nearby values: few significant bits */
             a = ldexp((double)(r >> 40), (int)(rnd() % 200) - 100);
             break;
-        default: /* the whole guarded range and beyond it */
-            a = ldexp(1.0 + (double)(r >> 12) * 0x1p-52, (int)(rnd() % 1960) - 980);
+        case 3: /* subnormals */
+            a = from_bits(r & 0x000FFFFFFFFFFFFFull);
+            break;
+        default: /* every exponent */
+            a = ldexp(1.0 + (double)(r >> 12) * 0x1p-52, (int)(rnd() % 2100) - 1075);
             break;
         }
         if (r & 1) a = -a;
@@ -180,8 +187,14 @@ int main(int argc, char** argv) {
         else m = 1.0 + (double)(rnd() >> 12) * 0x1p-52;
         run_divisor(ldexp(m, e), n);
     }
+    for (int k = 0; k < 4096; ++k) { /* many divisors, near-midpoint numerators only */
+        const divc d = make(ldexp(1.0 + (double)(rnd() >> 12) * 0x1p-52, (int)(rnd() % 121) - 60));
+        near_midpoints(&d, (int)(n / 4096 + 64));
+    }
     run_divisor(-3.0, n / 8); /* not guarded: the IEEE division throughout */
     run_divisor(0x1p-70, n / 8);
+    run_divisor(0x1.8p+40, n / 4); /* large divisors: subnormal quotients */
+    run_divisor(0x1.fffffffffffffp+59, n / 4);
     printf("checked %lld mismatches %lld fallbacks %lld near-midpoint %lld\n", checked, mism, fallbacks, hard);
     return mism ? 1 : 0;
 }

@@ -7,8 +7,8 @@ columns a multiple of 32).
   wrap of every halo box onto the tile itself), several tiles, 1 to 8 eta
   fields, the three boundary conditions, O off, Ck on and off, a stamp across
   both periodic seams and Ksp scans, graph-replayed runs.
-The handles ask for the one-pass form (nicr_config.step_form = 1); the
-default (AUTO) takes it for the reciprocal form only.
+The handles ask for the one-pass form (nicr_config.step_form = 1), which
+the default (AUTO) also takes wherever the grid allows it.
 
 * Against the two-kernel form (NICR_STEP_FORM=split) in child processes,
   with forced X chunks of 1, 3 and 7 planes (chunk prologues, chunk ends at

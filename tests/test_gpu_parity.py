@@ -178,25 +178,35 @@ def test_fast_form_deviation_from_drop_in(require_gpu, dim, mode):
         assert err <= 1e-10, (n, err)
 
 
-@pytest.mark.parametrize("dim,mode,step_form", [(2, "static", 0), (3, "static", 0), (3, "evolving", 0),
-                                                (3, "evolving", 1)])
-def test_tiny_and_subnormal_numerators(require_gpu, dim, mode, step_form):
+@pytest.mark.parametrize("dim,mode,step_form,shape", [(2, "static", 0, None), (3, "static", 0, None),
+                                                      (3, "evolving", 2, None), (3, "evolving", 1, (45, 32, 32))])
+def test_tiny_and_subnormal_numerators(require_gpu, dim, mode, step_form, shape):
     """O falling through every magnitude from 1e-3 to below the subnormals along
     X, and phi from 1e-50 to 1e-110 along the rows (h(phi) down to ~1e-330):
     flux, Laplacian and Ck numerators leave the exact-division range (biased
     exponent 123..1923) in most CTAs, whose chunks the drop-in form marches a
-    second time with IEEE division for those; fields stay bit-identical."""
-    shape = SHAPES[dim][1]
+    second time with IEEE division for those; fields stay bit-identical. The
+    last case runs the one-pass step kernel (rows a multiple of 16, columns of
+    32), the others the two-kernel form."""
+    import ctypes
+    shape = shape or SHAPES[dim][1]
+    extra = {"grain_diameter_grid": 26.} if step_form == 1 else {}   # <= 8 eta fields for the one pass
     cfg = cfg_for(dim, shape, bc="concentration", ck="legacy", nucleation="off", step_form=step_form,
-                  **MODES[mode])
+                  **MODES[mode], **extra)
     sol, orc = nicr.Solver(cfg), Oracle(cfg)
+    if step_form == 1:
+        assert 1 <= orc.neta <= 8, orc.neta
     o, cr, p, eta = smooth_fields(orc.shape, orc.neta, seed=7)
     idx = np.indices(orc.shape).astype(float)
     o = o * 10.0 ** (-330.0 * idx[0] / orc.shape[0])
     p = 10.0 ** (-50.0 - 60.0 * idx[1] / orc.shape[1])
     orc.set_fields(o, cr, p, np.array(eta) if eta else None)
     sol.set_fields(o, cr, p, eta if eta else None)
+    nicr.lib().nicr_profile(sol.h, 1)
     for _ in range(6):
         assert orc.step() == 0, orc.error()
         sol.step(1)
+    tot, cnt = ctypes.c_double(0), ctypes.c_longlong(0)
+    nicr.lib().nicr_profile_read(sol.h, 8, ctypes.byref(tot), ctypes.byref(cnt))   # the one-pass kernel
+    assert cnt.value == (6 if step_form == 1 else 0)
     compare_state(sol, orc)
