@@ -99,17 +99,17 @@ __device__ __forceinline__ double fdiv(double a, const DivC& d) {
 
 // Divisions of the cell arithmetic, as policies the shared arithmetic (lead
 // points, cell updates) is written against. DivRun<true>: the reciprocal form.
-// DivRun<false>: the exact quotient for numerators in the guarded range
-// (xdiv_flag), raising `bad` for any other numerator instead of branching, so
-// the march carries no branch or call per division; a CTA that raised it
-// marches its chunk again with DivExact before it publishes anything, so every
-// result is still the IEEE quotient.
+// DivRun<false>: the exact quotient (xdiv_flag), raising `bad` for the rare
+// quotients it cannot certify (subnormal, infinite or NaN, or a divisor out of
+// range) instead of branching, so the march carries no branch or call per
+// division; a CTA (or thread) that raised it marches again with DivExact
+// before it publishes anything, so every result is still the IEEE quotient.
 template <bool FAST>
 struct DivRun {
     const StepParams& P;
     unsigned& bad;
     __device__ double q(double v, const DivC& d) const {
-        if (FAST) return __dmul_rn(v, d.rb);
+        if (FAST) return v * d.rb;   // contracted into neighbouring adds where it can
         return xdiv_flag(v, d, bad);
     }
     __device__ double dvx(double v) const { return q(v, P.v_dx); }
