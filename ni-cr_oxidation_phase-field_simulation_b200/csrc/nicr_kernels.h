@@ -62,7 +62,7 @@ struct StepParams {
     Grid g;
     double dx, da, db, dt;       // spacing along X, rows, columns
     double dxdx, dada, dbdb;     // c.dx*c.dx etc. (lap denominators, 3S:193-195)
-    DivC v_dxdx, v_dada, v_dbdb, v_dx, v_da, v_db, v_dt;  // verified divisions by the same constants
+    DivC v_dxdx, v_dada, v_dbdb, v_dx, v_da, v_db, v_dt;  // exact divisions by the same constants
     double dtL;                  // dt * Physics::L
     double layer_o;
     double gbm1_o, gbm1_cr;      // gb_factor_o - 1, gb_factor_cr - 1
@@ -270,7 +270,7 @@ void launch_refresh(const StepParams& P, const double* o, const double* cr, cons
                     const double* gb, double* muO, double* muCr, double* mo, double* mc,
                     cudaStream_t stream);
 
-// Device self-check of the verified division: mismatches against IEEE a/b
+// Device self-check of the exact division: mismatches against IEEE a/b
 long long check_division(double b, long long n, unsigned long long seed, long long* tested);
 
 // ---- init --------------------------------------------------------------------
