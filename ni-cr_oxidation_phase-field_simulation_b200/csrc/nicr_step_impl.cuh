@@ -687,7 +687,7 @@ __device__ __forceinline__ unsigned eta_cell_pass(const StepParams& P, int neta,
             lap = dv.dvxx((__ldg(e + ixp) - 2. * ec + __ldg(e + ixm))) + dv.dvbb((__ldg(e + ibp) - 2. * ec + __ldg(e + ibm)));
         const double force = grain_deta(ec, S, phi, P.eta_W, P.eta_A) - P.eta_K * lap;
         const double v = ec - P.dt_etaL * force;
-        const bool fail = !isfinite(v) || v < -1.e-12 || v > 1. + 1.e-12;
+        const bool fail = !(v >= -1.e-12 && v <= 1. + 1.e-12);   // NaN fails both comparisons
         first_bad = (fail && first_bad < 0) ? q : first_bad;
         eta_next[(long long)q * g.nstore + idx] = v;
         const double sq = v * v;
@@ -809,7 +809,7 @@ __device__ __forceinline__ unsigned eta_march_pass(const StepParams& P, int n, c
                 lap = dv.dvxx((en[q] - 2. * c0 + ep[q])) + dv.dvbb((__ldg(e + cbp) - 2. * c0 + __ldg(e + cbm)));
             const double force = grain_deta(c0, S, phi, P.eta_W, P.eta_A) - P.eta_K * lap;
             const double v = c0 - P.dt_etaL * force;
-            bad |= (!isfinite(v) || v < -1.e-12 || v > 1. + 1.e-12) ? (1u << q) : 0u;
+            bad |= !(v >= -1.e-12 && v <= 1. + 1.e-12) ? (1u << q) : 0u;   // NaN fails both comparisons
             eta_next[(long long)q * g.nstore + base + rc] = v;
             const double sq = v * v;
             pairs += Sn * sq;
